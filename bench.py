@@ -1,0 +1,295 @@
+"""Benchmark: explicit MPM particle-steps/s on the B200.
+
+Workload (default): the 3D granular column collapse -- 200x100x50 hex8 cells
+of 0.01 m, MohrCoulomb (E=1e7, nu=0.3, phi=30, c=0, psi=0, rho=1800), USL,
+FLIP, frictional floor mu=0.4, dt=2e-6, 2x2x2 particles per cell in the block
+[0,1]x[0,1]x[0,0.5] (4,000,000 particles).  Synthetic seeded inputs.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on stdout (rank 0).  ``value`` is device-timed (CUDA events on
+the solver's stream, state resident in HBM); ``e2e`` goes through the public
+API with host arrays (load -> K steps -> read back); ``roofline`` reports the
+dominant kernel's algorithmic bytes per launch over its event-timed average
+duration; ``cpu_baseline`` times the CPU oracle on a bounded sample.
+Under torchrun (N>1) every rank runs an independent replica ("replicas
+only": the multi-GPU slab decomposition is not built), timing is the max over
+ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic bytes of the FP64 kernels, 3D MohrCoulomb USL:
+# per particle for the particle kernels, per node for the node kernel.
+BYTES_PER_PARTICLE = {
+    # x 24, cell 4, mass 8, v 24, volume 8, stress 48 read
+    "p2g": 116,
+    # read x u v 72, stress strain 96, F 72, volume density 16, cell 4,
+    # material 1, pvc 2, MC state 72; write x u v 72, stress strain 96,
+    # F 72, volume density 16, MC state 72
+    "g2p": 335 + 328,
+}
+BYTES_PER_ACTIVE_NODE = {
+    # read mass, momentum, forces 80, flags 5; write velocity, acceleration 48
+    "nodes_velocity": 133,
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--block", default="100,100,50", help="particle block in cells")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def dist_init(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """Sample nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[4:]))
+                except ValueError:
+                    continue
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r[1:5])
+                          if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_sample_problem():
+    """A bounded sample of the workload for the CPU oracle: the same column at
+    1/8 of its x-y footprint (mesh 50x25x50 cells, block 25x25x50 cells,
+    250,000 particles), same material, boundary conditions and step."""
+    from mpm_b200 import problems as P
+    return P.column_3d(shape=(50, 25, 50), block=(25, 25, 50))
+
+
+def time_cpu_oracle(seconds, warmup=1, max_steps=200):
+    """particle-steps/s of the CPU oracle (all host threads) on the sample."""
+    from oracle.oracle import build_oracle
+    prob = cpu_sample_problem()
+    threads = os.cpu_count() or 1
+    o = build_oracle(prob, nthreads=threads)
+    o.step(warmup)
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps:
+        o.step(1)
+        steps += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    rate = prob.nparticles * steps / dt
+    sample = (f"3D MohrCoulomb USL column, mesh 50x25x50 hex8, {prob.nparticles} particles "
+              f"(1/8 of the 4M footprint), {steps} steps after {warmup} warm-up, "
+              f"{dt:.1f} s wall, OpenMP {threads} threads")
+    return rate, threads, sample
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference CPU path (oracle port, the reference
+    cannot be built here) on the box's host cores."""
+    if rank != 0:
+        return
+    from oracle.oracle import build_oracle
+    prob = cpu_sample_problem()
+    threads = os.cpu_count() or 1
+    o = build_oracle(prob, nthreads=threads)
+    o.step(max(args.warmup, 1))
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    dt = time.perf_counter() - t0
+    rate = prob.nparticles * args.steps / dt
+    sample = (f"3D MohrCoulomb USL column, mesh 50x25x50 hex8, {prob.nparticles} particles, "
+              f"{args.steps} steps, OpenMP {threads} threads")
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": rate,
+        "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "3D granular column collapse, MohrCoulomb USL FP64 (sample)"},
+        "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world = dist_init(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    from mpm_b200 import problems as P
+    block = tuple(int(v) for v in args.block.split(","))
+    t0 = time.perf_counter()
+    prob = P.config_b(block=block)
+    dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
+    s = P.build_solver(prob, device=0 if world == 1 else 0)
+    setup_s = time.perf_counter() - t0
+    n = s.nparticles
+    s.step(args.warmup)
+    barrier(world)
+    clocks = Clocks(dev)
+    s.set_profiling(True)
+    launches0 = s.launch_count
+    ms = s.step_timed(args.steps)
+    launches = s.launch_count - launches0
+    prof = s.kernel_profile()
+    clk = clocks.stop()
+    s.set_profiling(False)
+    ms = max_over_ranks(ms, world)
+    value = world * n * args.steps / (ms / 1e3)
+
+    # end to end through the public API with host arrays
+    st = s.read()
+    h2d = sum(np.asarray(st[k]).nbytes for k in ("x", "u", "v", "stress", "strain", "F", "volume",
+                                                 "mass", "density", "cell", "material", "svars"))
+    barrier(world)
+    t1 = time.perf_counter()
+    s.load(st)
+    s.step(args.steps)
+    out = s.read()
+    e2e_s = max_over_ranks(time.perf_counter() - t1, world)
+    d2h = sum(np.asarray(out[k]).nbytes for k in out)
+    e2e = {"value": world * n * args.steps / e2e_s, "unit": "particle-steps/s",
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
+
+    # roofline of the dominant kernel
+    peak, peak_kind = measured_peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    name, (tot_ms, cnt) = dom
+    avg_s = tot_ms / max(cnt, 1) / 1e3
+    if name in BYTES_PER_PARTICLE:
+        bytes_launch = BYTES_PER_PARTICLE[name] * n
+    else:
+        bytes_launch = BYTES_PER_ACTIVE_NODE.get(name, 0) * prob.nnodes
+    achieved = bytes_launch / avg_s / 1e9
+    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_s * 1e3,
+                "traffic": None,
+                "kernel_shares": {k: v[0] / max(sum(x[0] for x in prof.values()), 1e-30)
+                                  for k, v in prof.items() if v[1]}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, threads, sample = time_cpu_oracle(args.cpu_sample_seconds)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+               "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"3D granular column collapse, MohrCoulomb USL FLIP FP64, "
+                                   f"200x100x50 hex8 dx=0.01, {n} particles",
+                       "particles": n, "nodes": prob.nnodes, "cells": prob.ncells,
+                       "dt": prob.analysis["dt"], "precision": "fp64",
+                       "l2": "state larger than L2 (no flush needed)",
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "setup_s": setup_s},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk, "kernels": {k: {"total_ms": v[0], "launches": v[1]}
+                                       for k, v in prof.items() if v[1]},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

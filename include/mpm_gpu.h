@@ -1,0 +1,183 @@
+/*
+ * mpm_gpu.h -- C ABI of the B200 explicit MPM step (libmpm_b200.so).
+ *
+ * Drop-in boundary for the explicit single-phase solver of geomechanics/mpm
+ * (MPMExplicit<Tdim> with the USF/USL schemes).  Plain pointers and sizes
+ * only; no C++ types, no exceptions cross this boundary.  Every call returns
+ * an mpm_status (0 = success); mpm_gpu_last_error() describes the last
+ * failure on a handle.  Host arrays passed in are copied before the call
+ * returns; read-back calls write into caller-allocated arrays.
+ *
+ * Reference interfaces replaced (paths in the geomechanics/mpm tree):
+ *   solver    include/solvers/mpm_explicit.tcc:24-199  MPMExplicit::solve
+ *             include/solvers/mpm_scheme/mpm_scheme.tcc:19-261 (USF/USL)
+ *   mesh      include/mesh/mesh.tcc:17-48, 211-256, 287-306 create nodes/cells
+ *   material  include/materials/material.h:97-106 Material<Tdim>::compute_stress
+ *             src/material.cc:30-53 factory keys LinearElastic2D/3D,
+ *             MohrCoulomb2D/3D with the JSON property names of
+ *             linear_elastic.tcc:20-24 and mohr_coulomb.tcc:9-71
+ *   BCs       include/loads_bcs/constraints.tcc:83-217 nodal velocity /
+ *             acceleration / friction constraints; mesh.tcc:1454-1467
+ *             particle velocity constraints
+ *   particles include/particles/particle.tcc:145-306 particle state (POD)
+ *
+ * Threading: one host thread per handle.  All device work of a handle runs
+ * on its own CUDA stream; mpm_gpu_step() returns once the steps are queued
+ * and their error word has been read (it synchronises the stream at the end
+ * of the call).
+ */
+#ifndef MPM_GPU_H
+#define MPM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mpm_gpu_solver* mpm_gpu_t;
+
+typedef enum {
+  MPM_OK = 0,
+  MPM_ERR_INVALID = -1,      /* bad argument or call order */
+  MPM_ERR_CUDA = -2,         /* a CUDA call failed */
+  MPM_ERR_OUTSIDE = -3,      /* particle(s) left the mesh, locate_particles on */
+  MPM_ERR_NONFINITE = -4,    /* NaN/Inf detected in particle state */
+  MPM_ERR_TIMEOUT = -5,      /* a bounded device wait gave up */
+  MPM_ERR_ALLOC = -6,        /* device allocation failed */
+  MPM_ERR_UNSUPPORTED = -7   /* feature outside the implemented path */
+} mpm_status;
+
+enum { MPM_SCHEME_USF = 0, MPM_SCHEME_USL = 1 };
+enum { MPM_VELOCITY_FLIP = 0, MPM_VELOCITY_PIC = 1 };
+enum { MPM_PRECISION_FP64 = 0, MPM_PRECISION_MIXED = 1 };
+
+/* Analysis settings (mpm_base.tcc:3-207; mpm_explicit.tcc:8-13, 145-153). */
+typedef struct {
+  int32_t dim;              /* 2 (quad4 / ED2Q4) or 3 (hex8 / ED3H8) */
+  int32_t scheme;           /* MPM_SCHEME_USF / MPM_SCHEME_USL */
+  int32_t velocity_update;  /* MPM_VELOCITY_FLIP / MPM_VELOCITY_PIC */
+  int32_t precision;        /* MPM_PRECISION_FP64 / MPM_PRECISION_MIXED */
+  double blending_ratio;    /* velocity_update_settings.blending_ratio */
+  double dt;
+  double damping_factor;    /* damping {type: Cundall, damping_factor} */
+  double gravity[3];
+  double gravity_ramping_time;
+  int32_t locate_particles; /* 1: a particle outside the mesh is an error,
+                               0: it is removed (mpm_scheme.tcc:245-261) */
+  int32_t device;           /* CUDA device ordinal */
+} mpm_gpu_config;
+
+/* Particle state, one row per particle, row-major.  x,u,v: n*3 (the third
+ * column is ignored in 2D); stress, strain: n*6 Voigt (xx,yy,zz,xy,yz,xz,
+ * engineering shear strain); F: n*9 row-major deformation gradient; volume,
+ * mass, density: n; cell: n (cell id, -1 = removed); material: n (material
+ * id); svars: n*9 MohrCoulomb state in the reference order (yield_state, phi,
+ * psi, cohesion, tension_cutoff, epsilon, rho, theta, pdstrain; zero for
+ * LinearElastic).  On load a NULL pointer means "default" (zeros; identity
+ * F; initial material state); on read-back a NULL pointer is skipped. */
+typedef struct {
+  double* x;
+  double* u;
+  double* v;
+  double* stress;
+  double* strain;
+  double* F;
+  double* volume;
+  double* mass;
+  double* density;
+  int64_t* cell;
+  int32_t* material;
+  double* svars;
+} mpm_gpu_particles;
+
+/* Create a solver on cfg->device. */
+int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out);
+int mpm_gpu_destroy(mpm_gpu_t h);
+const char* mpm_gpu_last_error(mpm_gpu_t h);
+
+/* Mesh: node coordinates (nnodes*dim) and cell connectivity
+ * (ncells*nodes_per_cell, node order of quadrilateral_element.tcc:1-7 /
+ * hexahedron_element.tcc:1-13).  Replaces Mesh::create_nodes/create_cells
+ * and find_cell_neighbours. */
+int mpm_gpu_set_mesh(mpm_gpu_t h, int64_t nnodes, const double* coords, int64_t ncells,
+                     int32_t nodes_per_cell, const int64_t* cell_nodes);
+
+/* Material<Tdim> factory: type "LinearElastic2D/3D" or "MohrCoulomb2D/3D",
+ * properties as the reference's JSON material object. */
+int mpm_gpu_add_material(mpm_gpu_t h, int32_t id, const char* type, const char* json_props);
+
+/* Nodal constraints (constraints.tcc:83-106, 192-217; node.tcc:349-505). */
+int mpm_gpu_add_velocity_constraints(mpm_gpu_t h, int64_t n, const int64_t* node_ids,
+                                     const int32_t* dirs, const double* values);
+int mpm_gpu_add_acceleration_constraints(mpm_gpu_t h, int64_t n, const int64_t* node_ids,
+                                         const int32_t* dirs, const double* values);
+int mpm_gpu_add_friction_constraints(mpm_gpu_t h, int64_t n, const int64_t* node_ids,
+                                     const int32_t* dirs, const int32_t* signs,
+                                     const double* mu);
+
+/* Create particles at coordinates (n*dim) with one material
+ * (mesh.tcc:2114-2148 read_particles_file / create_particles). */
+int mpm_gpu_add_particles(mpm_gpu_t h, int64_t n, const double* coords, int32_t material_id);
+
+/* Locate particles, volume = cell volume / particles in cell, mass =
+ * volume * density, material state initialised (mpm_base.tcc:347-473,
+ * particle.tcc:589-626, mpm_explicit.tcc:94-95).  Uploads the state. */
+int mpm_gpu_initialise(mpm_gpu_t h);
+
+/* Initial particle stresses, n*6 Voigt, in particle creation order
+ * (mpm_base.tcc:1591-1625 particles_stresses, mesh.tcc:1502-1524).  After
+ * mpm_gpu_initialise. */
+int mpm_gpu_assign_particle_stresses(mpm_gpu_t h, int64_t n, const double* stress);
+
+/* Particle velocity constraint on particle ids (n < 0: all particles)
+ * (mesh.tcc:1454-1467, particle.tcc:1190-1194). */
+int mpm_gpu_add_particle_velocity_constraint(mpm_gpu_t h, int64_t n, const int64_t* pids,
+                                             int32_t dir, double velocity);
+
+/* Replace the full particle state (e.g. restart from a checkpoint). */
+int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* p);
+
+/* Advance nsteps explicit steps (mpm_explicit.tcc:112-190). */
+int mpm_gpu_step(mpm_gpu_t h, int64_t nsteps);
+
+/* As mpm_gpu_step, and report the device time of the steps, measured with
+ * CUDA events on the solver's stream (the reference logs the same span as
+ * "solver duration", mpm_explicit.tcc:191-196). */
+int mpm_gpu_step_timed(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms);
+
+/* Per-kernel device timing (CUDA events around every launch on the solver's
+ * stream).  Enabling or disabling resets the counters.  Kernel indices run
+ * from 0 while the call succeeds; name receives a static string. */
+int mpm_gpu_set_profiling(mpm_gpu_t h, int32_t enable);
+int mpm_gpu_kernel_profile(mpm_gpu_t h, int32_t kernel, const char** name, double* total_ms,
+                           int64_t* launches);
+/* Kernels launched by this handle since profiling was last reset. */
+int64_t mpm_gpu_launch_count(mpm_gpu_t h);
+
+int64_t mpm_gpu_nparticles(mpm_gpu_t h);
+int64_t mpm_gpu_current_step(mpm_gpu_t h);
+int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out);
+
+/* Device addresses of the particle state (for zero-copy interop, e.g. torch).
+ * field: 0 x, 1 u, 2 v, 3 stress, 4 strain, 5 F, 6 volume, 7 density, 8 mass.
+ * Returns the base address; component c of particle p is at
+ * base[c * stride + p]; *ncomp receives the component count. */
+int mpm_gpu_device_field(mpm_gpu_t h, int32_t field, void** base, int64_t* stride,
+                         int32_t* ncomp);
+
+/* Material<Tdim>::compute_stress on a batch of independent points, on the
+ * device (the constitutive kernel of the step, exposed for unit checks):
+ * stress, dstrain, out: n*6; density: n; state: n*9 in/out. */
+int mpm_gpu_material_stress_batch(int32_t device, int32_t dim, const char* type,
+                                  const char* json_props, int64_t n, const double* stress,
+                                  const double* dstrain, const double* density, double* state,
+                                  double* out);
+
+/* Library version string. */
+const char* mpm_gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPM_GPU_H */

@@ -1,0 +1,1210 @@
+// mpm_gpu.cu -- C ABI (include/mpm_gpu.h): solver handle, host-side set-up
+// that mirrors the reference's MPMBase initialisation, device buffers and the
+// step loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/mpm_gpu.h"
+#include "json_lite.hpp"
+#include "mpm_kernels.h"
+#include "mpm_math.cuh"
+#include "mpm_state.cuh"
+
+using namespace mpm_b200;
+
+#define MPM_VERSION "mpm_b200 0.1.0 (sm_100a)"
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct InvalidArg : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+inline void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free();
+    if (count == 0) return;
+    ck(cudaMalloc(&p, sizeof(T) * count), "cudaMalloc");
+    n = count;
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void upload(const T* h, size_t count, cudaStream_t st) {
+    if (count > n) alloc(count);
+    if (count) ck(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, st), "H2D");
+  }
+  void download(T* h, size_t count, cudaStream_t st) const {
+    if (count) ck(cudaMemcpyAsync(h, p, sizeof(T) * count, cudaMemcpyDeviceToHost, st), "D2H");
+  }
+  ~DevBuf() { free(); }
+};
+
+struct HostBC {
+  std::map<unsigned, double> vel, acc;  // ascending direction (node.tcc std::map)
+  bool friction = false;
+  unsigned fdir = 0;
+  int fsign = 0;
+  double mu = 0;
+};
+
+}  // namespace
+
+namespace mpm_b200 {
+
+const char* kernel_name(int kid) {
+  static const char* names[K_NKERNELS] = {"p2g", "nodes_velocity", "stress_forces",
+                                          "nodes_acceleration", "g2p", "locate_fallback"};
+  return (kid >= 0 && kid < K_NKERNELS) ? names[kid] : "?";
+}
+
+struct ProfilerImpl {
+  std::vector<cudaEvent_t> pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  cudaEvent_t open_start = nullptr;
+  cudaEvent_t take() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      ck(cudaEventCreate(&e), "cudaEventCreate");
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+};
+
+void Profiler::begin(int kid, cudaStream_t st) {
+  (void)kid;
+  ++launches;
+  if (!enabled) return;
+  if (!impl) impl = new ProfilerImpl();
+  auto* P = static_cast<ProfilerImpl*>(impl);
+  P->open_start = P->take();
+  ck(cudaEventRecord(P->open_start, st), "cudaEventRecord");
+}
+
+void Profiler::end(int kid, cudaStream_t st) {
+  if (!enabled) return;
+  auto* P = static_cast<ProfilerImpl*>(impl);
+  cudaEvent_t e = P->take();
+  ck(cudaEventRecord(e, st), "cudaEventRecord");
+  P->pending.push_back({kid, {P->open_start, e}});
+}
+
+void Profiler::collect() {
+  if (!impl) return;
+  auto* P = static_cast<ProfilerImpl*>(impl);
+  for (auto& r : P->pending) {
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, r.second.first, r.second.second), "cudaEventElapsedTime");
+    total_ms[r.first] += ms;
+    count[r.first] += 1;
+    P->pool.push_back(r.second.first);
+    P->pool.push_back(r.second.second);
+  }
+  P->pending.clear();
+}
+
+void Profiler::reset() {
+  collect();
+  launches = 0;
+  for (int k = 0; k < K_NKERNELS; ++k) {
+    total_ms[k] = 0;
+    count[k] = 0;
+  }
+}
+
+Profiler::~Profiler() {
+  if (!impl) return;
+  auto* P = static_cast<ProfilerImpl*>(impl);
+  for (auto e : P->pool) cudaEventDestroy(e);
+  for (auto& r : P->pending) {
+    cudaEventDestroy(r.second.first);
+    cudaEventDestroy(r.second.second);
+  }
+  delete P;
+}
+
+}  // namespace mpm_b200
+
+struct mpm_gpu_solver {
+  mpm_gpu_config cfg{};
+  int dim = 3, nv = 8;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t step = 0;
+  bool mesh_set = false, initialised = false;
+
+  // mesh (host)
+  int64_t nnodes = 0, ncells = 0;
+  std::vector<double> coords;           // nnodes*dim
+  std::vector<int32_t> cell_nodes;      // ncells*nv
+  std::vector<CellGeom> geom;           // ncells
+  std::vector<double> cell_volume;      // ncells
+  std::vector<int32_t> nb_off, nb;      // neighbour CSR
+  std::vector<int32_t> bin_off, bin_cells;
+  double bmin[3] = {0, 0, 0}, bsize[3] = {1, 1, 1};
+  int32_t bn[3] = {1, 1, 1};
+  std::map<int64_t, HostBC> bcs;        // node id -> constraints
+  bool structured = false;
+  int32_t gcells[3] = {1, 1, 1};
+  std::vector<double> axis[3];
+
+  // materials
+  std::vector<MaterialParams> mats;
+  std::map<int32_t, int> mat_index;     // material id -> slot
+
+  // particles (host staging)
+  int64_t np = 0;
+  std::vector<double> p_coords;         // np*dim (creation)
+  std::vector<uint8_t> p_mat;
+  std::vector<std::map<unsigned, double>> p_vc;  // per particle velocity constraints
+  bool p_vc_dirty = false;
+
+  // device
+  DevState ds;
+  DevBuf<double> d_pf, d_sv, d_nf, d_ncoord;
+  DevBuf<int32_t> d_cell, d_bc_index, d_cell_nodes, d_nb_off, d_nb, d_bin_off, d_bin_cells, d_lost;
+  DevBuf<uint8_t> d_mat, d_active;
+  DevBuf<int16_t> d_pvc;
+  DevBuf<CellGeom> d_geom;
+  DevBuf<unsigned> d_words;  // [0] nlost, [1] err
+  DevBuf<MaterialParams> d_mats;
+  DevBuf<double> d_axis[3];
+  DevBuf<NodeBC> d_bcs;
+  DevBuf<ParticleVC> d_pvcs;
+  bool any_mc = false;
+  Profiler prof;
+
+  int nfields() const { return dim == 2 ? PF<2>::NF : PF<3>::NF; }
+  int nnf() const { return dim == 2 ? NF<2>::NNF : NF<3>::NNF; }
+};
+
+namespace {
+
+int fail(mpm_gpu_t h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+double norm_d(int dim, const double* a) {
+  double s = a[0] * a[0];
+  for (int i = 1; i < dim; ++i) s = s + a[i] * a[i];
+  return std::sqrt(s);
+}
+
+// cell.tcc:255-279 (centroid, mean length), :458-463 / :566-571 (local
+// coordinate lengths); quadrilateral_element.tcc:473-496 and
+// hexahedron_element.tcc:559-596 (volume)
+void cell_geometry(int dim, const double* X, CellGeom* g, double* volume) {
+  const int nv = dim == 2 ? 4 : 8;
+  for (int i = 0; i < 3; ++i) g->centroid[i] = g->len[i] = 0.;
+  for (int n = 0; n < nv; ++n)
+    for (int i = 0; i < dim; ++i) g->centroid[i] = g->centroid[i] + X[n * dim + i];
+  for (int i = 0; i < dim; ++i) g->centroid[i] = g->centroid[i] / nv;
+  static const int q4s[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
+  static const int h8s[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                 {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  const int ns = dim == 2 ? 4 : 12;
+  double ml = 0.;
+  for (int s = 0; s < ns; ++s) {
+    const int a = dim == 2 ? q4s[s][0] : h8s[s][0];
+    const int b = dim == 2 ? q4s[s][1] : h8s[s][1];
+    double d[3];
+    for (int i = 0; i < dim; ++i) d[i] = X[a * dim + i] - X[b * dim + i];
+    ml += norm_d(dim, d);
+  }
+  g->mean_length = ml / ns;
+  double d[3];
+  for (int i = 0; i < dim; ++i) d[i] = X[0 * dim + i] - X[1 * dim + i];
+  g->len[0] = norm_d(dim, d);
+  for (int i = 0; i < dim; ++i) d[i] = X[1 * dim + i] - X[2 * dim + i];
+  g->len[1] = norm_d(dim, d);
+  if (dim == 3) {
+    for (int i = 0; i < dim; ++i) d[i] = X[1 * dim + i] - X[5 * dim + i];
+    g->len[2] = norm_d(dim, d);
+  }
+  if (dim == 2) {
+    auto len = [&](int a, int b) {
+      double e[2] = {X[a * 2] - X[b * 2], X[a * 2 + 1] - X[b * 2 + 1]};
+      return norm_d(2, e);
+    };
+    const double a = len(0, 3), b = len(2, 3), c = len(1, 2), dd = len(0, 1);
+    const double p = len(0, 2), q = len(1, 3);
+    *volume = 0.25 * std::sqrt(4 * p * p * q * q - std::pow((a * a + c * c - b * b - dd * dd), 2.0));
+  } else {
+    auto row = [&](int n, double* r) { for (int i = 0; i < 3; ++i) r[i] = X[n * 3 + i]; };
+    auto sub = [](const double* x, const double* y, double* r) { for (int i = 0; i < 3; ++i) r[i] = x[i] - y[i]; };
+    auto add = [](const double* x, const double* y, double* r) { for (int i = 0; i < 3; ++i) r[i] = x[i] + y[i]; };
+    auto cross = [](const double* x, const double* y, double* r) {
+      r[0] = x[1] * y[2] - x[2] * y[1];
+      r[1] = x[2] * y[0] - x[0] * y[2];
+      r[2] = x[0] * y[1] - x[1] * y[0];
+    };
+    auto dot = [](const double* x, const double* y) { return (x[0] * y[0] + x[1] * y[1]) + x[2] * y[2]; };
+    double A[3], B[3], C[3], D[3], E[3], F[3], G[3], H[3];
+    row(7, A); row(6, B); row(2, C); row(3, D); row(4, E); row(5, F); row(1, G); row(0, H);
+    double t1[3], t2[3], bd[3], eb[3], de[3], x1[3], s1[3], s2[3], s3[3], s4[3], tmp[3];
+    sub(B, D, t1); sub(C, A, t2); cross(t1, t2, bd);
+    sub(E, B, t1); sub(F, A, t2); cross(t1, t2, eb);
+    sub(D, E, t1); sub(H, A, t2); cross(t1, t2, de);
+    add(bd, eb, tmp); add(tmp, de, s1);
+    sub(C, G, t1); sub(C, F, t2); cross(t1, t2, x1); add(bd, x1, s2);
+    sub(F, G, t1); sub(H, F, t2); cross(t1, t2, x1); add(eb, x1, s3);
+    sub(H, G, t1); sub(H, C, t2); cross(t1, t2, x1); add(de, x1, s4);
+    double ag[3], bg[3], eg[3], dg[3];
+    sub(A, G, ag); sub(B, G, bg); sub(E, G, eg); sub(D, G, dg);
+    *volume = (1.0 / 12) * dot(ag, s1) + (1.0 / 12) * dot(bg, s2) + (1.0 / 12) * dot(eg, s3) +
+              (1.0 / 12) * dot(dg, s4);
+  }
+}
+
+void build_bins(mpm_gpu_t h) {
+  const int dim = h->dim;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  double maxr = 0;
+  for (int64_t c = 0; c < h->ncells; ++c) {
+    const CellGeom& g = h->geom[c];
+    const double r = 2. * g.mean_length;
+    maxr = std::max(maxr, r);
+    for (int i = 0; i < dim; ++i) {
+      lo[i] = std::min(lo[i], g.centroid[i] - r);
+      hi[i] = std::max(hi[i], g.centroid[i] + r);
+    }
+  }
+  double extent = 0;
+  for (int i = 0; i < dim; ++i) extent = std::max(extent, hi[i] - lo[i]);
+  // widen every range by far more than the rounding of the bin arithmetic
+  const double pad = 1e-9 * std::max(extent, 1e-300);
+  int64_t total = 1;
+  for (int i = 0; i < 3; ++i) {
+    if (i >= dim) {
+      h->bn[i] = 1;
+      h->bmin[i] = 0;
+      h->bsize[i] = 1;
+      continue;
+    }
+    h->bmin[i] = lo[i] - 2 * pad;
+    h->bsize[i] = std::max(2. * maxr, 1e-300);
+    h->bn[i] = (int32_t)std::max<int64_t>(1, (int64_t)std::ceil((hi[i] + 2 * pad - h->bmin[i]) / h->bsize[i]) + 1);
+    total *= h->bn[i];
+  }
+  std::vector<std::vector<int32_t>> bins(total);
+  for (int64_t id = 0; id < h->ncells; ++id) {
+    const CellGeom& g = h->geom[id];
+    const double r = 2. * g.mean_length;
+    int64_t b0[3] = {0, 0, 0}, b1[3] = {0, 0, 0};
+    for (int i = 0; i < dim; ++i) {
+      b0[i] = std::max<int64_t>(0, (int64_t)std::floor((g.centroid[i] - r - pad - h->bmin[i]) / h->bsize[i]));
+      b1[i] = std::min<int64_t>(h->bn[i] - 1, (int64_t)std::floor((g.centroid[i] + r + pad - h->bmin[i]) / h->bsize[i]));
+    }
+    for (int64_t k = b0[2]; k <= b1[2]; ++k)
+      for (int64_t j = b0[1]; j <= b1[1]; ++j)
+        for (int64_t i = b0[0]; i <= b1[0]; ++i)
+          bins[(k * h->bn[1] + j) * h->bn[0] + i].push_back((int32_t)id);
+  }
+  h->bin_off.assign(total + 1, 0);
+  for (int64_t b = 0; b < total; ++b) h->bin_off[b + 1] = h->bin_off[b] + (int32_t)bins[b].size();
+  h->bin_cells.resize(h->bin_off[total]);
+  for (int64_t b = 0; b < total; ++b)
+    std::copy(bins[b].begin(), bins[b].end(), h->bin_cells.begin() + h->bin_off[b]);
+}
+
+// Recognise a tensor-product grid: node (i,j,k) = i + nx*(j + ny*k) sits at
+// (ax[i], ay[j], az[k]) with strictly increasing axes, and cell
+// (i,j,k) = i + cx*(j + cy*k) has the reference node order.
+bool detect_structured(mpm_gpu_t h) {
+  const int dim = h->dim;
+  const double* X = h->coords.data();
+  int64_t n[3] = {1, 1, 1};
+  // count nodes along x: until the y coordinate changes
+  int64_t stride = 1;
+  for (int d = 0; d < dim; ++d) {
+    int64_t c = 1;
+    while (stride * (c + 1) <= h->nnodes) {
+      bool same_other = true;
+      for (int e = 0; e < dim; ++e)
+        if (e != d && X[(stride * c) * dim + e] != X[0 * dim + e]) same_other = false;
+      if (!same_other || !(X[(stride * c) * dim + d] > X[(stride * (c - 1)) * dim + d])) break;
+      ++c;
+    }
+    n[d] = c;
+    stride *= c;
+  }
+  if (stride != h->nnodes) return false;
+  for (int d = 0; d < dim; ++d)
+    if (n[d] < 2) return false;
+  std::vector<double> ax[3];
+  int64_t st[3] = {1, n[0], n[0] * n[1]};
+  for (int d = 0; d < dim; ++d) {
+    ax[d].resize(n[d]);
+    for (int64_t i = 0; i < n[d]; ++i) ax[d][i] = X[(i * st[d]) * dim + d];
+  }
+  for (int64_t id = 0; id < h->nnodes; ++id) {
+    int64_t r = id;
+    for (int d = 0; d < dim; ++d) {
+      const int64_t i = r % n[d];
+      r /= n[d];
+      if (X[id * dim + d] != ax[d][i]) return false;
+    }
+  }
+  const int64_t cx = n[0] - 1, cy = n[1] - 1, cz = dim == 3 ? n[2] - 1 : 1;
+  if (cx * cy * cz != h->ncells) return false;
+  for (int64_t c = 0; c < h->ncells; ++c) {
+    const int64_t i = c % cx, j = (c / cx) % cy, k = c / (cx * cy);
+    auto nid = [&](int64_t a, int64_t b, int64_t e) { return a + n[0] * (b + n[1] * e); };
+    const int32_t* cn = &h->cell_nodes[c * h->nv];
+    if (dim == 2) {
+      const int64_t ref[4] = {nid(i, j, 0), nid(i + 1, j, 0), nid(i + 1, j + 1, 0), nid(i, j + 1, 0)};
+      for (int q = 0; q < 4; ++q)
+        if (cn[q] != ref[q]) return false;
+    } else {
+      const int64_t ref[8] = {nid(i, j, k),         nid(i + 1, j, k),     nid(i + 1, j + 1, k),
+                              nid(i, j + 1, k),     nid(i, j, k + 1),     nid(i + 1, j, k + 1),
+                              nid(i + 1, j + 1, k + 1), nid(i, j + 1, k + 1)};
+      for (int q = 0; q < 8; ++q)
+        if (cn[q] != ref[q]) return false;
+    }
+  }
+  h->gcells[0] = (int32_t)cx;
+  h->gcells[1] = (int32_t)cy;
+  h->gcells[2] = (int32_t)cz;
+  for (int d = 0; d < 3; ++d) h->axis[d] = d < dim ? ax[d] : std::vector<double>{0.0, 1.0};
+  return true;
+}
+
+// first cell in id order containing p (host twin of the device fallback)
+int32_t host_scan(mpm_gpu_t h, const double* p) {
+  if (h->structured) {
+    const double* ax[3] = {h->axis[0].data(), h->axis[1].data(), h->axis[2].data()};
+    return h->dim == 2 ? structured_scan<2>(p, h->gcells, ax, h->geom.data())
+                       : structured_scan<3>(p, h->gcells, ax, h->geom.data());
+  }
+  int64_t b[3] = {0, 0, 0};
+  for (int i = 0; i < h->dim; ++i) {
+    const double f = std::floor((p[i] - h->bmin[i]) / h->bsize[i]);
+    if (!(f >= 0) || f >= (double)h->bn[i]) return -1;
+    b[i] = (int64_t)f;
+  }
+  const int64_t bi = (b[2] * h->bn[1] + b[1]) * h->bn[0] + b[0];
+  for (int32_t j = h->bin_off[bi]; j < h->bin_off[bi + 1]; ++j) {
+    const int32_t c = h->bin_cells[j];
+    const CellGeom& g = h->geom[c];
+    double xi[3];
+    const bool in = h->dim == 2 ? point_in_cell<2>(p, g.centroid, g.len, g.mean_length, xi)
+                                : point_in_cell<3>(p, g.centroid, g.len, g.mean_length, xi);
+    if (in) return c;
+  }
+  return -1;
+}
+
+// MohrCoulomb / LinearElastic constructors (mohr_coulomb.tcc:3-81,
+// linear_elastic.tcc:3-49) from the reference's JSON property object
+MaterialParams make_material(int dim, const std::string& type, const Json& j) {
+  MaterialParams m{};
+  std::string base = type;
+  const std::string suffix = dim == 2 ? "2D" : "3D";
+  if (base.size() < 2 || base.substr(base.size() - 2) != suffix)
+    throw InvalidArg("material type \"" + type + "\" does not match the " + suffix + " solver");
+  base = base.substr(0, base.size() - 2);
+  auto req = [&](const char* k) {
+    if (!j.contains(k)) throw InvalidArg(std::string("material parameter not set: ") + k);
+    return j.at(k).as_double();
+  };
+  m.density = req("density");
+  m.E = req("youngs_modulus");
+  m.nu = req("poisson_ratio");
+  if (base == "LinearElastic") {
+    if (j.contains("stress_rate") && j.at("stress_rate").is_string() &&
+        (j.at("stress_rate").as_string() == "jaumann" ||
+         j.at("stress_rate").as_string() == "green_naghdi"))
+      throw InvalidArg("objective stress rates are not implemented on this path");
+    m.type = 0;
+    m.bulk = m.E / (3.0 * (1. - 2. * m.nu));
+    m.shear = m.E / (2.0 * (1. + m.nu));
+  } else if (base == "MohrCoulomb") {
+    m.type = 1;
+    double packing = 1.;
+    if (j.contains("packing_fraction"))
+      packing = j.at("packing_fraction").as_double();
+    else if (j.contains("porosity"))
+      packing = 1. - j.at("porosity").as_double();
+    const bool wet = j.contains("porosity") &&
+                     (j.contains("k_x") || j.contains("k_y") || j.contains("k_z"));
+    m.grain_density = wet ? m.density : m.density / packing;
+    m.min_packing = j.get("packing_fraction_minimum", 0.0);
+    if (!j.contains("softening")) throw InvalidArg("material parameter not set: softening");
+    m.softening = j.at("softening").as_bool() ? 1 : 0;
+    m.phi_peak = req("friction") * kPiD / 180.;
+    m.psi_peak = req("dilation") * kPiD / 180.;
+    m.c_peak = req("cohesion");
+    m.phi_res = req("residual_friction") * kPiD / 180.;
+    m.psi_res = req("residual_dilation") * kPiD / 180.;
+    m.c_res = req("residual_cohesion");
+    m.pd_peak = req("peak_pdstrain");
+    m.pd_res = req("residual_pdstrain");
+    m.tension_cutoff = req("tension_cutoff");
+    m.bulk = m.E / (3.0 * (1. - 2. * m.nu));
+    m.shear = m.E / (2.0 * (1 + m.nu));
+    const double apex = m.c_peak / std::tan(m.phi_peak);
+    m.tc_init = check_low(m.tension_cutoff < apex ? m.tension_cutoff : apex);
+  } else {
+    throw InvalidArg("unknown material type \"" + type + "\"");
+  }
+  const double G = m.shear;
+  m.a1 = m.bulk + (4.0 / 3.0) * G;
+  m.a2 = m.bulk - (2.0 / 3.0) * G;
+  return m;
+}
+
+void mc_init_state(const MaterialParams& m, double* sv) {
+  sv[SV_YIELD] = 0;
+  sv[SV_PHI] = m.phi_peak;
+  sv[SV_PSI] = m.psi_peak;
+  sv[SV_COH] = m.c_peak;
+  sv[SV_TC] = m.tc_init;
+  sv[SV_EPS] = sv[SV_RHO] = sv[SV_THETA] = sv[SV_PD] = 0.;
+}
+
+void upload_mesh(mpm_gpu_t h) {
+  cudaStream_t st = h->stream;
+  const int dim = h->dim;
+  std::vector<double> nc((size_t)dim * h->nnodes);
+  for (int64_t n = 0; n < h->nnodes; ++n)
+    for (int d = 0; d < dim; ++d) nc[(size_t)d * h->nnodes + n] = h->coords[n * dim + d];
+  h->d_ncoord.upload(nc.data(), nc.size(), st);
+  h->d_cell_nodes.upload(h->cell_nodes.data(), h->cell_nodes.size(), st);
+  h->d_geom.upload(h->geom.data(), h->geom.size(), st);
+  h->d_nb_off.upload(h->nb_off.data(), h->nb_off.size(), st);
+  h->d_nb.alloc(std::max<size_t>(1, h->nb.size()));
+  h->d_nb.upload(h->nb.data(), h->nb.size(), st);
+  h->d_bin_off.upload(h->bin_off.data(), h->bin_off.size(), st);
+  h->d_bin_cells.alloc(std::max<size_t>(1, h->bin_cells.size()));
+  h->d_bin_cells.upload(h->bin_cells.data(), h->bin_cells.size(), st);
+  h->d_nf.alloc((size_t)h->nnf() * h->nnodes);
+  h->d_active.alloc(h->nnodes);
+  ck(cudaMemsetAsync(h->d_active.p, 0, h->nnodes, st), "memset");
+  ck(cudaMemsetAsync(h->d_nf.p, 0, sizeof(double) * h->nnf() * h->nnodes, st), "memset");
+  h->d_words.alloc(2);
+  ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 2, st), "memset");
+  if (h->structured)
+    for (int d = 0; d < 3; ++d) h->d_axis[d].upload(h->axis[d].data(), h->axis[d].size(), st);
+}
+
+void upload_bcs(mpm_gpu_t h) {
+  std::vector<int32_t> index(h->nnodes, -1);
+  std::vector<NodeBC> table;
+  std::map<std::string, int> dedup;
+  for (auto& kv : h->bcs) {
+    NodeBC b{};
+    for (auto& c : kv.second.vel) {
+      b.vel_mask |= (uint8_t)(1u << c.first);
+      b.vel[c.first] = c.second;
+    }
+    for (auto& c : kv.second.acc) {
+      b.acc_mask |= (uint8_t)(1u << c.first);
+      b.acc[c.first] = c.second;
+    }
+    b.friction = kv.second.friction ? 1 : 0;
+    b.fric_dir = (uint8_t)kv.second.fdir;
+    b.fric_sign = kv.second.fsign;
+    b.mu = kv.second.mu;
+    std::string key(reinterpret_cast<const char*>(&b), sizeof(b));
+    auto it = dedup.find(key);
+    int slot;
+    if (it == dedup.end()) {
+      slot = (int)table.size();
+      table.push_back(b);
+      dedup[key] = slot;
+    } else {
+      slot = it->second;
+    }
+    index[kv.first] = slot;
+  }
+  if (table.empty()) table.push_back(NodeBC{});
+  h->d_bcs.upload(table.data(), table.size(), h->stream);
+  h->d_bc_index.upload(index.data(), index.size(), h->stream);
+}
+
+void upload_pvc(mpm_gpu_t h) {
+  std::vector<int16_t> idx(h->np, -1);
+  std::vector<ParticleVC> table;
+  std::map<std::string, int> dedup;
+  for (int64_t p = 0; p < h->np; ++p) {
+    if (p >= (int64_t)h->p_vc.size() || h->p_vc[p].empty()) continue;
+    ParticleVC r{};
+    for (auto& c : h->p_vc[p]) {
+      r.mask |= 1u << c.first;
+      r.value[c.first] = c.second;
+    }
+    std::string key(reinterpret_cast<const char*>(&r), sizeof(r));
+    auto it = dedup.find(key);
+    int slot;
+    if (it == dedup.end()) {
+      slot = (int)table.size();
+      if (slot > 32767) throw InvalidArg("too many distinct particle velocity constraints");
+      table.push_back(r);
+      dedup[key] = slot;
+    } else {
+      slot = it->second;
+    }
+    idx[p] = (int16_t)slot;
+  }
+  if (table.empty()) table.push_back(ParticleVC{});
+  h->d_pvcs.upload(table.data(), table.size(), h->stream);
+  h->d_pvc.upload(idx.data(), idx.size(), h->stream);
+  h->p_vc_dirty = false;
+}
+
+void allocate_particles(mpm_gpu_t h) {
+  const int64_t np = h->np;
+  h->d_pf.alloc((size_t)h->nfields() * np);
+  h->d_cell.alloc(np);
+  h->d_mat.alloc(np);
+  h->d_lost.alloc(std::max<int64_t>(1, np));
+  h->any_mc = false;
+  for (auto& m : h->mats) h->any_mc = h->any_mc || m.type == 1;
+  if (h->any_mc)
+    h->d_sv.alloc((size_t)SV_N * np);
+  else
+    h->d_sv.free();
+}
+
+void refresh_state(mpm_gpu_t h) {
+  DevState& s = h->ds;
+  s.np = h->np;
+  s.pf = h->d_pf.p;
+  s.sv = h->d_sv.p;
+  s.cell = h->d_cell.p;
+  s.mat = h->d_mat.p;
+  s.pvc = h->d_pvc.p;
+  s.nn = h->nnodes;
+  s.nf = h->d_nf.p;
+  s.active = h->d_active.p;
+  s.bc_index = h->d_bc_index.p;
+  s.ncells = h->ncells;
+  s.cell_nodes = h->d_cell_nodes.p;
+  s.ncoord = h->d_ncoord.p;
+  s.geom = h->d_geom.p;
+  s.nb_off = h->d_nb_off.p;
+  s.nb = h->d_nb.p;
+  s.bin_off = h->d_bin_off.p;
+  s.bin_cells = h->d_bin_cells.p;
+  for (int i = 0; i < 3; ++i) {
+    s.bmin[i] = h->bmin[i];
+    s.bsize[i] = h->bsize[i];
+    s.bn[i] = h->bn[i];
+  }
+  s.structured = h->structured ? 1 : 0;
+  for (int d = 0; d < 3; ++d) {
+    s.gcells[d] = h->gcells[d];
+    s.axis[d] = h->d_axis[d].p;
+  }
+  s.lost = h->d_lost.p;
+  s.nlost = h->d_words.p;
+  s.err = h->d_words.p + 1;
+  s.mats = h->d_mats.p;
+  s.bcs = h->d_bcs.p;
+  s.pvcs = h->d_pvcs.p;
+}
+
+// Pack host particle rows (ABI layout) into the device SoA field order.
+void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<int32_t>* cells) {
+  const int dim = h->dim;
+  const int64_t np = h->np;
+  std::vector<double> pf((size_t)h->nfields() * np, 0.0);
+  auto at = [&](int f, int64_t p) -> double& { return pf[(size_t)f * np + p]; };
+  const int X = dim == 2 ? PF<2>::X : PF<3>::X, U = dim == 2 ? PF<2>::U : PF<3>::U;
+  const int V = dim == 2 ? PF<2>::V : PF<3>::V, S = dim == 2 ? PF<2>::S : PF<3>::S;
+  const int E = dim == 2 ? PF<2>::E : PF<3>::E, Fo = dim == 2 ? PF<2>::F : PF<3>::F;
+  const int VOL = dim == 2 ? PF<2>::VOL : PF<3>::VOL, RHO = dim == 2 ? PF<2>::RHO : PF<3>::RHO;
+  const int MASS = dim == 2 ? PF<2>::MASS : PF<3>::MASS;
+  for (int64_t p = 0; p < np; ++p) {
+    for (int d = 0; d < dim; ++d) {
+      at(X + d, p) = in->x ? in->x[p * 3 + d] : h->p_coords[p * dim + d];
+      at(U + d, p) = in->u ? in->u[p * 3 + d] : 0.;
+      at(V + d, p) = in->v ? in->v[p * 3 + d] : 0.;
+    }
+    if (dim == 2) {
+      const int smap[4] = {0, 1, 2, 3};
+      for (int k = 0; k < 4; ++k) at(S + k, p) = in->stress ? in->stress[p * 6 + smap[k]] : 0.;
+      if (in->stress && (in->stress[p * 6 + 4] != 0. || in->stress[p * 6 + 5] != 0.))
+        throw InvalidArg("2D particle stress must have zero yz and xz components");
+      const int emap[3] = {0, 1, 3};
+      for (int k = 0; k < 3; ++k) at(E + k, p) = in->strain ? in->strain[p * 6 + emap[k]] : 0.;
+      if (in->strain && (in->strain[p * 6 + 2] != 0. || in->strain[p * 6 + 4] != 0. ||
+                         in->strain[p * 6 + 5] != 0.))
+        throw InvalidArg("2D particle strain must have zero zz, yz and xz components");
+      const int fmap[4] = {0, 1, 3, 4};
+      for (int k = 0; k < 4; ++k) at(Fo + k, p) = in->F ? in->F[p * 9 + fmap[k]] : (k == 0 || k == 3 ? 1. : 0.);
+      if (in->F && (in->F[p * 9 + 2] != 0. || in->F[p * 9 + 5] != 0. || in->F[p * 9 + 6] != 0. ||
+                    in->F[p * 9 + 7] != 0. || in->F[p * 9 + 8] != 1.))
+        throw InvalidArg("2D deformation gradient must have third row and column (0,0,1)");
+    } else {
+      for (int k = 0; k < 6; ++k) {
+        at(S + k, p) = in->stress ? in->stress[p * 6 + k] : 0.;
+        at(E + k, p) = in->strain ? in->strain[p * 6 + k] : 0.;
+      }
+      for (int k = 0; k < 9; ++k) at(Fo + k, p) = in->F ? in->F[p * 9 + k] : (k % 4 == 0 ? 1. : 0.);
+    }
+    const MaterialParams& m = h->mats[h->p_mat[p]];
+    at(RHO, p) = in->density ? in->density[p] : m.density;
+    at(VOL, p) = in->volume ? in->volume[p] : 0.;
+    at(MASS, p) = in->mass ? in->mass[p] : at(VOL, p) * at(RHO, p);
+  }
+  h->d_pf.upload(pf.data(), pf.size(), h->stream);
+  std::vector<int32_t> cell(np);
+  for (int64_t p = 0; p < np; ++p) {
+    if (in->cell) {
+      const int64_t c = in->cell[p];
+      if (c < -1 || c >= h->ncells) throw InvalidArg("particle cell id out of range");
+      cell[p] = (int32_t)c;
+    } else {
+      cell[p] = (*cells)[p];
+    }
+  }
+  h->d_cell.upload(cell.data(), np, h->stream);
+  h->d_mat.upload(h->p_mat.data(), np, h->stream);
+  if (h->any_mc) {
+    std::vector<double> sv((size_t)SV_N * np, 0.0);
+    for (int64_t p = 0; p < np; ++p) {
+      const MaterialParams& m = h->mats[h->p_mat[p]];
+      double s[SV_N] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      if (in->svars)
+        for (int k = 0; k < SV_N; ++k) s[k] = in->svars[p * SV_N + k];
+      else if (m.type == 1)
+        mc_init_state(m, s);
+      for (int k = 0; k < SV_N; ++k) sv[(size_t)k * np + p] = s[k];
+    }
+    h->d_sv.upload(sv.data(), sv.size(), h->stream);
+  }
+}
+
+#define MPM_GUARD(h)                                                   \
+  if (!(h)) return MPM_ERR_INVALID;                                    \
+  try {
+#define MPM_END(h)                                                     \
+  }                                                                    \
+  catch (const InvalidArg& e) { return fail(h, MPM_ERR_INVALID, e.what()); } \
+  catch (const CudaError& e) { return fail(h, MPM_ERR_CUDA, e.what()); }     \
+  catch (const std::exception& e) { return fail(h, MPM_ERR_INVALID, e.what()); }
+
+}  // namespace
+
+extern "C" {
+
+const char* mpm_gpu_version(void) { return MPM_VERSION; }
+
+int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out) {
+  if (!cfg || !out) return MPM_ERR_INVALID;
+  *out = nullptr;
+  if (cfg->dim != 2 && cfg->dim != 3) return MPM_ERR_INVALID;
+  if (cfg->scheme != MPM_SCHEME_USF && cfg->scheme != MPM_SCHEME_USL) return MPM_ERR_UNSUPPORTED;
+  if (cfg->velocity_update != MPM_VELOCITY_FLIP && cfg->velocity_update != MPM_VELOCITY_PIC)
+    return MPM_ERR_UNSUPPORTED;
+  if (cfg->precision != MPM_PRECISION_FP64) return MPM_ERR_UNSUPPORTED;
+  if (!(cfg->dt > 0)) return MPM_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MPM_ERR_CUDA;
+  if (cfg->device < 0 || cfg->device >= ndev) return MPM_ERR_INVALID;
+  auto* h = new mpm_gpu_solver();
+  h->cfg = *cfg;
+  h->dim = cfg->dim;
+  h->nv = cfg->dim == 2 ? 4 : 8;
+  if (cudaSetDevice(cfg->device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return MPM_ERR_CUDA;
+  }
+  *out = h;
+  return MPM_OK;
+}
+
+int mpm_gpu_destroy(mpm_gpu_t h) {
+  if (!h) return MPM_ERR_INVALID;
+  cudaSetDevice(h->cfg.device);
+  if (h->stream) {
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+  }
+  delete h;
+  return MPM_OK;
+}
+
+const char* mpm_gpu_last_error(mpm_gpu_t h) { return h ? h->err.c_str() : "null handle"; }
+
+int mpm_gpu_set_mesh(mpm_gpu_t h, int64_t nnodes, const double* coords, int64_t ncells,
+                     int32_t npc, const int64_t* cell_nodes) {
+  MPM_GUARD(h)
+  if (npc != h->nv) throw InvalidArg("nodes_per_cell must be 4 (2D quad4) or 8 (3D hex8)");
+  if (nnodes <= 0 || ncells <= 0 || !coords || !cell_nodes) throw InvalidArg("empty mesh");
+  if (nnodes > INT32_MAX || ncells > INT32_MAX / 8) throw InvalidArg("mesh too large for 32-bit indices");
+  if (h->mesh_set) throw InvalidArg("mesh already set");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const int dim = h->dim, nv = h->nv;
+  h->nnodes = nnodes;
+  h->ncells = ncells;
+  h->coords.assign(coords, coords + nnodes * dim);
+  h->cell_nodes.resize((size_t)ncells * nv);
+  h->geom.resize(ncells);
+  h->cell_volume.resize(ncells);
+  std::vector<std::vector<int32_t>> node_cells(nnodes);
+  std::vector<double> X(nv * dim);
+  for (int64_t c = 0; c < ncells; ++c) {
+    for (int i = 0; i < nv; ++i) {
+      const int64_t n = cell_nodes[c * nv + i];
+      if (n < 0 || n >= nnodes) throw InvalidArg("cell node id out of range");
+      h->cell_nodes[c * nv + i] = (int32_t)n;
+      for (int d = 0; d < dim; ++d) X[i * dim + d] = coords[n * dim + d];
+      node_cells[n].push_back((int32_t)c);
+    }
+    cell_geometry(dim, X.data(), &h->geom[c], &h->cell_volume[c]);
+    if (!(h->cell_volume[c] > 0)) throw InvalidArg("Negative or zero volume cell, misconfigured cell!");
+  }
+  // mesh.tcc:287-306 neighbours: cells sharing a node, ascending id
+  h->nb_off.assign(ncells + 1, 0);
+  h->nb.clear();
+  std::vector<int32_t> tmp;
+  for (int64_t c = 0; c < ncells; ++c) {
+    tmp.clear();
+    for (int i = 0; i < nv; ++i)
+      for (int32_t o : node_cells[h->cell_nodes[c * nv + i]])
+        if (o != c) tmp.push_back(o);
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    h->nb.insert(h->nb.end(), tmp.begin(), tmp.end());
+    h->nb_off[c + 1] = (int32_t)h->nb.size();
+  }
+  h->structured = detect_structured(h);
+  if (h->structured) {
+    h->bin_off.assign(2, 0);
+    h->bin_cells.clear();
+  } else {
+    build_bins(h);
+  }
+  upload_mesh(h);
+  h->mesh_set = true;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_add_material(mpm_gpu_t h, int32_t id, const char* type, const char* json_props) {
+  MPM_GUARD(h)
+  if (!type || !json_props) throw InvalidArg("null material type or properties");
+  if (h->mat_index.count(id)) throw InvalidArg("New material cannot be added, insertion failed");
+  if (h->mats.size() >= 255) throw InvalidArg("too many materials");
+  const Json j = parse_json(json_props);
+  MaterialParams m = make_material(h->dim, type, j);
+  h->mat_index[id] = (int)h->mats.size();
+  h->mats.push_back(m);
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  h->d_mats.upload(h->mats.data(), h->mats.size(), h->stream);
+  MPM_END(h)
+  return MPM_OK;
+}
+
+static int add_vel_acc(mpm_gpu_t h, int64_t n, const int64_t* nid, const int32_t* dir,
+                       const double* val, bool vel) {
+  MPM_GUARD(h)
+  if (!h->mesh_set) throw InvalidArg("set the mesh first");
+  for (int64_t i = 0; i < n; ++i) {
+    if (nid[i] < 0 || nid[i] >= h->nnodes) throw InvalidArg("constraint node id out of range");
+    if (dir[i] < 0 || dir[i] >= h->dim) throw InvalidArg("Constraint direction is out of bounds");
+    HostBC& b = h->bcs[nid[i]];
+    if (vel)
+      b.vel.insert(std::make_pair((unsigned)dir[i], val[i]));
+    else {
+      if (b.vel.count((unsigned)dir[i]))
+        throw InvalidArg("Acceleration and velocity constraints set in the same direction for the same node");
+      b.acc.insert(std::make_pair((unsigned)dir[i], val[i]));
+    }
+  }
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  upload_bcs(h);
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_add_velocity_constraints(mpm_gpu_t h, int64_t n, const int64_t* nid, const int32_t* dir,
+                                     const double* val) {
+  return add_vel_acc(h, n, nid, dir, val, true);
+}
+
+int mpm_gpu_add_acceleration_constraints(mpm_gpu_t h, int64_t n, const int64_t* nid,
+                                         const int32_t* dir, const double* val) {
+  return add_vel_acc(h, n, nid, dir, val, false);
+}
+
+int mpm_gpu_add_friction_constraints(mpm_gpu_t h, int64_t n, const int64_t* nid, const int32_t* dir,
+                                     const int32_t* sign, const double* mu) {
+  MPM_GUARD(h)
+  if (!h->mesh_set) throw InvalidArg("set the mesh first");
+  for (int64_t i = 0; i < n; ++i) {
+    if (nid[i] < 0 || nid[i] >= h->nnodes) throw InvalidArg("constraint node id out of range");
+    if (dir[i] < 0 || dir[i] >= h->dim) throw InvalidArg("Constraint direction is out of bounds");
+    HostBC& b = h->bcs[nid[i]];
+    b.friction = true;
+    b.fdir = (unsigned)dir[i];
+    b.fsign = sign[i];
+    b.mu = mu[i];
+  }
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  upload_bcs(h);
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_add_particles(mpm_gpu_t h, int64_t n, const double* coords, int32_t material_id) {
+  MPM_GUARD(h)
+  if (h->initialised) throw InvalidArg("particles are added before mpm_gpu_initialise");
+  auto it = h->mat_index.find(material_id);
+  if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
+  if (n < 0 || (n > 0 && !coords)) throw InvalidArg("bad particle array");
+  if (h->np + n > INT32_MAX) throw InvalidArg("too many particles for 32-bit indices");
+  h->p_coords.insert(h->p_coords.end(), coords, coords + n * h->dim);
+  h->p_mat.insert(h->p_mat.end(), (size_t)n, (uint8_t)it->second);
+  h->np += n;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_initialise(mpm_gpu_t h) {
+  MPM_GUARD(h)
+  if (!h->mesh_set) throw InvalidArg("set the mesh first");
+  if (h->mats.empty()) throw InvalidArg("no material");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const int64_t np = h->np;
+  std::vector<int32_t> cell(np);
+  std::vector<int64_t> count(h->ncells, 0);
+  for (int64_t p = 0; p < np; ++p) {
+    cell[p] = host_scan(h, &h->p_coords[p * h->dim]);
+    if (cell[p] < 0) throw InvalidArg("Particle outside the mesh domain");
+    ++count[cell[p]];
+  }
+  std::vector<double> vol(np), rho(np), mass(np);
+  for (int64_t p = 0; p < np; ++p) {
+    const MaterialParams& m = h->mats[h->p_mat[p]];
+    vol[p] = h->cell_volume[cell[p]] / (double)count[cell[p]];
+    rho[p] = m.density;
+    mass[p] = vol[p] * rho[p];
+  }
+  allocate_particles(h);
+  if (h->p_vc.size() < (size_t)np) h->p_vc.resize(np);
+  upload_pvc(h);
+  mpm_gpu_particles in{};
+  in.volume = vol.data();
+  in.density = rho.data();
+  in.mass = mass.data();
+  pack_particles(h, &in, &cell);
+  refresh_state(h);
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  h->initialised = true;
+  h->step = 0;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_assign_particle_stresses(mpm_gpu_t h, int64_t n, const double* stress) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("No particles have been assigned in mesh, cannot assign stresses");
+  if (n != h->np || !stress) throw InvalidArg("Number of particles in mesh and initial stresses don't match");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const int dim = h->dim;
+  const int S = dim == 2 ? PF<2>::S : PF<3>::S;
+  const int ns = dim == 2 ? PF<2>::NS : PF<3>::NS;
+  std::vector<double> cols((size_t)ns * n);
+  for (int64_t p = 0; p < n; ++p) {
+    if (dim == 2 && (stress[p * 6 + 4] != 0. || stress[p * 6 + 5] != 0.))
+      throw InvalidArg("2D particle stress must have zero yz and xz components");
+    for (int k = 0; k < ns; ++k) cols[(size_t)k * n + p] = stress[p * 6 + k];
+  }
+  ck(cudaMemcpyAsync(h->d_pf.p + (size_t)S * n, cols.data(), sizeof(double) * cols.size(),
+                     cudaMemcpyHostToDevice, h->stream), "H2D");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_add_particle_velocity_constraint(mpm_gpu_t h, int64_t n, const int64_t* pids,
+                                             int32_t dir, double velocity) {
+  MPM_GUARD(h)
+  if (dir < 0 || dir >= h->dim) throw InvalidArg("Invalid direction of velocity constraint");
+  if (h->p_vc.size() < (size_t)h->np) h->p_vc.resize(h->np);
+  if (n < 0) {
+    for (int64_t p = 0; p < h->np; ++p) h->p_vc[p][(unsigned)dir] = velocity;
+  } else {
+    for (int64_t i = 0; i < n; ++i) {
+      if (pids[i] < 0 || pids[i] >= h->np) throw InvalidArg("particle id out of range");
+      h->p_vc[pids[i]][(unsigned)dir] = velocity;
+    }
+  }
+  if (h->initialised) {
+    ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+    upload_pvc(h);
+    refresh_state(h);
+  }
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) {
+  MPM_GUARD(h)
+  if (!h->mesh_set) throw InvalidArg("set the mesh first");
+  if (!in || !in->x || !in->volume || !in->cell || !in->material)
+    throw InvalidArg("load_particles needs x, volume, cell and material");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  h->np = n;
+  h->p_coords.assign(n * h->dim, 0.);
+  h->p_mat.resize(n);
+  for (int64_t p = 0; p < n; ++p) {
+    auto it = h->mat_index.find(in->material[p]);
+    if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
+    h->p_mat[p] = (uint8_t)it->second;
+  }
+  h->p_vc.assign(n, {});
+  allocate_particles(h);
+  upload_pvc(h);
+  pack_particles(h, in, nullptr);
+  refresh_state(h);
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  h->initialised = true;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("initialise or load particles first");
+  if (nsteps < 0) throw InvalidArg("negative step count");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  StepArgs a{};
+  a.scheme = h->cfg.scheme;
+  a.flip = h->cfg.velocity_update == MPM_VELOCITY_FLIP ? 1 : 0;
+  a.remove_lost = h->cfg.locate_particles ? 0 : 1;
+  a.dt = h->cfg.dt;
+  a.beta = h->cfg.blending_ratio;
+  a.damping = h->cfg.damping_factor;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (elapsed_ms) {
+    ck(cudaEventCreate(&e0), "cudaEventCreate");
+    ck(cudaEventCreate(&e1), "cudaEventCreate");
+    ck(cudaEventRecord(e0, h->stream), "cudaEventRecord");
+  }
+  for (int64_t s = 0; s < nsteps; ++s) {
+    double gm = 1.0;  // mpm_explicit.tcc:145-153
+    if (h->cfg.gravity_ramping_time > 0.0)
+      gm = std::min(1.0, static_cast<double>(h->step) * h->cfg.dt / h->cfg.gravity_ramping_time);
+    for (int d = 0; d < 3; ++d) a.g[d] = d < h->dim ? gm * h->cfg.gravity[d] : 0.;
+    launch_step_fp64(h->dim, h->ds, a, h->stream, h->prof);
+    ck(cudaGetLastError(), "kernel launch");
+    ++h->step;
+  }
+  if (elapsed_ms) ck(cudaEventRecord(e1, h->stream), "cudaEventRecord");
+  unsigned words[2] = {0, 0};
+  ck(cudaMemcpyAsync(words, h->d_words.p, sizeof(words), cudaMemcpyDeviceToHost, h->stream), "D2H");
+  ck(cudaStreamSynchronize(h->stream), "step");
+  h->prof.collect();
+  if (elapsed_ms) {
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+    *elapsed_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (words[1] & ERR_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite particle position");
+  if (words[1] & ERR_OUTSIDE) return fail(h, MPM_ERR_OUTSIDE, "Particle(s) outside the mesh domain");
+  if (words[1] & ERR_BADCELL) return fail(h, MPM_ERR_INVALID, "corrupt particle cell index");
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_step(mpm_gpu_t h, int64_t nsteps) { return run_steps(h, nsteps, nullptr); }
+
+int mpm_gpu_step_timed(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
+  if (!elapsed_ms) return fail(h, MPM_ERR_INVALID, "null elapsed_ms");
+  return run_steps(h, nsteps, elapsed_ms);
+}
+
+int mpm_gpu_set_profiling(mpm_gpu_t h, int32_t enable) {
+  MPM_GUARD(h)
+  h->prof.reset();
+  h->prof.enabled = enable != 0;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_kernel_profile(mpm_gpu_t h, int32_t kernel, const char** name, double* total_ms,
+                           int64_t* launches) {
+  if (!h) return MPM_ERR_INVALID;
+  if (kernel < 0 || kernel >= K_NKERNELS) return fail(h, MPM_ERR_INVALID, "kernel index out of range");
+  if (name) *name = kernel_name(kernel);
+  if (total_ms) *total_ms = h->prof.total_ms[kernel];
+  if (launches) *launches = h->prof.count[kernel];
+  return MPM_OK;
+}
+
+int64_t mpm_gpu_launch_count(mpm_gpu_t h) { return h ? h->prof.launches : -1; }
+
+int64_t mpm_gpu_nparticles(mpm_gpu_t h) { return h ? h->np : -1; }
+int64_t mpm_gpu_current_step(mpm_gpu_t h) { return h ? h->step : -1; }
+
+int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("no particles");
+  if (!out) throw InvalidArg("null output");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const int dim = h->dim;
+  const int64_t np = h->np;
+  std::vector<double> pf((size_t)h->nfields() * np);
+  std::vector<int32_t> cell(np);
+  std::vector<double> sv;
+  h->d_pf.download(pf.data(), pf.size(), h->stream);
+  h->d_cell.download(cell.data(), np, h->stream);
+  if (h->any_mc) {
+    sv.resize((size_t)SV_N * np);
+    h->d_sv.download(sv.data(), sv.size(), h->stream);
+  }
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  auto at = [&](int f, int64_t p) { return pf[(size_t)f * np + p]; };
+  const int X = dim == 2 ? PF<2>::X : PF<3>::X, U = dim == 2 ? PF<2>::U : PF<3>::U;
+  const int V = dim == 2 ? PF<2>::V : PF<3>::V, S = dim == 2 ? PF<2>::S : PF<3>::S;
+  const int E = dim == 2 ? PF<2>::E : PF<3>::E, Fo = dim == 2 ? PF<2>::F : PF<3>::F;
+  const int VOL = dim == 2 ? PF<2>::VOL : PF<3>::VOL, RHO = dim == 2 ? PF<2>::RHO : PF<3>::RHO;
+  const int MASS = dim == 2 ? PF<2>::MASS : PF<3>::MASS;
+  for (int64_t p = 0; p < np; ++p) {
+    for (int d = 0; d < 3; ++d) {
+      const bool in = d < dim;
+      if (out->x) out->x[p * 3 + d] = in ? at(X + d, p) : 0.;
+      if (out->u) out->u[p * 3 + d] = in ? at(U + d, p) : 0.;
+      if (out->v) out->v[p * 3 + d] = in ? at(V + d, p) : 0.;
+    }
+    if (dim == 2) {
+      if (out->stress) {
+        for (int k = 0; k < 4; ++k) out->stress[p * 6 + k] = at(S + k, p);
+        out->stress[p * 6 + 4] = out->stress[p * 6 + 5] = 0.;
+      }
+      if (out->strain) {
+        out->strain[p * 6 + 0] = at(E + 0, p);
+        out->strain[p * 6 + 1] = at(E + 1, p);
+        out->strain[p * 6 + 2] = 0.;
+        out->strain[p * 6 + 3] = at(E + 2, p);
+        out->strain[p * 6 + 4] = out->strain[p * 6 + 5] = 0.;
+      }
+      if (out->F) {
+        double* F = out->F + p * 9;
+        F[0] = at(Fo + 0, p);
+        F[1] = at(Fo + 1, p);
+        F[2] = 0.;
+        F[3] = at(Fo + 2, p);
+        F[4] = at(Fo + 3, p);
+        F[5] = 0.;
+        F[6] = 0.;
+        F[7] = 0.;
+        F[8] = 1.;
+      }
+    } else {
+      if (out->stress)
+        for (int k = 0; k < 6; ++k) out->stress[p * 6 + k] = at(S + k, p);
+      if (out->strain)
+        for (int k = 0; k < 6; ++k) out->strain[p * 6 + k] = at(E + k, p);
+      if (out->F)
+        for (int k = 0; k < 9; ++k) out->F[p * 9 + k] = at(Fo + k, p);
+    }
+    if (out->volume) out->volume[p] = at(VOL, p);
+    if (out->density) out->density[p] = at(RHO, p);
+    if (out->mass) out->mass[p] = at(MASS, p);
+    if (out->cell) out->cell[p] = cell[p];
+    if (out->material) {
+      int32_t id = -1;
+      for (auto& kv : h->mat_index)
+        if (kv.second == h->p_mat[p]) id = kv.first;
+      out->material[p] = id;
+    }
+    if (out->svars)
+      for (int k = 0; k < SV_N; ++k) out->svars[p * SV_N + k] = h->any_mc ? sv[(size_t)k * np + p] : 0.;
+  }
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_device_field(mpm_gpu_t h, int32_t field, void** base, int64_t* stride, int32_t* ncomp) {
+  MPM_GUARD(h)
+  if (!h->initialised || !base || !stride || !ncomp) throw InvalidArg("bad call");
+  const int dim = h->dim;
+  int off = 0, nc = 0;
+  switch (field) {
+    case 0: off = dim == 2 ? PF<2>::X : PF<3>::X; nc = dim; break;
+    case 1: off = dim == 2 ? PF<2>::U : PF<3>::U; nc = dim; break;
+    case 2: off = dim == 2 ? PF<2>::V : PF<3>::V; nc = dim; break;
+    case 3: off = dim == 2 ? PF<2>::S : PF<3>::S; nc = dim == 2 ? 4 : 6; break;
+    case 4: off = dim == 2 ? PF<2>::E : PF<3>::E; nc = dim == 2 ? 3 : 6; break;
+    case 5: off = dim == 2 ? PF<2>::F : PF<3>::F; nc = dim == 2 ? 4 : 9; break;
+    case 6: off = dim == 2 ? PF<2>::VOL : PF<3>::VOL; nc = 1; break;
+    case 7: off = dim == 2 ? PF<2>::RHO : PF<3>::RHO; nc = 1; break;
+    case 8: off = dim == 2 ? PF<2>::MASS : PF<3>::MASS; nc = 1; break;
+    default: throw InvalidArg("unknown field");
+  }
+  *base = h->d_pf.p + (size_t)off * h->np;
+  *stride = h->np;
+  *ncomp = nc;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_material_stress_batch(int32_t device, int32_t dim, const char* type,
+                                  const char* json_props, int64_t n, const double* stress,
+                                  const double* dstrain, const double* density, double* state,
+                                  double* out) {
+  if (dim != 2 && dim != 3) return MPM_ERR_INVALID;
+  if (n < 0 || !type || !json_props || (n > 0 && (!stress || !dstrain || !density || !state || !out)))
+    return MPM_ERR_INVALID;
+  try {
+    const MaterialParams m = make_material(dim, type, parse_json(json_props));
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    cudaStream_t st;
+    ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+    DevBuf<double> ds, dd, dr, dv, dout;
+    ds.upload(stress, n * 6, st);
+    dd.upload(dstrain, n * 6, st);
+    dr.upload(density, n, st);
+    dv.upload(state, n * SV_N, st);
+    dout.alloc(std::max<int64_t>(1, n * 6));
+    launch_material_batch_fp64(dim, n, m, ds.p, dd.p, dr.p, dv.p, dout.p, st);
+    ck(cudaGetLastError(), "launch");
+    dout.download(out, n * 6, st);
+    dv.download(state, n * SV_N, st);
+    ck(cudaStreamSynchronize(st), "sync");
+    cudaStreamDestroy(st);
+  } catch (const InvalidArg&) {
+    return MPM_ERR_INVALID;
+  } catch (const CudaError&) {
+    return MPM_ERR_CUDA;
+  } catch (const std::exception&) {
+    return MPM_ERR_INVALID;
+  }
+  return MPM_OK;
+}
+
+}  // extern "C"

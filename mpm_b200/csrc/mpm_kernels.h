@@ -1,0 +1,57 @@
+// mpm_kernels.h -- launch entry points shared by the kernel translation units
+// and the C-ABI host code.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mpm_state.cuh"
+
+namespace mpm_b200 {
+
+struct StepArgs {
+  int scheme;        // 0 USF, 1 USL
+  int flip;          // 1 FLIP, 0 PIC
+  int remove_lost;   // locate_particles false: unlocatable particles removed
+  double dt;
+  double beta;       // FLIP/PIC blending ratio
+  double damping;    // Cundall damping factor
+  double g[3];       // gravity of this step (ramp applied)
+};
+
+// Kernels of one step, for launch counting and per-kernel event timing.
+enum KernelId {
+  K_P2G = 0,        // P2G of mass and momentum (and, in USL, forces)
+  K_NODES_VEL,      // nodal velocity (USF) or full nodal update (USL)
+  K_STRESS_FORCES,  // USF: stress update + force P2G
+  K_NODES_ACC,      // USF: nodal acceleration / velocity update
+  K_G2P,            // G2P (+ USL stress update) + locate
+  K_LOCATE,         // exhaustive locate for particles that left their neighbourhood
+  K_NKERNELS
+};
+const char* kernel_name(int kid);
+
+// Counts launches; when enabled, brackets every launch with a pair of CUDA
+// events on the launching stream and accumulates their elapsed times.
+struct Profiler {
+  bool enabled = false;
+  int64_t launches = 0;
+  double total_ms[K_NKERNELS] = {};
+  int64_t count[K_NKERNELS] = {};
+  void begin(int kid, cudaStream_t st);
+  void end(int kid, cudaStream_t st);
+  void collect();  // after the stream has been synchronised
+  void reset();
+  ~Profiler();
+  struct Pending;
+  void* impl = nullptr;
+};
+
+void launch_step_fp64(int dim, const DevState& s, const StepArgs& a, cudaStream_t st,
+                      Profiler& prof);
+void launch_material_batch_fp64(int dim, int64_t n, const MaterialParams& m, const double* stress,
+                                const double* dstrain, const double* density, double* state,
+                                double* out, cudaStream_t st);
+
+}  // namespace mpm_b200

@@ -1,0 +1,687 @@
+// mpm_math.cuh -- per-particle and per-node arithmetic of the explicit MPM
+// step, written for the device (and usable on the host for set-up).
+//
+// The arithmetic follows the reference solver (geomechanics/mpm) operation by
+// operation so that the FP64 path agrees with it to rounding: sums run in the
+// reference's loop order, 2x2/3x3 inverses are adjugate / determinant as in
+// Eigen's fixed-size inverse, and the FP64 translation unit is compiled with
+// --fmad=false so no multiply-add is fused.  File:line citations are relative
+// to the reference source tree.
+#pragma once
+
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define MPM_HD __host__ __device__ __forceinline__
+#else
+#define MPM_HD inline
+#endif
+
+namespace mpm_b200 {
+
+constexpr double kDblEps = 2.220446049250313080847e-16;  // numeric_limits<double>::epsilon
+constexpr double kPiD = 3.14159265358979323846;           // M_PI
+
+template <int DIM>
+struct Elem;
+template <>
+struct Elem<2> {
+  static constexpr int NV = 4;
+};
+template <>
+struct Elem<3> {
+  static constexpr int NV = 8;
+};
+
+// ------------------------------------------------------------ shape functions
+// quadrilateral_element.tcc:11-22, hexahedron_element.tcc:19-34
+template <int DIM, typename R>
+MPM_HD void shapefn(const R* xi, R* N) {
+  if constexpr (DIM == 2) {
+    N[0] = R(0.25) * (1 - xi[0]) * (1 - xi[1]);
+    N[1] = R(0.25) * (1 + xi[0]) * (1 - xi[1]);
+    N[2] = R(0.25) * (1 + xi[0]) * (1 + xi[1]);
+    N[3] = R(0.25) * (1 - xi[0]) * (1 + xi[1]);
+  } else {
+    N[0] = R(0.125) * (1 - xi[0]) * (1 - xi[1]) * (1 - xi[2]);
+    N[1] = R(0.125) * (1 + xi[0]) * (1 - xi[1]) * (1 - xi[2]);
+    N[2] = R(0.125) * (1 + xi[0]) * (1 + xi[1]) * (1 - xi[2]);
+    N[3] = R(0.125) * (1 - xi[0]) * (1 + xi[1]) * (1 - xi[2]);
+    N[4] = R(0.125) * (1 - xi[0]) * (1 - xi[1]) * (1 + xi[2]);
+    N[5] = R(0.125) * (1 + xi[0]) * (1 - xi[1]) * (1 + xi[2]);
+    N[6] = R(0.125) * (1 + xi[0]) * (1 + xi[1]) * (1 + xi[2]);
+    N[7] = R(0.125) * (1 - xi[0]) * (1 + xi[1]) * (1 + xi[2]);
+  }
+}
+
+// Gradient in natural coordinates, G[n*DIM + k] = dN_n / dxi_k
+// quadrilateral_element.tcc:26-43, hexahedron_element.tcc:38-74
+template <int DIM, typename R>
+MPM_HD void grad_shapefn(const R* xi, R* G) {
+  if constexpr (DIM == 2) {
+    G[0] = R(-0.25) * (1 - xi[1]);
+    G[2] = R(0.25) * (1 - xi[1]);
+    G[4] = R(0.25) * (1 + xi[1]);
+    G[6] = R(-0.25) * (1 + xi[1]);
+    G[1] = R(-0.25) * (1 - xi[0]);
+    G[3] = R(-0.25) * (1 + xi[0]);
+    G[5] = R(0.25) * (1 + xi[0]);
+    G[7] = R(0.25) * (1 - xi[0]);
+  } else {
+    G[0 * 3 + 0] = R(-0.125) * (1 - xi[1]) * (1 - xi[2]);
+    G[1 * 3 + 0] = R(0.125) * (1 - xi[1]) * (1 - xi[2]);
+    G[2 * 3 + 0] = R(0.125) * (1 + xi[1]) * (1 - xi[2]);
+    G[3 * 3 + 0] = R(-0.125) * (1 + xi[1]) * (1 - xi[2]);
+    G[4 * 3 + 0] = R(-0.125) * (1 - xi[1]) * (1 + xi[2]);
+    G[5 * 3 + 0] = R(0.125) * (1 - xi[1]) * (1 + xi[2]);
+    G[6 * 3 + 0] = R(0.125) * (1 + xi[1]) * (1 + xi[2]);
+    G[7 * 3 + 0] = R(-0.125) * (1 + xi[1]) * (1 + xi[2]);
+    G[0 * 3 + 1] = R(-0.125) * (1 - xi[0]) * (1 - xi[2]);
+    G[1 * 3 + 1] = R(-0.125) * (1 + xi[0]) * (1 - xi[2]);
+    G[2 * 3 + 1] = R(0.125) * (1 + xi[0]) * (1 - xi[2]);
+    G[3 * 3 + 1] = R(0.125) * (1 - xi[0]) * (1 - xi[2]);
+    G[4 * 3 + 1] = R(-0.125) * (1 - xi[0]) * (1 + xi[2]);
+    G[5 * 3 + 1] = R(-0.125) * (1 + xi[0]) * (1 + xi[2]);
+    G[6 * 3 + 1] = R(0.125) * (1 + xi[0]) * (1 + xi[2]);
+    G[7 * 3 + 1] = R(0.125) * (1 - xi[0]) * (1 + xi[2]);
+    G[0 * 3 + 2] = R(-0.125) * (1 - xi[0]) * (1 - xi[1]);
+    G[1 * 3 + 2] = R(-0.125) * (1 + xi[0]) * (1 - xi[1]);
+    G[2 * 3 + 2] = R(-0.125) * (1 + xi[0]) * (1 + xi[1]);
+    G[3 * 3 + 2] = R(-0.125) * (1 - xi[0]) * (1 + xi[1]);
+    G[4 * 3 + 2] = R(0.125) * (1 - xi[0]) * (1 - xi[1]);
+    G[5 * 3 + 2] = R(0.125) * (1 + xi[0]) * (1 - xi[1]);
+    G[6 * 3 + 2] = R(0.125) * (1 + xi[0]) * (1 + xi[1]);
+    G[7 * 3 + 2] = R(0.125) * (1 - xi[0]) * (1 + xi[1]);
+  }
+}
+
+// inverse by adjugate / determinant (Eigen fixed-size 2x2 / 3x3 inverse)
+template <int DIM, typename R>
+MPM_HD void inverse(const R* J, R* inv) {
+  if constexpr (DIM == 2) {
+    const R det = J[0] * J[3] - J[2] * J[1];
+    const R invdet = R(1) / det;
+    inv[0] = J[3] * invdet;
+    inv[2] = -J[2] * invdet;
+    inv[1] = -J[1] * invdet;
+    inv[3] = J[0] * invdet;
+  } else {
+#define MPM_COF(i, j)                                                    \
+  (J[(((i) + 1) % 3) * 3 + (((j) + 1) % 3)] * J[(((i) + 2) % 3) * 3 + (((j) + 2) % 3)] - \
+   J[(((i) + 1) % 3) * 3 + (((j) + 2) % 3)] * J[(((i) + 2) % 3) * 3 + (((j) + 1) % 3)])
+    const R c0 = MPM_COF(0, 0), c1 = MPM_COF(1, 0), c2 = MPM_COF(2, 0);
+    const R det = (c0 * J[0] + c1 * J[3]) + c2 * J[6];
+    const R invdet = R(1) / det;
+    inv[0] = c0 * invdet;
+    inv[1] = c1 * invdet;
+    inv[2] = c2 * invdet;
+    inv[3] = MPM_COF(0, 1) * invdet;
+    inv[4] = MPM_COF(1, 1) * invdet;
+    inv[5] = MPM_COF(2, 1) * invdet;
+    inv[6] = MPM_COF(0, 2) * invdet;
+    inv[7] = MPM_COF(1, 2) * invdet;
+    inv[8] = MPM_COF(2, 2) * invdet;
+#undef MPM_COF
+  }
+}
+
+// dN/dx = G inv(J)^T with J = G^T X (quadrilateral_element.tcc:295-309,
+// hexahedron_element.tcc:307-321).  X[n*DIM + c] nodal coordinates.
+template <int DIM, typename R>
+MPM_HD void dn_dx(const R* xi, const R* X, R* D) {
+  constexpr int NV = Elem<DIM>::NV;
+  R G[NV * DIM];
+  grad_shapefn<DIM>(xi, G);
+  R J[DIM * DIM], inv[DIM * DIM];
+#pragma unroll
+  for (int r = 0; r < DIM; ++r)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      R s = G[0 * DIM + r] * X[0 * DIM + c];
+#pragma unroll
+      for (int n = 1; n < NV; ++n) s = s + G[n * DIM + r] * X[n * DIM + c];
+      J[r * DIM + c] = s;
+    }
+  inverse<DIM>(J, inv);
+#pragma unroll
+  for (int n = 0; n < NV; ++n)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      R s = G[n * DIM + 0] * inv[c * DIM + 0];
+#pragma unroll
+      for (int k = 1; k < DIM; ++k) s = s + G[n * DIM + k] * inv[c * DIM + k];
+      D[n * DIM + c] = s;
+    }
+}
+
+// ------------------------------------------------------------------- location
+// Per-cell geometry (cell.tcc:255-279 centroid and mean length; local
+// coordinate lengths cell.tcc:458-463, 566-571), computed once on the host.
+struct CellGeom {
+  double centroid[3];
+  double len[3];
+  double mean_length;
+};
+
+// cell.tcc:324-384 with local_coordinates_point (isoparametric false).
+// Returns true when the point is inside; xi is clamped to +-(1 - eps).
+template <int DIM>
+MPM_HD bool point_in_cell(const double* p, const double* centroid, const double* len,
+                          double mean_length, double* xi) {
+  double d[DIM];
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) d[i] = p[i] - centroid[i];
+  double s = d[0] * d[0];
+#pragma unroll
+  for (int i = 1; i < DIM; ++i) s = s + d[i] * d[i];
+  const double length = sqrt(s);
+  if (!(length < (mean_length * 2.))) return false;
+  bool status = true;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) {
+    double x = 2. * (p[i] - centroid[i]) / len[i];
+    if (x < -1. || x > 1. || x != x) {
+      status = false;
+    } else {
+      if (x < -1. + kDblEps) x = -1. + kDblEps;
+      if (x > 1. - kDblEps) x = 1. - kDblEps;
+    }
+    xi[i] = x;
+  }
+  return status;
+}
+
+// xi of a particle in the cell it was last located in (bit-identical to the
+// value the locate step stored: same formula, same inputs).
+template <int DIM>
+MPM_HD void local_xi(const double* p, const double* centroid, const double* len, double* xi) {
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) {
+    double x = 2. * (p[i] - centroid[i]) / len[i];
+    if (x < -1. + kDblEps) x = -1. + kDblEps;
+    if (x > 1. - kDblEps) x = 1. - kDblEps;
+    xi[i] = x;
+  }
+}
+
+// Index of the axis interval [a[i], a[i+1]] holding v (largest i with
+// a[i] <= v, clamped to [0, ncell-1]); a has ncell+1 ascending entries.
+MPM_HD int axis_interval(const double* a, int ncell, double v) {
+  int lo = 0, hi = ncell;  // a[lo] <= v < a[hi] invariant on the clamped range
+  if (!(v >= a[0])) return 0;
+  if (v >= a[ncell]) return ncell - 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] <= v)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// The first cell in id order containing p on a tensor-product grid: the
+// same answer as scanning every cell (a containing cell's box holds p up to
+// rounding, so only the intervals around p's interval can contain it).
+template <int DIM>
+MPM_HD int structured_scan(const double* p, const int32_t* ncell, const double* const* axis,
+                           const CellGeom* geom) {
+  int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  for (int d = 0; d < DIM; ++d) {
+    if (!(p[d] == p[d])) return -1;
+    const int i = axis_interval(axis[d], ncell[d], p[d]);
+    lo[d] = i > 0 ? i - 1 : 0;
+    hi[d] = i + 1 < ncell[d] ? i + 1 : ncell[d] - 1;
+  }
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i) {
+        const int c = DIM == 2 ? i + ncell[0] * j : i + ncell[0] * (j + ncell[1] * k);
+        double xi[DIM];
+        const CellGeom& g = geom[c];
+        if (point_in_cell<DIM>(p, g.centroid, g.len, g.mean_length, xi)) return c;
+      }
+  return -1;
+}
+
+// ------------------------------------------------------------------ materials
+struct MaterialParams {
+  int type;  // 0 LinearElastic, 1 MohrCoulomb
+  int softening;
+  double density, E, nu;
+  double bulk, shear, a1, a2;  // elastic tensor entries (a1 diag, a2 off-diag, G shear)
+  double phi_peak, psi_peak, c_peak, phi_res, psi_res, c_res;
+  double pd_peak, pd_res, tension_cutoff;
+  double grain_density, min_packing;
+  double tc_init;  // initial tension cutoff state (mohr_coulomb.tcc:97-100)
+};
+
+enum { SV_YIELD = 0, SV_PHI, SV_PSI, SV_COH, SV_TC, SV_EPS, SV_RHO, SV_THETA, SV_PD, SV_N };
+
+MPM_HD double check_low(double v) { return v > 1.0e-15 ? v : 1.0e-15; }  // mohr_coulomb.h:124
+
+// De * b for the isotropic elastic tensor, summed over k = 0..5 in order with
+// the zero entries of the dense 6x6 skipped (they add exact zeros).
+MPM_HD void de_mul(const MaterialParams& m, const double* b, double* o) {
+  const double a1 = m.a1, a2 = m.a2, G = m.shear;
+  o[0] = (a1 * b[0] + a2 * b[1]) + a2 * b[2];
+  o[1] = (a2 * b[0] + a1 * b[1]) + a2 * b[2];
+  o[2] = (a2 * b[0] + a2 * b[1]) + a1 * b[2];
+  o[3] = G * b[3];
+  o[4] = G * b[4];
+  o[5] = G * b[5];
+}
+
+// (a^T De) . b (mohr_coulomb.tcc:433,454-455)
+MPM_HD double row_de_dot(const MaterialParams& m, const double* a, const double* b) {
+  const double a1 = m.a1, a2 = m.a2, G = m.shear;
+  const double r0 = (a[0] * a1 + a[1] * a2) + a[2] * a2;
+  const double r1 = (a[0] * a2 + a[1] * a1) + a[2] * a2;
+  const double r2 = (a[0] * a2 + a[1] * a2) + a[2] * a1;
+  const double r3 = a[3] * G, r4 = a[4] * G, r5 = a[5] * G;
+  return ((((r0 * b[0] + r1 * b[1]) + r2 * b[2]) + r3 * b[3]) + r4 * b[4]) + r5 * b[5];
+}
+
+// updated += -((lambda * De) * v)  (mohr_coulomb.tcc:463,468,502)
+MPM_HD void sub_lambda_de(const MaterialParams& m, double lambda, const double* v, double* u) {
+  const double l1 = lambda * m.a1, l2 = lambda * m.a2, lg = lambda * m.shear;
+  u[0] += -((l1 * v[0] + l2 * v[1]) + l2 * v[2]);
+  u[1] += -((l2 * v[0] + l1 * v[1]) + l2 * v[2]);
+  u[2] += -((l2 * v[0] + l2 * v[1]) + l1 * v[2]);
+  u[3] += -(lg * v[3]);
+  u[4] += -(lg * v[4]);
+  u[5] += -(lg * v[5]);
+}
+
+// material_utility.tcc:2-200
+MPM_HD double mu_p(const double* s) { return (1. / 3. * (s[0] + s[1] + s[2])); }
+MPM_HD double sq(double x) { return x * x; }
+MPM_HD double mu_j2(const double* s) {
+  return (sq(s[0] - s[1]) + sq(s[1] - s[2]) + sq(s[0] - s[2])) / 6.0 + sq(s[3]) + sq(s[4]) +
+         sq(s[5]);
+}
+MPM_HD double mu_j3(const double* s) {
+  const double p = mu_p(s);
+  const double d0 = s[0] - p, d1 = s[1] - p, d2 = s[2] - p;
+  return (d0 * d1 * d2) - (d2 * sq(s[3])) +
+         ((2 * s[3] * s[4] * s[5]) - (d0 * sq(s[4])) - (d1 * sq(s[5])));
+}
+
+struct Invariants {
+  double eps, rho, theta;
+};
+
+// mohr_coulomb.tcc:124-134 with lode_angle (material_utility.tcc:65-81)
+MPM_HD void mc_invariants(const double* s, double* sv) {
+  const double j2 = mu_j2(s);
+  const double j3 = mu_j3(s);
+  sv[SV_EPS] = mu_p(s) * sqrt(3.);
+  double v = 0.0;
+  if (fabs(j2) > kDblEps) v = (3. * sqrt(3.) / 2.) * (j3 / pow(j2, 1.5));
+  if (v > 1.0) v = 1.0;
+  if (v < -1.0) v = -1.0;
+  sv[SV_THETA] = (1. / 3.) * acos(v);
+  sv[SV_RHO] = sqrt(2. * j2);
+}
+
+enum { MC_ELASTIC = 0, MC_SHEAR = 1, MC_TENSILE = 2, MC_SEPARATED = 3 };
+
+// mohr_coulomb.tcc:139-191
+MPM_HD int mc_yield_state(double* yf, const double* sv) {
+  const double Tolerance = -1E-1;
+  const double epsilon = sv[SV_EPS], rho = sv[SV_RHO], theta = sv[SV_THETA];
+  const double phi = sv[SV_PHI], cohesion = sv[SV_COH], tension_cutoff = sv[SV_TC];
+  yf[0] = sqrt(2. / 3.) * cos(theta) * rho + epsilon / sqrt(3.) - tension_cutoff;
+  yf[1] = sqrt(1.5) * rho *
+              ((sin(theta + kPiD / 3.) / (sqrt(3.) * cos(phi))) +
+               (cos(theta + kPiD / 3.) * tan(phi) / 3.)) +
+          (epsilon / sqrt(3.)) * tan(phi) - cohesion;
+  int yield_type = MC_ELASTIC;
+  if (yf[0] > Tolerance && yf[1] > Tolerance) {
+    const double n_phi = (1. + sin(phi)) / (1. - sin(phi));
+    const double sigma_p = tension_cutoff * n_phi - 2. * cohesion * sqrt(n_phi);
+    const double alpha_p = sqrt(1. + n_phi * n_phi) + n_phi;
+    const double h = yf[0] + alpha_p * (sqrt(2. / 3.) * cos(theta - 4. * kPiD / 3.) * rho +
+                                        epsilon / sqrt(3.) - sigma_p);
+    yield_type = (h > kDblEps) ? MC_TENSILE : MC_SHEAR;
+  }
+  if (yf[0] < Tolerance && yf[1] > Tolerance) yield_type = MC_SHEAR;
+  if (yf[0] > Tolerance && yf[1] < Tolerance) yield_type = MC_TENSILE;
+  return yield_type;
+}
+
+// mohr_coulomb.tcc:195-344 (dF/dsigma, dP/dsigma, dP/dq, softening)
+MPM_HD void mc_df_dp(const MaterialParams& m, int yield_type, const double* sv, const double* s,
+                     double* df, double* dp, double* dp_dq, double* softening) {
+  const double rho = sv[SV_RHO], theta = sv[SV_THETA];
+  const double phi = sv[SV_PHI], psi = sv[SV_PSI], tension_cutoff = sv[SV_TC];
+  const double pdstrain = sv[SV_PD];
+  double df_depsilon, df_drho, df_dtheta;
+  if (yield_type == MC_TENSILE) {
+    df_depsilon = 1. / sqrt(3.);
+    df_drho = sqrt(2. / 3.) * cos(theta);
+    df_dtheta = -sqrt(2. / 3.) * rho * sin(theta);
+  } else {
+    df_depsilon = tan(phi) / sqrt(3.);
+    df_drho = sqrt(1.5) * ((sin(theta + kPiD / 3.) / (sqrt(3.) * cos(phi))) +
+                           (cos(theta + kPiD / 3.) * tan(phi) / 3.));
+    df_dtheta = sqrt(1.5) * rho *
+                ((cos(theta + kPiD / 3.) / (sqrt(3.) * cos(phi))) -
+                 (sin(theta + kPiD / 3.) * tan(phi) / 3.));
+  }
+  // dEpsilon/dsigma = dp/dsigma * sqrt(3); dRho/dsigma = dq/dsigma * sqrt(2/3)
+  const double deps_ds = 1. / 3. * sqrt(3.);
+  const double j2 = mu_j2(s);
+  const double q = sqrt(3 * j2);
+  const double pm = mu_p(s);
+  double dev[6] = {s[0] - pm, s[1] - pm, s[2] - pm, s[3], s[4], s[5]};
+  double drho_ds[6] = {0, 0, 0, 0, 0, 0};
+  if (fabs(q) > kDblEps) {
+    drho_ds[0] = 3. / (2. * q) * dev[0];
+    drho_ds[1] = 3. / (2. * q) * dev[1];
+    drho_ds[2] = 3. / (2. * q) * dev[2];
+    drho_ds[3] = 3. / q * dev[3];
+    drho_ds[4] = 3. / q * dev[4];
+    drho_ds[5] = 3. / q * dev[5];
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) drho_ds[i] *= sqrt(2. / 3.);
+  // dtheta/dsigma (material_utility.tcc:166-200)
+  double dtheta_ds[6];
+  {
+    const double j3 = mu_j3(s);
+    const double dj2[6] = {dev[0], dev[1], dev[2], dev[3] * 2.0, dev[4] * 2.0, dev[5] * 2.0};
+    const double dev1[3] = {dev[0], dev[3], dev[5]};
+    const double dev2[3] = {dev[3], dev[1], dev[4]};
+    const double dev3[3] = {dev[5], dev[4], dev[2]};
+    auto dot3 = [](const double* a, const double* b) {
+      return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
+    };
+    const double dj3[6] = {dot3(dev1, dev1) - (2. / 3.) * j2, dot3(dev2, dev2) - (2. / 3.) * j2,
+                           dot3(dev3, dev3) - (2. / 3.) * j2, 2.0 * dot3(dev1, dev2),
+                           2.0 * dot3(dev2, dev3),           2.0 * dot3(dev1, dev3)};
+    double dr_dj2 = -9.0 / 4.0 * sqrt(3.0) * j3;
+    double dr_dj3 = 3.0 / 2.0 * sqrt(3.0);
+    double dtheta_dr = -1.0 / 3.0;
+    if (fabs(j2) > kDblEps) {
+      const double r = j3 / 2.0 * pow(j2 / 3.0, -1.5);
+      dr_dj2 *= pow(j2, -2.5);
+      dr_dj3 *= pow(j2, -1.5);
+      const double factor = (fabs(1 - r * r) < kDblEps) ? kDblEps : fabs(1 - r * r);
+      dtheta_dr = -1.0 / (3.0 * sqrt(factor));
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) dtheta_ds[i] = dtheta_dr * ((dr_dj2 * dj2[i]) + (dr_dj3 * dj3[i]));
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+    df[i] = ((df_depsilon * (i < 3 ? deps_ds : 0.)) + (df_drho * drho_ds[i])) +
+            (df_dtheta * dtheta_ds[i]);
+  if (yield_type == MC_TENSILE) {
+    const double et_value = 0.6;
+    const double xit = 0.1;
+    const double ct = cos(theta), st = sin(theta);
+    double sqpart = 4. * (1 - et_value * et_value) * ct * ct + 5. * et_value * et_value -
+                    4. * et_value;
+    if (sqpart < kDblEps) sqpart = 1.E-5;
+    double rt_den = 2. * (1 - et_value * et_value) * ct + (2. * et_value - 1) * sqrt(sqpart);
+    const double rt_num =
+        4. * (1 - et_value * et_value) * ct * ct + (2. * et_value - 1) * (2. * et_value - 1);
+    if (fabs(rt_den) < kDblEps) rt_den = 1.E-5;
+    const double rt = rt_num / (3. * rt_den);
+    const double den = check_low(
+        sqrt(xit * xit * tension_cutoff * tension_cutoff + 1.5 * rt * rt * rho * rho));
+    const double dp_drt = 1.5 * rho * rho * rt / den;
+    const double dp_drho = 1.5 * rho * rt * rt / den;
+    const double dp_depsilon = 1. / sqrt(3.);
+    const double drtden_dtheta =
+        -2. * (1 - et_value * et_value) * st -
+        (2. * et_value - 1) * 4. * (1 - et_value * et_value) * ct * st /
+            sqrt(4. * (1 - et_value * et_value) * ct * ct + 5. * et_value * et_value -
+                 4. * et_value);
+    const double drtnum_dtheta = -8. * (1 - et_value * et_value) * ct * st;
+    const double drt_dtheta =
+        (drtnum_dtheta * rt_den - drtden_dtheta * rt_num) / (3. * rt_den * rt_den);
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+      dp[i] = ((dp_depsilon * (i < 3 ? deps_ds : 0.)) + (dp_drho * drho_ds[i])) +
+              (dp_drt * drt_dtheta * dtheta_ds[i]);
+    *dp_dq = dp_drho * sqrt(2. / 3.);
+  } else {
+    const double sphi = sin(phi), cphi = cos(phi);
+    const double ct = cos(theta), st = sin(theta);
+    const double r_mc = (3. - sphi) / (6 * cphi);
+    double e_val = (3. - sphi) / (3. + sphi);
+    if (e_val <= 0.5) e_val = 0.5 + 1.E-10;
+    if (e_val > 1.) e_val = 1.;
+    double sqpart = (4. * (1 - e_val * e_val) * sq(ct)) + (5 * e_val * e_val) - (4. * e_val);
+    if (sqpart < kDblEps) sqpart = 1.E-5;
+    double mm = (2. * (1 - e_val * e_val) * ct) + ((2. * e_val - 1) * sqrt(sqpart));
+    if (fabs(mm) < kDblEps) mm = 1.E-5;
+    const double l = (4. * (1. - e_val * e_val) * sq(ct)) + sq(2. * e_val - 1.);
+    const double r_mw = (l / mm) * r_mc;
+    const double xi = 0.1;
+    double omega = sq(xi * m.c_peak * tan(psi)) + sq(r_mw * sqrt(1.5) * rho);
+    if (omega < kDblEps) omega = 1.E-5;
+    const double dl_dtheta = -8. * (1. - e_val * e_val) * ct * st;
+    const double dm_dtheta =
+        (-2. * (1. - e_val * e_val) * st) + (0.5 * (2. * e_val - 1.) * dl_dtheta) / sqrt(sqpart);
+    const double drmw_dtheta = ((mm * dl_dtheta) - (l * dm_dtheta)) / (mm * mm);
+    const double dp_depsilon = tan(psi) / sqrt(3.);
+    const double dp_drho = 3. * rho * r_mw * r_mw / (2. * sqrt(omega));
+    const double dp_dtheta = (3. * rho * rho * r_mw * r_mc * drmw_dtheta) / (2. * sqrt(omega));
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+      dp[i] = ((dp_depsilon * (i < 3 ? deps_ds : 0.)) + (dp_drho * drho_ds[i])) +
+              (dp_dtheta * dtheta_ds[i]);
+    *dp_dq = dp_drho * sqrt(2. / 3.);
+  }
+  *softening = 0.;
+  if (m.softening && pdstrain > m.pd_peak && pdstrain < m.pd_res) {
+    const double dphi_dpstrain = (m.phi_res - m.phi_peak) / (m.pd_res - m.pd_peak);
+    const double dc_dpstrain = (m.c_res - m.c_peak) / (m.pd_res - m.pd_peak);
+    const double df_dphi =
+        sqrt(1.5) * rho *
+            ((sin(phi) * sin(theta + kPiD / 3.) / (sqrt(3.) * cos(phi) * cos(phi))) +
+             (cos(theta + kPiD / 3.) / (3. * cos(phi) * cos(phi)))) +
+        (mu_p(s) / (cos(phi) * cos(phi)));
+    const double df_dc = -1.;
+    *softening = (-1.) * ((df_dphi * dphi_dpstrain) + (df_dc * dc_dpstrain)) * (*dp_dq);
+  }
+}
+
+// MohrCoulomb<Tdim>::compute_stress (mohr_coulomb.tcc:348-513), stress_rate
+// None (infinitesimal_elasto_plastic.tcc:2-25).  sv holds the nine state
+// variables in the reference order.
+MPM_HD void mc_compute_stress(const MaterialParams& m, const double* stress,
+                              const double* dstrain, double density, double* sv, double* out) {
+  const double critical_density = m.min_packing * m.grain_density;
+  const double pdstrain = sv[SV_PD];
+  if (m.softening && pdstrain > m.pd_peak) {
+    if (pdstrain < m.pd_res) {
+      sv[SV_PHI] = m.phi_res + ((m.phi_peak - m.phi_res) * (pdstrain - m.pd_res) /
+                                (m.pd_peak - m.pd_res));
+      sv[SV_PSI] = m.psi_res + ((m.psi_peak - m.psi_res) * (pdstrain - m.pd_res) /
+                                (m.pd_peak - m.pd_res));
+      sv[SV_COH] = m.c_res + ((m.c_peak - m.c_res) * (pdstrain - m.pd_res) / (m.pd_peak - m.pd_res));
+    } else {
+      sv[SV_PHI] = m.phi_res;
+      sv[SV_PSI] = m.psi_res;
+      sv[SV_COH] = m.c_res;
+    }
+    const double apex = sv[SV_COH] / tan(sv[SV_PHI]);
+    if (sv[SV_TC] > apex) sv[SV_TC] = check_low(apex);
+  }
+  sv[SV_YIELD] = 0;
+  double trial[6];
+  {
+    double t[6];
+    de_mul(m, dstrain, t);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) trial[i] = stress[i] + t[i];
+  }
+  if (density <= critical_density) {
+    sv[SV_PD] += sqrt(3 * mu_j2(trial)) / 3.0 / m.shear;
+    sv[SV_YIELD] = 3;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) out[i] = 0.;
+    return;
+  }
+  mc_invariants(trial, sv);
+  double yf_trial[2];
+  int yt_trial = mc_yield_state(yf_trial, sv);
+  if (yt_trial == MC_ELASTIC) {
+    sv[SV_YIELD] = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) out[i] = trial[i];
+    return;
+  }
+  const double Tolerance = 1E-1;
+  double softening_trial = 0., dp_dq_trial = 0.;
+  double df_trial[6], dp_trial[6];
+  mc_df_dp(m, yt_trial, sv, trial, df_trial, dp_trial, &dp_dq_trial, &softening_trial);
+  double yield_trial = 0.;
+  if (yt_trial == MC_TENSILE) {
+    sv[SV_YIELD] = 2;
+    yield_trial = yf_trial[0];
+  }
+  if (yt_trial == MC_SHEAR) {
+    sv[SV_YIELD] = 1;
+    yield_trial = yf_trial[1];
+  }
+  double lambda_trial = yield_trial / (row_de_dot(m, df_trial, dp_trial) + softening_trial);
+  mc_invariants(stress, sv);
+  double yf[2];
+  const int yt = mc_yield_state(yf, sv);
+  double yield = 1.7976931348623157e308;
+  if (yt == MC_TENSILE) yield = yf[0];
+  if (yt == MC_SHEAR) yield = yf[1];
+  double softening = 0., dp_dq = 0.;
+  double df[6], dp[6];
+  mc_df_dp(m, yt, sv, stress, df, dp, &dp_dq, &softening);
+  const double lambda = row_de_dot(m, df, dstrain) / (row_de_dot(m, df, dp) + softening);
+  double upd[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) upd[i] = trial[i];
+  double dpdstrain;
+  if (fabs(yield) < Tolerance) {
+    sub_lambda_de(m, lambda, dp, upd);
+    dpdstrain = lambda * dp_dq;
+  } else {
+    sub_lambda_de(m, lambda_trial, dp_trial, upd);
+    dpdstrain = lambda_trial * dp_dq_trial;
+  }
+  for (int itr = 0; itr < 100; ++itr) {
+    mc_invariants(upd, sv);
+    yt_trial = mc_yield_state(yf_trial, sv);
+    if (yf_trial[0] < Tolerance && yf_trial[1] < Tolerance) break;
+    mc_df_dp(m, yt_trial, sv, upd, df_trial, dp_trial, &dp_dq_trial, &softening_trial);
+    if (yt_trial == MC_TENSILE) yield_trial = yf_trial[0];
+    if (yt_trial == MC_SHEAR) yield_trial = yf_trial[1];
+    lambda_trial = yield_trial / (row_de_dot(m, df_trial, dp_trial) + softening_trial);
+    sub_lambda_de(m, lambda_trial, dp_trial, upd);
+    dpdstrain += lambda_trial * dp_dq_trial;
+  }
+  mc_invariants(upd, sv);
+  sv[SV_PD] += dpdstrain;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) out[i] = upd[i];
+}
+
+// Material<Tdim>::compute_stress dispatch (material.h:97-106)
+MPM_HD void material_compute_stress(const MaterialParams& m, const double* stress,
+                                    const double* dstrain, double density, double* sv,
+                                    double* out) {
+  if (m.type == 0) {
+    double t[6];
+    de_mul(m, dstrain, t);  // linear_elastic.tcc:73-94
+#pragma unroll
+    for (int i = 0; i < 6; ++i) out[i] = stress[i] + t[i];
+  } else {
+    mc_compute_stress(m, stress, dstrain, density, sv, out);
+  }
+}
+
+// ---------------------------------------------------------------- node update
+struct NodeBC {
+  // velocity constraints (node.tcc:370-403); mask bit d = direction d
+  uint8_t vel_mask, acc_mask, friction, fric_dir;
+  int32_t fric_sign;
+  double vel[3];
+  double acc[3];
+  double mu;
+};
+
+template <int DIM>
+MPM_HD void apply_velocity_constraints(const NodeBC& bc, double* v, double* a) {
+#pragma unroll
+  for (int d = 0; d < DIM; ++d)
+    if (bc.vel_mask & (1u << d)) {
+      v[d] = bc.vel[d];
+      a[d] = 0.;
+    }
+}
+
+// node.tcc:510-657 (Cartesian boundaries)
+template <int DIM>
+MPM_HD void apply_friction_constraints(const NodeBC& bc, const double* vel, double* acc,
+                                       double dt) {
+  auto sign = [](double value) { return (value > 0.) ? 1. : -1.; };
+  const unsigned dir_n = bc.fric_dir;
+  const double sign_n = sign((double)bc.fric_sign);
+  const double mu = bc.mu;
+  if constexpr (DIM == 2) {
+    const unsigned dir_t = 1 - dir_n;
+    const double acc_n = acc[dir_n];
+    double acc_t = acc[dir_t];
+    const double vel_t = vel[dir_t];
+    if ((acc_n * sign_n) > 0.0) {
+      if (vel_t != 0.0) {
+        const double vel_net = dt * acc_t + vel_t;
+        const double vel_frictional = dt * mu * fabs(acc_n);
+        if (fabs(vel_net) <= vel_frictional)
+          acc_t = -vel_t / dt;
+        else
+          acc_t -= sign(vel_net) * mu * fabs(acc_n);
+      } else {
+        if (fabs(acc_t) <= mu * fabs(acc_n))
+          acc_t = 0.0;
+        else
+          acc_t -= sign(acc_t) * mu * fabs(acc_n);
+      }
+      acc[dir_t] = acc_t;
+    }
+  } else {
+    const unsigned t0 = dir_n == 0 ? 1 : 0;
+    const unsigned t1 = dir_n == 2 ? 1 : 2;
+    const double acc_n = acc[dir_n];
+    double acc_t = sqrt(acc[t0] * acc[t0] + acc[t1] * acc[t1]);
+    const double vel_t = sqrt(vel[t0] * vel[t0] + vel[t1] * vel[t1]);
+    if (acc_n * sign_n > 0.0) {
+      if (vel_t != 0.0) {
+        const double vn0 = vel[t0] + acc[t0] * dt;
+        const double vn1 = vel[t1] + acc[t1] * dt;
+        const double vel_net_t = sqrt(vn0 * vn0 + vn1 * vn1);
+        const double vel_fricion = mu * fabs(acc_n) * dt;
+        if (vel_net_t <= vel_fricion) {
+          acc[t0] = -vel[t0] / dt;
+          acc[t1] = -vel[t1] / dt;
+        } else {
+          acc[t0] -= mu * fabs(acc_n) * (vn0 / vel_net_t);
+          acc[t1] -= mu * fabs(acc_n) * (vn1 / vel_net_t);
+        }
+      } else {
+        if (acc_t <= mu * fabs(acc_n)) {
+          acc[t0] = 0;
+          acc[t1] = 0;
+        } else {
+          acc_t -= mu * fabs(acc_n);
+          acc[t0] -= mu * fabs(acc_n) * (acc[t0] / acc_t);
+          acc[t1] -= mu * fabs(acc_n) * (acc[t1] / acc_t);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace mpm_b200

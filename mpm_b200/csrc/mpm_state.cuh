@@ -1,0 +1,97 @@
+// mpm_state.cuh -- device-resident state of one solver and its field layout.
+//
+// Particles are structure-of-arrays: every scalar field is a contiguous array
+// of np doubles, so a warp reads 32 consecutive particles' value of a field
+// in one 256-byte transaction.  Fields that never change in 2D (stress yz/xz,
+// strain zz/yz/xz, the third row and column of F) are not stored in 2D.
+#pragma once
+
+#include <cstdint>
+
+#include "mpm_math.cuh"
+
+namespace mpm_b200 {
+
+// particle field offsets (units of np doubles)
+template <int DIM>
+struct PF;
+template <>
+struct PF<3> {
+  static constexpr int X = 0, U = 3, V = 6, S = 9, E = 15, F = 21, VOL = 30, RHO = 31,
+                       MASS = 32, NF = 33;
+  static constexpr int NS = 6, NE = 6, NFG = 9;
+};
+template <>
+struct PF<2> {
+  // stress xx,yy,zz,xy; strain xx,yy,xy; F 00,01,10,11
+  static constexpr int X = 0, U = 2, V = 4, S = 6, E = 10, F = 13, VOL = 17, RHO = 18,
+                       MASS = 19, NF = 20;
+  static constexpr int NS = 4, NE = 3, NFG = 4;
+};
+
+// node field offsets (units of nn doubles)
+template <int DIM>
+struct NF {
+  static constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM,
+                       NACC_FIELDS = 1 + 3 * DIM,  // accumulated by P2G, zeroed every step
+                       VEL = 1 + 3 * DIM, ACC = 1 + 4 * DIM, NNF = 1 + 5 * DIM;
+};
+
+// particle velocity constraint record: mask bit d => v[d] = value[d]
+struct ParticleVC {
+  uint32_t mask;
+  uint32_t pad;
+  double value[3];
+};
+
+enum ErrorBits : unsigned {
+  ERR_OUTSIDE = 1u,     // a particle left the mesh (locate_particles on)
+  ERR_NONFINITE = 2u,   // NaN or Inf in a particle position
+  ERR_BADCELL = 4u      // corrupt cell index found by a bounds check
+};
+
+struct DevState {
+  int64_t np = 0;          // particle rows
+  double* pf = nullptr;    // [PF::NF][np]
+  double* sv = nullptr;    // [SV_N][np] MohrCoulomb state (null when no MC)
+  int32_t* cell = nullptr; // [np] current cell, -1 removed
+  uint8_t* mat = nullptr;  // [np] material slot
+  int16_t* pvc = nullptr;  // [np] particle velocity constraint slot (-1 none)
+
+  int64_t nn = 0;          // nodes
+  double* nf = nullptr;    // [NF::NNF][nn]
+  uint8_t* active = nullptr;     // [nn] node belongs to a cell holding particles
+  int32_t* bc_index = nullptr;   // [nn] slot in bcs or -1
+
+  int64_t ncells = 0;
+  int32_t* cell_nodes = nullptr; // [ncells][NV]
+  double* ncoord = nullptr;      // [DIM][nn]
+  CellGeom* geom = nullptr;      // [ncells]
+  int32_t* nb_off = nullptr;     // [ncells + 1] neighbour CSR (ascending ids)
+  int32_t* nb = nullptr;
+
+  // uniform bins over the cells' containment spheres, for the exhaustive
+  // search (equivalent to scanning every cell in id order)
+  int32_t* bin_off = nullptr;
+  int32_t* bin_cells = nullptr;
+  double bmin[3] = {0, 0, 0};
+  double bsize[3] = {1, 1, 1};
+  int32_t bn[3] = {1, 1, 1};
+
+  // tensor-product grid (node (i,j,k) = i + nx*(j + ny*k) at (ax[i], ay[j],
+  // az[k]); lexicographic cells): the exhaustive search needs only the
+  // 3^dim cells around the axis interval that holds the point
+  int structured = 0;
+  int32_t gcells[3] = {1, 1, 1};     // cells per axis
+  const double* axis[3] = {nullptr, nullptr, nullptr};  // node coordinates per axis
+
+  int32_t* lost = nullptr;       // [np] particles not found in cell or neighbours
+  unsigned* nlost = nullptr;
+  unsigned* err = nullptr;       // ErrorBits
+
+  const MaterialParams* mats = nullptr;
+  const NodeBC* bcs = nullptr;
+  const ParticleVC* pvcs = nullptr;
+};
+
+}  // namespace mpm_b200

@@ -1,0 +1,233 @@
+"""Python host side of the explicit MPM step on the B200.
+
+``MPMExplicit`` mirrors the reference's solver surface (mpm::MPMExplicit,
+include/solvers/mpm_explicit.tcc): it is built from a ``Problem`` (mesh,
+materials, constraints, particles, analysis settings) or from the reference's
+own JSON input (``MPMExplicit.from_input``), and advances with ``solve()`` or
+``step(n)``.  All arithmetic runs in libmpm_b200.so through its C ABI.
+"""
+import ctypes as C
+import json
+
+import numpy as np
+
+from . import _native
+from ._native import MPMError
+
+SCHEMES = {"usf": 0, "usl": 1}
+VELOCITY_UPDATES = {"flip": 0, "pic": 1}
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _i64p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def _i32p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+class Solver:
+    """Thin owner of one ``mpm_gpu_t`` handle."""
+
+    def __init__(self, dim, scheme="usf", velocity_update="flip", dt=1e-5, gravity=(0, 0, 0),
+                 damping_factor=0.0, blending_ratio=1.0, gravity_ramping_time=0.0,
+                 locate_particles=True, precision="fp64", device=0):
+        L = _native.lib()
+        cfg = _native.Config()
+        cfg.dim = dim
+        cfg.scheme = SCHEMES[scheme]
+        cfg.velocity_update = VELOCITY_UPDATES[velocity_update]
+        cfg.precision = PRECISIONS[precision]
+        cfg.blending_ratio = blending_ratio
+        cfg.dt = dt
+        cfg.damping_factor = damping_factor
+        g = list(gravity) + [0.0] * (3 - len(gravity))
+        for i in range(3):
+            cfg.gravity[i] = g[i]
+        cfg.gravity_ramping_time = gravity_ramping_time
+        cfg.locate_particles = 1 if locate_particles else 0
+        cfg.device = device
+        h = C.c_void_p()
+        rc = L.mpm_gpu_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise MPMError(rc, "mpm_gpu_create failed")
+        self.h = h
+        self.dim = dim
+        self.L = L
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mpm_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        if rc != 0:
+            raise MPMError(rc, self.L.mpm_gpu_last_error(self.h).decode())
+
+    def set_mesh(self, coords, cells):
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        cells = np.ascontiguousarray(cells, dtype=np.int64)
+        self._ck(self.L.mpm_gpu_set_mesh(self.h, coords.shape[0], _dp(coords), cells.shape[0],
+                                         cells.shape[1], _i64p(cells)))
+
+    def add_material(self, mid, mtype, props):
+        self._ck(self.L.mpm_gpu_add_material(self.h, mid, mtype.encode(),
+                                             json.dumps(props).encode()))
+
+    def _nodal(self, fn, nid, direction, value):
+        nid = np.ascontiguousarray(nid, dtype=np.int64)
+        d = np.ascontiguousarray(direction, dtype=np.int32)
+        v = np.ascontiguousarray(value, dtype=np.float64)
+        self._ck(fn(self.h, len(nid), _i64p(nid), _i32p(d), _dp(v)))
+
+    def add_velocity_constraints(self, nid, direction, value):
+        self._nodal(self.L.mpm_gpu_add_velocity_constraints, nid, direction, value)
+
+    def add_acceleration_constraints(self, nid, direction, value):
+        self._nodal(self.L.mpm_gpu_add_acceleration_constraints, nid, direction, value)
+
+    def add_friction_constraints(self, nid, direction, sign_n, mu):
+        nid = np.ascontiguousarray(nid, dtype=np.int64)
+        d = np.ascontiguousarray(direction, dtype=np.int32)
+        s = np.ascontiguousarray(sign_n, dtype=np.int32)
+        m = np.ascontiguousarray(mu, dtype=np.float64)
+        self._ck(self.L.mpm_gpu_add_friction_constraints(self.h, len(nid), _i64p(nid), _i32p(d),
+                                                         _i32p(s), _dp(m)))
+
+    def add_particles(self, coords, material_id):
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        self._ck(self.L.mpm_gpu_add_particles(self.h, coords.shape[0], _dp(coords), material_id))
+
+    def initialise(self):
+        self._ck(self.L.mpm_gpu_initialise(self.h))
+
+    def assign_particle_stresses(self, stress):
+        stress = np.ascontiguousarray(stress, dtype=np.float64).reshape(-1, 6)
+        self._ck(self.L.mpm_gpu_assign_particle_stresses(self.h, stress.shape[0], _dp(stress)))
+
+    def add_particle_velocity_constraint(self, pids, direction, value):
+        if pids is None:
+            self._ck(self.L.mpm_gpu_add_particle_velocity_constraint(self.h, -1, None, direction,
+                                                                     value))
+            return
+        p = np.ascontiguousarray(pids, dtype=np.int64)
+        self._ck(self.L.mpm_gpu_add_particle_velocity_constraint(self.h, len(p), _i64p(p),
+                                                                 direction, value))
+
+    def step(self, n=1):
+        self._ck(self.L.mpm_gpu_step(self.h, n))
+
+    def step_timed(self, n=1):
+        """Advance n steps; return their device time in ms (CUDA events)."""
+        ms = C.c_double()
+        self._ck(self.L.mpm_gpu_step_timed(self.h, n, C.byref(ms)))
+        return ms.value
+
+    def set_profiling(self, enable=True):
+        self._ck(self.L.mpm_gpu_set_profiling(self.h, 1 if enable else 0))
+
+    def kernel_profile(self):
+        """{kernel name: (total ms, launches)} since profiling was enabled."""
+        out = {}
+        k = 0
+        while True:
+            name = C.c_char_p()
+            ms = C.c_double()
+            n = C.c_int64()
+            if self.L.mpm_gpu_kernel_profile(self.h, k, C.byref(name), C.byref(ms),
+                                             C.byref(n)) != 0:
+                break
+            out[name.value.decode()] = (ms.value, n.value)
+            k += 1
+        return out
+
+    @property
+    def launch_count(self):
+        return self.L.mpm_gpu_launch_count(self.h)
+
+    @property
+    def nparticles(self):
+        return self.L.mpm_gpu_nparticles(self.h)
+
+    @property
+    def current_step(self):
+        return self.L.mpm_gpu_current_step(self.h)
+
+    def read(self):
+        """Particle state as numpy arrays (rows = particles)."""
+        n = self.nparticles
+        out = {"x": np.zeros((n, 3)), "u": np.zeros((n, 3)), "v": np.zeros((n, 3)),
+               "stress": np.zeros((n, 6)), "strain": np.zeros((n, 6)), "F": np.zeros((n, 9)),
+               "volume": np.zeros(n), "mass": np.zeros(n), "density": np.zeros(n),
+               "cell": np.zeros(n, dtype=np.int64), "material": np.zeros(n, dtype=np.int32),
+               "svars": np.zeros((n, 9))}
+        P = _native.Particles()
+        for k, a in out.items():
+            if a.dtype == np.float64:
+                setattr(P, k, _dp(a))
+        P.cell = _i64p(out["cell"])
+        P.material = _i32p(out["material"])
+        self._ck(self.L.mpm_gpu_read_particles(self.h, C.byref(P)))
+        for k in ("x", "u", "v"):
+            out[k] = out[k][:, :self.dim]
+        return out
+
+    def load(self, state):
+        """Replace the particle state (arrays as returned by ``read``)."""
+        n = len(state["x"])
+        keep = {}
+        P = _native.Particles()
+        for k in ("x", "u", "v"):
+            if k in state:
+                a = np.zeros((n, 3))
+                a[:, :self.dim] = np.asarray(state[k])[:, :self.dim]
+                keep[k] = a
+                setattr(P, k, _dp(a))
+        for k in ("stress", "strain", "F", "volume", "mass", "density", "svars"):
+            if k in state:
+                keep[k] = np.ascontiguousarray(state[k], dtype=np.float64)
+                setattr(P, k, _dp(keep[k]))
+        keep["cell"] = np.ascontiguousarray(state["cell"], dtype=np.int64)
+        P.cell = _i64p(keep["cell"])
+        keep["material"] = np.ascontiguousarray(state["material"], dtype=np.int32)
+        P.material = _i32p(keep["material"])
+        self._ck(self.L.mpm_gpu_load_particles(self.h, n, C.byref(P)))
+
+    def device_field(self, field):
+        """(address, stride, ncomp) of a device-resident particle field."""
+        names = {"x": 0, "u": 1, "v": 2, "stress": 3, "strain": 4, "F": 5, "volume": 6,
+                 "density": 7, "mass": 8}
+        base = C.c_void_p()
+        stride = C.c_int64()
+        nc = C.c_int32()
+        self._ck(self.L.mpm_gpu_device_field(self.h, names[field], C.byref(base), C.byref(stride),
+                                             C.byref(nc)))
+        return base.value, stride.value, nc.value
+
+
+def material_stress_batch(dim, mtype, props, stress, dstrain, density, state=None, device=0):
+    """Material<Tdim>::compute_stress on the device for a batch of points."""
+    L = _native.lib()
+    stress = np.ascontiguousarray(stress, dtype=np.float64).reshape(-1, 6)
+    n = stress.shape[0]
+    dstrain = np.ascontiguousarray(dstrain, dtype=np.float64).reshape(n, 6)
+    density = np.ascontiguousarray(np.broadcast_to(np.asarray(density, dtype=np.float64), (n,)))
+    st = np.zeros((n, 9)) if state is None else np.array(state, dtype=np.float64).reshape(n, 9)
+    out = np.zeros((n, 6))
+    rc = L.mpm_gpu_material_stress_batch(device, dim, mtype.encode(), json.dumps(props).encode(),
+                                         n, _dp(stress), _dp(dstrain), _dp(density), _dp(st),
+                                         _dp(out))
+    if rc != 0:
+        raise MPMError(rc, "material_stress_batch failed")
+    return out, st
