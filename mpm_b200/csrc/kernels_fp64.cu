@@ -1,13 +1,18 @@
 // kernels_fp64.cu -- FP64 kernels of the explicit MPM step (USF and USL).
 //
 // Compiled with --fmad=false: every product and sum rounds on its own, as in
-// the reference's scalar C++ arithmetic, so the only differences from the
-// reference arithmetic are the order of the nodal sums and the device libm.
+// the reference's scalar C++ arithmetic.  The nodal sums are deterministic:
+// no floating-point atomics.  Each step sorts the particles by cell (counting
+// sort); lanes that own a cell add its particles' contributions slot by slot
+// in particle-id order; each node then adds the partial sums of its cells in
+// ascending cell id.  The per-particle arithmetic is the reference's; only the
+// order of the nodal sums differs (the reference adds in particle order).
 //
-// One step (USL):   p2g(mass, momentum, forces) -> node update -> g2p(+stress,
-//                   locate) -> locate fallback
-// One step (USF):   p2g(mass, momentum) -> node velocity -> stress + force p2g
-//                   -> node update -> g2p(locate) -> locate fallback
+// One step (USL):  sort -> p2g -> node update -> g2p(+stress, locate)
+// One step (USF):  sort -> p2g(mass, momentum) -> node velocity -> stress
+//                  -> p2g(forces) -> node update -> g2p(locate)
+// followed by the exhaustive locate of particles that left their
+// neighbourhood (usually none).
 #include <cuda_runtime.h>
 
 #include "mpm_kernels.h"
@@ -18,22 +23,11 @@ namespace mpm_b200 {
 namespace {
 
 template <int DIM>
-struct CellCtx {
-  static constexpr int NV = Elem<DIM>::NV;
-  int nid[NV];
-  double X[NV * DIM];
+struct PV {  // value offsets within a cell-slot partial
+  static constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM, N = 1 + 3 * DIM;
 };
 
-template <int DIM>
-__device__ __forceinline__ void load_cell(const DevState& s, int c, CellCtx<DIM>& cc) {
-  constexpr int NV = Elem<DIM>::NV;
-#pragma unroll
-  for (int i = 0; i < NV; ++i) cc.nid[i] = __ldg(&s.cell_nodes[(int64_t)c * NV + i]);
-#pragma unroll
-  for (int i = 0; i < NV; ++i)
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) cc.X[i * DIM + d] = __ldg(&s.ncoord[(int64_t)d * s.nn + cc.nid[i]]);
-}
+__device__ __forceinline__ void raise_err(const DevState& s, unsigned bits) { atomicOr(s.err, bits); }
 
 template <int DIM>
 __device__ __forceinline__ void load_x(const DevState& s, int64_t p, double* x) {
@@ -41,91 +35,364 @@ __device__ __forceinline__ void load_x(const DevState& s, int64_t p, double* x) 
   for (int d = 0; d < DIM; ++d) x[d] = s.pf[(int64_t)(PF<DIM>::X + d) * s.np + p];
 }
 
+// cell (i, j, k) of a tensor-product grid
 template <int DIM>
-__device__ __forceinline__ void particle_xi(const DevState& s, int c, const double* x, double* xi) {
-  const CellGeom& g = s.geom[c];
-  local_xi<DIM>(x, g.centroid, g.len, xi);
+__device__ __forceinline__ void cell_ijk(const DevState& s, int c, int* ijk) {
+  ijk[0] = c % s.gcells[0];
+  if constexpr (DIM == 2) {
+    ijk[1] = c / s.gcells[0];
+  } else {
+    ijk[1] = (c / s.gcells[0]) % s.gcells[1];
+    ijk[2] = c / (s.gcells[0] * s.gcells[1]);
+  }
 }
 
-__device__ __forceinline__ void raise_err(const DevState& s, unsigned bits) { atomicOr(s.err, bits); }
+// local node n of a cell -> offset (di, dj, dk) (quadrilateral_element.tcc:1-7,
+// hexahedron_element.tcc:1-13)
+__device__ __forceinline__ int off_i(int n) { return ((n & 3) == 1 || (n & 3) == 2) ? 1 : 0; }
+__device__ __forceinline__ int off_j(int n) { return ((n & 3) >= 2) ? 1 : 0; }
+__device__ __forceinline__ int off_k(int n) { return n >= 4 ? 1 : 0; }
 
-// ------------------------------------------------------------------------ P2G
-// particle.tcc:630-657 (mass, momentum), :893-898 (body force),
-// :915-949 (internal force)
-template <int DIM, bool FORCES>
-__global__ void __launch_bounds__(256) k_p2g(DevState s, double g0, double g1, double g2) {
+// node ids and nodal coordinates of a cell
+template <int DIM>
+__device__ __forceinline__ void cell_nodes_coords(const DevState& s, int c, int* nid, double* X) {
   constexpr int NV = Elem<DIM>::NV;
+  if (s.structured) {
+    int ijk[3] = {0, 0, 0};
+    cell_ijk<DIM>(s, c, ijk);
+    const int nx = s.gcells[0] + 1, ny = s.gcells[1] + 1;
+#pragma unroll
+    for (int n = 0; n < NV; ++n) {
+      const int i = ijk[0] + off_i(n), j = ijk[1] + off_j(n);
+      if constexpr (DIM == 2) {
+        nid[n] = i + nx * j;
+        X[n * 2 + 0] = __ldg(&s.axis[0][i]);
+        X[n * 2 + 1] = __ldg(&s.axis[1][j]);
+      } else {
+        const int k = ijk[2] + off_k(n);
+        nid[n] = i + nx * (j + ny * k);
+        X[n * 3 + 0] = __ldg(&s.axis[0][i]);
+        X[n * 3 + 1] = __ldg(&s.axis[1][j]);
+        X[n * 3 + 2] = __ldg(&s.axis[2][k]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int n = 0; n < NV; ++n) nid[n] = __ldg(&s.cell_nodes[(int64_t)c * NV + n]);
+#pragma unroll
+    for (int n = 0; n < NV; ++n)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) X[n * DIM + d] = __ldg(&s.ncoord[(int64_t)d * s.nn + nid[n]]);
+  }
+}
+
+// J^-1 at xi (quadrilateral_element.tcc:295-309, hexahedron_element.tcc:307-321)
+template <int DIM>
+__device__ __forceinline__ void jacobian_inverse(const double* xi, const double* X, double* inv) {
+  constexpr int NV = Elem<DIM>::NV;
+  double G[NV * DIM];
+  grad_shapefn<DIM>(xi, G);
+  double J[DIM * DIM];
+#pragma unroll
+  for (int r = 0; r < DIM; ++r)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      double a = G[0 * DIM + r] * X[0 * DIM + c];
+#pragma unroll
+      for (int n = 1; n < NV; ++n) a = a + G[n * DIM + r] * X[n * DIM + c];
+      J[r * DIM + c] = a;
+    }
+  inverse<DIM>(J, inv);
+}
+
+// dN_n/dx for one local node n given J^-1
+template <int DIM>
+__device__ __forceinline__ void dn_dx_node(const double* xi, const double* inv, int n, double* Dn) {
+  constexpr int NV = Elem<DIM>::NV;
+  double G[NV * DIM];
+  grad_shapefn<DIM>(xi, G);  // folded to the needed entries by the compiler
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    double a = G[n * DIM + 0] * inv[c * DIM + 0];
+#pragma unroll
+    for (int k = 1; k < DIM; ++k) a = a + G[n * DIM + k] * inv[c * DIM + k];
+    Dn[c] = a;
+  }
+}
+
+// Shape functions and natural gradients of the SPL slots a lane owns: all
+// of them in 2D; in 3D lane h owns slots 4h..4h+3, which share the z factor
+// (1 - xi_z) or (1 + xi_z).  Same operations and grouping as shapefn /
+// grad_shapefn (the z factor is the last product), with the lane's half
+// chosen by value selects so the two lanes of a cell do not diverge.
+template <int DIM>
+__device__ __forceinline__ void lane_shape(const double* xi, int h, double* Nk, double* Gk) {
+  if constexpr (DIM == 2) {
+    shapefn<2>(xi, Nk);
+    grad_shapefn<2>(xi, Gk);
+  } else {
+    const double xm = 1 - xi[0], xp = 1 + xi[0], ym = 1 - xi[1], yp = 1 + xi[1];
+    const double z = h ? (1 + xi[2]) : (1 - xi[2]);
+    const double zs = h ? 0.125 : -0.125;  // sign of d/dxi_z
+    // in-plane order of the four nodes of a face: (-,-), (+,-), (+,+), (-,+)
+    Nk[0] = 0.125 * xm * ym * z;
+    Nk[1] = 0.125 * xp * ym * z;
+    Nk[2] = 0.125 * xp * yp * z;
+    Nk[3] = 0.125 * xm * yp * z;
+    Gk[0 * 3 + 0] = -0.125 * ym * z;
+    Gk[1 * 3 + 0] = 0.125 * ym * z;
+    Gk[2 * 3 + 0] = 0.125 * yp * z;
+    Gk[3 * 3 + 0] = -0.125 * yp * z;
+    Gk[0 * 3 + 1] = -0.125 * xm * z;
+    Gk[1 * 3 + 1] = -0.125 * xp * z;
+    Gk[2 * 3 + 1] = 0.125 * xp * z;
+    Gk[3 * 3 + 1] = 0.125 * xm * z;
+    Gk[0 * 3 + 2] = zs * xm * ym;
+    Gk[1 * 3 + 2] = zs * xp * ym;
+    Gk[2 * 3 + 2] = zs * xp * yp;
+    Gk[3 * 3 + 2] = zs * xm * yp;
+  }
+}
+
+// ------------------------------------------------------------ counting sort
+__global__ void __launch_bounds__(256) k_count(DevState s) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= s.np) return;
   const int c = s.cell[p];
-  if (c < 0) return;
-  if (c >= s.ncells) {
-    raise_err(s, ERR_BADCELL);
+  if (c < 0 || c >= s.ncells) {
+    if (c >= s.ncells) raise_err(s, ERR_BADCELL);
+    s.rank[p] = -1;
     return;
   }
-  double x[DIM], xi[DIM], N[NV];
-  load_x<DIM>(s, p, x);
-  particle_xi<DIM>(s, c, x, xi);
-  shapefn<DIM>(xi, N);
-  CellCtx<DIM> cc;
-  load_cell<DIM>(s, c, cc);
-  const int64_t np = s.np, nn = s.nn;
-  const double m = s.pf[(int64_t)PF<DIM>::MASS * np + p];
-  double v[DIM];
+  s.rank[p] = atomicAdd(&s.cnt[c], 1);
+}
+
+// exclusive scan of n ints, SCAN_BLOCK per block (1024 threads x 4)
+__global__ void __launch_bounds__(1024) k_scan_local(const int32_t* in, int32_t* out,
+                                                     int32_t* bsum, int64_t n) {
+  __shared__ int32_t warp_tot[32];
+  const int64_t base = (int64_t)blockIdx.x * SCAN_BLOCK + threadIdx.x * 4;
+  int32_t v[4], e[4], t = 0;
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) v[d] = s.pf[(int64_t)(PF<DIM>::V + d) * np + p];
-#pragma unroll
-  for (int i = 0; i < NV; ++i) {
-    const int n = cc.nid[i];
-    const double mN = m * N[i];
-    atomicAdd(&s.nf[(int64_t)NF<DIM>::MASS * nn + n], mN);
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) atomicAdd(&s.nf[(int64_t)(NF<DIM>::MOM + d) * nn + n], mN * v[d]);
-    s.active[n] = 1;
+  for (int i = 0; i < 4; ++i) {
+    v[i] = (base + i < n) ? in[base + i] : 0;
+    e[i] = t;
+    t += v[i];
   }
-  if constexpr (FORCES) {
-    const double g[3] = {g0, g1, g2};
-    double D[NV * DIM];
-    dn_dx<DIM>(xi, cc.X, D);
-    const double vol = s.pf[(int64_t)PF<DIM>::VOL * np + p];
-    double sig[6];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t x = t;
 #pragma unroll
-    for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = s.pf[(int64_t)(PF<DIM>::S + k) * np + p];
-    const double sc = -1. * vol;
+  for (int off = 1; off < 32; off <<= 1) {
+    const int32_t y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) warp_tot[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int32_t z = warp_tot[lane];
 #pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      const int n = cc.nid[i];
+    for (int off = 1; off < 32; off <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, z, off);
+      if (lane >= off) z += y;
+    }
+    warp_tot[lane] = z;
+  }
+  __syncthreads();
+  const int32_t prefix = (w > 0 ? warp_tot[w - 1] : 0) + x - t;
 #pragma unroll
-      for (int d = 0; d < DIM; ++d)
-        atomicAdd(&s.nf[(int64_t)(NF<DIM>::FEXT + d) * nn + n], (g[d] * m) * N[i]);
-      const double* Dn = &D[i * DIM];
-      double f[DIM];
-      if constexpr (DIM == 2) {
-        f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
-        f[1] = Dn[1] * sig[1] + Dn[0] * sig[3];
-      } else {
-        f[0] = Dn[0] * sig[0] + Dn[1] * sig[3] + Dn[2] * sig[5];
-        f[1] = Dn[1] * sig[1] + Dn[0] * sig[3] + Dn[2] * sig[4];
-        f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
+  for (int i = 0; i < 4; ++i)
+    if (base + i < n) out[base + i] = prefix + e[i];
+  if (threadIdx.x == 1023 && bsum) bsum[blockIdx.x] = prefix + t;
+}
+
+// add the scanned block totals; start[n] = total
+__global__ void __launch_bounds__(256) k_scan_add(int32_t* out, const int32_t* bscan,
+                                                  const int32_t* bsum, int64_t n, int64_t nb) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] += bscan[i / SCAN_BLOCK];
+  if (i == 0) out[n] = bscan[nb - 1] + bsum[nb - 1];
+}
+
+__global__ void __launch_bounds__(256) k_fill(DevState s) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.np) return;
+  const int c = s.cell[p];
+  if (c < 0 || c >= s.ncells) return;
+  s.order[s.start[c] + s.rank[p]] = (int32_t)p;
+}
+
+// ---------------------------------------------------------------- P2G cells
+// Lanes per cell: 2 in 3D (4 slots each), 1 in 2D.  A lane adds, in particle
+// id order, the contributions of its cell's particles to its slots:
+//   mass m N (particle.tcc:643-655), momentum (m N) v, body force (g m) N
+//   (:893-898), internal force -V (dN . sigma) (:915-949).
+// MODE 0: mass and momentum; 1: forces; 2: all.
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(128) k_p2g_cells(DevState s, double g0, double g1, double g2) {
+  constexpr int NV = Elem<DIM>::NV;
+  constexpr int LPC = DIM == 3 ? 2 : 1;
+  constexpr int SPL = NV / LPC;
+  constexpr int NVAL = PV<DIM>::N;
+  constexpr bool MM = MODE != 1, FORCES = MODE != 0;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t c = t / LPC;
+  const int h = (int)(t % LPC);
+  const bool valid = c < s.ncells;
+  const int n = valid ? s.cnt[c] : 0;
+  const int s0 = valid ? s.start[c] : 0;
+  if constexpr (MODE != 1) {
+    // particle ids of the cell in ascending order (the fill order is not
+    // deterministic); the first lane of the cell sorts the short segment
+    if (h == 0 && n > 1) {
+      int32_t* seg = s.order + s0;
+      for (int a = 1; a < n; ++a) {
+        const int32_t key = seg[a];
+        int b = a - 1;
+        while (b >= 0 && seg[b] > key) {
+          seg[b + 1] = seg[b];
+          --b;
+        }
+        seg[b + 1] = key;
       }
+    }
+    __syncwarp();
+  }
+  if (!valid || n == 0) return;
+  int nid[NV];
+  double X[NV * DIM];
+  cell_nodes_coords<DIM>(s, (int)c, nid, X);
+  const CellGeom g = s.geom[c];
+  const int64_t np = s.np;
+  double acc[SPL][NVAL];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) atomicAdd(&s.nf[(int64_t)(NF<DIM>::FINT + d) * nn + n], f[d] * sc);
+  for (int k = 0; k < SPL; ++k)
+#pragma unroll
+    for (int v = 0; v < NVAL; ++v) acc[k][v] = 0.;
+  const double gv[3] = {g0, g1, g2};
+  for (int j = 0; j < n; ++j) {
+    const int64_t p = s.order[s0 + j];
+    double x[DIM], xi[DIM], Nk[SPL], Gk[SPL * DIM];
+    load_x<DIM>(s, p, x);
+    local_xi<DIM>(x, g.centroid, g.len, xi);
+    lane_shape<DIM>(xi, h, Nk, Gk);
+    const double m = s.pf[(int64_t)PF<DIM>::MASS * np + p];
+    if constexpr (MM) {
+      double v[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[d] = s.pf[(int64_t)(PF<DIM>::V + d) * np + p];
+#pragma unroll
+      for (int k = 0; k < SPL; ++k) {
+        const double mN = m * Nk[k];
+        acc[k][PV<DIM>::MASS] += mN;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) acc[k][PV<DIM>::MOM + d] += mN * v[d];
+      }
+    }
+    if constexpr (FORCES) {
+      double inv[DIM * DIM];
+      jacobian_inverse<DIM>(xi, X, inv);
+      const double sc = -1. * s.pf[(int64_t)PF<DIM>::VOL * np + p];
+      double sig[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = s.pf[(int64_t)(PF<DIM>::S + k) * np + p];
+#pragma unroll
+      for (int k = 0; k < SPL; ++k) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) acc[k][PV<DIM>::FEXT + d] += (gv[d] * m) * Nk[k];
+        double Dn[DIM];
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) {
+          double a = Gk[k * DIM + 0] * inv[q * DIM + 0];
+#pragma unroll
+          for (int r = 1; r < DIM; ++r) a = a + Gk[k * DIM + r] * inv[q * DIM + r];
+          Dn[q] = a;
+        }
+        double f[DIM];
+        if constexpr (DIM == 2) {
+          f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
+          f[1] = Dn[1] * sig[1] + Dn[0] * sig[3];
+        } else {
+          f[0] = Dn[0] * sig[0] + Dn[1] * sig[3] + Dn[2] * sig[5];
+          f[1] = Dn[1] * sig[1] + Dn[0] * sig[3] + Dn[2] * sig[4];
+          f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) acc[k][PV<DIM>::FINT + d] += f[d] * sc;
+      }
+    }
+  }
+  double* out = s.partials + ((int64_t)c * NV + h * SPL) * NVAL;
+#pragma unroll
+  for (int k = 0; k < SPL; ++k) {
+    if constexpr (MM) {
+      out[k * NVAL + PV<DIM>::MASS] = acc[k][PV<DIM>::MASS];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) out[k * NVAL + PV<DIM>::MOM + d] = acc[k][PV<DIM>::MOM + d];
+    }
+    if constexpr (FORCES) {
+#pragma unroll
+      for (int d = 0; d < 2 * DIM; ++d) out[k * NVAL + PV<DIM>::FEXT + d] = acc[k][PV<DIM>::FEXT + d];
     }
   }
 }
 
 // ---------------------------------------------------------------- node update
-// node.tcc:236-252 compute_velocity; node.tcc:309-345 Cundall update
+// Adds the partial sums of the node's cells (ascending cell id) for the value
+// range [v0, v0 + nv); returns false when no cell of the node holds particles
+// (the node is inactive, cell.tcc:171-177).
 template <int DIM>
-__device__ __forceinline__ void node_accel_update(const DevState& s, int64_t n, double m,
-                                                  double* vel, double* acc, int bci, double dt,
-                                                  double damping) {
-  const int64_t nn = s.nn;
+__device__ __forceinline__ bool gather_node(const DevState& s, int64_t node, int v0, int nv,
+                                            double* sum) {
+  constexpr int NV = Elem<DIM>::NV;
+  constexpr int NVAL = PV<DIM>::N;
+  for (int v = 0; v < nv; ++v) sum[v] = 0.;
+  bool active = false;
+  auto add = [&](int c, int slot) {
+    if (s.cnt[c] == 0) return;
+    const double* src = s.partials + ((int64_t)c * NV + slot) * NVAL + v0;
+    if (!active) {
+      for (int v = 0; v < nv; ++v) sum[v] = src[v];
+      active = true;
+    } else {
+      for (int v = 0; v < nv; ++v) sum[v] = sum[v] + src[v];
+    }
+  };
+  if (s.structured) {
+    const int nx = s.gcells[0] + 1, ny = s.gcells[1] + 1;
+    const int i = (int)(node % nx);
+    const int j = DIM == 2 ? (int)(node / nx) : (int)((node / nx) % ny);
+    const int k = DIM == 2 ? 0 : (int)(node / ((int64_t)nx * ny));
+    // slot of the node in the cell at offset (di, dj, dk) below/left of it
+    const int slot2[2][2] = {{0, 1}, {3, 2}};  // [dj][di]
+    const int kmin = DIM == 3 ? k - 1 : 0, kmax = DIM == 3 ? k : 0;
+    for (int ck = kmin; ck <= kmax; ++ck) {
+      if (DIM == 3 && (ck < 0 || ck >= s.gcells[2])) continue;
+      for (int cj = j - 1; cj <= j; ++cj) {
+        if (cj < 0 || cj >= s.gcells[1]) continue;
+        for (int ci = i - 1; ci <= i; ++ci) {
+          if (ci < 0 || ci >= s.gcells[0]) continue;
+          const int di = i - ci, dj = j - cj, dk = DIM == 3 ? k - ck : 0;
+          const int c = DIM == 2 ? ci + s.gcells[0] * cj : ci + s.gcells[0] * (cj + s.gcells[1] * ck);
+          add(c, slot2[dj][di] + 4 * dk);
+        }
+      }
+    }
+  } else {
+    for (int e = s.nc_off[node]; e < s.nc_off[node + 1]; ++e) add(s.nc_cell[e], s.nc_slot[e]);
+  }
+  return active;
+}
+
+// node.tcc:309-345 (Cundall form of the nodal update, always taken:
+// mpm_explicit.tcc:168-170)
+template <int DIM>
+__device__ __forceinline__ void node_accel_update(const DevState& s, double m, const double* fe,
+                                                  const double* fi, double* vel, double* acc,
+                                                  int bci, double dt, double damping) {
   if (!(m > 1.0E-15)) return;
   double uf[DIM];
 #pragma unroll
-  for (int d = 0; d < DIM; ++d)
-    uf[d] = s.nf[(int64_t)(NF<DIM>::FEXT + d) * nn + n] + s.nf[(int64_t)(NF<DIM>::FINT + d) * nn + n];
+  for (int d = 0; d < DIM; ++d) uf[d] = fe[d] + fi[d];
   double ss = uf[0] * uf[0];
 #pragma unroll
   for (int d = 1; d < DIM; ++d) ss = ss + uf[d] * uf[d];
@@ -153,36 +420,45 @@ __device__ __forceinline__ void node_accel_update(const DevState& s, int64_t n, 
     if (fabs(acc[d]) < 1.0E-15) acc[d] = 0.;
 }
 
-// MODE 0: velocity only (USF first pass); 1: velocity + acceleration (USL);
-// 2: acceleration only, velocity from the first pass (USF second pass)
+// MODE 0: velocity from momentum (node.tcc:236-252, USF first pass);
+// 1: velocity and then the acceleration update (USL);
+// 2: acceleration update on the velocity of the first pass (USF)
 template <int DIM, int MODE>
 __global__ void __launch_bounds__(256) k_nodes(DevState s, double dt, double damping) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= s.nn) return;
-  if (!s.active[n]) return;
   const int64_t nn = s.nn;
-  const double m = s.nf[(int64_t)NF<DIM>::MASS * nn + n];
+  double sum[PV<DIM>::N];
+  const int v0 = MODE == 2 ? PV<DIM>::FEXT : 0;
+  const int nv = MODE == 0 ? 1 + DIM : (MODE == 1 ? PV<DIM>::N : 2 * DIM);
+  if (!gather_node<DIM>(s, n, v0, nv, sum)) return;
   const int bci = s.bc_index[n];
   double vel[DIM], acc[DIM];
   if constexpr (MODE == 2) {
+    double mm[1];
+    gather_node<DIM>(s, n, PV<DIM>::MASS, 1, mm);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       vel[d] = s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + n];
       acc[d] = s.nf[(int64_t)(NF<DIM>::ACC + d) * nn + n];
     }
+    node_accel_update<DIM>(s, mm[0], &sum[0], &sum[DIM], vel, acc, bci, dt, damping);
   } else {
+    const double m = sum[PV<DIM>::MASS];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) vel[d] = acc[d] = 0.;
     if (m > 1.E-16) {
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) vel[d] = s.nf[(int64_t)(NF<DIM>::MOM + d) * nn + n] / m;
+      for (int d = 0; d < DIM; ++d) vel[d] = sum[PV<DIM>::MOM + d] / m;
 #pragma unroll
       for (int d = 0; d < DIM; ++d)
         if (fabs(vel[d]) < 1.E-15) vel[d] = 0.;
     }
     if (bci >= 0) apply_velocity_constraints<DIM>(s.bcs[bci], vel, acc);
+    if constexpr (MODE == 1)
+      node_accel_update<DIM>(s, m, &sum[PV<DIM>::FEXT], &sum[PV<DIM>::FINT], vel, acc, bci, dt,
+                             damping);
   }
-  if constexpr (MODE != 0) node_accel_update<DIM>(s, n, m, vel, acc, bci, dt, damping);
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
     s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + n] = vel[d];
@@ -192,69 +468,60 @@ __global__ void __launch_bounds__(256) k_nodes(DevState s, double dt, double dam
 
 // ------------------------------------------------------- stress and strain
 // mpm_scheme.tcc:75-103: F increment (particle.tcc:1580-1628), strain
-// (:819-876), volume (:598-605), material stress (:880-889), F (:1654-1658)
+// (:819-876), volume (:598-605), material stress (:880-889), F (:1654-1658).
+// D: dN/dx at the particle (start of step); the cell's centroid gradients
+// come from the per-cell table computed once from the mesh.
 template <int DIM>
-__device__ __forceinline__ void stress_update(const DevState& s, int64_t p, const CellCtx<DIM>& cc,
+__device__ __forceinline__ void stress_update(const DevState& s, int64_t p, int c, const int* nid,
                                               const double* D, double dt) {
   constexpr int NV = Elem<DIM>::NV;
   const int64_t np = s.np, nn = s.nn;
-  double vel[NV][DIM];
-#pragma unroll
-  for (int i = 0; i < NV; ++i)
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) vel[i][d] = s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + cc.nid[i]];
-  // deformation gradient increment
+  const double* Dc = s.dndx_c + (int64_t)c * NV * DIM;
   double Fi[DIM * DIM];
 #pragma unroll
   for (int r = 0; r < DIM; ++r)
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) Fi[r * DIM + c] = (r == c) ? 1. : 0.;
+    for (int q = 0; q < DIM; ++q) Fi[r * DIM + q] = (r == q) ? 1. : 0.;
+  double sr[6] = {0, 0, 0, 0, 0, 0};
+  double src[3] = {0, 0, 0};
 #pragma unroll
-  for (int i = 0; i < NV; ++i)
+  for (int i = 0; i < NV; ++i) {
+    double vel[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) vel[d] = s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + nid[i]];
 #pragma unroll
     for (int r = 0; r < DIM; ++r)
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) Fi[r * DIM + c] += vel[i][r] * D[i * DIM + c] * dt;
+      for (int q = 0; q < DIM; ++q) Fi[r * DIM + q] += vel[r] * D[i * DIM + q] * dt;
+    const double* Dn = &D[i * DIM];
+    double dc[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) dc[d] = __ldg(&Dc[i * DIM + d]);
+    if constexpr (DIM == 2) {
+      sr[0] += Dn[0] * vel[0];
+      sr[1] += Dn[1] * vel[1];
+      sr[3] += Dn[1] * vel[0] + Dn[0] * vel[1];
+      src[0] += dc[0] * vel[0];
+      src[1] += dc[1] * vel[1];
+    } else {
+      sr[0] += Dn[0] * vel[0];
+      sr[1] += Dn[1] * vel[1];
+      sr[2] += Dn[2] * vel[2];
+      sr[3] += Dn[1] * vel[0] + Dn[0] * vel[1];
+      sr[4] += Dn[2] * vel[1] + Dn[1] * vel[2];
+      sr[5] += Dn[2] * vel[0] + Dn[0] * vel[2];
+      src[0] += dc[0] * vel[0];
+      src[1] += dc[1] * vel[1];
+      src[2] += dc[2] * vel[2];
+    }
+  }
 #pragma unroll
   for (int r = 0; r < DIM; ++r)
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-      if (r != c && fabs(Fi[r * DIM + c]) < 1.E-15) Fi[r * DIM + c] = 0.;
-      if (r == c && fabs(Fi[r * DIM + c] - 1.) < 1.E-15) Fi[r * DIM + c] = 1.;
+    for (int q = 0; q < DIM; ++q) {
+      if (r != q && fabs(Fi[r * DIM + q]) < 1.E-15) Fi[r * DIM + q] = 0.;
+      if (r == q && fabs(Fi[r * DIM + q] - 1.) < 1.E-15) Fi[r * DIM + q] = 1.;
     }
-  // strain rate at the particle and at the cell centroid
-  double sr[6] = {0, 0, 0, 0, 0, 0};
-  double src[3] = {0, 0, 0};
-  double Dc[NV * DIM];
-  {
-    double xi0[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) xi0[d] = 0.;
-    dn_dx<DIM>(xi0, cc.X, Dc);
-  }
-  if constexpr (DIM == 2) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      sr[0] += D[i * 2 + 0] * vel[i][0];
-      sr[1] += D[i * 2 + 1] * vel[i][1];
-      sr[3] += D[i * 2 + 1] * vel[i][0] + D[i * 2 + 0] * vel[i][1];
-      src[0] += Dc[i * 2 + 0] * vel[i][0];
-      src[1] += Dc[i * 2 + 1] * vel[i][1];
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      sr[0] += D[i * 3 + 0] * vel[i][0];
-      sr[1] += D[i * 3 + 1] * vel[i][1];
-      sr[2] += D[i * 3 + 2] * vel[i][2];
-      sr[3] += D[i * 3 + 1] * vel[i][0] + D[i * 3 + 0] * vel[i][1];
-      sr[4] += D[i * 3 + 2] * vel[i][1] + D[i * 3 + 1] * vel[i][2];
-      sr[5] += D[i * 3 + 2] * vel[i][0] + D[i * 3 + 0] * vel[i][2];
-      src[0] += Dc[i * 3 + 0] * vel[i][0];
-      src[1] += Dc[i * 3 + 1] * vel[i][1];
-      src[2] += Dc[i * 3 + 2] * vel[i][2];
-    }
-  }
 #pragma unroll
   for (int k = 0; k < 6; ++k)
     if (fabs(sr[k]) < 1.E-15) sr[k] = 0.;
@@ -268,7 +535,6 @@ __device__ __forceinline__ void stress_update(const DevState& s, int64_t p, cons
 #pragma unroll
   for (int k = 1; k < DIM; ++k) ssum = ssum + src[k];
   const double dvol = dt * ssum;
-  // strain += dstrain
   if constexpr (DIM == 2) {
     const int map[3] = {0, 1, 3};
 #pragma unroll
@@ -277,14 +543,12 @@ __device__ __forceinline__ void stress_update(const DevState& s, int64_t p, cons
 #pragma unroll
     for (int k = 0; k < 6; ++k) s.pf[(int64_t)(PF<3>::E + k) * np + p] += dstrain[k];
   }
-  // volume and density
   double* volp = &s.pf[(int64_t)PF<DIM>::VOL * np + p];
   double* rhop = &s.pf[(int64_t)PF<DIM>::RHO * np + p];
   const double vol = *volp * (1. + dvol);
   const double rho = *rhop / (1. + dvol);
   *volp = vol;
   *rhop = rho;
-  // stress
   double sig[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
   for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = s.pf[(int64_t)(PF<DIM>::S + k) * np + p];
@@ -302,13 +566,12 @@ __device__ __forceinline__ void stress_update(const DevState& s, int64_t p, cons
   }
 #pragma unroll
   for (int k = 0; k < PF<DIM>::NS; ++k) s.pf[(int64_t)(PF<DIM>::S + k) * np + p] = out[k];
-  // F = F_inc * F
   if constexpr (DIM == 2) {
     double F[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) F[k] = s.pf[(int64_t)(PF<2>::F + k) * np + p];
-    // 3x3 product with F_inc(2,:) = (0,0,1) and F(2,:) = (0,0,1): the zero
-    // terms are exact and dropped
+    // 3x3 product with F_inc and F both (0,0,1) in the third row and column:
+    // the dropped terms are exact zeros
     const double r00 = Fi[0] * F[0] + Fi[1] * F[2];
     const double r01 = Fi[0] * F[1] + Fi[1] * F[3];
     const double r10 = Fi[2] * F[0] + Fi[3] * F[2];
@@ -324,57 +587,38 @@ __device__ __forceinline__ void stress_update(const DevState& s, int64_t p, cons
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        s.pf[(int64_t)(PF<3>::F + r * 3 + c) * np + p] =
-            (Fi[r * 3 + 0] * F[0 * 3 + c] + Fi[r * 3 + 1] * F[1 * 3 + c]) + Fi[r * 3 + 2] * F[2 * 3 + c];
+      for (int q = 0; q < 3; ++q)
+        s.pf[(int64_t)(PF<3>::F + r * 3 + q) * np + p] =
+            (Fi[r * 3 + 0] * F[0 * 3 + q] + Fi[r * 3 + 1] * F[1 * 3 + q]) + Fi[r * 3 + 2] * F[2 * 3 + q];
   }
 }
 
-// USF: stress update with the velocities of compute_velocity, then the force
-// P2G with the updated stress and volume (mpm_scheme.tcc:131-190)
+// dN/dx of all local nodes at xi
 template <int DIM>
-__global__ void __launch_bounds__(128) k_stress_forces(DevState s, double dt, double g0, double g1,
-                                                       double g2) {
+__device__ __forceinline__ void dn_dx_all(const double* xi, const double* X, double* D) {
+  constexpr int NV = Elem<DIM>::NV;
+  double inv[DIM * DIM];
+  jacobian_inverse<DIM>(xi, X, inv);
+#pragma unroll
+  for (int n = 0; n < NV; ++n) dn_dx_node<DIM>(xi, inv, n, &D[n * DIM]);
+}
+
+// USF: the stress update with the velocities of compute_velocity
+template <int DIM>
+__global__ void __launch_bounds__(128) k_stress(DevState s, double dt) {
   constexpr int NV = Elem<DIM>::NV;
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= s.np) return;
   const int c = s.cell[p];
   if (c < 0) return;
-  double x[DIM], xi[DIM], N[NV], D[NV * DIM];
+  double x[DIM], xi[DIM], D[NV * DIM], X[NV * DIM];
+  int nid[NV];
   load_x<DIM>(s, p, x);
-  particle_xi<DIM>(s, c, x, xi);
-  shapefn<DIM>(xi, N);
-  CellCtx<DIM> cc;
-  load_cell<DIM>(s, c, cc);
-  dn_dx<DIM>(xi, cc.X, D);
-  stress_update<DIM>(s, p, cc, D, dt);
-  const int64_t np = s.np, nn = s.nn;
-  const double m = s.pf[(int64_t)PF<DIM>::MASS * np + p];
-  const double vol = s.pf[(int64_t)PF<DIM>::VOL * np + p];
-  double sig[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-  for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = s.pf[(int64_t)(PF<DIM>::S + k) * np + p];
-  const double g[3] = {g0, g1, g2};
-  const double sc = -1. * vol;
-#pragma unroll
-  for (int i = 0; i < NV; ++i) {
-    const int n = cc.nid[i];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d)
-      atomicAdd(&s.nf[(int64_t)(NF<DIM>::FEXT + d) * nn + n], (g[d] * m) * N[i]);
-    const double* Dn = &D[i * DIM];
-    double f[DIM];
-    if constexpr (DIM == 2) {
-      f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
-      f[1] = Dn[1] * sig[1] + Dn[0] * sig[3];
-    } else {
-      f[0] = Dn[0] * sig[0] + Dn[1] * sig[3] + Dn[2] * sig[5];
-      f[1] = Dn[1] * sig[1] + Dn[0] * sig[3] + Dn[2] * sig[4];
-      f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
-    }
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) atomicAdd(&s.nf[(int64_t)(NF<DIM>::FINT + d) * nn + n], f[d] * sc);
-  }
+  const CellGeom& g = s.geom[c];
+  local_xi<DIM>(x, g.centroid, g.len, xi);
+  cell_nodes_coords<DIM>(s, c, nid, X);
+  dn_dx_all<DIM>(xi, X, D);
+  stress_update<DIM>(s, p, c, nid, D, dt);
 }
 
 // ------------------------------------------------------------------ locate
@@ -385,6 +629,27 @@ __device__ __forceinline__ int locate_near(const DevState& s, const double* x, i
   {
     const CellGeom& g = s.geom[c];
     if (point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi)) return c;
+  }
+  if (s.structured) {
+    // neighbours of a tensor-product cell: the 3^dim - 1 cells around it,
+    // ascending id (the node-sharing cells of mesh.tcc:287-306)
+    int ijk[3] = {0, 0, 0};
+    cell_ijk<DIM>(s, c, ijk);
+    const int kmin = DIM == 3 ? ijk[2] - 1 : 0, kmax = DIM == 3 ? ijk[2] + 1 : 0;
+    for (int k = kmin; k <= kmax; ++k) {
+      if (DIM == 3 && (k < 0 || k >= s.gcells[2])) continue;
+      for (int j = ijk[1] - 1; j <= ijk[1] + 1; ++j) {
+        if (j < 0 || j >= s.gcells[1]) continue;
+        for (int i = ijk[0] - 1; i <= ijk[0] + 1; ++i) {
+          if (i < 0 || i >= s.gcells[0]) continue;
+          const int nc = DIM == 2 ? i + s.gcells[0] * j : i + s.gcells[0] * (j + s.gcells[1] * k);
+          if (nc == c) continue;
+          const CellGeom& g = s.geom[nc];
+          if (point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi)) return nc;
+        }
+      }
+    }
+    return -1;
   }
   const int b = s.nb_off[c], e = s.nb_off[c + 1];
   for (int k = b; k < e; ++k) {
@@ -406,18 +671,19 @@ __global__ void __launch_bounds__(128) k_g2p(DevState s, double dt, double beta)
   const int c = s.cell[p];
   if (c < 0) return;
   const int64_t np = s.np, nn = s.nn;
-  double x[DIM], xi[DIM], N[NV];
+  double x[DIM], xi[DIM], N[NV], X[NV * DIM];
+  int nid[NV];
   load_x<DIM>(s, p, x);
-  particle_xi<DIM>(s, c, x, xi);
+  const CellGeom& g = s.geom[c];
+  local_xi<DIM>(x, g.centroid, g.len, xi);
   shapefn<DIM>(xi, N);
-  CellCtx<DIM> cc;
-  load_cell<DIM>(s, c, cc);
+  cell_nodes_coords<DIM>(s, c, nid, X);
   double nvel[DIM], nacc[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.;
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
-    const int n = cc.nid[i];
+    const int n = nid[i];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + n];
     if constexpr (FLIP) {
@@ -455,8 +721,8 @@ __global__ void __launch_bounds__(128) k_g2p(DevState s, double dt, double beta)
   for (int d = 0; d < DIM; ++d) s.pf[(int64_t)(PF<DIM>::V + d) * np + p] = v[d];
   if constexpr (STRESS) {
     double D[NV * DIM];
-    dn_dx<DIM>(xi, cc.X, D);
-    stress_update<DIM>(s, p, cc, D, dt);
+    dn_dx_all<DIM>(xi, X, D);
+    stress_update<DIM>(s, p, c, nid, D, dt);
   }
   bool finite = true;
 #pragma unroll
@@ -475,8 +741,8 @@ __global__ void __launch_bounds__(128) k_g2p(DevState s, double dt, double beta)
 }
 
 // Exhaustive search for particles not in their cell or its neighbours
-// (mesh.tcc:1136-1148, one thread: the first cell in id order that contains
-// the point).  Grid-stride over the lost list; usually empty.
+// (mesh.tcc:1136-1148 with one thread: the first cell in id order that
+// contains the point).  Grid-stride over the lost list; usually empty.
 template <int DIM>
 __global__ void k_locate_fallback(DevState s, int remove_lost) {
   const unsigned count = *s.nlost;
@@ -493,8 +759,10 @@ __global__ void k_locate_fallback(DevState s, int remove_lost) {
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
         const double f = floor((x[d] - s.bmin[d]) / s.bsize[d]);
-        if (!(f >= 0.) || f >= (double)s.bn[d]) inside = false;
-        else b[d] = (int)f;
+        if (!(f >= 0.) || f >= (double)s.bn[d])
+          inside = false;
+        else
+          b[d] = (int)f;
       }
       if (inside) {
         const int64_t bi = ((int64_t)b[2] * s.bn[1] + b[1]) * s.bn[0] + b[0];
@@ -521,18 +789,32 @@ __global__ void k_locate_fallback(DevState s, int remove_lost) {
 
 inline unsigned nblocks(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+void counting_sort(const DevState& s, cudaStream_t st) {
+  const int64_t nc = s.ncells;
+  cudaMemsetAsync(s.cnt, 0, sizeof(int32_t) * nc, st);
+  k_count<<<nblocks(s.np, 256), 256, 0, st>>>(s);
+  const int64_t nb = (nc + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  k_scan_local<<<(unsigned)nb, 1024, 0, st>>>(s.cnt, s.start, s.bsum, nc);
+  // block totals (nb <= SCAN_BLOCK is checked at set-up) scanned by one block
+  k_scan_local<<<1, 1024, 0, st>>>(s.bsum, s.bsum + nb, nullptr, nb);
+  k_scan_add<<<nblocks(nc, 256), 256, 0, st>>>(s.start, s.bsum + nb, s.bsum, nc, nb);
+  k_fill<<<nblocks(s.np, 256), 256, 0, st>>>(s);
+}
+
 template <int DIM>
 void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& pr) {
   const int64_t np = s.np, nn = s.nn;
   if (np == 0) return;
-  // Node::initialise (node.tcc:26-42): zero the accumulated fields and flags
-  cudaMemsetAsync(s.nf, 0, sizeof(double) * NF<DIM>::NACC_FIELDS * nn, st);
-  cudaMemsetAsync(s.active, 0, nn, st);
+  constexpr int LPC = DIM == 3 ? 2 : 1;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
-  const unsigned pb256 = nblocks(np, 256), pb128 = nblocks(np, 128), nb = nblocks(nn, 256);
+  const unsigned pb128 = nblocks(np, 128), nb = nblocks(nn, 256);
+  const unsigned cb = nblocks(s.ncells * LPC, 128);
+  pr.begin(K_SORT, st);
+  counting_sort(s, st);
+  pr.end(K_SORT, st);
   if (a.scheme == 1) {  // USL
     pr.begin(K_P2G, st);
-    k_p2g<DIM, true><<<pb256, 256, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    k_p2g_cells<DIM, 2><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
@@ -545,14 +827,17 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     pr.end(K_G2P, st);
   } else {  // USF
     pr.begin(K_P2G, st);
-    k_p2g<DIM, false><<<pb256, 256, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    k_p2g_cells<DIM, 0><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
-    pr.begin(K_STRESS_FORCES, st);
-    k_stress_forces<DIM><<<pb128, 128, 0, st>>>(s, a.dt, a.g[0], a.g[1], a.g[2]);
-    pr.end(K_STRESS_FORCES, st);
+    pr.begin(K_STRESS, st);
+    k_stress<DIM><<<pb128, 128, 0, st>>>(s, a.dt);
+    pr.end(K_STRESS, st);
+    pr.begin(K_P2G_FORCES, st);
+    k_p2g_cells<DIM, 1><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
     k_nodes<DIM, 2><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_ACC, st);

@@ -74,8 +74,9 @@ struct HostBC {
 namespace mpm_b200 {
 
 const char* kernel_name(int kid) {
-  static const char* names[K_NKERNELS] = {"p2g", "nodes_velocity", "stress_forces",
-                                          "nodes_acceleration", "g2p", "locate_fallback"};
+  static const char* names[K_NKERNELS] = {"sort",  "p2g",   "nodes_velocity", "stress",
+                                          "p2g_forces", "nodes_acceleration", "g2p",
+                                          "locate_fallback"};
   return (kid >= 0 && kid < K_NKERNELS) ? names[kid] : "?";
 }
 
@@ -193,6 +194,12 @@ struct mpm_gpu_solver {
   DevBuf<unsigned> d_words;  // [0] nlost, [1] err
   DevBuf<MaterialParams> d_mats;
   DevBuf<double> d_axis[3];
+  DevBuf<double> d_dndx_c, d_partials;
+  DevBuf<int32_t> d_nc_off, d_nc_cell, d_cnt, d_start, d_rank, d_order, d_bsum;
+  DevBuf<int8_t> d_nc_slot;
+  std::vector<double> dndx_c;                 // [ncells][nv][dim]
+  std::vector<int32_t> nc_off, nc_cell;       // node -> cells (general meshes)
+  std::vector<int8_t> nc_slot;
   DevBuf<NodeBC> d_bcs;
   DevBuf<ParticleVC> d_pvcs;
   bool any_mc = false;
@@ -511,6 +518,20 @@ void upload_mesh(mpm_gpu_t h) {
   ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 2, st), "memset");
   if (h->structured)
     for (int d = 0; d < 3; ++d) h->d_axis[d].upload(h->axis[d].data(), h->axis[d].size(), st);
+  h->d_dndx_c.upload(h->dndx_c.data(), h->dndx_c.size(), st);
+  if (!h->structured) {
+    h->d_nc_off.upload(h->nc_off.data(), h->nc_off.size(), st);
+    h->d_nc_cell.alloc(std::max<size_t>(1, h->nc_cell.size()));
+    h->d_nc_cell.upload(h->nc_cell.data(), h->nc_cell.size(), st);
+    h->d_nc_slot.alloc(std::max<size_t>(1, h->nc_slot.size()));
+    h->d_nc_slot.upload(h->nc_slot.data(), h->nc_slot.size(), st);
+  }
+  const int nval = 1 + 3 * dim;
+  h->d_partials.alloc((size_t)h->ncells * h->nv * nval);
+  h->d_cnt.alloc(h->ncells);
+  h->d_start.alloc(h->ncells + 1);
+  const int64_t nb = (h->ncells + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  h->d_bsum.alloc(2 * nb + 2);
 }
 
 void upload_bcs(mpm_gpu_t h) {
@@ -584,6 +605,8 @@ void allocate_particles(mpm_gpu_t h) {
   h->d_cell.alloc(np);
   h->d_mat.alloc(np);
   h->d_lost.alloc(std::max<int64_t>(1, np));
+  h->d_rank.alloc(std::max<int64_t>(1, np));
+  h->d_order.alloc(std::max<int64_t>(1, np));
   h->any_mc = false;
   for (auto& m : h->mats) h->any_mc = h->any_mc || m.type == 1;
   if (h->any_mc)
@@ -622,6 +645,16 @@ void refresh_state(mpm_gpu_t h) {
     s.gcells[d] = h->gcells[d];
     s.axis[d] = h->d_axis[d].p;
   }
+  s.nc_off = h->d_nc_off.p;
+  s.nc_cell = h->d_nc_cell.p;
+  s.nc_slot = h->d_nc_slot.p;
+  s.dndx_c = h->d_dndx_c.p;
+  s.cnt = h->d_cnt.p;
+  s.start = h->d_start.p;
+  s.rank = h->d_rank.p;
+  s.order = h->d_order.p;
+  s.bsum = h->d_bsum.p;
+  s.partials = h->d_partials.p;
   s.lost = h->d_lost.p;
   s.nlost = h->d_words.p;
   s.err = h->d_words.p + 1;
@@ -761,6 +794,7 @@ int mpm_gpu_set_mesh(mpm_gpu_t h, int64_t nnodes, const double* coords, int64_t 
   if (npc != h->nv) throw InvalidArg("nodes_per_cell must be 4 (2D quad4) or 8 (3D hex8)");
   if (nnodes <= 0 || ncells <= 0 || !coords || !cell_nodes) throw InvalidArg("empty mesh");
   if (nnodes > INT32_MAX || ncells > INT32_MAX / 8) throw InvalidArg("mesh too large for 32-bit indices");
+  if (ncells > (int64_t)SCAN_BLOCK * SCAN_BLOCK) throw InvalidArg("mesh too large for the cell sort");
   if (h->mesh_set) throw InvalidArg("mesh already set");
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
   const int dim = h->dim, nv = h->nv;
@@ -782,6 +816,40 @@ int mpm_gpu_set_mesh(mpm_gpu_t h, int64_t nnodes, const double* coords, int64_t 
     }
     cell_geometry(dim, X.data(), &h->geom[c], &h->cell_volume[c]);
     if (!(h->cell_volume[c] > 0)) throw InvalidArg("Negative or zero volume cell, misconfigured cell!");
+  }
+  // dN/dx at the cell centroid (cell.tcc:33-65), once per cell
+  h->dndx_c.resize((size_t)ncells * nv * dim);
+  for (int64_t c = 0; c < ncells; ++c) {
+    for (int i = 0; i < nv; ++i) {
+      const int64_t n = cell_nodes[c * nv + i];
+      for (int d = 0; d < dim; ++d) X[i * dim + d] = coords[n * dim + d];
+    }
+    double xi0[3] = {0., 0., 0.};
+    if (dim == 2)
+      dn_dx<2>(xi0, X.data(), &h->dndx_c[(size_t)c * nv * dim]);
+    else
+      dn_dx<3>(xi0, X.data(), &h->dndx_c[(size_t)c * nv * dim]);
+  }
+  // node -> (cell, slot), ascending cell id, for the nodal gather on general meshes
+  h->nc_off.assign(nnodes + 1, 0);
+  for (int64_t n = 0; n < nnodes; ++n) h->nc_off[n + 1] = h->nc_off[n] + (int32_t)node_cells[n].size();
+  h->nc_cell.resize(h->nc_off[nnodes]);
+  h->nc_slot.resize(h->nc_off[nnodes]);
+  for (int64_t n = 0; n < nnodes; ++n) {
+    std::vector<int32_t> cs = node_cells[n];
+    std::sort(cs.begin(), cs.end());
+    cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+    int32_t e = h->nc_off[n];
+    for (int32_t c : cs) {
+      for (int i = 0; i < nv; ++i)
+        if (h->cell_nodes[(size_t)c * nv + i] == n) {
+          h->nc_cell[e] = c;
+          h->nc_slot[e] = (int8_t)i;
+          ++e;
+          break;
+        }
+    }
+    h->nc_off[n + 1] = e;  // duplicates (a node listed twice in a cell) counted once
   }
   // mesh.tcc:287-306 neighbours: cells sharing a node, ascending id
   h->nb_off.assign(ncells + 1, 0);
@@ -805,6 +873,7 @@ int mpm_gpu_set_mesh(mpm_gpu_t h, int64_t nnodes, const double* coords, int64_t 
     build_bins(h);
   }
   upload_mesh(h);
+  upload_bcs(h);  // every node gets a (possibly empty) constraint slot
   h->mesh_set = true;
   MPM_END(h)
   return MPM_OK;
@@ -999,6 +1068,7 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
   if (!h->initialised) throw InvalidArg("initialise or load particles first");
   if (nsteps < 0) throw InvalidArg("negative step count");
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  refresh_state(h);  // constraint or material tables may have been reallocated
   StepArgs a{};
   a.scheme = h->cfg.scheme;
   a.flip = h->cfg.velocity_update == MPM_VELOCITY_FLIP ? 1 : 0;

@@ -22,14 +22,17 @@ struct StepArgs {
 
 // Kernels of one step, for launch counting and per-kernel event timing.
 enum KernelId {
-  K_P2G = 0,        // P2G of mass and momentum (and, in USL, forces)
+  K_SORT = 0,       // counting sort of particles by cell (count, scan, fill)
+  K_P2G,            // per-cell P2G of mass and momentum (and, in USL, forces)
   K_NODES_VEL,      // nodal velocity (USF) or full nodal update (USL)
-  K_STRESS_FORCES,  // USF: stress update + force P2G
+  K_STRESS,         // USF: stress update
+  K_P2G_FORCES,     // USF: per-cell P2G of the forces
   K_NODES_ACC,      // USF: nodal acceleration / velocity update
   K_G2P,            // G2P (+ USL stress update) + locate
   K_LOCATE,         // exhaustive locate for particles that left their neighbourhood
   K_NKERNELS
 };
+constexpr int SCAN_BLOCK = 4096;  // cells per block of the counting-sort scan
 const char* kernel_name(int kid);
 
 // Counts launches; when enabled, brackets every launch with a pair of CUDA

@@ -85,6 +85,22 @@ struct DevState {
   int32_t gcells[3] = {1, 1, 1};     // cells per axis
   const double* axis[3] = {nullptr, nullptr, nullptr};  // node coordinates per axis
 
+  // general meshes: cells around each node, ascending cell id, with the
+  // node's local index (slot) in that cell
+  int32_t* nc_off = nullptr;     // [nn + 1]
+  int32_t* nc_cell = nullptr;
+  int8_t* nc_slot = nullptr;
+  double* dndx_c = nullptr;      // [ncells][NV][DIM] dN/dx at the cell centroid
+
+  // per-step counting sort of particles by cell and the cell-slot partial
+  // sums of P2G (mass, momentum, external force, internal force per slot)
+  int32_t* cnt = nullptr;        // [ncells] particles per cell
+  int32_t* start = nullptr;      // [ncells + 1] exclusive scan of cnt
+  int32_t* rank = nullptr;       // [np] position of the particle within its cell
+  int32_t* order = nullptr;      // [np] particle ids grouped by cell
+  int32_t* bsum = nullptr;       // scan block totals
+  double* partials = nullptr;    // [ncells][NV][1 + 3 DIM]
+
   int32_t* lost = nullptr;       // [np] particles not found in cell or neighbours
   unsigned* nlost = nullptr;
   unsigned* err = nullptr;       // ErrorBits

@@ -1128,13 +1128,10 @@ void compute_stress_strain(Oracle& o, double dt) {
   }
 }
 
-void one_step(Oracle& o) {
-  const int dim = o.dim;
-  const double dt = o.cfg.dt;
+// mpm_scheme.tcc:19-40 MPMScheme::initialise
+void phase_initialise(Oracle& o) {
   const bool thr = o.cfg.nthreads > 1;
   const int64_t np = (int64_t)o.particles.size();
-  const int64_t nn = (int64_t)o.nodes.size();
-  // mpm_scheme.tcc:19-40 initialise
   for (auto& n : o.nodes) {  // node.tcc:26-42
     n.mass = 0;
     for (int i = 0; i < 3; ++i) n.mom[i] = n.fext[i] = n.fint[i] = n.vel[i] = n.acc[i] = 0;
@@ -1145,7 +1142,13 @@ void one_step(Oracle& o) {
       for (int i = 0; i < o.nv; ++i) o.nodes[c.nodes[i]].status = true;
 #pragma omp parallel for schedule(static) if (thr)
   for (int64_t p = 0; p < np; ++p) particle_compute_shapefn(o, o.particles[p]);
-  // mpm_scheme.tcc:44-71 compute_nodal_kinematics; particle.tcc:630-657
+}
+
+// particle.tcc:630-657 map_mass_momentum_to_nodes
+void phase_p2g_mass_momentum(Oracle& o) {
+  const int dim = o.dim;
+  const bool thr = o.cfg.nthreads > 1;
+  const int64_t np = (int64_t)o.particles.size();
 #pragma omp parallel for schedule(static) if (thr)
   for (int64_t p = 0; p < np; ++p) {
     Particle& P = o.particles[p];
@@ -1159,18 +1162,21 @@ void one_step(Oracle& o) {
       node_add(n, n.mom, mom, dim, thr);
     }
   }
-#pragma omp parallel for schedule(static) if (thr)
+}
+
+// mpm_scheme.tcc:66-70 compute_velocity on active nodes
+void phase_compute_velocity(Oracle& o) {
+  const int64_t nn = (int64_t)o.nodes.size();
+#pragma omp parallel for schedule(static) if (o.cfg.nthreads > 1)
   for (int64_t i = 0; i < nn; ++i)
     if (o.nodes[i].status) node_compute_velocity(o, o.nodes[i]);
-  // USF: stress first (mpm_scheme_usf.tcc:9-12)
-  if (o.cfg.scheme == 0) compute_stress_strain(o, dt);
-  // mpm_explicit.tcc:145-153 gravity ramp
-  double gmul = 1.0;
-  if (o.cfg.gravity_ramping_time > 0.0)
-    gmul = std::min(1.0, static_cast<double>(o.step) * dt / o.cfg.gravity_ramping_time);
-  double g[3];
-  for (int i = 0; i < dim; ++i) g[i] = gmul * o.cfg.gravity[i];
-  // mpm_scheme.tcc:131-190 compute_forces; particle.tcc:893-898, 931-949
+}
+
+// particle.tcc:893-898 map_body_force
+void phase_body_force(Oracle& o, const double* g) {
+  const int dim = o.dim;
+  const bool thr = o.cfg.nthreads > 1;
+  const int64_t np = (int64_t)o.particles.size();
 #pragma omp parallel for schedule(static) if (thr)
   for (int64_t p = 0; p < np; ++p) {
     Particle& P = o.particles[p];
@@ -1182,6 +1188,13 @@ void one_step(Oracle& o) {
       node_add(n, n.fext, fb, dim, thr);
     }
   }
+}
+
+// particle.tcc:915-949 map_internal_force
+void phase_internal_force(Oracle& o) {
+  const int dim = o.dim;
+  const bool thr = o.cfg.nthreads > 1;
+  const int64_t np = (int64_t)o.particles.size();
 #pragma omp parallel for schedule(static) if (thr)
   for (int64_t p = 0; p < np; ++p) {
     Particle& P = o.particles[p];
@@ -1204,14 +1217,24 @@ void one_step(Oracle& o) {
       node_add(n, n.fint, f, dim, thr);
     }
   }
-  // mpm_scheme.tcc:214-241 compute_particle_kinematics
-#pragma omp parallel for schedule(static) if (thr)
+}
+
+// mpm_scheme.tcc:222-233 node update on active nodes
+void phase_node_update(Oracle& o, double dt) {
+  const int64_t nn = (int64_t)o.nodes.size();
+#pragma omp parallel for schedule(static) if (o.cfg.nthreads > 1)
   for (int64_t i = 0; i < nn; ++i)
     if (o.nodes[i].status)
       node_compute_acceleration_velocity_cundall(o, o.nodes[i], dt, o.cfg.damping_factor);
+}
+
+// particle.tcc:1018-1067 FLIP / PIC, mesh.tcc:1454-1467 velocity constraints
+void phase_g2p(Oracle& o, double dt) {
+  const int dim = o.dim;
+  const int64_t np = (int64_t)o.particles.size();
   const double beta = o.cfg.blending_ratio;
-#pragma omp parallel for schedule(static) if (thr)
-  for (int64_t p = 0; p < np; ++p) {  // particle.tcc:1018-1067
+#pragma omp parallel for schedule(static) if (o.cfg.nthreads > 1)
+  for (int64_t p = 0; p < np; ++p) {
     Particle& P = o.particles[p];
     const Cell& c = o.cells[P.cell];
     double nvel[3] = {0, 0, 0}, nacc[3] = {0, 0, 0};
@@ -1229,11 +1252,31 @@ void one_step(Oracle& o) {
     }
     for (int d = 0; d < dim; ++d) P.x[d] += nvel[d] * dt;
     for (int d = 0; d < dim; ++d) P.u[d] += nvel[d] * dt;
-    // mesh.tcc:1454-1467, particle.tcc:1190-1194
     for (const auto& pc : P.pvc) P.v[pc.first] = pc.second;
   }
-  // USL: stress last (mpm_scheme_usl.tcc:14-17)
-  if (o.cfg.scheme == 1) compute_stress_strain(o, dt);
+}
+
+void current_gravity(const Oracle& o, double* g) {  // mpm_explicit.tcc:145-153
+  double gmul = 1.0;
+  if (o.cfg.gravity_ramping_time > 0.0)
+    gmul = std::min(1.0, static_cast<double>(o.step) * o.cfg.dt / o.cfg.gravity_ramping_time);
+  for (int i = 0; i < 3; ++i) g[i] = i < o.dim ? gmul * o.cfg.gravity[i] : 0.;
+}
+
+// mpm_explicit.tcc:128-179 one step (USF / USL)
+void one_step(Oracle& o) {
+  const double dt = o.cfg.dt;
+  phase_initialise(o);
+  phase_p2g_mass_momentum(o);
+  phase_compute_velocity(o);
+  if (o.cfg.scheme == 0) compute_stress_strain(o, dt);  // mpm_scheme_usf.tcc:9-12
+  double g[3];
+  current_gravity(o, g);
+  phase_body_force(o, g);
+  phase_internal_force(o);
+  phase_node_update(o, dt);
+  phase_g2p(o, dt);
+  if (o.cfg.scheme == 1) compute_stress_strain(o, dt);  // mpm_scheme_usl.tcc:14-17
 }
 
 }  // namespace
@@ -1515,15 +1558,54 @@ int mpmo_get_nodes(void* h, double* out) {
   Oracle& o = *(Oracle*)h;
   for (size_t i = 0; i < o.nodes.size(); ++i) {
     const Node& n = o.nodes[i];
-    double* r = out + i * 14;
+    double* r = out + i * 17;
     r[0] = n.mass;
     for (int d = 0; d < 3; ++d) {
       r[1 + d] = n.mom[d];
       r[4 + d] = n.fext[d];
       r[7 + d] = n.fint[d];
       r[10 + d] = n.vel[d];
+      r[13 + d] = n.acc[d];
     }
-    r[13] = 0;
+    r[16] = n.status ? 1. : 0.;
+  }
+  return 0;
+}
+
+int mpmo_set_nodes(void* h, const double* in) {
+  Oracle& o = *(Oracle*)h;
+  for (size_t i = 0; i < o.nodes.size(); ++i) {
+    Node& n = o.nodes[i];
+    const double* r = in + i * 17;
+    n.mass = r[0];
+    for (int d = 0; d < 3; ++d) {
+      n.mom[d] = r[1 + d];
+      n.fext[d] = r[4 + d];
+      n.fint[d] = r[7 + d];
+      n.vel[d] = r[10 + d];
+      n.acc[d] = r[13 + d];
+    }
+    n.status = r[16] != 0.;
+  }
+  return 0;
+}
+
+int mpmo_phase(void* h, int32_t phase, double dt, const double* gravity) {
+  Oracle& o = *(Oracle*)h;
+  switch (phase) {
+    case 0: phase_initialise(o); break;
+    case 1: phase_p2g_mass_momentum(o); break;
+    case 2: phase_compute_velocity(o); break;
+    case 3: compute_stress_strain(o, dt); break;
+    case 4: phase_body_force(o, gravity); break;
+    case 5: phase_internal_force(o); break;
+    case 6: phase_node_update(o, dt); break;
+    case 7: phase_g2p(o, dt); break;
+    case 8:
+      for (auto& P : o.particles)
+        if (!locate_particle(o, P)) return -2;
+      break;
+    default: o.err = "unknown phase"; return -1;
   }
   return 0;
 }

@@ -94,8 +94,15 @@ int mpmo_set_particles(void* h, const mpmo_particles* p);
 int64_t mpmo_nparticles(void* h);
 int mpmo_get_particles(void* h, mpmo_particles* p);
 int mpmo_step(void* h, int64_t nsteps);
-/* nodal state (mass, momentum[3], fext[3], fint[3], vel[3], acc[3]) n*14 */
+/* nodal state, 17 doubles per node: mass, momentum[3], fext[3], fint[3],
+ * vel[3], acc[3], status */
 int mpmo_get_nodes(void* h, double* out);
+int mpmo_set_nodes(void* h, const double* in);
+/* one phase of the scheme (mpm_scheme.tcc): 0 initialise (zero nodes,
+ * activate, shape functions), 1 P2G mass + momentum, 2 nodal velocity,
+ * 3 stress and strain, 4 body force (gravity[3]), 5 internal force,
+ * 6 nodal acceleration/velocity (Cundall), 7 G2P, 8 locate */
+int mpmo_phase(void* h, int32_t phase, double dt, const double* gravity);
 
 /* ---- unit-level entry points used by the known-answer tests ---- */
 /* shape functions and gradients at xi for a cell with nodal coordinates X

@@ -73,6 +73,8 @@ def lib():
         L.mpmo_get_particles.argtypes = [vp, C.POINTER(Particles)]
         L.mpmo_step.argtypes = [vp, i64]
         L.mpmo_get_nodes.argtypes = [vp, pd]
+        L.mpmo_set_nodes.argtypes = [vp, pd]
+        L.mpmo_phase.argtypes = [vp, i32, dbl, pd]
         L.mpmo_element_dn_dx.argtypes = [i32, pd, pd, pd, pd, pd]
         L.mpmo_material_stress.argtypes = [i32, i32, pd, i32, pd, pd, dbl, pd, pd]
         L.mpmo_mc_diagnostics.argtypes = [i32, pd, i32, pd, pd, pd]
@@ -312,10 +314,28 @@ class Oracle:
             P.cell = _i64p(a)
         self._check(lib().mpmo_set_particles(self.h, C.byref(P)))
 
+    NODE_COLS = {"mass": 0, "momentum": slice(1, 4), "external_force": slice(4, 7),
+                 "internal_force": slice(7, 10), "velocity": slice(10, 13),
+                 "acceleration": slice(13, 16), "status": 16}
+
     def nodes(self, nnodes):
-        out = np.zeros((nnodes, 14))
+        """nnodes x 17: mass, momentum[3], fext[3], fint[3], vel[3], acc[3], status."""
+        out = np.zeros((nnodes, 17))
         self._check(lib().mpmo_get_nodes(self.h, _dp(out)))
         return out
+
+    def set_nodes(self, table):
+        table = np.ascontiguousarray(table, dtype=np.float64)
+        self._check(lib().mpmo_set_nodes(self.h, _dp(table)))
+
+    PHASES = {"initialise": 0, "p2g_mass_momentum": 1, "compute_velocity": 2,
+              "stress_strain": 3, "body_force": 4, "internal_force": 5, "node_update": 6,
+              "g2p": 7, "locate": 8}
+
+    def phase(self, name, dt=0.0, gravity=(0.0, 0.0, 0.0)):
+        g = np.zeros(3)
+        g[:len(gravity)] = gravity
+        self._check(lib().mpmo_phase(self.h, self.PHASES[name], dt, _dp(g)))
 
 
 def build_oracle(prob, nthreads=1, **overrides):
