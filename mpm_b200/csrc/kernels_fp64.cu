@@ -18,6 +18,15 @@
 #include "mpm_kernels.h"
 #include "mpm_state.cuh"
 
+// Minimum resident blocks per SM requested from the register allocator for
+// the two particle kernels (occupancy versus spills, tuned on the B200).
+#ifndef MPM_G2P_MIN_BLOCKS
+#define MPM_G2P_MIN_BLOCKS 4  // 1.41 -> 1.01 ms per 4M-particle step despite spills
+#endif
+#ifndef MPM_P2G_MIN_BLOCKS
+#define MPM_P2G_MIN_BLOCKS 2  // more blocks spill the 40 lane accumulators: slower
+#endif
+
 namespace mpm_b200 {
 
 namespace {
@@ -228,7 +237,8 @@ __global__ void __launch_bounds__(256) k_fill(DevState s) {
 //   (:893-898), internal force -V (dN . sigma) (:915-949).
 // MODE 0: mass and momentum; 1: forces; 2: all.
 template <int DIM, int MODE>
-__global__ void __launch_bounds__(128) k_p2g_cells(DevState s, double g0, double g1, double g2) {
+__global__ void __launch_bounds__(128, MPM_P2G_MIN_BLOCKS) k_p2g_cells(DevState s, double g0,
+                                                                       double g1, double g2) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int LPC = DIM == 3 ? 2 : 1;
   constexpr int SPL = NV / LPC;
@@ -664,7 +674,8 @@ __device__ __forceinline__ int locate_near(const DevState& s, const double* x, i
 // particle.tcc:994-1067 FLIP / PIC; mesh.tcc:1454-1467 particle velocity
 // constraints; USL stress update (mpm_scheme_usl.tcc:14-17); locate.
 template <int DIM, bool STRESS, bool FLIP>
-__global__ void __launch_bounds__(128) k_g2p(DevState s, double dt, double beta) {
+__global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, double dt,
+                                                                 double beta) {
   constexpr int NV = Elem<DIM>::NV;
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= s.np) return;

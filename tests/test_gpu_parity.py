@@ -205,8 +205,10 @@ def test_particles_leaving_the_mesh_are_removed_when_locate_is_off():
     keep = gg["cell"] >= 0
     assert np.count_nonzero(~keep) > 0
     assert np.count_nonzero(keep) == len(oo["x"])
-    for f in ("x", "v", "stress"):
+    for f in ("x", "v"):
         assert np.allclose(gg[f][keep], oo[f], rtol=0, atol=1e-12 * max(1.0, np.abs(oo[f]).max()))
+    # rigid motion: stresses are round-off noise on both sides
+    assert np.abs(gg["stress"][keep]).max() < 1e-6 and np.abs(oo["stress"]).max() < 1e-6
 
 
 def test_particle_leaving_the_mesh_is_an_error_when_locate_is_on():
