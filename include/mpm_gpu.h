@@ -174,6 +174,24 @@ int mpm_gpu_material_stress_batch(int32_t device, int32_t dim, const char* type,
                                   const double* dstrain, const double* density, double* state,
                                   double* out);
 
+/* The same constitutive update for callers that cannot allocate device memory
+ * (a plugin inside another program's memory arena, code running during a
+ * stream capture, a real-time loop with a fixed memory budget).  No
+ * counterpart in the reference.  It allocates nothing: the points are staged in
+ * a fixed array of the library's device image (32768 points, 7.3 MB, held by
+ * every GPU that loads the library until the process exits).  n above 32768
+ * is rejected with MPM_ERR_INVALID and a message in err (errlen bytes, may be
+ * NULL).  All calls share the array; the entry point serialises its callers
+ * with a process-wide lock and waits for its copies, so its calls never
+ * overlap.  Its first call on a device looks up the array's address with that
+ * device current: make it before any stream capture begins.  Uses the legacy
+ * default stream. */
+int mpm_gpu_material_stress_batch_noalloc(int32_t device, int32_t dim, const char* type,
+                                          const char* json_props, int64_t n,
+                                          const double* stress, const double* dstrain,
+                                          const double* density, double* state, double* out,
+                                          char* err, int64_t errlen);
+
 /* Library version string. */
 const char* mpm_gpu_version(void);
 

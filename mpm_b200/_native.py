@@ -67,6 +67,9 @@ SIGNATURES = {
     "mpm_gpu_device_field": (C.c_int, [_vp, C.c_int32, C.POINTER(_vp), _pi64, _pi32]),
     "mpm_gpu_material_stress_batch": (C.c_int, [C.c_int32, C.c_int32, C.c_char_p, C.c_char_p,
                                                 C.c_int64, _pd, _pd, _pd, _pd, _pd]),
+    "mpm_gpu_material_stress_batch_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_char_p,
+                                                        C.c_char_p, C.c_int64, _pd, _pd, _pd,
+                                                        _pd, _pd, C.c_char_p, C.c_int64]),
     "mpm_gpu_version": (C.c_char_p, []),
 }
 

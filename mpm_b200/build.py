@@ -25,6 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("kernels_fp64.cu", ["--fmad=false"]),
     ("mpm_gpu.cu", []),
+    ("noalloc.cu", []),
 ]
 HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp"]
 

@@ -746,6 +746,13 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
 
 }  // namespace
 
+namespace mpm_b200 {
+// the material factory of the C ABI, shared with the no-allocation entry point
+MaterialParams material_from_json(int dim, const char* type, const char* json_props) {
+  return make_material(dim, type, parse_json(json_props));
+}
+}  // namespace mpm_b200
+
 extern "C" {
 
 const char* mpm_gpu_version(void) { return MPM_VERSION; }
