@@ -49,7 +49,7 @@ BYTES_PER_ACTIVE_NODE = {
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--block", default="100,100,50", help="particle block in cells")
@@ -92,7 +92,7 @@ def max_over_ranks(x, world):
 
 class Clocks:
     """Sample nvidia-smi clocks and throttle reasons during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -101,10 +101,20 @@ class Clocks:
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.p = None
+        time.sleep(1.0)  # nvidia-smi needs a moment before its first sample
+        self.window = [None, None]
+
+    def mark_start(self):
+        import datetime
+        self.window[0] = datetime.datetime.now()
+
+    def mark_end(self):
+        import datetime
+        self.window[1] = datetime.datetime.now()
 
     def stop(self):
         if self.p is None:
@@ -115,17 +125,25 @@ class Clocks:
         except subprocess.TimeoutExpired:
             self.p.kill()
         self.f.flush()
-        rows = []
+        import datetime
+        rows, all_rows = [], []
         with open(self.f.name) as f:
             for line in f:
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) < 9:
+                if len(parts) < 10:
                     continue
                 try:
-                    rows.append((float(parts[1]), float(parts[2]), parts[4:]))
+                    ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
+                    row = (float(parts[2]), float(parts[3]), parts[5:])
                 except ValueError:
                     continue
+                all_rows.append(row)
+                if self.window[0] and self.window[1] and self.window[0] <= ts <= self.window[1]:
+                    rows.append(row)
         os.unlink(self.f.name)
+        in_window = bool(rows)
+        if not rows:
+            rows = all_rows[-3:]  # the timed region was shorter than the sampling period
         if not rows:
             return None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -133,7 +151,7 @@ class Clocks:
                           if v.lower().startswith("active")})
         return {"sm_mhz": statistics.median(r[0] for r in rows),
                 "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "in_timed_window": in_window}
 
 
 def measured_peaks():
@@ -223,7 +241,9 @@ def main():
     clocks = Clocks(dev)
     s.set_profiling(True)
     launches0 = s.launch_count
+    clocks.mark_start()
     ms = s.step_timed(args.steps)
+    clocks.mark_end()
     launches = s.launch_count - launches0
     prof = s.kernel_profile()
     clk = clocks.stop()
