@@ -40,6 +40,7 @@ BYTES_PER_PARTICLE = {
     # F 72, volume density 16, MC state 72
     "g2p": 335 + 328,
 }
+DTYPES = {"fp64": "f64", "mixed": "f32+f64"}
 BYTES_PER_ACTIVE_NODE = {
     # read mass, momentum, forces 80, flags 5; write velocity, acceleration 48
     "nodes_velocity": 133,
@@ -53,6 +54,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--block", default="100,100,50", help="particle block in cells")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     return ap.parse_args()
@@ -233,7 +235,7 @@ def main():
     t0 = time.perf_counter()
     prob = P.config_b(block=block)
     dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
-    s = P.build_solver(prob, device=0 if world == 1 else 0)
+    s = P.build_solver(prob, precision=args.precision, device=dev)
     setup_s = time.perf_counter() - t0
     n = s.nparticles
     s.step(args.warmup)
@@ -293,11 +295,12 @@ def main():
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"3D granular column collapse, MohrCoulomb USL FLIP FP64, "
+            "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
+            "config": {"workload": f"3D granular column collapse, MohrCoulomb USL FLIP "
+                                   f"{args.precision.upper()}, "
                                    f"200x100x50 hex8 dx=0.01, {n} particles",
                        "particles": n, "nodes": prob.nnodes, "cells": prob.ncells,
-                       "dt": prob.analysis["dt"], "precision": "fp64",
+                       "dt": prob.analysis["dt"], "precision": args.precision,
                        "l2": "state larger than L2 (no flush needed)",
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "setup_s": setup_s},

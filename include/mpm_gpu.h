@@ -29,6 +29,7 @@
 #ifndef MPM_GPU_H
 #define MPM_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -57,7 +58,11 @@ typedef struct {
   int32_t dim;              /* 2 (quad4 / ED2Q4) or 3 (hex8 / ED3H8) */
   int32_t scheme;           /* MPM_SCHEME_USF / MPM_SCHEME_USL */
   int32_t velocity_update;  /* MPM_VELOCITY_FLIP / MPM_VELOCITY_PIC */
-  int32_t precision;        /* MPM_PRECISION_FP64 / MPM_PRECISION_MIXED */
+  int32_t precision;        /* MPM_PRECISION_FP64: every quantity in FP64, rounding as the
+                               reference's CPU run (the parity mode);
+                               MPM_PRECISION_MIXED: FP32 transfers and constitutive update
+                               with FP64 positions, displacements, nodal mass division and
+                               apex returns (no counterpart in the reference) */
   double blending_ratio;    /* velocity_update_settings.blending_ratio */
   double dt;
   double damping_factor;    /* damping {type: Cundall, damping_factor} */
@@ -159,10 +164,42 @@ int64_t mpm_gpu_nparticles(mpm_gpu_t h);
 int64_t mpm_gpu_current_step(mpm_gpu_t h);
 int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out);
 
+/* Particle output and checkpoint records.  Particle::pod (particle.tcc:180-306)
+ * of every particle in the mesh, in particle order, packed on the device into
+ * the caller's record layout: record i at records + i * record_size, field f
+ * (the 74 PODParticle fields in declaration order, pod_particle.h:12-62) at
+ * byte offset offsets[f] with size sizes[f] -- the reference's
+ * pod::particle::dst_size / dst_offset / dst_sizes (pod_particle.cc), so a
+ * std::vector<PODParticle> can receive them and go to H5TBmake_table as in
+ * Mesh::write_particles_hdf5 (mesh.tcc:1573-1613).  Sizes must be 8 for the
+ * doubles, id and cell_id, 4 for material_id and nstate_vars, 1 for the two
+ * bools, each field aligned to its size, record_size a multiple of 8.
+ * *nrecords receives the number of particles in the mesh; with capacity below
+ * it nothing is written and MPM_ERR_INVALID is returned. */
+int mpm_gpu_write_pod(mpm_gpu_t h, void* records, int64_t capacity, int64_t* nrecords,
+                      size_t record_size, const size_t* offsets, const size_t* sizes,
+                      int32_t nfields);
+
+/* Checkpoint resume (MPMBase::checkpoint_resume, mpm_base.tcc:509-546;
+ * Mesh::read_particles_hdf5, mesh.tcc:1663-1720; Particle::initialise_particle,
+ * particle.tcc:21-175): replace the particles by n records in the layout of
+ * mpm_gpu_write_pod.  Density is mass / volume; state variables are taken when
+ * the record's nstate_vars matches the material's, else initialised; each
+ * particle is located from its recorded cell (that cell, its neighbours, then
+ * every cell in id order).  A particle outside the mesh is an error. */
+int mpm_gpu_load_pod(mpm_gpu_t h, const void* records, int64_t n, size_t record_size,
+                     const size_t* offsets, const size_t* sizes, int32_t nfields);
+
+/* Set the step counter (the resume step of analysis.resume.step; it drives the
+ * gravity ramp, mpm_explicit.tcc:145-153). */
+int mpm_gpu_set_current_step(mpm_gpu_t h, int64_t step);
+
 /* Device addresses of the particle state (for zero-copy interop, e.g. torch).
  * field: 0 x, 1 u, 2 v, 3 stress, 4 strain, 5 F, 6 volume, 7 density, 8 mass.
  * Returns the base address; component c of particle p is at
- * base[c * stride + p]; *ncomp receives the component count. */
+ * base[c * stride + p] (doubles); *ncomp receives the component count.
+ * MPM_PRECISION_MIXED keeps only x and u in FP64 and returns
+ * MPM_ERR_UNSUPPORTED for the other fields. */
 int mpm_gpu_device_field(mpm_gpu_t h, int32_t field, void** base, int64_t* stride,
                          int32_t* ncomp);
 

@@ -41,6 +41,7 @@ _vp = C.c_void_p
 _pd = C.POINTER(C.c_double)
 _pi64 = C.POINTER(C.c_int64)
 _pi32 = C.POINTER(C.c_int32)
+_psz = C.POINTER(C.c_size_t)
 SIGNATURES = {
     "mpm_gpu_create": (C.c_int, [C.POINTER(Config), C.POINTER(_vp)]),
     "mpm_gpu_destroy": (C.c_int, [_vp]),
@@ -64,6 +65,10 @@ SIGNATURES = {
     "mpm_gpu_nparticles": (C.c_int64, [_vp]),
     "mpm_gpu_current_step": (C.c_int64, [_vp]),
     "mpm_gpu_read_particles": (C.c_int, [_vp, C.POINTER(Particles)]),
+    "mpm_gpu_write_pod": (C.c_int, [_vp, _vp, C.c_int64, _pi64, C.c_size_t, _psz, _psz,
+                                    C.c_int32]),
+    "mpm_gpu_load_pod": (C.c_int, [_vp, _vp, C.c_int64, C.c_size_t, _psz, _psz, C.c_int32]),
+    "mpm_gpu_set_current_step": (C.c_int, [_vp, C.c_int64]),
     "mpm_gpu_device_field": (C.c_int, [_vp, C.c_int32, C.POINTER(_vp), _pi64, _pi32]),
     "mpm_gpu_material_stress_batch": (C.c_int, [C.c_int32, C.c_int32, C.c_char_p, C.c_char_p,
                                                 C.c_int64, _pd, _pd, _pd, _pd, _pd]),

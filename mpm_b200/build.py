@@ -21,13 +21,15 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 
 # (source, extra flags): the FP64 kernels never fuse multiply-add so that they
-# round like the reference's scalar arithmetic.
+# round like the reference's scalar arithmetic; the mixed-precision kernels do.
 UNITS = [
     ("kernels_fp64.cu", ["--fmad=false"]),
+    ("kernels_mixed.cu", []),
     ("mpm_gpu.cu", []),
     ("noalloc.cu", []),
+    ("pod.cu", []),
 ]
-HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp"]
+HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp", "mpm_device.cuh"]
 
 
 def _newer(target, deps):

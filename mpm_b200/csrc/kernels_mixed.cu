@@ -1,0 +1,669 @@
+// kernels_mixed.cu -- mixed-precision kernels of the explicit MPM step.
+//
+// Arithmetic in FP32 with FP64 where it carries the result:
+//   * positions and displacements are stored and advanced in FP64;
+//   * the shape functions use a local coordinate computed in FP64 (x and the
+//     cell centroid are FP64) and then rounded;
+//   * P2G accumulates each cell slot with Kahan-compensated FP32 sums, the node
+//     adds its (at most eight) cell partials in FP64 and divides momentum by
+//     mass in FP64;
+//   * the MohrCoulomb return map runs in FP32 (its stress invariants and Lode
+//     angle derivatives in FP64, see mc_invariants) and is redone in FP64 for
+//     points at the apex of the yield surface (deviatoric trial stress below
+//     1e-2 of the stress magnitude), for returns that remove more than 90 % of
+//     the trial stress (the subtraction would cancel in FP32) and when the
+//     FP32 return is not finite; the plastic deviatoric strain is accumulated
+//     in FP64;
+//   * F, volume and density are stored as deviations (H = F - I,
+//     P = V / V0 - 1) so that FP32 keeps the 1e-9 per-step increments.
+// Same step structure as the FP64 path (kernels_fp64.cu): counting sort,
+// per-cell P2G, node gather and update, G2P + stress + locate.
+#include <cuda_runtime.h>
+
+#include "mpm_device.cuh"
+#include "mpm_kernels.h"
+#include "mpm_state.cuh"
+
+#ifndef MPM_MIXED_G2P_MIN_BLOCKS
+#define MPM_MIXED_G2P_MIN_BLOCKS 4
+#endif
+#ifndef MPM_MIXED_P2G_MIN_BLOCKS
+#define MPM_MIXED_P2G_MIN_BLOCKS 3
+#endif
+
+namespace mpm_b200 {
+namespace {
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+  const float y = v - c;
+  const float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+template <int DIM>
+__device__ __forceinline__ float pmf(const DevState& s, int f, int64_t p) {
+  return s.pm[(int64_t)f * s.np + p];
+}
+template <int DIM>
+__device__ __forceinline__ void set_pmf(const DevState& s, int f, int64_t p, float v) {
+  s.pm[(int64_t)f * s.np + p] = v;
+}
+
+// local coordinate in FP64, rounded to FP32 for the shape functions
+template <int DIM>
+__device__ __forceinline__ void xi_f32(const DevState& s, int c, const double* x, float* xf) {
+  const CellGeom& g = s.geom[c];
+  double xi[DIM];
+  local_xi<DIM>(x, g.centroid, g.len, xi);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) xf[d] = (float)xi[d];
+}
+
+// node ids and nodal coordinates relative to node 0 of the cell (FP32)
+template <int DIM>
+__device__ __forceinline__ void cell_nodes_rel(const DevState& s, int c, int* nid, float* Xr) {
+  constexpr int NV = Elem<DIM>::NV;
+  double X[NV * DIM];
+  cell_nodes_coords<DIM>(s, c, nid, X);
+#pragma unroll
+  for (int n = 0; n < NV; ++n)
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) Xr[n * DIM + d] = (float)(X[n * DIM + d] - X[d]);
+}
+
+// ---------------------------------------------------------------- P2G cells
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(128, MPM_MIXED_P2G_MIN_BLOCKS)
+    k_p2g_cells_mixed(DevState s, float g0, float g1, float g2) {
+  constexpr int NV = Elem<DIM>::NV;
+  constexpr int LPC = DIM == 3 ? 2 : 1;
+  constexpr int SPL = NV / LPC;
+  constexpr int NVAL = 1 + 3 * DIM;
+  constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM;
+  constexpr bool MM = MODE != 1, FORCES = MODE != 0;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t c = t / LPC;
+  const int h = (int)(t % LPC);
+  const bool valid = c < s.ncells;
+  const int n = valid ? s.cnt[c] : 0;
+  const int s0 = valid ? s.start[c] : 0;
+  if constexpr (MODE != 1) {
+    if (h == 0 && n > 1) {  // ascending particle ids within the cell
+      int32_t* seg = s.order + s0;
+      for (int a = 1; a < n; ++a) {
+        const int32_t key = seg[a];
+        int b = a - 1;
+        while (b >= 0 && seg[b] > key) {
+          seg[b + 1] = seg[b];
+          --b;
+        }
+        seg[b + 1] = key;
+      }
+    }
+    __syncwarp();
+  }
+  if (!valid || n == 0) return;
+  int nid[NV];
+  float Xr[NV * DIM];
+  cell_nodes_rel<DIM>(s, (int)c, nid, Xr);
+  float acc[SPL][NVAL], cmp[SPL][NVAL];
+#pragma unroll
+  for (int k = 0; k < SPL; ++k)
+#pragma unroll
+    for (int v = 0; v < NVAL; ++v) acc[k][v] = cmp[k][v] = 0.f;
+  const float gv[3] = {g0, g1, g2};
+  for (int j = 0; j < n; ++j) {
+    const int64_t p = s.order[s0 + j];
+    double x[DIM];
+    load_x<DIM>(s, p, x);
+    float xi[DIM], Nk[SPL], Gk[SPL * DIM];
+    xi_f32<DIM>(s, (int)c, x, xi);
+    lane_shape<DIM>(xi, h, Nk, Gk);
+    const float m = pmf<DIM>(s, PM<DIM>::MASS, p);
+    if constexpr (MM) {
+      float v[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[d] = pmf<DIM>(s, PM<DIM>::V + d, p);
+#pragma unroll
+      for (int k = 0; k < SPL; ++k) {
+        const float mN = m * Nk[k];
+        kahan_add(acc[k][MASS], cmp[k][MASS], mN);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) kahan_add(acc[k][MOM + d], cmp[k][MOM + d], mN * v[d]);
+      }
+    }
+    if constexpr (FORCES) {
+      float inv[DIM * DIM];
+      jacobian_inverse<DIM>(xi, Xr, inv);
+      const float vol = pmf<DIM>(s, PM<DIM>::V0, p) * (1.f + pmf<DIM>(s, PM<DIM>::JP, p));
+      const float sc = -vol;
+      constexpr int NS = PF<DIM>::NS;
+      float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k = 0; k < NS; ++k) sig[k] = pmf<DIM>(s, PM<DIM>::S + k, p);
+#pragma unroll
+      for (int k = 0; k < SPL; ++k) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) kahan_add(acc[k][FEXT + d], cmp[k][FEXT + d], (gv[d] * m) * Nk[k]);
+        float Dn[DIM];
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) {
+          float a = Gk[k * DIM + 0] * inv[q * DIM + 0];
+#pragma unroll
+          for (int r = 1; r < DIM; ++r) a = a + Gk[k * DIM + r] * inv[q * DIM + r];
+          Dn[q] = a;
+        }
+        float f[DIM];
+        if constexpr (DIM == 2) {
+          f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
+          f[1] = Dn[1] * sig[1] + Dn[0] * sig[3];
+        } else {
+          f[0] = Dn[0] * sig[0] + Dn[1] * sig[3] + Dn[2] * sig[5];
+          f[1] = Dn[1] * sig[1] + Dn[0] * sig[3] + Dn[2] * sig[4];
+          f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) kahan_add(acc[k][FINT + d], cmp[k][FINT + d], f[d] * sc);
+      }
+    }
+  }
+  float* out = s.partials_f + ((int64_t)c * NV + h * SPL) * NVAL;
+#pragma unroll
+  for (int k = 0; k < SPL; ++k) {
+    if constexpr (MM) {
+#pragma unroll
+      for (int v = MASS; v < FEXT; ++v) out[k * NVAL + v] = acc[k][v] - cmp[k][v];
+    }
+    if constexpr (FORCES) {
+#pragma unroll
+      for (int v = FEXT; v < NVAL; ++v) out[k * NVAL + v] = acc[k][v] - cmp[k][v];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- node update
+// The cell partials of a node (ascending cell id) added in FP64.
+template <int DIM>
+__device__ __forceinline__ bool gather_node_mixed(const DevState& s, int64_t node, int v0, int nv,
+                                                  double* sum) {
+  constexpr int NV = Elem<DIM>::NV;
+  constexpr int NVAL = 1 + 3 * DIM;
+  for (int v = 0; v < nv; ++v) sum[v] = 0.;
+  bool active = false;
+  auto add = [&](int c, int slot) {
+    if (s.cnt[c] == 0) return;
+    const float* src = s.partials_f + ((int64_t)c * NV + slot) * NVAL + v0;
+    for (int v = 0; v < nv; ++v) sum[v] += (double)src[v];
+    active = true;
+  };
+  if (s.structured) {
+    const int nx = s.gcells[0] + 1, ny = s.gcells[1] + 1;
+    const int i = (int)(node % nx);
+    const int j = DIM == 2 ? (int)(node / nx) : (int)((node / nx) % ny);
+    const int k = DIM == 2 ? 0 : (int)(node / ((int64_t)nx * ny));
+    const int slot2[2][2] = {{0, 1}, {3, 2}};
+    const int kmin = DIM == 3 ? k - 1 : 0, kmax = DIM == 3 ? k : 0;
+    for (int ck = kmin; ck <= kmax; ++ck) {
+      if (DIM == 3 && (ck < 0 || ck >= s.gcells[2])) continue;
+      for (int cj = j - 1; cj <= j; ++cj) {
+        if (cj < 0 || cj >= s.gcells[1]) continue;
+        for (int ci = i - 1; ci <= i; ++ci) {
+          if (ci < 0 || ci >= s.gcells[0]) continue;
+          const int di = i - ci, dj = j - cj, dk = DIM == 3 ? k - ck : 0;
+          const int c = DIM == 2 ? ci + s.gcells[0] * cj : ci + s.gcells[0] * (cj + s.gcells[1] * ck);
+          add(c, slot2[dj][di] + 4 * dk);
+        }
+      }
+    }
+  } else {
+    for (int e = s.nc_off[node]; e < s.nc_off[node + 1]; ++e) add(s.nc_cell[e], s.nc_slot[e]);
+  }
+  return active;
+}
+
+// node.tcc:309-345 in FP64 on the gathered sums
+template <int DIM>
+__device__ __forceinline__ void node_accel_update_d(const DevState& s, double m, const double* fe,
+                                                    const double* fi, double* vel, double* acc,
+                                                    int bci, double dt, double damping) {
+  if (!(m > 1.0E-15)) return;
+  double uf[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) uf[d] = fe[d] + fi[d];
+  double ss = uf[0] * uf[0];
+#pragma unroll
+  for (int d = 1; d < DIM; ++d) ss = ss + uf[d] * uf[d];
+  const double nrm = sqrt(ss);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const double sg = (vel[d] > 0.) ? 1. : ((vel[d] < 0.) ? -1. : 0.);
+    acc[d] = (uf[d] - damping * nrm * sg) / m;
+  }
+  if (bci >= 0) {
+    const NodeBC& bc = s.bcs[bci];
+    if (bc.friction) apply_friction_constraints<DIM>(bc, vel, acc, dt);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      if (bc.acc_mask & (1u << d)) acc[d] = bc.acc[d];
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) vel[d] += acc[d] * dt;
+  if (bci >= 0) apply_velocity_constraints<DIM>(s.bcs[bci], vel, acc);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d)
+    if (fabs(vel[d]) < 1.0E-15) vel[d] = 0.;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d)
+    if (fabs(acc[d]) < 1.0E-15) acc[d] = 0.;
+}
+
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(256) k_nodes_mixed(DevState s, double dt, double damping) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= s.nn) return;
+  const int64_t nn = s.nn;
+  constexpr int NVAL = 1 + 3 * DIM;
+  double sum[NVAL];
+  const int v0 = MODE == 2 ? 1 + DIM : 0;
+  const int nv = MODE == 0 ? 1 + DIM : (MODE == 1 ? NVAL : 2 * DIM);
+  if (!gather_node_mixed<DIM>(s, n, v0, nv, sum)) return;
+  const int bci = s.bc_index[n];
+  double vel[DIM], acc[DIM];
+  if constexpr (MODE == 2) {
+    double mm[1];
+    gather_node_mixed<DIM>(s, n, 0, 1, mm);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      vel[d] = (double)s.nfv[(int64_t)d * nn + n];
+      acc[d] = (double)s.nfv[(int64_t)(DIM + d) * nn + n];
+    }
+    node_accel_update_d<DIM>(s, mm[0], &sum[0], &sum[DIM], vel, acc, bci, dt, damping);
+  } else {
+    const double m = sum[0];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) vel[d] = acc[d] = 0.;
+    if (m > 1.E-16) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) vel[d] = sum[1 + d] / m;  // FP64 mass division
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        if (fabs(vel[d]) < 1.E-15) vel[d] = 0.;
+    }
+    if (bci >= 0) apply_velocity_constraints<DIM>(s.bcs[bci], vel, acc);
+    if constexpr (MODE == 1)
+      node_accel_update_d<DIM>(s, m, &sum[1 + DIM], &sum[1 + 2 * DIM], vel, acc, bci, dt, damping);
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    s.nfv[(int64_t)d * nn + n] = (float)vel[d];
+    s.nfv[(int64_t)(DIM + d) * nn + n] = (float)acc[d];
+  }
+}
+
+// ------------------------------------------------------- stress and strain
+// MohrCoulomb in FP32, redone in FP64 at the apex or when not finite.
+__device__ __forceinline__ void mc_update_mixed(const MaterialParams& md, const MaterialT<float>& mf,
+                                                const float* sig, const float* de, float rho,
+                                                float* svf, double& pd, float* out) {
+  float trial[6];
+  {
+    float t[6];
+    de_mul(mf, de, t);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) trial[i] = sig[i] + t[i];
+  }
+  float smax = 0.f;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) smax = fmaxf(smax, fabsf(trial[i]));
+  const float rho_dev = sqrtf(2.f * mu_j2(trial));
+  bool fp64 = rho_dev <= 1e-2f * smax;
+  if (!fp64) {
+    float sv[SV_N];
+#pragma unroll
+    for (int k = 0; k < SVF_N; ++k) sv[k] = svf[k];
+    sv[SV_PD] = 0.f;
+    double pd_try = pd;
+    bool ok = mc_compute_stress<float, double>(mf, sig, de, rho, sv, pd_try, out);
+    if (ok && sv[SV_YIELD] != 0.f) {
+      // a return that removes most of the trial stress cancels: redo in FP64
+      float omax = 0.f;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) omax = fmaxf(omax, fabsf(out[i]));
+      ok = omax >= 0.1f * smax;
+    }
+    if (ok) {
+#pragma unroll
+      for (int k = 0; k < SVF_N; ++k) svf[k] = sv[k];
+      pd = pd_try;
+      return;
+    }
+    fp64 = true;
+  }
+  double sd[6], ded[6], svd[SV_N], od[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    sd[i] = (double)sig[i];
+    ded[i] = (double)de[i];
+  }
+#pragma unroll
+  for (int k = 0; k < SVF_N; ++k) svd[k] = (double)svf[k];
+  svd[SV_PD] = pd;
+  mc_compute_stress<double, double>(md, sd, ded, (double)rho, svd, svd[SV_PD], od);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) out[i] = (float)od[i];
+#pragma unroll
+  for (int k = 0; k < SVF_N; ++k) svf[k] = (float)svd[k];
+  pd = svd[SV_PD];
+}
+
+// mpm_scheme.tcc:75-103 in FP32 on the deviation variables (H, P).
+template <int DIM>
+__device__ __forceinline__ void stress_update_mixed(const DevState& s, int64_t p, int c,
+                                                    const int* nid, const float* D, float dt) {
+  constexpr int NV = Elem<DIM>::NV;
+  constexpr int NS = PF<DIM>::NS;
+  const int64_t np = s.np, nn = s.nn;
+  const float* Dc = s.dndx_cf + (int64_t)c * NV * DIM;
+  float Hi[DIM * DIM];
+#pragma unroll
+  for (int r = 0; r < DIM * DIM; ++r) Hi[r] = 0.f;
+  float sr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float src[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    float vel[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) vel[d] = s.nfv[(int64_t)d * nn + nid[i]];
+#pragma unroll
+    for (int r = 0; r < DIM; ++r)
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) Hi[r * DIM + q] += vel[r] * D[i * DIM + q] * dt;
+    const float* Dn = &D[i * DIM];
+    float dc[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) dc[d] = __ldg(&Dc[i * DIM + d]);
+    if constexpr (DIM == 2) {
+      sr[0] += Dn[0] * vel[0];
+      sr[1] += Dn[1] * vel[1];
+      sr[3] += Dn[1] * vel[0] + Dn[0] * vel[1];
+      src[0] += dc[0] * vel[0];
+      src[1] += dc[1] * vel[1];
+    } else {
+      sr[0] += Dn[0] * vel[0];
+      sr[1] += Dn[1] * vel[1];
+      sr[2] += Dn[2] * vel[2];
+      sr[3] += Dn[1] * vel[0] + Dn[0] * vel[1];
+      sr[4] += Dn[2] * vel[1] + Dn[1] * vel[2];
+      sr[5] += Dn[2] * vel[0] + Dn[0] * vel[2];
+      src[0] += dc[0] * vel[0];
+      src[1] += dc[1] * vel[1];
+      src[2] += dc[2] * vel[2];
+    }
+  }
+  // F_inc = I + Hi with the reference's 1e-15 snapping (particle.tcc:1619-1626)
+#pragma unroll
+  for (int r = 0; r < DIM * DIM; ++r)
+    if (fabsf(Hi[r]) < 1.E-15f) Hi[r] = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+    if (fabsf(sr[k]) < 1.E-15f) sr[k] = 0.f;
+#pragma unroll
+  for (int k = 0; k < DIM; ++k)
+    if (fabsf(src[k]) < 1.E-15f) src[k] = 0.f;
+  float dstrain[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) dstrain[k] = sr[k] * dt;
+  float ssum = src[0];
+#pragma unroll
+  for (int k = 1; k < DIM; ++k) ssum += src[k];
+  const float dvol = dt * ssum;
+  if constexpr (DIM == 2) {
+    const int map[3] = {0, 1, 3};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      set_pmf<DIM>(s, PM<2>::E + k, p, pmf<DIM>(s, PM<2>::E + k, p) + dstrain[map[k]]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      set_pmf<DIM>(s, PM<3>::E + k, p, pmf<DIM>(s, PM<3>::E + k, p) + dstrain[k]);
+  }
+  // V *= (1 + dvol), rho /= (1 + dvol) as P = V / V0 - 1 (particle.tcc:598-605)
+  const float P = pmf<DIM>(s, PM<DIM>::JP, p);
+  const float Pn = P + dvol + P * dvol;
+  set_pmf<DIM>(s, PM<DIM>::JP, p, Pn);
+  const float rho = pmf<DIM>(s, PM<DIM>::RHO0, p) / (1.f + Pn);
+  float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int k = 0; k < NS; ++k) sig[k] = pmf<DIM>(s, PM<DIM>::S + k, p);
+  const int mi = s.mat[p];
+  float out[6];
+  if (s.mats_f[mi].type == 0) {
+    float t[6];
+    de_mul(s.mats_f[mi], dstrain, t);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) out[i] = sig[i] + t[i];
+  } else {
+    float svf[SVF_N];
+#pragma unroll
+    for (int k = 0; k < SVF_N; ++k) svf[k] = s.svf[(int64_t)k * np + p];
+    double* pdp = &s.pf[(int64_t)PDX<DIM>::PDS * np + p];
+    double pd = *pdp;
+    mc_update_mixed(s.mats[mi], s.mats_f[mi], sig, dstrain, rho, svf, pd, out);
+    *pdp = pd;
+    const int first = s.mats_f[mi].softening ? 0 : SV_EPS;  // phi..tc change only with softening
+    s.svf[(int64_t)SV_YIELD * np + p] = svf[SV_YIELD];
+#pragma unroll
+    for (int k = 1; k < SVF_N; ++k)
+      if (k >= first) s.svf[(int64_t)k * np + p] = svf[k];
+  }
+#pragma unroll
+  for (int k = 0; k < NS; ++k) set_pmf<DIM>(s, PM<DIM>::S + k, p, out[k]);
+  // F = F_inc F as H = H + Hi + Hi H
+  if constexpr (DIM == 2) {
+    float H[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) H[k] = pmf<DIM>(s, PM<2>::H + k, p);
+    const float n00 = H[0] + Hi[0] + (Hi[0] * H[0] + Hi[1] * H[2]);
+    const float n01 = H[1] + Hi[1] + (Hi[0] * H[1] + Hi[1] * H[3]);
+    const float n10 = H[2] + Hi[2] + (Hi[2] * H[0] + Hi[3] * H[2]);
+    const float n11 = H[3] + Hi[3] + (Hi[2] * H[1] + Hi[3] * H[3]);
+    set_pmf<DIM>(s, PM<2>::H + 0, p, n00);
+    set_pmf<DIM>(s, PM<2>::H + 1, p, n01);
+    set_pmf<DIM>(s, PM<2>::H + 2, p, n10);
+    set_pmf<DIM>(s, PM<2>::H + 3, p, n11);
+  } else {
+    float H[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) H[k] = pmf<DIM>(s, PM<3>::H + k, p);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        set_pmf<DIM>(s, PM<3>::H + r * 3 + q, p,
+                     H[r * 3 + q] + Hi[r * 3 + q] +
+                         ((Hi[r * 3 + 0] * H[0 * 3 + q] + Hi[r * 3 + 1] * H[1 * 3 + q]) +
+                          Hi[r * 3 + 2] * H[2 * 3 + q]));
+  }
+}
+
+template <int DIM>
+__device__ __forceinline__ void dn_dx_all_f(const float* xi, const float* Xr, float* D) {
+  constexpr int NV = Elem<DIM>::NV;
+  float inv[DIM * DIM];
+  jacobian_inverse<DIM>(xi, Xr, inv);
+  float G[NV * DIM];
+  grad_shapefn<DIM>(xi, G);
+#pragma unroll
+  for (int n = 0; n < NV; ++n)
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) {
+      float a = G[n * DIM + 0] * inv[q * DIM + 0];
+#pragma unroll
+      for (int r = 1; r < DIM; ++r) a = a + G[n * DIM + r] * inv[q * DIM + r];
+      D[n * DIM + q] = a;
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128) k_stress_mixed(DevState s, float dt) {
+  constexpr int NV = Elem<DIM>::NV;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.np) return;
+  const int c = s.cell[p];
+  if (c < 0) return;
+  double x[DIM];
+  load_x<DIM>(s, p, x);
+  float xi[DIM], D[NV * DIM], Xr[NV * DIM];
+  int nid[NV];
+  xi_f32<DIM>(s, c, x, xi);
+  cell_nodes_rel<DIM>(s, c, nid, Xr);
+  dn_dx_all_f<DIM>(xi, Xr, D);
+  stress_update_mixed<DIM>(s, p, c, nid, D, dt);
+}
+
+// --------------------------------------------------------------------- G2P
+template <int DIM, bool STRESS, bool FLIP>
+__global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
+    k_g2p_mixed(DevState s, double dt, float beta) {
+  constexpr int NV = Elem<DIM>::NV;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.np) return;
+  const int c = s.cell[p];
+  if (c < 0) return;
+  const int64_t np = s.np, nn = s.nn;
+  double x[DIM];
+  load_x<DIM>(s, p, x);
+  float xi[DIM], N[NV], Xr[NV * DIM];
+  int nid[NV];
+  xi_f32<DIM>(s, c, x, xi);
+  shapefn<DIM>(xi, N);
+  cell_nodes_rel<DIM>(s, c, nid, Xr);
+  float nvel[DIM], nacc[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.f;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * s.nfv[(int64_t)d * nn + nid[i]];
+    if constexpr (FLIP) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * s.nfv[(int64_t)(DIM + d) * nn + nid[i]];
+    }
+  }
+  const float dtf = (float)dt;
+  float v[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) v[d] = pmf<DIM>(s, PM<DIM>::V + d, p);
+  if constexpr (FLIP) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] += nacc[d] * dtf;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = beta * v[d] + (1.f - beta) * nvel[d];
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = nvel[d];
+  }
+  double xn[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const double dx = (double)nvel[d] * dt;  // FP64 position / displacement update
+    xn[d] = x[d] + dx;
+    s.pf[(int64_t)(PDX<DIM>::X + d) * np + p] = xn[d];
+    s.pf[(int64_t)(PDX<DIM>::U + d) * np + p] += dx;
+  }
+  const int pv = s.pvc[p];
+  if (pv >= 0) {
+    const ParticleVC& r = s.pvcs[pv];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      if (r.mask & (1u << d)) v[d] = (float)r.value[d];
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) set_pmf<DIM>(s, PM<DIM>::V + d, p, v[d]);
+  if constexpr (STRESS) {
+    float D[NV * DIM];
+    dn_dx_all_f<DIM>(xi, Xr, D);
+    stress_update_mixed<DIM>(s, p, c, nid, D, dtf);
+  }
+  bool finite = true;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) finite = finite && isfinite(xn[d]);
+  if (!finite) {
+    raise_err(s, ERR_NONFINITE);
+    s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+    return;
+  }
+  const int nc = locate_near<DIM>(s, xn, c);
+  if (nc >= 0) {
+    if (nc != c) s.cell[p] = nc;
+  } else {
+    s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+  }
+}
+
+inline unsigned nblk(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+template <int DIM>
+void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& pr) {
+  const int64_t np = s.np, nn = s.nn;
+  if (np == 0) return;
+  constexpr int LPC = DIM == 3 ? 2 : 1;
+  cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
+  const unsigned pb = nblk(np, 128), nb = nblk(nn, 256), cb = nblk(s.ncells * LPC, 128);
+  const float g0 = (float)a.g[0], g1 = (float)a.g[1], g2 = (float)a.g[2];
+  pr.begin(K_SORT, st);
+  counting_sort(s, st);
+  pr.end(K_SORT, st);
+  if (a.scheme == 1) {  // USL
+    pr.begin(K_P2G, st);
+    k_p2g_cells_mixed<DIM, 2><<<cb, 128, 0, st>>>(s, g0, g1, g2);
+    pr.end(K_P2G, st);
+    pr.begin(K_NODES_VEL, st);
+    k_nodes_mixed<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    pr.end(K_NODES_VEL, st);
+    pr.begin(K_G2P, st);
+    if (a.flip)
+      k_g2p_mixed<DIM, true, true><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
+    else
+      k_g2p_mixed<DIM, true, false><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
+    pr.end(K_G2P, st);
+  } else {  // USF
+    pr.begin(K_P2G, st);
+    k_p2g_cells_mixed<DIM, 0><<<cb, 128, 0, st>>>(s, g0, g1, g2);
+    pr.end(K_P2G, st);
+    pr.begin(K_NODES_VEL, st);
+    k_nodes_mixed<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    pr.end(K_NODES_VEL, st);
+    pr.begin(K_STRESS, st);
+    k_stress_mixed<DIM><<<pb, 128, 0, st>>>(s, (float)a.dt);
+    pr.end(K_STRESS, st);
+    pr.begin(K_P2G_FORCES, st);
+    k_p2g_cells_mixed<DIM, 1><<<cb, 128, 0, st>>>(s, g0, g1, g2);
+    pr.end(K_P2G_FORCES, st);
+    pr.begin(K_NODES_ACC, st);
+    k_nodes_mixed<DIM, 2><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    pr.end(K_NODES_ACC, st);
+    pr.begin(K_G2P, st);
+    if (a.flip)
+      k_g2p_mixed<DIM, false, true><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
+    else
+      k_g2p_mixed<DIM, false, false><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
+    pr.end(K_G2P, st);
+  }
+  pr.begin(K_LOCATE, st);
+  launch_locate_fallback(DIM, s, a.remove_lost, st);
+  pr.end(K_LOCATE, st);
+}
+
+}  // namespace
+
+void launch_step_mixed(int dim, const DevState& s, const StepArgs& a, cudaStream_t st,
+                       Profiler& prof) {
+  if (dim == 2)
+    step_mixed<2>(s, a, st, prof);
+  else
+    step_mixed<3>(s, a, st, prof);
+}
+
+}  // namespace mpm_b200

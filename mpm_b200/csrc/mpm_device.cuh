@@ -1,0 +1,190 @@
+// mpm_device.cuh -- device helpers shared by the FP64 and the mixed-precision
+// kernels: addressing of particle fields and cells, per-lane shape functions,
+// the Jacobian inverse and the locate search.  Each kernel translation unit
+// compiles them with its own floating-point contraction setting.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "mpm_math.cuh"
+#include "mpm_state.cuh"
+
+namespace mpm_b200 {
+namespace {
+
+template <int DIM>
+struct PV {  // value offsets within a cell-slot partial
+  static constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM, N = 1 + 3 * DIM;
+};
+
+__device__ __forceinline__ void raise_err(const DevState& s, unsigned bits) { atomicOr(s.err, bits); }
+
+template <int DIM>
+__device__ __forceinline__ void load_x(const DevState& s, int64_t p, double* x) {
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) x[d] = s.pf[(int64_t)(PF<DIM>::X + d) * s.np + p];
+}
+
+// cell (i, j, k) of a tensor-product grid
+template <int DIM>
+__device__ __forceinline__ void cell_ijk(const DevState& s, int c, int* ijk) {
+  ijk[0] = c % s.gcells[0];
+  if constexpr (DIM == 2) {
+    ijk[1] = c / s.gcells[0];
+  } else {
+    ijk[1] = (c / s.gcells[0]) % s.gcells[1];
+    ijk[2] = c / (s.gcells[0] * s.gcells[1]);
+  }
+}
+
+// local node n of a cell -> offset (di, dj, dk) (quadrilateral_element.tcc:1-7,
+// hexahedron_element.tcc:1-13)
+__device__ __forceinline__ int off_i(int n) { return ((n & 3) == 1 || (n & 3) == 2) ? 1 : 0; }
+__device__ __forceinline__ int off_j(int n) { return ((n & 3) >= 2) ? 1 : 0; }
+__device__ __forceinline__ int off_k(int n) { return n >= 4 ? 1 : 0; }
+
+// node ids and nodal coordinates of a cell
+template <int DIM>
+__device__ __forceinline__ void cell_nodes_coords(const DevState& s, int c, int* nid, double* X) {
+  constexpr int NV = Elem<DIM>::NV;
+  if (s.structured) {
+    int ijk[3] = {0, 0, 0};
+    cell_ijk<DIM>(s, c, ijk);
+    const int nx = s.gcells[0] + 1, ny = s.gcells[1] + 1;
+#pragma unroll
+    for (int n = 0; n < NV; ++n) {
+      const int i = ijk[0] + off_i(n), j = ijk[1] + off_j(n);
+      if constexpr (DIM == 2) {
+        nid[n] = i + nx * j;
+        X[n * 2 + 0] = __ldg(&s.axis[0][i]);
+        X[n * 2 + 1] = __ldg(&s.axis[1][j]);
+      } else {
+        const int k = ijk[2] + off_k(n);
+        nid[n] = i + nx * (j + ny * k);
+        X[n * 3 + 0] = __ldg(&s.axis[0][i]);
+        X[n * 3 + 1] = __ldg(&s.axis[1][j]);
+        X[n * 3 + 2] = __ldg(&s.axis[2][k]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int n = 0; n < NV; ++n) nid[n] = __ldg(&s.cell_nodes[(int64_t)c * NV + n]);
+#pragma unroll
+    for (int n = 0; n < NV; ++n)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) X[n * DIM + d] = __ldg(&s.ncoord[(int64_t)d * s.nn + nid[n]]);
+  }
+}
+
+// J^-1 at xi (quadrilateral_element.tcc:295-309, hexahedron_element.tcc:307-321)
+template <int DIM, typename R>
+__device__ __forceinline__ void jacobian_inverse(const R* xi, const R* X, R* inv) {
+  constexpr int NV = Elem<DIM>::NV;
+  R G[NV * DIM];
+  grad_shapefn<DIM>(xi, G);
+  R J[DIM * DIM];
+#pragma unroll
+  for (int r = 0; r < DIM; ++r)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      R a = G[0 * DIM + r] * X[0 * DIM + c];
+#pragma unroll
+      for (int n = 1; n < NV; ++n) a = a + G[n * DIM + r] * X[n * DIM + c];
+      J[r * DIM + c] = a;
+    }
+  inverse<DIM>(J, inv);
+}
+
+// dN_n/dx for one local node n given J^-1
+template <int DIM>
+__device__ __forceinline__ void dn_dx_node(const double* xi, const double* inv, int n, double* Dn) {
+  constexpr int NV = Elem<DIM>::NV;
+  double G[NV * DIM];
+  grad_shapefn<DIM>(xi, G);  // folded to the needed entries by the compiler
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    double a = G[n * DIM + 0] * inv[c * DIM + 0];
+#pragma unroll
+    for (int k = 1; k < DIM; ++k) a = a + G[n * DIM + k] * inv[c * DIM + k];
+    Dn[c] = a;
+  }
+}
+
+// Shape functions and natural gradients of the SPL slots a lane owns: all
+// of them in 2D; in 3D lane h owns slots 4h..4h+3, which share the z factor
+// (1 - xi_z) or (1 + xi_z).  Same operations and grouping as shapefn /
+// grad_shapefn (the z factor is the last product), with the lane's half
+// chosen by value selects so the two lanes of a cell do not diverge.
+template <int DIM, typename R>
+__device__ __forceinline__ void lane_shape(const R* xi, int h, R* Nk, R* Gk) {
+  if constexpr (DIM == 2) {
+    shapefn<2>(xi, Nk);
+    grad_shapefn<2>(xi, Gk);
+  } else {
+    const R xm = 1 - xi[0], xp = 1 + xi[0], ym = 1 - xi[1], yp = 1 + xi[1];
+    const R z = h ? (1 + xi[2]) : (1 - xi[2]);
+    const R e = R(0.125);
+    const R zs = h ? e : -e;  // sign of d/dxi_z
+    // in-plane order of the four nodes of a face: (-,-), (+,-), (+,+), (-,+)
+    Nk[0] = e * xm * ym * z;
+    Nk[1] = e * xp * ym * z;
+    Nk[2] = e * xp * yp * z;
+    Nk[3] = e * xm * yp * z;
+    Gk[0 * 3 + 0] = -e * ym * z;
+    Gk[1 * 3 + 0] = e * ym * z;
+    Gk[2 * 3 + 0] = e * yp * z;
+    Gk[3 * 3 + 0] = -e * yp * z;
+    Gk[0 * 3 + 1] = -e * xm * z;
+    Gk[1 * 3 + 1] = -e * xp * z;
+    Gk[2 * 3 + 1] = e * xp * z;
+    Gk[3 * 3 + 1] = e * xm * z;
+    Gk[0 * 3 + 2] = zs * xm * ym;
+    Gk[1 * 3 + 2] = zs * xp * ym;
+    Gk[2 * 3 + 2] = zs * xp * yp;
+    Gk[3 * 3 + 2] = zs * xm * yp;
+  }
+}
+
+
+// ------------------------------------------------------------------ locate
+// mesh.tcc:1116-1151: the current cell, then neighbours in ascending id
+template <int DIM>
+__device__ __forceinline__ int locate_near(const DevState& s, const double* x, int c) {
+  double xi[DIM];
+  {
+    const CellGeom& g = s.geom[c];
+    if (point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi)) return c;
+  }
+  if (s.structured) {
+    // neighbours of a tensor-product cell: the 3^dim - 1 cells around it,
+    // ascending id (the node-sharing cells of mesh.tcc:287-306)
+    int ijk[3] = {0, 0, 0};
+    cell_ijk<DIM>(s, c, ijk);
+    const int kmin = DIM == 3 ? ijk[2] - 1 : 0, kmax = DIM == 3 ? ijk[2] + 1 : 0;
+    for (int k = kmin; k <= kmax; ++k) {
+      if (DIM == 3 && (k < 0 || k >= s.gcells[2])) continue;
+      for (int j = ijk[1] - 1; j <= ijk[1] + 1; ++j) {
+        if (j < 0 || j >= s.gcells[1]) continue;
+        for (int i = ijk[0] - 1; i <= ijk[0] + 1; ++i) {
+          if (i < 0 || i >= s.gcells[0]) continue;
+          const int nc = DIM == 2 ? i + s.gcells[0] * j : i + s.gcells[0] * (j + s.gcells[1] * k);
+          if (nc == c) continue;
+          const CellGeom& g = s.geom[nc];
+          if (point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi)) return nc;
+        }
+      }
+    }
+    return -1;
+  }
+  const int b = s.nb_off[c], e = s.nb_off[c + 1];
+  for (int k = b; k < e; ++k) {
+    const int nc = s.nb[k];
+    const CellGeom& g = s.geom[nc];
+    if (point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi)) return nc;
+  }
+  return -1;
+}
+
+
+}  // namespace
+}  // namespace mpm_b200

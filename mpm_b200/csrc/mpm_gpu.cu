@@ -205,7 +205,28 @@ struct mpm_gpu_solver {
   bool any_mc = false;
   Profiler prof;
 
+  // per-particle data the step never changes, kept for the PODParticle
+  // records: id, natural size [3][np], acceleration [3][np]
+  std::vector<uint64_t> p_id;
+  std::vector<double> p_nsize, p_acc;
+  bool aux_dirty = true;
+  DevBuf<uint64_t> d_pid;
+  DevBuf<double> d_nsize, d_pacc;
+  DevBuf<int32_t> d_matid, d_list;
+  DevBuf<uint32_t> d_nstate;
+  DevBuf<uint8_t> d_stage;
+  uint8_t* h_stage = nullptr;  // pinned, two halves
+  size_t h_stage_bytes = 0;
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+
+  // mixed precision: d_pf holds [x, u, pdstrain] in FP64, the rest is FP32
+  bool mixed = false;
+  DevBuf<float> d_pm, d_svf, d_nfv, d_partials_f, d_dndx_cf;
+  DevBuf<MaterialT<float>> d_mats_f;
+
   int nfields() const { return dim == 2 ? PF<2>::NF : PF<3>::NF; }
+  int nfields_x() const { return dim == 2 ? PDX<2>::ND : PDX<3>::ND; }
+  int nfields_m() const { return dim == 2 ? PM<2>::NF : PM<3>::NF; }
   int nnf() const { return dim == 2 ? NF<2>::NNF : NF<3>::NNF; }
 };
 
@@ -477,6 +498,10 @@ MaterialParams make_material(int dim, const std::string& type, const Json& j) {
     m.shear = m.E / (2.0 * (1 + m.nu));
     const double apex = m.c_peak / std::tan(m.phi_peak);
     m.tc_init = check_low(m.tension_cutoff < apex ? m.tension_cutoff : apex);
+    m.sin_phi = std::sin(m.phi_peak);
+    m.cos_phi = std::cos(m.phi_peak);
+    m.tan_phi = std::tan(m.phi_peak);
+    m.tan_psi = std::tan(m.psi_peak);
   } else {
     throw InvalidArg("unknown material type \"" + type + "\"");
   }
@@ -518,7 +543,15 @@ void upload_mesh(mpm_gpu_t h) {
   ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 2, st), "memset");
   if (h->structured)
     for (int d = 0; d < 3; ++d) h->d_axis[d].upload(h->axis[d].data(), h->axis[d].size(), st);
-  h->d_dndx_c.upload(h->dndx_c.data(), h->dndx_c.size(), st);
+  if (h->mixed) {
+    std::vector<float> f(h->dndx_c.begin(), h->dndx_c.end());
+    h->d_dndx_cf.upload(f.data(), f.size(), st);
+    h->d_nfv.alloc((size_t)2 * dim * h->nnodes);
+    ck(cudaMemsetAsync(h->d_nfv.p, 0, sizeof(float) * 2 * dim * h->nnodes, st), "memset");
+    ck(cudaStreamSynchronize(st), "sync");  // f is a stack temporary
+  } else {
+    h->d_dndx_c.upload(h->dndx_c.data(), h->dndx_c.size(), st);
+  }
   if (!h->structured) {
     h->d_nc_off.upload(h->nc_off.data(), h->nc_off.size(), st);
     h->d_nc_cell.alloc(std::max<size_t>(1, h->nc_cell.size()));
@@ -527,7 +560,10 @@ void upload_mesh(mpm_gpu_t h) {
     h->d_nc_slot.upload(h->nc_slot.data(), h->nc_slot.size(), st);
   }
   const int nval = 1 + 3 * dim;
-  h->d_partials.alloc((size_t)h->ncells * h->nv * nval);
+  if (h->mixed)
+    h->d_partials_f.alloc((size_t)h->ncells * h->nv * nval);
+  else
+    h->d_partials.alloc((size_t)h->ncells * h->nv * nval);
   h->d_cnt.alloc(h->ncells);
   h->d_start.alloc(h->ncells + 1);
   const int64_t nb = (h->ncells + SCAN_BLOCK - 1) / SCAN_BLOCK;
@@ -601,7 +637,8 @@ void upload_pvc(mpm_gpu_t h) {
 
 void allocate_particles(mpm_gpu_t h) {
   const int64_t np = h->np;
-  h->d_pf.alloc((size_t)h->nfields() * np);
+  h->d_pf.alloc((size_t)(h->mixed ? h->nfields_x() : h->nfields()) * np);
+  if (h->mixed) h->d_pm.alloc((size_t)h->nfields_m() * np);
   h->d_cell.alloc(np);
   h->d_mat.alloc(np);
   h->d_lost.alloc(std::max<int64_t>(1, np));
@@ -609,10 +646,12 @@ void allocate_particles(mpm_gpu_t h) {
   h->d_order.alloc(std::max<int64_t>(1, np));
   h->any_mc = false;
   for (auto& m : h->mats) h->any_mc = h->any_mc || m.type == 1;
-  if (h->any_mc)
+  h->d_sv.free();
+  h->d_svf.free();
+  if (h->any_mc && h->mixed)
+    h->d_svf.alloc((size_t)SVF_N * np);
+  else if (h->any_mc)
     h->d_sv.alloc((size_t)SV_N * np);
-  else
-    h->d_sv.free();
 }
 
 void refresh_state(mpm_gpu_t h) {
@@ -661,6 +700,124 @@ void refresh_state(mpm_gpu_t h) {
   s.mats = h->d_mats.p;
   s.bcs = h->d_bcs.p;
   s.pvcs = h->d_pvcs.p;
+  s.pm = h->d_pm.p;
+  s.svf = h->d_svf.p;
+  s.nfv = h->d_nfv.p;
+  s.partials_f = h->d_partials_f.p;
+  s.dndx_cf = h->d_dndx_cf.p;
+  s.mats_f = h->d_mats_f.p;
+}
+
+// Offsets of the FP64 particle layout (PF) for the solver's dimension.
+struct Layout {
+  int X, U, V, S, E, F, VOL, RHO, MASS, NF, NS, NE, NFG;
+};
+Layout layout(int dim) {
+  if (dim == 2)
+    return {PF<2>::X, PF<2>::U,   PF<2>::V,    PF<2>::S,  PF<2>::E,  PF<2>::F,  PF<2>::VOL,
+            PF<2>::RHO, PF<2>::MASS, PF<2>::NF, PF<2>::NS, PF<2>::NE, PF<2>::NFG};
+  return {PF<3>::X, PF<3>::U,   PF<3>::V,    PF<3>::S,  PF<3>::E,  PF<3>::F,  PF<3>::VOL,
+          PF<3>::RHO, PF<3>::MASS, PF<3>::NF, PF<3>::NS, PF<3>::NE, PF<3>::NFG};
+}
+struct LayoutM {
+  int V, S, E, H, V0, RHO0, JP, MASS, NF, PDS;
+};
+LayoutM layout_m(int dim) {
+  if (dim == 2)
+    return {PM<2>::V, PM<2>::S, PM<2>::E, PM<2>::H, PM<2>::V0, PM<2>::RHO0, PM<2>::JP, PM<2>::MASS,
+            PM<2>::NF, PDX<2>::PDS};
+  return {PM<3>::V, PM<3>::S, PM<3>::E, PM<3>::H, PM<3>::V0, PM<3>::RHO0, PM<3>::JP, PM<3>::MASS,
+          PM<3>::NF, PDX<3>::PDS};
+}
+bool identity_entry(int dim, int k) { return dim == 2 ? (k == 0 || k == 3) : (k % 4 == 0); }
+
+// Upload particle fields given in the FP64 layout (pf: [PF::NF][np], sv:
+// [SV_N][np] or empty).  The mixed path keeps x, u and pdstrain in FP64 and
+// stores the rest in FP32, F as H = F - I and volume / density as the initial
+// values with P = V / V0 - 1 = 0.
+void upload_particle_fields(mpm_gpu_t h, const std::vector<double>& pf, const std::vector<double>& sv) {
+  const int64_t np = h->np;
+  const int dim = h->dim;
+  if (!h->mixed) {
+    h->d_pf.upload(pf.data(), pf.size(), h->stream);
+    if (h->any_mc) h->d_sv.upload(sv.data(), sv.size(), h->stream);
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    return;
+  }
+  const Layout L = layout(dim);
+  const LayoutM M = layout_m(dim);
+  std::vector<double> px((size_t)h->nfields_x() * np, 0.0);
+  std::vector<float> pm((size_t)h->nfields_m() * np, 0.f);
+  for (int64_t p = 0; p < np; ++p) {
+    auto f = [&](int o) { return pf[(size_t)o * np + p]; };
+    for (int d = 0; d < dim; ++d) {
+      px[(size_t)(PDX<3>::X + d) * np + p] = f(L.X + d);
+      px[(size_t)(dim + d) * np + p] = f(L.U + d);
+      pm[(size_t)(M.V + d) * np + p] = (float)f(L.V + d);
+    }
+    px[(size_t)M.PDS * np + p] = h->any_mc ? sv[(size_t)SV_PD * np + p] : 0.;
+    for (int k = 0; k < L.NS; ++k) pm[(size_t)(M.S + k) * np + p] = (float)f(L.S + k);
+    for (int k = 0; k < L.NE; ++k) pm[(size_t)(M.E + k) * np + p] = (float)f(L.E + k);
+    for (int k = 0; k < L.NFG; ++k)
+      pm[(size_t)(M.H + k) * np + p] = (float)(f(L.F + k) - (identity_entry(dim, k) ? 1. : 0.));
+    pm[(size_t)M.V0 * np + p] = (float)f(L.VOL);
+    pm[(size_t)M.RHO0 * np + p] = (float)f(L.RHO);
+    pm[(size_t)M.JP * np + p] = 0.f;
+    pm[(size_t)M.MASS * np + p] = (float)f(L.MASS);
+  }
+  h->d_pf.upload(px.data(), px.size(), h->stream);
+  h->d_pm.upload(pm.data(), pm.size(), h->stream);
+  std::vector<float> svf;
+  if (h->any_mc) {
+    svf.resize((size_t)SVF_N * np);
+    for (size_t i = 0; i < svf.size(); ++i) svf[i] = (float)sv[i];
+    h->d_svf.upload(svf.data(), svf.size(), h->stream);
+  }
+  ck(cudaStreamSynchronize(h->stream), "sync");
+}
+
+// Download the particle fields into the FP64 layout (inverse of
+// upload_particle_fields).
+void download_particle_fields(mpm_gpu_t h, std::vector<double>& pf, std::vector<double>& sv) {
+  const int64_t np = h->np;
+  const int dim = h->dim;
+  pf.assign((size_t)h->nfields() * np, 0.0);
+  sv.assign(h->any_mc ? (size_t)SV_N * np : 0, 0.0);
+  if (!h->mixed) {
+    h->d_pf.download(pf.data(), pf.size(), h->stream);
+    if (h->any_mc) h->d_sv.download(sv.data(), sv.size(), h->stream);
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    return;
+  }
+  const Layout L = layout(dim);
+  const LayoutM M = layout_m(dim);
+  std::vector<double> px((size_t)h->nfields_x() * np);
+  std::vector<float> pm((size_t)h->nfields_m() * np);
+  std::vector<float> svf(h->any_mc ? (size_t)SVF_N * np : 0);
+  h->d_pf.download(px.data(), px.size(), h->stream);
+  h->d_pm.download(pm.data(), pm.size(), h->stream);
+  if (h->any_mc) h->d_svf.download(svf.data(), svf.size(), h->stream);
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  for (int64_t p = 0; p < np; ++p) {
+    auto m = [&](int o) { return (double)pm[(size_t)o * np + p]; };
+    auto at = [&](int o) -> double& { return pf[(size_t)o * np + p]; };
+    for (int d = 0; d < dim; ++d) {
+      at(L.X + d) = px[(size_t)d * np + p];
+      at(L.U + d) = px[(size_t)(dim + d) * np + p];
+      at(L.V + d) = m(M.V + d);
+    }
+    for (int k = 0; k < L.NS; ++k) at(L.S + k) = m(M.S + k);
+    for (int k = 0; k < L.NE; ++k) at(L.E + k) = m(M.E + k);
+    for (int k = 0; k < L.NFG; ++k) at(L.F + k) = m(M.H + k) + (identity_entry(dim, k) ? 1. : 0.);
+    const double jp = m(M.JP);
+    at(L.VOL) = m(M.V0) * (1. + jp);
+    at(L.RHO) = m(M.RHO0) / (1. + jp);
+    at(L.MASS) = m(M.MASS);
+    if (h->any_mc) {
+      for (int k = 0; k < SVF_N; ++k) sv[(size_t)k * np + p] = (double)svf[(size_t)k * np + p];
+      sv[(size_t)SV_PD * np + p] = px[(size_t)M.PDS * np + p];
+    }
+  }
 }
 
 // Pack host particle rows (ABI layout) into the device SoA field order.
@@ -707,7 +864,6 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
     at(VOL, p) = in->volume ? in->volume[p] : 0.;
     at(MASS, p) = in->mass ? in->mass[p] : at(VOL, p) * at(RHO, p);
   }
-  h->d_pf.upload(pf.data(), pf.size(), h->stream);
   std::vector<int32_t> cell(np);
   for (int64_t p = 0; p < np; ++p) {
     if (in->cell) {
@@ -720,8 +876,9 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
   }
   h->d_cell.upload(cell.data(), np, h->stream);
   h->d_mat.upload(h->p_mat.data(), np, h->stream);
+  std::vector<double> sv;
   if (h->any_mc) {
-    std::vector<double> sv((size_t)SV_N * np, 0.0);
+    sv.assign((size_t)SV_N * np, 0.0);
     for (int64_t p = 0; p < np; ++p) {
       const MaterialParams& m = h->mats[h->p_mat[p]];
       double s[SV_N] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -731,8 +888,8 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
         mc_init_state(m, s);
       for (int k = 0; k < SV_N; ++k) sv[(size_t)k * np + p] = s[k];
     }
-    h->d_sv.upload(sv.data(), sv.size(), h->stream);
   }
+  upload_particle_fields(h, pf, sv);
 }
 
 #define MPM_GUARD(h)                                                   \
@@ -764,7 +921,8 @@ int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out) {
   if (cfg->scheme != MPM_SCHEME_USF && cfg->scheme != MPM_SCHEME_USL) return MPM_ERR_UNSUPPORTED;
   if (cfg->velocity_update != MPM_VELOCITY_FLIP && cfg->velocity_update != MPM_VELOCITY_PIC)
     return MPM_ERR_UNSUPPORTED;
-  if (cfg->precision != MPM_PRECISION_FP64) return MPM_ERR_UNSUPPORTED;
+  if (cfg->precision != MPM_PRECISION_FP64 && cfg->precision != MPM_PRECISION_MIXED)
+    return MPM_ERR_UNSUPPORTED;
   if (!(cfg->dt > 0)) return MPM_ERR_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MPM_ERR_CUDA;
@@ -773,6 +931,7 @@ int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out) {
   h->cfg = *cfg;
   h->dim = cfg->dim;
   h->nv = cfg->dim == 2 ? 4 : 8;
+  h->mixed = cfg->precision == MPM_PRECISION_MIXED;
   if (cudaSetDevice(cfg->device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete h;
@@ -789,6 +948,9 @@ int mpm_gpu_destroy(mpm_gpu_t h) {
     cudaStreamSynchronize(h->stream);
     cudaStreamDestroy(h->stream);
   }
+  if (h->h_stage) cudaFreeHost(h->h_stage);
+  for (auto& e : h->stage_ev)
+    if (e) cudaEventDestroy(e);
   delete h;
   return MPM_OK;
 }
@@ -897,6 +1059,12 @@ int mpm_gpu_add_material(mpm_gpu_t h, int32_t id, const char* type, const char* 
   h->mats.push_back(m);
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
   h->d_mats.upload(h->mats.data(), h->mats.size(), h->stream);
+  if (h->mixed) {
+    std::vector<MaterialT<float>> mf;
+    for (auto& x : h->mats) mf.push_back(material_cast<float>(x));
+    h->d_mats_f.upload(mf.data(), mf.size(), h->stream);
+  }
+  ck(cudaStreamSynchronize(h->stream), "sync");
   MPM_END(h)
   return MPM_OK;
 }
@@ -980,8 +1148,17 @@ int mpm_gpu_initialise(mpm_gpu_t h) {
     ++count[cell[p]];
   }
   std::vector<double> vol(np), rho(np), mass(np);
+  h->p_id.resize(np);
+  h->p_nsize.assign((size_t)3 * np, 0.0);
+  h->p_acc.assign((size_t)3 * np, 0.0);
+  h->aux_dirty = true;
   for (int64_t p = 0; p < np; ++p) {
     const MaterialParams& m = h->mats[h->p_mat[p]];
+    h->p_id[p] = (uint64_t)p;
+    // Particle::assign_volume (particle.tcc:557-583): unit element length 2
+    // over the cell's particle count to the power 1/dim
+    const double ns = 2.0 / std::pow((double)count[cell[p]], 1.0 / h->dim);
+    for (int d = 0; d < h->dim; ++d) h->p_nsize[(size_t)d * np + p] = ns;
     vol[p] = h->cell_volume[cell[p]] / (double)count[cell[p]];
     rho[p] = m.density;
     mass[p] = vol[p] * rho[p];
@@ -1016,8 +1193,16 @@ int mpm_gpu_assign_particle_stresses(mpm_gpu_t h, int64_t n, const double* stres
       throw InvalidArg("2D particle stress must have zero yz and xz components");
     for (int k = 0; k < ns; ++k) cols[(size_t)k * n + p] = stress[p * 6 + k];
   }
-  ck(cudaMemcpyAsync(h->d_pf.p + (size_t)S * n, cols.data(), sizeof(double) * cols.size(),
-                     cudaMemcpyHostToDevice, h->stream), "H2D");
+  if (h->mixed) {
+    const std::vector<float> colf(cols.begin(), cols.end());
+    const int SM = dim == 2 ? PM<2>::S : PM<3>::S;
+    ck(cudaMemcpyAsync(h->d_pm.p + (size_t)SM * n, colf.data(), sizeof(float) * colf.size(),
+                       cudaMemcpyHostToDevice, h->stream), "H2D");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+  } else {
+    ck(cudaMemcpyAsync(h->d_pf.p + (size_t)S * n, cols.data(), sizeof(double) * cols.size(),
+                       cudaMemcpyHostToDevice, h->stream), "H2D");
+  }
   ck(cudaStreamSynchronize(h->stream), "sync");
   MPM_END(h)
   return MPM_OK;
@@ -1060,6 +1245,13 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
     h->p_mat[p] = (uint8_t)it->second;
   }
   h->p_vc.assign(n, {});
+  if ((int64_t)h->p_id.size() != n) {
+    h->p_id.resize(n);
+    for (int64_t p = 0; p < n; ++p) h->p_id[p] = (uint64_t)p;
+    h->p_nsize.assign((size_t)3 * n, 0.0);
+    h->p_acc.assign((size_t)3 * n, 0.0);
+  }
+  h->aux_dirty = true;
   allocate_particles(h);
   upload_pvc(h);
   pack_particles(h, in, nullptr);
@@ -1094,7 +1286,10 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
     if (h->cfg.gravity_ramping_time > 0.0)
       gm = std::min(1.0, static_cast<double>(h->step) * h->cfg.dt / h->cfg.gravity_ramping_time);
     for (int d = 0; d < 3; ++d) a.g[d] = d < h->dim ? gm * h->cfg.gravity[d] : 0.;
-    launch_step_fp64(h->dim, h->ds, a, h->stream, h->prof);
+    if (h->mixed)
+      launch_step_mixed(h->dim, h->ds, a, h->stream, h->prof);
+    else
+      launch_step_fp64(h->dim, h->ds, a, h->stream, h->prof);
     ck(cudaGetLastError(), "kernel launch");
     ++h->step;
   }
@@ -1154,16 +1349,10 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
   const int dim = h->dim;
   const int64_t np = h->np;
-  std::vector<double> pf((size_t)h->nfields() * np);
+  std::vector<double> pf, sv;
   std::vector<int32_t> cell(np);
-  std::vector<double> sv;
-  h->d_pf.download(pf.data(), pf.size(), h->stream);
   h->d_cell.download(cell.data(), np, h->stream);
-  if (h->any_mc) {
-    sv.resize((size_t)SV_N * np);
-    h->d_sv.download(sv.data(), sv.size(), h->stream);
-  }
-  ck(cudaStreamSynchronize(h->stream), "sync");
+  download_particle_fields(h, pf, sv);
   auto at = [&](int f, int64_t p) { return pf[(size_t)f * np + p]; };
   const int X = dim == 2 ? PF<2>::X : PF<3>::X, U = dim == 2 ? PF<2>::U : PF<3>::U;
   const int V = dim == 2 ? PF<2>::V : PF<3>::V, S = dim == 2 ? PF<2>::S : PF<3>::S;
@@ -1226,10 +1415,299 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   return MPM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// PODParticle field sizes (pod_particle.cc dst_sizes): the two bools, the two
+// unsigned, everything else 8 bytes
+size_t pod_expected_size(int f) {
+  if (f == 40 || f == 50) return 1;
+  if (f == 52 || f == 53) return 4;
+  return 8;
+}
+
+void check_pod_layout(size_t record_size, const size_t* offsets, const size_t* sizes,
+                      int32_t nfields, PodLayout& L) {
+  if (nfields != POD_NFIELDS) throw InvalidArg("a PODParticle record has 74 fields");
+  if (!offsets || !sizes) throw InvalidArg("null record layout");
+  if (record_size == 0 || record_size % 8 != 0 || record_size > (1u << 16))
+    throw InvalidArg("record size must be a positive multiple of 8 bytes");
+  for (int f = 0; f < POD_NFIELDS; ++f) {
+    if (sizes[f] != pod_expected_size(f))
+      throw InvalidArg("PODParticle field " + std::to_string(f) + " has size " +
+                       std::to_string(sizes[f]) + ", expected " +
+                       std::to_string(pod_expected_size(f)));
+    if (offsets[f] % sizes[f] != 0 || offsets[f] + sizes[f] > record_size)
+      throw InvalidArg("PODParticle field " + std::to_string(f) +
+                       " is misaligned or outside the record");
+    L.offset[f] = (int32_t)offsets[f];
+  }
+  L.record_size = (int64_t)record_size;
+}
+
+// Byte runs of a record covered by fields (the rest -- padding, a vtable
+// pointer -- is never written into the caller's records).
+std::vector<std::pair<size_t, size_t>> pod_runs(const size_t* offsets, const size_t* sizes) {
+  std::vector<std::pair<size_t, size_t>> r;
+  for (int f = 0; f < POD_NFIELDS; ++f) r.emplace_back(offsets[f], offsets[f] + sizes[f]);
+  std::sort(r.begin(), r.end());
+  std::vector<std::pair<size_t, size_t>> m;
+  for (auto& x : r) {
+    if (!m.empty() && x.first <= m.back().second)
+      m.back().second = std::max(m.back().second, x.second);
+    else
+      m.push_back(x);
+  }
+  return m;
+}
+
+void upload_pod_aux(mpm_gpu_t h) {
+  if (!h->aux_dirty) return;
+  const int64_t np = h->np;
+  h->d_pid.upload(h->p_id.data(), np, h->stream);
+  h->d_nsize.upload(h->p_nsize.data(), 3 * np, h->stream);
+  h->d_pacc.upload(h->p_acc.data(), 3 * np, h->stream);
+  std::vector<int32_t> ids(h->mats.size(), -1);
+  std::vector<uint32_t> nstate(h->mats.size(), 0);
+  for (auto& kv : h->mat_index) ids[kv.second] = kv.first;
+  for (size_t i = 0; i < h->mats.size(); ++i) nstate[i] = h->mats[i].type == 1 ? SV_N : 0;
+  h->d_matid.upload(ids.data(), ids.size(), h->stream);
+  h->d_nstate.upload(nstate.data(), nstate.size(), h->stream);
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  h->aux_dirty = false;
+}
+
+// Mesh::locate_particle_cells (mesh.tcc:1116-1151) on the host: the recorded
+// cell, its neighbours in ascending id, then every cell in id order.
+int32_t host_locate(mpm_gpu_t h, const double* x, int64_t hint) {
+  auto inside = [&](int64_t c) {
+    const CellGeom& g = h->geom[c];
+    double xi[3];
+    return h->dim == 2 ? point_in_cell<2>(x, g.centroid, g.len, g.mean_length, xi)
+                       : point_in_cell<3>(x, g.centroid, g.len, g.mean_length, xi);
+  };
+  if (hint >= 0 && hint < h->ncells) {
+    if (inside(hint)) return (int32_t)hint;
+    if (h->structured) {
+      int ijk[3] = {0, 0, 0};
+      int64_t c = hint;
+      ijk[0] = (int)(c % h->gcells[0]);
+      c /= h->gcells[0];
+      if (h->dim == 2) {
+        ijk[1] = (int)c;
+      } else {
+        ijk[1] = (int)(c % h->gcells[1]);
+        ijk[2] = (int)(c / h->gcells[1]);
+      }
+      const int kmin = h->dim == 3 ? ijk[2] - 1 : 0, kmax = h->dim == 3 ? ijk[2] + 1 : 0;
+      for (int k = kmin; k <= kmax; ++k) {
+        if (h->dim == 3 && (k < 0 || k >= h->gcells[2])) continue;
+        for (int j = ijk[1] - 1; j <= ijk[1] + 1; ++j) {
+          if (j < 0 || j >= h->gcells[1]) continue;
+          for (int i = ijk[0] - 1; i <= ijk[0] + 1; ++i) {
+            if (i < 0 || i >= h->gcells[0]) continue;
+            const int64_t nc = h->dim == 2 ? i + (int64_t)h->gcells[0] * j
+                                           : i + (int64_t)h->gcells[0] * (j + (int64_t)h->gcells[1] * k);
+            if (nc != hint && inside(nc)) return (int32_t)nc;
+          }
+        }
+      }
+    } else {
+      for (int32_t k = h->nb_off[hint]; k < h->nb_off[hint + 1]; ++k)
+        if (inside(h->nb[k])) return h->nb[k];
+    }
+  }
+  return host_scan(h, x);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mpm_gpu_write_pod(mpm_gpu_t h, void* records, int64_t capacity, int64_t* nrecords,
+                      size_t record_size, const size_t* offsets, const size_t* sizes,
+                      int32_t nfields) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("no particles");
+  if (!nrecords) throw InvalidArg("null nrecords");
+  PodLayout L{};
+  check_pod_layout(record_size, offsets, sizes, nfields, L);
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  refresh_state(h);
+  const int64_t np = h->np;
+  std::vector<int32_t> cell(np);
+  h->d_cell.download(cell.data(), np, h->stream);
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  std::vector<int32_t> list;
+  list.reserve(np);
+  for (int64_t p = 0; p < np; ++p)
+    if (cell[p] >= 0) list.push_back((int32_t)p);
+  const int64_t count = (int64_t)list.size();
+  *nrecords = count;
+  if (count > capacity) throw InvalidArg("record capacity is below the number of particles in the mesh");
+  if (count == 0) return MPM_OK;
+  if (!records) throw InvalidArg("null records");
+  upload_pod_aux(h);
+  h->d_list.upload(list.data(), list.size(), h->stream);
+  const auto runs = pod_runs(offsets, sizes);
+  // chunks of at most 64 MiB, packed on the device and copied to pinned
+  // memory in turn; the host scatters chunk i while the device packs i + 1
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (64 << 20) / (int64_t)record_size));
+  const size_t bytes = (size_t)chunk * record_size;
+  if (h->d_stage.n < 2 * bytes) h->d_stage.alloc(2 * bytes);
+  if (h->h_stage_bytes < 2 * bytes) {
+    if (h->h_stage) cudaFreeHost(h->h_stage);
+    h->h_stage = nullptr;
+    h->h_stage_bytes = 0;
+    ck(cudaHostAlloc(reinterpret_cast<void**>(&h->h_stage), 2 * bytes, cudaHostAllocDefault),
+       "cudaHostAlloc");
+    h->h_stage_bytes = 2 * bytes;
+  }
+  for (auto& e : h->stage_ev)
+    if (!e) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  PodAux a{h->d_pid.p, h->d_nsize.p, h->d_pacc.p, h->d_matid.p, h->d_nstate.p};
+  int64_t pend_first[2] = {-1, -1}, pend_n[2] = {0, 0};
+  auto drain = [&](int k) {
+    if (pend_first[k] < 0) return;
+    ck(cudaEventSynchronize(h->stage_ev[k]), "pod copy");
+    const uint8_t* src = h->h_stage + (size_t)k * bytes;
+    uint8_t* dst = static_cast<uint8_t*>(records) + (size_t)pend_first[k] * record_size;
+    for (int64_t i = 0; i < pend_n[k]; ++i)
+      for (auto& r : runs)
+        std::memcpy(dst + i * record_size + r.first, src + i * record_size + r.first,
+                    r.second - r.first);
+    pend_first[k] = -1;
+  };
+  int k = 0;
+  for (int64_t first = 0; first < count; first += chunk, k ^= 1) {
+    const int64_t n = std::min<int64_t>(chunk, count - first);
+    drain(k);
+    launch_pod_pack(h->dim, h->mixed, h->ds, a, L, h->d_list.p + first, n,
+                    h->d_stage.p + (size_t)k * bytes, h->stream);
+    ck(cudaGetLastError(), "pod pack");
+    ck(cudaMemcpyAsync(h->h_stage + (size_t)k * bytes, h->d_stage.p + (size_t)k * bytes,
+                       (size_t)n * record_size, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    ck(cudaEventRecord(h->stage_ev[k], h->stream), "cudaEventRecord");
+    pend_first[k] = first;
+    pend_n[k] = n;
+  }
+  drain(k);
+  drain(k ^ 1);
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_load_pod(mpm_gpu_t h, const void* records, int64_t n, size_t record_size,
+                     const size_t* offsets, const size_t* sizes, int32_t nfields) {
+  MPM_GUARD(h)
+  if (!h->mesh_set) throw InvalidArg("set the mesh first");
+  if (h->mats.empty()) throw InvalidArg("no material");
+  if (n <= 0 || !records) throw InvalidArg("no records");
+  if (n > INT32_MAX) throw InvalidArg("too many particles for 32-bit indices");
+  PodLayout L{};
+  check_pod_layout(record_size, offsets, sizes, nfields, L);
+  const int dim = h->dim;
+  const uint8_t* base = static_cast<const uint8_t*>(records);
+  auto dbl = [&](int64_t i, int f) {
+    double v;
+    std::memcpy(&v, base + i * record_size + offsets[f], 8);
+    return v;
+  };
+  auto u64 = [&](int64_t i, int f) {
+    uint64_t v;
+    std::memcpy(&v, base + i * record_size + offsets[f], 8);
+    return v;
+  };
+  auto u32 = [&](int64_t i, int f) {
+    uint32_t v;
+    std::memcpy(&v, base + i * record_size + offsets[f], 4);
+    return v;
+  };
+  std::vector<double> x(3 * n), u(3 * n), v(3 * n), st(6 * n), sn(6 * n), F(9 * n), vol(n),
+      mass(n), rho(n), sv((size_t)SV_N * n, 0.0);
+  std::vector<int64_t> cell(n);
+  std::vector<int32_t> mat(n);
+  std::vector<uint64_t> ids(n);
+  std::vector<double> nsize((size_t)3 * n, 0.0), acc((size_t)3 * n, 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    ids[i] = u64(i, 0);
+    mass[i] = dbl(i, 1);
+    vol[i] = dbl(i, 2);
+    if (!(vol[i] > 0.)) throw InvalidArg("Particle volume cannot be negative");
+    rho[i] = mass[i] / vol[i];  // particle.tcc:46-47
+    for (int d = 0; d < 3; ++d) {
+      const bool in = d < dim;
+      x[i * 3 + d] = in ? dbl(i, 4 + d) : 0.;
+      u[i * 3 + d] = in ? dbl(i, 7 + d) : 0.;
+      v[i * 3 + d] = in ? dbl(i, 13 + d) : 0.;
+      if (in) {
+        nsize[(size_t)d * n + i] = dbl(i, 10 + d);
+        acc[(size_t)d * n + i] = dbl(i, 16 + d);
+      }
+    }
+    for (int k = 0; k < 6; ++k) {
+      st[i * 6 + k] = dbl(i, 19 + k);
+      sn[i * 6 + k] = dbl(i, 25 + k);
+    }
+    for (int k = 0; k < 9; ++k) F[i * 9 + k] = dbl(i, 31 + k);
+    if (dim == 2) {  // the 2D state has no out-of-plane components
+      st[i * 6 + 4] = st[i * 6 + 5] = 0.;
+      sn[i * 6 + 2] = sn[i * 6 + 4] = sn[i * 6 + 5] = 0.;
+    }
+    const uint32_t mid = u32(i, 52);
+    auto it = h->mat_index.find((int32_t)mid);
+    if (it == h->mat_index.end()) throw InvalidArg("Material is invalid to assign to particle!");
+    mat[i] = (int32_t)mid;
+    const MaterialParams& m = h->mats[it->second];
+    double s9[SV_N] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (m.type == 1) {
+      mc_init_state(m, s9);
+      if (u32(i, 53) == (uint32_t)SV_N)  // particle.tcc:160-168
+        for (int k = 0; k < SV_N; ++k) s9[k] = dbl(i, 54 + k);
+    }
+    for (int k = 0; k < SV_N; ++k) sv[i * SV_N + k] = s9[k];
+    const uint64_t c = u64(i, 51);
+    cell[i] = host_locate(h, &x[i * 3], c < (uint64_t)h->ncells ? (int64_t)c : -1);
+    if (cell[i] < 0) throw InvalidArg("Particle outside the mesh domain");
+  }
+  mpm_gpu_particles in{};
+  in.x = x.data();
+  in.u = u.data();
+  in.v = v.data();
+  in.stress = st.data();
+  in.strain = sn.data();
+  in.F = F.data();
+  in.volume = vol.data();
+  in.mass = mass.data();
+  in.density = rho.data();
+  in.cell = cell.data();
+  in.material = mat.data();
+  in.svars = sv.data();
+  const int rc = mpm_gpu_load_particles(h, n, &in);
+  if (rc != MPM_OK) return rc;
+  h->p_id = std::move(ids);
+  h->p_nsize = std::move(nsize);
+  h->p_acc = std::move(acc);
+  h->aux_dirty = true;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_set_current_step(mpm_gpu_t h, int64_t step) {
+  MPM_GUARD(h)
+  if (step < 0) throw InvalidArg("negative step");
+  h->step = step;
+  MPM_END(h)
+  return MPM_OK;
+}
+
 int mpm_gpu_device_field(mpm_gpu_t h, int32_t field, void** base, int64_t* stride, int32_t* ncomp) {
   MPM_GUARD(h)
   if (!h->initialised || !base || !stride || !ncomp) throw InvalidArg("bad call");
   const int dim = h->dim;
+  if (h->mixed && field != 0 && field != 1)
+    return fail(h, MPM_ERR_UNSUPPORTED, "mixed precision: only x and u are FP64 device fields");
   int off = 0, nc = 0;
   switch (field) {
     case 0: off = dim == 2 ? PF<2>::X : PF<3>::X; nc = dim; break;

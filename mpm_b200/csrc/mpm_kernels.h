@@ -53,6 +53,26 @@ struct Profiler {
 
 void launch_step_fp64(int dim, const DevState& s, const StepArgs& a, cudaStream_t st,
                       Profiler& prof);
+void launch_step_mixed(int dim, const DevState& s, const StepArgs& a, cudaStream_t st,
+                       Profiler& prof);
+// shared by both paths: the per-step counting sort and the exhaustive locate
+void counting_sort(const DevState& s, cudaStream_t st);
+void launch_locate_fallback(int dim, const DevState& s, int remove_lost, cudaStream_t st);
+// PODParticle records (pod_particle.h:12-62): 74 fields, caller's layout
+constexpr int POD_NFIELDS = 74;
+struct PodLayout {
+  int32_t offset[POD_NFIELDS];  // byte offset of each field in a record
+  int64_t record_size;
+};
+struct PodAux {                 // per-particle data the step never changes
+  const uint64_t* id;           // [np] particle id
+  const double* nsize;          // [3][np] natural particle size
+  const double* acc;            // [3][np] particle acceleration
+  const int32_t* material_id;   // [material slot] material id
+  const uint32_t* nstate;       // [material slot] number of state variables
+};
+void launch_pod_pack(int dim, bool mixed, const DevState& s, const PodAux& a, const PodLayout& L,
+                     const int32_t* list, int64_t count, uint8_t* out, cudaStream_t st);
 void launch_material_batch_fp64(int dim, int64_t n, const MaterialParams& m, const double* stress,
                                 const double* dstrain, const double* density, double* state,
                                 double* out, cudaStream_t st);

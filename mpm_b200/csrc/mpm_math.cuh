@@ -9,6 +9,7 @@
 // to the reference source tree.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 
 #ifdef __CUDACC__
@@ -245,25 +246,72 @@ MPM_HD int structured_scan(const double* p, const int32_t* ncell, const double* 
 }
 
 // ------------------------------------------------------------------ materials
-struct MaterialParams {
+// Material parameters in the working precision R (double on the FP64 path;
+// float on the mixed path, converted once per material).
+template <typename R>
+struct MaterialT {
   int type;  // 0 LinearElastic, 1 MohrCoulomb
   int softening;
-  double density, E, nu;
-  double bulk, shear, a1, a2;  // elastic tensor entries (a1 diag, a2 off-diag, G shear)
-  double phi_peak, psi_peak, c_peak, phi_res, psi_res, c_res;
-  double pd_peak, pd_res, tension_cutoff;
-  double grain_density, min_packing;
-  double tc_init;  // initial tension cutoff state (mohr_coulomb.tcc:97-100)
+  R density, E, nu;
+  R bulk, shear, a1, a2;  // elastic tensor entries (a1 diag, a2 off-diag, G shear)
+  R phi_peak, psi_peak, c_peak, phi_res, psi_res, c_res;
+  R pd_peak, pd_res, tension_cutoff;
+  R grain_density, min_packing;
+  R tc_init;  // initial tension cutoff state (mohr_coulomb.tcc:97-100)
+  // sin, cos, tan of the peak friction angle and tan of the peak dilation
+  // angle, computed once on the host (they enter every yield-function
+  // evaluation; softening replaces them per point)
+  R sin_phi, cos_phi, tan_phi, tan_psi;
 };
+using MaterialParams = MaterialT<double>;
+
+template <typename R>
+MPM_HD MaterialT<R> material_cast(const MaterialParams& m) {
+  MaterialT<R> r;
+  r.type = m.type;
+  r.softening = m.softening;
+  r.density = R(m.density);
+  r.E = R(m.E);
+  r.nu = R(m.nu);
+  r.bulk = R(m.bulk);
+  r.shear = R(m.shear);
+  r.a1 = R(m.a1);
+  r.a2 = R(m.a2);
+  r.phi_peak = R(m.phi_peak);
+  r.psi_peak = R(m.psi_peak);
+  r.c_peak = R(m.c_peak);
+  r.phi_res = R(m.phi_res);
+  r.psi_res = R(m.psi_res);
+  r.c_res = R(m.c_res);
+  r.pd_peak = R(m.pd_peak);
+  r.pd_res = R(m.pd_res);
+  r.tension_cutoff = R(m.tension_cutoff);
+  r.grain_density = R(m.grain_density);
+  r.min_packing = R(m.min_packing);
+  r.tc_init = R(m.tc_init);
+  r.sin_phi = R(m.sin_phi);
+  r.cos_phi = R(m.cos_phi);
+  r.tan_phi = R(m.tan_phi);
+  r.tan_psi = R(m.tan_psi);
+  return r;
+}
 
 enum { SV_YIELD = 0, SV_PHI, SV_PSI, SV_COH, SV_TC, SV_EPS, SV_RHO, SV_THETA, SV_PD, SV_N };
 
-MPM_HD double check_low(double v) { return v > 1.0e-15 ? v : 1.0e-15; }  // mohr_coulomb.h:124
+template <typename R>
+MPM_HD R check_low(R v) {  // mohr_coulomb.h:124
+  return v > R(1.0e-15) ? v : R(1.0e-15);
+}
+template <typename R>
+MPM_HD R dbl_eps() {  // numeric_limits<double>::epsilon, the reference's threshold
+  return R(kDblEps);
+}
 
 // De * b for the isotropic elastic tensor, summed over k = 0..5 in order with
 // the zero entries of the dense 6x6 skipped (they add exact zeros).
-MPM_HD void de_mul(const MaterialParams& m, const double* b, double* o) {
-  const double a1 = m.a1, a2 = m.a2, G = m.shear;
+template <typename R>
+MPM_HD void de_mul(const MaterialT<R>& m, const R* b, R* o) {
+  const R a1 = m.a1, a2 = m.a2, G = m.shear;
   o[0] = (a1 * b[0] + a2 * b[1]) + a2 * b[2];
   o[1] = (a2 * b[0] + a1 * b[1]) + a2 * b[2];
   o[2] = (a2 * b[0] + a2 * b[1]) + a1 * b[2];
@@ -273,18 +321,20 @@ MPM_HD void de_mul(const MaterialParams& m, const double* b, double* o) {
 }
 
 // (a^T De) . b (mohr_coulomb.tcc:433,454-455)
-MPM_HD double row_de_dot(const MaterialParams& m, const double* a, const double* b) {
-  const double a1 = m.a1, a2 = m.a2, G = m.shear;
-  const double r0 = (a[0] * a1 + a[1] * a2) + a[2] * a2;
-  const double r1 = (a[0] * a2 + a[1] * a1) + a[2] * a2;
-  const double r2 = (a[0] * a2 + a[1] * a2) + a[2] * a1;
-  const double r3 = a[3] * G, r4 = a[4] * G, r5 = a[5] * G;
+template <typename R>
+MPM_HD R row_de_dot(const MaterialT<R>& m, const R* a, const R* b) {
+  const R a1 = m.a1, a2 = m.a2, G = m.shear;
+  const R r0 = (a[0] * a1 + a[1] * a2) + a[2] * a2;
+  const R r1 = (a[0] * a2 + a[1] * a1) + a[2] * a2;
+  const R r2 = (a[0] * a2 + a[1] * a2) + a[2] * a1;
+  const R r3 = a[3] * G, r4 = a[4] * G, r5 = a[5] * G;
   return ((((r0 * b[0] + r1 * b[1]) + r2 * b[2]) + r3 * b[3]) + r4 * b[4]) + r5 * b[5];
 }
 
 // updated += -((lambda * De) * v)  (mohr_coulomb.tcc:463,468,502)
-MPM_HD void sub_lambda_de(const MaterialParams& m, double lambda, const double* v, double* u) {
-  const double l1 = lambda * m.a1, l2 = lambda * m.a2, lg = lambda * m.shear;
+template <typename R>
+MPM_HD void sub_lambda_de(const MaterialT<R>& m, R lambda, const R* v, R* u) {
+  const R l1 = lambda * m.a1, l2 = lambda * m.a2, lg = lambda * m.shear;
   u[0] += -((l1 * v[0] + l2 * v[1]) + l2 * v[2]);
   u[1] += -((l2 * v[0] + l1 * v[1]) + l2 * v[2]);
   u[2] += -((l2 * v[0] + l2 * v[1]) + l1 * v[2]);
@@ -294,209 +344,294 @@ MPM_HD void sub_lambda_de(const MaterialParams& m, double lambda, const double* 
 }
 
 // material_utility.tcc:2-200
-MPM_HD double mu_p(const double* s) { return (1. / 3. * (s[0] + s[1] + s[2])); }
-MPM_HD double sq(double x) { return x * x; }
-MPM_HD double mu_j2(const double* s) {
-  return (sq(s[0] - s[1]) + sq(s[1] - s[2]) + sq(s[0] - s[2])) / 6.0 + sq(s[3]) + sq(s[4]) +
+template <typename R>
+MPM_HD R mu_p(const R* s) {
+  return (R(1) / R(3) * (s[0] + s[1] + s[2]));
+}
+template <typename R>
+MPM_HD R sq(R x) {
+  return x * x;
+}
+template <typename R>
+MPM_HD R mu_j2(const R* s) {
+  return (sq(s[0] - s[1]) + sq(s[1] - s[2]) + sq(s[0] - s[2])) / R(6) + sq(s[3]) + sq(s[4]) +
          sq(s[5]);
 }
-MPM_HD double mu_j3(const double* s) {
-  const double p = mu_p(s);
-  const double d0 = s[0] - p, d1 = s[1] - p, d2 = s[2] - p;
+template <typename R>
+MPM_HD R mu_j3(const R* s) {
+  const R p = mu_p(s);
+  const R d0 = s[0] - p, d1 = s[1] - p, d2 = s[2] - p;
   return (d0 * d1 * d2) - (d2 * sq(s[3])) +
-         ((2 * s[3] * s[4] * s[5]) - (d0 * sq(s[4])) - (d1 * sq(s[5])));
+         ((R(2) * s[3] * s[4] * s[5]) - (d0 * sq(s[4])) - (d1 * sq(s[5])));
 }
 
-struct Invariants {
-  double eps, rho, theta;
+// sin and cos of an FP64 angle in one evaluation
+MPM_HD void sin_cos(double x, double* sn, double* cs) {
+#ifdef __CUDA_ARCH__
+  sincos(x, sn, cs);
+#else
+  *sn = std::sin(x);
+  *cs = std::cos(x);
+#endif
+}
+
+// Trigonometric values of the Lode angle theta of one invariant evaluation:
+// cos, sin of theta, theta + pi/3 and theta - 4 pi/3 all follow from one
+// sin/cos evaluation of theta by the angle-addition formulas.
+template <typename R>
+struct LodeTrig {
+  R ct, st;    // cos theta, sin theta
+  R sp3, cp3;  // sin (theta + pi/3), cos (theta + pi/3)
+  R cm43;      // cos (theta - 4 pi/3)
+};
+// Friction and dilation angle functions of one return (fixed during a
+// return: softening moves phi and psi only before the predictor).
+template <typename R>
+struct FrictionTrig {
+  R sphi, cphi, tphi, tpsi;
 };
 
-// mohr_coulomb.tcc:124-134 with lode_angle (material_utility.tcc:65-81)
-MPM_HD void mc_invariants(const double* s, double* sv) {
-  const double j2 = mu_j2(s);
-  const double j3 = mu_j3(s);
-  sv[SV_EPS] = mu_p(s) * sqrt(3.);
+template <typename R>
+MPM_HD FrictionTrig<R> friction_trig(const MaterialT<R>& m, const R* sv) {
+  FrictionTrig<R> t;
+  if (sv[SV_PHI] == m.phi_peak && sv[SV_PSI] == m.psi_peak) {
+    t.sphi = m.sin_phi;
+    t.cphi = m.cos_phi;
+    t.tphi = m.tan_phi;
+    t.tpsi = m.tan_psi;
+  } else {
+    t.sphi = sin(sv[SV_PHI]);
+    t.cphi = cos(sv[SV_PHI]);
+    t.tphi = tan(sv[SV_PHI]);
+    t.tpsi = tan(sv[SV_PSI]);
+  }
+  return t;
+}
+
+// mohr_coulomb.tcc:124-134 with lode_angle (material_utility.tcc:65-81).
+// Evaluated in FP64 for every working precision R: the Lode angle is acos of
+// a ratio that reaches +-1 on triaxial stress paths (a geostatic K0 state is
+// one), where acos turns a rounding error e of the ratio into an angle error
+// of about sqrt(2e) -- 5e-4 rad from FP32 rounding, which moves the returned
+// stress by 1e-4 of its magnitude.
+template <typename R>
+MPM_HD void mc_invariants(const R* s, R* sv, LodeTrig<R>& lt) {
+  const double d[6] = {double(s[0]), double(s[1]), double(s[2]),
+                       double(s[3]), double(s[4]), double(s[5])};
+  const double j2 = mu_j2(d);
+  const double j3 = mu_j3(d);
+  sv[SV_EPS] = R(mu_p(d) * sqrt(3.0));
   double v = 0.0;
-  if (fabs(j2) > kDblEps) v = (3. * sqrt(3.) / 2.) * (j3 / pow(j2, 1.5));
+  if (fabs(j2) > kDblEps) v = (3.0 * sqrt(3.0) / 2.0) * (j3 / (j2 * sqrt(j2)));
   if (v > 1.0) v = 1.0;
   if (v < -1.0) v = -1.0;
-  sv[SV_THETA] = (1. / 3.) * acos(v);
-  sv[SV_RHO] = sqrt(2. * j2);
+  const double theta = (1.0 / 3.0) * acos(v);
+  sv[SV_THETA] = R(theta);
+  sv[SV_RHO] = R(sqrt(2.0 * j2));
+  double sn, cs;
+  sin_cos(theta, &sn, &cs);
+  const double h = 0.5, r3 = 0.86602540378443864676;  // cos, sin of pi/3
+  lt.ct = R(cs);
+  lt.st = R(sn);
+  lt.sp3 = R(sn * h + cs * r3);
+  lt.cp3 = R(cs * h - sn * r3);
+  lt.cm43 = R(-(cs * h) - sn * r3);
 }
 
 enum { MC_ELASTIC = 0, MC_SHEAR = 1, MC_TENSILE = 2, MC_SEPARATED = 3 };
 
 // mohr_coulomb.tcc:139-191
-MPM_HD int mc_yield_state(double* yf, const double* sv) {
-  const double Tolerance = -1E-1;
-  const double epsilon = sv[SV_EPS], rho = sv[SV_RHO], theta = sv[SV_THETA];
-  const double phi = sv[SV_PHI], cohesion = sv[SV_COH], tension_cutoff = sv[SV_TC];
-  yf[0] = sqrt(2. / 3.) * cos(theta) * rho + epsilon / sqrt(3.) - tension_cutoff;
-  yf[1] = sqrt(1.5) * rho *
-              ((sin(theta + kPiD / 3.) / (sqrt(3.) * cos(phi))) +
-               (cos(theta + kPiD / 3.) * tan(phi) / 3.)) +
-          (epsilon / sqrt(3.)) * tan(phi) - cohesion;
+template <typename R>
+MPM_HD int mc_yield_state(R* yf, const R* sv, const LodeTrig<R>& lt, const FrictionTrig<R>& ft) {
+  const R Tolerance = R(-1E-1);
+  const R epsilon = sv[SV_EPS], rho = sv[SV_RHO];
+  const R cohesion = sv[SV_COH], tension_cutoff = sv[SV_TC];
+  yf[0] = sqrt(R(2) / R(3)) * lt.ct * rho + epsilon / sqrt(R(3)) - tension_cutoff;
+  yf[1] = sqrt(R(1.5)) * rho * ((lt.sp3 / (sqrt(R(3)) * ft.cphi)) + (lt.cp3 * ft.tphi / R(3))) +
+          (epsilon / sqrt(R(3))) * ft.tphi - cohesion;
   int yield_type = MC_ELASTIC;
   if (yf[0] > Tolerance && yf[1] > Tolerance) {
-    const double n_phi = (1. + sin(phi)) / (1. - sin(phi));
-    const double sigma_p = tension_cutoff * n_phi - 2. * cohesion * sqrt(n_phi);
-    const double alpha_p = sqrt(1. + n_phi * n_phi) + n_phi;
-    const double h = yf[0] + alpha_p * (sqrt(2. / 3.) * cos(theta - 4. * kPiD / 3.) * rho +
-                                        epsilon / sqrt(3.) - sigma_p);
-    yield_type = (h > kDblEps) ? MC_TENSILE : MC_SHEAR;
+    const R n_phi = (R(1) + ft.sphi) / (R(1) - ft.sphi);
+    const R sigma_p = tension_cutoff * n_phi - R(2) * cohesion * sqrt(n_phi);
+    const R alpha_p = sqrt(R(1) + n_phi * n_phi) + n_phi;
+    const R h = yf[0] + alpha_p * (sqrt(R(2) / R(3)) * lt.cm43 * rho + epsilon / sqrt(R(3)) - sigma_p);
+    yield_type = (h > dbl_eps<R>()) ? MC_TENSILE : MC_SHEAR;
   }
   if (yf[0] < Tolerance && yf[1] > Tolerance) yield_type = MC_SHEAR;
   if (yf[0] > Tolerance && yf[1] < Tolerance) yield_type = MC_TENSILE;
   return yield_type;
 }
 
-// mohr_coulomb.tcc:195-344 (dF/dsigma, dP/dsigma, dP/dq, softening)
-MPM_HD void mc_df_dp(const MaterialParams& m, int yield_type, const double* sv, const double* s,
-                     double* df, double* dp, double* dp_dq, double* softening) {
-  const double rho = sv[SV_RHO], theta = sv[SV_THETA];
-  const double phi = sv[SV_PHI], psi = sv[SV_PSI], tension_cutoff = sv[SV_TC];
-  const double pdstrain = sv[SV_PD];
-  double df_depsilon, df_drho, df_dtheta;
+// mohr_coulomb.tcc:195-344 (dF/dsigma, dP/dsigma, dP/dq, softening).  pdstrain
+// is passed separately (it is kept in FP64 on every path).
+template <typename R>
+MPM_HD void mc_df_dp(const MaterialT<R>& m, int yield_type, const R* sv, const LodeTrig<R>& lt,
+                     const FrictionTrig<R>& ft, R pdstrain, const R* s, R* df, R* dp, R* dp_dq,
+                     R* softening) {
+  const R eps = dbl_eps<R>();
+  const R rho = sv[SV_RHO];
+  const R phi = sv[SV_PHI], tension_cutoff = sv[SV_TC];
+  const R ct = lt.ct, st = lt.st;
+  R df_depsilon, df_drho, df_dtheta;
   if (yield_type == MC_TENSILE) {
-    df_depsilon = 1. / sqrt(3.);
-    df_drho = sqrt(2. / 3.) * cos(theta);
-    df_dtheta = -sqrt(2. / 3.) * rho * sin(theta);
+    df_depsilon = R(1) / sqrt(R(3));
+    df_drho = sqrt(R(2) / R(3)) * ct;
+    df_dtheta = -sqrt(R(2) / R(3)) * rho * st;
   } else {
-    df_depsilon = tan(phi) / sqrt(3.);
-    df_drho = sqrt(1.5) * ((sin(theta + kPiD / 3.) / (sqrt(3.) * cos(phi))) +
-                           (cos(theta + kPiD / 3.) * tan(phi) / 3.));
-    df_dtheta = sqrt(1.5) * rho *
-                ((cos(theta + kPiD / 3.) / (sqrt(3.) * cos(phi))) -
-                 (sin(theta + kPiD / 3.) * tan(phi) / 3.));
+    df_depsilon = ft.tphi / sqrt(R(3));
+    df_drho = sqrt(R(1.5)) * ((lt.sp3 / (sqrt(R(3)) * ft.cphi)) + (lt.cp3 * ft.tphi / R(3)));
+    df_dtheta = sqrt(R(1.5)) * rho * ((lt.cp3 / (sqrt(R(3)) * ft.cphi)) - (lt.sp3 * ft.tphi / R(3)));
   }
   // dEpsilon/dsigma = dp/dsigma * sqrt(3); dRho/dsigma = dq/dsigma * sqrt(2/3)
-  const double deps_ds = 1. / 3. * sqrt(3.);
-  const double j2 = mu_j2(s);
-  const double q = sqrt(3 * j2);
-  const double pm = mu_p(s);
-  double dev[6] = {s[0] - pm, s[1] - pm, s[2] - pm, s[3], s[4], s[5]};
-  double drho_ds[6] = {0, 0, 0, 0, 0, 0};
-  if (fabs(q) > kDblEps) {
-    drho_ds[0] = 3. / (2. * q) * dev[0];
-    drho_ds[1] = 3. / (2. * q) * dev[1];
-    drho_ds[2] = 3. / (2. * q) * dev[2];
-    drho_ds[3] = 3. / q * dev[3];
-    drho_ds[4] = 3. / q * dev[4];
-    drho_ds[5] = 3. / q * dev[5];
+  const R deps_ds = R(1) / R(3) * sqrt(R(3));
+  const R j2 = mu_j2(s);
+  const R q = sqrt(R(3) * j2);
+  const R pm = mu_p(s);
+  const R dev[6] = {s[0] - pm, s[1] - pm, s[2] - pm, s[3], s[4], s[5]};
+  R drho_ds[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+  if (fabs(q) > eps) {
+    drho_ds[0] = R(3) / (R(2) * q) * dev[0];
+    drho_ds[1] = R(3) / (R(2) * q) * dev[1];
+    drho_ds[2] = R(3) / (R(2) * q) * dev[2];
+    drho_ds[3] = R(3) / q * dev[3];
+    drho_ds[4] = R(3) / q * dev[4];
+    drho_ds[5] = R(3) / q * dev[5];
   }
 #pragma unroll
-  for (int i = 0; i < 6; ++i) drho_ds[i] *= sqrt(2. / 3.);
-  // dtheta/dsigma (material_utility.tcc:166-200)
-  double dtheta_ds[6];
+  for (int i = 0; i < 6; ++i) drho_ds[i] *= sqrt(R(2) / R(3));
+  // dtheta/dsigma (material_utility.tcc:166-200), in FP64 for every R for
+  // the reason given at mc_invariants (1 - r^2 vanishes on triaxial paths)
+  R dtheta_ds[6];
   {
-    const double j3 = mu_j3(s);
-    const double dj2[6] = {dev[0], dev[1], dev[2], dev[3] * 2.0, dev[4] * 2.0, dev[5] * 2.0};
-    const double dev1[3] = {dev[0], dev[3], dev[5]};
-    const double dev2[3] = {dev[3], dev[1], dev[4]};
-    const double dev3[3] = {dev[5], dev[4], dev[2]};
+    const double sd[6] = {double(s[0]), double(s[1]), double(s[2]),
+                          double(s[3]), double(s[4]), double(s[5])};
+    const double j2d = mu_j2(sd);
+    const double pmd = mu_p(sd);
+    const double dv[6] = {sd[0] - pmd, sd[1] - pmd, sd[2] - pmd, sd[3], sd[4], sd[5]};
+    const double j3 = mu_j3(sd);
+    const double dj2[6] = {dv[0], dv[1], dv[2], dv[3] * 2.0, dv[4] * 2.0, dv[5] * 2.0};
+    const double dev1[3] = {dv[0], dv[3], dv[5]};
+    const double dev2[3] = {dv[3], dv[1], dv[4]};
+    const double dev3[3] = {dv[5], dv[4], dv[2]};
     auto dot3 = [](const double* a, const double* b) {
       return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
     };
-    const double dj3[6] = {dot3(dev1, dev1) - (2. / 3.) * j2, dot3(dev2, dev2) - (2. / 3.) * j2,
-                           dot3(dev3, dev3) - (2. / 3.) * j2, 2.0 * dot3(dev1, dev2),
-                           2.0 * dot3(dev2, dev3),           2.0 * dot3(dev1, dev3)};
+    const double dj3[6] = {dot3(dev1, dev1) - (2.0 / 3.0) * j2d,
+                           dot3(dev2, dev2) - (2.0 / 3.0) * j2d,
+                           dot3(dev3, dev3) - (2.0 / 3.0) * j2d,
+                           2.0 * dot3(dev1, dev2),
+                           2.0 * dot3(dev2, dev3),
+                           2.0 * dot3(dev1, dev3)};
     double dr_dj2 = -9.0 / 4.0 * sqrt(3.0) * j3;
     double dr_dj3 = 3.0 / 2.0 * sqrt(3.0);
     double dtheta_dr = -1.0 / 3.0;
-    if (fabs(j2) > kDblEps) {
-      const double r = j3 / 2.0 * pow(j2 / 3.0, -1.5);
-      dr_dj2 *= pow(j2, -2.5);
-      dr_dj3 *= pow(j2, -1.5);
-      const double factor = (fabs(1 - r * r) < kDblEps) ? kDblEps : fabs(1 - r * r);
+    if (fabs(j2d) > kDblEps) {
+      // j2^-1.5 and j2^-2.5 from one square root
+      const double p15 = 1.0 / (j2d * sqrt(j2d));
+      const double r = j3 / 2.0 * (3.0 * sqrt(3.0)) * p15;
+      dr_dj2 *= p15 / j2d;
+      dr_dj3 *= p15;
+      const double factor = (fabs(1.0 - r * r) < kDblEps) ? kDblEps : fabs(1.0 - r * r);
       dtheta_dr = -1.0 / (3.0 * sqrt(factor));
     }
 #pragma unroll
-    for (int i = 0; i < 6; ++i) dtheta_ds[i] = dtheta_dr * ((dr_dj2 * dj2[i]) + (dr_dj3 * dj3[i]));
+    for (int i = 0; i < 6; ++i) dtheta_ds[i] = R(dtheta_dr * ((dr_dj2 * dj2[i]) + (dr_dj3 * dj3[i])));
   }
 #pragma unroll
   for (int i = 0; i < 6; ++i)
-    df[i] = ((df_depsilon * (i < 3 ? deps_ds : 0.)) + (df_drho * drho_ds[i])) +
+    df[i] = ((df_depsilon * (i < 3 ? deps_ds : R(0))) + (df_drho * drho_ds[i])) +
             (df_dtheta * dtheta_ds[i]);
   if (yield_type == MC_TENSILE) {
-    const double et_value = 0.6;
-    const double xit = 0.1;
-    const double ct = cos(theta), st = sin(theta);
-    double sqpart = 4. * (1 - et_value * et_value) * ct * ct + 5. * et_value * et_value -
-                    4. * et_value;
-    if (sqpart < kDblEps) sqpart = 1.E-5;
-    double rt_den = 2. * (1 - et_value * et_value) * ct + (2. * et_value - 1) * sqrt(sqpart);
-    const double rt_num =
-        4. * (1 - et_value * et_value) * ct * ct + (2. * et_value - 1) * (2. * et_value - 1);
-    if (fabs(rt_den) < kDblEps) rt_den = 1.E-5;
-    const double rt = rt_num / (3. * rt_den);
-    const double den = check_low(
-        sqrt(xit * xit * tension_cutoff * tension_cutoff + 1.5 * rt * rt * rho * rho));
-    const double dp_drt = 1.5 * rho * rho * rt / den;
-    const double dp_drho = 1.5 * rho * rt * rt / den;
-    const double dp_depsilon = 1. / sqrt(3.);
-    const double drtden_dtheta =
-        -2. * (1 - et_value * et_value) * st -
-        (2. * et_value - 1) * 4. * (1 - et_value * et_value) * ct * st /
-            sqrt(4. * (1 - et_value * et_value) * ct * ct + 5. * et_value * et_value -
-                 4. * et_value);
-    const double drtnum_dtheta = -8. * (1 - et_value * et_value) * ct * st;
-    const double drt_dtheta =
-        (drtnum_dtheta * rt_den - drtden_dtheta * rt_num) / (3. * rt_den * rt_den);
+    const R et_value = R(0.6);
+    const R xit = R(0.1);
+    R sqpart = R(4) * (R(1) - et_value * et_value) * ct * ct + R(5) * et_value * et_value -
+               R(4) * et_value;
+    if (sqpart < eps) sqpart = R(1.E-5);
+    R rt_den = R(2) * (R(1) - et_value * et_value) * ct + (R(2) * et_value - R(1)) * sqrt(sqpart);
+    const R rt_num = R(4) * (R(1) - et_value * et_value) * ct * ct +
+                     (R(2) * et_value - R(1)) * (R(2) * et_value - R(1));
+    if (fabs(rt_den) < eps) rt_den = R(1.E-5);
+    const R rt = rt_num / (R(3) * rt_den);
+    const R den = check_low(
+        sqrt(xit * xit * tension_cutoff * tension_cutoff + R(1.5) * rt * rt * rho * rho));
+    const R dp_drt = R(1.5) * rho * rho * rt / den;
+    const R dp_drho = R(1.5) * rho * rt * rt / den;
+    const R dp_depsilon = R(1) / sqrt(R(3));
+    const R drtden_dtheta =
+        R(-2) * (R(1) - et_value * et_value) * st -
+        (R(2) * et_value - R(1)) * R(4) * (R(1) - et_value * et_value) * ct * st /
+            sqrt(R(4) * (R(1) - et_value * et_value) * ct * ct + R(5) * et_value * et_value -
+                 R(4) * et_value);
+    const R drtnum_dtheta = R(-8) * (R(1) - et_value * et_value) * ct * st;
+    const R drt_dtheta =
+        (drtnum_dtheta * rt_den - drtden_dtheta * rt_num) / (R(3) * rt_den * rt_den);
 #pragma unroll
     for (int i = 0; i < 6; ++i)
-      dp[i] = ((dp_depsilon * (i < 3 ? deps_ds : 0.)) + (dp_drho * drho_ds[i])) +
+      dp[i] = ((dp_depsilon * (i < 3 ? deps_ds : R(0))) + (dp_drho * drho_ds[i])) +
               (dp_drt * drt_dtheta * dtheta_ds[i]);
-    *dp_dq = dp_drho * sqrt(2. / 3.);
+    *dp_dq = dp_drho * sqrt(R(2) / R(3));
   } else {
-    const double sphi = sin(phi), cphi = cos(phi);
-    const double ct = cos(theta), st = sin(theta);
-    const double r_mc = (3. - sphi) / (6 * cphi);
-    double e_val = (3. - sphi) / (3. + sphi);
-    if (e_val <= 0.5) e_val = 0.5 + 1.E-10;
-    if (e_val > 1.) e_val = 1.;
-    double sqpart = (4. * (1 - e_val * e_val) * sq(ct)) + (5 * e_val * e_val) - (4. * e_val);
-    if (sqpart < kDblEps) sqpart = 1.E-5;
-    double mm = (2. * (1 - e_val * e_val) * ct) + ((2. * e_val - 1) * sqrt(sqpart));
-    if (fabs(mm) < kDblEps) mm = 1.E-5;
-    const double l = (4. * (1. - e_val * e_val) * sq(ct)) + sq(2. * e_val - 1.);
-    const double r_mw = (l / mm) * r_mc;
-    const double xi = 0.1;
-    double omega = sq(xi * m.c_peak * tan(psi)) + sq(r_mw * sqrt(1.5) * rho);
-    if (omega < kDblEps) omega = 1.E-5;
-    const double dl_dtheta = -8. * (1. - e_val * e_val) * ct * st;
-    const double dm_dtheta =
-        (-2. * (1. - e_val * e_val) * st) + (0.5 * (2. * e_val - 1.) * dl_dtheta) / sqrt(sqpart);
-    const double drmw_dtheta = ((mm * dl_dtheta) - (l * dm_dtheta)) / (mm * mm);
-    const double dp_depsilon = tan(psi) / sqrt(3.);
-    const double dp_drho = 3. * rho * r_mw * r_mw / (2. * sqrt(omega));
-    const double dp_dtheta = (3. * rho * rho * r_mw * r_mc * drmw_dtheta) / (2. * sqrt(omega));
+    const R sphi = ft.sphi, cphi = ft.cphi;
+    const R r_mc = (R(3) - sphi) / (R(6) * cphi);
+    R e_val = (R(3) - sphi) / (R(3) + sphi);
+    if (e_val <= R(0.5)) e_val = R(0.5) + R(1.E-10);
+    if (e_val > R(1)) e_val = R(1);
+    R sqpart = (R(4) * (R(1) - e_val * e_val) * sq(ct)) + (R(5) * e_val * e_val) - (R(4) * e_val);
+    if (sqpart < eps) sqpart = R(1.E-5);
+    R mm = (R(2) * (R(1) - e_val * e_val) * ct) + ((R(2) * e_val - R(1)) * sqrt(sqpart));
+    if (fabs(mm) < eps) mm = R(1.E-5);
+    const R l = (R(4) * (R(1) - e_val * e_val) * sq(ct)) + sq(R(2) * e_val - R(1));
+    const R r_mw = (l / mm) * r_mc;
+    const R xi = R(0.1);
+    R omega = sq(xi * m.c_peak * ft.tpsi) + sq(r_mw * sqrt(R(1.5)) * rho);
+    if (omega < eps) omega = R(1.E-5);
+    const R dl_dtheta = R(-8) * (R(1) - e_val * e_val) * ct * st;
+    const R dm_dtheta = (R(-2) * (R(1) - e_val * e_val) * st) +
+                        (R(0.5) * (R(2) * e_val - R(1)) * dl_dtheta) / sqrt(sqpart);
+    const R drmw_dtheta = ((mm * dl_dtheta) - (l * dm_dtheta)) / (mm * mm);
+    const R dp_depsilon = ft.tpsi / sqrt(R(3));
+    const R dp_drho = R(3) * rho * r_mw * r_mw / (R(2) * sqrt(omega));
+    const R dp_dtheta = (R(3) * rho * rho * r_mw * r_mc * drmw_dtheta) / (R(2) * sqrt(omega));
 #pragma unroll
     for (int i = 0; i < 6; ++i)
-      dp[i] = ((dp_depsilon * (i < 3 ? deps_ds : 0.)) + (dp_drho * drho_ds[i])) +
+      dp[i] = ((dp_depsilon * (i < 3 ? deps_ds : R(0))) + (dp_drho * drho_ds[i])) +
               (dp_dtheta * dtheta_ds[i]);
-    *dp_dq = dp_drho * sqrt(2. / 3.);
+    *dp_dq = dp_drho * sqrt(R(2) / R(3));
   }
-  *softening = 0.;
+  *softening = R(0);
   if (m.softening && pdstrain > m.pd_peak && pdstrain < m.pd_res) {
-    const double dphi_dpstrain = (m.phi_res - m.phi_peak) / (m.pd_res - m.pd_peak);
-    const double dc_dpstrain = (m.c_res - m.c_peak) / (m.pd_res - m.pd_peak);
-    const double df_dphi =
-        sqrt(1.5) * rho *
-            ((sin(phi) * sin(theta + kPiD / 3.) / (sqrt(3.) * cos(phi) * cos(phi))) +
-             (cos(theta + kPiD / 3.) / (3. * cos(phi) * cos(phi)))) +
-        (mu_p(s) / (cos(phi) * cos(phi)));
-    const double df_dc = -1.;
-    *softening = (-1.) * ((df_dphi * dphi_dpstrain) + (df_dc * dc_dpstrain)) * (*dp_dq);
+    const R dphi_dpstrain = (m.phi_res - m.phi_peak) / (m.pd_res - m.pd_peak);
+    const R dc_dpstrain = (m.c_res - m.c_peak) / (m.pd_res - m.pd_peak);
+    const R df_dphi =
+        sqrt(R(1.5)) * rho *
+            ((ft.sphi * lt.sp3 / (sqrt(R(3)) * ft.cphi * ft.cphi)) +
+             (lt.cp3 / (R(3) * ft.cphi * ft.cphi))) +
+        (mu_p(s) / (ft.cphi * ft.cphi));
+    const R df_dc = R(-1);
+    *softening = R(-1) * ((df_dphi * dphi_dpstrain) + (df_dc * dc_dpstrain)) * (*dp_dq);
   }
+  (void)phi;
+}
+
+template <typename R>
+MPM_HD R huge_value() {
+  return R(1.7976931348623157e308);
+}
+template <>
+MPM_HD float huge_value<float>() {
+  return 3.402823466e38f;
 }
 
 // MohrCoulomb<Tdim>::compute_stress (mohr_coulomb.tcc:348-513), stress_rate
-// None (infinitesimal_elasto_plastic.tcc:2-25).  sv holds the nine state
-// variables in the reference order.
-MPM_HD void mc_compute_stress(const MaterialParams& m, const double* stress,
-                              const double* dstrain, double density, double* sv, double* out) {
-  const double critical_density = m.min_packing * m.grain_density;
-  const double pdstrain = sv[SV_PD];
+// None (infinitesimal_elasto_plastic.tcc:2-25).  sv holds the state variables
+// in the reference order; the plastic deviatoric strain (slot SV_PD) is kept in
+// PD (double on every path).  Returns false when a return iteration left the
+// state non-finite (the caller of the mixed path then redoes the point in FP64).
+template <typename R, typename PD>
+MPM_HD bool mc_compute_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R density,
+                              R* sv, PD& pdstrain_io, R* out) {
+  const R critical_density = m.min_packing * m.grain_density;
+  const R pdstrain = R(pdstrain_io);
   if (m.softening && pdstrain > m.pd_peak) {
     if (pdstrain < m.pd_res) {
       sv[SV_PHI] = m.phi_res + ((m.phi_peak - m.phi_res) * (pdstrain - m.pd_res) /
@@ -509,61 +644,64 @@ MPM_HD void mc_compute_stress(const MaterialParams& m, const double* stress,
       sv[SV_PSI] = m.psi_res;
       sv[SV_COH] = m.c_res;
     }
-    const double apex = sv[SV_COH] / tan(sv[SV_PHI]);
+    const R apex = sv[SV_COH] / tan(sv[SV_PHI]);
     if (sv[SV_TC] > apex) sv[SV_TC] = check_low(apex);
   }
-  sv[SV_YIELD] = 0;
-  double trial[6];
+  sv[SV_YIELD] = R(0);
+  R trial[6];
   {
-    double t[6];
+    R t[6];
     de_mul(m, dstrain, t);
 #pragma unroll
     for (int i = 0; i < 6; ++i) trial[i] = stress[i] + t[i];
   }
   if (density <= critical_density) {
-    sv[SV_PD] += sqrt(3 * mu_j2(trial)) / 3.0 / m.shear;
-    sv[SV_YIELD] = 3;
+    pdstrain_io += PD(sqrt(R(3) * mu_j2(trial)) / R(3) / m.shear);
+    sv[SV_YIELD] = R(3);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) out[i] = 0.;
-    return;
+    for (int i = 0; i < 6; ++i) out[i] = R(0);
+    return true;
   }
-  mc_invariants(trial, sv);
-  double yf_trial[2];
-  int yt_trial = mc_yield_state(yf_trial, sv);
+  const FrictionTrig<R> ft = friction_trig(m, sv);
+  LodeTrig<R> lt;
+  mc_invariants(trial, sv, lt);
+  R yf_trial[2];
+  int yt_trial = mc_yield_state(yf_trial, sv, lt, ft);
   if (yt_trial == MC_ELASTIC) {
-    sv[SV_YIELD] = 0;
+    sv[SV_YIELD] = R(0);
 #pragma unroll
     for (int i = 0; i < 6; ++i) out[i] = trial[i];
-    return;
+    return true;
   }
-  const double Tolerance = 1E-1;
-  double softening_trial = 0., dp_dq_trial = 0.;
-  double df_trial[6], dp_trial[6];
-  mc_df_dp(m, yt_trial, sv, trial, df_trial, dp_trial, &dp_dq_trial, &softening_trial);
-  double yield_trial = 0.;
+  const R Tolerance = R(1E-1);
+  R softening_trial = R(0), dp_dq_trial = R(0);
+  R df_trial[6], dp_trial[6];
+  mc_df_dp(m, yt_trial, sv, lt, ft, pdstrain, trial, df_trial, dp_trial, &dp_dq_trial,
+           &softening_trial);
+  R yield_trial = R(0);
   if (yt_trial == MC_TENSILE) {
-    sv[SV_YIELD] = 2;
+    sv[SV_YIELD] = R(2);
     yield_trial = yf_trial[0];
   }
   if (yt_trial == MC_SHEAR) {
-    sv[SV_YIELD] = 1;
+    sv[SV_YIELD] = R(1);
     yield_trial = yf_trial[1];
   }
-  double lambda_trial = yield_trial / (row_de_dot(m, df_trial, dp_trial) + softening_trial);
-  mc_invariants(stress, sv);
-  double yf[2];
-  const int yt = mc_yield_state(yf, sv);
-  double yield = 1.7976931348623157e308;
+  R lambda_trial = yield_trial / (row_de_dot(m, df_trial, dp_trial) + softening_trial);
+  mc_invariants(stress, sv, lt);
+  R yf[2];
+  const int yt = mc_yield_state(yf, sv, lt, ft);
+  R yield = huge_value<R>();
   if (yt == MC_TENSILE) yield = yf[0];
   if (yt == MC_SHEAR) yield = yf[1];
-  double softening = 0., dp_dq = 0.;
-  double df[6], dp[6];
-  mc_df_dp(m, yt, sv, stress, df, dp, &dp_dq, &softening);
-  const double lambda = row_de_dot(m, df, dstrain) / (row_de_dot(m, df, dp) + softening);
-  double upd[6];
+  R softening = R(0), dp_dq = R(0);
+  R df[6], dp[6];
+  mc_df_dp(m, yt, sv, lt, ft, pdstrain, stress, df, dp, &dp_dq, &softening);
+  const R lambda = row_de_dot(m, df, dstrain) / (row_de_dot(m, df, dp) + softening);
+  R upd[6];
 #pragma unroll
   for (int i = 0; i < 6; ++i) upd[i] = trial[i];
-  double dpdstrain;
+  R dpdstrain;
   if (fabs(yield) < Tolerance) {
     sub_lambda_de(m, lambda, dp, upd);
     dpdstrain = lambda * dp_dq;
@@ -572,34 +710,52 @@ MPM_HD void mc_compute_stress(const MaterialParams& m, const double* stress,
     dpdstrain = lambda_trial * dp_dq_trial;
   }
   for (int itr = 0; itr < 100; ++itr) {
-    mc_invariants(upd, sv);
-    yt_trial = mc_yield_state(yf_trial, sv);
+    mc_invariants(upd, sv, lt);
+    yt_trial = mc_yield_state(yf_trial, sv, lt, ft);
     if (yf_trial[0] < Tolerance && yf_trial[1] < Tolerance) break;
-    mc_df_dp(m, yt_trial, sv, upd, df_trial, dp_trial, &dp_dq_trial, &softening_trial);
+    mc_df_dp(m, yt_trial, sv, lt, ft, pdstrain, upd, df_trial, dp_trial, &dp_dq_trial,
+             &softening_trial);
     if (yt_trial == MC_TENSILE) yield_trial = yf_trial[0];
     if (yt_trial == MC_SHEAR) yield_trial = yf_trial[1];
     lambda_trial = yield_trial / (row_de_dot(m, df_trial, dp_trial) + softening_trial);
     sub_lambda_de(m, lambda_trial, dp_trial, upd);
     dpdstrain += lambda_trial * dp_dq_trial;
   }
-  mc_invariants(upd, sv);
-  sv[SV_PD] += dpdstrain;
+  mc_invariants(upd, sv, lt);
+  pdstrain_io += PD(dpdstrain);
+  bool finite = true;
 #pragma unroll
-  for (int i = 0; i < 6; ++i) out[i] = upd[i];
+  for (int i = 0; i < 6; ++i) {
+    out[i] = upd[i];
+    finite = finite && (upd[i] - upd[i] == R(0));
+  }
+  return finite;
 }
 
 // Material<Tdim>::compute_stress dispatch (material.h:97-106)
+template <typename R, typename PD>
+MPM_HD bool material_compute_stress(const MaterialT<R>& m, const R* stress, const R* dstrain,
+                                    R density, R* sv, PD& pdstrain, R* out) {
+  if (m.type == 0) {
+    R t[6];
+    de_mul(m, dstrain, t);  // linear_elastic.tcc:73-94
+#pragma unroll
+    for (int i = 0; i < 6; ++i) out[i] = stress[i] + t[i];
+    return true;
+  }
+  return mc_compute_stress(m, stress, dstrain, density, sv, pdstrain, out);
+}
+
+// FP64 form used by the FP64 kernels: the state array holds pdstrain in SV_PD.
 MPM_HD void material_compute_stress(const MaterialParams& m, const double* stress,
                                     const double* dstrain, double density, double* sv,
                                     double* out) {
   if (m.type == 0) {
-    double t[6];
-    de_mul(m, dstrain, t);  // linear_elastic.tcc:73-94
-#pragma unroll
-    for (int i = 0; i < 6; ++i) out[i] = stress[i] + t[i];
-  } else {
-    mc_compute_stress(m, stress, dstrain, density, sv, out);
+    double pd = 0.;
+    material_compute_stress<double, double>(m, stress, dstrain, density, sv, pd, out);
+    return;
   }
+  material_compute_stress<double, double>(m, stress, dstrain, density, sv, sv[SV_PD], out);
 }
 
 // ---------------------------------------------------------------- node update

@@ -29,6 +29,28 @@ struct PF<2> {
   static constexpr int NS = 4, NE = 3, NFG = 4;
 };
 
+// Mixed precision: FP64 buffer [x (DIM), u (DIM), pdstrain] (DevState::pf
+// points at it, so x and u keep the FP64 offsets) and an FP32 buffer with
+// v, stress, strain, H = F - I, the initial volume and density, P = V/V0 - 1
+// (volume and density follow as V0 (1 + P) and rho0 / (1 + P)) and the mass.
+// Slowly varying quantities are stored as deviations so that FP32 keeps the
+// small per-step increments.
+template <int DIM>
+struct PDX {
+  static constexpr int X = 0, U = DIM, PDS = 2 * DIM, ND = 2 * DIM + 1;
+};
+template <int DIM>
+struct PM;
+template <>
+struct PM<3> {
+  static constexpr int V = 0, S = 3, E = 9, H = 15, V0 = 24, RHO0 = 25, JP = 26, MASS = 27, NF = 28;
+};
+template <>
+struct PM<2> {
+  static constexpr int V = 0, S = 2, E = 6, H = 9, V0 = 13, RHO0 = 14, JP = 15, MASS = 16, NF = 17;
+};
+constexpr int SVF_N = 8;  // MohrCoulomb state in FP32: SV_YIELD .. SV_THETA
+
 // node field offsets (units of nn doubles)
 template <int DIM>
 struct NF {
@@ -104,6 +126,14 @@ struct DevState {
   int32_t* lost = nullptr;       // [np] particles not found in cell or neighbours
   unsigned* nlost = nullptr;
   unsigned* err = nullptr;       // ErrorBits
+
+  // mixed precision (null on the FP64 path)
+  float* pm = nullptr;            // [PM::NF][np]
+  float* svf = nullptr;           // [SVF_N][np]
+  float* nfv = nullptr;           // [2 DIM][nn] nodal velocity, acceleration
+  float* partials_f = nullptr;    // [ncells][NV][1 + 3 DIM]
+  float* dndx_cf = nullptr;       // [ncells][NV][DIM]
+  const MaterialT<float>* mats_f = nullptr;
 
   const MaterialParams* mats = nullptr;
   const NodeBC* bcs = nullptr;

@@ -1,0 +1,170 @@
+// pod.cu -- packing of the device particle state into the reference's
+// PODParticle records (Particle::pod, particle.tcc:180-306; record layout
+// pod_particle.h:12-62 and the field table of pod_particle.cc) for the HDF5
+// particle table (Mesh::write_particles_hdf5, mesh.tcc:1573-1613).
+//
+// The record layout is the caller's: byte offset and size of each of the 74
+// fields, as the reference passes them to H5TBmake_table.  One thread writes
+// one field of one record, so consecutive threads write neighbouring bytes of
+// a record.
+#include <cuda_runtime.h>
+
+#include "mpm_kernels.h"
+#include "mpm_state.cuh"
+
+namespace mpm_b200 {
+namespace {
+
+template <int DIM, bool MIXED>
+__device__ __forceinline__ double pf_value(const DevState& s, int f, int c, int64_t p) {
+  // FP64 layout offset f + component c, read from whichever buffer holds it
+  const int64_t np = s.np;
+  if constexpr (!MIXED) {
+    return s.pf[(int64_t)(f + c) * np + p];
+  } else {
+    if (f == PF<DIM>::X) return s.pf[(int64_t)(PDX<DIM>::X + c) * np + p];
+    if (f == PF<DIM>::U) return s.pf[(int64_t)(PDX<DIM>::U + c) * np + p];
+    const float* m = s.pm;
+    if (f == PF<DIM>::V) return (double)m[(int64_t)(PM<DIM>::V + c) * np + p];
+    if (f == PF<DIM>::S) return (double)m[(int64_t)(PM<DIM>::S + c) * np + p];
+    if (f == PF<DIM>::E) return (double)m[(int64_t)(PM<DIM>::E + c) * np + p];
+    if (f == PF<DIM>::F) {
+      const bool diag = DIM == 2 ? (c == 0 || c == 3) : (c % 4 == 0);
+      return (double)m[(int64_t)(PM<DIM>::H + c) * np + p] + (diag ? 1.0 : 0.0);
+    }
+    const double jp = (double)m[(int64_t)PM<DIM>::JP * np + p];
+    if (f == PF<DIM>::VOL) return (double)m[(int64_t)PM<DIM>::V0 * np + p] * (1.0 + jp);
+    if (f == PF<DIM>::RHO) return (double)m[(int64_t)PM<DIM>::RHO0 * np + p] / (1.0 + jp);
+    return (double)m[(int64_t)PM<DIM>::MASS * np + p];  // MASS
+  }
+}
+
+template <int DIM, bool MIXED>
+__device__ __forceinline__ double svar_value(const DevState& s, int k, int64_t p) {
+  const int64_t np = s.np;
+  if constexpr (!MIXED) {
+    return s.sv[(int64_t)k * np + p];
+  } else {
+    if (k == SV_PD) return s.pf[(int64_t)PDX<DIM>::PDS * np + p];
+    return (double)s.svf[(int64_t)k * np + p];
+  }
+}
+
+// Value of field f (PODParticle order) of particle p; kind: 0 double,
+// 1 unsigned 64-bit, 2 unsigned 32-bit, 3 bool.
+template <int DIM, bool MIXED>
+__device__ void pod_field(const DevState& s, const PodAux& a, int f, int64_t p, double& dv,
+                          uint64_t& uv, int& kind) {
+  kind = 0;
+  dv = 0.0;
+  uv = 0;
+  const int64_t np = s.np;
+  auto vec3 = [&](int off, int c) { return c < DIM ? pf_value<DIM, MIXED>(s, off, c, p) : 0.0; };
+  if (f == 0) {  // id
+    kind = 1;
+    uv = a.id[p];
+  } else if (f == 1) {
+    dv = pf_value<DIM, MIXED>(s, PF<DIM>::MASS, 0, p);
+  } else if (f == 2) {
+    dv = pf_value<DIM, MIXED>(s, PF<DIM>::VOL, 0, p);
+  } else if (f == 3) {  // pressure: not a state variable of LinearElastic / MohrCoulomb
+    dv = 0.0;
+  } else if (f < 7) {
+    dv = vec3(PF<DIM>::X, f - 4);
+  } else if (f < 10) {
+    dv = vec3(PF<DIM>::U, f - 7);
+  } else if (f < 13) {
+    dv = a.nsize[(int64_t)(f - 10) * np + p];
+  } else if (f < 16) {
+    dv = vec3(PF<DIM>::V, f - 13);
+  } else if (f < 19) {
+    dv = a.acc[(int64_t)(f - 16) * np + p];
+  } else if (f < 25) {  // stress xx yy zz xy yz xz
+    const int k = f - 19;
+    dv = k < PF<DIM>::NS ? pf_value<DIM, MIXED>(s, PF<DIM>::S, k, p) : 0.0;
+  } else if (f < 31) {  // strain xx yy zz xy yz xz (2D stores xx yy xy)
+    const int k = f - 25;
+    if constexpr (DIM == 3) {
+      dv = pf_value<DIM, MIXED>(s, PF<3>::E, k, p);
+    } else {
+      dv = k == 0 ? pf_value<DIM, MIXED>(s, PF<2>::E, 0, p)
+                  : (k == 1 ? pf_value<DIM, MIXED>(s, PF<2>::E, 1, p)
+                            : (k == 3 ? pf_value<DIM, MIXED>(s, PF<2>::E, 2, p) : 0.0));
+    }
+  } else if (f < 40) {  // deformation gradient, row major 3x3
+    const int r = (f - 31) / 3, c = (f - 31) % 3;
+    if constexpr (DIM == 3) {
+      dv = pf_value<DIM, MIXED>(s, PF<3>::F, r * 3 + c, p);
+    } else {
+      dv = (r < 2 && c < 2) ? pf_value<DIM, MIXED>(s, PF<2>::F, r * 2 + c, p)
+                            : (r == 2 && c == 2 ? 1.0 : 0.0);
+    }
+  } else if (f == 40) {  // initialise_mapping_matrix: no affine velocity update
+    kind = 3;
+  } else if (f < 50) {  // mapping matrix
+    dv = 0.0;
+  } else if (f == 50) {  // status
+    kind = 3;
+    uv = s.cell[p] >= 0 ? 1 : 0;
+  } else if (f == 51) {  // cell id
+    kind = 1;
+    uv = (uint64_t)(int64_t)s.cell[p];
+  } else if (f == 52) {
+    kind = 2;
+    uv = (uint32_t)a.material_id[s.mat[p]];
+  } else if (f == 53) {
+    kind = 2;
+    uv = a.nstate[s.mat[p]];
+  } else {  // svars[0..19]
+    const int k = f - 54;
+    dv = (k < SV_N && a.nstate[s.mat[p]] > 0) ? svar_value<DIM, MIXED>(s, k, p) : 0.0;
+  }
+}
+
+template <int DIM, bool MIXED>
+__global__ void __launch_bounds__(256) k_pod_pack(DevState s, PodAux a, PodLayout L,
+                                                  const int32_t* list, int64_t count,
+                                                  uint8_t* out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count * POD_NFIELDS) return;
+  const int64_t i = t / POD_NFIELDS;
+  const int f = (int)(t % POD_NFIELDS);
+  const int64_t p = list[i];
+  double dv;
+  uint64_t uv;
+  int kind;
+  pod_field<DIM, MIXED>(s, a, f, p, dv, uv, kind);
+  uint8_t* dst = out + i * L.record_size + L.offset[f];
+  // sizes and alignments were checked on the host: 8-byte fields at 8-byte
+  // offsets, 4-byte at 4-byte, records a multiple of 8 bytes
+  if (kind == 0)
+    *reinterpret_cast<double*>(dst) = dv;
+  else if (kind == 1)
+    *reinterpret_cast<uint64_t*>(dst) = uv;
+  else if (kind == 2)
+    *reinterpret_cast<uint32_t*>(dst) = (uint32_t)uv;
+  else
+    *dst = (uint8_t)(uv ? 1 : 0);
+}
+
+}  // namespace
+
+void launch_pod_pack(int dim, bool mixed, const DevState& s, const PodAux& a, const PodLayout& L,
+                     const int32_t* list, int64_t count, uint8_t* out, cudaStream_t st) {
+  if (count <= 0) return;
+  const int64_t threads = count * POD_NFIELDS;
+  const unsigned blocks = (unsigned)((threads + 255) / 256);
+  if (dim == 2) {
+    if (mixed)
+      k_pod_pack<2, true><<<blocks, 256, 0, st>>>(s, a, L, list, count, out);
+    else
+      k_pod_pack<2, false><<<blocks, 256, 0, st>>>(s, a, L, list, count, out);
+  } else {
+    if (mixed)
+      k_pod_pack<3, true><<<blocks, 256, 0, st>>>(s, a, L, list, count, out);
+    else
+      k_pod_pack<3, false><<<blocks, 256, 0, st>>>(s, a, L, list, count, out);
+  }
+}
+
+}  // namespace mpm_b200

@@ -221,8 +221,9 @@ def config_b(block=(100, 100, 50)):
     return column_3d(block=block)
 
 
-def build_solver(prob, solver_cls=None, **overrides):
-    """Create and initialise a GPU solver for ``prob``."""
+def build_solver(prob, solver_cls=None, with_particles=True, **overrides):
+    """Create and initialise a GPU solver for ``prob`` (mesh, materials and
+    constraints only with ``with_particles=False``, e.g. before a resume)."""
     from .solver import Solver
     a = dict(prob.analysis)
     a.update(overrides)
@@ -233,12 +234,13 @@ def build_solver(prob, solver_cls=None, **overrides):
                                blending_ratio=a.get("blending_ratio", 1.0),
                                gravity_ramping_time=a.get("gravity_ramping_time", 0.0),
                                locate_particles=a.get("locate_particles", True),
-                               precision=a.get("precision", "fp64"))
-    apply_problem(prob, s)
+                               precision=a.get("precision", "fp64"),
+                               device=a.get("device", 0))
+    apply_problem(prob, s, with_particles=with_particles)
     return s
 
 
-def apply_problem(prob, s):
+def apply_problem(prob, s, with_particles=True):
     """Feed a problem into any object with the solver's set-up methods (the GPU
     solver or the CPU oracle)."""
     s.set_mesh(prob.coords, prob.cells)
@@ -248,6 +250,8 @@ def apply_problem(prob, s):
         s.add_velocity_constraints(*prob.velocity_constraints)
     if prob.friction_constraints is not None:
         s.add_friction_constraints(*prob.friction_constraints)
+    if not with_particles:
+        return s
     for pts, mid in prob.particles:
         s.add_particles(pts, mid)
     s.initialise()

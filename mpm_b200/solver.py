@@ -204,6 +204,34 @@ class Solver:
         P.material = _i32p(keep["material"])
         self._ck(self.L.mpm_gpu_load_particles(self.h, n, C.byref(P)))
 
+    def write_pod(self, dtype=None):
+        """PODParticle records of the particles in the mesh (particle.tcc:180-306),
+        packed on the device, as a numpy structured array."""
+        from . import pod
+        dtype = pod.POD_DTYPE if dtype is None else dtype
+        size, offs, sizes = pod.layout(dtype)
+        cap = self.nparticles
+        out = np.zeros(cap, dtype=dtype)
+        n = C.c_int64()
+        psz = C.POINTER(C.c_size_t)
+        self._ck(self.L.mpm_gpu_write_pod(self.h, out.ctypes.data_as(C.c_void_p), cap, C.byref(n),
+                                          size, offs.ctypes.data_as(psz),
+                                          sizes.ctypes.data_as(psz), 74))
+        return out[:n.value]
+
+    def load_pod(self, records):
+        """Checkpoint resume from PODParticle records (mesh.tcc:1663-1720)."""
+        from . import pod
+        records = np.ascontiguousarray(records)
+        size, offs, sizes = pod.layout(records.dtype)
+        psz = C.POINTER(C.c_size_t)
+        self._ck(self.L.mpm_gpu_load_pod(self.h, records.ctypes.data_as(C.c_void_p), len(records),
+                                         size, offs.ctypes.data_as(psz),
+                                         sizes.ctypes.data_as(psz), 74))
+
+    def set_current_step(self, step):
+        self._ck(self.L.mpm_gpu_set_current_step(self.h, int(step)))
+
     def device_field(self, field):
         """(address, stride, ncomp) of a device-resident particle field."""
         names = {"x": 0, "u": 1, "v": 2, "stress": 3, "strain": 4, "F": 5, "volume": 6,

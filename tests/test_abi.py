@@ -61,3 +61,17 @@ def test_product_does_not_reference_the_oracle():
                 text = open(os.path.join(dirpath, f)).read()
                 assert "mpm_oracle" not in text and "import oracle" not in text \
                     and "from oracle" not in text, f
+
+
+def test_pod_record_table_matches_the_reference_field_list():
+    """74 fields in PODParticle order with the sizes of pod_particle.cc."""
+    from mpm_b200 import pod
+    assert len(pod.NAMES) == 74
+    assert pod.NAMES[:4] == ["id", "mass", "volume", "pressure"]
+    assert pod.NAMES[40] == "initialise_mapping_matrix" and pod.NAMES[50] == "status"
+    assert pod.NAMES[51:54] == ["cell_id", "material_id", "nstate_vars"]
+    assert pod.NAMES[54] == "svars_0" and pod.NAMES[73] == "svars_19"
+    size, offs, sizes = pod.layout()
+    expect = [1 if i in (40, 50) else 4 if i in (52, 53) else 8 for i in range(74)]
+    assert list(sizes) == expect
+    assert all(o % s == 0 for o, s in zip(offs, sizes)) and size % 8 == 0
