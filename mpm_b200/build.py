@@ -29,7 +29,7 @@ UNITS = [
     ("noalloc.cu", []),
     ("pod.cu", []),
 ]
-HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp", "mpm_device.cuh"]
+HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp", "mpm_device.cuh", "mpm_bulk.cuh"]
 
 
 def _newer(target, deps):

@@ -15,6 +15,7 @@
 // neighbourhood (usually none).
 #include <cuda_runtime.h>
 
+#include "mpm_bulk.cuh"
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
 #include "mpm_state.cuh"
@@ -345,16 +346,36 @@ __global__ void __launch_bounds__(256) k_nodes(DevState s, double dt, double dam
   }
 }
 
+// One particle's fields, read and written in global memory (GlobalRow) or in
+// the block's shared-memory staging (SmemRow, STAGE_T particles per row).
+struct GlobalRow {
+  const DevState& s;
+  int64_t p;
+  __device__ __forceinline__ double& f(int field) const { return s.pf[(int64_t)field * s.np + p]; }
+  __device__ __forceinline__ double& sv(int k) const { return s.sv[(int64_t)k * s.np + p]; }
+  __device__ __forceinline__ int mat() const { return s.mat[p]; }
+};
+constexpr int STAGE_T = 128;  // particles per staged block (= PAD_PARTICLES)
+struct SmemRow {
+  double* rows;  // [field][STAGE_T]
+  double* svr;   // [SV_N][STAGE_T]
+  int t;
+  int m;
+  __device__ __forceinline__ double& f(int field) const { return rows[field * STAGE_T + t]; }
+  __device__ __forceinline__ double& sv(int k) const { return svr[k * STAGE_T + t]; }
+  __device__ __forceinline__ int mat() const { return m; }
+};
+
 // ------------------------------------------------------- stress and strain
 // mpm_scheme.tcc:75-103: F increment (particle.tcc:1580-1628), strain
 // (:819-876), volume (:598-605), material stress (:880-889), F (:1654-1658).
 // D: dN/dx at the particle (start of step); the cell's centroid gradients
 // come from the per-cell table computed once from the mesh.
-template <int DIM>
-__device__ __forceinline__ void stress_update(const DevState& s, int64_t p, int c, const int* nid,
-                                              const double* D, double dt) {
+template <int DIM, class Row>
+__device__ __forceinline__ void stress_update(const DevState& s, const Row& r, int c,
+                                              const int* nid, const double* D, double dt) {
   constexpr int NV = Elem<DIM>::NV;
-  const int64_t np = s.np, nn = s.nn;
+  const int64_t nn = s.nn;
   const double* Dc = s.dndx_c + (int64_t)c * NV * DIM;
   double Fi[DIM * DIM];
 #pragma unroll
@@ -417,58 +438,58 @@ __device__ __forceinline__ void stress_update(const DevState& s, int64_t p, int 
   if constexpr (DIM == 2) {
     const int map[3] = {0, 1, 3};
 #pragma unroll
-    for (int k = 0; k < 3; ++k) s.pf[(int64_t)(PF<2>::E + k) * np + p] += dstrain[map[k]];
+    for (int k = 0; k < 3; ++k) r.f(PF<2>::E + k) += dstrain[map[k]];
   } else {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) s.pf[(int64_t)(PF<3>::E + k) * np + p] += dstrain[k];
+    for (int k = 0; k < 6; ++k) r.f(PF<3>::E + k) += dstrain[k];
   }
-  double* volp = &s.pf[(int64_t)PF<DIM>::VOL * np + p];
-  double* rhop = &s.pf[(int64_t)PF<DIM>::RHO * np + p];
+  double* volp = &r.f(PF<DIM>::VOL);
+  double* rhop = &r.f(PF<DIM>::RHO);
   const double vol = *volp * (1. + dvol);
   const double rho = *rhop / (1. + dvol);
   *volp = vol;
   *rhop = rho;
   double sig[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-  for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = s.pf[(int64_t)(PF<DIM>::S + k) * np + p];
-  const MaterialParams& mp = s.mats[s.mat[p]];
+  for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = r.f(PF<DIM>::S + k);
+  const MaterialParams& mp = s.mats[r.mat()];
   double out[6];
   if (mp.type == 0) {
     material_compute_stress(mp, sig, dstrain, rho, nullptr, out);
   } else {
     double sv[SV_N];
 #pragma unroll
-    for (int k = 0; k < SV_N; ++k) sv[k] = s.sv[(int64_t)k * np + p];
+    for (int k = 0; k < SV_N; ++k) sv[k] = r.sv(k);
     material_compute_stress(mp, sig, dstrain, rho, sv, out);
 #pragma unroll
-    for (int k = 0; k < SV_N; ++k) s.sv[(int64_t)k * np + p] = sv[k];
+    for (int k = 0; k < SV_N; ++k) r.sv(k) = sv[k];
   }
 #pragma unroll
-  for (int k = 0; k < PF<DIM>::NS; ++k) s.pf[(int64_t)(PF<DIM>::S + k) * np + p] = out[k];
+  for (int k = 0; k < PF<DIM>::NS; ++k) r.f(PF<DIM>::S + k) = out[k];
   if constexpr (DIM == 2) {
     double F[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) F[k] = s.pf[(int64_t)(PF<2>::F + k) * np + p];
+    for (int k = 0; k < 4; ++k) F[k] = r.f(PF<2>::F + k);
     // 3x3 product with F_inc and F both (0,0,1) in the third row and column:
     // the dropped terms are exact zeros
     const double r00 = Fi[0] * F[0] + Fi[1] * F[2];
     const double r01 = Fi[0] * F[1] + Fi[1] * F[3];
     const double r10 = Fi[2] * F[0] + Fi[3] * F[2];
     const double r11 = Fi[2] * F[1] + Fi[3] * F[3];
-    s.pf[(int64_t)(PF<2>::F + 0) * np + p] = r00;
-    s.pf[(int64_t)(PF<2>::F + 1) * np + p] = r01;
-    s.pf[(int64_t)(PF<2>::F + 2) * np + p] = r10;
-    s.pf[(int64_t)(PF<2>::F + 3) * np + p] = r11;
+    r.f(PF<2>::F + 0) = r00;
+    r.f(PF<2>::F + 1) = r01;
+    r.f(PF<2>::F + 2) = r10;
+    r.f(PF<2>::F + 3) = r11;
   } else {
     double F[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) F[k] = s.pf[(int64_t)(PF<3>::F + k) * np + p];
+    for (int k = 0; k < 9; ++k) F[k] = r.f(PF<3>::F + k);
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
+    for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int q = 0; q < 3; ++q)
-        s.pf[(int64_t)(PF<3>::F + r * 3 + q) * np + p] =
-            (Fi[r * 3 + 0] * F[0 * 3 + q] + Fi[r * 3 + 1] * F[1 * 3 + q]) + Fi[r * 3 + 2] * F[2 * 3 + q];
+        r.f(PF<3>::F + a * 3 + q) =
+            (Fi[a * 3 + 0] * F[0 * 3 + q] + Fi[a * 3 + 1] * F[1 * 3 + q]) + Fi[a * 3 + 2] * F[2 * 3 + q];
   }
 }
 
@@ -497,7 +518,7 @@ __global__ void __launch_bounds__(128) k_stress(DevState s, double dt) {
   local_xi<DIM>(x, g.centroid, g.len, xi);
   cell_nodes_coords<DIM>(s, c, nid, X);
   dn_dx_all<DIM>(xi, X, D);
-  stress_update<DIM>(s, p, c, nid, D, dt);
+  stress_update<DIM>(s, GlobalRow{s, p}, c, nid, D, dt);
 }
 
 // --------------------------------------------------------------------- G2P
@@ -563,7 +584,7 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
   if constexpr (STRESS) {
     double D[NV * DIM];
     dn_dx_all<DIM>(xi, X, D);
-    stress_update<DIM>(s, p, c, nid, D, dt);
+    stress_update<DIM>(s, GlobalRow{s, p}, c, nid, D, dt);
   }
   bool finite = true;
 #pragma unroll
@@ -579,6 +600,162 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
   } else {
     s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
   }
+}
+
+// USL G2P + stress update + locate with the block's particle slices staged in
+// shared memory by the bulk-copy engine.  One thread issues the copies of
+// every field slice (1 KB each) at block start: phase A (x, u, v, cell,
+// material, velocity-constraint slot) and phase B (stress, strain, F,
+// volume, density, MohrCoulomb state).  The threads gather nodal values while
+// phase B is in flight, update the staged rows in place and one thread stores
+// the rows back with bulk copies.  The arithmetic is k_g2p<DIM, true, FLIP>'s.
+static_assert(STAGE_T == PAD_PARTICLES, "staged slices are whole padded blocks");
+template <int DIM>
+constexpr int staged_rows() { return PF<DIM>::MASS; }  // fields X .. RHO
+template <int DIM>
+constexpr size_t staged_smem_bytes(bool mc) {
+  return (size_t)(staged_rows<DIM>() + (mc ? SV_N : 0)) * STAGE_T * 8 + STAGE_T * (4 + 1 + 2);
+}
+
+template <int DIM, bool FLIP>
+__global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
+    k_g2p_staged(DevState s, double dt, double beta) {
+  constexpr int NV = Elem<DIM>::NV;
+  constexpr int T = STAGE_T;
+  constexpr int ROWS = staged_rows<DIM>();
+  constexpr int ROWS_A = PF<DIM>::S;  // x, u, v
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar[2];
+  __shared__ int timed_out;
+  const bool mc = s.sv != nullptr;
+  double* rows = reinterpret_cast<double*>(smem);
+  double* svr = rows + ROWS * T;
+  int32_t* scell = reinterpret_cast<int32_t*>(svr + (mc ? SV_N * T : 0));
+  uint8_t* smat = reinterpret_cast<uint8_t*>(scell + T);
+  int16_t* spvc = reinterpret_cast<int16_t*>(smat + T);
+  const int t = threadIdx.x;
+  const int64_t p0 = (int64_t)blockIdx.x * T;
+  const int64_t np = s.np, nn = s.nn;
+  if (t == 0) {
+    timed_out = 0;
+    bulk::mbar_init(&bar[0], 1);
+    bulk::mbar_init(&bar[1], 1);
+    bulk::fence_barrier_init();
+  }
+  __syncthreads();
+  if (t == 0) {
+    bulk::mbar_arrive_expect_tx(&bar[0], ROWS_A * T * 8 + T * (4 + 1 + 2));
+    for (int f = 0; f < ROWS_A; ++f) bulk::load(rows + f * T, s.pf + f * np + p0, T * 8, &bar[0]);
+    bulk::load(scell, s.cell + p0, T * 4, &bar[0]);
+    bulk::load(smat, s.mat + p0, T, &bar[0]);
+    bulk::load(spvc, s.pvc + p0, T * 2, &bar[0]);
+    bulk::mbar_arrive_expect_tx(&bar[1], (ROWS - ROWS_A + (mc ? SV_N : 0)) * T * 8);
+    for (int f = ROWS_A; f < ROWS; ++f) bulk::load(rows + f * T, s.pf + f * np + p0, T * 8, &bar[1]);
+    if (mc)
+      for (int k = 0; k < SV_N; ++k) bulk::load(svr + k * T, s.sv + k * np + p0, T * 8, &bar[1]);
+  }
+  const bool okA = bulk::mbar_wait(&bar[0], 0);
+  const int c = okA ? scell[t] : -1;
+  const int64_t p = p0 + t;
+  const SmemRow r{rows, svr, t, okA ? (int)smat[t] : 0};
+  double xn[DIM];
+  const bool active = c >= 0;
+  double xi[DIM];
+  if (active) {
+    double x[DIM], N[NV], X[NV * DIM];
+    int nid[NV];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) x[d] = r.f(PF<DIM>::X + d);
+    const CellGeom& g = s.geom[c];
+    local_xi<DIM>(x, g.centroid, g.len, xi);
+    shapefn<DIM>(xi, N);
+    cell_nodes_coords<DIM>(s, c, nid, X);
+    double nvel[DIM], nacc[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      const int n = nid[i];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + n];
+      if constexpr (FLIP) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * s.nf[(int64_t)(NF<DIM>::ACC + d) * nn + n];
+      }
+    }
+    double v[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = r.f(PF<DIM>::V + d);
+    if constexpr (FLIP) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[d] += nacc[d] * dt;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[d] = beta * v[d] + (1.0 - beta) * nvel[d];
+    } else {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[d] = nvel[d];
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      xn[d] = x[d] + nvel[d] * dt;
+      r.f(PF<DIM>::X + d) = xn[d];
+      r.f(PF<DIM>::U + d) += nvel[d] * dt;
+    }
+    const int pv = spvc[t];
+    if (pv >= 0) {
+      const ParticleVC& vc = s.pvcs[pv];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        if (vc.mask & (1u << d)) v[d] = vc.value[d];
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) r.f(PF<DIM>::V + d) = v[d];
+  }
+  const bool okB = okA && bulk::mbar_wait(&bar[1], 0);
+  if (!okA || !okB) timed_out = 1;
+  if (active && okB) {
+    // node ids and coordinates again rather than kept live across the wait
+    double X[NV * DIM], D[NV * DIM];
+    int nid[NV];
+    cell_nodes_coords<DIM>(s, c, nid, X);
+    dn_dx_all<DIM>(xi, X, D);
+    stress_update<DIM>(s, r, c, nid, D, dt);
+  }
+  bulk::fence_shared_to_async();
+  __syncthreads();
+  if (timed_out) {
+    // copies that never completed: report, give in-flight copies a last
+    // bounded wait, store nothing
+    if (t == 0) {
+      raise_err(s, ERR_TIMEOUT);
+      bulk::mbar_wait(&bar[0], 0);
+      bulk::mbar_wait(&bar[1], 0);
+    }
+    return;
+  }
+  if (t == 0) {
+    for (int f = 0; f < ROWS; ++f) bulk::store(s.pf + f * np + p0, rows + f * T, T * 8);
+    if (mc)
+      for (int k = 0; k < SV_N; ++k) bulk::store(s.sv + k * np + p0, svr + k * T, T * 8);
+    bulk::store_commit();
+  }
+  if (active) {
+    bool finite = true;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) finite = finite && isfinite(xn[d]);
+    if (!finite) {
+      raise_err(s, ERR_NONFINITE);
+      s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+    } else {
+      const int nc = locate_near<DIM>(s, xn, c);
+      if (nc >= 0) {
+        if (nc != c) s.cell[p] = nc;
+      } else {
+        s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+      }
+    }
+  }
+  if (t == 0) bulk::store_wait_all();
 }
 
 // Exhaustive search for particles not in their cell or its neighbours
@@ -642,6 +819,18 @@ void counting_sort_impl(const DevState& s, cudaStream_t st) {
   k_fill<<<nblocks(s.np, 256), 256, 0, st>>>(s);
 }
 
+// Ask for the shared-memory carveout that lets MIN_BLOCKS staged blocks share
+// an SM (set once per kernel).
+template <class K>
+void prefer_shared_memory(K kernel) {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    done = true;
+  }
+}
+
 template <int DIM>
 void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& pr) {
   const int64_t np = s.np, nn = s.nn;
@@ -661,10 +850,14 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
-    if (a.flip)
-      k_g2p<DIM, true, true><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
-    else
-      k_g2p<DIM, true, false><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
+    const size_t sm = staged_smem_bytes<DIM>(s.sv != nullptr);
+    if (a.flip) {
+      prefer_shared_memory(k_g2p_staged<DIM, true>);
+      k_g2p_staged<DIM, true><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
+    } else {
+      prefer_shared_memory(k_g2p_staged<DIM, false>);
+      k_g2p_staged<DIM, false><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
+    }
     pr.end(K_G2P, st);
   } else {  // USF
     pr.begin(K_P2G, st);

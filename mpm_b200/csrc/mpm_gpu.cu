@@ -177,8 +177,12 @@ struct mpm_gpu_solver {
   std::vector<MaterialParams> mats;
   std::map<int32_t, int> mat_index;     // material id -> slot
 
-  // particles (host staging)
+  // particles (host staging).  On the device every particle field is an
+  // array of npad = np rounded up to a multiple of PAD_PARTICLES entries; the
+  // padding rows are removed particles (cell -1), so a block's slice of a
+  // field is one aligned contiguous segment.
   int64_t np = 0;
+  int64_t npad = 0;
   std::vector<double> p_coords;         // np*dim (creation)
   std::vector<uint8_t> p_mat;
   std::vector<std::map<unsigned, double>> p_vc;  // per particle velocity constraints
@@ -225,6 +229,10 @@ struct mpm_gpu_solver {
   DevBuf<MaterialT<float>> d_mats_f;
 
   int nfields() const { return dim == 2 ? PF<2>::NF : PF<3>::NF; }
+  void set_np(int64_t n) {
+    np = n;
+    npad = (n + PAD_PARTICLES - 1) / PAD_PARTICLES * PAD_PARTICLES;
+  }
   int nfields_x() const { return dim == 2 ? PDX<2>::ND : PDX<3>::ND; }
   int nfields_m() const { return dim == 2 ? PM<2>::NF : PM<3>::NF; }
   int nnf() const { return dim == 2 ? NF<2>::NNF : NF<3>::NNF; }
@@ -606,7 +614,7 @@ void upload_bcs(mpm_gpu_t h) {
 }
 
 void upload_pvc(mpm_gpu_t h) {
-  std::vector<int16_t> idx(h->np, -1);
+  std::vector<int16_t> idx(h->npad, -1);
   std::vector<ParticleVC> table;
   std::map<std::string, int> dedup;
   for (int64_t p = 0; p < h->np; ++p) {
@@ -636,7 +644,7 @@ void upload_pvc(mpm_gpu_t h) {
 }
 
 void allocate_particles(mpm_gpu_t h) {
-  const int64_t np = h->np;
+  const int64_t np = h->npad;
   h->d_pf.alloc((size_t)(h->mixed ? h->nfields_x() : h->nfields()) * np);
   if (h->mixed) h->d_pm.alloc((size_t)h->nfields_m() * np);
   h->d_cell.alloc(np);
@@ -656,7 +664,7 @@ void allocate_particles(mpm_gpu_t h) {
 
 void refresh_state(mpm_gpu_t h) {
   DevState& s = h->ds;
-  s.np = h->np;
+  s.np = h->npad;
   s.pf = h->d_pf.p;
   s.sv = h->d_sv.p;
   s.cell = h->d_cell.p;
@@ -731,12 +739,12 @@ LayoutM layout_m(int dim) {
 }
 bool identity_entry(int dim, int k) { return dim == 2 ? (k == 0 || k == 3) : (k % 4 == 0); }
 
-// Upload particle fields given in the FP64 layout (pf: [PF::NF][np], sv:
-// [SV_N][np] or empty).  The mixed path keeps x, u and pdstrain in FP64 and
+// Upload particle fields given in the FP64 layout (pf: [PF::NF][npad], sv:
+// [SV_N][npad] or empty).  The mixed path keeps x, u and pdstrain in FP64 and
 // stores the rest in FP32, F as H = F - I and volume / density as the initial
 // values with P = V / V0 - 1 = 0.
 void upload_particle_fields(mpm_gpu_t h, const std::vector<double>& pf, const std::vector<double>& sv) {
-  const int64_t np = h->np;
+  const int64_t np = h->npad;
   const int dim = h->dim;
   if (!h->mixed) {
     h->d_pf.upload(pf.data(), pf.size(), h->stream);
@@ -779,7 +787,7 @@ void upload_particle_fields(mpm_gpu_t h, const std::vector<double>& pf, const st
 // Download the particle fields into the FP64 layout (inverse of
 // upload_particle_fields).
 void download_particle_fields(mpm_gpu_t h, std::vector<double>& pf, std::vector<double>& sv) {
-  const int64_t np = h->np;
+  const int64_t np = h->npad;
   const int dim = h->dim;
   pf.assign((size_t)h->nfields() * np, 0.0);
   sv.assign(h->any_mc ? (size_t)SV_N * np : 0, 0.0);
@@ -823,9 +831,9 @@ void download_particle_fields(mpm_gpu_t h, std::vector<double>& pf, std::vector<
 // Pack host particle rows (ABI layout) into the device SoA field order.
 void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<int32_t>* cells) {
   const int dim = h->dim;
-  const int64_t np = h->np;
-  std::vector<double> pf((size_t)h->nfields() * np, 0.0);
-  auto at = [&](int f, int64_t p) -> double& { return pf[(size_t)f * np + p]; };
+  const int64_t np = h->np, ns = h->npad;
+  std::vector<double> pf((size_t)h->nfields() * ns, 0.0);
+  auto at = [&](int f, int64_t p) -> double& { return pf[(size_t)f * ns + p]; };
   const int X = dim == 2 ? PF<2>::X : PF<3>::X, U = dim == 2 ? PF<2>::U : PF<3>::U;
   const int V = dim == 2 ? PF<2>::V : PF<3>::V, S = dim == 2 ? PF<2>::S : PF<3>::S;
   const int E = dim == 2 ? PF<2>::E : PF<3>::E, Fo = dim == 2 ? PF<2>::F : PF<3>::F;
@@ -864,7 +872,7 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
     at(VOL, p) = in->volume ? in->volume[p] : 0.;
     at(MASS, p) = in->mass ? in->mass[p] : at(VOL, p) * at(RHO, p);
   }
-  std::vector<int32_t> cell(np);
+  std::vector<int32_t> cell(ns, -1);
   for (int64_t p = 0; p < np; ++p) {
     if (in->cell) {
       const int64_t c = in->cell[p];
@@ -874,11 +882,13 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
       cell[p] = (*cells)[p];
     }
   }
-  h->d_cell.upload(cell.data(), np, h->stream);
-  h->d_mat.upload(h->p_mat.data(), np, h->stream);
+  h->d_cell.upload(cell.data(), ns, h->stream);
+  std::vector<uint8_t> mat(h->p_mat);
+  mat.resize(ns, 0);
+  h->d_mat.upload(mat.data(), ns, h->stream);
   std::vector<double> sv;
   if (h->any_mc) {
-    sv.assign((size_t)SV_N * np, 0.0);
+    sv.assign((size_t)SV_N * ns, 0.0);
     for (int64_t p = 0; p < np; ++p) {
       const MaterialParams& m = h->mats[h->p_mat[p]];
       double s[SV_N] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -886,10 +896,11 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
         for (int k = 0; k < SV_N; ++k) s[k] = in->svars[p * SV_N + k];
       else if (m.type == 1)
         mc_init_state(m, s);
-      for (int k = 0; k < SV_N; ++k) sv[(size_t)k * np + p] = s[k];
+      for (int k = 0; k < SV_N; ++k) sv[(size_t)k * ns + p] = s[k];
     }
   }
   upload_particle_fields(h, pf, sv);
+  ck(cudaStreamSynchronize(h->stream), "sync");
 }
 
 #define MPM_GUARD(h)                                                   \
@@ -1129,7 +1140,7 @@ int mpm_gpu_add_particles(mpm_gpu_t h, int64_t n, const double* coords, int32_t 
   if (h->np + n > INT32_MAX) throw InvalidArg("too many particles for 32-bit indices");
   h->p_coords.insert(h->p_coords.end(), coords, coords + n * h->dim);
   h->p_mat.insert(h->p_mat.end(), (size_t)n, (uint8_t)it->second);
-  h->np += n;
+  h->set_np(h->np + n);
   MPM_END(h)
   return MPM_OK;
 }
@@ -1187,20 +1198,21 @@ int mpm_gpu_assign_particle_stresses(mpm_gpu_t h, int64_t n, const double* stres
   const int dim = h->dim;
   const int S = dim == 2 ? PF<2>::S : PF<3>::S;
   const int ns = dim == 2 ? PF<2>::NS : PF<3>::NS;
-  std::vector<double> cols((size_t)ns * n);
+  const int64_t npad = h->npad;
+  std::vector<double> cols((size_t)ns * npad, 0.0);
   for (int64_t p = 0; p < n; ++p) {
     if (dim == 2 && (stress[p * 6 + 4] != 0. || stress[p * 6 + 5] != 0.))
       throw InvalidArg("2D particle stress must have zero yz and xz components");
-    for (int k = 0; k < ns; ++k) cols[(size_t)k * n + p] = stress[p * 6 + k];
+    for (int k = 0; k < ns; ++k) cols[(size_t)k * npad + p] = stress[p * 6 + k];
   }
   if (h->mixed) {
     const std::vector<float> colf(cols.begin(), cols.end());
     const int SM = dim == 2 ? PM<2>::S : PM<3>::S;
-    ck(cudaMemcpyAsync(h->d_pm.p + (size_t)SM * n, colf.data(), sizeof(float) * colf.size(),
+    ck(cudaMemcpyAsync(h->d_pm.p + (size_t)SM * npad, colf.data(), sizeof(float) * colf.size(),
                        cudaMemcpyHostToDevice, h->stream), "H2D");
     ck(cudaStreamSynchronize(h->stream), "sync");
   } else {
-    ck(cudaMemcpyAsync(h->d_pf.p + (size_t)S * n, cols.data(), sizeof(double) * cols.size(),
+    ck(cudaMemcpyAsync(h->d_pf.p + (size_t)S * npad, cols.data(), sizeof(double) * cols.size(),
                        cudaMemcpyHostToDevice, h->stream), "H2D");
   }
   ck(cudaStreamSynchronize(h->stream), "sync");
@@ -1236,7 +1248,7 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
   if (!in || !in->x || !in->volume || !in->cell || !in->material)
     throw InvalidArg("load_particles needs x, volume, cell and material");
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
-  h->np = n;
+  h->set_np(n);
   h->p_coords.assign(n * h->dim, 0.);
   h->p_mat.resize(n);
   for (int64_t p = 0; p < n; ++p) {
@@ -1308,6 +1320,7 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
   if (words[1] & ERR_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite particle position");
   if (words[1] & ERR_OUTSIDE) return fail(h, MPM_ERR_OUTSIDE, "Particle(s) outside the mesh domain");
   if (words[1] & ERR_BADCELL) return fail(h, MPM_ERR_INVALID, "corrupt particle cell index");
+  if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded wait on a device copy ran out");
   MPM_END(h)
   return MPM_OK;
 }
@@ -1353,7 +1366,8 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   std::vector<int32_t> cell(np);
   h->d_cell.download(cell.data(), np, h->stream);
   download_particle_fields(h, pf, sv);
-  auto at = [&](int f, int64_t p) { return pf[(size_t)f * np + p]; };
+  const int64_t ns = h->npad;
+  auto at = [&](int f, int64_t p) { return pf[(size_t)f * ns + p]; };
   const int X = dim == 2 ? PF<2>::X : PF<3>::X, U = dim == 2 ? PF<2>::U : PF<3>::U;
   const int V = dim == 2 ? PF<2>::V : PF<3>::V, S = dim == 2 ? PF<2>::S : PF<3>::S;
   const int E = dim == 2 ? PF<2>::E : PF<3>::E, Fo = dim == 2 ? PF<2>::F : PF<3>::F;
@@ -1409,7 +1423,7 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
       out->material[p] = id;
     }
     if (out->svars)
-      for (int k = 0; k < SV_N; ++k) out->svars[p * SV_N + k] = h->any_mc ? sv[(size_t)k * np + p] : 0.;
+      for (int k = 0; k < SV_N; ++k) out->svars[p * SV_N + k] = h->any_mc ? sv[(size_t)k * ns + p] : 0.;
   }
   MPM_END(h)
   return MPM_OK;
@@ -1464,10 +1478,18 @@ std::vector<std::pair<size_t, size_t>> pod_runs(const size_t* offsets, const siz
 
 void upload_pod_aux(mpm_gpu_t h) {
   if (!h->aux_dirty) return;
-  const int64_t np = h->np;
-  h->d_pid.upload(h->p_id.data(), np, h->stream);
-  h->d_nsize.upload(h->p_nsize.data(), 3 * np, h->stream);
-  h->d_pacc.upload(h->p_acc.data(), 3 * np, h->stream);
+  const int64_t np = h->np, ns = h->npad;
+  std::vector<uint64_t> id(h->p_id);
+  id.resize(ns, 0);
+  std::vector<double> nsz((size_t)3 * ns, 0.0), acc((size_t)3 * ns, 0.0);
+  for (int d = 0; d < 3; ++d)
+    for (int64_t p = 0; p < np; ++p) {
+      nsz[(size_t)d * ns + p] = h->p_nsize[(size_t)d * np + p];
+      acc[(size_t)d * ns + p] = h->p_acc[(size_t)d * np + p];
+    }
+  h->d_pid.upload(id.data(), ns, h->stream);
+  h->d_nsize.upload(nsz.data(), 3 * ns, h->stream);
+  h->d_pacc.upload(acc.data(), 3 * ns, h->stream);
   std::vector<int32_t> ids(h->mats.size(), -1);
   std::vector<uint32_t> nstate(h->mats.size(), 0);
   for (auto& kv : h->mat_index) ids[kv.second] = kv.first;
@@ -1721,8 +1743,8 @@ int mpm_gpu_device_field(mpm_gpu_t h, int32_t field, void** base, int64_t* strid
     case 8: off = dim == 2 ? PF<2>::MASS : PF<3>::MASS; nc = 1; break;
     default: throw InvalidArg("unknown field");
   }
-  *base = h->d_pf.p + (size_t)off * h->np;
-  *stride = h->np;
+  *base = h->d_pf.p + (size_t)off * h->npad;
+  *stride = h->npad;
   *ncomp = nc;
   MPM_END(h)
   return MPM_OK;

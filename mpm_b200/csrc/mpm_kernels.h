@@ -33,6 +33,9 @@ enum KernelId {
   K_NKERNELS
 };
 constexpr int SCAN_BLOCK = 4096;  // cells per block of the counting-sort scan
+// particle arrays are padded to a multiple of this (the particle-kernel block
+// size), so every block's slice of a field is a whole aligned segment
+constexpr int PAD_PARTICLES = 128;
 const char* kernel_name(int kid);
 
 // Counts launches; when enabled, brackets every launch with a pair of CUDA
