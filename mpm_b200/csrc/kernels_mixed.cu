@@ -20,6 +20,7 @@
 // per-cell P2G, node gather and update, G2P + stress + locate.
 #include <cuda_runtime.h>
 
+#include "mpm_bulk.cuh"
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
 #include "mpm_state.cuh"
@@ -357,17 +358,43 @@ __device__ __forceinline__ void mc_update_mixed(const MaterialParams& md, const 
   pd = svd[SV_PD];
 }
 
-// mpm_scheme.tcc:75-103 in FP32 on the deviation variables (H, P).
+// One particle's mixed-precision fields in global memory (MGlobalRow) or in
+// the block's shared-memory staging (MSmemRow, MSTAGE_T particles per row):
+// m(f) the FP32 field f of PM, svf(k) the FP32 MohrCoulomb state, pd() the
+// FP64 plastic deviatoric strain.
 template <int DIM>
-__device__ __forceinline__ void stress_update_mixed(const DevState& s, int64_t p, int c,
+struct MGlobalRow {
+  const DevState& s;
+  int64_t p;
+  __device__ __forceinline__ float& m(int f) const { return s.pm[(int64_t)f * s.np + p]; }
+  __device__ __forceinline__ float& svf(int k) const { return s.svf[(int64_t)k * s.np + p]; }
+  __device__ __forceinline__ double& pd() const { return s.pf[(int64_t)PDX<DIM>::PDS * s.np + p]; }
+  __device__ __forceinline__ int mat() const { return s.mat[p]; }
+};
+constexpr int MSTAGE_T = 128;  // particles per staged block (= PAD_PARTICLES)
+struct MSmemRow {
+  double* pdr;   // [MSTAGE_T] pdstrain
+  float* mrows;  // [PM field][MSTAGE_T]
+  float* svr;    // [SVF_N][MSTAGE_T]
+  int t;
+  int mi;
+  __device__ __forceinline__ float& m(int f) const { return mrows[f * MSTAGE_T + t]; }
+  __device__ __forceinline__ float& svf(int k) const { return svr[k * MSTAGE_T + t]; }
+  __device__ __forceinline__ double& pd() const { return pdr[t]; }
+  __device__ __forceinline__ int mat() const { return mi; }
+};
+
+// mpm_scheme.tcc:75-103 in FP32 on the deviation variables (H, P).
+template <int DIM, class Row>
+__device__ __forceinline__ void stress_update_mixed(const DevState& s, const Row& r, int c,
                                                     const int* nid, const float* D, float dt) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int NS = PF<DIM>::NS;
-  const int64_t np = s.np, nn = s.nn;
+  const int64_t nn = s.nn;
   const float* Dc = s.dndx_cf + (int64_t)c * NV * DIM;
   float Hi[DIM * DIM];
 #pragma unroll
-  for (int r = 0; r < DIM * DIM; ++r) Hi[r] = 0.f;
+  for (int a = 0; a < DIM * DIM; ++a) Hi[a] = 0.f;
   float sr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float src[3] = {0.f, 0.f, 0.f};
 #pragma unroll
@@ -376,9 +403,9 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, int64_t p
 #pragma unroll
     for (int d = 0; d < DIM; ++d) vel[d] = s.nfv[(int64_t)d * nn + nid[i]];
 #pragma unroll
-    for (int r = 0; r < DIM; ++r)
+    for (int a = 0; a < DIM; ++a)
 #pragma unroll
-      for (int q = 0; q < DIM; ++q) Hi[r * DIM + q] += vel[r] * D[i * DIM + q] * dt;
+      for (int q = 0; q < DIM; ++q) Hi[a * DIM + q] += vel[a] * D[i * DIM + q] * dt;
     const float* Dn = &D[i * DIM];
     float dc[DIM];
 #pragma unroll
@@ -403,8 +430,8 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, int64_t p
   }
   // F_inc = I + Hi with the reference's 1e-15 snapping (particle.tcc:1619-1626)
 #pragma unroll
-  for (int r = 0; r < DIM * DIM; ++r)
-    if (fabsf(Hi[r]) < 1.E-15f) Hi[r] = 0.f;
+  for (int a = 0; a < DIM * DIM; ++a)
+    if (fabsf(Hi[a]) < 1.E-15f) Hi[a] = 0.f;
 #pragma unroll
   for (int k = 0; k < 6; ++k)
     if (fabsf(sr[k]) < 1.E-15f) sr[k] = 0.f;
@@ -421,22 +448,20 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, int64_t p
   if constexpr (DIM == 2) {
     const int map[3] = {0, 1, 3};
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
-      set_pmf<DIM>(s, PM<2>::E + k, p, pmf<DIM>(s, PM<2>::E + k, p) + dstrain[map[k]]);
+    for (int k = 0; k < 3; ++k) r.m(PM<2>::E + k) += dstrain[map[k]];
   } else {
 #pragma unroll
-    for (int k = 0; k < 6; ++k)
-      set_pmf<DIM>(s, PM<3>::E + k, p, pmf<DIM>(s, PM<3>::E + k, p) + dstrain[k]);
+    for (int k = 0; k < 6; ++k) r.m(PM<3>::E + k) += dstrain[k];
   }
   // V *= (1 + dvol), rho /= (1 + dvol) as P = V / V0 - 1 (particle.tcc:598-605)
-  const float P = pmf<DIM>(s, PM<DIM>::JP, p);
+  const float P = r.m(PM<DIM>::JP);
   const float Pn = P + dvol + P * dvol;
-  set_pmf<DIM>(s, PM<DIM>::JP, p, Pn);
-  const float rho = pmf<DIM>(s, PM<DIM>::RHO0, p) / (1.f + Pn);
+  r.m(PM<DIM>::JP) = Pn;
+  const float rho = r.m(PM<DIM>::RHO0) / (1.f + Pn);
   float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-  for (int k = 0; k < NS; ++k) sig[k] = pmf<DIM>(s, PM<DIM>::S + k, p);
-  const int mi = s.mat[p];
+  for (int k = 0; k < NS; ++k) sig[k] = r.m(PM<DIM>::S + k);
+  const int mi = r.mat();
   float out[6];
   if (s.mats_f[mi].type == 0) {
     float t[6];
@@ -446,44 +471,42 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, int64_t p
   } else {
     float svf[SVF_N];
 #pragma unroll
-    for (int k = 0; k < SVF_N; ++k) svf[k] = s.svf[(int64_t)k * np + p];
-    double* pdp = &s.pf[(int64_t)PDX<DIM>::PDS * np + p];
-    double pd = *pdp;
+    for (int k = 0; k < SVF_N; ++k) svf[k] = r.svf(k);
+    double pd = r.pd();
     mc_update_mixed(s.mats[mi], s.mats_f[mi], sig, dstrain, rho, svf, pd, out);
-    *pdp = pd;
+    r.pd() = pd;
     const int first = s.mats_f[mi].softening ? 0 : SV_EPS;  // phi..tc change only with softening
-    s.svf[(int64_t)SV_YIELD * np + p] = svf[SV_YIELD];
+    r.svf(SV_YIELD) = svf[SV_YIELD];
 #pragma unroll
     for (int k = 1; k < SVF_N; ++k)
-      if (k >= first) s.svf[(int64_t)k * np + p] = svf[k];
+      if (k >= first) r.svf(k) = svf[k];
   }
 #pragma unroll
-  for (int k = 0; k < NS; ++k) set_pmf<DIM>(s, PM<DIM>::S + k, p, out[k]);
+  for (int k = 0; k < NS; ++k) r.m(PM<DIM>::S + k) = out[k];
   // F = F_inc F as H = H + Hi + Hi H
   if constexpr (DIM == 2) {
     float H[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) H[k] = pmf<DIM>(s, PM<2>::H + k, p);
+    for (int k = 0; k < 4; ++k) H[k] = r.m(PM<2>::H + k);
     const float n00 = H[0] + Hi[0] + (Hi[0] * H[0] + Hi[1] * H[2]);
     const float n01 = H[1] + Hi[1] + (Hi[0] * H[1] + Hi[1] * H[3]);
     const float n10 = H[2] + Hi[2] + (Hi[2] * H[0] + Hi[3] * H[2]);
     const float n11 = H[3] + Hi[3] + (Hi[2] * H[1] + Hi[3] * H[3]);
-    set_pmf<DIM>(s, PM<2>::H + 0, p, n00);
-    set_pmf<DIM>(s, PM<2>::H + 1, p, n01);
-    set_pmf<DIM>(s, PM<2>::H + 2, p, n10);
-    set_pmf<DIM>(s, PM<2>::H + 3, p, n11);
+    r.m(PM<2>::H + 0) = n00;
+    r.m(PM<2>::H + 1) = n01;
+    r.m(PM<2>::H + 2) = n10;
+    r.m(PM<2>::H + 3) = n11;
   } else {
     float H[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) H[k] = pmf<DIM>(s, PM<3>::H + k, p);
+    for (int k = 0; k < 9; ++k) H[k] = r.m(PM<3>::H + k);
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
+    for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int q = 0; q < 3; ++q)
-        set_pmf<DIM>(s, PM<3>::H + r * 3 + q, p,
-                     H[r * 3 + q] + Hi[r * 3 + q] +
-                         ((Hi[r * 3 + 0] * H[0 * 3 + q] + Hi[r * 3 + 1] * H[1 * 3 + q]) +
-                          Hi[r * 3 + 2] * H[2 * 3 + q]));
+        r.m(PM<3>::H + a * 3 + q) =
+            H[a * 3 + q] + Hi[a * 3 + q] +
+            ((Hi[a * 3 + 0] * H[0 * 3 + q] + Hi[a * 3 + 1] * H[1 * 3 + q]) + Hi[a * 3 + 2] * H[2 * 3 + q]);
   }
 }
 
@@ -519,7 +542,7 @@ __global__ void __launch_bounds__(128) k_stress_mixed(DevState s, float dt) {
   xi_f32<DIM>(s, c, x, xi);
   cell_nodes_rel<DIM>(s, c, nid, Xr);
   dn_dx_all_f<DIM>(xi, Xr, D);
-  stress_update_mixed<DIM>(s, p, c, nid, D, dt);
+  stress_update_mixed<DIM>(s, MGlobalRow<DIM>{s, p}, c, nid, D, dt);
 }
 
 // --------------------------------------------------------------------- G2P
@@ -584,7 +607,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   if constexpr (STRESS) {
     float D[NV * DIM];
     dn_dx_all_f<DIM>(xi, Xr, D);
-    stress_update_mixed<DIM>(s, p, c, nid, D, dtf);
+    stress_update_mixed<DIM>(s, MGlobalRow<DIM>{s, p}, c, nid, D, dtf);
   }
   bool finite = true;
 #pragma unroll
@@ -599,6 +622,174 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
     if (nc != c) s.cell[p] = nc;
   } else {
     s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+  }
+}
+
+// USL G2P + stress update + locate with the block's particle slices staged in
+// shared memory by the bulk-copy engine (as k_g2p_staged of the FP64 path):
+// phase A x, u (FP64), v (FP32), cell, material, velocity-constraint slot;
+// phase B pdstrain (FP64), stress .. P (FP32), MohrCoulomb state (FP32).  The
+// arithmetic is k_g2p_mixed<DIM, true, FLIP>'s.
+static_assert(MSTAGE_T == PAD_PARTICLES, "staged slices are whole padded blocks");
+template <int DIM>
+constexpr size_t mixed_staged_smem_bytes(bool mc) {
+  return (size_t)PDX<DIM>::ND * MSTAGE_T * 8 + (size_t)(PM<DIM>::MASS + (mc ? SVF_N : 0)) * MSTAGE_T * 4 +
+         MSTAGE_T * (4 + 1 + 2);
+}
+
+template <int DIM, bool FLIP>
+__global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
+    k_g2p_mixed_staged(DevState s, double dt, float beta) {
+  constexpr int NV = Elem<DIM>::NV;
+  constexpr int T = MSTAGE_T;
+  constexpr int XROWS = PDX<DIM>::ND;   // x, u, pdstrain
+  constexpr int MROWS = PM<DIM>::MASS;  // v .. P
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar[2];
+  __shared__ int timed_out;
+  const bool mc = s.svf != nullptr;
+  double* xr = reinterpret_cast<double*>(smem);
+  float* mr = reinterpret_cast<float*>(xr + XROWS * T);
+  float* svr = mr + MROWS * T;
+  int32_t* scell = reinterpret_cast<int32_t*>(svr + (mc ? SVF_N * T : 0));
+  uint8_t* smat = reinterpret_cast<uint8_t*>(scell + T);
+  int16_t* spvc = reinterpret_cast<int16_t*>(smat + T);
+  const int t = threadIdx.x;
+  const int64_t p0 = (int64_t)blockIdx.x * T;
+  const int64_t np = s.np, nn = s.nn;
+  if (t == 0) {
+    timed_out = 0;
+    bulk::mbar_init(&bar[0], 1);
+    bulk::mbar_init(&bar[1], 1);
+    bulk::fence_barrier_init();
+  }
+  __syncthreads();
+  if (t == 0) {
+    bulk::mbar_arrive_expect_tx(&bar[0], 2 * DIM * T * 8 + DIM * T * 4 + T * (4 + 1 + 2));
+    for (int f = 0; f < 2 * DIM; ++f) bulk::load(xr + f * T, s.pf + f * np + p0, T * 8, &bar[0]);
+    for (int f = PM<DIM>::V; f < PM<DIM>::V + DIM; ++f)
+      bulk::load(mr + f * T, s.pm + f * np + p0, T * 4, &bar[0]);
+    bulk::load(scell, s.cell + p0, T * 4, &bar[0]);
+    bulk::load(smat, s.mat + p0, T, &bar[0]);
+    bulk::load(spvc, s.pvc + p0, T * 2, &bar[0]);
+    bulk::mbar_arrive_expect_tx(&bar[1], T * 8 + (MROWS - DIM + (mc ? SVF_N : 0)) * T * 4);
+    bulk::load(xr + PDX<DIM>::PDS * T, s.pf + PDX<DIM>::PDS * np + p0, T * 8, &bar[1]);
+    for (int f = PM<DIM>::V + DIM; f < MROWS; ++f)
+      bulk::load(mr + f * T, s.pm + f * np + p0, T * 4, &bar[1]);
+    if (mc)
+      for (int k = 0; k < SVF_N; ++k) bulk::load(svr + k * T, s.svf + k * np + p0, T * 4, &bar[1]);
+  }
+  const bool okA = bulk::mbar_wait(&bar[0], 0);
+  const int c = okA ? scell[t] : -1;
+  const int64_t p = p0 + t;
+  const MSmemRow r{xr + PDX<DIM>::PDS * T, mr, svr, t, okA ? (int)smat[t] : 0};
+  double xn[DIM];
+  const bool active = c >= 0;
+  float xi[DIM];
+  if (active) {
+    double x[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) x[d] = xr[(PDX<DIM>::X + d) * T + t];
+    float N[NV], Xr[NV * DIM];
+    int nid[NV];
+    xi_f32<DIM>(s, c, x, xi);
+    shapefn<DIM>(xi, N);
+    cell_nodes_rel<DIM>(s, c, nid, Xr);
+    float nvel[DIM], nacc[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.f;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * s.nfv[(int64_t)d * nn + nid[i]];
+      if constexpr (FLIP) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * s.nfv[(int64_t)(DIM + d) * nn + nid[i]];
+      }
+    }
+    const float dtf = (float)dt;
+    float v[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = r.m(PM<DIM>::V + d);
+    if constexpr (FLIP) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[d] += nacc[d] * dtf;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[d] = beta * v[d] + (1.f - beta) * nvel[d];
+    } else {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[d] = nvel[d];
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const double dx = (double)nvel[d] * dt;  // FP64 position / displacement update
+      xn[d] = x[d] + dx;
+      xr[(PDX<DIM>::X + d) * T + t] = xn[d];
+      xr[(PDX<DIM>::U + d) * T + t] += dx;
+    }
+    const int pv = spvc[t];
+    if (pv >= 0) {
+      const ParticleVC& vc = s.pvcs[pv];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        if (vc.mask & (1u << d)) v[d] = (float)vc.value[d];
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) r.m(PM<DIM>::V + d) = v[d];
+  }
+  const bool okB = okA && bulk::mbar_wait(&bar[1], 0);
+  if (!okA || !okB) timed_out = 1;
+  if (active && okB) {
+    // node ids and coordinates again rather than kept live across the wait
+    float Xr[NV * DIM], D[NV * DIM];
+    int nid[NV];
+    cell_nodes_rel<DIM>(s, c, nid, Xr);
+    dn_dx_all_f<DIM>(xi, Xr, D);
+    stress_update_mixed<DIM>(s, r, c, nid, D, (float)dt);
+  }
+  bulk::fence_shared_to_async();
+  __syncthreads();
+  if (timed_out) {
+    if (t == 0) {
+      raise_err(s, ERR_TIMEOUT);
+      bulk::mbar_wait(&bar[0], 0);
+      bulk::mbar_wait(&bar[1], 0);
+    }
+    return;
+  }
+  if (t == 0) {
+    for (int f = 0; f < XROWS; ++f) bulk::store(s.pf + f * np + p0, xr + f * T, T * 8);
+    for (int f = 0; f < MROWS; ++f) bulk::store(s.pm + f * np + p0, mr + f * T, T * 4);
+    if (mc)
+      for (int k = 0; k < SVF_N; ++k) bulk::store(s.svf + k * np + p0, svr + k * T, T * 4);
+    bulk::store_commit();
+  }
+  if (active) {
+    bool finite = true;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) finite = finite && isfinite(xn[d]);
+    if (!finite) {
+      raise_err(s, ERR_NONFINITE);
+      s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+    } else {
+      const int nc = locate_near<DIM>(s, xn, c);
+      if (nc >= 0) {
+        if (nc != c) s.cell[p] = nc;
+      } else {
+        s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+      }
+    }
+  }
+  if (t == 0) bulk::store_wait_all();
+}
+
+template <class K>
+void prefer_shared_memory(K kernel) {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    done = true;
   }
 }
 
@@ -623,10 +814,14 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     k_nodes_mixed<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
-    if (a.flip)
-      k_g2p_mixed<DIM, true, true><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
-    else
-      k_g2p_mixed<DIM, true, false><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
+    const size_t sm = mixed_staged_smem_bytes<DIM>(s.svf != nullptr);
+    if (a.flip) {
+      prefer_shared_memory(k_g2p_mixed_staged<DIM, true>);
+      k_g2p_mixed_staged<DIM, true><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
+    } else {
+      prefer_shared_memory(k_g2p_mixed_staged<DIM, false>);
+      k_g2p_mixed_staged<DIM, false><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
+    }
     pr.end(K_G2P, st);
   } else {  // USF
     pr.begin(K_P2G, st);
