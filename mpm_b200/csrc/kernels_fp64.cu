@@ -15,6 +15,8 @@
 // neighbourhood (usually none).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "mpm_bulk.cuh"
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
@@ -24,6 +26,9 @@
 // the two particle kernels (occupancy versus spills, tuned on the B200).
 #ifndef MPM_G2P_MIN_BLOCKS
 #define MPM_G2P_MIN_BLOCKS 4  // 1.41 -> 1.01 ms per 4M-particle step despite spills
+#endif
+#ifndef MPM_MC_RETURN_MIN_BLOCKS
+#define MPM_MC_RETURN_MIN_BLOCKS 4
 #endif
 #ifndef MPM_P2G_MIN_BLOCKS
 #define MPM_P2G_MIN_BLOCKS 2  // more blocks spill the 40 lane accumulators: slower
@@ -351,6 +356,7 @@ __global__ void __launch_bounds__(256) k_nodes(DevState s, double dt, double dam
 struct GlobalRow {
   const DevState& s;
   int64_t p;
+  __device__ __forceinline__ int64_t index() const { return p; }
   __device__ __forceinline__ double& f(int field) const { return s.pf[(int64_t)field * s.np + p]; }
   __device__ __forceinline__ double& sv(int k) const { return s.sv[(int64_t)k * s.np + p]; }
   __device__ __forceinline__ int mat() const { return s.mat[p]; }
@@ -361,6 +367,8 @@ struct SmemRow {
   double* svr;   // [SV_N][STAGE_T]
   int t;
   int m;
+  int64_t p;
+  __device__ __forceinline__ int64_t index() const { return p; }
   __device__ __forceinline__ double& f(int field) const { return rows[field * STAGE_T + t]; }
   __device__ __forceinline__ double& sv(int k) const { return svr[k * STAGE_T + t]; }
   __device__ __forceinline__ int mat() const { return m; }
@@ -454,18 +462,30 @@ __device__ __forceinline__ void stress_update(const DevState& s, const Row& r, i
   for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = r.f(PF<DIM>::S + k);
   const MaterialParams& mp = s.mats[r.mat()];
   double out[6];
+  bool deferred = false;
   if (mp.type == 0) {
     material_compute_stress(mp, sig, dstrain, rho, nullptr, out);
   } else {
     double sv[SV_N];
 #pragma unroll
     for (int k = 0; k < SV_N; ++k) sv[k] = r.sv(k);
-    material_compute_stress(mp, sig, dstrain, rho, sv, out);
+    if (mc_stress<double, double, true>(mp, sig, dstrain, rho, sv, sv[SV_PD], out) == MC_DEFERRED) {
+      // plastic: the return runs in k_mc_return from the unchanged stress and state
+      deferred = true;
+      const unsigned i = defer_slot(s);
+      s.plist[i] = (int32_t)r.index();
 #pragma unroll
-    for (int k = 0; k < SV_N; ++k) r.sv(k) = sv[k];
+      for (int k = 0; k < 6; ++k) s.pbuf[(int64_t)k * s.np + i] = dstrain[k];
+      s.pbuf[(int64_t)6 * s.np + i] = rho;
+    } else {
+#pragma unroll
+      for (int k = 0; k < SV_N; ++k) r.sv(k) = sv[k];
+    }
   }
+  if (!deferred) {
 #pragma unroll
-  for (int k = 0; k < PF<DIM>::NS; ++k) r.f(PF<DIM>::S + k) = out[k];
+    for (int k = 0; k < PF<DIM>::NS; ++k) r.f(PF<DIM>::S + k) = out[k];
+  }
   if constexpr (DIM == 2) {
     double F[4];
 #pragma unroll
@@ -657,7 +677,7 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
   const bool okA = bulk::mbar_wait(&bar[0], 0);
   const int c = okA ? scell[t] : -1;
   const int64_t p = p0 + t;
-  const SmemRow r{rows, svr, t, okA ? (int)smat[t] : 0};
+  const SmemRow r{rows, svr, t, okA ? (int)smat[t] : 0, p0 + t};
   double xn[DIM];
   const bool active = c >= 0;
   double xi[DIM];
@@ -758,6 +778,31 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
   if (t == 0) bulk::store_wait_all();
 }
 
+// The MohrCoulomb returns deferred by stress_update, one thread per listed
+// particle (grid-stride), from the particle's stress and state before the
+// step's update: the same call, with the same inputs, as the undeferred update.
+template <int DIM>
+__global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return(DevState s) {
+  const unsigned n = *s.nplastic;
+  const int64_t np = s.np;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int64_t p = s.plist[i];
+    double sig[6] = {0, 0, 0, 0, 0, 0}, de[6], sv[SV_N], out[6];
+#pragma unroll
+    for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = s.pf[(int64_t)(PF<DIM>::S + k) * np + p];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) de[k] = s.pbuf[(int64_t)k * np + i];
+    const double rho = s.pbuf[(int64_t)6 * np + i];
+#pragma unroll
+    for (int k = 0; k < SV_N; ++k) sv[k] = s.sv[(int64_t)k * np + p];
+    material_compute_stress(s.mats[s.mat[p]], sig, de, rho, sv, out);
+#pragma unroll
+    for (int k = 0; k < SV_N; ++k) s.sv[(int64_t)k * np + p] = sv[k];
+#pragma unroll
+    for (int k = 0; k < PF<DIM>::NS; ++k) s.pf[(int64_t)(PF<DIM>::S + k) * np + p] = out[k];
+  }
+}
+
 // Exhaustive search for particles not in their cell or its neighbours
 // (mesh.tcc:1136-1148 with one thread: the first cell in id order that
 // contains the point).  Grid-stride over the lost list; usually empty.
@@ -837,7 +882,15 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
   if (np == 0) return;
   constexpr int LPC = DIM == 3 ? 2 : 1;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
+  if (s.sv) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
   const unsigned pb128 = nblocks(np, 128), nb = nblocks(nn, 256);
+  const unsigned mcb = (unsigned)std::min<int64_t>(nblocks(np, 128), 148 * 8);
+  auto mc_returns = [&]() {
+    if (!s.sv) return;
+    pr.begin(K_MC_RETURN, st);
+    k_mc_return<DIM><<<mcb, 128, 0, st>>>(s);
+    pr.end(K_MC_RETURN, st);
+  };
   const unsigned cb = nblocks(s.ncells * LPC, 128);
   pr.begin(K_SORT, st);
   counting_sort_impl(s, st);
@@ -859,6 +912,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
       k_g2p_staged<DIM, false><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
     }
     pr.end(K_G2P, st);
+    mc_returns();
   } else {  // USF
     pr.begin(K_P2G, st);
     k_p2g_cells<DIM, 0><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
@@ -869,6 +923,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     pr.begin(K_STRESS, st);
     k_stress<DIM><<<pb128, 128, 0, st>>>(s, a.dt);
     pr.end(K_STRESS, st);
+    mc_returns();
     pr.begin(K_P2G_FORCES, st);
     k_p2g_cells<DIM, 1><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
     pr.end(K_P2G_FORCES, st);

@@ -7,13 +7,13 @@
 //   * P2G accumulates each cell slot with Kahan-compensated FP32 sums, the node
 //     adds its (at most eight) cell partials in FP64 and divides momentum by
 //     mass in FP64;
-//   * the MohrCoulomb return map runs in FP32 (its stress invariants and Lode
-//     angle derivatives in FP64, see mc_invariants) and is redone in FP64 for
-//     points at the apex of the yield surface (deviatoric trial stress below
-//     1e-2 of the stress magnitude), for returns that remove more than 90 % of
-//     the trial stress (the subtraction would cancel in FP32) and when the
-//     FP32 return is not finite; the plastic deviatoric strain is accumulated
-//     in FP64;
+//   * the MohrCoulomb elastic predictor and yield check run in FP32 (stress
+//     invariants in FP64, see mc_invariants); plastic returns, points at the
+//     apex and separated points run in FP64 in a dense second kernel (an FP32
+//     return cancels when it removes most of the trial stress and near the
+//     apex, and plastic points are few and scattered, so batching them keeps
+//     the elastic lanes of a warp from waiting on the return iterations);
+//     the plastic deviatoric strain is kept in FP64;
 //   * F, volume and density are stored as deviations (H = F - I,
 //     P = V / V0 - 1) so that FP32 keeps the 1e-9 per-step increments.
 // Same step structure as the FP64 path (kernels_fp64.cu): counting sort,
@@ -27,6 +27,9 @@
 
 #ifndef MPM_MIXED_G2P_MIN_BLOCKS
 #define MPM_MIXED_G2P_MIN_BLOCKS 4
+#endif
+#ifndef MPM_MC_RETURN_MIN_BLOCKS
+#define MPM_MC_RETURN_MIN_BLOCKS 4
 #endif
 #ifndef MPM_MIXED_P2G_MIN_BLOCKS
 #define MPM_MIXED_P2G_MIN_BLOCKS 3
@@ -303,10 +306,14 @@ __global__ void __launch_bounds__(256) k_nodes_mixed(DevState s, double dt, doub
 }
 
 // ------------------------------------------------------- stress and strain
-// MohrCoulomb in FP32, redone in FP64 at the apex or when not finite.
-__device__ __forceinline__ void mc_update_mixed(const MaterialParams& md, const MaterialT<float>& mf,
-                                                const float* sig, const float* de, float rho,
-                                                float* svf, double& pd, float* out) {
+// MohrCoulomb elastic predictor and yield check in FP32 (invariants in FP64):
+// true with out and svf updated when the trial stress is elastic and away
+// from the apex of the yield surface (deviatoric trial stress above 1e-2 of
+// the stress magnitude); false for every other point (plastic, apex,
+// separated), which the caller defers to the FP64 return of
+// k_mc_return_mixed with its inputs unchanged.
+__device__ __forceinline__ bool mc_elastic_mixed(const MaterialT<float>& mf, const float* sig,
+                                                 const float* de, float rho, float* svf, float* out) {
   float trial[6];
   {
     float t[6];
@@ -318,54 +325,30 @@ __device__ __forceinline__ void mc_update_mixed(const MaterialParams& md, const 
 #pragma unroll
   for (int i = 0; i < 6; ++i) smax = fmaxf(smax, fabsf(trial[i]));
   const float rho_dev = sqrtf(2.f * mu_j2(trial));
-  bool fp64 = rho_dev <= 1e-2f * smax;
-  if (!fp64) {
-    float sv[SV_N];
+  if (rho_dev <= 1e-2f * smax) return false;
+  float sv[SV_N];
 #pragma unroll
-    for (int k = 0; k < SVF_N; ++k) sv[k] = svf[k];
-    sv[SV_PD] = 0.f;
-    double pd_try = pd;
-    bool ok = mc_compute_stress<float, double>(mf, sig, de, rho, sv, pd_try, out);
-    if (ok && sv[SV_YIELD] != 0.f) {
-      // a return that removes most of the trial stress cancels: redo in FP64
-      float omax = 0.f;
+  for (int k = 0; k < SVF_N; ++k) sv[k] = svf[k];
+  sv[SV_PD] = 0.f;
+  double pd_unused = 0.0;
+  if (mc_stress<float, double, true>(mf, sig, de, rho, sv, pd_unused, out) != MC_OK ||
+      sv[SV_YIELD] != 0.f)
+    return false;
 #pragma unroll
-      for (int i = 0; i < 6; ++i) omax = fmaxf(omax, fabsf(out[i]));
-      ok = omax >= 0.1f * smax;
-    }
-    if (ok) {
-#pragma unroll
-      for (int k = 0; k < SVF_N; ++k) svf[k] = sv[k];
-      pd = pd_try;
-      return;
-    }
-    fp64 = true;
-  }
-  double sd[6], ded[6], svd[SV_N], od[6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    sd[i] = (double)sig[i];
-    ded[i] = (double)de[i];
-  }
-#pragma unroll
-  for (int k = 0; k < SVF_N; ++k) svd[k] = (double)svf[k];
-  svd[SV_PD] = pd;
-  mc_compute_stress<double, double>(md, sd, ded, (double)rho, svd, svd[SV_PD], od);
-#pragma unroll
-  for (int i = 0; i < 6; ++i) out[i] = (float)od[i];
-#pragma unroll
-  for (int k = 0; k < SVF_N; ++k) svf[k] = (float)svd[k];
-  pd = svd[SV_PD];
+  for (int k = 0; k < SVF_N; ++k) svf[k] = sv[k];
+  return true;
 }
 
 // One particle's mixed-precision fields in global memory (MGlobalRow) or in
 // the block's shared-memory staging (MSmemRow, MSTAGE_T particles per row):
 // m(f) the FP32 field f of PM, svf(k) the FP32 MohrCoulomb state, pd() the
-// FP64 plastic deviatoric strain.
+// FP64 plastic deviatoric strain (read only by the deferred returns, which
+// work in global memory).
 template <int DIM>
 struct MGlobalRow {
   const DevState& s;
   int64_t p;
+  __device__ __forceinline__ int64_t index() const { return p; }
   __device__ __forceinline__ float& m(int f) const { return s.pm[(int64_t)f * s.np + p]; }
   __device__ __forceinline__ float& svf(int k) const { return s.svf[(int64_t)k * s.np + p]; }
   __device__ __forceinline__ double& pd() const { return s.pf[(int64_t)PDX<DIM>::PDS * s.np + p]; }
@@ -373,14 +356,14 @@ struct MGlobalRow {
 };
 constexpr int MSTAGE_T = 128;  // particles per staged block (= PAD_PARTICLES)
 struct MSmemRow {
-  double* pdr;   // [MSTAGE_T] pdstrain
   float* mrows;  // [PM field][MSTAGE_T]
   float* svr;    // [SVF_N][MSTAGE_T]
   int t;
   int mi;
+  int64_t p;
+  __device__ __forceinline__ int64_t index() const { return p; }
   __device__ __forceinline__ float& m(int f) const { return mrows[f * MSTAGE_T + t]; }
   __device__ __forceinline__ float& svf(int k) const { return svr[k * MSTAGE_T + t]; }
-  __device__ __forceinline__ double& pd() const { return pdr[t]; }
   __device__ __forceinline__ int mat() const { return mi; }
 };
 
@@ -463,6 +446,7 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, const Row
   for (int k = 0; k < NS; ++k) sig[k] = r.m(PM<DIM>::S + k);
   const int mi = r.mat();
   float out[6];
+  bool deferred = false;
   if (s.mats_f[mi].type == 0) {
     float t[6];
     de_mul(s.mats_f[mi], dstrain, t);
@@ -472,17 +456,26 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, const Row
     float svf[SVF_N];
 #pragma unroll
     for (int k = 0; k < SVF_N; ++k) svf[k] = r.svf(k);
-    double pd = r.pd();
-    mc_update_mixed(s.mats[mi], s.mats_f[mi], sig, dstrain, rho, svf, pd, out);
-    r.pd() = pd;
-    const int first = s.mats_f[mi].softening ? 0 : SV_EPS;  // phi..tc change only with softening
-    r.svf(SV_YIELD) = svf[SV_YIELD];
+    if (mc_elastic_mixed(s.mats_f[mi], sig, dstrain, rho, svf, out)) {
+      const int first = s.mats_f[mi].softening ? 0 : SV_EPS;  // phi..tc change only with softening
+      r.svf(SV_YIELD) = svf[SV_YIELD];
 #pragma unroll
-    for (int k = 1; k < SVF_N; ++k)
-      if (k >= first) r.svf(k) = svf[k];
+      for (int k = 1; k < SVF_N; ++k)
+        if (k >= first) r.svf(k) = svf[k];
+    } else {
+      // plastic, apex or separated: the FP64 update of k_mc_return_mixed
+      deferred = true;
+      const unsigned i = defer_slot(s);
+      s.plist[i] = (int32_t)r.index();
+#pragma unroll
+      for (int k = 0; k < 6; ++k) s.pbuf_f[(int64_t)k * s.np + i] = dstrain[k];
+      s.pbuf_f[(int64_t)6 * s.np + i] = rho;
+    }
   }
+  if (!deferred) {
 #pragma unroll
-  for (int k = 0; k < NS; ++k) r.m(PM<DIM>::S + k) = out[k];
+    for (int k = 0; k < NS; ++k) r.m(PM<DIM>::S + k) = out[k];
+  }
   // F = F_inc F as H = H + Hi + Hi H
   if constexpr (DIM == 2) {
     float H[4];
@@ -628,12 +621,12 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
 // USL G2P + stress update + locate with the block's particle slices staged in
 // shared memory by the bulk-copy engine (as k_g2p_staged of the FP64 path):
 // phase A x, u (FP64), v (FP32), cell, material, velocity-constraint slot;
-// phase B pdstrain (FP64), stress .. P (FP32), MohrCoulomb state (FP32).  The
-// arithmetic is k_g2p_mixed<DIM, true, FLIP>'s.
+// phase B stress .. P (FP32), MohrCoulomb state (FP32).  The arithmetic is
+// k_g2p_mixed<DIM, true, FLIP>'s.
 static_assert(MSTAGE_T == PAD_PARTICLES, "staged slices are whole padded blocks");
 template <int DIM>
 constexpr size_t mixed_staged_smem_bytes(bool mc) {
-  return (size_t)PDX<DIM>::ND * MSTAGE_T * 8 + (size_t)(PM<DIM>::MASS + (mc ? SVF_N : 0)) * MSTAGE_T * 4 +
+  return (size_t)2 * DIM * MSTAGE_T * 8 + (size_t)(PM<DIM>::MASS + (mc ? SVF_N : 0)) * MSTAGE_T * 4 +
          MSTAGE_T * (4 + 1 + 2);
 }
 
@@ -642,7 +635,7 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
     k_g2p_mixed_staged(DevState s, double dt, float beta) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int T = MSTAGE_T;
-  constexpr int XROWS = PDX<DIM>::ND;   // x, u, pdstrain
+  constexpr int XROWS = 2 * DIM;       // x, u
   constexpr int MROWS = PM<DIM>::MASS;  // v .. P
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar[2];
@@ -666,14 +659,13 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   __syncthreads();
   if (t == 0) {
     bulk::mbar_arrive_expect_tx(&bar[0], 2 * DIM * T * 8 + DIM * T * 4 + T * (4 + 1 + 2));
-    for (int f = 0; f < 2 * DIM; ++f) bulk::load(xr + f * T, s.pf + f * np + p0, T * 8, &bar[0]);
+    for (int f = 0; f < XROWS; ++f) bulk::load(xr + f * T, s.pf + f * np + p0, T * 8, &bar[0]);
     for (int f = PM<DIM>::V; f < PM<DIM>::V + DIM; ++f)
       bulk::load(mr + f * T, s.pm + f * np + p0, T * 4, &bar[0]);
     bulk::load(scell, s.cell + p0, T * 4, &bar[0]);
     bulk::load(smat, s.mat + p0, T, &bar[0]);
     bulk::load(spvc, s.pvc + p0, T * 2, &bar[0]);
-    bulk::mbar_arrive_expect_tx(&bar[1], T * 8 + (MROWS - DIM + (mc ? SVF_N : 0)) * T * 4);
-    bulk::load(xr + PDX<DIM>::PDS * T, s.pf + PDX<DIM>::PDS * np + p0, T * 8, &bar[1]);
+    bulk::mbar_arrive_expect_tx(&bar[1], (MROWS - DIM + (mc ? SVF_N : 0)) * T * 4);
     for (int f = PM<DIM>::V + DIM; f < MROWS; ++f)
       bulk::load(mr + f * T, s.pm + f * np + p0, T * 4, &bar[1]);
     if (mc)
@@ -682,7 +674,7 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   const bool okA = bulk::mbar_wait(&bar[0], 0);
   const int c = okA ? scell[t] : -1;
   const int64_t p = p0 + t;
-  const MSmemRow r{xr + PDX<DIM>::PDS * T, mr, svr, t, okA ? (int)smat[t] : 0};
+  const MSmemRow r{mr, svr, t, okA ? (int)smat[t] : 0, p0 + t};
   double xn[DIM];
   const bool active = c >= 0;
   float xi[DIM];
@@ -793,6 +785,50 @@ void prefer_shared_memory(K kernel) {
   }
 }
 
+// The MohrCoulomb updates deferred by stress_update_mixed, one thread per
+// listed particle: the full FP64 update (mohr_coulomb.tcc:348-513) from the
+// FP32 stress and state before the step's update, rounded back to FP32.
+template <int DIM>
+__global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return_mixed(DevState s) {
+  const unsigned n = *s.nplastic;
+  const int64_t np = s.np;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int64_t p = s.plist[i];
+    const MGlobalRow<DIM> r{s, p};
+    const int mi = s.mat[p];
+    float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, de[6], svf[SVF_N], out[6];
+#pragma unroll
+    for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = r.m(PM<DIM>::S + k);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) de[k] = s.pbuf_f[(int64_t)k * np + i];
+    const float rho = s.pbuf_f[(int64_t)6 * np + i];
+#pragma unroll
+    for (int k = 0; k < SVF_N; ++k) svf[k] = r.svf(k);
+    double sd[6], ded[6], svd[SV_N], od[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      sd[k] = (double)sig[k];
+      ded[k] = (double)de[k];
+    }
+#pragma unroll
+    for (int k = 0; k < SVF_N; ++k) svd[k] = (double)svf[k];
+    svd[SV_PD] = r.pd();
+    mc_compute_stress<double, double>(s.mats[mi], sd, ded, (double)rho, svd, svd[SV_PD], od);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) out[k] = (float)od[k];
+#pragma unroll
+    for (int k = 0; k < SVF_N; ++k) svf[k] = (float)svd[k];
+    r.pd() = svd[SV_PD];
+    const int first = s.mats_f[mi].softening ? 0 : SV_EPS;  // phi..tc change only with softening
+    r.svf(SV_YIELD) = svf[SV_YIELD];
+#pragma unroll
+    for (int k = 1; k < SVF_N; ++k)
+      if (k >= first) r.svf(k) = svf[k];
+#pragma unroll
+    for (int k = 0; k < PF<DIM>::NS; ++k) r.m(PM<DIM>::S + k) = out[k];
+  }
+}
+
 inline unsigned nblk(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 template <int DIM>
@@ -801,7 +837,15 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
   if (np == 0) return;
   constexpr int LPC = DIM == 3 ? 2 : 1;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
+  if (s.svf) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
   const unsigned pb = nblk(np, 128), nb = nblk(nn, 256), cb = nblk(s.ncells * LPC, 128);
+  const unsigned mcb = (unsigned)(pb < 148 * 8 ? pb : 148 * 8);
+  auto mc_returns = [&]() {
+    if (!s.svf) return;
+    pr.begin(K_MC_RETURN, st);
+    k_mc_return_mixed<DIM><<<mcb, 128, 0, st>>>(s);
+    pr.end(K_MC_RETURN, st);
+  };
   const float g0 = (float)a.g[0], g1 = (float)a.g[1], g2 = (float)a.g[2];
   pr.begin(K_SORT, st);
   counting_sort(s, st);
@@ -823,6 +867,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
       k_g2p_mixed_staged<DIM, false><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
     }
     pr.end(K_G2P, st);
+    mc_returns();
   } else {  // USF
     pr.begin(K_P2G, st);
     k_p2g_cells_mixed<DIM, 0><<<cb, 128, 0, st>>>(s, g0, g1, g2);
@@ -833,6 +878,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     pr.begin(K_STRESS, st);
     k_stress_mixed<DIM><<<pb, 128, 0, st>>>(s, (float)a.dt);
     pr.end(K_STRESS, st);
+    mc_returns();
     pr.begin(K_P2G_FORCES, st);
     k_p2g_cells_mixed<DIM, 1><<<cb, 128, 0, st>>>(s, g0, g1, g2);
     pr.end(K_P2G_FORCES, st);

@@ -4,6 +4,7 @@
 // compiles them with its own floating-point contraction setting.
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "mpm_math.cuh"
@@ -18,6 +19,18 @@ struct PV {  // value offsets within a cell-slot partial
 };
 
 __device__ __forceinline__ void raise_err(const DevState& s, unsigned bits) { atomicOr(s.err, bits); }
+
+// A slot in the deferred MohrCoulomb return list (one atomic per group of
+// lanes that defer together).  Each particle defers at most once per step, so
+// slots stay below the particle count.
+__device__ __forceinline__ unsigned defer_slot(const DevState& s) {
+  namespace cg = cooperative_groups;
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(s.nplastic, g.size());
+  base = g.shfl(base, 0);
+  return base + g.thread_rank();
+}
 
 template <int DIM>
 __device__ __forceinline__ void load_x(const DevState& s, int64_t p, double* x) {

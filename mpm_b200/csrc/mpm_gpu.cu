@@ -76,7 +76,7 @@ namespace mpm_b200 {
 const char* kernel_name(int kid) {
   static const char* names[K_NKERNELS] = {"sort",  "p2g",   "nodes_velocity", "stress",
                                           "p2g_forces", "nodes_acceleration", "g2p",
-                                          "locate_fallback"};
+                                          "mc_return", "locate_fallback"};
   return (kid >= 0 && kid < K_NKERNELS) ? names[kid] : "?";
 }
 
@@ -195,7 +195,9 @@ struct mpm_gpu_solver {
   DevBuf<uint8_t> d_mat, d_active;
   DevBuf<int16_t> d_pvc;
   DevBuf<CellGeom> d_geom;
-  DevBuf<unsigned> d_words;  // [0] nlost, [1] err
+  DevBuf<unsigned> d_words;  // [0] nlost, [1] err, [2] nplastic
+  DevBuf<int32_t> d_plist;
+  DevBuf<double> d_pbuf;
   DevBuf<MaterialParams> d_mats;
   DevBuf<double> d_axis[3];
   DevBuf<double> d_dndx_c, d_partials;
@@ -547,8 +549,8 @@ void upload_mesh(mpm_gpu_t h) {
   h->d_active.alloc(h->nnodes);
   ck(cudaMemsetAsync(h->d_active.p, 0, h->nnodes, st), "memset");
   ck(cudaMemsetAsync(h->d_nf.p, 0, sizeof(double) * h->nnf() * h->nnodes, st), "memset");
-  h->d_words.alloc(2);
-  ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 2, st), "memset");
+  h->d_words.alloc(4);
+  ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 4, st), "memset");
   if (h->structured)
     for (int d = 0; d < 3; ++d) h->d_axis[d].upload(h->axis[d].data(), h->axis[d].size(), st);
   if (h->mixed) {
@@ -656,6 +658,12 @@ void allocate_particles(mpm_gpu_t h) {
   for (auto& m : h->mats) h->any_mc = h->any_mc || m.type == 1;
   h->d_sv.free();
   h->d_svf.free();
+  h->d_plist.free();
+  h->d_pbuf.free();
+  if (h->any_mc) {
+    h->d_plist.alloc(np);
+    h->d_pbuf.alloc((size_t)7 * np);
+  }
   if (h->any_mc && h->mixed)
     h->d_svf.alloc((size_t)SVF_N * np);
   else if (h->any_mc)
@@ -705,6 +713,10 @@ void refresh_state(mpm_gpu_t h) {
   s.lost = h->d_lost.p;
   s.nlost = h->d_words.p;
   s.err = h->d_words.p + 1;
+  s.nplastic = h->d_words.p + 2;
+  s.plist = h->any_mc ? h->d_plist.p : nullptr;
+  s.pbuf = h->any_mc ? h->d_pbuf.p : nullptr;
+  s.pbuf_f = h->any_mc ? reinterpret_cast<float*>(h->d_pbuf.p) : nullptr;
   s.mats = h->d_mats.p;
   s.bcs = h->d_bcs.p;
   s.pvcs = h->d_pvcs.p;

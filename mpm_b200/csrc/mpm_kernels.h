@@ -29,6 +29,7 @@ enum KernelId {
   K_P2G_FORCES,     // USF: per-cell P2G of the forces
   K_NODES_ACC,      // USF: nodal acceleration / velocity update
   K_G2P,            // G2P (+ USL stress update) + locate
+  K_MC_RETURN,      // MohrCoulomb plastic returns deferred by the stress update
   K_LOCATE,         // exhaustive locate for particles that left their neighbourhood
   K_NKERNELS
 };

@@ -622,14 +622,23 @@ MPM_HD float huge_value<float>() {
   return 3.402823466e38f;
 }
 
+// Outcome of mc_stress: the stress is in out (MC_OK), a return iteration left
+// it non-finite (MC_NONFINITE), or the trial stress is plastic and DEFER asked
+// to stop there (MC_DEFERRED: out, sv and pdstrain hold nothing to keep; the
+// caller redoes the whole update later, with the same inputs).
+enum { MC_OK = 0, MC_NONFINITE = 1, MC_DEFERRED = 2 };
+
 // MohrCoulomb<Tdim>::compute_stress (mohr_coulomb.tcc:348-513), stress_rate
 // None (infinitesimal_elasto_plastic.tcc:2-25).  sv holds the state variables
 // in the reference order; the plastic deviatoric strain (slot SV_PD) is kept in
-// PD (double on every path).  Returns false when a return iteration left the
-// state non-finite (the caller of the mixed path then redoes the point in FP64).
-template <typename R, typename PD>
-MPM_HD bool mc_compute_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R density,
-                              R* sv, PD& pdstrain_io, R* out) {
+// PD (double on every path).  With DEFER the elastic predictor and the yield
+// check run, and a plastic point returns MC_DEFERRED before the corrector: the
+// step kernels finish elastic points in place and hand plastic ones to a
+// dense kernel, so that the few plastic lanes of a warp do not hold the
+// elastic ones through the return iterations.
+template <typename R, typename PD, bool DEFER>
+MPM_HD int mc_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R density, R* sv,
+                     PD& pdstrain_io, R* out) {
   const R critical_density = m.min_packing * m.grain_density;
   const R pdstrain = R(pdstrain_io);
   if (m.softening && pdstrain > m.pd_peak) {
@@ -660,7 +669,7 @@ MPM_HD bool mc_compute_stress(const MaterialT<R>& m, const R* stress, const R* d
     sv[SV_YIELD] = R(3);
 #pragma unroll
     for (int i = 0; i < 6; ++i) out[i] = R(0);
-    return true;
+    return MC_OK;
   }
   const FrictionTrig<R> ft = friction_trig(m, sv);
   LodeTrig<R> lt;
@@ -671,8 +680,9 @@ MPM_HD bool mc_compute_stress(const MaterialT<R>& m, const R* stress, const R* d
     sv[SV_YIELD] = R(0);
 #pragma unroll
     for (int i = 0; i < 6; ++i) out[i] = trial[i];
-    return true;
+    return MC_OK;
   }
+  if constexpr (DEFER) return MC_DEFERRED;
   const R Tolerance = R(1E-1);
   R softening_trial = R(0), dp_dq_trial = R(0);
   R df_trial[6], dp_trial[6];
@@ -729,7 +739,14 @@ MPM_HD bool mc_compute_stress(const MaterialT<R>& m, const R* stress, const R* d
     out[i] = upd[i];
     finite = finite && (upd[i] - upd[i] == R(0));
   }
-  return finite;
+  return finite ? MC_OK : MC_NONFINITE;
+}
+
+// The full update; false when the return left the stress non-finite.
+template <typename R, typename PD>
+MPM_HD bool mc_compute_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R density,
+                              R* sv, PD& pdstrain_io, R* out) {
+  return mc_stress<R, PD, false>(m, stress, dstrain, density, sv, pdstrain_io, out) == MC_OK;
 }
 
 // Material<Tdim>::compute_stress dispatch (material.h:97-106)

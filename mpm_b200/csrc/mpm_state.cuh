@@ -126,6 +126,12 @@ struct DevState {
 
   int32_t* lost = nullptr;       // [np] particles not found in cell or neighbours
   unsigned* nlost = nullptr;
+  // particles whose MohrCoulomb trial stress is plastic this step, with the
+  // inputs of their deferred return: strain increment (6) and density
+  int32_t* plist = nullptr;      // [np]
+  double* pbuf = nullptr;        // [7][np] (FP64 path)
+  float* pbuf_f = nullptr;       // [7][np] (mixed path, same allocation)
+  unsigned* nplastic = nullptr;
   unsigned* err = nullptr;       // ErrorBits
 
   // mixed precision (null on the FP64 path)
