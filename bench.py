@@ -3,12 +3,16 @@
 Workload (default): the 3D granular column collapse -- 200x100x50 hex8 cells
 of 0.01 m, MohrCoulomb (E=1e7, nu=0.3, phi=30, c=0, psi=0, rho=1800), USL,
 FLIP, frictional floor mu=0.4, dt=2e-6, 2x2x2 particles per cell in the block
-[0,1]x[0,1]x[0,0.5] (4,000,000 particles).  Synthetic seeded inputs.
+[0,1]x[0,1]x[0,0.5] (4,000,000 particles), K0 geostatic initial stress.
+Synthetic seeded inputs.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision mixed|fp64]
 
 One JSON line on stdout (rank 0).  ``value`` is device-timed (CUDA events on
-the solver's stream, state resident in HBM); ``e2e`` goes through the public
+the solver's stream, state resident in HBM) for the chosen precision (mixed by
+default); ``fp64`` holds the FP64 path timed on the same workload and steps and
+the mixed path's per-field deviation from it; ``e2e`` goes through the public
 API with host arrays (load -> K steps -> read back); ``roofline`` reports the
 dominant kernel's algorithmic bytes per launch over its event-timed average
 duration; ``cpu_baseline`` times the CPU oracle on a bounded sample.
@@ -30,21 +34,25 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic bytes of the FP64 kernels, 3D MohrCoulomb USL:
-# per particle for the particle kernels, per node for the node kernel.
+# Algorithmic bytes per particle of the particle kernels, 3D MohrCoulomb USL
+# (compulsory particle-state traffic: every field read once, every field the
+# kernel changes written once; nodal gathers hit L2 and are not counted).
 BYTES_PER_PARTICLE = {
-    # x 24, cell 4, mass 8, v 24, volume 8, stress 48 read
-    "p2g": 116,
-    # read x u v 72, stress strain 96, F 72, volume density 16, cell 4,
-    # material 1, pvc 2, MC state 72; write x u v 72, stress strain 96,
-    # F 72, volume density 16, MC state 72
-    "g2p": 335 + 328,
+    "fp64": {
+        # read x u v 72, stress strain 96, F 72, volume density 16, cell 4,
+        # material 1, constraint slot 2, MC state 72
+        "g2p": 335 + 296,   # write x u v stress strain F V rho 256, MC state that changes 40
+        "p2g": 116,         # read x 24, v 24, mass 8, stress 48, volume 8, order 4
+    },
+    "mixed": {
+        # read x u 48 (FP64), v stress strain H V0 rho0 P 108 (FP32), MC state
+        # 32, cell material slot 7; write x u 48, v stress strain H P 100, MC 16
+        "g2p": 195 + 164,
+        "p2g": 68,          # read x 24, v 12, mass 4, stress 24, V0 P 8 (FP32)
+    },
 }
 DTYPES = {"fp64": "f64", "mixed": "f32+f64"}
-BYTES_PER_ACTIVE_NODE = {
-    # read mass, momentum, forces 80, flags 5; write velocity, acceleration 48
-    "nodes_velocity": 133,
-}
+FIELDS = ("u", "v", "stress", "strain", "F", "volume", "density")
 
 
 def parse():
@@ -54,7 +62,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--block", default="100,100,50", help="particle block in cells")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--no-fp64-arm", action="store_true",
+                    help="skip the FP64 run reported beside the mixed one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     return ap.parse_args()
@@ -224,6 +234,39 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def time_arm(prob, precision, args, world, dev, clocks=None):
+    """Build a solver, run the warm-up, time K steps on the device."""
+    from mpm_b200 import problems as P
+    t0 = time.perf_counter()
+    s = P.build_solver(prob, precision=precision, device=dev)
+    setup_s = time.perf_counter() - t0
+    s.step(args.warmup)
+    barrier(world)
+    s.set_profiling(True)
+    launches0 = s.launch_count
+    if clocks:
+        clocks.mark_start()
+    ms = s.step_timed(args.steps)
+    if clocks:
+        clocks.mark_end()
+    launches = s.launch_count - launches0
+    prof = s.kernel_profile()
+    s.set_profiling(False)
+    ms = max_over_ranks(ms, world)
+    return s, ms, prof, launches, setup_s
+
+
+def field_errors(a, b):
+    """max |a - b| / max |b| per field (F compared as F - I)."""
+    out = {}
+    for k in FIELDS:
+        x, y = np.asarray(a[k], float), np.asarray(b[k], float)
+        if k == "F":
+            x, y = x - np.eye(3).reshape(1, 9), y - np.eye(3).reshape(1, 9)
+        out[k] = float(np.max(np.abs(x - y)) / max(np.max(np.abs(y)), 1e-300))
+    return out
+
+
 def main():
     args = parse()
     rank, world = dist_init(args.gpus)
@@ -232,29 +275,27 @@ def main():
         return
     from mpm_b200 import problems as P
     block = tuple(int(v) for v in args.block.split(","))
-    t0 = time.perf_counter()
     prob = P.config_b(block=block)
     dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
-    s = P.build_solver(prob, precision=args.precision, device=dev)
-    setup_s = time.perf_counter() - t0
-    n = s.nparticles
-    s.step(args.warmup)
-    barrier(world)
     clocks = Clocks(dev)
-    s.set_profiling(True)
-    launches0 = s.launch_count
-    clocks.mark_start()
-    ms = s.step_timed(args.steps)
-    clocks.mark_end()
-    launches = s.launch_count - launches0
-    prof = s.kernel_profile()
+    s, ms, prof, launches, setup_s = time_arm(prob, args.precision, args, world, dev, clocks)
     clk = clocks.stop()
-    s.set_profiling(False)
-    ms = max_over_ranks(ms, world)
+    n = s.nparticles
     value = world * n * args.steps / (ms / 1e3)
+    state = s.read()
+
+    # the FP64 path on the same workload and steps, with the mixed path's
+    # per-field deviation from it
+    fp64 = None
+    if args.precision == "mixed" and not args.no_fp64_arm:
+        s64, ms64, prof64, _, _ = time_arm(prob, "fp64", args, world, dev)
+        fp64 = {"value": world * n * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
+                "kernels_ms_per_launch": {k: v[0] / v[1] for k, v in prof64.items() if v[1]},
+                "mixed_vs_fp64_field_errors": field_errors(state, s64.read())}
+        del s64
 
     # end to end through the public API with host arrays
-    st = s.read()
+    st = state
     h2d = sum(np.asarray(st[k]).nbytes for k in ("x", "u", "v", "stress", "strain", "F", "volume",
                                                  "mass", "density", "cell", "material", "svars"))
     barrier(world)
@@ -272,17 +313,15 @@ def main():
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     name, (tot_ms, cnt) = dom
     avg_s = tot_ms / max(cnt, 1) / 1e3
-    if name in BYTES_PER_PARTICLE:
-        bytes_launch = BYTES_PER_PARTICLE[name] * n
-    else:
-        bytes_launch = BYTES_PER_ACTIVE_NODE.get(name, 0) * prob.nnodes
+    bpp = BYTES_PER_PARTICLE[args.precision]
+    bytes_launch = bpp.get(name, 0) * n
     achieved = bytes_launch / avg_s / 1e9
+    total = max(sum(x[0] for x in prof.values()), 1e-30)
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_s * 1e3,
-                "traffic": None,
-                "kernel_shares": {k: v[0] / max(sum(x[0] for x in prof.values()), 1e-30)
-                                  for k, v in prof.items() if v[1]}}
+                "bytes_per_particle": bpp.get(name, 0), "bytes_per_launch": bytes_launch,
+                "avg_launch_ms": avg_s * 1e3, "traffic": None,
+                "kernel_shares": {k: v[0] / total for k, v in prof.items() if v[1]}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -304,6 +343,7 @@ def main():
                        "l2": "state larger than L2 (no flush needed)",
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "setup_s": setup_s},
+            "fp64": fp64,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "kernels": {k: {"total_ms": v[0], "launches": v[1]}
                                        for k, v in prof.items() if v[1]},

@@ -755,8 +755,10 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
   }
   if (t == 0) {
     for (int f = 0; f < ROWS; ++f) bulk::store(s.pf + f * np + p0, rows + f * T, T * 8);
-    if (mc)
-      for (int k = 0; k < SV_N; ++k) bulk::store(s.sv + k * np + p0, svr + k * T, T * 8);
+    if (mc)  // phi, psi, cohesion and tension cutoff change only with softening
+      for (int k = 0; k < SV_N; ++k)
+        if (s.any_softening || k == SV_YIELD || k >= SV_EPS)
+          bulk::store(s.sv + k * np + p0, svr + k * T, T * 8);
     bulk::store_commit();
   }
   if (active) {

@@ -751,9 +751,12 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   }
   if (t == 0) {
     for (int f = 0; f < XROWS; ++f) bulk::store(s.pf + f * np + p0, xr + f * T, T * 8);
-    for (int f = 0; f < MROWS; ++f) bulk::store(s.pm + f * np + p0, mr + f * T, T * 4);
-    if (mc)
-      for (int k = 0; k < SVF_N; ++k) bulk::store(s.svf + k * np + p0, svr + k * T, T * 4);
+    for (int f = 0; f < MROWS; ++f)  // the initial volume and density never change
+      if (f != PM<DIM>::V0 && f != PM<DIM>::RHO0) bulk::store(s.pm + f * np + p0, mr + f * T, T * 4);
+    if (mc)  // phi, psi, cohesion and tension cutoff change only with softening
+      for (int k = 0; k < SVF_N; ++k)
+        if (s.any_softening || k == SV_YIELD || k >= SV_EPS)
+          bulk::store(s.svf + k * np + p0, svr + k * T, T * 4);
     bulk::store_commit();
   }
   if (active) {

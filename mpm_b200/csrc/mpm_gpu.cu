@@ -714,6 +714,8 @@ void refresh_state(mpm_gpu_t h) {
   s.nlost = h->d_words.p;
   s.err = h->d_words.p + 1;
   s.nplastic = h->d_words.p + 2;
+  s.any_softening = 0;
+  for (auto& m : h->mats) s.any_softening |= (m.type == 1 && m.softening) ? 1 : 0;
   s.plist = h->any_mc ? h->d_plist.p : nullptr;
   s.pbuf = h->any_mc ? h->d_pbuf.p : nullptr;
   s.pbuf_f = h->any_mc ? reinterpret_cast<float*>(h->d_pbuf.p) : nullptr;

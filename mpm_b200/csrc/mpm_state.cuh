@@ -142,6 +142,7 @@ struct DevState {
   float* dndx_cf = nullptr;       // [ncells][NV][DIM]
   const MaterialT<float>* mats_f = nullptr;
 
+  int any_softening = 0;          // some MohrCoulomb material softens (phi..tc vary)
   const MaterialParams* mats = nullptr;
   const NodeBC* bcs = nullptr;
   const ParticleVC* pvcs = nullptr;
