@@ -867,14 +867,16 @@ void counting_sort_impl(const DevState& s, cudaStream_t st) {
 }
 
 // Ask for the shared-memory carveout that lets MIN_BLOCKS staged blocks share
-// an SM (set once per kernel).
-template <class K>
-void prefer_shared_memory(K kernel) {
-  static bool done = false;
-  if (!done) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+// an SM (set once per kernel and device).
+template <auto Kernel>
+void prefer_shared_memory() {
+  static unsigned done = 0;  // one bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 32 && !(done & (1u << dev))) {
+    cudaFuncSetAttribute(Kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)cudaSharedmemCarveoutMaxShared);
-    done = true;
+    done |= 1u << dev;
   }
 }
 
@@ -907,10 +909,10 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     pr.begin(K_G2P, st);
     const size_t sm = staged_smem_bytes<DIM>(s.sv != nullptr);
     if (a.flip) {
-      prefer_shared_memory(k_g2p_staged<DIM, true>);
+      prefer_shared_memory<k_g2p_staged<DIM, true>>();
       k_g2p_staged<DIM, true><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
     } else {
-      prefer_shared_memory(k_g2p_staged<DIM, false>);
+      prefer_shared_memory<k_g2p_staged<DIM, false>>();
       k_g2p_staged<DIM, false><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
     }
     pr.end(K_G2P, st);

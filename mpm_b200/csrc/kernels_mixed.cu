@@ -778,13 +778,15 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   if (t == 0) bulk::store_wait_all();
 }
 
-template <class K>
-void prefer_shared_memory(K kernel) {
-  static bool done = false;
-  if (!done) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+template <auto Kernel>
+void prefer_shared_memory() {
+  static unsigned done = 0;  // one bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 32 && !(done & (1u << dev))) {
+    cudaFuncSetAttribute(Kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)cudaSharedmemCarveoutMaxShared);
-    done = true;
+    done |= 1u << dev;
   }
 }
 
@@ -863,10 +865,10 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     pr.begin(K_G2P, st);
     const size_t sm = mixed_staged_smem_bytes<DIM>(s.svf != nullptr);
     if (a.flip) {
-      prefer_shared_memory(k_g2p_mixed_staged<DIM, true>);
+      prefer_shared_memory<k_g2p_mixed_staged<DIM, true>>();
       k_g2p_mixed_staged<DIM, true><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
     } else {
-      prefer_shared_memory(k_g2p_mixed_staged<DIM, false>);
+      prefer_shared_memory<k_g2p_mixed_staged<DIM, false>>();
       k_g2p_mixed_staged<DIM, false><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
     }
     pr.end(K_G2P, st);
