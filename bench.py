@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--block", default="100,100,50", help="particle block in cells")
+    ap.add_argument("--workload", default="column", choices=["column", "footing"],
+                    help="column: the 4M-particle granular column (default); footing: the "
+                         "16M-particle footing on a slope over a foundation")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-fp64-arm", action="store_true",
                     help="skip the FP64 run reported beside the mixed one")
@@ -275,7 +278,7 @@ def main():
         return
     from mpm_b200 import problems as P
     block = tuple(int(v) for v in args.block.split(","))
-    prob = P.config_b(block=block)
+    prob = P.config_b(block=block) if args.workload == "column" else P.config_e()
     dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
     clocks = Clocks(dev)
     s, ms, prof, launches, setup_s = time_arm(prob, args.precision, args, world, dev, clocks)
@@ -324,7 +327,7 @@ def main():
                 "kernel_shares": {k: v[0] / total for k, v in prof.items() if v[1]}}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "column":
         rate, threads, sample = time_cpu_oracle(args.cpu_sample_seconds)
         cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                "sample": sample}
@@ -335,9 +338,12 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
-            "config": {"workload": f"3D granular column collapse, MohrCoulomb USL FLIP "
-                                   f"{args.precision.upper()}, "
-                                   f"200x100x50 hex8 dx=0.01, {n} particles",
+            "config": {"workload": (f"3D granular column collapse, MohrCoulomb USL FLIP "
+                                    f"{args.precision.upper()}, 200x100x50 hex8 dx=0.01, "
+                                    f"{n} particles") if args.workload == "column" else
+                                   (f"3D footing on a MohrCoulomb slope over a LinearElastic "
+                                    f"foundation, USL FLIP {args.precision.upper()}, 400x200x100 "
+                                    f"hex8 dx=0.005, {n} particles"),
                        "particles": n, "nodes": prob.nnodes, "cells": prob.ncells,
                        "dt": prob.analysis["dt"], "precision": args.precision,
                        "l2": "state larger than L2 (no flush needed)",

@@ -998,7 +998,6 @@ int mpm_gpu_set_mesh(mpm_gpu_t h, int64_t nnodes, const double* coords, int64_t 
   h->cell_nodes.resize((size_t)ncells * nv);
   h->geom.resize(ncells);
   h->cell_volume.resize(ncells);
-  std::vector<std::vector<int32_t>> node_cells(nnodes);
   std::vector<double> X(nv * dim);
   for (int64_t c = 0; c < ncells; ++c) {
     for (int i = 0; i < nv; ++i) {
@@ -1006,7 +1005,6 @@ int mpm_gpu_set_mesh(mpm_gpu_t h, int64_t nnodes, const double* coords, int64_t 
       if (n < 0 || n >= nnodes) throw InvalidArg("cell node id out of range");
       h->cell_nodes[c * nv + i] = (int32_t)n;
       for (int d = 0; d < dim; ++d) X[i * dim + d] = coords[n * dim + d];
-      node_cells[n].push_back((int32_t)c);
     }
     cell_geometry(dim, X.data(), &h->geom[c], &h->cell_volume[c]);
     if (!(h->cell_volume[c] > 0)) throw InvalidArg("Negative or zero volume cell, misconfigured cell!");
@@ -1024,6 +1022,25 @@ int mpm_gpu_set_mesh(mpm_gpu_t h, int64_t nnodes, const double* coords, int64_t 
     else
       dn_dx<3>(xi0, X.data(), &h->dndx_c[(size_t)c * nv * dim]);
   }
+  // A tensor-product grid needs no connectivity tables: node ids, neighbours
+  // and the cells around a node follow from (i, j, k).
+  h->structured = detect_structured(h);
+  if (h->structured) {
+    h->nc_off.assign(nnodes + 1, 0);
+    h->nc_cell.clear();
+    h->nc_slot.clear();
+    h->nb_off.assign(ncells + 1, 0);
+    h->nb.clear();
+    h->bin_off.assign(2, 0);
+    h->bin_cells.clear();
+    upload_mesh(h);
+    upload_bcs(h);  // every node gets a (possibly empty) constraint slot
+    h->mesh_set = true;
+    return MPM_OK;
+  }
+  std::vector<std::vector<int32_t>> node_cells(nnodes);
+  for (int64_t c = 0; c < ncells; ++c)
+    for (int i = 0; i < nv; ++i) node_cells[h->cell_nodes[c * nv + i]].push_back((int32_t)c);
   // node -> (cell, slot), ascending cell id, for the nodal gather on general meshes
   h->nc_off.assign(nnodes + 1, 0);
   for (int64_t n = 0; n < nnodes; ++n) h->nc_off[n + 1] = h->nc_off[n] + (int32_t)node_cells[n].size();
@@ -1059,13 +1076,7 @@ int mpm_gpu_set_mesh(mpm_gpu_t h, int64_t nnodes, const double* coords, int64_t 
     h->nb.insert(h->nb.end(), tmp.begin(), tmp.end());
     h->nb_off[c + 1] = (int32_t)h->nb.size();
   }
-  h->structured = detect_structured(h);
-  if (h->structured) {
-    h->bin_off.assign(2, 0);
-    h->bin_cells.clear();
-  } else {
-    build_bins(h);
-  }
+  build_bins(h);
   upload_mesh(h);
   upload_bcs(h);  // every node gets a (possibly empty) constraint slot
   h->mesh_set = true;

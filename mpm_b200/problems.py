@@ -210,6 +210,63 @@ def column_3d(shape=(200, 100, 50), block=(100, 100, 50), dx=0.01, E=1e7, nu=0.3
                    name="column3d")
 
 
+def footing_slope(shape=(400, 200, 100), dx=0.005, foundation=20, slope_height=40, slope_top=30,
+                  footing=(5, 25), dt=1e-6, nsteps=1000, mu=0.4, scheme="usl",
+                  velocity_update="flip", footing_velocity=-0.05, seed=SEED_BASE + 4):
+    """3D slope on a foundation under a rigid footing (16M particles by default).
+
+    LinearElastic foundation (E=5e7, nu=0.3, rho=1800) filling the lowest
+    ``foundation`` cell layers of the whole x-y plane; MohrCoulomb slope (phi=35,
+    c=2 kPa, psi=0, rho=1800) on top: ``slope_height`` layers, the layer k above
+    the foundation spanning x cells [0, slope_top + slope_height - k) (a 45 deg
+    face); 2x2x2 particles per filled cell.  The footing is the set of slope
+    particles in the top layer with x cells in [footing[0], footing[1]),
+    driven down at ``footing_velocity`` m/s by a particle velocity constraint
+    (mesh.tcc:1454-1467).  Slip walls, frictional floor, gravity -z, K0
+    geostatic initial stress under the local surface."""
+    coords, cells = structured_mesh(3, shape, dx)
+    nx, ny = shape[0], shape[1]
+    found = quarter_point_particles(3, [(0, nx), (0, ny), (0, foundation)], dx, seed=seed)
+    layers = []
+    for k in range(slope_height):
+        w = min(slope_top + slope_height - k, nx)
+        layers.append(quarter_point_particles(
+            3, [(0, w), (0, ny), (foundation + k, foundation + k + 1)], dx, seed=seed + 1 + k))
+    slope = np.concatenate(layers)
+
+    def surface(x):  # top of the material above x
+        cells_x = np.floor(x / dx)
+        k_top = np.clip(slope_top + slope_height - cells_x, 0, slope_height)
+        return (foundation + k_top) * dx
+
+    rho, nu = 1800.0, 0.3
+    st_f = geostatic_stress(found, 3, rho, nu, surface(found[:, 0]))
+    st_s = geostatic_stress(slope, 3, rho, nu, surface(slope[:, 0]))
+    top_z = (foundation + slope_height - 1) * dx
+    on_footing = ((slope[:, 2] > top_z) & (slope[:, 0] >= footing[0] * dx) &
+                  (slope[:, 0] < footing[1] * dx))
+    pids = len(found) + np.nonzero(on_footing)[0]
+    vc = slip_box(coords, 3)
+    floor = boundary_nodes(coords, 2, coords[:, 2].min())
+    fc = (floor, np.full(len(floor), 2), np.full(len(floor), -1), np.full(len(floor), mu))
+    mats = [(0, "LinearElastic3D", linear_elastic(5e7, nu, rho)),
+            (1, "MohrCoulomb3D", mohr_coulomb(1e7, nu, rho, 35.0, 2000.0, 0.0))]
+    return Problem(dim=3, shape=shape, dx=dx, coords=coords, cells=cells, materials=mats,
+                   particles=[(found, 0), (slope, 1)], velocity_constraints=vc,
+                   friction_constraints=fc,
+                   particle_velocity_constraints=[(pids, 2, footing_velocity)],
+                   initial_stress=np.concatenate([st_f, st_s]),
+                   analysis=dict(scheme=scheme, velocity_update=velocity_update, dt=dt,
+                                 nsteps=nsteps, gravity=(0.0, 0.0, -9.81), damping_factor=0.0),
+                   name="footing_slope")
+
+
+def config_e():
+    """3D footing on a MohrCoulomb slope over a LinearElastic foundation,
+    400x200x100 hex8 cells of 5 mm, 16,032,000 particles."""
+    return footing_slope()
+
+
 def config_a():
     """2D explicit USF column collapse, LinearElastic, 3,200 particles."""
     return column_2d()

@@ -122,3 +122,17 @@ def test_read_load_round_trip():
     B = b.read()
     for k in A:
         np.testing.assert_allclose(B[k], A[k], rtol=1e-6, atol=0, err_msg=k)
+
+
+def test_footing_on_slope_mixed():
+    """Two materials and a footing constraint, USL, 200 steps: the footing
+    yields the slope under it; the FP32 elastic predictor and stored stress put
+    the stress field within a few 1e-4 of the FP64 path, the kinematic fields
+    within a few 1e-5."""
+    prob = P.footing_slope(shape=(40, 10, 20), foundation=4, slope_height=8, slope_top=6,
+                           footing=(1, 5), dt=1e-5)
+    m, f = _run(prob, 200, "mixed"), _run(prob, 200, "fp64")
+    assert np.array_equal(m["cell"], f["cell"])
+    errs = _errors(m, f)
+    assert all(v <= 3e-4 for v in errs.values()), errs
+    assert errs["u"] <= 1e-5 and errs["v"] <= 5e-5, errs

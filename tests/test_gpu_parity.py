@@ -249,3 +249,22 @@ def test_runs_are_bitwise_deterministic(scheme):
     ra, rb = a.read(), b.read()
     for f in ("cell", "x", "v", "stress", "svars"):
         assert np.array_equal(ra[f], rb[f]), f
+
+
+def small_footing(**kw):
+    base = dict(shape=(40, 10, 20), foundation=4, slope_height=8, slope_top=6, footing=(1, 5),
+                dt=1e-5)
+    base.update(kw)
+    return P.footing_slope(**base)
+
+
+@pytest.mark.parametrize("scheme", ["usf", "usl"])
+def test_footing_on_slope_two_materials(scheme):
+    """LinearElastic foundation + MohrCoulomb slope (c = 2 kPa) with a footing
+    driven by a particle velocity constraint: two material slots, the
+    constraint set, friction floor, 40 steps."""
+    prob = small_footing(scheme=scheme)
+    for s, g, o in _run_both(prob, [10, 40]):
+        assert_parity(g, o, label=f"footing step {s}")
+    fp = prob.particle_velocity_constraints[0][0]
+    assert np.allclose(g["v"][fp, 2], -0.05)
