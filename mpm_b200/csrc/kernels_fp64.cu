@@ -634,7 +634,7 @@ template <int DIM>
 constexpr int staged_rows() { return PF<DIM>::MASS; }  // fields X .. RHO
 template <int DIM>
 constexpr size_t staged_smem_bytes(bool mc) {
-  return (size_t)(staged_rows<DIM>() + (mc ? SV_N : 0)) * STAGE_T * 8 + STAGE_T * (4 + 1 + 2);
+  return (size_t)(staged_rows<DIM>() + (mc ? SV_N : 0)) * STAGE_T * 8 + STAGE_T * (4 + 2 + 2);
 }
 
 template <int DIM, bool FLIP>
@@ -651,7 +651,7 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
   double* rows = reinterpret_cast<double*>(smem);
   double* svr = rows + ROWS * T;
   int32_t* scell = reinterpret_cast<int32_t*>(svr + (mc ? SV_N * T : 0));
-  uint8_t* smat = reinterpret_cast<uint8_t*>(scell + T);
+  uint16_t* smat = reinterpret_cast<uint16_t*>(scell + T);
   int16_t* spvc = reinterpret_cast<int16_t*>(smat + T);
   const int t = threadIdx.x;
   const int64_t p0 = (int64_t)blockIdx.x * T;
@@ -664,10 +664,10 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
   }
   __syncthreads();
   if (t == 0) {
-    bulk::mbar_arrive_expect_tx(&bar[0], ROWS_A * T * 8 + T * (4 + 1 + 2));
+    bulk::mbar_arrive_expect_tx(&bar[0], ROWS_A * T * 8 + T * (4 + 2 + 2));
     for (int f = 0; f < ROWS_A; ++f) bulk::load(rows + f * T, s.pf + f * np + p0, T * 8, &bar[0]);
     bulk::load(scell, s.cell + p0, T * 4, &bar[0]);
-    bulk::load(smat, s.mat + p0, T, &bar[0]);
+    bulk::load(smat, s.mat + p0, T * 2, &bar[0]);
     bulk::load(spvc, s.pvc + p0, T * 2, &bar[0]);
     bulk::mbar_arrive_expect_tx(&bar[1], (ROWS - ROWS_A + (mc ? SV_N : 0)) * T * 8);
     for (int f = ROWS_A; f < ROWS; ++f) bulk::load(rows + f * T, s.pf + f * np + p0, T * 8, &bar[1]);

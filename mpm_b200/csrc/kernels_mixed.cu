@@ -627,7 +627,7 @@ static_assert(MSTAGE_T == PAD_PARTICLES, "staged slices are whole padded blocks"
 template <int DIM>
 constexpr size_t mixed_staged_smem_bytes(bool mc) {
   return (size_t)2 * DIM * MSTAGE_T * 8 + (size_t)(PM<DIM>::MASS + (mc ? SVF_N : 0)) * MSTAGE_T * 4 +
-         MSTAGE_T * (4 + 1 + 2);
+         MSTAGE_T * (4 + 2 + 2);
 }
 
 template <int DIM, bool FLIP>
@@ -645,7 +645,7 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   float* mr = reinterpret_cast<float*>(xr + XROWS * T);
   float* svr = mr + MROWS * T;
   int32_t* scell = reinterpret_cast<int32_t*>(svr + (mc ? SVF_N * T : 0));
-  uint8_t* smat = reinterpret_cast<uint8_t*>(scell + T);
+  uint16_t* smat = reinterpret_cast<uint16_t*>(scell + T);
   int16_t* spvc = reinterpret_cast<int16_t*>(smat + T);
   const int t = threadIdx.x;
   const int64_t p0 = (int64_t)blockIdx.x * T;
@@ -658,12 +658,12 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   }
   __syncthreads();
   if (t == 0) {
-    bulk::mbar_arrive_expect_tx(&bar[0], 2 * DIM * T * 8 + DIM * T * 4 + T * (4 + 1 + 2));
+    bulk::mbar_arrive_expect_tx(&bar[0], 2 * DIM * T * 8 + DIM * T * 4 + T * (4 + 2 + 2));
     for (int f = 0; f < XROWS; ++f) bulk::load(xr + f * T, s.pf + f * np + p0, T * 8, &bar[0]);
     for (int f = PM<DIM>::V; f < PM<DIM>::V + DIM; ++f)
       bulk::load(mr + f * T, s.pm + f * np + p0, T * 4, &bar[0]);
     bulk::load(scell, s.cell + p0, T * 4, &bar[0]);
-    bulk::load(smat, s.mat + p0, T, &bar[0]);
+    bulk::load(smat, s.mat + p0, T * 2, &bar[0]);
     bulk::load(spvc, s.pvc + p0, T * 2, &bar[0]);
     bulk::mbar_arrive_expect_tx(&bar[1], (MROWS - DIM + (mc ? SVF_N : 0)) * T * 4);
     for (int f = PM<DIM>::V + DIM; f < MROWS; ++f)

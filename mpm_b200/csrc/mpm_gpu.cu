@@ -184,7 +184,7 @@ struct mpm_gpu_solver {
   int64_t np = 0;
   int64_t npad = 0;
   std::vector<double> p_coords;         // np*dim (creation)
-  std::vector<uint8_t> p_mat;
+  std::vector<uint16_t> p_mat;
   std::vector<std::map<unsigned, double>> p_vc;  // per particle velocity constraints
   bool p_vc_dirty = false;
 
@@ -192,7 +192,8 @@ struct mpm_gpu_solver {
   DevState ds;
   DevBuf<double> d_pf, d_sv, d_nf, d_ncoord;
   DevBuf<int32_t> d_cell, d_bc_index, d_cell_nodes, d_nb_off, d_nb, d_bin_off, d_bin_cells, d_lost;
-  DevBuf<uint8_t> d_mat, d_active;
+  DevBuf<uint16_t> d_mat;
+  DevBuf<uint8_t> d_active;
   DevBuf<int16_t> d_pvc;
   DevBuf<CellGeom> d_geom;
   DevBuf<unsigned> d_words;  // [0] nlost, [1] err, [2] nplastic
@@ -224,6 +225,14 @@ struct mpm_gpu_solver {
   uint8_t* h_stage = nullptr;  // pinned, two halves
   size_t h_stage_bytes = 0;
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+
+  // one captured step, replayed while the device state and step arguments
+  // stay the same
+  cudaGraphExec_t graph = nullptr;
+  DevState graph_state{};
+  StepArgs graph_args{};
+  int64_t graph_launches = 0;
+  bool graph_ok = true;
 
   // mixed precision: d_pf holds [x, u, pdstrain] in FP64, the rest is FP32
   bool mixed = false;
@@ -897,7 +906,7 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
     }
   }
   h->d_cell.upload(cell.data(), ns, h->stream);
-  std::vector<uint8_t> mat(h->p_mat);
+  std::vector<uint16_t> mat(h->p_mat);
   mat.resize(ns, 0);
   h->d_mat.upload(mat.data(), ns, h->stream);
   std::vector<double> sv;
@@ -976,6 +985,7 @@ int mpm_gpu_destroy(mpm_gpu_t h) {
   if (h->h_stage) cudaFreeHost(h->h_stage);
   for (auto& e : h->stage_ev)
     if (e) cudaEventDestroy(e);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
   delete h;
   return MPM_OK;
 }
@@ -1088,7 +1098,7 @@ int mpm_gpu_add_material(mpm_gpu_t h, int32_t id, const char* type, const char* 
   MPM_GUARD(h)
   if (!type || !json_props) throw InvalidArg("null material type or properties");
   if (h->mat_index.count(id)) throw InvalidArg("New material cannot be added, insertion failed");
-  if (h->mats.size() >= 255) throw InvalidArg("too many materials");
+  if (h->mats.size() >= 65535) throw InvalidArg("too many materials");
   const Json j = parse_json(json_props);
   MaterialParams m = make_material(h->dim, type, j);
   h->mat_index[id] = (int)h->mats.size();
@@ -1164,7 +1174,7 @@ int mpm_gpu_add_particles(mpm_gpu_t h, int64_t n, const double* coords, int32_t 
   if (n < 0 || (n > 0 && !coords)) throw InvalidArg("bad particle array");
   if (h->np + n > INT32_MAX) throw InvalidArg("too many particles for 32-bit indices");
   h->p_coords.insert(h->p_coords.end(), coords, coords + n * h->dim);
-  h->p_mat.insert(h->p_mat.end(), (size_t)n, (uint8_t)it->second);
+  h->p_mat.insert(h->p_mat.end(), (size_t)n, (uint16_t)it->second);
   h->set_np(h->np + n);
   MPM_END(h)
   return MPM_OK;
@@ -1279,7 +1289,7 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
   for (int64_t p = 0; p < n; ++p) {
     auto it = h->mat_index.find(in->material[p]);
     if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
-    h->p_mat[p] = (uint8_t)it->second;
+    h->p_mat[p] = (uint16_t)it->second;
   }
   h->p_vc.assign(n, {});
   if ((int64_t)h->p_id.size() != n) {
@@ -1297,6 +1307,12 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
   h->initialised = true;
   MPM_END(h)
   return MPM_OK;
+}
+
+static bool same_step(const DevState& a, const DevState& b, const StepArgs& x, const StepArgs& y) {
+  return std::memcmp(&a, &b, sizeof(DevState)) == 0 && x.scheme == y.scheme && x.flip == y.flip &&
+         x.remove_lost == y.remove_lost && x.dt == y.dt && x.beta == y.beta &&
+         x.damping == y.damping && x.g[0] == y.g[0] && x.g[1] == y.g[1] && x.g[2] == y.g[2];
 }
 
 static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
@@ -1318,15 +1334,55 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
     ck(cudaEventCreate(&e1), "cudaEventCreate");
     ck(cudaEventRecord(e0, h->stream), "cudaEventRecord");
   }
+  auto launch = [&]() {
+    if (h->mixed)
+      launch_step_mixed(h->dim, h->ds, a, h->stream, h->prof);
+    else
+      launch_step_fp64(h->dim, h->ds, a, h->stream, h->prof);
+  };
+  // A step whose device state and arguments match the captured one replays the
+  // captured CUDA graph (one graph launch instead of the step's kernel
+  // launches).  The first step of a call runs eagerly (it sets the kernels'
+  // shared-memory attributes outside any capture); profiling runs eagerly.
+  bool eager_done = false;
   for (int64_t s = 0; s < nsteps; ++s) {
     double gm = 1.0;  // mpm_explicit.tcc:145-153
     if (h->cfg.gravity_ramping_time > 0.0)
       gm = std::min(1.0, static_cast<double>(h->step) * h->cfg.dt / h->cfg.gravity_ramping_time);
     for (int d = 0; d < 3; ++d) a.g[d] = d < h->dim ? gm * h->cfg.gravity[d] : 0.;
-    if (h->mixed)
-      launch_step_mixed(h->dim, h->ds, a, h->stream, h->prof);
-    else
-      launch_step_fp64(h->dim, h->ds, a, h->stream, h->prof);
+    const bool graphable = h->graph_ok && !h->prof.enabled && eager_done;
+    if (graphable && h->graph && same_step(h->graph_state, h->ds, h->graph_args, a)) {
+      ck(cudaGraphLaunch(h->graph, h->stream), "cudaGraphLaunch");
+      h->prof.launches += h->graph_launches;
+    } else if (graphable) {
+      if (h->graph) cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+      const int64_t l0 = h->prof.launches;
+      cudaGraph_t g = nullptr;
+      bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        launch();
+        ok = cudaStreamEndCapture(h->stream, &g) == cudaSuccess && g != nullptr;
+        ok = ok && cudaGraphInstantiate(&h->graph, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+      }
+      if (ok) {
+        h->graph_state = h->ds;
+        h->graph_args = a;
+        h->graph_launches = h->prof.launches - l0;
+        ck(cudaGraphLaunch(h->graph, h->stream), "cudaGraphLaunch");
+      } else {  // capture not possible here: launch eagerly from now on
+        cudaGetLastError();
+        if (h->graph) cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+        h->graph_ok = false;
+        h->prof.launches = l0;
+        launch();
+      }
+    } else {
+      launch();
+      eager_done = true;
+    }
     ck(cudaGetLastError(), "kernel launch");
     ++h->step;
   }
@@ -1391,6 +1447,8 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   std::vector<int32_t> cell(np);
   h->d_cell.download(cell.data(), np, h->stream);
   download_particle_fields(h, pf, sv);
+  std::vector<int32_t> slot_id(h->mats.size(), -1);  // material slot -> id
+  for (auto& kv : h->mat_index) slot_id[kv.second] = kv.first;
   const int64_t ns = h->npad;
   auto at = [&](int f, int64_t p) { return pf[(size_t)f * ns + p]; };
   const int X = dim == 2 ? PF<2>::X : PF<3>::X, U = dim == 2 ? PF<2>::U : PF<3>::U;
@@ -1441,12 +1499,7 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
     if (out->density) out->density[p] = at(RHO, p);
     if (out->mass) out->mass[p] = at(MASS, p);
     if (out->cell) out->cell[p] = cell[p];
-    if (out->material) {
-      int32_t id = -1;
-      for (auto& kv : h->mat_index)
-        if (kv.second == h->p_mat[p]) id = kv.first;
-      out->material[p] = id;
-    }
+    if (out->material) out->material[p] = slot_id[h->p_mat[p]];
     if (out->svars)
       for (int k = 0; k < SV_N; ++k) out->svars[p * SV_N + k] = h->any_mc ? sv[(size_t)k * ns + p] : 0.;
   }

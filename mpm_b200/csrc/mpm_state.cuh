@@ -78,7 +78,7 @@ struct DevState {
   double* pf = nullptr;    // [PF::NF][np]
   double* sv = nullptr;    // [SV_N][np] MohrCoulomb state (null when no MC)
   int32_t* cell = nullptr; // [np] current cell, -1 removed
-  uint8_t* mat = nullptr;  // [np] material slot
+  uint16_t* mat = nullptr; // [np] material slot
   int16_t* pvc = nullptr;  // [np] particle velocity constraint slot (-1 none)
 
   int64_t nn = 0;          // nodes
