@@ -34,21 +34,33 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic bytes per particle of the particle kernels, 3D MohrCoulomb USL
+# Algorithmic bytes per particle of the particle kernels, MohrCoulomb USL
 # (compulsory particle-state traffic: every field read once, every field the
 # kernel changes written once; nodal gathers hit L2 and are not counted).
 BYTES_PER_PARTICLE = {
-    "fp64": {
+    ("fp64", 3): {
         # read x u v 72, stress strain 96, F 72, volume density 16, cell 4,
-        # material 1, constraint slot 2, MC state 72
-        "g2p": 335 + 296,   # write x u v stress strain F V rho 256, MC state that changes 40
+        # material 2, constraint slot 2, MC state 72
+        "g2p": 336 + 296,   # write x u v stress strain F V rho 256, MC state that changes 40
         "p2g": 116,         # read x 24, v 24, mass 8, stress 48, volume 8, order 4
     },
-    "mixed": {
+    ("mixed", 3): {
         # read x u 48 (FP64), v stress strain H V0 rho0 P 108 (FP32), MC state
-        # 32, cell material slot 7; write x u 48, v stress strain H P 100, MC 16
-        "g2p": 195 + 164,
+        # 32, cell material slot 8; write x u 48, v stress strain H P 100, MC 16
+        "g2p": 196 + 164,
         "p2g": 68,          # read x 24, v 12, mass 4, stress 24, V0 P 8 (FP32)
+    },
+    ("fp64", 2): {
+        # read x u v 48, stress 32, strain 24, F 32, V rho 16, MC 72, slots 8;
+        # write the first 152 + MC that changes 40
+        "g2p": 232 + 192,
+        "p2g": 84,
+    },
+    ("mixed", 2): {
+        # read x u 32, v stress strain H V0 rho0 P 64, MC 32, slots 8; write
+        # x u 32, v stress strain H P 56, MC 16
+        "g2p": 136 + 104,
+        "p2g": 52,
     },
 }
 DTYPES = {"fp64": "f64", "mixed": "f32+f64"}
@@ -62,9 +74,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--block", default="100,100,50", help="particle block in cells")
-    ap.add_argument("--workload", default="column", choices=["column", "footing"],
+    ap.add_argument("--workload", default="column", choices=["column", "footing", "ensemble"],
                     help="column: the 4M-particle granular column (default); footing: the "
-                         "16M-particle footing on a slope over a foundation")
+                         "16M-particle footing on a slope over a foundation; ensemble: 512 "
+                         "independent 2D slopes in one solver")
+    ap.add_argument("--profile-steps", type=int, default=20,
+                    help="steps timed per kernel after the timed window")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-fp64-arm", action="store_true",
                     help="skip the FP64 run reported beside the mixed one")
@@ -238,14 +253,15 @@ def run_reference(args, rank, world):
 
 
 def time_arm(prob, precision, args, world, dev, clocks=None):
-    """Build a solver, run the warm-up, time K steps on the device."""
+    """Build a solver, run the warm-up, time K steps on the device (the
+    production path: steps replayed from the captured CUDA graph), then time
+    a short window per kernel (profiling launches eagerly)."""
     from mpm_b200 import problems as P
     t0 = time.perf_counter()
     s = P.build_solver(prob, precision=precision, device=dev)
     setup_s = time.perf_counter() - t0
     s.step(args.warmup)
     barrier(world)
-    s.set_profiling(True)
     launches0 = s.launch_count
     if clocks:
         clocks.mark_start()
@@ -253,9 +269,11 @@ def time_arm(prob, precision, args, world, dev, clocks=None):
     if clocks:
         clocks.mark_end()
     launches = s.launch_count - launches0
+    ms = max_over_ranks(ms, world)
+    s.set_profiling(True)
+    s.step_timed(args.profile_steps)
     prof = s.kernel_profile()
     s.set_profiling(False)
-    ms = max_over_ranks(ms, world)
     return s, ms, prof, launches, setup_s
 
 
@@ -278,7 +296,13 @@ def main():
         return
     from mpm_b200 import problems as P
     block = tuple(int(v) for v in args.block.split(","))
-    prob = P.config_b(block=block) if args.workload == "column" else P.config_e()
+    if args.workload == "column":
+        prob = P.config_b(block=block)
+    elif args.workload == "footing":
+        prob = P.config_e()
+    else:
+        from mpm_b200 import ensemble as E
+        prob, _ = E.ensemble_problem(E.random_runs(512))
     dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
     clocks = Clocks(dev)
     s, ms, prof, launches, setup_s = time_arm(prob, args.precision, args, world, dev, clocks)
@@ -316,7 +340,7 @@ def main():
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     name, (tot_ms, cnt) = dom
     avg_s = tot_ms / max(cnt, 1) / 1e3
-    bpp = BYTES_PER_PARTICLE[args.precision]
+    bpp = BYTES_PER_PARTICLE[(args.precision, prob.dim)]
     bytes_launch = bpp.get(name, 0) * n
     achieved = bytes_launch / avg_s / 1e9
     total = max(sum(x[0] for x in prof.values()), 1e-30)
@@ -343,10 +367,15 @@ def main():
                                     f"{n} particles") if args.workload == "column" else
                                    (f"3D footing on a MohrCoulomb slope over a LinearElastic "
                                     f"foundation, USL FLIP {args.precision.upper()}, 400x200x100 "
-                                    f"hex8 dx=0.005, {n} particles"),
+                                    f"hex8 dx=0.005, {n} particles") if args.workload == "footing"
+                                   else (f"512 independent 2D MohrCoulomb slopes in one solver "
+                                         f"(N ~ U[2000, 40000], phi ~ U[20, 40], c ~ U[0, 5 kPa]), "
+                                         f"USL FLIP {args.precision.upper()}, dx=0.01, {n} "
+                                         f"particles"),
                        "particles": n, "nodes": prob.nnodes, "cells": prob.ncells,
                        "dt": prob.analysis["dt"], "precision": args.precision,
                        "l2": "state larger than L2 (no flush needed)",
+                       "kernel_profile_steps": args.profile_steps,
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "setup_s": setup_s},
             "fp64": fp64,
