@@ -190,6 +190,24 @@ int mpm_gpu_write_pod(mpm_gpu_t h, void* records, int64_t capacity, int64_t* nre
 int mpm_gpu_load_pod(mpm_gpu_t h, const void* records, int64_t n, size_t record_size,
                      const size_t* offsets, const size_t* sizes, int32_t nfields);
 
+/* Sensitivities (no counterpart in the reference): derivatives of the whole
+ * particle state with respect to up to two material parameters, carried by
+ * every step after this call (forward-mode differentiation of the FP64 USL
+ * step: P2G, node update with its boundary conditions, G2P, strain, volume,
+ * MohrCoulomb return; discrete decisions follow the values).  kinds[k]:
+ * 0 Young's modulus (Pa), 1 friction angle (degrees; peak and residual),
+ * 2 cohesion (Pa; peak and residual), 3 dilation angle (degrees; peak and
+ * residual), of material material_ids[k].  The derivatives start at zero for
+ * the particle fields and at the parameter's own derivative for the state
+ * variables it initialises.  n = 0 turns sensitivities off.  FP64 precision
+ * and USL only (MPM_ERR_UNSUPPORTED otherwise); loading particles turns them
+ * off.  A step carrying derivatives costs about three value-only steps. */
+int mpm_gpu_set_sensitivities(mpm_gpu_t h, int32_t n, const int32_t* material_ids,
+                              const int32_t* kinds);
+/* d(field)/d(parameter k) for every particle: out[k][p][c], k < n, with c < 3
+ * for field 0 x, 1 u, 2 v and c < 6 for field 3 stress (unused components 0). */
+int mpm_gpu_read_sensitivities(mpm_gpu_t h, int32_t field, double* out);
+
 /* Set the step counter (the resume step of analysis.resume.step; it drives the
  * gravity ramp, mpm_explicit.tcc:145-153). */
 int mpm_gpu_set_current_step(mpm_gpu_t h, int64_t step);

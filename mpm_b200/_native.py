@@ -69,6 +69,8 @@ SIGNATURES = {
                                     C.c_int32]),
     "mpm_gpu_load_pod": (C.c_int, [_vp, _vp, C.c_int64, C.c_size_t, _psz, _psz, C.c_int32]),
     "mpm_gpu_set_current_step": (C.c_int, [_vp, C.c_int64]),
+    "mpm_gpu_set_sensitivities": (C.c_int, [_vp, C.c_int32, _pi32, _pi32]),
+    "mpm_gpu_read_sensitivities": (C.c_int, [_vp, C.c_int32, _pd]),
     "mpm_gpu_device_field": (C.c_int, [_vp, C.c_int32, C.POINTER(_vp), _pi64, _pi32]),
     "mpm_gpu_material_stress_batch": (C.c_int, [C.c_int32, C.c_int32, C.c_char_p, C.c_char_p,
                                                 C.c_int64, _pd, _pd, _pd, _pd, _pd]),

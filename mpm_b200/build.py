@@ -28,8 +28,9 @@ UNITS = [
     ("mpm_gpu.cu", []),
     ("noalloc.cu", []),
     ("pod.cu", []),
+    ("kernels_tangent.cu", ["--fmad=false"]),
 ]
-HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp", "mpm_device.cuh", "mpm_bulk.cuh"]
+HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp", "mpm_device.cuh", "mpm_bulk.cuh", "mpm_dual.cuh"]
 
 
 def _newer(target, deps):

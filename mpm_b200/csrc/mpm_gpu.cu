@@ -234,6 +234,13 @@ struct mpm_gpu_solver {
   int64_t graph_launches = 0;
   bool graph_ok = true;
 
+  // sensitivities: tangent buffers (layouts of pf, sv, nf, partials)
+  int ntangent = 0;
+  DevBuf<double> d_pft[MAX_TANGENTS], d_svt[MAX_TANGENTS], d_nft[MAX_TANGENTS],
+      d_partt[MAX_TANGENTS];
+  DevBuf<unsigned char> d_mats_t;
+  DevBuf<double> d_prep, d_prept[MAX_TANGENTS], d_tpbuf;
+
   // mixed precision: d_pf holds [x, u, pdstrain] in FP64, the rest is FP32
   bool mixed = false;
   DevBuf<float> d_pm, d_svf, d_nfv, d_partials_f, d_dndx_cf;
@@ -723,6 +730,17 @@ void refresh_state(mpm_gpu_t h) {
   s.nlost = h->d_words.p;
   s.err = h->d_words.p + 1;
   s.nplastic = h->d_words.p + 2;
+  for (int k = 0; k < MAX_TANGENTS; ++k) {
+    const bool on = h->ntangent > 0;
+    s.pft[k] = on ? h->d_pft[k].p : nullptr;
+    s.svt[k] = on ? h->d_svt[k].p : nullptr;
+    s.nft[k] = on ? h->d_nft[k].p : nullptr;
+    s.partt[k] = on ? h->d_partt[k].p : nullptr;
+  }
+  s.mats_t = h->ntangent > 0 ? h->d_mats_t.p : nullptr;
+  s.prep = h->ntangent > 0 ? h->d_prep.p : nullptr;
+  s.tpbuf = h->ntangent > 0 ? h->d_tpbuf.p : nullptr;
+  for (int k = 0; k < MAX_TANGENTS; ++k) s.prept[k] = h->ntangent > 0 ? h->d_prept[k].p : nullptr;
   s.any_softening = 0;
   for (auto& m : h->mats) s.any_softening |= (m.type == 1 && m.softening) ? 1 : 0;
   s.plist = h->any_mc ? h->d_plist.p : nullptr;
@@ -1292,6 +1310,7 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
     h->p_mat[p] = (uint16_t)it->second;
   }
   h->p_vc.assign(n, {});
+  h->ntangent = 0;  // a new state has no tangents
   if ((int64_t)h->p_id.size() != n) {
     h->p_id.resize(n);
     for (int64_t p = 0; p < n; ++p) h->p_id[p] = (uint64_t)p;
@@ -1335,7 +1354,9 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
     ck(cudaEventRecord(e0, h->stream), "cudaEventRecord");
   }
   auto launch = [&]() {
-    if (h->mixed)
+    if (h->ntangent > 0)
+      launch_step_tangent(h->dim, h->ds, a, h->stream, h->prof);
+    else if (h->mixed)
       launch_step_mixed(h->dim, h->ds, a, h->stream, h->prof);
     else
       launch_step_fp64(h->dim, h->ds, a, h->stream, h->prof);
@@ -1790,6 +1811,95 @@ int mpm_gpu_load_pod(mpm_gpu_t h, const void* records, int64_t n, size_t record_
   h->p_nsize = std::move(nsize);
   h->p_acc = std::move(acc);
   h->aux_dirty = true;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_set_sensitivities(mpm_gpu_t h, int32_t n, const int32_t* material_ids,
+                              const int32_t* kinds) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("initialise or load particles first");
+  if (n < 0 || n > MAX_TANGENTS) throw InvalidArg("at most 2 parameters are differentiated");
+  if (n > 0 && (!material_ids || !kinds)) throw InvalidArg("null parameter list");
+  if (n > 0 && h->mixed) return fail(h, MPM_ERR_UNSUPPORTED, "sensitivities run in FP64 only");
+  if (n > 0 && h->cfg.scheme != MPM_SCHEME_USL)
+    return fail(h, MPM_ERR_UNSUPPORTED, "sensitivities follow the USL scheme only");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  std::vector<TangentParam> params(n);
+  for (int k = 0; k < n; ++k) {
+    auto it = h->mat_index.find(material_ids[k]);
+    if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
+    if (kinds[k] < TP_YOUNGS_MODULUS || kinds[k] > TP_DILATION) throw InvalidArg("unknown parameter kind");
+    if (kinds[k] != TP_YOUNGS_MODULUS && h->mats[it->second].type != 1)
+      throw InvalidArg("friction, cohesion and dilation are MohrCoulomb parameters");
+    params[k] = TangentParam{it->second, kinds[k]};
+  }
+  h->ntangent = 0;
+  if (n == 0) {
+    refresh_state(h);
+    return MPM_OK;
+  }
+  const int64_t np = h->npad;
+  const int nval = 1 + 3 * h->dim;
+  const size_t nprep = (size_t)h->nv * (1 + h->dim) * np;
+  h->d_prep.alloc(nprep);
+  if (h->any_mc) h->d_tpbuf.alloc((size_t)7 * (1 + MAX_TANGENTS) * np);
+  for (int k = 0; k < MAX_TANGENTS; ++k) {
+    h->d_prept[k].alloc(nprep);
+    h->d_pft[k].alloc((size_t)h->nfields() * np);
+    h->d_nft[k].alloc((size_t)h->nnf() * h->nnodes);
+    h->d_partt[k].alloc((size_t)h->ncells * h->nv * nval);
+    ck(cudaMemsetAsync(h->d_pft[k].p, 0, sizeof(double) * h->nfields() * np, h->stream), "memset");
+    ck(cudaMemsetAsync(h->d_nft[k].p, 0, sizeof(double) * h->nnf() * h->nnodes, h->stream), "memset");
+    h->d_svt[k].free();
+  }
+  // material tables and the initial state-variable derivatives
+  std::vector<unsigned char> mt(tangent_material_bytes() * h->mats.size());
+  std::vector<double> seed((size_t)h->mats.size() * SV_N * MAX_TANGENTS);
+  make_tangent_materials(h->mats.data(), (int)h->mats.size(), params.data(), n, mt.data(),
+                         seed.data());
+  h->d_mats_t.upload(mt.data(), mt.size(), h->stream);
+  if (h->any_mc) {
+    for (int k = 0; k < MAX_TANGENTS; ++k) {
+      std::vector<double> svt((size_t)SV_N * np, 0.0);
+      for (int64_t p = 0; p < h->np; ++p)
+        for (int v = 0; v < SV_N; ++v)
+          svt[(size_t)v * np + p] = seed[((size_t)h->p_mat[p] * SV_N + v) * MAX_TANGENTS + k];
+      h->d_svt[k].upload(svt.data(), svt.size(), h->stream);
+    }
+  }
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  h->ntangent = n;
+  refresh_state(h);
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_read_sensitivities(mpm_gpu_t h, int32_t field, double* out) {
+  MPM_GUARD(h)
+  if (h->ntangent == 0) throw InvalidArg("no sensitivities enabled");
+  if (!out) throw InvalidArg("null output");
+  const int dim = h->dim;
+  int off = 0, nc = 0;
+  switch (field) {
+    case 0: off = dim == 2 ? PF<2>::X : PF<3>::X; nc = dim; break;
+    case 1: off = dim == 2 ? PF<2>::U : PF<3>::U; nc = dim; break;
+    case 2: off = dim == 2 ? PF<2>::V : PF<3>::V; nc = dim; break;
+    case 3: off = dim == 2 ? PF<2>::S : PF<3>::S; nc = dim == 2 ? 4 : 6; break;
+    default: throw InvalidArg("field: 0 x, 1 u, 2 v, 3 stress");
+  }
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const int64_t np = h->np, ns = h->npad;
+  const int width = field == 3 ? 6 : 3;
+  std::vector<double> col((size_t)nc * ns);
+  for (int k = 0; k < h->ntangent; ++k) {
+    ck(cudaMemcpyAsync(col.data(), h->d_pft[k].p + (size_t)off * ns, sizeof(double) * nc * ns,
+                       cudaMemcpyDeviceToHost, h->stream), "D2H");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    double* o = out + (size_t)k * np * width;
+    for (int64_t p = 0; p < np; ++p)
+      for (int c = 0; c < width; ++c) o[p * width + c] = c < nc ? col[(size_t)c * ns + p] : 0.0;
+  }
   MPM_END(h)
   return MPM_OK;
 }

@@ -77,6 +77,19 @@ struct PodAux {                 // per-particle data the step never changes
 };
 void launch_pod_pack(int dim, bool mixed, const DevState& s, const PodAux& a, const PodLayout& L,
                      const int32_t* list, int64_t count, uint8_t* out, cudaStream_t st);
+// Tangent (sensitivity) step: material parameters differentiated
+enum { TP_YOUNGS_MODULUS = 0, TP_FRICTION = 1, TP_COHESION = 2, TP_DILATION = 3 };
+struct TangentParam {
+  int32_t material_slot;
+  int32_t kind;
+};
+constexpr int MAX_TANGENTS = 2;
+void launch_step_tangent(int dim, const DevState& s, const StepArgs& a, cudaStream_t st,
+                         Profiler& prof);
+size_t tangent_material_bytes();
+// fills out (nmats MaterialT<Dual>) and sv_seed (nmats x SV_N x MAX_TANGENTS)
+void make_tangent_materials(const MaterialParams* mats, int nmats, const TangentParam* params,
+                            int nparams, void* out, double* sv_seed);
 void launch_material_batch_fp64(int dim, int64_t n, const MaterialParams& m, const double* stress,
                                 const double* dstrain, const double* density, double* state,
                                 double* out, cudaStream_t st);

@@ -365,6 +365,24 @@ MPM_HD R mu_j3(const R* s) {
          ((R(2) * s[3] * s[4] * s[5]) - (d0 * sq(s[4])) - (d1 * sq(s[5])));
 }
 
+// The type the stress invariants are evaluated in for a working type R: FP64
+// for FP32 and FP64 (see mc_invariants), the tangent type itself for tangents.
+template <typename R>
+struct HighPrecision {
+  using T = double;
+};
+
+// Value-preserving hook for the tangent type: the identity for plain numbers.
+// For tangents (mpm_dual.cuh) it drops the derivative of a Lode-angle quantity
+// within a small distance of a triaxial corner of the yield surface, where
+// the derivative of theta(sigma) is unbounded.
+template <typename T>
+MPM_HD T lode_corner(const T& x, double /*dist_to_corner*/) {
+  return x;
+}
+MPM_HD double value(double x) { return x; }
+MPM_HD float value(float x) { return x; }
+
 // sin and cos of an FP64 angle in one evaluation
 MPM_HD void sin_cos(double x, double* sn, double* cs) {
 #ifdef __CUDA_ARCH__
@@ -416,19 +434,19 @@ MPM_HD FrictionTrig<R> friction_trig(const MaterialT<R>& m, const R* sv) {
 // stress by 1e-4 of its magnitude.
 template <typename R>
 MPM_HD void mc_invariants(const R* s, R* sv, LodeTrig<R>& lt) {
-  const double d[6] = {double(s[0]), double(s[1]), double(s[2]),
-                       double(s[3]), double(s[4]), double(s[5])};
-  const double j2 = mu_j2(d);
-  const double j3 = mu_j3(d);
+  using H = typename HighPrecision<R>::T;
+  const H d[6] = {H(s[0]), H(s[1]), H(s[2]), H(s[3]), H(s[4]), H(s[5])};
+  const H j2 = mu_j2(d);
+  const H j3 = mu_j3(d);
   sv[SV_EPS] = R(mu_p(d) * sqrt(3.0));
-  double v = 0.0;
+  H v = H(0.0);
   if (fabs(j2) > kDblEps) v = (3.0 * sqrt(3.0) / 2.0) * (j3 / (j2 * sqrt(j2)));
-  if (v > 1.0) v = 1.0;
-  if (v < -1.0) v = -1.0;
-  const double theta = (1.0 / 3.0) * acos(v);
+  if (v > 1.0) v = H(1.0);
+  if (v < -1.0) v = H(-1.0);
+  const H theta = lode_corner((1.0 / 3.0) * acos(v), value(1.0 - v * v));
   sv[SV_THETA] = R(theta);
   sv[SV_RHO] = R(sqrt(2.0 * j2));
-  double sn, cs;
+  H sn, cs;
   sin_cos(theta, &sn, &cs);
   const double h = 0.5, r3 = 0.86602540378443864676;  // cos, sin of pi/3
   lt.ct = R(cs);
@@ -503,35 +521,34 @@ MPM_HD void mc_df_dp(const MaterialT<R>& m, int yield_type, const R* sv, const L
   // the reason given at mc_invariants (1 - r^2 vanishes on triaxial paths)
   R dtheta_ds[6];
   {
-    const double sd[6] = {double(s[0]), double(s[1]), double(s[2]),
-                          double(s[3]), double(s[4]), double(s[5])};
-    const double j2d = mu_j2(sd);
-    const double pmd = mu_p(sd);
-    const double dv[6] = {sd[0] - pmd, sd[1] - pmd, sd[2] - pmd, sd[3], sd[4], sd[5]};
-    const double j3 = mu_j3(sd);
-    const double dj2[6] = {dv[0], dv[1], dv[2], dv[3] * 2.0, dv[4] * 2.0, dv[5] * 2.0};
-    const double dev1[3] = {dv[0], dv[3], dv[5]};
-    const double dev2[3] = {dv[3], dv[1], dv[4]};
-    const double dev3[3] = {dv[5], dv[4], dv[2]};
-    auto dot3 = [](const double* a, const double* b) {
-      return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
-    };
-    const double dj3[6] = {dot3(dev1, dev1) - (2.0 / 3.0) * j2d,
-                           dot3(dev2, dev2) - (2.0 / 3.0) * j2d,
-                           dot3(dev3, dev3) - (2.0 / 3.0) * j2d,
-                           2.0 * dot3(dev1, dev2),
-                           2.0 * dot3(dev2, dev3),
-                           2.0 * dot3(dev1, dev3)};
-    double dr_dj2 = -9.0 / 4.0 * sqrt(3.0) * j3;
-    double dr_dj3 = 3.0 / 2.0 * sqrt(3.0);
-    double dtheta_dr = -1.0 / 3.0;
+    using H = typename HighPrecision<R>::T;
+    const H sd[6] = {H(s[0]), H(s[1]), H(s[2]), H(s[3]), H(s[4]), H(s[5])};
+    const H j2d = mu_j2(sd);
+    const H pmd = mu_p(sd);
+    const H dv[6] = {sd[0] - pmd, sd[1] - pmd, sd[2] - pmd, sd[3], sd[4], sd[5]};
+    const H j3 = mu_j3(sd);
+    const H dj2[6] = {dv[0], dv[1], dv[2], dv[3] * 2.0, dv[4] * 2.0, dv[5] * 2.0};
+    const H dev1[3] = {dv[0], dv[3], dv[5]};
+    const H dev2[3] = {dv[3], dv[1], dv[4]};
+    const H dev3[3] = {dv[5], dv[4], dv[2]};
+    auto dot3 = [](const H* a, const H* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; };
+    const H dj3[6] = {dot3(dev1, dev1) - (2.0 / 3.0) * j2d,
+                      dot3(dev2, dev2) - (2.0 / 3.0) * j2d,
+                      dot3(dev3, dev3) - (2.0 / 3.0) * j2d,
+                      2.0 * dot3(dev1, dev2),
+                      2.0 * dot3(dev2, dev3),
+                      2.0 * dot3(dev1, dev3)};
+    H dr_dj2 = -9.0 / 4.0 * sqrt(3.0) * j3;
+    H dr_dj3 = H(3.0 / 2.0 * sqrt(3.0));
+    H dtheta_dr = H(-1.0 / 3.0);
     if (fabs(j2d) > kDblEps) {
       // j2^-1.5 and j2^-2.5 from one square root
-      const double p15 = 1.0 / (j2d * sqrt(j2d));
-      const double r = j3 / 2.0 * (3.0 * sqrt(3.0)) * p15;
+      const H p15 = 1.0 / (j2d * sqrt(j2d));
+      const H r = j3 / 2.0 * (3.0 * sqrt(3.0)) * p15;
       dr_dj2 *= p15 / j2d;
       dr_dj3 *= p15;
-      const double factor = (fabs(1.0 - r * r) < kDblEps) ? kDblEps : fabs(1.0 - r * r);
+      const H factor = lode_corner((fabs(1.0 - r * r) < kDblEps) ? H(kDblEps) : fabs(1.0 - r * r),
+                                   value(fabs(1.0 - r * r)));
       dtheta_dr = -1.0 / (3.0 * sqrt(factor));
     }
 #pragma unroll
@@ -785,40 +802,39 @@ struct NodeBC {
   double mu;
 };
 
-template <int DIM>
-MPM_HD void apply_velocity_constraints(const NodeBC& bc, double* v, double* a) {
+template <int DIM, typename R>
+MPM_HD void apply_velocity_constraints(const NodeBC& bc, R* v, R* a) {
 #pragma unroll
   for (int d = 0; d < DIM; ++d)
     if (bc.vel_mask & (1u << d)) {
-      v[d] = bc.vel[d];
-      a[d] = 0.;
+      v[d] = R(bc.vel[d]);
+      a[d] = R(0.);
     }
 }
 
 // node.tcc:510-657 (Cartesian boundaries)
-template <int DIM>
-MPM_HD void apply_friction_constraints(const NodeBC& bc, const double* vel, double* acc,
-                                       double dt) {
-  auto sign = [](double value) { return (value > 0.) ? 1. : -1.; };
+template <int DIM, typename R>
+MPM_HD void apply_friction_constraints(const NodeBC& bc, const R* vel, R* acc, double dt) {
+  auto sign = [](const R& value) { return (value > 0.) ? 1. : -1.; };
   const unsigned dir_n = bc.fric_dir;
-  const double sign_n = sign((double)bc.fric_sign);
+  const double sign_n = bc.fric_sign > 0 ? 1. : -1.;
   const double mu = bc.mu;
   if constexpr (DIM == 2) {
     const unsigned dir_t = 1 - dir_n;
-    const double acc_n = acc[dir_n];
-    double acc_t = acc[dir_t];
-    const double vel_t = vel[dir_t];
+    const R acc_n = acc[dir_n];
+    R acc_t = acc[dir_t];
+    const R vel_t = vel[dir_t];
     if ((acc_n * sign_n) > 0.0) {
       if (vel_t != 0.0) {
-        const double vel_net = dt * acc_t + vel_t;
-        const double vel_frictional = dt * mu * fabs(acc_n);
+        const R vel_net = dt * acc_t + vel_t;
+        const R vel_frictional = dt * mu * fabs(acc_n);
         if (fabs(vel_net) <= vel_frictional)
           acc_t = -vel_t / dt;
         else
           acc_t -= sign(vel_net) * mu * fabs(acc_n);
       } else {
         if (fabs(acc_t) <= mu * fabs(acc_n))
-          acc_t = 0.0;
+          acc_t = R(0.0);
         else
           acc_t -= sign(acc_t) * mu * fabs(acc_n);
       }
@@ -827,15 +843,15 @@ MPM_HD void apply_friction_constraints(const NodeBC& bc, const double* vel, doub
   } else {
     const unsigned t0 = dir_n == 0 ? 1 : 0;
     const unsigned t1 = dir_n == 2 ? 1 : 2;
-    const double acc_n = acc[dir_n];
-    double acc_t = sqrt(acc[t0] * acc[t0] + acc[t1] * acc[t1]);
-    const double vel_t = sqrt(vel[t0] * vel[t0] + vel[t1] * vel[t1]);
+    const R acc_n = acc[dir_n];
+    R acc_t = sqrt(acc[t0] * acc[t0] + acc[t1] * acc[t1]);
+    const R vel_t = sqrt(vel[t0] * vel[t0] + vel[t1] * vel[t1]);
     if (acc_n * sign_n > 0.0) {
       if (vel_t != 0.0) {
-        const double vn0 = vel[t0] + acc[t0] * dt;
-        const double vn1 = vel[t1] + acc[t1] * dt;
-        const double vel_net_t = sqrt(vn0 * vn0 + vn1 * vn1);
-        const double vel_fricion = mu * fabs(acc_n) * dt;
+        const R vn0 = vel[t0] + acc[t0] * dt;
+        const R vn1 = vel[t1] + acc[t1] * dt;
+        const R vel_net_t = sqrt(vn0 * vn0 + vn1 * vn1);
+        const R vel_fricion = mu * fabs(acc_n) * dt;
         if (vel_net_t <= vel_fricion) {
           acc[t0] = -vel[t0] / dt;
           acc[t1] = -vel[t1] / dt;
@@ -845,8 +861,8 @@ MPM_HD void apply_friction_constraints(const NodeBC& bc, const double* vel, doub
         }
       } else {
         if (acc_t <= mu * fabs(acc_n)) {
-          acc[t0] = 0;
-          acc[t1] = 0;
+          acc[t0] = R(0.);
+          acc[t1] = R(0.);
         } else {
           acc_t -= mu * fabs(acc_n);
           acc[t0] -= mu * fabs(acc_n) * (acc[t0] / acc_t);

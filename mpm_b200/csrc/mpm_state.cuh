@@ -143,6 +143,17 @@ struct DevState {
   const MaterialT<float>* mats_f = nullptr;
 
   int any_softening = 0;          // some MohrCoulomb material softens (phi..tc vary)
+
+  // tangents (derivatives with respect to NT material parameters), each in the
+  // layout of its value array; null unless sensitivities are enabled
+  double* pft[2] = {nullptr, nullptr};       // particle fields, layout of pf
+  double* svt[2] = {nullptr, nullptr};       // MohrCoulomb state, layout of sv
+  double* nft[2] = {nullptr, nullptr};       // nodal v, a, layout of nf
+  double* partt[2] = {nullptr, nullptr};     // cell-slot partials
+  const void* mats_t = nullptr;              // [materials] MaterialT<Dual>
+  double* tpbuf = nullptr;                   // [7][1 + NT][np] deferred-return inputs
+  double* prep = nullptr;                    // [NV (1 + DIM)][np] N, dN/dx at the step start
+  double* prept[2] = {nullptr, nullptr};
   const MaterialParams* mats = nullptr;
   const NodeBC* bcs = nullptr;
   const ParticleVC* pvcs = nullptr;

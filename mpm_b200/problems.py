@@ -267,6 +267,21 @@ def config_e():
     return footing_slope()
 
 
+def calibration_column(phi=30.0, E=1e7, shape=(80, 40, 30), block=(40, 40, 20), dx=0.02,
+                       dt=1e-5, c=1000.0, nsteps=2000):
+    """Config D: the 3D MohrCoulomb column (phi, E) whose final positions a
+    calibration matches, 40x40x20 filled cells of 2 cm in an 80x40x30 mesh
+    (256,000 particles), USL, dt 1e-5, K0 geostatic start.  The cohesion
+    (1 kPa by default) keeps the gradient away from the c = 0 apex, where the
+    reference's return is undefined."""
+    return column_3d(shape=shape, block=block, dx=dx, E=E, phi=phi, c=c, psi=0.0, dt=dt,
+                     nsteps=nsteps, scheme="usl")
+
+
+def config_d(phi=30.0, E=1e7):
+    return calibration_column(phi=phi, E=E)
+
+
 def config_a():
     """2D explicit USF column collapse, LinearElastic, 3,200 particles."""
     return column_2d()

@@ -229,6 +229,29 @@ class Solver:
                                          size, offs.ctypes.data_as(psz),
                                          sizes.ctypes.data_as(psz), 74))
 
+    SENSITIVITY_KINDS = {"youngs_modulus": 0, "friction": 1, "cohesion": 2, "dilation": 3}
+    SENSITIVITY_FIELDS = {"x": 0, "u": 1, "v": 2, "stress": 3}
+
+    def set_sensitivities(self, params):
+        """Carry derivatives with respect to up to two material parameters,
+        given as [(material_id, "youngs_modulus" | "friction" | "cohesion" |
+        "dilation"), ...]; an empty list turns them off."""
+        n = len(params)
+        mids = np.array([m for m, _ in params], dtype=np.int32)
+        kinds = np.array([self.SENSITIVITY_KINDS[k] for _, k in params], dtype=np.int32)
+        self._ck(self.L.mpm_gpu_set_sensitivities(self.h, n, _i32p(mids), _i32p(kinds)))
+        self._nsens = n
+
+    def read_sensitivities(self, field="x"):
+        """d(field)/d(parameter): array (n_parameters, n_particles, dim) for x,
+        u, v; (n_parameters, n_particles, 6) for stress."""
+        n = getattr(self, "_nsens", 0)
+        width = 6 if field == "stress" else 3
+        out = np.zeros((max(n, 1), self.nparticles, width))
+        self._ck(self.L.mpm_gpu_read_sensitivities(self.h, self.SENSITIVITY_FIELDS[field],
+                                                   _dp(out)))
+        return out if field == "stress" else out[:, :, :self.dim]
+
     def set_current_step(self, step):
         self._ck(self.L.mpm_gpu_set_current_step(self.h, int(step)))
 
