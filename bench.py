@@ -74,10 +74,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--block", default="100,100,50", help="particle block in cells")
-    ap.add_argument("--workload", default="column", choices=["column", "footing", "ensemble"],
+    ap.add_argument("--workload", default="column",
+                    choices=["column", "footing", "ensemble", "calibration"],
                     help="column: the 4M-particle granular column (default); footing: the "
                          "16M-particle footing on a slope over a foundation; ensemble: 512 "
-                         "independent 2D slopes in one solver")
+                         "independent 2D slopes in one solver; calibration: derivatives of "
+                         "the 256k-particle column's final positions with respect to (E, phi)")
     ap.add_argument("--profile-steps", type=int, default=20,
                     help="steps timed per kernel after the timed window")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
@@ -288,11 +290,76 @@ def field_errors(a, b):
     return out
 
 
+def run_calibration(args, rank, world):
+    """Config D: the FP64 forward run and the run carrying derivatives with
+    respect to (E, phi), timed on the device, and the gradient of the loss
+    |x_final - x_target|^2 (target run at E = 8e6, phi = 32) against central
+    differences of the FP64 path (relative step 1e-6)."""
+    from mpm_b200 import problems as P
+    from mpm_b200.sensitivity import run_with_sensitivities
+    params = [(0, "youngs_modulus"), (0, "friction")]
+    theta = np.array([1e7, 30.0])
+    dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
+    build = lambda th: P.build_solver(P.config_d(phi=th[1], E=th[0]), precision="fp64", device=dev)
+
+    def final_x(th):
+        s = build(th)
+        s.step(args.steps)
+        x = s.read()["x"]
+        s.close()
+        return x
+
+    f = build(theta)
+    f.step(args.warmup)
+    ms_f = max_over_ranks(f.step_timed(args.steps), world)
+    n = f.nparticles
+    f.close()
+    t = build(theta)
+    t.set_sensitivities(params)
+    t.step(args.warmup)
+    ms_t = max_over_ranks(t.step_timed(args.steps), world)
+    t.close()
+    target = final_x((8e6, 32.0))
+    x, J = run_with_sensitivities(build, theta, params, args.steps)
+    grad = 2.0 * np.einsum("pd,kpd->k", x - target, J)
+    fd = []
+    for k in range(2):
+        h = 1e-6 * theta[k]
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd.append((np.sum((final_x(tp) - target) ** 2) - np.sum((final_x(tm) - target) ** 2))
+                  / (2 * h))
+    if rank == 0:
+        value = world * n * args.steps / (ms_t / 1e3)
+        line = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_t / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 + 2 tangents", "data": "synthetic",
+            "config": {"workload": f"calibration column (config D): 80x40x30 hex8 dx=0.02, {n} "
+                                   f"particles, MohrCoulomb c=1 kPa, USL, dt=1e-5, derivatives "
+                                   f"w.r.t. (E, phi)", "particles": n},
+            "forward": {"value": world * n * args.steps / (ms_f / 1e3),
+                        "ms_per_step": ms_f / args.steps},
+            "tangent_over_forward": ms_t / ms_f,
+            "gradient": {"loss": "sum |x_final - x_target|^2, target E=8e6, phi=32",
+                         "at": theta.tolist(), "tangent": grad.tolist(), "central_fd": fd,
+                         "fd_relative_step": 1e-6,
+                         "relative_error": [abs(g - d) / max(abs(d), 1e-300)
+                                            for g, d in zip(grad, fd)]},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world = dist_init(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "calibration":
+        run_calibration(args, rank, world)
         return
     from mpm_b200 import problems as P
     block = tuple(int(v) for v in args.block.split(","))

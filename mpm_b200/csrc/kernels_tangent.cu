@@ -276,6 +276,19 @@ __global__ void __launch_bounds__(128) k_nodes_tangent(DevState s, double dt, do
     for (int d = 0; d < DIM; ++d)
       if (fabs(acc[d]) < 1.0E-15) acc[d] = D(0.);
   }
+  // A node that a particle only grazes (it just entered the node's cells) has
+  // a mass many orders below a particle's; the quotient rule for momentum /
+  // mass then subtracts two nearly equal derivatives and divides by that mass,
+  // and the rounding error, amplified by 1 / mass, reaches the particles
+  // through dN/dx (which is not small there).  Such nodes keep their values
+  // and pass no derivatives.
+  if (m.v < s.tangent_mass_floor) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      vel[d] = D(vel[d].v);
+      acc[d] = D(acc[d].v);
+    }
+  }
   double* const* t = const_cast<double* const*>(s.nft);
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {

@@ -146,17 +146,16 @@ MPM_HD void sin_cos(const Dual& x, Dual* sn, Dual* cs) {
 }
 MPM_HD double value(const Dual& a) { return a.v; }
 
-// Within this distance (1 - cos^2 3 theta) of a triaxial corner of the
-// MohrCoulomb surface the Lode angle's derivative is taken as zero: theta is
-// acos of a ratio, so d theta / d sigma grows without bound at the corner and
-// tangents through a return there would blow up; values are unchanged.
+// Within MPM_LODE_CORNER_TOL of a triaxial corner of the MohrCoulomb surface
+// (distance 1 - cos^2 3 theta) the Lode angle's derivative is taken as zero
+// (values are unchanged): theta is acos of a ratio, so d theta / d sigma
+// grows without bound at the corner.
 #ifndef MPM_LODE_CORNER_TOL
 #define MPM_LODE_CORNER_TOL 1e-8
 #endif
 template <>
 MPM_HD Dual lode_corner<Dual>(const Dual& x, double dist_to_corner) {
-  const double dist = dist_to_corner;
-  return dist < MPM_LODE_CORNER_TOL ? Dual(x.v) : x;
+  return dist_to_corner < MPM_LODE_CORNER_TOL ? Dual(x.v) : x;
 }
 
 template <>

@@ -236,6 +236,7 @@ struct mpm_gpu_solver {
 
   // sensitivities: tangent buffers (layouts of pf, sv, nf, partials)
   int ntangent = 0;
+  double tangent_mass_floor = 0.0;
   DevBuf<double> d_pft[MAX_TANGENTS], d_svt[MAX_TANGENTS], d_nft[MAX_TANGENTS],
       d_partt[MAX_TANGENTS];
   DevBuf<unsigned char> d_mats_t;
@@ -740,6 +741,7 @@ void refresh_state(mpm_gpu_t h) {
   s.mats_t = h->ntangent > 0 ? h->d_mats_t.p : nullptr;
   s.prep = h->ntangent > 0 ? h->d_prep.p : nullptr;
   s.tpbuf = h->ntangent > 0 ? h->d_tpbuf.p : nullptr;
+  s.tangent_mass_floor = h->tangent_mass_floor;
   for (int k = 0; k < MAX_TANGENTS; ++k) s.prept[k] = h->ntangent > 0 ? h->d_prept[k].p : nullptr;
   s.any_softening = 0;
   for (auto& m : h->mats) s.any_softening |= (m.type == 1 && m.softening) ? 1 : 0;
@@ -1869,6 +1871,16 @@ int mpm_gpu_set_sensitivities(mpm_gpu_t h, int32_t n, const int32_t* material_id
     }
   }
   ck(cudaStreamSynchronize(h->stream), "sync");
+  // nodes below 1e-3 of the mean particle mass pass no derivatives
+  {
+    std::vector<double> mass(h->np);
+    const int MASSF = h->dim == 2 ? PF<2>::MASS : PF<3>::MASS;
+    ck(cudaMemcpy(mass.data(), h->d_pf.p + (size_t)MASSF * h->npad, sizeof(double) * h->np,
+                  cudaMemcpyDeviceToHost), "D2H");
+    double sum = 0.0;
+    for (double v : mass) sum += v;
+    h->tangent_mass_floor = h->np > 0 ? 1e-3 * sum / (double)h->np : 0.0;
+  }
   h->ntangent = n;
   refresh_state(h);
   MPM_END(h)

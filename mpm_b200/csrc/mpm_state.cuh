@@ -152,6 +152,7 @@ struct DevState {
   double* partt[2] = {nullptr, nullptr};     // cell-slot partials
   const void* mats_t = nullptr;              // [materials] MaterialT<Dual>
   double* tpbuf = nullptr;                   // [7][1 + NT][np] deferred-return inputs
+  double tangent_mass_floor = 0.0;           // nodes lighter than this carry no tangents
   double* prep = nullptr;                    // [NV (1 + DIM)][np] N, dN/dx at the step start
   double* prept[2] = {nullptr, nullptr};
   const MaterialParams* mats = nullptr;

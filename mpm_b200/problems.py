@@ -268,14 +268,18 @@ def config_e():
 
 
 def calibration_column(phi=30.0, E=1e7, shape=(80, 40, 30), block=(40, 40, 20), dx=0.02,
-                       dt=1e-5, c=1000.0, nsteps=2000):
+                       dt=1e-5, c=1000.0, tension_cutoff=0.0, nsteps=2000):
     """Config D: the 3D MohrCoulomb column (phi, E) whose final positions a
     calibration matches, 40x40x20 filled cells of 2 cm in an 80x40x30 mesh
-    (256,000 particles), USL, dt 1e-5, K0 geostatic start.  The cohesion
-    (1 kPa by default) keeps the gradient away from the c = 0 apex, where the
-    reference's return is undefined."""
-    return column_3d(shape=shape, block=block, dx=dx, E=E, phi=phi, c=c, psi=0.0, dt=dt,
-                     nsteps=nsteps, scheme="usl")
+    (256,000 particles), USL, dt 1e-5, K0 geostatic start.  Cohesion (1 kPa)
+    and tension cutoff (0, the reference's default) are not calibrated."""
+    p = column_3d(shape=shape, block=block, dx=dx, E=E, phi=phi, c=c, psi=0.0, dt=dt,
+                  nsteps=nsteps, scheme="usl")
+    mid, mt, props = p.materials[0]
+    props = dict(props)
+    props["tension_cutoff"] = tension_cutoff
+    p.materials[0] = (mid, mt, props)
+    return p
 
 
 def config_d(phi=30.0, E=1e7):

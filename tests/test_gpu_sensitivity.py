@@ -16,10 +16,10 @@ pytestmark = pytest.mark.gpu
 PARAMS = [(0, "youngs_modulus"), (0, "friction")]
 
 
-def _prob(theta, c=200.0):
+def _prob(theta):
     E, phi = theta
     return P.calibration_column(phi=phi, E=E, shape=(16, 8, 12), block=(8, 6, 8), dx=0.01,
-                                dt=5e-6, c=c)
+                                dt=5e-6, c=200.0, tension_cutoff=0.0)
 
 
 def _build(theta):
@@ -38,16 +38,12 @@ def test_tangent_run_values_equal_the_fp64_run():
         assert np.array_equal(A[k], B[k]), k
 
 
-def _prob_tc(theta, c=500.0, tension_cutoff=1e4):
+def _prob_tc(theta):
     """Column with cohesion 500 Pa and a 10 kPa tension cutoff: shear returns
     during the run, a loss that is smooth in (E, phi)."""
-    p = _prob(theta, c=c)
-    mid, mt, props = p.materials[0]
-    props = dict(props)
-    props["tension_cutoff"] = tension_cutoff
-    p.materials[0] = (mid, mt, props)
-    p.analysis["dt"] = 1e-5
-    return p
+    E, phi = theta
+    return P.calibration_column(phi=phi, E=E, shape=(16, 8, 12), block=(8, 6, 8), dx=0.01,
+                                dt=1e-5, c=500.0, tension_cutoff=1e4)
 
 
 def test_gradient_of_a_calibration_loss_matches_central_differences():
