@@ -14,6 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libmpm_b200.so")
+RUNNER = os.path.join(LIBDIR, "mpm_gpu_run")
+CXX = os.environ.get("CXX", "g++")
 ROOT = os.path.dirname(HERE)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -57,6 +59,14 @@ def build(force=False, verbose=False):
             subprocess.check_call(cmd)
     if force or _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+    # the C++ host driver over the C ABI (reads the reference's input files)
+    src = os.path.join(HERE, "host", "mpm_gpu_run.cpp")
+    if force or _newer(RUNNER, [src, LIB] + hdrs):
+        cmd = [CXX, "-O2", "-std=c++17", "-Wall", "-I", CSRC, "-I", os.path.join(ROOT, "include"),
+               src, "-o", RUNNER, "-L", LIBDIR, "-lmpm_b200", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)

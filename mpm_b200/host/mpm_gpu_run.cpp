@@ -1,0 +1,428 @@
+// mpm_gpu_run -- runs an explicit MPM analysis written in the reference's
+// input format on the GPU, through the C ABI of libmpm_b200.so.
+//
+//   mpm_gpu_run -f <input directory> [-i mpm.json] [--precision fp64|mixed]
+//               [--device N] [--parse-only]
+//
+// The host side of the drop-in: it reads what MPMBase reads for an explicit
+// single-phase analysis (mpm_base.tcc:3-207, 347-473, 1550-1625;
+// mpm_explicit.tcc:8-13, 62-108) -- the analysis object (scheme,
+// velocity_update and blending ratio, dt, nsteps, locate_particles, Cundall
+// damping), external loading (gravity, optional ramping time), materials,
+// the mesh and particle files (io_mesh_ascii.tcc: mesh, particles,
+// particle stresses, velocity and friction constraints), particle entity sets
+// (io.cc:159-194) with particle velocity constraints -- and calls the same
+// steps on the library.  At the end it prints the solver duration as
+// mpm_explicit.tcc:191-196 does and writes the particles' PODParticle records
+// (pod_particle.h:12-62; the reference would hand them to H5TBmake_table) to
+// <post_processing.path>/particles-<uuid>-<nsteps>.pod: a 16-byte header
+// ("MPMPOD01", record count as int64) then the records, 74 fields in
+// declaration order at natural alignment.
+//
+// --parse-only reads and checks the input and prints a summary without
+// touching a GPU.
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <cstdlib>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "json_lite.hpp"
+#include "mpm_gpu.h"
+
+using mpm_b200::Json;
+
+namespace {
+
+struct Input {
+  int dim = 3;
+  std::string scheme = "usf", vupdate = "flip", uuid = "mpm", out_path = "results/";
+  double beta = 1.0, dt = 0.0, damping = 0.0, ramp = 0.0;
+  double gravity[3] = {0, 0, 0};
+  long nsteps = 0;
+  bool locate = true;
+  std::vector<double> coords;         // nnodes x dim
+  std::vector<int64_t> cells;         // ncells x nv
+  int64_t nnodes = 0, ncells = 0;
+  struct Mat {
+    int id;
+    std::string type, json;
+  };
+  std::vector<Mat> mats;
+  struct PSet {
+    std::vector<double> x;            // n x dim
+    int material;
+  };
+  std::vector<PSet> psets;
+  std::vector<double> stresses;       // nparticles x 6 (optional)
+  std::vector<int64_t> vnid, fnid;
+  std::vector<int32_t> vdir, fdir, fsign;
+  std::vector<double> vval, fmu;
+  struct PVC {
+    std::vector<int64_t> ids;         // empty: every particle (set -1)
+    int dir;
+    double v;
+  };
+  std::vector<PVC> pvcs;
+  int64_t nparticles() const {
+    int64_t n = 0;
+    for (auto& p : psets) n += (int64_t)p.x.size() / dim;
+    return n;
+  }
+};
+
+std::string read_file(const std::string& path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) throw std::runtime_error("cannot open " + path);
+  std::stringstream ss;
+  ss << f.rdbuf();
+  return ss.str();
+}
+
+// Data lines of a reference ASCII file: comment lines (# or !) and blank
+// lines skipped (io_mesh_ascii.tcc:4-140).
+std::vector<std::string> data_lines(const std::string& path) {
+  std::ifstream f(path);
+  if (!f) throw std::runtime_error("cannot open " + path);
+  std::vector<std::string> out;
+  std::string line;
+  while (std::getline(f, line)) {
+    const size_t a = line.find_first_not_of(" \t\r");
+    if (a == std::string::npos) continue;
+    if (line.find('#') != std::string::npos || line.find('!') != std::string::npos) continue;
+    out.push_back(line.substr(a));
+  }
+  return out;
+}
+
+std::string fmt_double(double v) {
+  char b[40];
+  std::snprintf(b, sizeof(b), "%.17g", v);
+  return b;
+}
+
+std::string dump(const Json& j) {
+  switch (j.type) {
+    case Json::Null: return "null";
+    case Json::Bool: return j.b ? "true" : "false";
+    case Json::Number: return fmt_double(j.num);
+    case Json::String: {
+      std::string s = "\"";
+      for (char c : j.str) {
+        if (c == '"' || c == '\\') s += '\\';
+        s += c;
+      }
+      return s + "\"";
+    }
+    case Json::Array: {
+      std::string s = "[";
+      for (size_t i = 0; i < j.arr.size(); ++i) s += (i ? "," : "") + dump(j.arr[i]);
+      return s + "]";
+    }
+    default: {
+      std::string s = "{";
+      for (size_t i = 0; i < j.obj.size(); ++i)
+        s += (i ? ",\"" : "\"") + j.obj[i].first + "\":" + dump(j.obj[i].second);
+      return s + "}";
+    }
+  }
+}
+
+std::string join(const std::string& dir, const std::string& f) {
+  if (f.empty() || f[0] == '/') return f;
+  return dir.empty() || dir.back() == '/' ? dir + f : dir + "/" + f;
+}
+
+Input read_input(const std::string& dir, const std::string& file) {
+  Input in;
+  const Json root = mpm_b200::parse_json(read_file(join(dir, file)));
+  const Json& an = root.at("analysis");
+  const std::string type = an.at("type").as_string();  // MPMExplicit2D / 3D
+  if (type.find("MPMExplicit") != 0) throw std::runtime_error("analysis type " + type + " is not explicit");
+  in.dim = type.size() >= 2 && type.substr(type.size() - 2) == "2D" ? 2 : 3;
+  in.dt = an.at("dt").as_double();
+  in.nsteps = (long)an.at("nsteps").as_double();
+  if (an.contains("mpm_scheme")) in.scheme = an.at("mpm_scheme").as_string();
+  if (an.contains("velocity_update")) {
+    const Json& vu = an.at("velocity_update");
+    in.vupdate = vu.is_bool() ? (vu.as_bool() ? "pic" : "flip") : vu.as_string();
+  }
+  if (an.contains("velocity_update_settings") && an.at("velocity_update_settings").contains("blending_ratio")) {
+    in.beta = an.at("velocity_update_settings").at("blending_ratio").as_double();
+    if (in.beta < 0. || in.beta > 1.) in.beta = 1.0;  // mpm_base.tcc:89-91
+  }
+  if (an.contains("locate_particles")) in.locate = an.at("locate_particles").as_bool();
+  if (an.contains("damping")) {
+    const Json& d = an.at("damping");
+    if (d.contains("type") && d.at("type").as_string() == "Cundall") in.damping = d.get("damping_factor", 0.0);
+  }
+  if (an.contains("uuid")) in.uuid = an.at("uuid").as_string();
+  if (root.contains("post_processing") && root.at("post_processing").contains("path"))
+    in.out_path = root.at("post_processing").at("path").as_string();
+  if (root.contains("external_loading_conditions") &&
+      root.at("external_loading_conditions").contains("gravity")) {
+    const Json& g = root.at("external_loading_conditions").at("gravity");
+    const Json& gv = g.is_array() ? g : g.at("gravity");
+    if (!g.is_array() && g.contains("ramping_time")) in.ramp = g.at("ramping_time").as_double();
+    if ((int)gv.size() != in.dim) throw std::runtime_error("gravity dimension is invalid");
+    for (int d = 0; d < in.dim; ++d) in.gravity[d] = gv.at(d).as_double();
+  }
+  for (const Json& m : root.at("materials").arr)
+    in.mats.push_back({(int)m.at("id").as_double(), m.at("type").as_string(), dump(m)});
+  // mesh (io_mesh_ascii.tcc: "nnodes ncells", node coordinates, cell node ids)
+  const Json& mesh = root.at("mesh");
+  {
+    const auto lines = data_lines(join(dir, mesh.at("mesh").as_string()));
+    if (lines.empty()) throw std::runtime_error("empty mesh file");
+    std::istringstream h(lines[0]);
+    h >> in.nnodes >> in.ncells;
+    const int nv = in.dim == 2 ? 4 : 8;
+    if ((int64_t)lines.size() < 1 + in.nnodes + in.ncells) throw std::runtime_error("mesh file too short");
+    in.coords.resize((size_t)in.nnodes * in.dim);
+    for (int64_t n = 0; n < in.nnodes; ++n) {
+      std::istringstream l(lines[1 + n]);
+      for (int d = 0; d < in.dim; ++d) l >> in.coords[n * in.dim + d];
+    }
+    in.cells.resize((size_t)in.ncells * nv);
+    for (int64_t c = 0; c < in.ncells; ++c) {
+      std::istringstream l(lines[1 + in.nnodes + c]);
+      for (int k = 0; k < nv; ++k) l >> in.cells[c * nv + k];
+    }
+  }
+  // particles (a count, then coordinates), one file per generator
+  for (const Json& p : root.at("particles").arr) {
+    const Json& g = p.at("generator");
+    if (g.at("type").as_string() != "file") throw std::runtime_error("particle generator must be a file");
+    const auto lines = data_lines(join(dir, g.at("location").as_string()));
+    Input::PSet ps;
+    ps.material = (int)g.at("material_id").as_double();
+    std::istringstream h(lines.at(0));
+    int64_t n = 0;
+    h >> n;
+    ps.x.resize((size_t)n * in.dim);
+    for (int64_t i = 0; i < n; ++i) {
+      std::istringstream l(lines.at(1 + i));
+      for (int d = 0; d < in.dim; ++d) l >> ps.x[i * in.dim + d];
+    }
+    in.psets.push_back(std::move(ps));
+  }
+  if (mesh.contains("particles_stresses")) {
+    const Json& ps = mesh.at("particles_stresses");
+    if (ps.at("type").as_string() != "file") throw std::runtime_error("only file particle stresses are read");
+    const auto lines = data_lines(join(dir, ps.at("location").as_string()));
+    std::istringstream h(lines.at(0));
+    int64_t n = 0;
+    h >> n;
+    in.stresses.resize((size_t)n * 6);
+    for (int64_t i = 0; i < n; ++i) {
+      std::istringstream l(lines.at(1 + i));
+      for (int k = 0; k < 6; ++k) l >> in.stresses[i * 6 + k];
+    }
+  }
+  if (mesh.contains("boundary_conditions")) {
+    const Json& bc = mesh.at("boundary_conditions");
+    if (bc.contains("velocity_constraints"))
+      for (const Json& v : bc.at("velocity_constraints").arr)
+        for (const auto& line : data_lines(join(dir, v.at("file").as_string()))) {
+          std::istringstream l(line);
+          int64_t n;
+          int d;
+          double val;
+          l >> n >> d >> val;
+          in.vnid.push_back(n);
+          in.vdir.push_back(d);
+          in.vval.push_back(val);
+        }
+    if (bc.contains("friction_constraints"))
+      for (const Json& v : bc.at("friction_constraints").arr)
+        for (const auto& line : data_lines(join(dir, v.at("file").as_string()))) {
+          std::istringstream l(line);
+          int64_t n;
+          int d, sgn;
+          double mu;
+          l >> n >> d >> sgn >> mu;
+          in.fnid.push_back(n);
+          in.fdir.push_back(d);
+          in.fsign.push_back(sgn);
+          in.fmu.push_back(mu);
+        }
+    if (bc.contains("particles_velocity_constraints")) {
+      std::map<long, std::vector<int64_t>> sets;
+      if (mesh.contains("entity_sets")) {
+        const Json es = mpm_b200::parse_json(read_file(join(dir, mesh.at("entity_sets").as_string())));
+        if (es.contains("particle_sets"))
+          for (const Json& s : es.at("particle_sets").arr) {
+            std::vector<int64_t> ids;
+            for (const Json& i : s.at("set").arr) ids.push_back((int64_t)i.as_double());
+            sets[(long)s.at("id").as_double()] = ids;
+          }
+      }
+      for (const Json& c : bc.at("particles_velocity_constraints").arr) {
+        const long set = (long)c.at("pset_id").as_double();
+        Input::PVC p;
+        p.dir = (int)c.at("dir").as_double();
+        p.v = c.at("velocity").as_double();
+        if (set != -1) {
+          auto it = sets.find(set);
+          if (it == sets.end()) throw std::runtime_error("unknown particle set " + std::to_string(set));
+          p.ids = it->second;
+        }
+        in.pvcs.push_back(std::move(p));
+      }
+    }
+  }
+  return in;
+}
+
+// PODParticle data members at natural alignment (no vtable)
+struct PodRecord {
+  uint64_t id;
+  double mass, volume, pressure;
+  double coord[3], displacement[3], nsize[3], velocity[3], acceleration[3];
+  double stress[6], strain[6], defgrad[9];
+  bool initialise_mapping_matrix;
+  double mapping_matrix[9];
+  bool status;
+  uint64_t cell_id;
+  uint32_t material_id, nstate_vars;
+  double svars[20];
+};
+
+void pod_layout(size_t* off, size_t* sz) {
+  int f = 0;
+  auto put = [&](size_t o, size_t s, int count) {
+    for (int k = 0; k < count; ++k) {
+      off[f] = o + k * s;
+      sz[f] = s;
+      ++f;
+    }
+  };
+  put(offsetof(PodRecord, id), 8, 1);
+  put(offsetof(PodRecord, mass), 8, 1);
+  put(offsetof(PodRecord, volume), 8, 1);
+  put(offsetof(PodRecord, pressure), 8, 1);
+  put(offsetof(PodRecord, coord), 8, 3);
+  put(offsetof(PodRecord, displacement), 8, 3);
+  put(offsetof(PodRecord, nsize), 8, 3);
+  put(offsetof(PodRecord, velocity), 8, 3);
+  put(offsetof(PodRecord, acceleration), 8, 3);
+  put(offsetof(PodRecord, stress), 8, 6);
+  put(offsetof(PodRecord, strain), 8, 6);
+  put(offsetof(PodRecord, defgrad), 8, 9);
+  put(offsetof(PodRecord, initialise_mapping_matrix), 1, 1);
+  put(offsetof(PodRecord, mapping_matrix), 8, 9);
+  put(offsetof(PodRecord, status), 1, 1);
+  put(offsetof(PodRecord, cell_id), 8, 1);
+  put(offsetof(PodRecord, material_id), 4, 1);
+  put(offsetof(PodRecord, nstate_vars), 4, 1);
+  put(offsetof(PodRecord, svars), 8, 20);
+}
+
+int check(mpm_gpu_t h, int rc, const char* what) {
+  if (rc != MPM_OK) {
+    std::fprintf(stderr, "mpm_gpu_run: %s failed (%d): %s\n", what, rc, h ? mpm_gpu_last_error(h) : "");
+    std::exit(1);
+  }
+  return rc;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  std::string dir, file = "mpm.json", precision = "fp64";
+  int device = 0;
+  bool parse_only = false;
+  for (int i = 1; i < argc; ++i) {
+    const std::string a = argv[i];
+    if (a == "-f" && i + 1 < argc) dir = argv[++i];
+    else if (a == "-i" && i + 1 < argc) file = argv[++i];
+    else if (a == "--precision" && i + 1 < argc) precision = argv[++i];
+    else if (a == "--device" && i + 1 < argc) device = std::atoi(argv[++i]);
+    else if (a == "--parse-only") parse_only = true;
+    else {
+      std::fprintf(stderr, "usage: mpm_gpu_run -f <dir> [-i mpm.json] [--precision fp64|mixed] "
+                           "[--device N] [--parse-only]\n");
+      return 2;
+    }
+  }
+  Input in;
+  try {
+    in = read_input(dir, file);
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "mpm_gpu_run: %s\n", e.what());
+    return 1;
+  }
+  const int64_t np = in.nparticles();
+  std::printf("dim %d nodes %lld cells %lld particles %lld materials %zu scheme %s velocity_update %s "
+              "dt %g nsteps %ld velocity_constraints %zu friction_constraints %zu "
+              "particle_velocity_constraints %zu stresses %s\n",
+              in.dim, (long long)in.nnodes, (long long)in.ncells, (long long)np, in.mats.size(),
+              in.scheme.c_str(), in.vupdate.c_str(), in.dt, in.nsteps, in.vnid.size(), in.fnid.size(),
+              in.pvcs.size(), in.stresses.empty() ? "no" : "yes");
+  if (parse_only) return 0;
+
+  mpm_gpu_config cfg{};
+  cfg.dim = in.dim;
+  cfg.scheme = in.scheme == "usl" ? MPM_SCHEME_USL : MPM_SCHEME_USF;
+  cfg.velocity_update = in.vupdate == "pic" ? MPM_VELOCITY_PIC : MPM_VELOCITY_FLIP;
+  cfg.precision = precision == "mixed" ? MPM_PRECISION_MIXED : MPM_PRECISION_FP64;
+  cfg.blending_ratio = in.beta;
+  cfg.dt = in.dt;
+  cfg.damping_factor = in.damping;
+  for (int d = 0; d < 3; ++d) cfg.gravity[d] = in.gravity[d];
+  cfg.gravity_ramping_time = in.ramp;
+  cfg.locate_particles = in.locate ? 1 : 0;
+  cfg.device = device;
+  mpm_gpu_t h = nullptr;
+  check(nullptr, mpm_gpu_create(&cfg, &h), "create");
+  check(h, mpm_gpu_set_mesh(h, in.nnodes, in.coords.data(), in.ncells, in.dim == 2 ? 4 : 8,
+                            in.cells.data()), "set_mesh");
+  for (auto& m : in.mats) check(h, mpm_gpu_add_material(h, m.id, m.type.c_str(), m.json.c_str()), "add_material");
+  if (!in.vnid.empty())
+    check(h, mpm_gpu_add_velocity_constraints(h, (int64_t)in.vnid.size(), in.vnid.data(), in.vdir.data(),
+                                              in.vval.data()), "velocity constraints");
+  if (!in.fnid.empty())
+    check(h, mpm_gpu_add_friction_constraints(h, (int64_t)in.fnid.size(), in.fnid.data(), in.fdir.data(),
+                                              in.fsign.data(), in.fmu.data()), "friction constraints");
+  for (auto& p : in.psets)
+    check(h, mpm_gpu_add_particles(h, (int64_t)p.x.size() / in.dim, p.x.data(), p.material), "add_particles");
+  check(h, mpm_gpu_initialise(h), "initialise");
+  if (!in.stresses.empty())
+    check(h, mpm_gpu_assign_particle_stresses(h, (int64_t)in.stresses.size() / 6, in.stresses.data()),
+          "particle stresses");
+  for (auto& c : in.pvcs)
+    check(h, mpm_gpu_add_particle_velocity_constraint(h, c.ids.empty() ? -1 : (int64_t)c.ids.size(),
+                                                      c.ids.data(), c.dir, c.v), "particle velocity constraint");
+  double ms = 0.0;
+  check(h, mpm_gpu_step_timed(h, in.nsteps, &ms), "step");
+  std::printf("Explicit solver duration: %.3f ms\n", ms);
+
+  std::vector<PodRecord> rec((size_t)np);
+  std::memset(rec.data(), 0, rec.size() * sizeof(PodRecord));
+  size_t off[74], sz[74];
+  pod_layout(off, sz);
+  int64_t n = 0;
+  check(h, mpm_gpu_write_pod(h, rec.data(), np, &n, sizeof(PodRecord), off, sz, 74), "write_pod");
+  const std::string out = join(dir, in.out_path);
+  std::string cmd = "mkdir -p '" + out + "'";
+  if (std::system(cmd.c_str()) != 0) std::fprintf(stderr, "mpm_gpu_run: cannot create %s\n", out.c_str());
+  const std::string path = join(out, "particles-" + in.uuid + "-" + std::to_string(in.nsteps) + ".pod");
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) {
+    std::fprintf(stderr, "mpm_gpu_run: cannot write %s\n", path.c_str());
+    return 1;
+  }
+  std::fwrite("MPMPOD01", 1, 8, f);
+  std::fwrite(&n, sizeof(n), 1, f);
+  std::fwrite(rec.data(), sizeof(PodRecord), (size_t)n, f);
+  std::fclose(f);
+  std::printf("wrote %lld records to %s\n", (long long)n, path.c_str());
+  mpm_gpu_destroy(h);
+  return 0;
+}

@@ -340,8 +340,9 @@ def apply_problem(prob, s, with_particles=True):
 
 def write_reference_input(prob, outdir, nsteps=None, output_steps=None):
     """Write the problem as the reference's input: mpm.json, mesh.txt,
-    particles.txt, velocity-constraints.txt, friction-constraints.txt
-    (formats of io_mesh_ascii.tcc and tests/io/write_mesh_particles.cc)."""
+    particles-<k>.txt, velocity-constraints.txt, friction-constraints.txt,
+    particles-stresses.txt and entity_sets.json (formats of io_mesh_ascii.tcc,
+    tests/io/write_mesh_particles.cc, mpm_base.tcc:1550-1625, io.cc:159-194)."""
     os.makedirs(outdir, exist_ok=True)
     dim = prob.dim
     with open(os.path.join(outdir, "mesh.txt"), "w") as f:
@@ -371,6 +372,13 @@ def write_reference_input(prob, outdir, nsteps=None, output_steps=None):
             for n, d, s, m in zip(*prob.friction_constraints):
                 f.write(f"{int(n)}\t{int(d)}\t{int(s)}\t{repr(float(m))}\n")
         bcs["friction_constraints"] = [{"file": "friction-constraints.txt"}]
+    psets, pvcs = [], []
+    for k, (pids, d, v) in enumerate(prob.particle_velocity_constraints):
+        ids = np.arange(prob.nparticles) if pids is None else np.asarray(pids)
+        psets.append({"id": k, "set": [int(i) for i in ids]})
+        pvcs.append({"pset_id": k, "dir": int(d), "velocity": float(v)})
+    if pvcs:
+        bcs["particles_velocity_constraints"] = pvcs
     a = prob.analysis
     nsteps = nsteps if nsteps is not None else a.get("nsteps", 1)
     cfg = {
@@ -383,16 +391,27 @@ def write_reference_input(prob, outdir, nsteps=None, output_steps=None):
                                      "material_id": mid, "type": "file"}}
                       for k, (name, mid) in enumerate(pfiles)],
         "materials": [dict(props, id=mid, type=mtype) for mid, mtype, props in prob.materials],
-        "external_loading_conditions": {"gravity": list(a.get("gravity", [0.0] * dim))},
+        "external_loading_conditions": (
+            {"gravity": {"gravity": list(a.get("gravity", [0.0] * dim)),
+                         "ramping_time": a["gravity_ramping_time"]}}
+            if a.get("gravity_ramping_time", 0.0) > 0 else
+            {"gravity": list(a.get("gravity", [0.0] * dim))}),
         "analysis": {"type": f"MPMExplicit{dim}D", "mpm_scheme": a.get("scheme", "usf"),
                      "velocity_update": a.get("velocity_update", "flip"),
                      "locate_particles": a.get("locate_particles", True), "dt": a["dt"],
                      "uuid": prob.name, "nsteps": nsteps,
+                     "velocity_update_settings": {"blending_ratio": a.get("blending_ratio", 1.0)},
                      "damping": {"type": "Cundall", "damping_factor": a.get("damping_factor", 0.0)}},
         "post_processing": {"path": "results/", "output_steps": output_steps or nsteps},
     }
+    if prob.initial_stress is not None:
+        with open(os.path.join(outdir, "particles-stresses.txt"), "w") as f:
+            f.write(f"{len(prob.initial_stress)}\n")
+            for row in prob.initial_stress:
+                f.write("\t".join(repr(float(v)) for v in row) + "\n")
+        cfg["mesh"]["particles_stresses"] = {"type": "file", "location": "particles-stresses.txt"}
     with open(os.path.join(outdir, "mpm.json"), "w") as f:
         json.dump(cfg, f, indent=2)
     with open(os.path.join(outdir, "entity_sets.json"), "w") as f:
-        json.dump({"node_sets": [], "particle_sets": []}, f)
+        json.dump({"node_sets": [], "particle_sets": psets}, f)
     return os.path.join(outdir, "mpm.json")
