@@ -49,14 +49,15 @@ typedef enum {
   MPM_ERR_UNSUPPORTED = -7   /* feature outside the implemented path */
 } mpm_status;
 
-enum { MPM_SCHEME_USF = 0, MPM_SCHEME_USL = 1 };
+enum { MPM_SCHEME_USF = 0, MPM_SCHEME_USL = 1, MPM_SCHEME_MUSL = 2 };
 enum { MPM_VELOCITY_FLIP = 0, MPM_VELOCITY_PIC = 1 };
 enum { MPM_PRECISION_FP64 = 0, MPM_PRECISION_MIXED = 1 };
 
 /* Analysis settings (mpm_base.tcc:3-207; mpm_explicit.tcc:8-13, 145-153). */
 typedef struct {
   int32_t dim;              /* 2 (quad4 / ED2Q4) or 3 (hex8 / ED3H8) */
-  int32_t scheme;           /* MPM_SCHEME_USF / MPM_SCHEME_USL */
+  int32_t scheme;           /* MPM_SCHEME_USF / MPM_SCHEME_USL / MPM_SCHEME_MUSL (FP64;
+                               mpm_scheme_musl.tcc:20-35) */
   int32_t velocity_update;  /* MPM_VELOCITY_FLIP / MPM_VELOCITY_PIC */
   int32_t precision;        /* MPM_PRECISION_FP64: every quantity in FP64, rounding as the
                                reference's CPU run (the parity mode);

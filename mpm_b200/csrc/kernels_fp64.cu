@@ -780,6 +780,96 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
   if (t == 0) bulk::store_wait_all();
 }
 
+// MUSL particle kinematics (particle.tcc:994-1067 as in k_g2p): the new
+// positions go to xnext, so that the second mapping of mass and momentum and
+// the stress update of the step still see the step-start positions (the
+// reference keeps each particle's shape functions until the next step).
+template <int DIM, bool FLIP>
+__global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p_musl(DevState s, double dt,
+                                                                      double beta) {
+  constexpr int NV = Elem<DIM>::NV;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.np) return;
+  const int c = s.cell[p];
+  if (c < 0) return;
+  const int64_t np = s.np, nn = s.nn;
+  double x[DIM], xi[DIM], N[NV], X[NV * DIM];
+  int nid[NV];
+  load_x<DIM>(s, p, x);
+  const CellGeom& g = s.geom[c];
+  local_xi<DIM>(x, g.centroid, g.len, xi);
+  shapefn<DIM>(xi, N);
+  cell_nodes_coords<DIM>(s, c, nid, X);
+  double nvel[DIM], nacc[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    const int n = nid[i];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + n];
+    if constexpr (FLIP) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * s.nf[(int64_t)(NF<DIM>::ACC + d) * nn + n];
+    }
+  }
+  double v[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) v[d] = s.pf[(int64_t)(PF<DIM>::V + d) * np + p];
+  if constexpr (FLIP) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] += nacc[d] * dt;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = beta * v[d] + (1.0 - beta) * nvel[d];
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = nvel[d];
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    s.xnext[(int64_t)d * np + p] = x[d] + nvel[d] * dt;
+    s.pf[(int64_t)(PF<DIM>::U + d) * np + p] += nvel[d] * dt;
+  }
+  const int pv = s.pvc[p];
+  if (pv >= 0) {
+    const ParticleVC& r = s.pvcs[pv];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      if (r.mask & (1u << d)) v[d] = r.value[d];
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) s.pf[(int64_t)(PF<DIM>::V + d) * np + p] = v[d];
+}
+
+// MUSL end of step: the new positions replace the old, then locate
+template <int DIM>
+__global__ void __launch_bounds__(128) k_commit_locate(DevState s) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.np) return;
+  const int c = s.cell[p];
+  if (c < 0) return;
+  const int64_t np = s.np;
+  double xn[DIM];
+  bool finite = true;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    xn[d] = s.xnext[(int64_t)d * np + p];
+    s.pf[(int64_t)(PF<DIM>::X + d) * np + p] = xn[d];
+    finite = finite && isfinite(xn[d]);
+  }
+  if (!finite) {
+    raise_err(s, ERR_NONFINITE);
+    s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+    return;
+  }
+  const int nc = locate_near<DIM>(s, xn, c);
+  if (nc >= 0) {
+    if (nc != c) s.cell[p] = nc;
+  } else {
+    s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+  }
+}
+
 // The MohrCoulomb returns deferred by stress_update, one thread per listed
 // particle (grid-stride), from the particle's stress and state before the
 // step's update: the same call, with the same inputs, as the undeferred update.
@@ -899,7 +989,35 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
   pr.begin(K_SORT, st);
   counting_sort_impl(s, st);
   pr.end(K_SORT, st);
-  if (a.scheme == 1) {  // USL
+  if (a.scheme == 2) {  // MUSL (mpm_scheme_musl.tcc)
+    pr.begin(K_P2G, st);
+    k_p2g_cells<DIM, 2><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    pr.end(K_P2G, st);
+    pr.begin(K_NODES_VEL, st);
+    k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    pr.end(K_NODES_VEL, st);
+    pr.begin(K_G2P, st);
+    if (a.flip)
+      k_g2p_musl<DIM, true><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
+    else
+      k_g2p_musl<DIM, false><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
+    pr.end(K_G2P, st);
+    // mass and momentum again with the updated velocities, nodal velocity,
+    // then the stress update (mpm_scheme_musl.tcc:13-35)
+    pr.begin(K_P2G_FORCES, st);
+    k_p2g_cells<DIM, 0><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    pr.end(K_P2G_FORCES, st);
+    pr.begin(K_NODES_ACC, st);
+    k_nodes<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    pr.end(K_NODES_ACC, st);
+    pr.begin(K_STRESS, st);
+    k_stress<DIM><<<pb128, 128, 0, st>>>(s, a.dt);
+    pr.end(K_STRESS, st);
+    mc_returns();
+    pr.begin(K_LOCATE, st);
+    k_commit_locate<DIM><<<pb128, 128, 0, st>>>(s);
+    pr.end(K_LOCATE, st);
+  } else if (a.scheme == 1) {  // USL
     pr.begin(K_P2G, st);
     k_p2g_cells<DIM, 2><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
     pr.end(K_P2G, st);

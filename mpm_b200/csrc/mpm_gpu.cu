@@ -190,7 +190,7 @@ struct mpm_gpu_solver {
 
   // device
   DevState ds;
-  DevBuf<double> d_pf, d_sv, d_nf, d_ncoord;
+  DevBuf<double> d_pf, d_sv, d_nf, d_ncoord, d_xnext;
   DevBuf<int32_t> d_cell, d_bc_index, d_cell_nodes, d_nb_off, d_nb, d_bin_off, d_bin_cells, d_lost;
   DevBuf<uint16_t> d_mat;
   DevBuf<uint8_t> d_active;
@@ -668,6 +668,7 @@ void allocate_particles(mpm_gpu_t h) {
   if (h->mixed) h->d_pm.alloc((size_t)h->nfields_m() * np);
   h->d_cell.alloc(np);
   h->d_mat.alloc(np);
+  if (h->cfg.scheme == MPM_SCHEME_MUSL) h->d_xnext.alloc((size_t)h->dim * np);
   h->d_lost.alloc(std::max<int64_t>(1, np));
   h->d_rank.alloc(std::max<int64_t>(1, np));
   h->d_order.alloc(std::max<int64_t>(1, np));
@@ -728,6 +729,7 @@ void refresh_state(mpm_gpu_t h) {
   s.bsum = h->d_bsum.p;
   s.partials = h->d_partials.p;
   s.lost = h->d_lost.p;
+  s.xnext = h->d_xnext.p;
   s.nlost = h->d_words.p;
   s.err = h->d_words.p + 1;
   s.nplastic = h->d_words.p + 2;
@@ -972,7 +974,11 @@ int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out) {
   if (!cfg || !out) return MPM_ERR_INVALID;
   *out = nullptr;
   if (cfg->dim != 2 && cfg->dim != 3) return MPM_ERR_INVALID;
-  if (cfg->scheme != MPM_SCHEME_USF && cfg->scheme != MPM_SCHEME_USL) return MPM_ERR_UNSUPPORTED;
+  if (cfg->scheme != MPM_SCHEME_USF && cfg->scheme != MPM_SCHEME_USL &&
+      cfg->scheme != MPM_SCHEME_MUSL)
+    return MPM_ERR_UNSUPPORTED;
+  if (cfg->scheme == MPM_SCHEME_MUSL && cfg->precision != MPM_PRECISION_FP64)
+    return MPM_ERR_UNSUPPORTED;
   if (cfg->velocity_update != MPM_VELOCITY_FLIP && cfg->velocity_update != MPM_VELOCITY_PIC)
     return MPM_ERR_UNSUPPORTED;
   if (cfg->precision != MPM_PRECISION_FP64 && cfg->precision != MPM_PRECISION_MIXED)

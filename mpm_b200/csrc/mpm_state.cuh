@@ -124,6 +124,7 @@ struct DevState {
   int32_t* bsum = nullptr;       // scan block totals
   double* partials = nullptr;    // [ncells][NV][1 + 3 DIM]
 
+  double* xnext = nullptr;       // [DIM][np] MUSL: positions at the end of the step
   int32_t* lost = nullptr;       // [np] particles not found in cell or neighbours
   unsigned* nlost = nullptr;
   // particles whose MohrCoulomb trial stress is plastic this step, with the

@@ -369,7 +369,7 @@ int main(int argc, char** argv) {
 
   mpm_gpu_config cfg{};
   cfg.dim = in.dim;
-  cfg.scheme = in.scheme == "usl" ? MPM_SCHEME_USL : MPM_SCHEME_USF;
+  cfg.scheme = in.scheme == "usl" ? MPM_SCHEME_USL : (in.scheme == "musl" ? MPM_SCHEME_MUSL : MPM_SCHEME_USF);
   cfg.velocity_update = in.vupdate == "pic" ? MPM_VELOCITY_PIC : MPM_VELOCITY_FLIP;
   cfg.precision = precision == "mixed" ? MPM_PRECISION_MIXED : MPM_PRECISION_FP64;
   cfg.blending_ratio = in.beta;

@@ -14,7 +14,7 @@ import numpy as np
 from . import _native
 from ._native import MPMError
 
-SCHEMES = {"usf": 0, "usl": 1}
+SCHEMES = {"usf": 0, "usl": 1, "musl": 2}
 VELOCITY_UPDATES = {"flip": 0, "pic": 1}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 

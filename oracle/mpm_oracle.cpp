@@ -1277,6 +1277,20 @@ void one_step(Oracle& o) {
   phase_node_update(o, dt);
   phase_g2p(o, dt);
   if (o.cfg.scheme == 1) compute_stress_strain(o, dt);  // mpm_scheme_usl.tcc:14-17
+  if (o.cfg.scheme == 2) {
+    // mpm_scheme_musl.tcc:20-35: mass and momentum of the active nodes set to
+    // zero and mapped again with the updated particle velocities (the
+    // particles keep the shape functions of the step start), nodal velocity,
+    // then the stress update on it (mpm_scheme_musl.tcc:13-17)
+    for (auto& n : o.nodes)
+      if (n.status) {
+        n.mass = 0;
+        for (int d = 0; d < 3; ++d) n.mom[d] = 0;
+      }
+    phase_p2g_mass_momentum(o);
+    phase_compute_velocity(o);
+    compute_stress_strain(o, dt);
+  }
 }
 
 }  // namespace

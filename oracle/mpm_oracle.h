@@ -27,7 +27,7 @@ extern "C" {
 
 typedef struct {
   int32_t dim;              /* 2 or 3 */
-  int32_t scheme;           /* 0 = USF, 1 = USL */
+  int32_t scheme;           /* 0 = USF, 1 = USL, 2 = MUSL */
   int32_t velocity_update;  /* 0 = FLIP, 1 = PIC */
   int32_t locate_particles; /* 1: unlocatable particle is an error, 0: removed */
   double blending_ratio;

@@ -182,7 +182,7 @@ class Oracle:
                  gravity_ramping_time=0.0, locate_particles=True, nthreads=1):
         cfg = Config()
         cfg.dim = dim
-        cfg.scheme = {"usf": 0, "usl": 1}[scheme]
+        cfg.scheme = {"usf": 0, "usl": 1, "musl": 2}[scheme]
         cfg.velocity_update = {"flip": 0, "pic": 1}[velocity_update]
         cfg.locate_particles = 1 if locate_particles else 0
         cfg.blending_ratio = blending_ratio

@@ -268,3 +268,18 @@ def test_footing_on_slope_two_materials(scheme):
         assert_parity(g, o, label=f"footing step {s}")
     fp = prob.particle_velocity_constraints[0][0]
     assert np.allclose(g["v"][fp, 2], -0.05)
+
+
+@pytest.mark.parametrize("vupd", ["flip", "pic"])
+def test_2d_linear_elastic_column_musl(vupd):
+    """MUSL (mpm_scheme_musl.tcc): a second mapping of mass and momentum with
+    the updated particle velocities before the stress update."""
+    prob = small_column_2d(scheme="musl", velocity_update=vupd)
+    for s, g, o in _run_both(prob, [1, 30, 100]):
+        assert_parity(g, o, label=f"2D MUSL {vupd} step {s}")
+
+
+def test_3d_mohr_coulomb_column_musl():
+    prob = small_column_3d(scheme="musl", c=2000., psi=5.)
+    for s, g, o in _run_both(prob, [1, 20, 50]):
+        assert_parity(g, o, label=f"3D MUSL step {s}")
