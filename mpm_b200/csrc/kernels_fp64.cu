@@ -22,6 +22,10 @@
 #include "mpm_kernels.h"
 #include "mpm_state.cuh"
 
+#ifndef MPM_P2G_LANES_3D
+#define MPM_P2G_LANES_3D 2  // lanes per hex8 cell in P2G (2: 4 slots each, 4: 2 slots each)
+#endif
+
 // Minimum resident blocks per SM requested from the register allocator for
 // the two particle kernels (occupancy versus spills, tuned on the B200).
 #ifndef MPM_G2P_MIN_BLOCKS
@@ -32,6 +36,9 @@
 #endif
 #ifndef MPM_P2G_MIN_BLOCKS
 #define MPM_P2G_MIN_BLOCKS 2  // more blocks spill the 40 lane accumulators: slower
+#endif
+#ifndef MPM_P2G_BOX_MIN_BLOCKS
+#define MPM_P2G_BOX_MIN_BLOCKS 3  // box cells hold no nodal coordinates: 0.53 -> 0.45 ms (4M, 3D)
 #endif
 
 namespace mpm_b200 {
@@ -111,11 +118,11 @@ __global__ void __launch_bounds__(256) k_fill(DevState s) {
 //   mass m N (particle.tcc:643-655), momentum (m N) v, body force (g m) N
 //   (:893-898), internal force -V (dN . sigma) (:915-949).
 // MODE 0: mass and momentum; 1: forces; 2: all.
-template <int DIM, int MODE>
-__global__ void __launch_bounds__(128, MPM_P2G_MIN_BLOCKS) k_p2g_cells(DevState s, double g0,
-                                                                       double g1, double g2) {
+template <int DIM, int MODE, bool BOX>
+__global__ void __launch_bounds__(128, BOX ? MPM_P2G_BOX_MIN_BLOCKS : MPM_P2G_MIN_BLOCKS)
+    k_p2g_cells(DevState s, double g0, double g1, double g2) {
   constexpr int NV = Elem<DIM>::NV;
-  constexpr int LPC = DIM == 3 ? 2 : 1;
+  constexpr int LPC = DIM == 3 ? MPM_P2G_LANES_3D : 1;
   constexpr int SPL = NV / LPC;
   constexpr int NVAL = PV<DIM>::N;
   constexpr bool MM = MODE != 1, FORCES = MODE != 0;
@@ -144,8 +151,8 @@ __global__ void __launch_bounds__(128, MPM_P2G_MIN_BLOCKS) k_p2g_cells(DevState 
   }
   if (!valid || n == 0) return;
   int nid[NV];
-  double X[NV * DIM];
-  cell_nodes_coords<DIM>(s, (int)c, nid, X);
+  double X[NV * DIM];  // nodal coordinates (J^-1 of a box cell needs none)
+  if constexpr (!BOX) cell_nodes_coords<DIM>(s, (int)c, nid, X);
   const CellGeom g = s.geom[c];
   const int64_t np = s.np;
   double acc[SPL][NVAL];
@@ -159,7 +166,20 @@ __global__ void __launch_bounds__(128, MPM_P2G_MIN_BLOCKS) k_p2g_cells(DevState 
     double x[DIM], xi[DIM], Nk[SPL], Gk[SPL * DIM];
     load_x<DIM>(s, p, x);
     local_xi<DIM>(x, g.centroid, g.len, xi);
-    lane_shape<DIM>(xi, h, Nk, Gk);
+    if constexpr (DIM == 3 && LPC == 4) {
+      // lane h owns slots 2h, 2h+1: the half (z factor) h / 2, pair h % 2
+      double N4[4], G4[12];
+      lane_shape<DIM>(xi, h / 2, N4, G4);
+      const int k0 = (h % 2) * 2;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        Nk[k] = N4[k0 + k];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Gk[k * 3 + d] = G4[(k0 + k) * 3 + d];
+      }
+    } else {
+      lane_shape<DIM>(xi, h, Nk, Gk);
+    }
     const double m = s.pf[(int64_t)PF<DIM>::MASS * np + p];
     if constexpr (MM) {
       double v[DIM];
@@ -174,8 +194,7 @@ __global__ void __launch_bounds__(128, MPM_P2G_MIN_BLOCKS) k_p2g_cells(DevState 
       }
     }
     if constexpr (FORCES) {
-      double inv[DIM * DIM];
-      jacobian_inverse<DIM>(xi, X, inv);
+      const CellMap<DIM, BOX, double> map = cell_map<DIM, BOX>(s, (int)c, xi, X);
       const double sc = -1. * s.pf[(int64_t)PF<DIM>::VOL * np + p];
       double sig[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -185,13 +204,7 @@ __global__ void __launch_bounds__(128, MPM_P2G_MIN_BLOCKS) k_p2g_cells(DevState 
 #pragma unroll
         for (int d = 0; d < DIM; ++d) acc[k][PV<DIM>::FEXT + d] += (gv[d] * m) * Nk[k];
         double Dn[DIM];
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) {
-          double a = Gk[k * DIM + 0] * inv[q * DIM + 0];
-#pragma unroll
-          for (int r = 1; r < DIM; ++r) a = a + Gk[k * DIM + r] * inv[q * DIM + r];
-          Dn[q] = a;
-        }
+        map.grad(&Gk[k * DIM], Dn);
         double f[DIM];
         if constexpr (DIM == 2) {
           f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
@@ -514,17 +527,17 @@ __device__ __forceinline__ void stress_update(const DevState& s, const Row& r, i
 }
 
 // dN/dx of all local nodes at xi
-template <int DIM>
-__device__ __forceinline__ void dn_dx_all(const double* xi, const double* X, double* D) {
+template <int DIM, bool BOX>
+__device__ __forceinline__ void dn_dx_all(const DevState& s, int c, const double* xi,
+                                          const double* X, double* D) {
   constexpr int NV = Elem<DIM>::NV;
-  double inv[DIM * DIM];
-  jacobian_inverse<DIM>(xi, X, inv);
+  const CellMap<DIM, BOX, double> map = cell_map<DIM, BOX>(s, c, xi, X);
 #pragma unroll
-  for (int n = 0; n < NV; ++n) dn_dx_node<DIM>(xi, inv, n, &D[n * DIM]);
+  for (int n = 0; n < NV; ++n) dn_dx_node<DIM>(xi, map, n, &D[n * DIM]);
 }
 
 // USF: the stress update with the velocities of compute_velocity
-template <int DIM>
+template <int DIM, bool BOX>
 __global__ void __launch_bounds__(128) k_stress(DevState s, double dt) {
   constexpr int NV = Elem<DIM>::NV;
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -536,15 +549,15 @@ __global__ void __launch_bounds__(128) k_stress(DevState s, double dt) {
   load_x<DIM>(s, p, x);
   const CellGeom& g = s.geom[c];
   local_xi<DIM>(x, g.centroid, g.len, xi);
-  cell_nodes_coords<DIM>(s, c, nid, X);
-  dn_dx_all<DIM>(xi, X, D);
+  cell_nodes_for<DIM, BOX>(s, c, nid, X);
+  dn_dx_all<DIM, BOX>(s, c, xi, X, D);
   stress_update<DIM>(s, GlobalRow{s, p}, c, nid, D, dt);
 }
 
 // --------------------------------------------------------------------- G2P
 // particle.tcc:994-1067 FLIP / PIC; mesh.tcc:1454-1467 particle velocity
 // constraints; USL stress update (mpm_scheme_usl.tcc:14-17); locate.
-template <int DIM, bool STRESS, bool FLIP>
+template <int DIM, bool STRESS, bool FLIP, bool BOX>
 __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, double dt,
                                                                  double beta) {
   constexpr int NV = Elem<DIM>::NV;
@@ -559,7 +572,7 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
   const CellGeom& g = s.geom[c];
   local_xi<DIM>(x, g.centroid, g.len, xi);
   shapefn<DIM>(xi, N);
-  cell_nodes_coords<DIM>(s, c, nid, X);
+  cell_nodes_for<DIM, BOX>(s, c, nid, X);
   double nvel[DIM], nacc[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.;
@@ -603,7 +616,7 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
   for (int d = 0; d < DIM; ++d) s.pf[(int64_t)(PF<DIM>::V + d) * np + p] = v[d];
   if constexpr (STRESS) {
     double D[NV * DIM];
-    dn_dx_all<DIM>(xi, X, D);
+    dn_dx_all<DIM, BOX>(s, c, xi, X, D);
     stress_update<DIM>(s, GlobalRow{s, p}, c, nid, D, dt);
   }
   bool finite = true;
@@ -628,7 +641,7 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
 // material, velocity-constraint slot) and phase B (stress, strain, F,
 // volume, density, MohrCoulomb state).  The threads gather nodal values while
 // phase B is in flight, update the staged rows in place and one thread stores
-// the rows back with bulk copies.  The arithmetic is k_g2p<DIM, true, FLIP>'s.
+// the rows back with bulk copies.  The arithmetic is k_g2p<DIM, true, FLIP, BOX>'s.
 static_assert(STAGE_T == PAD_PARTICLES, "staged slices are whole padded blocks");
 template <int DIM>
 constexpr int staged_rows() { return PF<DIM>::MASS; }  // fields X .. RHO
@@ -637,7 +650,7 @@ constexpr size_t staged_smem_bytes(bool mc) {
   return (size_t)(staged_rows<DIM>() + (mc ? SV_N : 0)) * STAGE_T * 8 + STAGE_T * (4 + 2 + 2);
 }
 
-template <int DIM, bool FLIP>
+template <int DIM, bool FLIP, bool BOX>
 __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
     k_g2p_staged(DevState s, double dt, double beta) {
   constexpr int NV = Elem<DIM>::NV;
@@ -689,7 +702,7 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
     const CellGeom& g = s.geom[c];
     local_xi<DIM>(x, g.centroid, g.len, xi);
     shapefn<DIM>(xi, N);
-    cell_nodes_coords<DIM>(s, c, nid, X);
+    cell_nodes_for<DIM, BOX>(s, c, nid, X);
     double nvel[DIM], nacc[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.;
@@ -737,8 +750,8 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
     // node ids and coordinates again rather than kept live across the wait
     double X[NV * DIM], D[NV * DIM];
     int nid[NV];
-    cell_nodes_coords<DIM>(s, c, nid, X);
-    dn_dx_all<DIM>(xi, X, D);
+    cell_nodes_for<DIM, BOX>(s, c, nid, X);
+    dn_dx_all<DIM, BOX>(s, c, xi, X, D);
     stress_update<DIM>(s, r, c, nid, D, dt);
   }
   bulk::fence_shared_to_async();
@@ -784,7 +797,7 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
 // positions go to xnext, so that the second mapping of mass and momentum and
 // the stress update of the step still see the step-start positions (the
 // reference keeps each particle's shape functions until the next step).
-template <int DIM, bool FLIP>
+template <int DIM, bool FLIP, bool BOX>
 __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p_musl(DevState s, double dt,
                                                                       double beta) {
   constexpr int NV = Elem<DIM>::NV;
@@ -799,7 +812,7 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p_musl(DevState s
   const CellGeom& g = s.geom[c];
   local_xi<DIM>(x, g.centroid, g.len, xi);
   shapefn<DIM>(xi, N);
-  cell_nodes_coords<DIM>(s, c, nid, X);
+  cell_nodes_for<DIM, BOX>(s, c, nid, X);
   double nvel[DIM], nacc[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.;
@@ -970,11 +983,11 @@ void prefer_shared_memory() {
   }
 }
 
-template <int DIM>
+template <int DIM, bool BOX>
 void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& pr) {
   const int64_t np = s.np, nn = s.nn;
   if (np == 0) return;
-  constexpr int LPC = DIM == 3 ? 2 : 1;
+  constexpr int LPC = DIM == 3 ? MPM_P2G_LANES_3D : 1;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
   if (s.sv) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
   const unsigned pb128 = nblocks(np, 128), nb = nblocks(nn, 256);
@@ -991,27 +1004,27 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
   pr.end(K_SORT, st);
   if (a.scheme == 2) {  // MUSL (mpm_scheme_musl.tcc)
     pr.begin(K_P2G, st);
-    k_p2g_cells<DIM, 2><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    k_p2g_cells<DIM, 2, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
     if (a.flip)
-      k_g2p_musl<DIM, true><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
+      k_g2p_musl<DIM, true, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
     else
-      k_g2p_musl<DIM, false><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
+      k_g2p_musl<DIM, false, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
     pr.end(K_G2P, st);
     // mass and momentum again with the updated velocities, nodal velocity,
     // then the stress update (mpm_scheme_musl.tcc:13-35)
     pr.begin(K_P2G_FORCES, st);
-    k_p2g_cells<DIM, 0><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    k_p2g_cells<DIM, 0, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
     k_nodes<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_STRESS, st);
-    k_stress<DIM><<<pb128, 128, 0, st>>>(s, a.dt);
+    k_stress<DIM, BOX><<<pb128, 128, 0, st>>>(s, a.dt);
     pr.end(K_STRESS, st);
     mc_returns();
     pr.begin(K_LOCATE, st);
@@ -1019,7 +1032,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     pr.end(K_LOCATE, st);
   } else if (a.scheme == 1) {  // USL
     pr.begin(K_P2G, st);
-    k_p2g_cells<DIM, 2><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    k_p2g_cells<DIM, 2, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
@@ -1027,36 +1040,36 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     pr.begin(K_G2P, st);
     const size_t sm = staged_smem_bytes<DIM>(s.sv != nullptr);
     if (a.flip) {
-      prefer_shared_memory<k_g2p_staged<DIM, true>>();
-      k_g2p_staged<DIM, true><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
+      prefer_shared_memory<k_g2p_staged<DIM, true, BOX>>();
+      k_g2p_staged<DIM, true, BOX><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
     } else {
-      prefer_shared_memory<k_g2p_staged<DIM, false>>();
-      k_g2p_staged<DIM, false><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
+      prefer_shared_memory<k_g2p_staged<DIM, false, BOX>>();
+      k_g2p_staged<DIM, false, BOX><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
     }
     pr.end(K_G2P, st);
     mc_returns();
   } else {  // USF
     pr.begin(K_P2G, st);
-    k_p2g_cells<DIM, 0><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    k_p2g_cells<DIM, 0, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_STRESS, st);
-    k_stress<DIM><<<pb128, 128, 0, st>>>(s, a.dt);
+    k_stress<DIM, BOX><<<pb128, 128, 0, st>>>(s, a.dt);
     pr.end(K_STRESS, st);
     mc_returns();
     pr.begin(K_P2G_FORCES, st);
-    k_p2g_cells<DIM, 1><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    k_p2g_cells<DIM, 1, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
     k_nodes<DIM, 2><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_G2P, st);
     if (a.flip)
-      k_g2p<DIM, false, true><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
+      k_g2p<DIM, false, true, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
     else
-      k_g2p<DIM, false, false><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
+      k_g2p<DIM, false, false, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
     pr.end(K_G2P, st);
   }
   pr.begin(K_LOCATE, st);
@@ -1090,10 +1103,12 @@ __global__ void k_material_batch(int64_t n, MaterialParams m, const double* stre
 
 void launch_step_fp64(int dim, const DevState& s, const StepArgs& a, cudaStream_t st,
                       Profiler& prof) {
+  // the particle kernels are compiled for tensor-product grids (box cells)
+  // and for general meshes
   if (dim == 2)
-    step_impl<2>(s, a, st, prof);
+    s.structured ? step_impl<2, true>(s, a, st, prof) : step_impl<2, false>(s, a, st, prof);
   else
-    step_impl<3>(s, a, st, prof);
+    s.structured ? step_impl<3, true>(s, a, st, prof) : step_impl<3, false>(s, a, st, prof);
 }
 
 void counting_sort(const DevState& s, cudaStream_t st) { counting_sort_impl(s, st); }

@@ -25,6 +25,10 @@
 #include "mpm_kernels.h"
 #include "mpm_state.cuh"
 
+#ifndef MPM_P2G_LANES_3D
+#define MPM_P2G_LANES_3D 2  // lanes per hex8 cell in P2G (2: 4 slots each, 4: 2 slots each)
+#endif
+
 #ifndef MPM_MIXED_G2P_MIN_BLOCKS
 #define MPM_MIXED_G2P_MIN_BLOCKS 4
 #endif
@@ -64,10 +68,16 @@ __device__ __forceinline__ void xi_f32(const DevState& s, int c, const double* x
   for (int d = 0; d < DIM; ++d) xf[d] = (float)xi[d];
 }
 
-// node ids and nodal coordinates relative to node 0 of the cell (FP32)
-template <int DIM>
+// node ids and nodal coordinates relative to node 0 of the cell (FP32); the
+// coordinates are not needed (nor set) for the box cells of a tensor-product
+// grid
+template <int DIM, bool BOX>
 __device__ __forceinline__ void cell_nodes_rel(const DevState& s, int c, int* nid, float* Xr) {
   constexpr int NV = Elem<DIM>::NV;
+  if constexpr (BOX) {
+    grid_cell_nodes<DIM>(s, c, nid);
+    return;
+  }
   double X[NV * DIM];
   cell_nodes_coords<DIM>(s, c, nid, X);
 #pragma unroll
@@ -77,11 +87,11 @@ __device__ __forceinline__ void cell_nodes_rel(const DevState& s, int c, int* ni
 }
 
 // ---------------------------------------------------------------- P2G cells
-template <int DIM, int MODE>
+template <int DIM, int MODE, bool BOX>
 __global__ void __launch_bounds__(128, MPM_MIXED_P2G_MIN_BLOCKS)
     k_p2g_cells_mixed(DevState s, float g0, float g1, float g2) {
   constexpr int NV = Elem<DIM>::NV;
-  constexpr int LPC = DIM == 3 ? 2 : 1;
+  constexpr int LPC = DIM == 3 ? MPM_P2G_LANES_3D : 1;
   constexpr int SPL = NV / LPC;
   constexpr int NVAL = 1 + 3 * DIM;
   constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM;
@@ -110,7 +120,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_P2G_MIN_BLOCKS)
   if (!valid || n == 0) return;
   int nid[NV];
   float Xr[NV * DIM];
-  cell_nodes_rel<DIM>(s, (int)c, nid, Xr);
+  cell_nodes_rel<DIM, BOX>(s, (int)c, nid, Xr);
   float acc[SPL][NVAL], cmp[SPL][NVAL];
 #pragma unroll
   for (int k = 0; k < SPL; ++k)
@@ -123,7 +133,20 @@ __global__ void __launch_bounds__(128, MPM_MIXED_P2G_MIN_BLOCKS)
     load_x<DIM>(s, p, x);
     float xi[DIM], Nk[SPL], Gk[SPL * DIM];
     xi_f32<DIM>(s, (int)c, x, xi);
-    lane_shape<DIM>(xi, h, Nk, Gk);
+    if constexpr (DIM == 3 && LPC == 4) {
+      // lane h owns slots 2h, 2h+1: the half (z factor) h / 2, pair h % 2
+      float N4[4], G4[12];
+      lane_shape<DIM>(xi, h / 2, N4, G4);
+      const int k0 = (h % 2) * 2;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        Nk[k] = N4[k0 + k];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Gk[k * 3 + d] = G4[(k0 + k) * 3 + d];
+      }
+    } else {
+      lane_shape<DIM>(xi, h, Nk, Gk);
+    }
     const float m = pmf<DIM>(s, PM<DIM>::MASS, p);
     if constexpr (MM) {
       float v[DIM];
@@ -138,8 +161,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_P2G_MIN_BLOCKS)
       }
     }
     if constexpr (FORCES) {
-      float inv[DIM * DIM];
-      jacobian_inverse<DIM>(xi, Xr, inv);
+      const CellMap<DIM, BOX, float> map = cell_map<DIM, BOX>(s, (int)c, xi, Xr);
       const float vol = pmf<DIM>(s, PM<DIM>::V0, p) * (1.f + pmf<DIM>(s, PM<DIM>::JP, p));
       const float sc = -vol;
       constexpr int NS = PF<DIM>::NS;
@@ -151,13 +173,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_P2G_MIN_BLOCKS)
 #pragma unroll
         for (int d = 0; d < DIM; ++d) kahan_add(acc[k][FEXT + d], cmp[k][FEXT + d], (gv[d] * m) * Nk[k]);
         float Dn[DIM];
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) {
-          float a = Gk[k * DIM + 0] * inv[q * DIM + 0];
-#pragma unroll
-          for (int r = 1; r < DIM; ++r) a = a + Gk[k * DIM + r] * inv[q * DIM + r];
-          Dn[q] = a;
-        }
+        map.grad(&Gk[k * DIM], Dn);
         float f[DIM];
         if constexpr (DIM == 2) {
           f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
@@ -503,25 +519,18 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, const Row
   }
 }
 
-template <int DIM>
-__device__ __forceinline__ void dn_dx_all_f(const float* xi, const float* Xr, float* D) {
+template <int DIM, bool BOX>
+__device__ __forceinline__ void dn_dx_all_f(const DevState& s, int c, const float* xi,
+                                            const float* Xr, float* D) {
   constexpr int NV = Elem<DIM>::NV;
-  float inv[DIM * DIM];
-  jacobian_inverse<DIM>(xi, Xr, inv);
+  const CellMap<DIM, BOX, float> map = cell_map<DIM, BOX>(s, c, xi, Xr);
   float G[NV * DIM];
   grad_shapefn<DIM>(xi, G);
 #pragma unroll
-  for (int n = 0; n < NV; ++n)
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) {
-      float a = G[n * DIM + 0] * inv[q * DIM + 0];
-#pragma unroll
-      for (int r = 1; r < DIM; ++r) a = a + G[n * DIM + r] * inv[q * DIM + r];
-      D[n * DIM + q] = a;
-    }
+  for (int n = 0; n < NV; ++n) map.grad(&G[n * DIM], &D[n * DIM]);
 }
 
-template <int DIM>
+template <int DIM, bool BOX>
 __global__ void __launch_bounds__(128) k_stress_mixed(DevState s, float dt) {
   constexpr int NV = Elem<DIM>::NV;
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -533,13 +542,13 @@ __global__ void __launch_bounds__(128) k_stress_mixed(DevState s, float dt) {
   float xi[DIM], D[NV * DIM], Xr[NV * DIM];
   int nid[NV];
   xi_f32<DIM>(s, c, x, xi);
-  cell_nodes_rel<DIM>(s, c, nid, Xr);
-  dn_dx_all_f<DIM>(xi, Xr, D);
+  cell_nodes_rel<DIM, BOX>(s, c, nid, Xr);
+  dn_dx_all_f<DIM, BOX>(s, c, xi, Xr, D);
   stress_update_mixed<DIM>(s, MGlobalRow<DIM>{s, p}, c, nid, D, dt);
 }
 
 // --------------------------------------------------------------------- G2P
-template <int DIM, bool STRESS, bool FLIP>
+template <int DIM, bool STRESS, bool FLIP, bool BOX>
 __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
     k_g2p_mixed(DevState s, double dt, float beta) {
   constexpr int NV = Elem<DIM>::NV;
@@ -554,7 +563,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   int nid[NV];
   xi_f32<DIM>(s, c, x, xi);
   shapefn<DIM>(xi, N);
-  cell_nodes_rel<DIM>(s, c, nid, Xr);
+  cell_nodes_rel<DIM, BOX>(s, c, nid, Xr);
   float nvel[DIM], nacc[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.f;
@@ -599,7 +608,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   for (int d = 0; d < DIM; ++d) set_pmf<DIM>(s, PM<DIM>::V + d, p, v[d]);
   if constexpr (STRESS) {
     float D[NV * DIM];
-    dn_dx_all_f<DIM>(xi, Xr, D);
+    dn_dx_all_f<DIM, BOX>(s, c, xi, Xr, D);
     stress_update_mixed<DIM>(s, MGlobalRow<DIM>{s, p}, c, nid, D, dtf);
   }
   bool finite = true;
@@ -622,7 +631,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
 // shared memory by the bulk-copy engine (as k_g2p_staged of the FP64 path):
 // phase A x, u (FP64), v (FP32), cell, material, velocity-constraint slot;
 // phase B stress .. P (FP32), MohrCoulomb state (FP32).  The arithmetic is
-// k_g2p_mixed<DIM, true, FLIP>'s.
+// k_g2p_mixed<DIM, true, FLIP, BOX>'s.
 static_assert(MSTAGE_T == PAD_PARTICLES, "staged slices are whole padded blocks");
 template <int DIM>
 constexpr size_t mixed_staged_smem_bytes(bool mc) {
@@ -630,7 +639,7 @@ constexpr size_t mixed_staged_smem_bytes(bool mc) {
          MSTAGE_T * (4 + 2 + 2);
 }
 
-template <int DIM, bool FLIP>
+template <int DIM, bool FLIP, bool BOX>
 __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
     k_g2p_mixed_staged(DevState s, double dt, float beta) {
   constexpr int NV = Elem<DIM>::NV;
@@ -686,7 +695,7 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
     int nid[NV];
     xi_f32<DIM>(s, c, x, xi);
     shapefn<DIM>(xi, N);
-    cell_nodes_rel<DIM>(s, c, nid, Xr);
+    cell_nodes_rel<DIM, BOX>(s, c, nid, Xr);
     float nvel[DIM], nacc[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.f;
@@ -735,8 +744,8 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
     // node ids and coordinates again rather than kept live across the wait
     float Xr[NV * DIM], D[NV * DIM];
     int nid[NV];
-    cell_nodes_rel<DIM>(s, c, nid, Xr);
-    dn_dx_all_f<DIM>(xi, Xr, D);
+    cell_nodes_rel<DIM, BOX>(s, c, nid, Xr);
+    dn_dx_all_f<DIM, BOX>(s, c, xi, Xr, D);
     stress_update_mixed<DIM>(s, r, c, nid, D, (float)dt);
   }
   bulk::fence_shared_to_async();
@@ -836,11 +845,11 @@ __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return_mix
 
 inline unsigned nblk(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
-template <int DIM>
+template <int DIM, bool BOX>
 void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& pr) {
   const int64_t np = s.np, nn = s.nn;
   if (np == 0) return;
-  constexpr int LPC = DIM == 3 ? 2 : 1;
+  constexpr int LPC = DIM == 3 ? MPM_P2G_LANES_3D : 1;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
   if (s.svf) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
   const unsigned pb = nblk(np, 128), nb = nblk(nn, 256), cb = nblk(s.ncells * LPC, 128);
@@ -857,7 +866,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
   pr.end(K_SORT, st);
   if (a.scheme == 1) {  // USL
     pr.begin(K_P2G, st);
-    k_p2g_cells_mixed<DIM, 2><<<cb, 128, 0, st>>>(s, g0, g1, g2);
+    k_p2g_cells_mixed<DIM, 2, BOX><<<cb, 128, 0, st>>>(s, g0, g1, g2);
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes_mixed<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
@@ -865,36 +874,36 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     pr.begin(K_G2P, st);
     const size_t sm = mixed_staged_smem_bytes<DIM>(s.svf != nullptr);
     if (a.flip) {
-      prefer_shared_memory<k_g2p_mixed_staged<DIM, true>>();
-      k_g2p_mixed_staged<DIM, true><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
+      prefer_shared_memory<k_g2p_mixed_staged<DIM, true, BOX>>();
+      k_g2p_mixed_staged<DIM, true, BOX><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
     } else {
-      prefer_shared_memory<k_g2p_mixed_staged<DIM, false>>();
-      k_g2p_mixed_staged<DIM, false><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
+      prefer_shared_memory<k_g2p_mixed_staged<DIM, false, BOX>>();
+      k_g2p_mixed_staged<DIM, false, BOX><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
     }
     pr.end(K_G2P, st);
     mc_returns();
   } else {  // USF
     pr.begin(K_P2G, st);
-    k_p2g_cells_mixed<DIM, 0><<<cb, 128, 0, st>>>(s, g0, g1, g2);
+    k_p2g_cells_mixed<DIM, 0, BOX><<<cb, 128, 0, st>>>(s, g0, g1, g2);
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes_mixed<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_STRESS, st);
-    k_stress_mixed<DIM><<<pb, 128, 0, st>>>(s, (float)a.dt);
+    k_stress_mixed<DIM, BOX><<<pb, 128, 0, st>>>(s, (float)a.dt);
     pr.end(K_STRESS, st);
     mc_returns();
     pr.begin(K_P2G_FORCES, st);
-    k_p2g_cells_mixed<DIM, 1><<<cb, 128, 0, st>>>(s, g0, g1, g2);
+    k_p2g_cells_mixed<DIM, 1, BOX><<<cb, 128, 0, st>>>(s, g0, g1, g2);
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
     k_nodes_mixed<DIM, 2><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_G2P, st);
     if (a.flip)
-      k_g2p_mixed<DIM, false, true><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
+      k_g2p_mixed<DIM, false, true, BOX><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
     else
-      k_g2p_mixed<DIM, false, false><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
+      k_g2p_mixed<DIM, false, false, BOX><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
     pr.end(K_G2P, st);
   }
   pr.begin(K_LOCATE, st);
@@ -906,10 +915,12 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
 
 void launch_step_mixed(int dim, const DevState& s, const StepArgs& a, cudaStream_t st,
                        Profiler& prof) {
+  // the particle kernels are compiled for tensor-product grids (box cells)
+  // and for general meshes
   if (dim == 2)
-    step_mixed<2>(s, a, st, prof);
+    s.structured ? step_mixed<2, true>(s, a, st, prof) : step_mixed<2, false>(s, a, st, prof);
   else
-    step_mixed<3>(s, a, st, prof);
+    s.structured ? step_mixed<3, true>(s, a, st, prof) : step_mixed<3, false>(s, a, st, prof);
 }
 
 }  // namespace mpm_b200

@@ -97,20 +97,32 @@ __global__ void __launch_bounds__(128) k_prep_tangent(DevState s) {
   const int c = s.cell[p];
   if (c < 0) return;
   const CellGeom g = s.geom[c];
-  D x[DIM], xi[DIM], N[NV], G[NV * DIM], inv[DIM * DIM];
-  int nid[NV];
-  double X[NV * DIM];
+  D x[DIM], xi[DIM], N[NV], G[NV * DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) x[d] = pfield<DIM>(s, PF<DIM>::X + d, p);
   xi_dual<DIM>(g, x, xi);
   shapefn<DIM>(xi, N);
   grad_shapefn<DIM>(xi, G);
-  cell_nodes_coords<DIM>(s, c, nid, X);
-  jinv_dual<DIM>(xi, X, inv);
   double* const* t = const_cast<double* const*>(s.prept);
   const int64_t np = s.np;
 #pragma unroll
   for (int n = 0; n < NV; ++n) st(s.prep, t, (int64_t)n * np + p, N[n]);
+  if (s.structured) {
+    // box cell: dN/dx = dN/dxi * (2 / len) per axis (CellMap<DIM, true>)
+    int ijk[3] = {0, 0, 0};
+    cell_ijk<DIM>(s, c, ijk);
+#pragma unroll
+    for (int n = 0; n < NV; ++n)
+#pragma unroll
+      for (int q = 0; q < DIM; ++q)
+        st(s.prep, t, (int64_t)(NV + n * DIM + q) * np + p, G[n * DIM + q] * s.axis_ihl[q][ijk[q]]);
+    return;
+  }
+  int nid[NV];
+  double X[NV * DIM];
+  D inv[DIM * DIM];
+  cell_nodes_coords<DIM>(s, c, nid, X);
+  jinv_dual<DIM>(xi, X, inv);
 #pragma unroll
   for (int n = 0; n < NV; ++n)
 #pragma unroll

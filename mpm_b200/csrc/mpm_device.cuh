@@ -56,6 +56,23 @@ __device__ __forceinline__ int off_i(int n) { return ((n & 3) == 1 || (n & 3) ==
 __device__ __forceinline__ int off_j(int n) { return ((n & 3) >= 2) ? 1 : 0; }
 __device__ __forceinline__ int off_k(int n) { return n >= 4 ? 1 : 0; }
 
+// node ids of a cell of a tensor-product grid
+template <int DIM>
+__device__ __forceinline__ void grid_cell_nodes(const DevState& s, int c, int* nid) {
+  constexpr int NV = Elem<DIM>::NV;
+  int ijk[3] = {0, 0, 0};
+  cell_ijk<DIM>(s, c, ijk);
+  const int nx = s.gcells[0] + 1, ny = s.gcells[1] + 1;
+#pragma unroll
+  for (int n = 0; n < NV; ++n) {
+    const int i = ijk[0] + off_i(n), j = ijk[1] + off_j(n);
+    if constexpr (DIM == 2)
+      nid[n] = i + nx * j;
+    else
+      nid[n] = i + nx * (j + ny * (ijk[2] + off_k(n)));
+  }
+}
+
 // node ids and nodal coordinates of a cell
 template <int DIM>
 __device__ __forceinline__ void cell_nodes_coords(const DevState& s, int c, int* nid, double* X) {
@@ -108,19 +125,73 @@ __device__ __forceinline__ void jacobian_inverse(const R* xi, const R* X, R* inv
   inverse<DIM>(J, inv);
 }
 
-// dN_n/dx for one local node n given J^-1
-template <int DIM>
-__device__ __forceinline__ void dn_dx_node(const double* xi, const double* inv, int n, double* Dn) {
+// Map of local (xi) gradients to physical (x) gradients in one cell:
+// dN/dx_c = sum_k dN/dxi_k J^-1[c][k] (quadrilateral_element.tcc:295-309,
+// hexahedron_element.tcc:307-321, with J^-1 from the nodal coordinates).
+//
+// BOX: the cell is an axis-aligned box of a tensor-product grid, whose
+// Jacobian is diag(len / 2) at every xi; dN/dx_c = dN/dxi_c * (2 / len_c)
+// from the per-axis table, with no nodal coordinates and no per-point J.
+// The products with the zero entries of J^-1 that the general map adds can
+// change only the sign of a zero.
+template <int DIM, bool BOX, typename R>
+struct CellMap;
+
+template <int DIM, typename R>
+struct CellMap<DIM, true, R> {
+  R ihl[DIM];
+  __device__ __forceinline__ void grad(const R* g, R* d) const {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) d[c] = g[c] * ihl[c];
+  }
+};
+
+template <int DIM, typename R>
+struct CellMap<DIM, false, R> {
+  R inv[DIM * DIM];
+  __device__ __forceinline__ void grad(const R* g, R* d) const {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      R a = g[0] * inv[c * DIM + 0];
+#pragma unroll
+      for (int k = 1; k < DIM; ++k) a = a + g[k] * inv[c * DIM + k];
+      d[c] = a;
+    }
+  }
+};
+
+// the map of cell c at xi (X: the nodal coordinates, not read for a box)
+template <int DIM, bool BOX, typename R>
+__device__ __forceinline__ CellMap<DIM, BOX, R> cell_map(const DevState& s, int c, const R* xi,
+                                                         const R* X) {
+  CellMap<DIM, BOX, R> m;
+  if constexpr (BOX) {
+    int ijk[3] = {0, 0, 0};
+    cell_ijk<DIM>(s, c, ijk);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) m.ihl[d] = R(__ldg(&s.axis_ihl[d][ijk[d]]));
+  } else {
+    jacobian_inverse<DIM>(xi, X, m.inv);
+  }
+  return m;
+}
+
+// node ids of cell c and, off a tensor-product grid, its nodal coordinates
+template <int DIM, bool BOX>
+__device__ __forceinline__ void cell_nodes_for(const DevState& s, int c, int* nid, double* X) {
+  if constexpr (BOX)
+    grid_cell_nodes<DIM>(s, c, nid);
+  else
+    cell_nodes_coords<DIM>(s, c, nid, X);
+}
+
+// dN_n/dx for one local node n
+template <int DIM, class Map>
+__device__ __forceinline__ void dn_dx_node(const double* xi, const Map& map, int n, double* Dn) {
   constexpr int NV = Elem<DIM>::NV;
   double G[NV * DIM];
   grad_shapefn<DIM>(xi, G);  // folded to the needed entries by the compiler
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) {
-    double a = G[n * DIM + 0] * inv[c * DIM + 0];
-#pragma unroll
-    for (int k = 1; k < DIM; ++k) a = a + G[n * DIM + k] * inv[c * DIM + k];
-    Dn[c] = a;
-  }
+  map.grad(&G[n * DIM], Dn);
 }
 
 // Shape functions and natural gradients of the SPL slots a lane owns: all

@@ -172,6 +172,7 @@ struct mpm_gpu_solver {
   bool structured = false;
   int32_t gcells[3] = {1, 1, 1};
   std::vector<double> axis[3];
+  std::vector<double> axis_ihl[3];  // 2 / (axis[i + 1] - axis[i]): J^-1 of the box cells
 
   // materials
   std::vector<MaterialParams> mats;
@@ -201,6 +202,7 @@ struct mpm_gpu_solver {
   DevBuf<double> d_pbuf;
   DevBuf<MaterialParams> d_mats;
   DevBuf<double> d_axis[3];
+  DevBuf<double> d_axis_ihl[3];
   DevBuf<double> d_dndx_c, d_partials;
   DevBuf<int32_t> d_nc_off, d_nc_cell, d_cnt, d_start, d_rank, d_order, d_bsum;
   DevBuf<int8_t> d_nc_slot;
@@ -446,7 +448,12 @@ bool detect_structured(mpm_gpu_t h) {
   h->gcells[0] = (int32_t)cx;
   h->gcells[1] = (int32_t)cy;
   h->gcells[2] = (int32_t)cz;
-  for (int d = 0; d < 3; ++d) h->axis[d] = d < dim ? ax[d] : std::vector<double>{0.0, 1.0};
+  for (int d = 0; d < 3; ++d) {
+    h->axis[d] = d < dim ? ax[d] : std::vector<double>{0.0, 1.0};
+    const std::vector<double>& a = h->axis[d];
+    h->axis_ihl[d].resize(a.size() - 1);
+    for (size_t i = 0; i + 1 < a.size(); ++i) h->axis_ihl[d][i] = 2. / (a[i + 1] - a[i]);
+  }
   return true;
 }
 
@@ -569,7 +576,10 @@ void upload_mesh(mpm_gpu_t h) {
   h->d_words.alloc(4);
   ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 4, st), "memset");
   if (h->structured)
-    for (int d = 0; d < 3; ++d) h->d_axis[d].upload(h->axis[d].data(), h->axis[d].size(), st);
+    for (int d = 0; d < 3; ++d) {
+      h->d_axis[d].upload(h->axis[d].data(), h->axis[d].size(), st);
+      h->d_axis_ihl[d].upload(h->axis_ihl[d].data(), h->axis_ihl[d].size(), st);
+    }
   if (h->mixed) {
     std::vector<float> f(h->dndx_c.begin(), h->dndx_c.end());
     h->d_dndx_cf.upload(f.data(), f.size(), st);
@@ -717,6 +727,7 @@ void refresh_state(mpm_gpu_t h) {
   for (int d = 0; d < 3; ++d) {
     s.gcells[d] = h->gcells[d];
     s.axis[d] = h->d_axis[d].p;
+    s.axis_ihl[d] = h->d_axis_ihl[d].p;
   }
   s.nc_off = h->d_nc_off.p;
   s.nc_cell = h->d_nc_cell.p;

@@ -107,6 +107,7 @@ struct DevState {
   int structured = 0;
   int32_t gcells[3] = {1, 1, 1};     // cells per axis
   const double* axis[3] = {nullptr, nullptr, nullptr};  // node coordinates per axis
+  const double* axis_ihl[3] = {nullptr, nullptr, nullptr};  // 2 / cell length per axis interval
 
   // general meshes: cells around each node, ascending cell id, with the
   // node's local index (slot) in that cell
