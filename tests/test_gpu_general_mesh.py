@@ -1,0 +1,103 @@
+"""General meshes (not a tensor-product grid) against the CPU oracle.
+
+On a general mesh the particle kernels read each cell's node ids and nodal
+coordinates from the connectivity tables and evaluate J^-1 at every point
+(quadrilateral_element.tcc:295-309, hexahedron_element.tcc:307-321), and the
+locate step searches the cell-neighbour lists instead of the grid axes.  Two
+kinds of meshes take that path here:
+
+* renumbered: a column mesh with its node ids permuted, the geometry
+  unchanged (the grid detection needs x-fastest node ids);
+* distorted: interior nodes of a column mesh displaced by up to 15% of the
+  cell size, so the cells are general quadrilaterals / hexahedra.
+
+FP64 bar as in test_gpu_parity: cell ids bit-exact, fields within FP64_RTOL.
+"""
+import numpy as np
+import pytest
+
+from mpm_b200 import problems as P
+from tests.parity import assert_parity, field_errors, mc_state_errors
+from tests.test_gpu_parity import _run_both, small_column_2d, small_column_3d
+
+pytestmark = pytest.mark.gpu
+
+
+def renumber_nodes(prob, seed=11):
+    """The same mesh with node ids permuted (constraints follow the nodes)."""
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(prob.nnodes)  # old id -> new id
+    coords = np.empty_like(prob.coords)
+    coords[perm] = prob.coords
+    prob.coords = coords
+    prob.cells = perm[prob.cells]
+    if prob.velocity_constraints is not None:
+        nid, d, v = prob.velocity_constraints
+        prob.velocity_constraints = (perm[nid], d, v)
+    if prob.friction_constraints is not None:
+        nid, d, sgn, mu = prob.friction_constraints
+        prob.friction_constraints = (perm[nid], d, sgn, mu)
+    return prob
+
+
+def distort_interior(prob, frac=0.15, seed=12):
+    """Interior nodes moved by up to frac * dx per axis; nodes on the bounding
+    box stay, so the wall constraints keep their meaning."""
+    rng = np.random.default_rng(seed)
+    c = prob.coords
+    lo, hi = c.min(axis=0), c.max(axis=0)
+    interior = np.all((c > lo + 1e-12) & (c < hi - 1e-12), axis=1)
+    shift = rng.uniform(-frac, frac, c.shape) * prob.dx
+    prob.coords = c + shift * interior[:, None]
+    return prob
+
+
+@pytest.mark.parametrize("mesh", ["renumbered", "distorted"])
+@pytest.mark.parametrize("scheme", ["usf", "usl", "musl"])
+def test_2d_linear_elastic_column(mesh, scheme):
+    prob = small_column_2d(scheme=scheme)
+    prob = renumber_nodes(prob) if mesh == "renumbered" else distort_interior(prob)
+    for s, g, o in _run_both(prob, [1, 10, 100]):
+        assert_parity(g, o, label=f"2D LE {mesh} {scheme} step {s}")
+
+
+@pytest.mark.parametrize("mesh", ["renumbered", "distorted"])
+@pytest.mark.parametrize("scheme", ["usf", "usl"])
+def test_3d_mohr_coulomb_column_with_friction(mesh, scheme):
+    prob = small_column_3d(scheme=scheme, dt=1e-5, c=2000., psi=5.)
+    prob = renumber_nodes(prob) if mesh == "renumbered" else distort_interior(prob)
+    for s, g, o in _run_both(prob, [1, 10, 50]):
+        assert_parity(g, o, label=f"3D MC {mesh} {scheme} step {s}")
+        errs = mc_state_errors(g, o)
+        assert np.array_equal(g["svars"][:, 0], o["svars"][:, 0]), "yield states differ"
+        assert errs["pdstrain"] < 1e-9 and errs["epsilon"] < 1e-9, errs
+
+
+def test_renumbered_mesh_matches_the_grid_run():
+    """Same geometry through both kernel paths: the per-axis J^-1 of a box
+    cell and the general J^-1 differ by rounding only."""
+    grid = P.build_solver(small_column_3d(scheme="usl", dt=1e-5, c=2000., psi=5.))
+    gen = P.build_solver(renumber_nodes(small_column_3d(scheme="usl", dt=1e-5, c=2000., psi=5.)))
+    grid.step(50)
+    gen.step(50)
+    a, b = grid.read(), gen.read()
+    assert np.array_equal(a["cell"], b["cell"])
+    errs = field_errors(b, a, ("x", "u", "v", "stress", "strain"))
+    assert all(v < 1e-10 for v in errs.values()), errs
+
+
+@pytest.mark.parametrize("mesh", ["renumbered", "distorted"])
+def test_mixed_precision_on_general_mesh(mesh):
+    """The mixed-precision kernels' general-mesh path: within 1e-5 of FP64."""
+    def make():
+        prob = small_column_3d(scheme="usl", dt=1e-5, c=2000., psi=5.)
+        return renumber_nodes(prob) if mesh == "renumbered" else distort_interior(prob)
+
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = P.build_solver(make(), precision=prec)
+        s.step(50)
+        out[prec] = s.read()
+    assert np.array_equal(out["mixed"]["cell"], out["fp64"]["cell"])
+    errs = field_errors(out["mixed"], out["fp64"], ("u", "v", "stress", "strain"))
+    assert all(v <= 1e-5 for v in errs.values()), errs
