@@ -16,15 +16,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "mpm_bulk.cuh"
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
 #include "mpm_state.cuh"
-
-#ifndef MPM_P2G_LANES_3D
-#define MPM_P2G_LANES_3D 2  // lanes per hex8 cell in P2G (2: 4 slots each, 4: 2 slots each)
-#endif
 
 // Minimum resident blocks per SM requested from the register allocator for
 // the two particle kernels (occupancy versus spills, tuned on the B200).
@@ -34,11 +31,8 @@
 #ifndef MPM_MC_RETURN_MIN_BLOCKS
 #define MPM_MC_RETURN_MIN_BLOCKS 4
 #endif
-#ifndef MPM_P2G_MIN_BLOCKS
-#define MPM_P2G_MIN_BLOCKS 2  // more blocks spill the 40 lane accumulators: slower
-#endif
-#ifndef MPM_P2G_BOX_MIN_BLOCKS
-#define MPM_P2G_BOX_MIN_BLOCKS 3  // box cells hold no nodal coordinates: 0.53 -> 0.45 ms (4M, 3D)
+#ifndef MPM_P2G_TILE_MIN_BLOCKS
+#define MPM_P2G_TILE_MIN_BLOCKS 4  // 64 registers on a grid: 0.39 -> 0.345 ms (4M, 3D); 5, 6 spill
 #endif
 
 namespace mpm_b200 {
@@ -112,99 +106,125 @@ __global__ void __launch_bounds__(256) k_fill(DevState s) {
   s.order[s.start[c] + s.rank[p]] = (int32_t)p;
 }
 
-// ---------------------------------------------------------------- P2G cells
-// Lanes per cell: 2 in 3D (4 slots each), 1 in 2D.  A lane adds, in particle
-// id order, the contributions of its cell's particles to its slots:
+// ---------------------------------------------------------------- P2G tiles
+// Cell-slot partials: for slot k of cell c (its local node k), the sums over
+// the cell's particles, in particle id order, of
 //   mass m N (particle.tcc:643-655), momentum (m N) v, body force (g m) N
 //   (:893-898), internal force -V (dN . sigma) (:915-949).
 // MODE 0: mass and momentum; 1: forces; 2: all.
+//
+// Computed by cell tiles: a block takes p2g_tile_t / NV consecutive cells,
+// whose particles are one contiguous range of the sorted order.  The block
+// stages that range in chunks of p2g_tile_t particles (one particle per
+// thread: local coordinates, mass, velocity, volume, stress and, off a
+// tensor-product grid, J^-1) in shared memory; then thread (cell, slot) adds
+// its slot's contributions of the cell's particles to 1 + 3 DIM accumulators:
+// few registers per thread, coalesced particle reads, no atomics.
 template <int DIM, int MODE, bool BOX>
-__global__ void __launch_bounds__(128, BOX ? MPM_P2G_BOX_MIN_BLOCKS : MPM_P2G_MIN_BLOCKS)
-    k_p2g_cells(DevState s, double g0, double g1, double g2) {
+struct TileRows {
+  static constexpr bool MM = MODE != 1, FORCES = MODE != 0;
+  static constexpr int XI = 0, M = DIM, V = DIM + 1;
+  static constexpr int SC = V + (MM ? DIM : 0);  // -volume
+  static constexpr int S = SC + 1;
+  static constexpr int INV = S + (FORCES ? PF<DIM>::NS : 0);
+  static constexpr int N = INV + (FORCES && !BOX ? DIM * DIM : 0);
+};
+
+template <int DIM, int MODE, bool BOX>
+__global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_P2G_TILE_MIN_BLOCKS)
+    k_p2g_tiles(DevState s, double g0, double g1, double g2) {
   constexpr int NV = Elem<DIM>::NV;
-  constexpr int LPC = DIM == 3 ? MPM_P2G_LANES_3D : 1;
-  constexpr int SPL = NV / LPC;
+  constexpr int T = p2g_tile_t<BOX>();
+  constexpr int CB = T / NV;
   constexpr int NVAL = PV<DIM>::N;
-  constexpr bool MM = MODE != 1, FORCES = MODE != 0;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t c = t / LPC;
-  const int h = (int)(t % LPC);
-  const bool valid = c < s.ncells;
-  const int n = valid ? s.cnt[c] : 0;
-  const int s0 = valid ? s.start[c] : 0;
-  if constexpr (MODE != 1) {
-    // particle ids of the cell in ascending order (the fill order is not
-    // deterministic); the first lane of the cell sorts the short segment
-    if (h == 0 && n > 1) {
-      int32_t* seg = s.order + s0;
-      for (int a = 1; a < n; ++a) {
-        const int32_t key = seg[a];
-        int b = a - 1;
-        while (b >= 0 && seg[b] > key) {
-          seg[b + 1] = seg[b];
-          --b;
-        }
-        seg[b + 1] = key;
-      }
-    }
-    __syncwarp();
+  using RW = TileRows<DIM, MODE, BOX>;
+  constexpr bool MM = RW::MM, FORCES = RW::FORCES;
+  __shared__ double rows[RW::N][T];
+  const int t = threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * CB;
+  if (c0 >= s.ncells) return;
+  const int64_t c1 = c0 + CB < s.ncells ? c0 + CB : s.ncells;
+  const int64_t q_begin = s.start[c0], q_end = s.start[c1 - 1] + s.cnt[c1 - 1];
+  if (q_begin == q_end) return;  // no particles in the tile (the whole block)
+  // this thread's cell and slot
+  const int64_t c = c0 + t / NV;
+  const int k = t % NV;
+  const bool mine = c < c1;
+  const int64_t a0 = mine ? s.start[c] : 0;
+  const int64_t a1 = mine ? a0 + s.cnt[c] : 0;
+  // each cell's particle ids in ascending order in the first mapping of a step
+  if constexpr (MODE != 1) sort_cell_ids<NV>(s.order + a0, (int)(a1 - a0), k);
+  CellMap<DIM, BOX, double> box_map;
+  if constexpr (BOX && FORCES) {
+    if (a1 > a0) box_map = cell_map<DIM, true, double>(s, (int)c, nullptr, nullptr);
   }
-  if (!valid || n == 0) return;
-  int nid[NV];
-  double X[NV * DIM];  // nodal coordinates (J^-1 of a box cell needs none)
-  if constexpr (!BOX) cell_nodes_coords<DIM>(s, (int)c, nid, X);
-  const CellGeom g = s.geom[c];
   const int64_t np = s.np;
-  double acc[SPL][NVAL];
-#pragma unroll
-  for (int k = 0; k < SPL; ++k)
-#pragma unroll
-    for (int v = 0; v < NVAL; ++v) acc[k][v] = 0.;
   const double gv[3] = {g0, g1, g2};
-  for (int j = 0; j < n; ++j) {
-    const int64_t p = s.order[s0 + j];
-    double x[DIM], xi[DIM], Nk[SPL], Gk[SPL * DIM];
-    load_x<DIM>(s, p, x);
-    local_xi<DIM>(x, g.centroid, g.len, xi);
-    if constexpr (DIM == 3 && LPC == 4) {
-      // lane h owns slots 2h, 2h+1: the half (z factor) h / 2, pair h % 2
-      double N4[4], G4[12];
-      lane_shape<DIM>(xi, h / 2, N4, G4);
-      const int k0 = (h % 2) * 2;
+  double acc[NVAL];
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        Nk[k] = N4[k0 + k];
+  for (int v = 0; v < NVAL; ++v) acc[v] = 0.;
+  for (int64_t q0 = q_begin; q0 < q_end; q0 += T) {
+    if (q0 != q_begin) __syncthreads();  // the previous chunk is consumed
+    if (q0 + t < q_end) {
+      const int64_t p = s.order[q0 + t];
+      const int pc = s.cell[p];
+      const CellGeom& g = s.geom[pc];
+      double x[DIM], xi[DIM];
+      load_x<DIM>(s, p, x);
+      local_xi<DIM>(x, g.centroid, g.len, xi);
 #pragma unroll
-        for (int d = 0; d < 3; ++d) Gk[k * 3 + d] = G4[(k0 + k) * 3 + d];
+      for (int d = 0; d < DIM; ++d) rows[RW::XI + d][t] = xi[d];
+      rows[RW::M][t] = s.pf[(int64_t)PF<DIM>::MASS * np + p];
+      if constexpr (MM) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) rows[RW::V + d][t] = s.pf[(int64_t)(PF<DIM>::V + d) * np + p];
       }
-    } else {
-      lane_shape<DIM>(xi, h, Nk, Gk);
-    }
-    const double m = s.pf[(int64_t)PF<DIM>::MASS * np + p];
-    if constexpr (MM) {
-      double v[DIM];
+      if constexpr (FORCES) {
+        rows[RW::SC][t] = -1. * s.pf[(int64_t)PF<DIM>::VOL * np + p];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) v[d] = s.pf[(int64_t)(PF<DIM>::V + d) * np + p];
+        for (int q = 0; q < PF<DIM>::NS; ++q) rows[RW::S + q][t] = s.pf[(int64_t)(PF<DIM>::S + q) * np + p];
+        if constexpr (!BOX) {
+          int nid[NV];
+          double X[NV * DIM];
+          cell_nodes_coords<DIM>(s, pc, nid, X);
+          const CellMap<DIM, false, double> m = cell_map<DIM, false>(s, pc, xi, X);
 #pragma unroll
-      for (int k = 0; k < SPL; ++k) {
-        const double mN = m * Nk[k];
-        acc[k][PV<DIM>::MASS] += mN;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) acc[k][PV<DIM>::MOM + d] += mN * v[d];
+          for (int q = 0; q < DIM * DIM; ++q) rows[RW::INV + q][t] = m.inv[q];
+        }
       }
     }
-    if constexpr (FORCES) {
-      const CellMap<DIM, BOX, double> map = cell_map<DIM, BOX>(s, (int)c, xi, X);
-      const double sc = -1. * s.pf[(int64_t)PF<DIM>::VOL * np + p];
-      double sig[6] = {0, 0, 0, 0, 0, 0};
+    __syncthreads();
+    const int64_t j0 = a0 > q0 ? a0 : q0;
+    const int64_t j1 = a1 < q0 + T ? a1 : q0 + T;
+    for (int64_t j = j0; j < j1; ++j) {
+      const int r = (int)(j - q0);
+      double xi[DIM], N, G[DIM];
 #pragma unroll
-      for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = s.pf[(int64_t)(PF<DIM>::S + k) * np + p];
+      for (int d = 0; d < DIM; ++d) xi[d] = rows[RW::XI + d][r];
+      node_shape<DIM>(xi, k, N, G);
+      const double m = rows[RW::M][r];
+      if constexpr (MM) {
+        const double mN = m * N;
+        acc[PV<DIM>::MASS] += mN;
 #pragma unroll
-      for (int k = 0; k < SPL; ++k) {
+        for (int d = 0; d < DIM; ++d) acc[PV<DIM>::MOM + d] += mN * rows[RW::V + d][r];
+      }
+      if constexpr (FORCES) {
+        const double sc = rows[RW::SC][r];
+        double sig[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) acc[k][PV<DIM>::FEXT + d] += (gv[d] * m) * Nk[k];
+        for (int q = 0; q < PF<DIM>::NS; ++q) sig[q] = rows[RW::S + q][r];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) acc[PV<DIM>::FEXT + d] += (gv[d] * m) * N;
         double Dn[DIM];
-        map.grad(&Gk[k * DIM], Dn);
+        if constexpr (BOX) {
+          box_map.grad(G, Dn);
+        } else {
+          CellMap<DIM, false, double> m2;
+#pragma unroll
+          for (int q = 0; q < DIM * DIM; ++q) m2.inv[q] = rows[RW::INV + q][r];
+          m2.grad(G, Dn);
+        }
         double f[DIM];
         if constexpr (DIM == 2) {
           f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
@@ -215,22 +235,20 @@ __global__ void __launch_bounds__(128, BOX ? MPM_P2G_BOX_MIN_BLOCKS : MPM_P2G_MI
           f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
         }
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) acc[k][PV<DIM>::FINT + d] += f[d] * sc;
+        for (int d = 0; d < DIM; ++d) acc[PV<DIM>::FINT + d] += f[d] * sc;
       }
     }
   }
-  double* out = s.partials + ((int64_t)c * NV + h * SPL) * NVAL;
+  if (!mine || a1 == a0) return;  // empty cells keep no partials
+  double* out = s.partials + ((int64_t)c * NV + k) * NVAL;
+  if constexpr (MM) {
+    out[PV<DIM>::MASS] = acc[PV<DIM>::MASS];
 #pragma unroll
-  for (int k = 0; k < SPL; ++k) {
-    if constexpr (MM) {
-      out[k * NVAL + PV<DIM>::MASS] = acc[k][PV<DIM>::MASS];
+    for (int d = 0; d < DIM; ++d) out[PV<DIM>::MOM + d] = acc[PV<DIM>::MOM + d];
+  }
+  if constexpr (FORCES) {
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) out[k * NVAL + PV<DIM>::MOM + d] = acc[k][PV<DIM>::MOM + d];
-    }
-    if constexpr (FORCES) {
-#pragma unroll
-      for (int d = 0; d < 2 * DIM; ++d) out[k * NVAL + PV<DIM>::FEXT + d] = acc[k][PV<DIM>::FEXT + d];
-    }
+    for (int d = 0; d < 2 * DIM; ++d) out[PV<DIM>::FEXT + d] = acc[PV<DIM>::FEXT + d];
   }
 }
 
@@ -987,7 +1005,6 @@ template <int DIM, bool BOX>
 void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& pr) {
   const int64_t np = s.np, nn = s.nn;
   if (np == 0) return;
-  constexpr int LPC = DIM == 3 ? MPM_P2G_LANES_3D : 1;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
   if (s.sv) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
   const unsigned pb128 = nblocks(np, 128), nb = nblocks(nn, 256);
@@ -998,13 +1015,18 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     k_mc_return<DIM><<<mcb, 128, 0, st>>>(s);
     pr.end(K_MC_RETURN, st);
   };
-  const unsigned cb = nblocks(s.ncells * LPC, 128);
+  auto p2g = [&](auto mode) {
+    constexpr int MODE = decltype(mode)::value;
+    constexpr int TT = p2g_tile_t<BOX>();
+    k_p2g_tiles<DIM, MODE, BOX><<<nblocks(s.ncells, TT / Elem<DIM>::NV), TT, 0, st>>>(
+        s, a.g[0], a.g[1], a.g[2]);
+  };
   pr.begin(K_SORT, st);
   counting_sort_impl(s, st);
   pr.end(K_SORT, st);
   if (a.scheme == 2) {  // MUSL (mpm_scheme_musl.tcc)
     pr.begin(K_P2G, st);
-    k_p2g_cells<DIM, 2, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    p2g(std::integral_constant<int, 2>{});
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
@@ -1018,7 +1040,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     // mass and momentum again with the updated velocities, nodal velocity,
     // then the stress update (mpm_scheme_musl.tcc:13-35)
     pr.begin(K_P2G_FORCES, st);
-    k_p2g_cells<DIM, 0, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    p2g(std::integral_constant<int, 0>{});
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
     k_nodes<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
@@ -1032,7 +1054,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     pr.end(K_LOCATE, st);
   } else if (a.scheme == 1) {  // USL
     pr.begin(K_P2G, st);
-    k_p2g_cells<DIM, 2, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    p2g(std::integral_constant<int, 2>{});
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
@@ -1050,7 +1072,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     mc_returns();
   } else {  // USF
     pr.begin(K_P2G, st);
-    k_p2g_cells<DIM, 0, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    p2g(std::integral_constant<int, 0>{});
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
@@ -1060,7 +1082,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     pr.end(K_STRESS, st);
     mc_returns();
     pr.begin(K_P2G_FORCES, st);
-    k_p2g_cells<DIM, 1, BOX><<<cb, 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+    p2g(std::integral_constant<int, 1>{});
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
     k_nodes<DIM, 2><<<nb, 256, 0, st>>>(s, a.dt, a.damping);

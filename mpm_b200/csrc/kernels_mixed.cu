@@ -25,18 +25,14 @@
 #include "mpm_kernels.h"
 #include "mpm_state.cuh"
 
-#ifndef MPM_P2G_LANES_3D
-#define MPM_P2G_LANES_3D 2  // lanes per hex8 cell in P2G (2: 4 slots each, 4: 2 slots each)
-#endif
-
 #ifndef MPM_MIXED_G2P_MIN_BLOCKS
 #define MPM_MIXED_G2P_MIN_BLOCKS 4
 #endif
 #ifndef MPM_MC_RETURN_MIN_BLOCKS
 #define MPM_MC_RETURN_MIN_BLOCKS 4
 #endif
-#ifndef MPM_MIXED_P2G_MIN_BLOCKS
-#define MPM_MIXED_P2G_MIN_BLOCKS 3
+#ifndef MPM_MIXED_P2G_TILE_MIN_BLOCKS
+#define MPM_MIXED_P2G_TILE_MIN_BLOCKS 5  // 48 registers, small spills: 0.32 -> 0.26 ms (4M, 3D)
 #endif
 
 namespace mpm_b200 {
@@ -86,94 +82,114 @@ __device__ __forceinline__ void cell_nodes_rel(const DevState& s, int c, int* ni
     for (int d = 0; d < DIM; ++d) Xr[n * DIM + d] = (float)(X[n * DIM + d] - X[d]);
 }
 
-// ---------------------------------------------------------------- P2G cells
+// ---------------------------------------------------------------- P2G tiles
+// The FP64 path's cell tiles (k_p2g_tiles) in FP32: staged local coordinates
+// (the FP64 local coordinate rounded), mass, velocity, -V0 (1 + P), stress
+// and, off a tensor-product grid, J^-1; per (cell, slot) thread 1 + 3 DIM
+// Kahan-compensated FP32 sums over the cell's particles in id order.
 template <int DIM, int MODE, bool BOX>
-__global__ void __launch_bounds__(128, MPM_MIXED_P2G_MIN_BLOCKS)
-    k_p2g_cells_mixed(DevState s, float g0, float g1, float g2) {
+struct MTileRows {
+  static constexpr bool MM = MODE != 1, FORCES = MODE != 0;
+  static constexpr int XI = 0, M = DIM, V = DIM + 1;
+  static constexpr int SC = V + (MM ? DIM : 0);
+  static constexpr int S = SC + 1;
+  static constexpr int INV = S + (FORCES ? PF<DIM>::NS : 0);
+  static constexpr int N = INV + (FORCES && !BOX ? DIM * DIM : 0);
+};
+
+template <int DIM, int MODE, bool BOX>
+__global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOCKS)
+    k_p2g_tiles_mixed(DevState s, float g0, float g1, float g2) {
   constexpr int NV = Elem<DIM>::NV;
-  constexpr int LPC = DIM == 3 ? MPM_P2G_LANES_3D : 1;
-  constexpr int SPL = NV / LPC;
+  constexpr int T = p2g_tile_t<BOX>();
+  constexpr int CB = T / NV;
   constexpr int NVAL = 1 + 3 * DIM;
   constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM;
-  constexpr bool MM = MODE != 1, FORCES = MODE != 0;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t c = t / LPC;
-  const int h = (int)(t % LPC);
-  const bool valid = c < s.ncells;
-  const int n = valid ? s.cnt[c] : 0;
-  const int s0 = valid ? s.start[c] : 0;
-  if constexpr (MODE != 1) {
-    if (h == 0 && n > 1) {  // ascending particle ids within the cell
-      int32_t* seg = s.order + s0;
-      for (int a = 1; a < n; ++a) {
-        const int32_t key = seg[a];
-        int b = a - 1;
-        while (b >= 0 && seg[b] > key) {
-          seg[b + 1] = seg[b];
-          --b;
-        }
-        seg[b + 1] = key;
-      }
-    }
-    __syncwarp();
+  using RW = MTileRows<DIM, MODE, BOX>;
+  constexpr bool MM = RW::MM, FORCES = RW::FORCES;
+  __shared__ float rows[RW::N][T];
+  const int t = threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * CB;
+  if (c0 >= s.ncells) return;
+  const int64_t c1 = c0 + CB < s.ncells ? c0 + CB : s.ncells;
+  const int64_t q_begin = s.start[c0], q_end = s.start[c1 - 1] + s.cnt[c1 - 1];
+  if (q_begin == q_end) return;  // no particles in the tile (the whole block)
+  const int64_t c = c0 + t / NV;
+  const int k = t % NV;
+  const bool mine = c < c1;
+  const int64_t a0 = mine ? s.start[c] : 0;
+  const int64_t a1 = mine ? a0 + s.cnt[c] : 0;
+  if constexpr (MODE != 1) sort_cell_ids<NV>(s.order + a0, (int)(a1 - a0), k);
+  CellMap<DIM, BOX, float> box_map;
+  if constexpr (BOX && FORCES) {
+    if (a1 > a0) box_map = cell_map<DIM, true, float>(s, (int)c, nullptr, nullptr);
   }
-  if (!valid || n == 0) return;
-  int nid[NV];
-  float Xr[NV * DIM];
-  cell_nodes_rel<DIM, BOX>(s, (int)c, nid, Xr);
-  float acc[SPL][NVAL], cmp[SPL][NVAL];
-#pragma unroll
-  for (int k = 0; k < SPL; ++k)
-#pragma unroll
-    for (int v = 0; v < NVAL; ++v) acc[k][v] = cmp[k][v] = 0.f;
   const float gv[3] = {g0, g1, g2};
-  for (int j = 0; j < n; ++j) {
-    const int64_t p = s.order[s0 + j];
-    double x[DIM];
-    load_x<DIM>(s, p, x);
-    float xi[DIM], Nk[SPL], Gk[SPL * DIM];
-    xi_f32<DIM>(s, (int)c, x, xi);
-    if constexpr (DIM == 3 && LPC == 4) {
-      // lane h owns slots 2h, 2h+1: the half (z factor) h / 2, pair h % 2
-      float N4[4], G4[12];
-      lane_shape<DIM>(xi, h / 2, N4, G4);
-      const int k0 = (h % 2) * 2;
+  float acc[NVAL], cmp[NVAL];
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        Nk[k] = N4[k0 + k];
+  for (int v = 0; v < NVAL; ++v) acc[v] = cmp[v] = 0.f;
+  for (int64_t q0 = q_begin; q0 < q_end; q0 += T) {
+    if (q0 != q_begin) __syncthreads();  // the previous chunk is consumed
+    if (q0 + t < q_end) {
+      const int64_t p = s.order[q0 + t];
+      const int pc = s.cell[p];
+      double x[DIM];
+      load_x<DIM>(s, p, x);
+      float xi[DIM];
+      xi_f32<DIM>(s, pc, x, xi);
 #pragma unroll
-        for (int d = 0; d < 3; ++d) Gk[k * 3 + d] = G4[(k0 + k) * 3 + d];
+      for (int d = 0; d < DIM; ++d) rows[RW::XI + d][t] = xi[d];
+      rows[RW::M][t] = pmf<DIM>(s, PM<DIM>::MASS, p);
+      if constexpr (MM) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) rows[RW::V + d][t] = pmf<DIM>(s, PM<DIM>::V + d, p);
       }
-    } else {
-      lane_shape<DIM>(xi, h, Nk, Gk);
-    }
-    const float m = pmf<DIM>(s, PM<DIM>::MASS, p);
-    if constexpr (MM) {
-      float v[DIM];
+      if constexpr (FORCES) {
+        rows[RW::SC][t] = -(pmf<DIM>(s, PM<DIM>::V0, p) * (1.f + pmf<DIM>(s, PM<DIM>::JP, p)));
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) v[d] = pmf<DIM>(s, PM<DIM>::V + d, p);
+        for (int q = 0; q < PF<DIM>::NS; ++q) rows[RW::S + q][t] = pmf<DIM>(s, PM<DIM>::S + q, p);
+        if constexpr (!BOX) {
+          int nid[NV];
+          float Xr[NV * DIM];
+          cell_nodes_rel<DIM, false>(s, pc, nid, Xr);
+          const CellMap<DIM, false, float> m = cell_map<DIM, false>(s, pc, xi, Xr);
 #pragma unroll
-      for (int k = 0; k < SPL; ++k) {
-        const float mN = m * Nk[k];
-        kahan_add(acc[k][MASS], cmp[k][MASS], mN);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) kahan_add(acc[k][MOM + d], cmp[k][MOM + d], mN * v[d]);
+          for (int q = 0; q < DIM * DIM; ++q) rows[RW::INV + q][t] = m.inv[q];
+        }
       }
     }
-    if constexpr (FORCES) {
-      const CellMap<DIM, BOX, float> map = cell_map<DIM, BOX>(s, (int)c, xi, Xr);
-      const float vol = pmf<DIM>(s, PM<DIM>::V0, p) * (1.f + pmf<DIM>(s, PM<DIM>::JP, p));
-      const float sc = -vol;
-      constexpr int NS = PF<DIM>::NS;
-      float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    __syncthreads();
+    const int64_t j0 = a0 > q0 ? a0 : q0;
+    const int64_t j1 = a1 < q0 + T ? a1 : q0 + T;
+    for (int64_t j = j0; j < j1; ++j) {
+      const int r = (int)(j - q0);
+      float xi[DIM], N, G[DIM];
 #pragma unroll
-      for (int k = 0; k < NS; ++k) sig[k] = pmf<DIM>(s, PM<DIM>::S + k, p);
+      for (int d = 0; d < DIM; ++d) xi[d] = rows[RW::XI + d][r];
+      node_shape<DIM>(xi, k, N, G);
+      const float m = rows[RW::M][r];
+      if constexpr (MM) {
+        const float mN = m * N;
+        kahan_add(acc[MASS], cmp[MASS], mN);
 #pragma unroll
-      for (int k = 0; k < SPL; ++k) {
+        for (int d = 0; d < DIM; ++d) kahan_add(acc[MOM + d], cmp[MOM + d], mN * rows[RW::V + d][r]);
+      }
+      if constexpr (FORCES) {
+        const float sc = rows[RW::SC][r];
+        float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) kahan_add(acc[k][FEXT + d], cmp[k][FEXT + d], (gv[d] * m) * Nk[k]);
+        for (int q = 0; q < PF<DIM>::NS; ++q) sig[q] = rows[RW::S + q][r];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) kahan_add(acc[FEXT + d], cmp[FEXT + d], (gv[d] * m) * N);
         float Dn[DIM];
-        map.grad(&Gk[k * DIM], Dn);
+        if constexpr (BOX) {
+          box_map.grad(G, Dn);
+        } else {
+          CellMap<DIM, false, float> m2;
+#pragma unroll
+          for (int q = 0; q < DIM * DIM; ++q) m2.inv[q] = rows[RW::INV + q][r];
+          m2.grad(G, Dn);
+        }
         float f[DIM];
         if constexpr (DIM == 2) {
           f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
@@ -184,21 +200,19 @@ __global__ void __launch_bounds__(128, MPM_MIXED_P2G_MIN_BLOCKS)
           f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
         }
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) kahan_add(acc[k][FINT + d], cmp[k][FINT + d], f[d] * sc);
+        for (int d = 0; d < DIM; ++d) kahan_add(acc[FINT + d], cmp[FINT + d], f[d] * sc);
       }
     }
   }
-  float* out = s.partials_f + ((int64_t)c * NV + h * SPL) * NVAL;
+  if (!mine || a1 == a0) return;  // empty cells keep no partials
+  float* out = s.partials_f + ((int64_t)c * NV + k) * NVAL;
+  if constexpr (MM) {
 #pragma unroll
-  for (int k = 0; k < SPL; ++k) {
-    if constexpr (MM) {
+    for (int v = MASS; v < FEXT; ++v) out[v] = acc[v] - cmp[v];
+  }
+  if constexpr (FORCES) {
 #pragma unroll
-      for (int v = MASS; v < FEXT; ++v) out[k * NVAL + v] = acc[k][v] - cmp[k][v];
-    }
-    if constexpr (FORCES) {
-#pragma unroll
-      for (int v = FEXT; v < NVAL; ++v) out[k * NVAL + v] = acc[k][v] - cmp[k][v];
-    }
+    for (int v = FEXT; v < NVAL; ++v) out[v] = acc[v] - cmp[v];
   }
 }
 
@@ -849,10 +863,10 @@ template <int DIM, bool BOX>
 void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& pr) {
   const int64_t np = s.np, nn = s.nn;
   if (np == 0) return;
-  constexpr int LPC = DIM == 3 ? MPM_P2G_LANES_3D : 1;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
   if (s.svf) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
-  const unsigned pb = nblk(np, 128), nb = nblk(nn, 256), cb = nblk(s.ncells * LPC, 128);
+  const unsigned pb = nblk(np, 128), nb = nblk(nn, 256), tile = p2g_tile_t<BOX>();
+  const unsigned tb = nblk(s.ncells, tile / Elem<DIM>::NV);
   const unsigned mcb = (unsigned)(pb < 148 * 8 ? pb : 148 * 8);
   auto mc_returns = [&]() {
     if (!s.svf) return;
@@ -866,7 +880,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
   pr.end(K_SORT, st);
   if (a.scheme == 1) {  // USL
     pr.begin(K_P2G, st);
-    k_p2g_cells_mixed<DIM, 2, BOX><<<cb, 128, 0, st>>>(s, g0, g1, g2);
+    k_p2g_tiles_mixed<DIM, 2, BOX><<<tb, tile, 0, st>>>(s, g0, g1, g2);
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes_mixed<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
@@ -884,7 +898,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     mc_returns();
   } else {  // USF
     pr.begin(K_P2G, st);
-    k_p2g_cells_mixed<DIM, 0, BOX><<<cb, 128, 0, st>>>(s, g0, g1, g2);
+    k_p2g_tiles_mixed<DIM, 0, BOX><<<tb, tile, 0, st>>>(s, g0, g1, g2);
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
     k_nodes_mixed<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
@@ -894,7 +908,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     pr.end(K_STRESS, st);
     mc_returns();
     pr.begin(K_P2G_FORCES, st);
-    k_p2g_cells_mixed<DIM, 1, BOX><<<cb, 128, 0, st>>>(s, g0, g1, g2);
+    k_p2g_tiles_mixed<DIM, 1, BOX><<<tb, tile, 0, st>>>(s, g0, g1, g2);
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
     k_nodes_mixed<DIM, 2><<<nb, 256, 0, st>>>(s, a.dt, a.damping);

@@ -194,38 +194,91 @@ __device__ __forceinline__ void dn_dx_node(const double* xi, const Map& map, int
   map.grad(&G[n * DIM], Dn);
 }
 
-// Shape functions and natural gradients of the SPL slots a lane owns: all
-// of them in 2D; in 3D lane h owns slots 4h..4h+3, which share the z factor
-// (1 - xi_z) or (1 + xi_z).  Same operations and grouping as shapefn /
-// grad_shapefn (the z factor is the last product), with the lane's half
-// chosen by value selects so the two lanes of a cell do not diverge.
+// ------------------------------------------------------------ P2G cell tiles
+// Threads per tile: 256 on a tensor-product grid; 128 on a general mesh,
+// whose staged rows add J^-1 and whose threads need more registers.
+template <bool BOX>
+constexpr int p2g_tile_t() { return BOX ? 256 : 128; }
+
+// Particle ids of one cell in ascending order (the fill order is not
+// deterministic), by the cell's NV threads of a block (k = 0 .. NV - 1):
+// thread k ranks entries k, k + NV, ... (sort_per_thread<NV>() of them, 16
+// per cell) against the whole segment; after a block barrier the caller
+// writes them to their ranks (ids are distinct).  A longer segment is left to
+// thread 0.
+template <int NV>
+constexpr int sort_per_thread() { return 16 / NV; }
+template <int NV>
+__device__ __forceinline__ bool rank_cell_segment(const int32_t* seg, int n, int k, int32_t* id,
+                                                  int* rank) {
+  if (n > 16) return false;
+#pragma unroll
+  for (int r = 0; r < sort_per_thread<NV>(); ++r) {
+    const int i = k + NV * r;
+    if (i < n) {
+      const int32_t e = seg[i];
+      int below = 0;
+      for (int j = 0; j < n; ++j) below += seg[j] < e ? 1 : 0;
+      id[r] = e;
+      rank[r] = below;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void insertion_sort(int32_t* seg, int n) {
+  for (int a = 1; a < n; ++a) {
+    const int32_t key = seg[a];
+    int b = a - 1;
+    while (b >= 0 && seg[b] > key) {
+      seg[b + 1] = seg[b];
+      --b;
+    }
+    seg[b + 1] = key;
+  }
+}
+
+// The ranking and the writes, with the block barriers between and after
+// them: every thread of the block calls this (n = 0 for threads without a
+// cell).
+template <int NV>
+__device__ __forceinline__ void sort_cell_ids(int32_t* seg, int n, int k) {
+  constexpr int SPT = sort_per_thread<NV>();
+  int32_t id[SPT];
+  int rank[SPT];
+  const bool ranked = rank_cell_segment<NV>(seg, n, k, id, rank);
+  __syncthreads();
+  if (ranked) {
+#pragma unroll
+    for (int r = 0; r < SPT; ++r)
+      if (k + NV * r < n) seg[rank[r]] = id[r];
+  } else if (k == 0) {
+    insertion_sort(seg, n);
+  }
+  __syncthreads();
+}
+
+// Shape function and natural gradient of one local node n, with shapefn /
+// grad_shapefn's operations and grouping (the constant first, then the x, y
+// and z factors in that order, skipping the differentiated one).
 template <int DIM, typename R>
-__device__ __forceinline__ void lane_shape(const R* xi, int h, R* Nk, R* Gk) {
+__device__ __forceinline__ void node_shape(const R* xi, int n, R& N, R* G) {
+  const bool px = off_i(n), py = off_j(n);
+  const R a = px ? 1 + xi[0] : 1 - xi[0];
+  const R b = py ? 1 + xi[1] : 1 - xi[1];
   if constexpr (DIM == 2) {
-    shapefn<2>(xi, Nk);
-    grad_shapefn<2>(xi, Gk);
+    const R e = R(0.25);
+    N = e * a * b;
+    G[0] = (px ? e : -e) * b;
+    G[1] = (py ? e : -e) * a;
   } else {
-    const R xm = 1 - xi[0], xp = 1 + xi[0], ym = 1 - xi[1], yp = 1 + xi[1];
-    const R z = h ? (1 + xi[2]) : (1 - xi[2]);
+    const bool pz = off_k(n);
+    const R z = pz ? 1 + xi[2] : 1 - xi[2];
     const R e = R(0.125);
-    const R zs = h ? e : -e;  // sign of d/dxi_z
-    // in-plane order of the four nodes of a face: (-,-), (+,-), (+,+), (-,+)
-    Nk[0] = e * xm * ym * z;
-    Nk[1] = e * xp * ym * z;
-    Nk[2] = e * xp * yp * z;
-    Nk[3] = e * xm * yp * z;
-    Gk[0 * 3 + 0] = -e * ym * z;
-    Gk[1 * 3 + 0] = e * ym * z;
-    Gk[2 * 3 + 0] = e * yp * z;
-    Gk[3 * 3 + 0] = -e * yp * z;
-    Gk[0 * 3 + 1] = -e * xm * z;
-    Gk[1 * 3 + 1] = -e * xp * z;
-    Gk[2 * 3 + 1] = e * xp * z;
-    Gk[3 * 3 + 1] = e * xm * z;
-    Gk[0 * 3 + 2] = zs * xm * ym;
-    Gk[1 * 3 + 2] = zs * xp * ym;
-    Gk[2 * 3 + 2] = zs * xp * yp;
-    Gk[3 * 3 + 2] = zs * xm * yp;
+    N = e * a * b * z;
+    G[0] = (px ? e : -e) * b * z;
+    G[1] = (py ? e : -e) * a * z;
+    G[2] = (pz ? e : -e) * a * b;
   }
 }
 
