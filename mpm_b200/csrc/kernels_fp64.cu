@@ -1021,7 +1021,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     k_p2g_tiles<DIM, MODE, BOX><<<nblocks(s.ncells, TT / Elem<DIM>::NV), TT, 0, st>>>(
         s, a.g[0], a.g[1], a.g[2]);
   };
-  pr.begin(K_SORT, st);
+  pr.begin(K_SORT, st, SORT_KERNELS);
   counting_sort_impl(s, st);
   pr.end(K_SORT, st);
   if (a.scheme == 2) {  // MUSL (mpm_scheme_musl.tcc)

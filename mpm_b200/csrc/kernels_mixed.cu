@@ -875,7 +875,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     pr.end(K_MC_RETURN, st);
   };
   const float g0 = (float)a.g[0], g1 = (float)a.g[1], g2 = (float)a.g[2];
-  pr.begin(K_SORT, st);
+  pr.begin(K_SORT, st, SORT_KERNELS);
   counting_sort(s, st);
   pr.end(K_SORT, st);
   if (a.scheme == 1) {  // USL

@@ -554,7 +554,7 @@ void step_tangent(const DevState& s, const StepArgs& a, cudaStream_t st, Profile
   if (s.np == 0) return;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
   if (s.sv) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
-  pr.begin(K_SORT, st);
+  pr.begin(K_SORT, st, SORT_KERNELS);
   counting_sort(s, st);
   pr.end(K_SORT, st);
   pr.begin(K_P2G, st);

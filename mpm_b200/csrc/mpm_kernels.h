@@ -39,14 +39,16 @@ constexpr int SCAN_BLOCK = 4096;  // cells per block of the counting-sort scan
 constexpr int PAD_PARTICLES = 128;
 const char* kernel_name(int kid);
 
-// Counts launches; when enabled, brackets every launch with a pair of CUDA
-// events on the launching stream and accumulates their elapsed times.
+// Counts kernel launches; when enabled, brackets every phase (one kernel, or
+// the SORT_KERNELS kernels of the counting sort) with a pair of CUDA events on
+// the launching stream and accumulates their elapsed times.
+constexpr int SORT_KERNELS = 5;  // count, two scan levels, scan add, fill
 struct Profiler {
   bool enabled = false;
   int64_t launches = 0;
   double total_ms[K_NKERNELS] = {};
   int64_t count[K_NKERNELS] = {};
-  void begin(int kid, cudaStream_t st);
+  void begin(int kid, cudaStream_t st, int kernels = 1);
   void end(int kid, cudaStream_t st);
   void collect();  // after the stream has been synchronised
   void reset();
