@@ -26,7 +26,7 @@
 #include "mpm_state.cuh"
 
 #ifndef MPM_MIXED_G2P_MIN_BLOCKS
-#define MPM_MIXED_G2P_MIN_BLOCKS 4
+#define MPM_MIXED_G2P_MIN_BLOCKS 6  // 80 registers, no spills: 0.478 -> 0.374 ms (4M, 3D)
 #endif
 #ifndef MPM_MC_RETURN_MIN_BLOCKS
 #define MPM_MC_RETURN_MIN_BLOCKS 4
