@@ -40,16 +40,28 @@ namespace mpm_b200 {
 namespace {
 
 // ------------------------------------------------------------ counting sort
+// Per-cell counts and each particle's slot within its cell.  The lanes of a
+// warp in the same cell (most of them: particles are stored in cell order)
+// share one atomic; the slot order within a cell is not deterministic either
+// way and P2G sorts every cell's segment.
 __global__ void __launch_bounds__(256) k_count(DevState s) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= s.np) return;
-  const int c = s.cell[p];
-  if (c < 0 || c >= s.ncells) {
-    if (c >= s.ncells) raise_err(s, ERR_BADCELL);
-    s.rank[p] = -1;
+  const bool in = p < s.np;
+  const int c = in ? s.cell[p] : -1;
+  if (c >= s.ncells) raise_err(s, ERR_BADCELL);
+  const bool valid = c >= 0 && c < s.ncells;
+  const unsigned active = __ballot_sync(0xffffffffu, valid);  // every lane of the warp
+  if (!valid) {
+    if (in) s.rank[p] = -1;
     return;
   }
-  s.rank[p] = atomicAdd(&s.cnt[c], 1);
+  const unsigned same = __match_any_sync(active, c);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(same) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&s.cnt[c], __popc(same));
+  base = __shfl_sync(same, base, leader);
+  s.rank[p] = base + __popc(same & ((1u << lane) - 1u));
 }
 
 // exclusive scan of n ints, SCAN_BLOCK per block (1024 threads x 4)
@@ -264,7 +276,6 @@ __device__ __forceinline__ bool gather_node(const DevState& s, int64_t node, int
   for (int v = 0; v < nv; ++v) sum[v] = 0.;
   bool active = false;
   auto add = [&](int c, int slot) {
-    if (s.cnt[c] == 0) return;
     const double* src = s.partials + ((int64_t)c * NV + slot) * NVAL + v0;
     if (!active) {
       for (int v = 0; v < nv; ++v) sum[v] = src[v];
@@ -274,27 +285,15 @@ __device__ __forceinline__ bool gather_node(const DevState& s, int64_t node, int
     }
   };
   if (s.structured) {
-    const int nx = s.gcells[0] + 1, ny = s.gcells[1] + 1;
-    const int i = (int)(node % nx);
-    const int j = DIM == 2 ? (int)(node / nx) : (int)((node / nx) % ny);
-    const int k = DIM == 2 ? 0 : (int)(node / ((int64_t)nx * ny));
-    // slot of the node in the cell at offset (di, dj, dk) below/left of it
-    const int slot2[2][2] = {{0, 1}, {3, 2}};  // [dj][di]
-    const int kmin = DIM == 3 ? k - 1 : 0, kmax = DIM == 3 ? k : 0;
-    for (int ck = kmin; ck <= kmax; ++ck) {
-      if (DIM == 3 && (ck < 0 || ck >= s.gcells[2])) continue;
-      for (int cj = j - 1; cj <= j; ++cj) {
-        if (cj < 0 || cj >= s.gcells[1]) continue;
-        for (int ci = i - 1; ci <= i; ++ci) {
-          if (ci < 0 || ci >= s.gcells[0]) continue;
-          const int di = i - ci, dj = j - cj, dk = DIM == 3 ? k - ck : 0;
-          const int c = DIM == 2 ? ci + s.gcells[0] * cj : ci + s.gcells[0] * (cj + s.gcells[1] * ck);
-          add(c, slot2[dj][di] + 4 * dk);
-        }
-      }
-    }
+    constexpr int NC = DIM == 2 ? 4 : 8;
+    int cid[NC], slot[NC], count[NC];
+    grid_node_cells<DIM>(s, (int)node, cid, slot, count);
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
+      if (count[q] > 0) add(cid[q], slot[q]);
   } else {
-    for (int e = s.nc_off[node]; e < s.nc_off[node + 1]; ++e) add(s.nc_cell[e], s.nc_slot[e]);
+    for (int e = s.nc_off[node]; e < s.nc_off[node + 1]; ++e)
+      if (s.cnt[s.nc_cell[e]] > 0) add(s.nc_cell[e], s.nc_slot[e]);
   }
   return active;
 }

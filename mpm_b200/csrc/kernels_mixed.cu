@@ -226,32 +226,20 @@ __device__ __forceinline__ bool gather_node_mixed(const DevState& s, int64_t nod
   for (int v = 0; v < nv; ++v) sum[v] = 0.;
   bool active = false;
   auto add = [&](int c, int slot) {
-    if (s.cnt[c] == 0) return;
     const float* src = s.partials_f + ((int64_t)c * NV + slot) * NVAL + v0;
     for (int v = 0; v < nv; ++v) sum[v] += (double)src[v];
     active = true;
   };
   if (s.structured) {
-    const int nx = s.gcells[0] + 1, ny = s.gcells[1] + 1;
-    const int i = (int)(node % nx);
-    const int j = DIM == 2 ? (int)(node / nx) : (int)((node / nx) % ny);
-    const int k = DIM == 2 ? 0 : (int)(node / ((int64_t)nx * ny));
-    const int slot2[2][2] = {{0, 1}, {3, 2}};
-    const int kmin = DIM == 3 ? k - 1 : 0, kmax = DIM == 3 ? k : 0;
-    for (int ck = kmin; ck <= kmax; ++ck) {
-      if (DIM == 3 && (ck < 0 || ck >= s.gcells[2])) continue;
-      for (int cj = j - 1; cj <= j; ++cj) {
-        if (cj < 0 || cj >= s.gcells[1]) continue;
-        for (int ci = i - 1; ci <= i; ++ci) {
-          if (ci < 0 || ci >= s.gcells[0]) continue;
-          const int di = i - ci, dj = j - cj, dk = DIM == 3 ? k - ck : 0;
-          const int c = DIM == 2 ? ci + s.gcells[0] * cj : ci + s.gcells[0] * (cj + s.gcells[1] * ck);
-          add(c, slot2[dj][di] + 4 * dk);
-        }
-      }
-    }
+    constexpr int NC = DIM == 2 ? 4 : 8;
+    int cid[NC], slot[NC], count[NC];
+    grid_node_cells<DIM>(s, (int)node, cid, slot, count);
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
+      if (count[q] > 0) add(cid[q], slot[q]);
   } else {
-    for (int e = s.nc_off[node]; e < s.nc_off[node + 1]; ++e) add(s.nc_cell[e], s.nc_slot[e]);
+    for (int e = s.nc_off[node]; e < s.nc_off[node + 1]; ++e)
+      if (s.cnt[s.nc_cell[e]] > 0) add(s.nc_cell[e], s.nc_slot[e]);
   }
   return active;
 }

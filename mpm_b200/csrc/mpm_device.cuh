@@ -73,6 +73,33 @@ __device__ __forceinline__ void grid_cell_nodes(const DevState& s, int c, int* n
   }
 }
 
+// The cells around node `node` of a tensor-product grid, in ascending cell
+// id: their ids, the node's slot (local node) in each, and each cell's
+// particle count (0 for positions outside the grid).  All counts are loaded
+// before any is used.
+template <int DIM>
+__device__ __forceinline__ void grid_node_cells(const DevState& s, int node, int* cid, int* slot,
+                                                int* count) {
+  constexpr int NC = DIM == 2 ? 4 : 8;
+  const int gx = s.gcells[0], gy = s.gcells[1], gz = s.gcells[2];
+  const int nx = gx + 1, ny = gy + 1;
+  const int i = node % nx;
+  const int j = DIM == 2 ? node / nx : (node / nx) % ny;
+  const int k = DIM == 2 ? 0 : node / (nx * ny);
+#pragma unroll
+  for (int q = 0; q < NC; ++q) {
+    const int a = q & 1, b = (q >> 1) & 1, e = q >> 2;  // cell (i - 1 + a, j - 1 + b, k - 1 + e)
+    const int ci = i - 1 + a, cj = j - 1 + b, ck = k - 1 + e;
+    bool in = ci >= 0 && ci < gx && cj >= 0 && cj < gy;
+    if constexpr (DIM == 3) in = in && ck >= 0 && ck < gz;
+    const int c = DIM == 2 ? ci + gx * cj : ci + gx * (cj + gy * ck);
+    cid[q] = in ? c : 0;
+    // the node sits at offset (1 - a, 1 - b, 1 - e) in the cell
+    slot[q] = (b ? (a ? 0 : 1) : (a ? 3 : 2)) + (DIM == 3 && !e ? 4 : 0);
+    count[q] = in ? s.cnt[c] : 0;
+  }
+}
+
 // node ids and nodal coordinates of a cell
 template <int DIM>
 __device__ __forceinline__ void cell_nodes_coords(const DevState& s, int c, int* nid, double* X) {
