@@ -10,7 +10,7 @@
 //
 // Value arrays keep the FP64 layout (DevState::pf, sv, nf, partials); the
 // derivative k of each lives in the same layout in pft[k], svt[k], nft[k],
-// partt[k].  Cells hold NV lanes, one per node slot, so a lane keeps 1 + 3 DIM
+// partt[k].  P2G runs by cell tiles, one thread per cell slot holding 1 + 3 DIM
 // Dual sums.
 #include <cuda_runtime.h>
 
@@ -22,10 +22,19 @@
 #include "mpm_state.cuh"
 
 #ifndef MPM_TANGENT_G2P_MIN_BLOCKS
-#define MPM_TANGENT_G2P_MIN_BLOCKS 1
+#define MPM_TANGENT_G2P_MIN_BLOCKS 1  // the stress part
+#endif
+#ifndef MPM_TANGENT_NODES_MIN_BLOCKS
+#define MPM_TANGENT_NODES_MIN_BLOCKS 1
+#endif
+#ifndef MPM_TANGENT_RETURN_MIN_BLOCKS
+#define MPM_TANGENT_RETURN_MIN_BLOCKS 1
+#endif
+#ifndef MPM_TANGENT_KIN_MIN_BLOCKS
+#define MPM_TANGENT_KIN_MIN_BLOCKS 4  // the kinematics part
 #endif
 #ifndef MPM_TANGENT_P2G_MIN_BLOCKS
-#define MPM_TANGENT_P2G_MIN_BLOCKS 1
+#define MPM_TANGENT_P2G_MIN_BLOCKS 4  // 128 registers on a grid, no spills
 #endif
 
 namespace mpm_b200 {
@@ -86,113 +95,158 @@ __device__ __forceinline__ void jinv_dual(const D* xi, const double* X, D* inv) 
   inverse<DIM>(J, inv);
 }
 
-// Shape functions and dN/dx of every particle at the start of the step
-// (positions do not change between P2G and G2P), with their derivatives:
-// computed once here, read by both.
-template <int DIM>
-__global__ void __launch_bounds__(128) k_prep_tangent(DevState s) {
-  constexpr int NV = Elem<DIM>::NV;
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= s.np) return;
-  const int c = s.cell[p];
-  if (c < 0) return;
-  const CellGeom g = s.geom[c];
-  D x[DIM], xi[DIM], N[NV], G[NV * DIM];
+// dN/dx of one local node from its natural gradient G at the particle, with
+// the FP64 step's operations: box cells of a tensor-product grid take
+// dN/dxi * (2 / len) per axis (CellMap<DIM, true>: ihl), other cells
+// J^-1 at xi (inv).
+template <int DIM, bool BOX>
+__device__ __forceinline__ void grad_dual(const D* G, const double* ihl, const D* inv, D* Dn) {
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) x[d] = pfield<DIM>(s, PF<DIM>::X + d, p);
-  xi_dual<DIM>(g, x, xi);
-  shapefn<DIM>(xi, N);
-  grad_shapefn<DIM>(xi, G);
-  double* const* t = const_cast<double* const*>(s.prept);
-  const int64_t np = s.np;
+  for (int q = 0; q < DIM; ++q) {
+    if constexpr (BOX) {
+      Dn[q] = G[q] * ihl[q];
+    } else {
+      D a = G[0] * inv[q * DIM + 0];
 #pragma unroll
-  for (int n = 0; n < NV; ++n) st(s.prep, t, (int64_t)n * np + p, N[n]);
-  if (s.structured) {
-    // box cell: dN/dx = dN/dxi * (2 / len) per axis (CellMap<DIM, true>)
-    int ijk[3] = {0, 0, 0};
-    cell_ijk<DIM>(s, c, ijk);
-#pragma unroll
-    for (int n = 0; n < NV; ++n)
-#pragma unroll
-      for (int q = 0; q < DIM; ++q)
-        st(s.prep, t, (int64_t)(NV + n * DIM + q) * np + p, G[n * DIM + q] * s.axis_ihl[q][ijk[q]]);
-    return;
-  }
-  int nid[NV];
-  double X[NV * DIM];
-  D inv[DIM * DIM];
-  cell_nodes_coords<DIM>(s, c, nid, X);
-  jinv_dual<DIM>(xi, X, inv);
-#pragma unroll
-  for (int n = 0; n < NV; ++n)
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) {
-      D a = G[n * DIM + 0] * inv[q * DIM + 0];
-#pragma unroll
-      for (int k = 1; k < DIM; ++k) a = a + G[n * DIM + k] * inv[q * DIM + k];
-      st(s.prep, t, (int64_t)(NV + n * DIM + q) * np + p, a);
+      for (int e = 1; e < DIM; ++e) a = a + G[e] * inv[q * DIM + e];
+      Dn[q] = a;
     }
+  }
 }
 
-// ---------------------------------------------------------------- P2G cells
-template <int DIM>
-__global__ void __launch_bounds__(128, MPM_TANGENT_P2G_MIN_BLOCKS) k_p2g_tangent(DevState s, double g0, double g1, double g2) {
+// ---------------------------------------------------------------- P2G tiles
+// k_p2g_tiles on Dual values: a block takes tangent_tile_t / NV consecutive
+// cells, stages their particles (local coordinates, velocity, -V, stress and,
+// off a tensor-product grid, J^-1, each a Dual of 1 + NT doubles, and the
+// mass) in shared memory, and thread (cell, slot k) adds its slot's
+// contributions in particle id order.  N and dN/dx of slot k come from
+// node_shape with the FP64 tiles' operations, so the values are the FP64
+// step's bit for bit.
+template <bool BOX>
+constexpr int tangent_tile_t() { return BOX ? 128 : 64; }
+
+template <int DIM, bool BOX>
+__global__ void __launch_bounds__(tangent_tile_t<BOX>(), MPM_TANGENT_P2G_MIN_BLOCKS)
+    k_p2g_tiles_tangent(DevState s, double g0, double g1, double g2) {
   constexpr int NV = Elem<DIM>::NV;
+  constexpr int T = tangent_tile_t<BOX>();
+  constexpr int CB = T / NV;
   constexpr int NVAL = 1 + 3 * DIM;
   constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t c = t / NV;
-  const int slot = (int)(t % NV);
-  const bool valid = c < s.ncells;
-  const int n = valid ? s.cnt[c] : 0;
-  const int s0 = valid ? s.start[c] : 0;
-  if (slot == 0 && n > 1) {  // ascending particle ids within the cell
-    int32_t* seg = s.order + s0;
-    for (int a = 1; a < n; ++a) {
-      const int32_t key = seg[a];
-      int b = a - 1;
-      while (b >= 0 && seg[b] > key) {
-        seg[b + 1] = seg[b];
-        --b;
-      }
-      seg[b + 1] = key;
-    }
+  constexpr int NS = PF<DIM>::NS;
+  constexpr int W = 1 + NT;  // doubles per staged Dual
+  constexpr int R_XI = 0, R_V = DIM, R_SC = 2 * DIM, R_S = 2 * DIM + 1, R_INV = R_S + NS;
+  constexpr int NDUAL = R_INV + (BOX ? 0 : DIM * DIM);
+  __shared__ double rows[NDUAL * W + 1][T];  // the last row: mass
+  auto put = [&](int f, int t, const D& x) {
+    rows[f * W][t] = x.v;
+#pragma unroll
+    for (int q = 0; q < NT; ++q) rows[f * W + 1 + q][t] = x.d[q];
+  };
+  auto get = [&](int f, int r) {
+    D x;
+    x.v = rows[f * W][r];
+#pragma unroll
+    for (int q = 0; q < NT; ++q) x.d[q] = rows[f * W + 1 + q][r];
+    return x;
+  };
+  const int t = threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * CB;
+  if (c0 >= s.ncells) return;
+  const int64_t c1 = c0 + CB < s.ncells ? c0 + CB : s.ncells;
+  const int64_t q_begin = s.start[c0], q_end = s.start[c1 - 1] + s.cnt[c1 - 1];
+  if (q_begin == q_end) return;  // no particles in the tile (the whole block)
+  const int64_t c = c0 + t / NV;
+  const int k = t % NV;
+  const bool mine = c < c1;
+  const int64_t a0 = mine ? s.start[c] : 0;
+  const int64_t a1 = mine ? a0 + s.cnt[c] : 0;
+  sort_cell_ids<NV>(s.order + a0, (int)(a1 - a0), k);  // ascending particle ids
+  double ihl[DIM];  // J^-1 of a box cell
+  if constexpr (BOX) {
+    int ijk[3] = {0, 0, 0};
+    if (a1 > a0) cell_ijk<DIM>(s, (int)c, ijk);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) ihl[d] = a1 > a0 ? s.axis_ihl[d][ijk[d]] : 0.;
   }
-  __syncwarp();
-  if (!valid || n == 0) return;
-  D acc[NVAL];
   const double gv[3] = {g0, g1, g2};
   const int64_t np = s.np;
-  for (int j = 0; j < n; ++j) {
-    const int64_t p = s.order[s0 + j];
-    const double m = s.pf[(int64_t)PF<DIM>::MASS * np + p];  // the mass carries no tangent
-    const D Nk = ld(s.prep, s.prept, (int64_t)slot * np + p);
-    const D mN = m * Nk;
-    acc[MASS] += mN;
+  D acc[NVAL];
+  for (int64_t q0 = q_begin; q0 < q_end; q0 += T) {
+    if (q0 != q_begin) __syncthreads();  // the previous chunk is consumed
+    if (q0 + t < q_end) {
+      const int64_t p = s.order[q0 + t];
+      const int pc = s.cell[p];
+      D x[DIM], xi[DIM];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) acc[MOM + d] += mN * pfield<DIM>(s, PF<DIM>::V + d, p);
+      for (int d = 0; d < DIM; ++d) x[d] = pfield<DIM>(s, PF<DIM>::X + d, p);
+      xi_dual<DIM>(s.geom[pc], x, xi);
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) acc[FEXT + d] += (gv[d] * m) * Nk;
-    D Dn[DIM];
+      for (int d = 0; d < DIM; ++d) put(R_XI + d, t, xi[d]);
 #pragma unroll
-    for (int q = 0; q < DIM; ++q) Dn[q] = ld(s.prep, s.prept, (int64_t)(NV + slot * DIM + q) * np + p);
-    D sig[6];
+      for (int d = 0; d < DIM; ++d) put(R_V + d, t, pfield<DIM>(s, PF<DIM>::V + d, p));
+      put(R_SC, t, -1. * pfield<DIM>(s, PF<DIM>::VOL, p));
 #pragma unroll
-    for (int k = 0; k < PF<DIM>::NS; ++k) sig[k] = pfield<DIM>(s, PF<DIM>::S + k, p);
-    const D sc = -1. * pfield<DIM>(s, PF<DIM>::VOL, p);
-    D f[DIM];
-    if constexpr (DIM == 2) {
-      f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
-      f[1] = Dn[1] * sig[1] + Dn[0] * sig[3];
-    } else {
-      f[0] = Dn[0] * sig[0] + Dn[1] * sig[3] + Dn[2] * sig[5];
-      f[1] = Dn[1] * sig[1] + Dn[0] * sig[3] + Dn[2] * sig[4];
-      f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
+      for (int q = 0; q < NS; ++q) put(R_S + q, t, pfield<DIM>(s, PF<DIM>::S + q, p));
+      rows[NDUAL * W][t] = s.pf[(int64_t)PF<DIM>::MASS * np + p];  // the mass carries no tangent
+      if constexpr (!BOX) {
+        int nid[NV];
+        double X[NV * DIM];
+        D inv[DIM * DIM];
+        cell_nodes_coords<DIM>(s, pc, nid, X);
+        jinv_dual<DIM>(xi, X, inv);
+#pragma unroll
+        for (int q = 0; q < DIM * DIM; ++q) put(R_INV + q, t, inv[q]);
+      }
     }
+    __syncthreads();
+    const int64_t j0 = a0 > q0 ? a0 : q0;
+    const int64_t j1 = a1 < q0 + T ? a1 : q0 + T;
+    for (int64_t j = j0; j < j1; ++j) {
+      const int r = (int)(j - q0);
+      D xi[DIM], Nk, G[DIM];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) acc[FINT + d] += f[d] * sc;
+      for (int d = 0; d < DIM; ++d) xi[d] = get(R_XI + d, r);
+      node_shape<DIM>(xi, k, Nk, G);
+      const double m = rows[NDUAL * W][r];
+      const D mN = m * Nk;
+      acc[MASS] += mN;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) acc[MOM + d] += mN * get(R_V + d, r);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) acc[FEXT + d] += (gv[d] * m) * Nk;
+      D Dn[DIM];
+      if constexpr (BOX) {
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) Dn[q] = G[q] * ihl[q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) {
+          D a = G[0] * get(R_INV + q * DIM + 0, r);
+#pragma unroll
+          for (int e = 1; e < DIM; ++e) a = a + G[e] * get(R_INV + q * DIM + e, r);
+          Dn[q] = a;
+        }
+      }
+      D sig[6];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) sig[q] = get(R_S + q, r);
+      const D sc = get(R_SC, r);
+      D f[DIM];
+      if constexpr (DIM == 2) {
+        f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
+        f[1] = Dn[1] * sig[1] + Dn[0] * sig[3];
+      } else {
+        f[0] = Dn[0] * sig[0] + Dn[1] * sig[3] + Dn[2] * sig[5];
+        f[1] = Dn[1] * sig[1] + Dn[0] * sig[3] + Dn[2] * sig[4];
+        f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
+      }
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) acc[FINT + d] += f[d] * sc;
+    }
   }
-  const int64_t o = ((int64_t)c * NV + slot) * NVAL;
+  if (!mine || a1 == a0) return;  // empty cells keep no partials
+  const int64_t o = ((int64_t)c * NV + k) * NVAL;
 #pragma unroll
   for (int v = 0; v < NVAL; ++v) st(s.partials, const_cast<double* const*>(s.partt), o + v, acc[v]);
 }
@@ -228,7 +282,7 @@ __device__ __forceinline__ bool gather_node_tangent(const DevState& s, int64_t n
 
 // USL node update (node.tcc:236-252 then :309-345) on Dual values
 template <int DIM>
-__global__ void __launch_bounds__(128) k_nodes_tangent(DevState s, double dt, double damping) {
+__global__ void __launch_bounds__(128, MPM_TANGENT_NODES_MIN_BLOCKS) k_nodes_tangent(DevState s, double dt, double damping) {
   constexpr int NVAL = 1 + 3 * DIM;
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= s.nn) return;
@@ -298,9 +352,14 @@ __global__ void __launch_bounds__(128) k_nodes_tangent(DevState s, double dt, do
 }
 
 // --------------------------------------------------------------------- G2P
-// k_g2p<DIM, true, FLIP> and stress_update of the FP64 step on Dual values.
-template <int DIM, bool FLIP>
-__global__ void __launch_bounds__(128, MPM_TANGENT_G2P_MIN_BLOCKS) k_g2p_tangent(DevState s, double dt, double beta) {
+// stress_update of the FP64 step on Dual values (strain, F, volume, density,
+// material; plastic MohrCoulomb points deferred to k_mc_return_tangent), then
+// k_g2p<DIM, true, FLIP>'s kinematics and locate: two kernels, so that the
+// register-heavy Dual material update does not hold the kinematics to its
+// occupancy.  The stress kernel runs first: both work at the step-start
+// position.
+template <int DIM, bool BOX>
+__global__ void __launch_bounds__(128, MPM_TANGENT_G2P_MIN_BLOCKS) k_stress_tangent(DevState s, double dt) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int NS = PF<DIM>::NS;
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -310,60 +369,25 @@ __global__ void __launch_bounds__(128, MPM_TANGENT_G2P_MIN_BLOCKS) k_g2p_tangent
   const int64_t nn = s.nn;
   double* const* nt = s.nft;
   const int64_t np = s.np;
-  D x[DIM], N[NV];
+  D x[DIM], xi[DIM];
   int nid[NV];
   double X[NV * DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) x[d] = pfield<DIM>(s, PF<DIM>::X + d, p);
-#pragma unroll
-  for (int n = 0; n < NV; ++n) N[n] = ld(s.prep, s.prept, (int64_t)n * np + p);
+  xi_dual<DIM>(s.geom[c], x, xi);  // at the step-start position
   cell_nodes_coords<DIM>(s, c, nid, X);
-  D nvel[DIM], nacc[DIM];
+  // stress update (mpm_scheme.tcc:75-103) with dN/dx at the particle, one
+  // node at a time
+  double ihl[DIM];
+  D inv[DIM * DIM];
+  if constexpr (BOX) {
+    int ijk[3] = {0, 0, 0};
+    cell_ijk<DIM>(s, c, ijk);
 #pragma unroll
-  for (int i = 0; i < NV; ++i) {
-#pragma unroll
-    for (int d = 0; d < DIM; ++d)
-      nvel[d] += N[i] * ld(s.nf, nt, (int64_t)(NF<DIM>::VEL + d) * nn + nid[i]);
-    if constexpr (FLIP) {
-#pragma unroll
-      for (int d = 0; d < DIM; ++d)
-        nacc[d] += N[i] * ld(s.nf, nt, (int64_t)(NF<DIM>::ACC + d) * nn + nid[i]);
-    }
-  }
-  D v[DIM];
-#pragma unroll
-  for (int d = 0; d < DIM; ++d) v[d] = pfield<DIM>(s, PF<DIM>::V + d, p);
-  if constexpr (FLIP) {
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) v[d] += nacc[d] * dt;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) v[d] = beta * v[d] + (1.0 - beta) * nvel[d];
+    for (int d = 0; d < DIM; ++d) ihl[d] = s.axis_ihl[d][ijk[d]];
   } else {
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) v[d] = nvel[d];
+    jinv_dual<DIM>(xi, X, inv);
   }
-  double xn[DIM];
-#pragma unroll
-  for (int d = 0; d < DIM; ++d) {
-    const D xd = x[d] + nvel[d] * dt;
-    xn[d] = xd.v;
-    set_pfield<DIM>(s, PF<DIM>::X + d, p, xd);
-    set_pfield<DIM>(s, PF<DIM>::U + d, p, pfield<DIM>(s, PF<DIM>::U + d, p) + nvel[d] * dt);
-  }
-  const int pv = s.pvc[p];
-  if (pv >= 0) {
-    const ParticleVC& r = s.pvcs[pv];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d)
-      if (r.mask & (1u << d)) v[d] = D(r.value[d]);
-  }
-#pragma unroll
-  for (int d = 0; d < DIM; ++d) set_pfield<DIM>(s, PF<DIM>::V + d, p, v[d]);
-
-  // stress update (mpm_scheme.tcc:75-103) with dN/dx at the particle
-  D Dm[NV * DIM];
-#pragma unroll
-  for (int n = 0; n < NV * DIM; ++n) Dm[n] = ld(s.prep, s.prept, (int64_t)(NV + n) * np + p);
   const double* Dc = s.dndx_c + (int64_t)c * NV * DIM;
   D Fi[DIM * DIM];
 #pragma unroll
@@ -374,11 +398,13 @@ __global__ void __launch_bounds__(128, MPM_TANGENT_G2P_MIN_BLOCKS) k_g2p_tangent
     D vel[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) vel[d] = ld(s.nf, nt, (int64_t)(NF<DIM>::VEL + d) * nn + nid[i]);
+    D Ni, G[DIM], Dn[DIM];
+    node_shape<DIM>(xi, i, Ni, G);
+    grad_dual<DIM, BOX>(G, ihl, inv, Dn);
 #pragma unroll
     for (int r = 0; r < DIM; ++r)
 #pragma unroll
-      for (int q = 0; q < DIM; ++q) Fi[r * DIM + q] += vel[r] * Dm[i * DIM + q] * dt;
-    const D* Dn = &Dm[i * DIM];
+      for (int q = 0; q < DIM; ++q) Fi[r * DIM + q] += vel[r] * Dn[q] * dt;
     if constexpr (DIM == 2) {
       sr[0] += Dn[0] * vel[0];
       sr[1] += Dn[1] * vel[1];
@@ -431,6 +457,28 @@ __global__ void __launch_bounds__(128, MPM_TANGENT_G2P_MIN_BLOCKS) k_g2p_tangent
   const D rho = pfield<DIM>(s, PF<DIM>::RHO, p) / (1. + dvol);
   set_pfield<DIM>(s, PF<DIM>::VOL, p, vol);
   set_pfield<DIM>(s, PF<DIM>::RHO, p, rho);
+  // F update (independent of the stress; done first so that Fi is not live
+  // through the material update)
+  if constexpr (DIM == 2) {
+    D F[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) F[k] = pfield<DIM>(s, PF<2>::F + k, p);
+    set_pfield<DIM>(s, PF<2>::F + 0, p, Fi[0] * F[0] + Fi[1] * F[2]);
+    set_pfield<DIM>(s, PF<2>::F + 1, p, Fi[0] * F[1] + Fi[1] * F[3]);
+    set_pfield<DIM>(s, PF<2>::F + 2, p, Fi[2] * F[0] + Fi[3] * F[2]);
+    set_pfield<DIM>(s, PF<2>::F + 3, p, Fi[2] * F[1] + Fi[3] * F[3]);
+  } else {
+    D F[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) F[k] = pfield<DIM>(s, PF<3>::F + k, p);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        set_pfield<DIM>(s, PF<3>::F + a * 3 + q, p,
+                        (Fi[a * 3 + 0] * F[0 * 3 + q] + Fi[a * 3 + 1] * F[1 * 3 + q]) +
+                            Fi[a * 3 + 2] * F[2 * 3 + q]);
+  }
   D sig[6];
 #pragma unroll
   for (int k = 0; k < NS; ++k) sig[k] = pfield<DIM>(s, PF<DIM>::S + k, p);
@@ -466,26 +514,71 @@ __global__ void __launch_bounds__(128, MPM_TANGENT_G2P_MIN_BLOCKS) k_g2p_tangent
 #pragma unroll
     for (int k = 0; k < NS; ++k) set_pfield<DIM>(s, PF<DIM>::S + k, p, out[k]);
   }
-  if constexpr (DIM == 2) {
-    D F[4];
+}
+
+template <int DIM, bool FLIP>
+__global__ void __launch_bounds__(128, MPM_TANGENT_KIN_MIN_BLOCKS) k_g2p_tangent(DevState s, double dt, double beta) {
+  constexpr int NV = Elem<DIM>::NV;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.np) return;
+  const int c = s.cell[p];
+  if (c < 0) return;
+  const int64_t nn = s.nn;
+  double* const* nt = s.nft;
+  D x[DIM], xi[DIM], N[NV];
+  int nid[NV];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) F[k] = pfield<DIM>(s, PF<2>::F + k, p);
-    set_pfield<DIM>(s, PF<2>::F + 0, p, Fi[0] * F[0] + Fi[1] * F[2]);
-    set_pfield<DIM>(s, PF<2>::F + 1, p, Fi[0] * F[1] + Fi[1] * F[3]);
-    set_pfield<DIM>(s, PF<2>::F + 2, p, Fi[2] * F[0] + Fi[3] * F[2]);
-    set_pfield<DIM>(s, PF<2>::F + 3, p, Fi[2] * F[1] + Fi[3] * F[3]);
+  for (int d = 0; d < DIM; ++d) x[d] = pfield<DIM>(s, PF<DIM>::X + d, p);
+  xi_dual<DIM>(s.geom[c], x, xi);  // at the step-start position
+  shapefn<DIM>(xi, N);
+  if (s.structured) {
+    grid_cell_nodes<DIM>(s, c, nid);
   } else {
-    D F[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) F[k] = pfield<DIM>(s, PF<3>::F + k, p);
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int q = 0; q < 3; ++q)
-        set_pfield<DIM>(s, PF<3>::F + a * 3 + q, p,
-                        (Fi[a * 3 + 0] * F[0 * 3 + q] + Fi[a * 3 + 1] * F[1 * 3 + q]) +
-                            Fi[a * 3 + 2] * F[2 * 3 + q]);
+    for (int n = 0; n < NV; ++n) nid[n] = s.cell_nodes[(int64_t)c * NV + n];
   }
+  D nvel[DIM], nacc[DIM];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      nvel[d] += N[i] * ld(s.nf, nt, (int64_t)(NF<DIM>::VEL + d) * nn + nid[i]);
+    if constexpr (FLIP) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        nacc[d] += N[i] * ld(s.nf, nt, (int64_t)(NF<DIM>::ACC + d) * nn + nid[i]);
+    }
+  }
+  D v[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) v[d] = pfield<DIM>(s, PF<DIM>::V + d, p);
+  if constexpr (FLIP) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] += nacc[d] * dt;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = beta * v[d] + (1.0 - beta) * nvel[d];
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = nvel[d];
+  }
+  double xn[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const D xd = x[d] + nvel[d] * dt;
+    xn[d] = xd.v;
+    set_pfield<DIM>(s, PF<DIM>::X + d, p, xd);
+    set_pfield<DIM>(s, PF<DIM>::U + d, p, pfield<DIM>(s, PF<DIM>::U + d, p) + nvel[d] * dt);
+  }
+  const int pv = s.pvc[p];
+  if (pv >= 0) {
+    const ParticleVC& r = s.pvcs[pv];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      if (r.mask & (1u << d)) v[d] = D(r.value[d]);
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) set_pfield<DIM>(s, PF<DIM>::V + d, p, v[d]);
+
   // locate on the values
   bool finite = true;
 #pragma unroll
@@ -503,9 +596,9 @@ __global__ void __launch_bounds__(128, MPM_TANGENT_G2P_MIN_BLOCKS) k_g2p_tangent
   }
 }
 
-// the MohrCoulomb returns deferred by k_g2p_tangent (dense, grid-stride)
+// the MohrCoulomb returns deferred by k_stress_tangent (dense, grid-stride)
 template <int DIM>
-__global__ void __launch_bounds__(128) k_mc_return_tangent(DevState s) {
+__global__ void __launch_bounds__(128, MPM_TANGENT_RETURN_MIN_BLOCKS) k_mc_return_tangent(DevState s) {
   const unsigned n = *s.nplastic;
   const int64_t np = s.np;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -546,13 +639,21 @@ void step_tangent(const DevState& s, const StepArgs& a, cudaStream_t st, Profile
   counting_sort(s, st);
   pr.end(K_SORT, st);
   pr.begin(K_P2G, st);
-  k_prep_tangent<DIM><<<nblk(s.np, 128), 128, 0, st>>>(s);
-  k_p2g_tangent<DIM><<<nblk(s.ncells * NV, 128), 128, 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+  if (s.structured)
+    k_p2g_tiles_tangent<DIM, true><<<nblk(s.ncells, tangent_tile_t<true>() / NV),
+                                     tangent_tile_t<true>(), 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
+  else
+    k_p2g_tiles_tangent<DIM, false><<<nblk(s.ncells, tangent_tile_t<false>() / NV),
+                                      tangent_tile_t<false>(), 0, st>>>(s, a.g[0], a.g[1], a.g[2]);
   pr.end(K_P2G, st);
   pr.begin(K_NODES_VEL, st);
   k_nodes_tangent<DIM><<<nblk(s.nn, 128), 128, 0, st>>>(s, a.dt, a.damping);
   pr.end(K_NODES_VEL, st);
-  pr.begin(K_G2P, st);
+  pr.begin(K_G2P, st, 2);
+  if (s.structured)
+    k_stress_tangent<DIM, true><<<nblk(s.np, 128), 128, 0, st>>>(s, a.dt);
+  else
+    k_stress_tangent<DIM, false><<<nblk(s.np, 128), 128, 0, st>>>(s, a.dt);
   if (a.flip)
     k_g2p_tangent<DIM, true><<<nblk(s.np, 128), 128, 0, st>>>(s, a.dt, a.beta);
   else

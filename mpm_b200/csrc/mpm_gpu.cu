@@ -242,7 +242,7 @@ struct mpm_gpu_solver {
   DevBuf<double> d_pft[MAX_TANGENTS], d_svt[MAX_TANGENTS], d_nft[MAX_TANGENTS],
       d_partt[MAX_TANGENTS];
   DevBuf<unsigned char> d_mats_t;
-  DevBuf<double> d_prep, d_prept[MAX_TANGENTS], d_tpbuf;
+  DevBuf<double> d_tpbuf;
 
   // mixed precision: d_pf holds [x, u, pdstrain] in FP64, the rest is FP32
   bool mixed = false;
@@ -752,10 +752,8 @@ void refresh_state(mpm_gpu_t h) {
     s.partt[k] = on ? h->d_partt[k].p : nullptr;
   }
   s.mats_t = h->ntangent > 0 ? h->d_mats_t.p : nullptr;
-  s.prep = h->ntangent > 0 ? h->d_prep.p : nullptr;
   s.tpbuf = h->ntangent > 0 ? h->d_tpbuf.p : nullptr;
   s.tangent_mass_floor = h->tangent_mass_floor;
-  for (int k = 0; k < MAX_TANGENTS; ++k) s.prept[k] = h->ntangent > 0 ? h->d_prept[k].p : nullptr;
   s.any_softening = 0;
   for (auto& m : h->mats) s.any_softening |= (m.type == 1 && m.softening) ? 1 : 0;
   s.plist = h->any_mc ? h->d_plist.p : nullptr;
@@ -1860,11 +1858,8 @@ int mpm_gpu_set_sensitivities(mpm_gpu_t h, int32_t n, const int32_t* material_id
   }
   const int64_t np = h->npad;
   const int nval = 1 + 3 * h->dim;
-  const size_t nprep = (size_t)h->nv * (1 + h->dim) * np;
-  h->d_prep.alloc(nprep);
   if (h->any_mc) h->d_tpbuf.alloc((size_t)7 * (1 + MAX_TANGENTS) * np);
   for (int k = 0; k < MAX_TANGENTS; ++k) {
-    h->d_prept[k].alloc(nprep);
     h->d_pft[k].alloc((size_t)h->nfields() * np);
     h->d_nft[k].alloc((size_t)h->nnf() * h->nnodes);
     h->d_partt[k].alloc((size_t)h->ncells * h->nv * nval);

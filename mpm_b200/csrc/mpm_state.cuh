@@ -155,8 +155,6 @@ struct DevState {
   const void* mats_t = nullptr;              // [materials] MaterialT<Dual>
   double* tpbuf = nullptr;                   // [7][1 + NT][np] deferred-return inputs
   double tangent_mass_floor = 0.0;           // nodes lighter than this carry no tangents
-  double* prep = nullptr;                    // [NV (1 + DIM)][np] N, dN/dx at the step start
-  double* prept[2] = {nullptr, nullptr};
   const MaterialParams* mats = nullptr;
   const NodeBC* bcs = nullptr;
   const ParticleVC* pvcs = nullptr;
