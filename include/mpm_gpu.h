@@ -50,7 +50,15 @@ typedef enum {
 } mpm_status;
 
 enum { MPM_SCHEME_USF = 0, MPM_SCHEME_USL = 1, MPM_SCHEME_MUSL = 2 };
-enum { MPM_VELOCITY_FLIP = 0, MPM_VELOCITY_PIC = 1 };
+/* particle velocity update, in the order of the reference's VelocityUpdate
+ * (data_types.h:50) */
+enum {
+  MPM_VELOCITY_FLIP = 0,
+  MPM_VELOCITY_PIC = 1,
+  MPM_VELOCITY_ASFLIP = 2,
+  MPM_VELOCITY_TPIC = 3,
+  MPM_VELOCITY_APIC = 4
+};
 enum { MPM_PRECISION_FP64 = 0, MPM_PRECISION_MIXED = 1 };
 
 /* Analysis settings (mpm_base.tcc:3-207; mpm_explicit.tcc:8-13, 145-153). */
@@ -58,7 +66,10 @@ typedef struct {
   int32_t dim;              /* 2 (quad4 / ED2Q4) or 3 (hex8 / ED3H8) */
   int32_t scheme;           /* MPM_SCHEME_USF / MPM_SCHEME_USL / MPM_SCHEME_MUSL (FP64;
                                mpm_scheme_musl.tcc:20-35) */
-  int32_t velocity_update;  /* MPM_VELOCITY_FLIP / MPM_VELOCITY_PIC */
+  int32_t velocity_update;  /* MPM_VELOCITY_FLIP / PIC (particle.tcc:1018-1067), or the
+                               affine ASFLIP / APIC and Taylor TPIC updates, which carry a
+                               mapping matrix per particle (particle.tcc:630-721,
+                               1071-1139, 1663-1730; FP64, USF and USL) */
   int32_t precision;        /* MPM_PRECISION_FP64: every quantity in FP64, rounding as the
                                reference's CPU run (the parity mode);
                                MPM_PRECISION_MIXED: FP32 transfers and constitutive update
@@ -96,6 +107,13 @@ typedef struct {
   int32_t* material;
   double* svars;
 } mpm_gpu_particles;
+
+/* The mapping matrix of the ASFLIP / APIC / TPIC velocity updates (the
+ * particle's mapping_matrix_), n*9 row-major: its leading dim x dim block
+ * (zeros elsewhere on read).  MPM_ERR_UNSUPPORTED for FLIP and PIC.  A new
+ * particle starts from zero (particle.tcc:666-669). */
+int mpm_gpu_read_mapping_matrix(mpm_gpu_t h, double* out);
+int mpm_gpu_load_mapping_matrix(mpm_gpu_t h, const double* in);
 
 /* Create a solver on cfg->device. */
 int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out);

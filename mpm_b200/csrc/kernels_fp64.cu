@@ -132,24 +132,75 @@ __global__ void __launch_bounds__(256) k_fill(DevState s) {
 // tensor-product grid, J^-1) in shared memory; then thread (cell, slot) adds
 // its slot's contributions of the cell's particles to 1 + 3 DIM accumulators:
 // few registers per thread, coalesced particle reads, no atomics.
-template <int DIM, int MODE, bool BOX>
+// The matrix M of the mapping velocity v + M r_i of particle p in cell c
+// (position x, local coordinates xi): B D^-1 (AFF 1) with the shape tensor
+// D = sum_i N_i r_i r_i^T, or B (AFF 2).
+template <int DIM, int AFF>
+__device__ __forceinline__ void mapping_velocity_matrix(const DevState& s, int64_t p, int c,
+                                                        const double* x, const double* xi,
+                                                        double* M) {
+  constexpr int NV = Elem<DIM>::NV;
+  double B[DIM * DIM];
+#pragma unroll
+  for (int q = 0; q < DIM * DIM; ++q) B[q] = s.mapb[(int64_t)q * s.np + p];
+  if constexpr (AFF == 2) {
+#pragma unroll
+    for (int q = 0; q < DIM * DIM; ++q) M[q] = B[q];
+  } else {
+    int nid[NV];
+    double X[NV * DIM], N[NV], T[DIM * DIM], Ti[DIM * DIM];
+    cell_nodes_coords<DIM>(s, c, nid, X);
+    shapefn<DIM>(xi, N);
+#pragma unroll
+    for (int q = 0; q < DIM * DIM; ++q) T[q] = 0.;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double r[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) r[d] = X[i * DIM + d] - x[d];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) T[a * DIM + b] += (N[i] * r[a]) * r[b];
+    }
+    inverse<DIM>(T, Ti);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) {
+        double sum = B[a * DIM + 0] * Ti[0 * DIM + b];
+#pragma unroll
+        for (int k = 1; k < DIM; ++k) sum = sum + B[a * DIM + k] * Ti[k * DIM + b];
+        M[a * DIM + b] = sum;
+      }
+  }
+}
+
+// AFF: the mass-momentum mapping velocity of the velocity update
+// (particle.tcc:630-718): 0 the particle velocity (FLIP, PIC); 1 the affine
+// v + B D^-1 r_i (APIC, ASFLIP; D the shape tensor sum_i N_i r_i r_i^T,
+// r_i = x_i - x_p); 2 the Taylor v + B r_i (TPIC).  B is the particle's
+// mapping matrix.
+template <int DIM, int MODE, bool BOX, int AFF>
 struct TileRows {
   static constexpr bool MM = MODE != 1, FORCES = MODE != 0;
   static constexpr int XI = 0, M = DIM, V = DIM + 1;
   static constexpr int SC = V + (MM ? DIM : 0);  // -volume
   static constexpr int S = SC + 1;
   static constexpr int INV = S + (FORCES ? PF<DIM>::NS : 0);
-  static constexpr int N = INV + (FORCES && !BOX ? DIM * DIM : 0);
+  static constexpr int XP = INV + (FORCES && !BOX ? DIM * DIM : 0);  // particle position
+  static constexpr int MV = XP + (MM && AFF ? DIM : 0);              // velocity map matrix
+  static constexpr int N = MV + (MM && AFF ? DIM * DIM : 0);
 };
 
-template <int DIM, int MODE, bool BOX>
-__global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_P2G_TILE_MIN_BLOCKS)
+template <int DIM, int MODE, bool BOX, int AFF>
+__global__ void __launch_bounds__(p2g_tile_t<BOX, AFF>(), MPM_P2G_TILE_MIN_BLOCKS)
     k_p2g_tiles(DevState s, double g0, double g1, double g2) {
   constexpr int NV = Elem<DIM>::NV;
-  constexpr int T = p2g_tile_t<BOX>();
+  constexpr int T = p2g_tile_t<BOX, AFF>();
   constexpr int CB = T / NV;
   constexpr int NVAL = PV<DIM>::N;
-  using RW = TileRows<DIM, MODE, BOX>;
+  using RW = TileRows<DIM, MODE, BOX, AFF>;
   constexpr bool MM = RW::MM, FORCES = RW::FORCES;
   __shared__ double rows[RW::N][T];
   const int t = threadIdx.x;
@@ -170,6 +221,14 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_P2G_TILE_MIN_BLOCKS)
   if constexpr (BOX && FORCES) {
     if (a1 > a0) box_map = cell_map<DIM, true, double>(s, (int)c, nullptr, nullptr);
   }
+  double xk[DIM];  // this slot's node, for the branch vectors of the mapping velocity
+  if constexpr (MM && AFF) {
+    int nid[NV];
+    double X[NV * DIM];
+    if (a1 > a0) cell_nodes_coords<DIM>(s, (int)c, nid, X);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xk[d] = a1 > a0 ? X[k * DIM + d] : 0.;
+  }
   const int64_t np = s.np;
   const double gv[3] = {g0, g1, g2};
   double acc[NVAL];
@@ -186,6 +245,14 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_P2G_TILE_MIN_BLOCKS)
       local_xi<DIM>(x, g.centroid, g.len, xi);
 #pragma unroll
       for (int d = 0; d < DIM; ++d) rows[RW::XI + d][t] = xi[d];
+      if constexpr (MM && AFF) {
+        double Mv[DIM * DIM];
+        mapping_velocity_matrix<DIM, AFF>(s, p, pc, x, xi, Mv);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) rows[RW::XP + d][t] = x[d];
+#pragma unroll
+        for (int q = 0; q < DIM * DIM; ++q) rows[RW::MV + q][t] = Mv[q];
+      }
       rows[RW::M][t] = s.pf[(int64_t)PF<DIM>::MASS * np + p];
       if constexpr (MM) {
 #pragma unroll
@@ -218,8 +285,23 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_P2G_TILE_MIN_BLOCKS)
       if constexpr (MM) {
         const double mN = m * N;
         acc[PV<DIM>::MASS] += mN;
+        double mv[DIM];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) acc[PV<DIM>::MOM + d] += mN * rows[RW::V + d][r];
+        for (int d = 0; d < DIM; ++d) mv[d] = rows[RW::V + d][r];
+        if constexpr (AFF) {
+          double br[DIM];
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) br[d] = xk[d] - rows[RW::XP + d][r];
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) {
+            double sum = rows[RW::MV + a * DIM + 0][r] * br[0];
+#pragma unroll
+            for (int b = 1; b < DIM; ++b) sum = sum + rows[RW::MV + a * DIM + b][r] * br[b];
+            mv[a] += sum;
+          }
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) acc[PV<DIM>::MOM + d] += mN * mv[d];
       }
       if constexpr (FORCES) {
         const double sc = rows[RW::SC][r];
@@ -574,10 +656,12 @@ __global__ void __launch_bounds__(128) k_stress(DevState s, double dt) {
 // --------------------------------------------------------------------- G2P
 // particle.tcc:994-1067 FLIP / PIC; mesh.tcc:1454-1467 particle velocity
 // constraints; USL stress update (mpm_scheme_usl.tcc:14-17); locate.
-template <int DIM, bool STRESS, bool FLIP, bool BOX>
+template <int DIM, bool STRESS, int VU, bool BOX>
 __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, double dt,
                                                                  double beta) {
   constexpr int NV = Elem<DIM>::NV;
+  constexpr bool FLIP = VU == 0, ASFLIP = VU == 2, TPIC = VU == 3;  // 1 PIC, 4 APIC
+  constexpr bool ACC = FLIP || ASFLIP;  // nodal acceleration interpolated
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= s.np) return;
   const int c = s.cell[p];
@@ -589,7 +673,10 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
   const CellGeom& g = s.geom[c];
   local_xi<DIM>(x, g.centroid, g.len, xi);
   shapefn<DIM>(xi, N);
-  cell_nodes_for<DIM, BOX>(s, c, nid, X);
+  if constexpr (VU >= 2)
+    cell_nodes_coords<DIM>(s, c, nid, X);  // the branch vectors need the nodes
+  else
+    cell_nodes_for<DIM, BOX>(s, c, nid, X);
   double nvel[DIM], nacc[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.;
@@ -598,9 +685,82 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
     const int n = nid[i];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + n];
-    if constexpr (FLIP) {
+    if constexpr (ACC) {
 #pragma unroll
       for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * s.nf[(int64_t)(NF<DIM>::ACC + d) * nn + n];
+    }
+  }
+  double sep[DIM];  // the velocity that moves the particle
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) sep[d] = nvel[d];
+  if constexpr (VU >= 2) {
+    // mapping matrix at the step-start position (particle.tcc:1663-1704):
+    // affine B = sum_i N_i v_i r_i^T (APIC, ASFLIP) or the velocity
+    // gradient sum_i v_i dN_i/dx^T (TPIC); entries below 1e-15 set to 0
+    double B[DIM * DIM], D[NV * DIM];
+#pragma unroll
+    for (int q = 0; q < DIM * DIM; ++q) B[q] = 0.;
+    if constexpr (TPIC || ASFLIP) dn_dx_all<DIM, BOX>(s, c, xi, X, D);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double vel[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) vel[d] = s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + nid[i]];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) {
+          if constexpr (TPIC)
+            B[a * DIM + b] += vel[a] * D[i * DIM + b];
+          else
+            B[a * DIM + b] += (N[i] * vel[a]) * (X[i * DIM + b] - x[b]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < DIM * DIM; ++q) {
+      if (fabs(B[q]) < 1.E-15) B[q] = 0.;
+      s.mapb[(int64_t)q * np + p] = B[q];
+    }
+    if constexpr (ASFLIP) {
+      // beta (particle.tcc:1711-1730): 0 next to a velocity-constrained node
+      // or when the deformation gradient increment compresses
+      double bp = 1.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        const int bci = s.bc_index[nid[i]];
+        if (bci >= 0 && s.bcs[bci].vel_mask != 0) bp = 0.0;
+      }
+      double Fi[9] = {1., 0., 0., 0., 1., 0., 0., 0., 1.};
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          const double va = s.nf[(int64_t)(NF<DIM>::VEL + a) * nn + nid[i]];
+#pragma unroll
+          for (int b = 0; b < DIM; ++b) Fi[a * 3 + b] += va * D[i * DIM + b] * dt;
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) {
+          if (a != b && fabs(Fi[a * 3 + b]) < 1.E-15) Fi[a * 3 + b] = 0.;
+          if (a == b && fabs(Fi[a * 3 + b] - 1.) < 1.E-15) Fi[a * 3 + b] = 1.;
+        }
+      const double J = Fi[0] * (Fi[4] * Fi[8] - Fi[5] * Fi[7]) -
+                       Fi[1] * (Fi[3] * Fi[8] - Fi[5] * Fi[6]) +
+                       Fi[2] * (Fi[3] * Fi[7] - Fi[4] * Fi[6]);
+      if (J < 1.0) bp = 0.0;
+      // particle.tcc:1096-1110: FLIP/PIC blend for the velocity, the
+      // separable blend for the position
+      double flip[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        flip[d] = s.pf[(int64_t)(PF<DIM>::V + d) * np + p] + nacc[d] * dt;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) nacc[d] = flip[d];  // keeps the FLIP velocity
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) sep[d] = bp * beta * flip[d] + (1.0 - bp * beta) * nvel[d];
     }
   }
   double v[DIM];
@@ -611,6 +771,9 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
     for (int d = 0; d < DIM; ++d) v[d] += nacc[d] * dt;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) v[d] = beta * v[d] + (1.0 - beta) * nvel[d];
+  } else if constexpr (ASFLIP) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = beta * nacc[d] + (1.0 - beta) * nvel[d];
   } else {
 #pragma unroll
     for (int d = 0; d < DIM; ++d) v[d] = nvel[d];
@@ -618,9 +781,9 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
   double xn[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    xn[d] = x[d] + nvel[d] * dt;
+    xn[d] = x[d] + sep[d] * dt;
     s.pf[(int64_t)(PF<DIM>::X + d) * np + p] = xn[d];
-    s.pf[(int64_t)(PF<DIM>::U + d) * np + p] += nvel[d] * dt;
+    s.pf[(int64_t)(PF<DIM>::U + d) * np + p] += sep[d] * dt;
   }
   const int pv = s.pvc[p];
   if (pv >= 0) {
@@ -658,7 +821,7 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
 // material, velocity-constraint slot) and phase B (stress, strain, F,
 // volume, density, MohrCoulomb state).  The threads gather nodal values while
 // phase B is in flight, update the staged rows in place and one thread stores
-// the rows back with bulk copies.  The arithmetic is k_g2p<DIM, true, FLIP, BOX>'s.
+// the rows back with bulk copies.  The arithmetic is k_g2p<DIM, true, FLIP ? 0 : 1, BOX>'s.
 static_assert(STAGE_T == PAD_PARTICLES, "staged slices are whole padded blocks");
 template <int DIM>
 constexpr int staged_rows() { return PF<DIM>::MASS; }  // fields X .. RHO
@@ -1016,9 +1179,29 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
   };
   auto p2g = [&](auto mode) {
     constexpr int MODE = decltype(mode)::value;
-    constexpr int TT = p2g_tile_t<BOX>();
-    k_p2g_tiles<DIM, MODE, BOX><<<nblocks(s.ncells, TT / Elem<DIM>::NV), TT, 0, st>>>(
-        s, a.g[0], a.g[1], a.g[2]);
+    auto launch = [&](auto aff) {
+      constexpr int AFF = decltype(aff)::value;
+      constexpr int TT = p2g_tile_t<BOX, AFF>();
+      k_p2g_tiles<DIM, MODE, BOX, AFF><<<nblocks(s.ncells, TT / Elem<DIM>::NV), TT, 0, st>>>(
+          s, a.g[0], a.g[1], a.g[2]);
+    };
+    if constexpr (MODE != 1) {  // the mass-momentum mapping velocity
+      if (a.vupd == 2 || a.vupd == 4) return launch(std::integral_constant<int, 1>{});
+      if (a.vupd == 3) return launch(std::integral_constant<int, 2>{});
+    }
+    launch(std::integral_constant<int, 0>{});
+  };
+  // unstaged G2P (USF kinematics, or USL with its stress update) for the
+  // velocity update of the run
+  auto g2p = [&](auto stress) {
+    constexpr bool STRESS = decltype(stress)::value;
+    switch (a.vupd) {
+      case 0: k_g2p<DIM, STRESS, 0, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta); break;
+      case 1: k_g2p<DIM, STRESS, 1, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta); break;
+      case 2: k_g2p<DIM, STRESS, 2, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta); break;
+      case 3: k_g2p<DIM, STRESS, 3, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta); break;
+      default: k_g2p<DIM, STRESS, 4, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta); break;
+    }
   };
   pr.begin(K_SORT, st, SORT_KERNELS);
   counting_sort_impl(s, st);
@@ -1060,7 +1243,9 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
     const size_t sm = staged_smem_bytes<DIM>(s.sv != nullptr);
-    if (a.flip) {
+    if (a.vupd >= 2) {  // the mapping-matrix updates: G2P and stress unstaged
+      g2p(std::true_type{});
+    } else if (a.flip) {
       prefer_shared_memory<k_g2p_staged<DIM, true, BOX>>();
       k_g2p_staged<DIM, true, BOX><<<pb128, STAGE_T, sm, st>>>(s, a.dt, a.beta);
     } else {
@@ -1087,10 +1272,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     k_nodes<DIM, 2><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_G2P, st);
-    if (a.flip)
-      k_g2p<DIM, false, true, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
-    else
-      k_g2p<DIM, false, false, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta);
+    g2p(std::false_type{});
     pr.end(K_G2P, st);
   }
   pr.begin(K_LOCATE, st);

@@ -223,9 +223,10 @@ __device__ __forceinline__ void dn_dx_node(const double* xi, const Map& map, int
 
 // ------------------------------------------------------------ P2G cell tiles
 // Threads per tile: 256 on a tensor-product grid; 128 on a general mesh,
-// whose staged rows add J^-1 and whose threads need more registers.
-template <bool BOX>
-constexpr int p2g_tile_t() { return BOX ? 256 : 128; }
+// whose staged rows add J^-1 and whose threads need more registers, and with
+// an affine or Taylor mapping velocity (AFF), whose rows add the matrix.
+template <bool BOX, int AFF = 0>
+constexpr int p2g_tile_t() { return BOX && !AFF ? 256 : 128; }
 
 // Particle ids of one cell in ascending order (the fill order is not
 // deterministic), by the cell's NV threads of a block (k = 0 .. NV - 1):

@@ -191,7 +191,7 @@ struct mpm_gpu_solver {
 
   // device
   DevState ds;
-  DevBuf<double> d_pf, d_sv, d_nf, d_ncoord, d_xnext;
+  DevBuf<double> d_pf, d_sv, d_nf, d_ncoord, d_xnext, d_mapb;
   DevBuf<int32_t> d_cell, d_bc_index, d_cell_nodes, d_nb_off, d_nb, d_bin_off, d_bin_cells, d_lost;
   DevBuf<uint16_t> d_mat;
   DevBuf<uint8_t> d_active;
@@ -679,6 +679,11 @@ void allocate_particles(mpm_gpu_t h) {
   h->d_cell.alloc(np);
   h->d_mat.alloc(np);
   if (h->cfg.scheme == MPM_SCHEME_MUSL) h->d_xnext.alloc((size_t)h->dim * np);
+  if (h->cfg.velocity_update >= MPM_VELOCITY_ASFLIP) {
+    h->d_mapb.alloc((size_t)h->dim * h->dim * np);
+    ck(cudaMemsetAsync(h->d_mapb.p, 0, sizeof(double) * h->dim * h->dim * np, h->stream),
+       "memset");
+  }
   h->d_lost.alloc(std::max<int64_t>(1, np));
   h->d_rank.alloc(std::max<int64_t>(1, np));
   h->d_order.alloc(std::max<int64_t>(1, np));
@@ -703,6 +708,7 @@ void refresh_state(mpm_gpu_t h) {
   s.np = h->npad;
   s.pf = h->d_pf.p;
   s.sv = h->d_sv.p;
+  s.mapb = h->d_mapb.p;
   s.cell = h->d_cell.p;
   s.mat = h->d_mat.p;
   s.pvc = h->d_pvc.p;
@@ -988,7 +994,12 @@ int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out) {
     return MPM_ERR_UNSUPPORTED;
   if (cfg->scheme == MPM_SCHEME_MUSL && cfg->precision != MPM_PRECISION_FP64)
     return MPM_ERR_UNSUPPORTED;
-  if (cfg->velocity_update != MPM_VELOCITY_FLIP && cfg->velocity_update != MPM_VELOCITY_PIC)
+  if (cfg->velocity_update < MPM_VELOCITY_FLIP || cfg->velocity_update > MPM_VELOCITY_APIC)
+    return MPM_ERR_UNSUPPORTED;
+  // the mapping-matrix updates run on the FP64 USF / USL path (MUSL's second
+  // mapping would take its branch vectors from the updated positions)
+  if (cfg->velocity_update >= MPM_VELOCITY_ASFLIP &&
+      (cfg->precision != MPM_PRECISION_FP64 || cfg->scheme == MPM_SCHEME_MUSL))
     return MPM_ERR_UNSUPPORTED;
   if (cfg->precision != MPM_PRECISION_FP64 && cfg->precision != MPM_PRECISION_MIXED)
     return MPM_ERR_UNSUPPORTED;
@@ -1346,7 +1357,7 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
 }
 
 static bool same_step(const DevState& a, const DevState& b, const StepArgs& x, const StepArgs& y) {
-  return std::memcmp(&a, &b, sizeof(DevState)) == 0 && x.scheme == y.scheme && x.flip == y.flip &&
+  return std::memcmp(&a, &b, sizeof(DevState)) == 0 && x.scheme == y.scheme && x.flip == y.flip && x.vupd == y.vupd &&
          x.remove_lost == y.remove_lost && x.dt == y.dt && x.beta == y.beta &&
          x.damping == y.damping && x.g[0] == y.g[0] && x.g[1] == y.g[1] && x.g[2] == y.g[2];
 }
@@ -1360,6 +1371,7 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
   StepArgs a{};
   a.scheme = h->cfg.scheme;
   a.flip = h->cfg.velocity_update == MPM_VELOCITY_FLIP ? 1 : 0;
+  a.vupd = h->cfg.velocity_update;
   a.remove_lost = h->cfg.locate_particles ? 0 : 1;
   a.dt = h->cfg.dt;
   a.beta = h->cfg.blending_ratio;
@@ -1473,6 +1485,45 @@ int64_t mpm_gpu_launch_count(mpm_gpu_t h) { return h ? h->prof.launches : -1; }
 
 int64_t mpm_gpu_nparticles(mpm_gpu_t h) { return h ? h->np : -1; }
 int64_t mpm_gpu_current_step(mpm_gpu_t h) { return h ? h->step : -1; }
+
+int mpm_gpu_read_mapping_matrix(mpm_gpu_t h, double* out) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("no particles");
+  if (!out) throw InvalidArg("null output");
+  if (h->cfg.velocity_update < MPM_VELOCITY_ASFLIP)
+    return fail(h, MPM_ERR_UNSUPPORTED, "no mapping matrix: FLIP and PIC carry none");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const int dim = h->dim;
+  const int64_t np = h->np, ns = h->npad;
+  std::vector<double> b((size_t)dim * dim * ns);
+  h->d_mapb.download(b.data(), b.size(), h->stream);
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  for (int64_t p = 0; p < np; ++p)
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c)
+        out[p * 9 + a * 3 + c] = (a < dim && c < dim) ? b[(size_t)(a * dim + c) * ns + p] : 0.;
+  return MPM_OK;
+  MPM_END(h)
+}
+
+int mpm_gpu_load_mapping_matrix(mpm_gpu_t h, const double* in) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("no particles");
+  if (!in) throw InvalidArg("null input");
+  if (h->cfg.velocity_update < MPM_VELOCITY_ASFLIP)
+    return fail(h, MPM_ERR_UNSUPPORTED, "no mapping matrix: FLIP and PIC carry none");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const int dim = h->dim;
+  const int64_t np = h->np, ns = h->npad;
+  std::vector<double> b((size_t)dim * dim * ns, 0.0);
+  for (int64_t p = 0; p < np; ++p)
+    for (int a = 0; a < dim; ++a)
+      for (int c = 0; c < dim; ++c) b[(size_t)(a * dim + c) * ns + p] = in[p * 9 + a * 3 + c];
+  h->d_mapb.upload(b.data(), b.size(), h->stream);
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  return MPM_OK;
+  MPM_END(h)
+}
 
 int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   MPM_GUARD(h)
@@ -1841,6 +1892,8 @@ int mpm_gpu_set_sensitivities(mpm_gpu_t h, int32_t n, const int32_t* material_id
   if (n > 0 && h->mixed) return fail(h, MPM_ERR_UNSUPPORTED, "sensitivities run in FP64 only");
   if (n > 0 && h->cfg.scheme != MPM_SCHEME_USL)
     return fail(h, MPM_ERR_UNSUPPORTED, "sensitivities follow the USL scheme only");
+  if (n > 0 && h->cfg.velocity_update >= MPM_VELOCITY_ASFLIP)
+    return fail(h, MPM_ERR_UNSUPPORTED, "sensitivities follow the FLIP and PIC updates only");
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
   std::vector<TangentParam> params(n);
   for (int k = 0; k < n; ++k) {

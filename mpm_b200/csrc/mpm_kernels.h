@@ -13,6 +13,7 @@ namespace mpm_b200 {
 struct StepArgs {
   int scheme;        // 0 USF, 1 USL
   int flip;          // 1 FLIP, 0 PIC
+  int vupd;          // MPM_VELOCITY_*: 0 FLIP, 1 PIC, 2 ASFLIP, 3 TPIC, 4 APIC
   int remove_lost;   // locate_particles false: unlocatable particles removed
   double dt;
   double beta;       // FLIP/PIC blending ratio

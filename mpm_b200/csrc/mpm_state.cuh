@@ -108,6 +108,7 @@ struct DevState {
   int32_t gcells[3] = {1, 1, 1};     // cells per axis
   const double* axis[3] = {nullptr, nullptr, nullptr};  // node coordinates per axis
   const double* axis_ihl[3] = {nullptr, nullptr, nullptr};  // 2 / cell length per axis interval
+  double* mapb = nullptr;  // [DIM * DIM][np] mapping matrix (ASFLIP, TPIC, APIC), row-major
 
   // general meshes: cells around each node, ascending cell id, with the
   // node's local index (slot) in that cell

@@ -370,7 +370,17 @@ int main(int argc, char** argv) {
   mpm_gpu_config cfg{};
   cfg.dim = in.dim;
   cfg.scheme = in.scheme == "usl" ? MPM_SCHEME_USL : (in.scheme == "musl" ? MPM_SCHEME_MUSL : MPM_SCHEME_USF);
-  cfg.velocity_update = in.vupdate == "pic" ? MPM_VELOCITY_PIC : MPM_VELOCITY_FLIP;
+  // mpm_base.tcc: velocity_update "flip", "pic", "asflip", "tpic", "apic"
+  if (in.vupdate == "pic")
+    cfg.velocity_update = MPM_VELOCITY_PIC;
+  else if (in.vupdate == "asflip")
+    cfg.velocity_update = MPM_VELOCITY_ASFLIP;
+  else if (in.vupdate == "tpic")
+    cfg.velocity_update = MPM_VELOCITY_TPIC;
+  else if (in.vupdate == "apic")
+    cfg.velocity_update = MPM_VELOCITY_APIC;
+  else
+    cfg.velocity_update = MPM_VELOCITY_FLIP;
   cfg.precision = precision == "mixed" ? MPM_PRECISION_MIXED : MPM_PRECISION_FP64;
   cfg.blending_ratio = in.beta;
   cfg.dt = in.dt;

@@ -15,7 +15,9 @@ from . import _native
 from ._native import MPMError
 
 SCHEMES = {"usf": 0, "usl": 1, "musl": 2}
-VELOCITY_UPDATES = {"flip": 0, "pic": 1}
+# the reference's VelocityUpdate order (data_types.h:50); asflip, tpic and apic
+# carry a mapping matrix per particle (``read()["mapping"]``)
+VELOCITY_UPDATES = {"flip": 0, "pic": 1, "asflip": 2, "tpic": 3, "apic": 4}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 
 
@@ -42,6 +44,7 @@ class Solver:
         cfg.dim = dim
         cfg.scheme = SCHEMES[scheme]
         cfg.velocity_update = VELOCITY_UPDATES[velocity_update]
+        self.mapped = cfg.velocity_update >= VELOCITY_UPDATES["asflip"]
         cfg.precision = PRECISIONS[precision]
         cfg.blending_ratio = blending_ratio
         cfg.dt = dt
@@ -181,6 +184,9 @@ class Solver:
         self._ck(self.L.mpm_gpu_read_particles(self.h, C.byref(P)))
         for k in ("x", "u", "v"):
             out[k] = out[k][:, :self.dim]
+        if self.mapped:
+            out["mapping"] = np.zeros((n, 9))
+            self._ck(self.L.mpm_gpu_read_mapping_matrix(self.h, _dp(out["mapping"])))
         return out
 
     def load(self, state):
@@ -203,6 +209,9 @@ class Solver:
         keep["material"] = np.ascontiguousarray(state["material"], dtype=np.int32)
         P.material = _i32p(keep["material"])
         self._ck(self.L.mpm_gpu_load_particles(self.h, n, C.byref(P)))
+        if self.mapped and "mapping" in state:
+            keep["mapping"] = np.ascontiguousarray(state["mapping"], dtype=np.float64)
+            self._ck(self.L.mpm_gpu_load_mapping_matrix(self.h, _dp(keep["mapping"])))
 
     def write_pod(self, dtype=None):
         """PODParticle records of the particles in the mesh (particle.tcc:180-306),

@@ -687,6 +687,7 @@ struct Particle {
   double sv[9];
   int status;
   std::vector<std::pair<unsigned, double>> pvc;  // particle velocity constraints
+  double B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};      // mapping matrix (row-major dim x dim)
 };
 
 struct Oracle {
@@ -1144,7 +1145,37 @@ void phase_initialise(Oracle& o) {
   for (int64_t p = 0; p < np; ++p) particle_compute_shapefn(o, o.particles[p]);
 }
 
-// particle.tcc:630-657 map_mass_momentum_to_nodes
+// The matrix M of the affine (APIC, ASFLIP: B D^-1 with the shape tensor
+// D = sum_i N_i r_i r_i^T, r_i = x_i - x_p; particle.tcc:661-694) or Taylor
+// (TPIC: B; :697-718) mapping velocity v + M r_i.  False for FLIP / PIC.
+bool mapping_velocity_matrix(const Oracle& o, const Particle& P, double* M) {
+  const int dim = o.dim, vu = o.cfg.velocity_update;
+  if (vu != 2 && vu != 3 && vu != 4) return false;
+  if (vu == 3) {
+    for (int i = 0; i < dim * dim; ++i) M[i] = P.B[i];
+    return true;
+  }
+  const Cell& c = o.cells[P.cell];
+  double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < o.nv; ++i) {
+    const double* X = o.nodes[c.nodes[i]].coord;
+    double r[3];
+    for (int d = 0; d < dim; ++d) r[d] = X[d] - P.x[d];
+    for (int a = 0; a < dim; ++a)
+      for (int b = 0; b < dim; ++b) T[a * dim + b] += (P.N[i] * r[a]) * r[b];
+  }
+  double Ti[9];
+  inverse(dim, T, Ti);
+  for (int a = 0; a < dim; ++a)
+    for (int b = 0; b < dim; ++b) {
+      double s = P.B[a * dim + 0] * Ti[0 * dim + b];
+      for (int k = 1; k < dim; ++k) s = s + P.B[a * dim + k] * Ti[k * dim + b];
+      M[a * dim + b] = s;
+    }
+  return true;
+}
+
+// particle.tcc:630-718 map_mass_momentum_to_nodes (plain, affine, Taylor)
 void phase_p2g_mass_momentum(Oracle& o) {
   const int dim = o.dim;
   const bool thr = o.cfg.nthreads > 1;
@@ -1153,11 +1184,24 @@ void phase_p2g_mass_momentum(Oracle& o) {
   for (int64_t p = 0; p < np; ++p) {
     Particle& P = o.particles[p];
     const Cell& c = o.cells[P.cell];
+    double M[9];
+    const bool mapped = mapping_velocity_matrix(o, P, M);
     for (int i = 0; i < o.nv; ++i) {
       Node& n = o.nodes[c.nodes[i]];
       const double mN = P.mass * P.N[i];
+      double mv[3];
+      for (int d = 0; d < dim; ++d) mv[d] = P.v[d];
+      if (mapped) {
+        double r[3];
+        for (int d = 0; d < dim; ++d) r[d] = n.coord[d] - P.x[d];
+        for (int a = 0; a < dim; ++a) {
+          double s = M[a * dim + 0] * r[0];
+          for (int b = 1; b < dim; ++b) s = s + M[a * dim + b] * r[b];
+          mv[a] += s;
+        }
+      }
       double mom[3];
-      for (int d = 0; d < dim; ++d) mom[d] = mN * P.v[d];
+      for (int d = 0; d < dim; ++d) mom[d] = mN * mv[d];
       node_add(n, &n.mass, &mN, 1, thr);
       node_add(n, n.mom, mom, dim, thr);
     }
@@ -1228,9 +1272,30 @@ void phase_node_update(Oracle& o, double dt) {
       node_compute_acceleration_velocity_cundall(o, o.nodes[i], dt, o.cfg.damping_factor);
 }
 
-// particle.tcc:1018-1067 FLIP / PIC, mesh.tcc:1454-1467 velocity constraints
+// |B_ij| < 1e-15 set to 0 (particle.tcc:1671-1676, 1700-1704)
+void clean_small(int dim, double* B) {
+  for (int i = 0; i < dim * dim; ++i)
+    if (std::fabs(B[i]) < 1.E-15) B[i] = 0.;
+}
+
+// particle.tcc:1711-1730 ASFLIP beta: 0 next to a velocity-constrained node
+// or when the deformation gradient increment compresses (det < 1)
+double asflip_beta(const Oracle& o, const Particle& P, double dt) {
+  const Cell& c = o.cells[P.cell];
+  for (int i = 0; i < o.nv; ++i)
+    if (!o.nodes[c.nodes[i]].vel_c.empty()) return 0.0;
+  Particle Q = P;
+  update_deformation_gradient_increment(o, Q, dt);
+  const double* F = Q.Finc;
+  const double J = F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
+                   F[2] * (F[3] * F[7] - F[4] * F[6]);
+  return J < 1.0 ? 0.0 : 1.0;
+}
+
+// particle.tcc:994-1139 FLIP / PIC / ASFLIP / APIC / TPIC position and
+// velocity update, mesh.tcc:1454-1467 velocity constraints
 void phase_g2p(Oracle& o, double dt) {
-  const int dim = o.dim;
+  const int dim = o.dim, vu = o.cfg.velocity_update;
   const int64_t np = (int64_t)o.particles.size();
   const double beta = o.cfg.blending_ratio;
 #pragma omp parallel for schedule(static) if (o.cfg.nthreads > 1)
@@ -1238,20 +1303,51 @@ void phase_g2p(Oracle& o, double dt) {
     Particle& P = o.particles[p];
     const Cell& c = o.cells[P.cell];
     double nvel[3] = {0, 0, 0}, nacc[3] = {0, 0, 0};
+    const bool with_acc = vu == 0 || vu == 2;
     for (int i = 0; i < o.nv; ++i) {
       const Node& n = o.nodes[c.nodes[i]];
       for (int d = 0; d < dim; ++d) nvel[d] += P.N[i] * n.vel[d];
-      if (o.cfg.velocity_update == 0)
+      if (with_acc)
         for (int d = 0; d < dim; ++d) nacc[d] += P.N[i] * n.acc[d];
     }
-    if (o.cfg.velocity_update == 0) {
-      for (int d = 0; d < dim; ++d) P.v[d] += nacc[d] * dt;
-      for (int d = 0; d < dim; ++d) P.v[d] = beta * P.v[d] + (1.0 - beta) * nvel[d];
-    } else {
-      for (int d = 0; d < dim; ++d) P.v[d] = nvel[d];
+    if (vu == 2 || vu == 4) {  // compute_affine_mapping_matrix, at the step-start position
+      double B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int i = 0; i < o.nv; ++i) {
+        const Node& n = o.nodes[c.nodes[i]];
+        for (int a = 0; a < dim; ++a)
+          for (int b = 0; b < dim; ++b) B[a * dim + b] += (P.N[i] * n.vel[a]) * (n.coord[b] - P.x[b]);
+      }
+      clean_small(dim, B);
+      for (int i = 0; i < 9; ++i) P.B[i] = B[i];
     }
-    for (int d = 0; d < dim; ++d) P.x[d] += nvel[d] * dt;
-    for (int d = 0; d < dim; ++d) P.u[d] += nvel[d] * dt;
+    if (vu == 3) {  // compute_velocity_gradient
+      double B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int i = 0; i < o.nv; ++i) {
+        const Node& n = o.nodes[c.nodes[i]];
+        for (int a = 0; a < dim; ++a)
+          for (int b = 0; b < dim; ++b) B[a * dim + b] += n.vel[a] * P.dndx[i * dim + b];
+      }
+      clean_small(dim, B);
+      for (int i = 0; i < 9; ++i) P.B[i] = B[i];
+    }
+    if (vu == 2) {
+      const double bp = asflip_beta(o, P, dt);
+      double flip[3], sep[3];
+      for (int d = 0; d < dim; ++d) flip[d] = P.v[d] + nacc[d] * dt;
+      for (int d = 0; d < dim; ++d) P.v[d] = beta * flip[d] + (1.0 - beta) * nvel[d];
+      for (int d = 0; d < dim; ++d) sep[d] = bp * beta * flip[d] + (1.0 - bp * beta) * nvel[d];
+      for (int d = 0; d < dim; ++d) P.x[d] += sep[d] * dt;
+      for (int d = 0; d < dim; ++d) P.u[d] += sep[d] * dt;
+    } else {
+      if (vu == 0) {
+        for (int d = 0; d < dim; ++d) P.v[d] += nacc[d] * dt;
+        for (int d = 0; d < dim; ++d) P.v[d] = beta * P.v[d] + (1.0 - beta) * nvel[d];
+      } else {
+        for (int d = 0; d < dim; ++d) P.v[d] = nvel[d];
+      }
+      for (int d = 0; d < dim; ++d) P.x[d] += nvel[d] * dt;
+      for (int d = 0; d < dim; ++d) P.u[d] += nvel[d] * dt;
+    }
     for (const auto& pc : P.pvc) P.v[pc.first] = pc.second;
   }
 }
@@ -1498,6 +1594,9 @@ int mpmo_set_particles(void* h, const mpmo_particles* in) {
     if (in->density) P.rho = in->density[p];
     if (in->svars)
       for (int i = 0; i < 9; ++i) P.sv[i] = in->svars[p * 9 + i];
+    if (in->mapping)
+      for (int a = 0; a < dim; ++a)
+        for (int b = 0; b < dim; ++b) P.B[a * dim + b] = in->mapping[p * 9 + a * 3 + b];
     if (in->cell) P.cell = in->cell[p];
     if (P.cell != kNone) o.cells[P.cell].particles.push_back(P.id);
   }
@@ -1534,6 +1633,10 @@ int mpmo_get_particles(void* h, mpmo_particles* out) {
     if (out->svars)
       for (int i = 0; i < 9; ++i) out->svars[p * 9 + i] = P.sv[i];
     if (out->status) out->status[p] = P.status;
+    if (out->mapping)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+          out->mapping[p * 9 + a * 3 + b] = (a < o.dim && b < o.dim) ? P.B[a * o.dim + b] : 0.;
   }
   return 0;
 }

@@ -28,7 +28,8 @@ extern "C" {
 typedef struct {
   int32_t dim;              /* 2 or 3 */
   int32_t scheme;           /* 0 = USF, 1 = USL, 2 = MUSL */
-  int32_t velocity_update;  /* 0 = FLIP, 1 = PIC */
+  int32_t velocity_update;  /* 0 = FLIP, 1 = PIC, 2 = ASFLIP, 3 = TPIC, 4 = APIC
+                               (data_types.h:50 VelocityUpdate order) */
   int32_t locate_particles; /* 1: unlocatable particle is an error, 0: removed */
   double blending_ratio;
   double dt;
@@ -62,6 +63,8 @@ typedef struct {
   int32_t* material;
   double* svars;
   int32_t* status;
+  double* mapping; /* n*9 row-major mapping matrix (affine / Taylor updates;
+                      the leading dim x dim block) */
 } mpmo_particles;
 
 void* mpmo_create(const mpmo_config* cfg);

@@ -36,12 +36,17 @@ class Config(C.Structure):
                 ("pad_", C.c_int32)]
 
 
+# velocity_update names -> the reference's VelocityUpdate order (data_types.h:50)
+VELOCITY_UPDATES = {"flip": 0, "pic": 1, "asflip": 2, "tpic": 3, "apic": 4}
+
+
 class Particles(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_double)) for n in (
         "x", "u", "v", "a", "stress", "strain", "dstrain", "strain_rate", "F",
         "volume", "mass", "density", "xi")] + [
         ("cell", C.POINTER(C.c_int64)), ("material", C.POINTER(C.c_int32)),
-        ("svars", C.POINTER(C.c_double)), ("status", C.POINTER(C.c_int32))]
+        ("svars", C.POINTER(C.c_double)), ("status", C.POINTER(C.c_int32)),
+        ("mapping", C.POINTER(C.c_double))]
 
 
 _lib = None
@@ -183,7 +188,7 @@ class Oracle:
         cfg = Config()
         cfg.dim = dim
         cfg.scheme = {"usf": 0, "usl": 1, "musl": 2}[scheme]
-        cfg.velocity_update = {"flip": 0, "pic": 1}[velocity_update]
+        cfg.velocity_update = VELOCITY_UPDATES[velocity_update]
         cfg.locate_particles = 1 if locate_particles else 0
         cfg.blending_ratio = blending_ratio
         cfg.dt = dt
@@ -288,6 +293,8 @@ class Oracle:
         P.svars = _dp(arrs["svars"])
         arrs["status"] = np.zeros(n, dtype=np.int32)
         P.status = _i32p(arrs["status"])
+        arrs["mapping"] = np.zeros((n, 9))
+        P.mapping = _dp(arrs["mapping"])
         self._check(lib().mpmo_get_particles(self.h, C.byref(P)))
         for f in FIELDS3:
             arrs[f] = arrs[f][:, :self.dim]
@@ -303,7 +310,7 @@ class Oracle:
                 a[:, :self.dim] = np.asarray(arrs[f])[:, :self.dim]
                 keep.append(a)
                 setattr(P, f, _dp(a))
-        for f in ("stress", "strain", "F", "volume", "mass", "density", "svars"):
+        for f in ("stress", "strain", "F", "volume", "mass", "density", "svars", "mapping"):
             if f in arrs:
                 a = np.ascontiguousarray(arrs[f], dtype=np.float64)
                 keep.append(a)
