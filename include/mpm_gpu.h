@@ -108,6 +108,15 @@ typedef struct {
   double* svars;
 } mpm_gpu_particles;
 
+/* Local coordinates of the cells (mesh "isoparametric", mpm_base.tcc:767-784;
+ * cell.tcc:335-384, 617-826): 1 the isoparametric map (the reference's
+ * default), 0 the Cartesian formula of local_coordinates_point (the default
+ * here).  On a tensor-product grid both give the same coordinates to rounding
+ * and the Cartesian formula is used; on a general mesh 1 takes the inverse of
+ * the bilinear / trilinear map.  Before mpm_gpu_initialise / particle loads;
+ * FP64 and mixed precision, not with sensitivities. */
+int mpm_gpu_set_isoparametric(mpm_gpu_t h, int32_t isoparametric);
+
 /* The mapping matrix of the ASFLIP / APIC / TPIC velocity updates (the
  * particle's mapping_matrix_), n*9 row-major: its leading dim x dim block
  * (zeros elsewhere on read).  MPM_ERR_UNSUPPORTED for FLIP and PIC.  A new

@@ -29,7 +29,7 @@
 #define MPM_G2P_MIN_BLOCKS 4  // 1.41 -> 1.01 ms per 4M-particle step despite spills
 #endif
 #ifndef MPM_MC_RETURN_MIN_BLOCKS
-#define MPM_MC_RETURN_MIN_BLOCKS 4
+#define MPM_MC_RETURN_MIN_BLOCKS 6  // 0.167 -> 0.155 ms at step 400 of the 4M column
 #endif
 #ifndef MPM_P2G_TILE_MIN_BLOCKS
 #define MPM_P2G_TILE_MIN_BLOCKS 4  // 64 registers on a grid: 0.39 -> 0.345 ms (4M, 3D); 5, 6 spill
@@ -239,10 +239,9 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX, AFF>(), MPM_P2G_TILE_MIN_BLOCK
     if (q0 + t < q_end) {
       const int64_t p = s.order[q0 + t];
       const int pc = s.cell[p];
-      const CellGeom& g = s.geom[pc];
       double x[DIM], xi[DIM];
       load_x<DIM>(s, p, x);
-      local_xi<DIM>(x, g.centroid, g.len, xi);
+      particle_xi<DIM, BOX>(s, pc, x, xi);
 #pragma unroll
       for (int d = 0; d < DIM; ++d) rows[RW::XI + d][t] = xi[d];
       if constexpr (MM && AFF) {
@@ -646,8 +645,7 @@ __global__ void __launch_bounds__(128) k_stress(DevState s, double dt) {
   double x[DIM], xi[DIM], D[NV * DIM], X[NV * DIM];
   int nid[NV];
   load_x<DIM>(s, p, x);
-  const CellGeom& g = s.geom[c];
-  local_xi<DIM>(x, g.centroid, g.len, xi);
+  particle_xi<DIM, BOX>(s, c, x, xi);
   cell_nodes_for<DIM, BOX>(s, c, nid, X);
   dn_dx_all<DIM, BOX>(s, c, xi, X, D);
   stress_update<DIM>(s, GlobalRow{s, p}, c, nid, D, dt);
@@ -670,8 +668,7 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p(DevState s, dou
   double x[DIM], xi[DIM], N[NV], X[NV * DIM];
   int nid[NV];
   load_x<DIM>(s, p, x);
-  const CellGeom& g = s.geom[c];
-  local_xi<DIM>(x, g.centroid, g.len, xi);
+  particle_xi<DIM, BOX>(s, c, x, xi);
   shapefn<DIM>(xi, N);
   if constexpr (VU >= 2)
     cell_nodes_coords<DIM>(s, c, nid, X);  // the branch vectors need the nodes
@@ -879,8 +876,7 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
     int nid[NV];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) x[d] = r.f(PF<DIM>::X + d);
-    const CellGeom& g = s.geom[c];
-    local_xi<DIM>(x, g.centroid, g.len, xi);
+    particle_xi<DIM, BOX>(s, c, x, xi);
     shapefn<DIM>(xi, N);
     cell_nodes_for<DIM, BOX>(s, c, nid, X);
     double nvel[DIM], nacc[DIM];
@@ -989,8 +985,7 @@ __global__ void __launch_bounds__(128, MPM_G2P_MIN_BLOCKS) k_g2p_musl(DevState s
   double x[DIM], xi[DIM], N[NV], X[NV * DIM];
   int nid[NV];
   load_x<DIM>(s, p, x);
-  const CellGeom& g = s.geom[c];
-  local_xi<DIM>(x, g.centroid, g.len, xi);
+  particle_xi<DIM, BOX>(s, c, x, xi);
   shapefn<DIM>(xi, N);
   cell_nodes_for<DIM, BOX>(s, c, nid, X);
   double nvel[DIM], nacc[DIM];
@@ -1116,9 +1111,8 @@ __global__ void k_locate_fallback(DevState s, int remove_lost) {
         const int64_t bi = ((int64_t)b[2] * s.bn[1] + b[1]) * s.bn[0] + b[0];
         for (int j = s.bin_off[bi]; j < s.bin_off[bi + 1]; ++j) {
           const int cid = s.bin_cells[j];
-          const CellGeom& g = s.geom[cid];
           double xi[DIM];
-          if (point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi)) {
+          if (cell_point_in<DIM>(s, cid, x, xi)) {
             found = cid;
             break;
           }

@@ -29,7 +29,7 @@
 #define MPM_MIXED_G2P_MIN_BLOCKS 6  // 80 registers, no spills: 0.478 -> 0.374 ms (4M, 3D)
 #endif
 #ifndef MPM_MC_RETURN_MIN_BLOCKS
-#define MPM_MC_RETURN_MIN_BLOCKS 4
+#define MPM_MC_RETURN_MIN_BLOCKS 6  // 0.167 -> 0.155 ms at step 400 of the 4M column
 #endif
 #ifndef MPM_MIXED_P2G_TILE_MIN_BLOCKS
 #define MPM_MIXED_P2G_TILE_MIN_BLOCKS 5  // 48 registers, small spills: 0.32 -> 0.26 ms (4M, 3D)
@@ -55,11 +55,10 @@ __device__ __forceinline__ void set_pmf(const DevState& s, int f, int64_t p, flo
 }
 
 // local coordinate in FP64, rounded to FP32 for the shape functions
-template <int DIM>
+template <int DIM, bool BOX>
 __device__ __forceinline__ void xi_f32(const DevState& s, int c, const double* x, float* xf) {
-  const CellGeom& g = s.geom[c];
   double xi[DIM];
-  local_xi<DIM>(x, g.centroid, g.len, xi);
+  particle_xi<DIM, BOX>(s, c, x, xi);
 #pragma unroll
   for (int d = 0; d < DIM; ++d) xf[d] = (float)xi[d];
 }
@@ -136,7 +135,7 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
       double x[DIM];
       load_x<DIM>(s, p, x);
       float xi[DIM];
-      xi_f32<DIM>(s, pc, x, xi);
+      xi_f32<DIM, BOX>(s, pc, x, xi);
 #pragma unroll
       for (int d = 0; d < DIM; ++d) rows[RW::XI + d][t] = xi[d];
       rows[RW::M][t] = pmf<DIM>(s, PM<DIM>::MASS, p);
@@ -543,7 +542,7 @@ __global__ void __launch_bounds__(128) k_stress_mixed(DevState s, float dt) {
   load_x<DIM>(s, p, x);
   float xi[DIM], D[NV * DIM], Xr[NV * DIM];
   int nid[NV];
-  xi_f32<DIM>(s, c, x, xi);
+  xi_f32<DIM, BOX>(s, c, x, xi);
   cell_nodes_rel<DIM, BOX>(s, c, nid, Xr);
   dn_dx_all_f<DIM, BOX>(s, c, xi, Xr, D);
   stress_update_mixed<DIM>(s, MGlobalRow<DIM>{s, p}, c, nid, D, dt);
@@ -563,7 +562,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   load_x<DIM>(s, p, x);
   float xi[DIM], N[NV], Xr[NV * DIM];
   int nid[NV];
-  xi_f32<DIM>(s, c, x, xi);
+  xi_f32<DIM, BOX>(s, c, x, xi);
   shapefn<DIM>(xi, N);
   cell_nodes_rel<DIM, BOX>(s, c, nid, Xr);
   float nvel[DIM], nacc[DIM];
@@ -695,7 +694,7 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
     for (int d = 0; d < DIM; ++d) x[d] = xr[(PDX<DIM>::X + d) * T + t];
     float N[NV], Xr[NV * DIM];
     int nid[NV];
-    xi_f32<DIM>(s, c, x, xi);
+    xi_f32<DIM, BOX>(s, c, x, xi);
     shapefn<DIM>(xi, N);
     cell_nodes_rel<DIM, BOX>(s, c, nid, Xr);
     float nvel[DIM], nacc[DIM];

@@ -312,14 +312,53 @@ __device__ __forceinline__ void node_shape(const R* xi, int n, R& N, R* G) {
 
 
 // ------------------------------------------------------------------ locate
+// cell.tcc:335-384 for cell c: the Cartesian local coordinates, or on a
+// general mesh with s.iso the isoparametric ones
+template <int DIM>
+__device__ __forceinline__ bool cell_point_in(const DevState& s, int c, const double* x,
+                                              double* xi) {
+  const CellGeom& g = s.geom[c];
+  if (s.iso) {
+    constexpr int NV = Elem<DIM>::NV;
+    int nid[NV];
+    double X[NV * DIM];
+    cell_nodes_coords<DIM>(s, c, nid, X);
+    return point_in_cell_iso<DIM>(x, X, g.centroid, g.mean_length, xi);
+  }
+  return point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi);
+}
+
+// Local coordinates of a particle at x in the cell it was last located in,
+// bit-identical to the value the locate step found (same function, same
+// inputs): the Cartesian formula on box cells and without s.iso, else the
+// isoparametric map, clamped to +-(1 - eps) as the locate step does.
+template <int DIM, bool BOX>
+__device__ __forceinline__ void particle_xi(const DevState& s, int c, const double* x,
+                                            double* xi) {
+  const CellGeom& g = s.geom[c];
+  if constexpr (!BOX) {
+    if (s.iso) {
+      constexpr int NV = Elem<DIM>::NV;
+      int nid[NV];
+      double X[NV * DIM];
+      cell_nodes_coords<DIM>(s, c, nid, X);
+      iso_local_xi<DIM>(x, X, xi);
+#pragma unroll
+      for (int i = 0; i < DIM; ++i) {
+        if (xi[i] < -1. + kDblEps) xi[i] = -1. + kDblEps;
+        if (xi[i] > 1. - kDblEps) xi[i] = 1. - kDblEps;
+      }
+      return;
+    }
+  }
+  local_xi<DIM>(x, g.centroid, g.len, xi);
+}
+
 // mesh.tcc:1116-1151: the current cell, then neighbours in ascending id
 template <int DIM>
 __device__ __forceinline__ int locate_near(const DevState& s, const double* x, int c) {
   double xi[DIM];
-  {
-    const CellGeom& g = s.geom[c];
-    if (point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi)) return c;
-  }
+  if (cell_point_in<DIM>(s, c, x, xi)) return c;
   if (s.structured) {
     // neighbours of a tensor-product cell: the 3^dim - 1 cells around it,
     // ascending id (the node-sharing cells of mesh.tcc:287-306)
@@ -334,8 +373,7 @@ __device__ __forceinline__ int locate_near(const DevState& s, const double* x, i
           if (i < 0 || i >= s.gcells[0]) continue;
           const int nc = DIM == 2 ? i + s.gcells[0] * j : i + s.gcells[0] * (j + s.gcells[1] * k);
           if (nc == c) continue;
-          const CellGeom& g = s.geom[nc];
-          if (point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi)) return nc;
+          if (cell_point_in<DIM>(s, nc, x, xi)) return nc;
         }
       }
     }
@@ -344,8 +382,7 @@ __device__ __forceinline__ int locate_near(const DevState& s, const double* x, i
   const int b = s.nb_off[c], e = s.nb_off[c + 1];
   for (int k = b; k < e; ++k) {
     const int nc = s.nb[k];
-    const CellGeom& g = s.geom[nc];
-    if (point_in_cell<DIM>(x, g.centroid, g.len, g.mean_length, xi)) return nc;
+    if (cell_point_in<DIM>(s, nc, x, xi)) return nc;
   }
   return -1;
 }

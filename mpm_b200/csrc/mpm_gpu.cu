@@ -170,6 +170,7 @@ struct mpm_gpu_solver {
   int32_t bn[3] = {1, 1, 1};
   std::map<int64_t, HostBC> bcs;        // node id -> constraints
   bool structured = false;
+  bool isoparametric = false;  // general cells: isoparametric local coordinates
   int32_t gcells[3] = {1, 1, 1};
   std::vector<double> axis[3];
   std::vector<double> axis_ihl[3];  // 2 / (axis[i + 1] - axis[i]): J^-1 of the box cells
@@ -457,6 +458,21 @@ bool detect_structured(mpm_gpu_t h) {
   return true;
 }
 
+// cell.tcc:335-384 for cell c on the host (host twin of cell_point_in)
+bool host_point_in(mpm_gpu_t h, int64_t c, const double* p, double* xi) {
+  const CellGeom& g = h->geom[c];
+  if (h->isoparametric && !h->structured) {
+    double X[8 * 3];
+    for (int i = 0; i < h->nv; ++i)
+      for (int d = 0; d < h->dim; ++d)
+        X[i * h->dim + d] = h->coords[(size_t)h->cell_nodes[(size_t)c * h->nv + i] * h->dim + d];
+    return h->dim == 2 ? point_in_cell_iso<2>(p, X, g.centroid, g.mean_length, xi)
+                       : point_in_cell_iso<3>(p, X, g.centroid, g.mean_length, xi);
+  }
+  return h->dim == 2 ? point_in_cell<2>(p, g.centroid, g.len, g.mean_length, xi)
+                     : point_in_cell<3>(p, g.centroid, g.len, g.mean_length, xi);
+}
+
 // first cell in id order containing p (host twin of the device fallback)
 int32_t host_scan(mpm_gpu_t h, const double* p) {
   if (h->structured) {
@@ -473,11 +489,8 @@ int32_t host_scan(mpm_gpu_t h, const double* p) {
   const int64_t bi = (b[2] * h->bn[1] + b[1]) * h->bn[0] + b[0];
   for (int32_t j = h->bin_off[bi]; j < h->bin_off[bi + 1]; ++j) {
     const int32_t c = h->bin_cells[j];
-    const CellGeom& g = h->geom[c];
     double xi[3];
-    const bool in = h->dim == 2 ? point_in_cell<2>(p, g.centroid, g.len, g.mean_length, xi)
-                                : point_in_cell<3>(p, g.centroid, g.len, g.mean_length, xi);
-    if (in) return c;
+    if (host_point_in(h, c, p, xi)) return c;
   }
   return -1;
 }
@@ -709,6 +722,7 @@ void refresh_state(mpm_gpu_t h) {
   s.pf = h->d_pf.p;
   s.sv = h->d_sv.p;
   s.mapb = h->d_mapb.p;
+  s.iso = h->isoparametric && !h->structured ? 1 : 0;
   s.cell = h->d_cell.p;
   s.mat = h->d_mat.p;
   s.pvc = h->d_pvc.p;
@@ -1486,6 +1500,14 @@ int64_t mpm_gpu_launch_count(mpm_gpu_t h) { return h ? h->prof.launches : -1; }
 int64_t mpm_gpu_nparticles(mpm_gpu_t h) { return h ? h->np : -1; }
 int64_t mpm_gpu_current_step(mpm_gpu_t h) { return h ? h->step : -1; }
 
+int mpm_gpu_set_isoparametric(mpm_gpu_t h, int32_t isoparametric) {
+  MPM_GUARD(h)
+  if (h->initialised) throw InvalidArg("set the local-coordinate map before the particles");
+  h->isoparametric = isoparametric != 0;
+  return MPM_OK;
+  MPM_END(h)
+}
+
 int mpm_gpu_read_mapping_matrix(mpm_gpu_t h, double* out) {
   MPM_GUARD(h)
   if (!h->initialised) throw InvalidArg("no particles");
@@ -1671,10 +1693,8 @@ void upload_pod_aux(mpm_gpu_t h) {
 // cell, its neighbours in ascending id, then every cell in id order.
 int32_t host_locate(mpm_gpu_t h, const double* x, int64_t hint) {
   auto inside = [&](int64_t c) {
-    const CellGeom& g = h->geom[c];
     double xi[3];
-    return h->dim == 2 ? point_in_cell<2>(x, g.centroid, g.len, g.mean_length, xi)
-                       : point_in_cell<3>(x, g.centroid, g.len, g.mean_length, xi);
+    return host_point_in(h, c, x, xi);
   };
   if (hint >= 0 && hint < h->ncells) {
     if (inside(hint)) return (int32_t)hint;
@@ -1894,6 +1914,8 @@ int mpm_gpu_set_sensitivities(mpm_gpu_t h, int32_t n, const int32_t* material_id
     return fail(h, MPM_ERR_UNSUPPORTED, "sensitivities follow the USL scheme only");
   if (n > 0 && h->cfg.velocity_update >= MPM_VELOCITY_ASFLIP)
     return fail(h, MPM_ERR_UNSUPPORTED, "sensitivities follow the FLIP and PIC updates only");
+  if (n > 0 && h->isoparametric && !h->structured)
+    return fail(h, MPM_ERR_UNSUPPORTED, "sensitivities take Cartesian local coordinates only");
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
   std::vector<TangentParam> params(n);
   for (int k = 0; k < n; ++k) {

@@ -192,6 +192,79 @@ MPM_HD bool point_in_cell(const double* p, const double* centroid, const double*
   return status;
 }
 
+// Isoparametric local coordinates (cell.tcc:617-826 transform_real_to_unit_cell
+// for quad4 / hex8): the xi with sum_i N_i(xi) X_i = p, by Newton iterations on
+// the bilinear / trilinear map from the cell centre until the step is below
+// 1e-12 (the next error is at rounding level; at most 50 iterations).  The
+// reference tries an analytical (2D) or affine guess and Newton with a line
+// search and keeps the smallest residual; every accepted solution is the same
+// root to rounding for a convex cell.  False when the iteration did not
+// converge or the point maps to a non-finite xi.
+template <int DIM>
+MPM_HD bool iso_local_xi(const double* p, const double* X, double* xi) {
+  constexpr int NV = DIM == 2 ? 4 : 8;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) xi[d] = 0.;
+  for (int it = 0; it < 50; ++it) {
+    double N[NV], G[NV * DIM], r[DIM], Jm[DIM * DIM], Ji[DIM * DIM];
+    shapefn<DIM>(xi, N);
+    grad_shapefn<DIM>(xi, G);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      double xa = N[0] * X[0 * DIM + a];
+      for (int i = 1; i < NV; ++i) xa = xa + N[i] * X[i * DIM + a];
+      r[a] = xa - p[a];
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) {  // dx_a / dxi_b
+        double j = X[0 * DIM + a] * G[0 * DIM + b];
+        for (int i = 1; i < NV; ++i) j = j + X[i * DIM + a] * G[i * DIM + b];
+        Jm[a * DIM + b] = j;
+      }
+    }
+    inverse<DIM>(Jm, Ji);
+    double step = 0.;
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) {
+      double dxi = Ji[b * DIM + 0] * r[0];
+#pragma unroll
+      for (int a = 1; a < DIM; ++a) dxi = dxi + Ji[b * DIM + a] * r[a];
+      xi[b] -= dxi;
+      step = step > fabs(dxi) ? step : fabs(dxi);
+    }
+    if (!(step == step)) return false;
+    if (step < 1e-12) return true;  // quadratic convergence: xi now at rounding level
+  }
+  return false;
+}
+
+// cell.tcc:335-384 with transform_real_to_unit_cell (isoparametric true);
+// X: the cell's nodal coordinates.
+template <int DIM>
+MPM_HD bool point_in_cell_iso(const double* p, const double* X, const double* centroid,
+                              double mean_length, double* xi) {
+  double d[DIM];
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) d[i] = p[i] - centroid[i];
+  double s = d[0] * d[0];
+#pragma unroll
+  for (int i = 1; i < DIM; ++i) s = s + d[i] * d[i];
+  if (!(sqrt(s) < (mean_length * 2.))) return false;
+  if (!iso_local_xi<DIM>(p, X, xi)) return false;
+  bool status = true;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) {
+    double x = xi[i];
+    if (x < -1. || x > 1. || x != x) {
+      status = false;
+    } else {
+      if (x < -1. + kDblEps) x = -1. + kDblEps;
+      if (x > 1. - kDblEps) x = 1. - kDblEps;
+    }
+    xi[i] = x;
+  }
+  return status;
+}
+
 // xi of a particle in the cell it was last located in (bit-identical to the
 // value the locate step stored: same formula, same inputs).
 template <int DIM>

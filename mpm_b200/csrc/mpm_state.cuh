@@ -109,6 +109,7 @@ struct DevState {
   const double* axis[3] = {nullptr, nullptr, nullptr};  // node coordinates per axis
   const double* axis_ihl[3] = {nullptr, nullptr, nullptr};  // 2 / cell length per axis interval
   double* mapb = nullptr;  // [DIM * DIM][np] mapping matrix (ASFLIP, TPIC, APIC), row-major
+  int iso = 0;             // general cells take isoparametric local coordinates
 
   // general meshes: cells around each node, ascending cell id, with the
   // node's local index (slot) in that cell

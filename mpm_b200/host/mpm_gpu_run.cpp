@@ -47,6 +47,7 @@ struct Input {
   double gravity[3] = {0, 0, 0};
   long nsteps = 0;
   bool locate = true;
+  bool isoparametric = true;          // mesh "isoparametric" (mpm_base.tcc:767-784 default)
   std::vector<double> coords;         // nnodes x dim
   std::vector<int64_t> cells;         // ncells x nv
   int64_t nnodes = 0, ncells = 0;
@@ -177,6 +178,7 @@ Input read_input(const std::string& dir, const std::string& file) {
     in.mats.push_back({(int)m.at("id").as_double(), m.at("type").as_string(), dump(m)});
   // mesh (io_mesh_ascii.tcc: "nnodes ncells", node coordinates, cell node ids)
   const Json& mesh = root.at("mesh");
+  if (mesh.contains("isoparametric")) in.isoparametric = mesh.at("isoparametric").as_bool();
   {
     const auto lines = data_lines(join(dir, mesh.at("mesh").as_string()));
     if (lines.empty()) throw std::runtime_error("empty mesh file");
@@ -393,6 +395,7 @@ int main(int argc, char** argv) {
   check(nullptr, mpm_gpu_create(&cfg, &h), "create");
   check(h, mpm_gpu_set_mesh(h, in.nnodes, in.coords.data(), in.ncells, in.dim == 2 ? 4 : 8,
                             in.cells.data()), "set_mesh");
+  check(h, mpm_gpu_set_isoparametric(h, in.isoparametric ? 1 : 0), "set_isoparametric");
   for (auto& m : in.mats) check(h, mpm_gpu_add_material(h, m.id, m.type.c_str(), m.json.c_str()), "add_material");
   if (!in.vnid.empty())
     check(h, mpm_gpu_add_velocity_constraints(h, (int64_t)in.vnid.size(), in.vnid.data(), in.vdir.data(),

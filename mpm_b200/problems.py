@@ -312,6 +312,8 @@ def build_solver(prob, solver_cls=None, with_particles=True, **overrides):
                                locate_particles=a.get("locate_particles", True),
                                precision=a.get("precision", "fp64"),
                                device=a.get("device", 0))
+    if a.get("isoparametric", False):
+        s.set_isoparametric(True)
     apply_problem(prob, s, with_particles=with_particles)
     return s
 

@@ -167,6 +167,11 @@ class Solver:
     def current_step(self):
         return self.L.mpm_gpu_current_step(self.h)
 
+    def set_isoparametric(self, on=True):
+        """Isoparametric local coordinates on a general mesh (the mesh's
+        "isoparametric" flag; before the particles are added)."""
+        self._ck(self.L.mpm_gpu_set_isoparametric(self.h, 1 if on else 0))
+
     def read(self):
         """Particle state as numpy arrays (rows = particles)."""
         n = self.nparticles

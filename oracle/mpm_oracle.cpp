@@ -791,12 +791,52 @@ bool approx_point_in_cell(const Oracle& o, const Cell& c, const double* p) {
   return length < (c.mean_length * 2.);
 }
 
-// cell.tcc:335-384 (isoparametric false)
+// cell.tcc:617-826 transform_real_to_unit_cell for quad4 / hex8: the root of
+// sum_i N_i(xi) X_i = p.  The reference keeps the best of an analytical (2D) or
+// affine guess and Newton iterations with a line search; this restatement runs
+// Newton from the cell centre to a step below 1e-12 (quadratic convergence:
+// the root to rounding for a convex cell).  False when it does not converge.
+bool transform_real_to_unit_cell(const Oracle& o, const Cell& c, const double* p, double* xi) {
+  const int dim = o.dim, nv = o.nv;
+  for (int d = 0; d < dim; ++d) xi[d] = 0.;
+  for (int it = 0; it < 50; ++it) {
+    double N[8], G[8 * 3], r[3], Jm[9], Ji[9];
+    shapefn(dim, xi, N);
+    grad_shapefn(dim, xi, G);
+    for (int a = 0; a < dim; ++a) {
+      double xa = N[0] * c.X[0 * dim + a];
+      for (int i = 1; i < nv; ++i) xa = xa + N[i] * c.X[i * dim + a];
+      r[a] = xa - p[a];
+      for (int b = 0; b < dim; ++b) {
+        double j = c.X[0 * dim + a] * G[0 * dim + b];
+        for (int i = 1; i < nv; ++i) j = j + c.X[i * dim + a] * G[i * dim + b];
+        Jm[a * dim + b] = j;
+      }
+    }
+    inverse(dim, Jm, Ji);
+    double step = 0.;
+    for (int b = 0; b < dim; ++b) {
+      double dxi = Ji[b * dim + 0] * r[0];
+      for (int a = 1; a < dim; ++a) dxi = dxi + Ji[b * dim + a] * r[a];
+      xi[b] -= dxi;
+      step = std::max(step, std::fabs(dxi));
+    }
+    if (!(step == step)) return false;
+    if (step < 1e-12) return true;  // quadratic convergence: xi now at rounding level
+  }
+  return false;
+}
+
+// cell.tcc:335-384
 bool is_point_in_cell(const Oracle& o, const Cell& c, const double* p, double* xi) {
   for (int i = 0; i < o.dim; ++i) xi[i] = std::numeric_limits<double>::max();
   if (!approx_point_in_cell(o, c, p)) return false;
   bool status = true;
-  local_coordinates_point(o, c, p, xi);
+  if (o.cfg.isoparametric) {
+    if (!transform_real_to_unit_cell(o, c, p, xi)) return false;
+  } else {
+    local_coordinates_point(o, c, p, xi);
+  }
   const double tolerance = kEps;
   for (int i = 0; i < o.dim; ++i) {
     if (xi[i] < -1. || xi[i] > 1. || std::isnan(xi[i]))

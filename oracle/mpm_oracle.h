@@ -37,7 +37,8 @@ typedef struct {
   double gravity[3];
   double gravity_ramping_time;
   int32_t nthreads; /* 1 = deterministic golden mode */
-  int32_t pad_;
+  int32_t isoparametric; /* 1: local coordinates by the isoparametric map
+                            (cell.tcc:617-826), 0: the Cartesian formula */
 } mpmo_config;
 
 /* Particle state as flat arrays, one record per particle (AoS in this API).

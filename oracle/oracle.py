@@ -33,7 +33,7 @@ class Config(C.Structure):
                 ("blending_ratio", C.c_double), ("dt", C.c_double),
                 ("damping_factor", C.c_double), ("gravity", C.c_double * 3),
                 ("gravity_ramping_time", C.c_double), ("nthreads", C.c_int32),
-                ("pad_", C.c_int32)]
+                ("isoparametric", C.c_int32)]
 
 
 # velocity_update names -> the reference's VelocityUpdate order (data_types.h:50)
@@ -184,12 +184,14 @@ class Oracle:
 
     def __init__(self, dim, scheme="usf", velocity_update="flip", dt=1e-3,
                  gravity=(0, 0, 0), damping_factor=0.0, blending_ratio=1.0,
-                 gravity_ramping_time=0.0, locate_particles=True, nthreads=1):
+                 gravity_ramping_time=0.0, locate_particles=True, nthreads=1,
+                 isoparametric=False):
         cfg = Config()
         cfg.dim = dim
         cfg.scheme = {"usf": 0, "usl": 1, "musl": 2}[scheme]
         cfg.velocity_update = VELOCITY_UPDATES[velocity_update]
         cfg.locate_particles = 1 if locate_particles else 0
+        cfg.isoparametric = 1 if isoparametric else 0
         cfg.blending_ratio = blending_ratio
         cfg.dt = dt
         cfg.damping_factor = damping_factor
@@ -355,5 +357,6 @@ def build_oracle(prob, nthreads=1, **overrides):
                gravity=a.get("gravity", (0, 0, 0)), damping_factor=a.get("damping_factor", 0.0),
                blending_ratio=a.get("blending_ratio", 1.0),
                gravity_ramping_time=a.get("gravity_ramping_time", 0.0),
-               locate_particles=a.get("locate_particles", True), nthreads=nthreads)
+               locate_particles=a.get("locate_particles", True), nthreads=nthreads,
+               isoparametric=a.get("isoparametric", False))
     return apply_problem(prob, o)

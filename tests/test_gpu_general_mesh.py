@@ -101,3 +101,45 @@ def test_mixed_precision_on_general_mesh(mesh):
     assert np.array_equal(out["mixed"]["cell"], out["fp64"]["cell"])
     errs = field_errors(out["mixed"], out["fp64"], ("u", "v", "stress", "strain"))
     assert all(v <= 1e-5 for v in errs.values()), errs
+
+
+@pytest.mark.parametrize("scheme", ["usf", "usl"])
+def test_isoparametric_2d_distorted_column(scheme):
+    """Isoparametric local coordinates (cell.tcc:617-826) on a distorted mesh:
+    the locate step and every kernel's local coordinates take the inverse of
+    the bilinear map."""
+    prob = distort_interior(small_column_2d(scheme=scheme), frac=0.2)
+    prob.analysis["isoparametric"] = True
+    for s, g, o in _run_both(prob, [1, 10, 100]):
+        assert_parity(g, o, label=f"2D LE isoparametric {scheme} step {s}")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_isoparametric_3d_distorted_mohr_coulomb(precision):
+    prob = distort_interior(small_column_3d(scheme="usl", dt=1e-5, c=2000., psi=5.), frac=0.2)
+    prob.analysis["isoparametric"] = True
+    if precision == "fp64":
+        for s, g, o in _run_both(prob, [1, 10, 50]):
+            assert_parity(g, o, label=f"3D MC isoparametric step {s}")
+        return
+    out = {}
+    for prec in ("fp64", "mixed"):
+        sol = P.build_solver(prob, precision=prec)
+        sol.step(50)
+        out[prec] = sol.read()
+    assert np.array_equal(out["mixed"]["cell"], out["fp64"]["cell"])
+    errs = field_errors(out["mixed"], out["fp64"], ("u", "v", "stress", "strain"))
+    assert all(v <= 1e-5 for v in errs.values()), errs
+
+
+def test_isoparametric_differs_from_cartesian_on_a_distorted_mesh():
+    """The two local-coordinate maps give different positions on a distorted
+    mesh (the flag is not ignored)."""
+    runs = {}
+    for iso in (False, True):
+        prob = distort_interior(small_column_2d(scheme="usl"), frac=0.2)
+        prob.analysis["isoparametric"] = iso
+        sol = P.build_solver(prob)
+        sol.step(20)
+        runs[iso] = sol.read()
+    assert np.max(np.abs(runs[True]["x"] - runs[False]["x"])) > 1e-9
