@@ -149,6 +149,14 @@ int mpm_gpu_add_friction_constraints(mpm_gpu_t h, int64_t n, const int64_t* node
                                      const int32_t* dirs, const int32_t* signs,
                                      const double* mu);
 
+/* General (rotated) boundaries (mesh boundary_conditions "nodal_euler_angles",
+ * mpm_base.tcc:1041-1063, mesh.tcc:1318-1345): node ids and dim Euler angles
+ * per node (n*dim, radians).  The velocity, acceleration and friction
+ * constraints of those nodes act on the components of the node's rotated
+ * frame (node.tcc:370-483, 510-657). */
+int mpm_gpu_set_nodal_euler_angles(mpm_gpu_t h, int64_t n, const int64_t* node_ids,
+                                   const double* angles);
+
 /* Create particles at coordinates (n*dim) with one material
  * (mesh.tcc:2114-2148 read_particles_file / create_particles). */
 int mpm_gpu_add_particles(mpm_gpu_t h, int64_t n, const double* coords, int32_t material_id);

@@ -67,6 +67,7 @@ SIGNATURES = {
     "mpm_gpu_read_particles": (C.c_int, [_vp, C.POINTER(Particles)]),
     "mpm_gpu_read_mapping_matrix": (C.c_int, [_vp, _pd]),
     "mpm_gpu_set_isoparametric": (C.c_int, [_vp, C.c_int32]),
+    "mpm_gpu_set_nodal_euler_angles": (C.c_int, [_vp, C.c_int64, _pi64, _pd]),
     "mpm_gpu_load_mapping_matrix": (C.c_int, [_vp, _pd]),
     "mpm_gpu_write_pod": (C.c_int, [_vp, _vp, C.c_int64, _pi64, C.c_size_t, _psz, _psz,
                                     C.c_int32]),

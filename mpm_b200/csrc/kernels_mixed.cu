@@ -264,9 +264,7 @@ __device__ __forceinline__ void node_accel_update_d(const DevState& s, double m,
   if (bci >= 0) {
     const NodeBC& bc = s.bcs[bci];
     if (bc.friction) apply_friction_constraints<DIM>(bc, vel, acc, dt);
-#pragma unroll
-    for (int d = 0; d < DIM; ++d)
-      if (bc.acc_mask & (1u << d)) acc[d] = bc.acc[d];
+    apply_acceleration_constraints<DIM>(bc, acc);
   }
 #pragma unroll
   for (int d = 0; d < DIM; ++d) vel[d] += acc[d] * dt;

@@ -316,9 +316,7 @@ __global__ void __launch_bounds__(128, MPM_TANGENT_NODES_MIN_BLOCKS) k_nodes_tan
     if (bci >= 0) {
       const NodeBC& bc = s.bcs[bci];
       if (bc.friction) apply_friction_constraints<DIM>(bc, vel, acc, dt);
-#pragma unroll
-      for (int d = 0; d < DIM; ++d)
-        if (bc.acc_mask & (1u << d)) acc[d] = D(bc.acc[d]);
+      apply_acceleration_constraints<DIM>(bc, acc);
     }
 #pragma unroll
     for (int d = 0; d < DIM; ++d) vel[d] += acc[d] * dt;

@@ -67,6 +67,8 @@ struct HostBC {
   unsigned fdir = 0;
   int fsign = 0;
   double mu = 0;
+  bool rotated = false;  // general boundary: constraints in the frame of these angles
+  double angles[3] = {0, 0, 0};
 };
 
 }  // namespace
@@ -638,6 +640,20 @@ void upload_bcs(mpm_gpu_t h) {
     b.fric_dir = (uint8_t)kv.second.fdir;
     b.fric_sign = kv.second.fsign;
     b.mu = kv.second.mu;
+    if (kv.second.rotated) {
+      b.rotated = 1;
+      euler_rotation(h->dim, kv.second.angles, b.rot);
+      // the inverse of the leading dim x dim block (Eigen's fixed-size inverse)
+      double Rd[9], Ri[9];
+      for (int a = 0; a < h->dim; ++a)
+        for (int c = 0; c < h->dim; ++c) Rd[a * h->dim + c] = b.rot[a * 3 + c];
+      if (h->dim == 2)
+        inverse<2>(Rd, Ri);
+      else
+        inverse<3>(Rd, Ri);
+      for (int a = 0; a < h->dim; ++a)
+        for (int c = 0; c < h->dim; ++c) b.irot[a * 3 + c] = Ri[a * h->dim + c];
+    }
     std::string key(reinterpret_cast<const char*>(&b), sizeof(b));
     auto it = dedup.find(key);
     int slot;
@@ -1205,6 +1221,23 @@ int mpm_gpu_add_velocity_constraints(mpm_gpu_t h, int64_t n, const int64_t* nid,
 int mpm_gpu_add_acceleration_constraints(mpm_gpu_t h, int64_t n, const int64_t* nid,
                                          const int32_t* dir, const double* val) {
   return add_vel_acc(h, n, nid, dir, val, false);
+}
+
+int mpm_gpu_set_nodal_euler_angles(mpm_gpu_t h, int64_t n, const int64_t* nid,
+                                   const double* angles) {
+  MPM_GUARD(h)
+  if (!h->mesh_set) throw InvalidArg("set the mesh first");
+  if (n > 0 && (!nid || !angles)) throw InvalidArg("null node ids or angles");
+  for (int64_t i = 0; i < n; ++i) {
+    if (nid[i] < 0 || nid[i] >= h->nnodes) throw InvalidArg("Euler angle node id out of range");
+    HostBC& b = h->bcs[nid[i]];
+    b.rotated = true;
+    for (int d = 0; d < 3; ++d) b.angles[d] = d < h->dim ? angles[i * h->dim + d] : 0.;
+  }
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  upload_bcs(h);
+  MPM_END(h)
+  return MPM_OK;
 }
 
 int mpm_gpu_add_friction_constraints(mpm_gpu_t h, int64_t n, const int64_t* nid, const int32_t* dir,

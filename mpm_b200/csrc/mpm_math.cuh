@@ -873,25 +873,108 @@ struct NodeBC {
   double vel[3];
   double acc[3];
   double mu;
+  // general boundaries (node.h assign_rotation_matrix): the constraint
+  // directions are those of the node's local frame, rot maps local to global
+  // components, irot = rot^-1 (both row-major, leading DIM x DIM block)
+  int32_t rotated;
+  double rot[9], irot[9];
 };
+
+// Rotation of a node's local frame from its Euler angles (radians): in 2D
+// the rotation by alpha + beta; in 3D Rz(alpha) Rx(gamma) Rz(beta) (angles
+// alpha, beta, gamma as mesh.tcc:1318-1345 reads them).  Row-major into R.
+MPM_HD void euler_rotation(int dim, const double* angles, double* R) {
+  const double ca = cos(angles[0]), sa = sin(angles[0]);
+  const double cb = cos(angles[1]), sb = sin(angles[1]);
+  const double cacb = ca * cb, casb = ca * sb, sacb = sa * cb, sasb = sa * sb;
+  if (dim == 2) {
+    R[0] = cacb - sasb;
+    R[1] = -casb - sacb;
+    R[3] = sacb + casb;
+    R[4] = -sasb + cacb;
+    return;
+  }
+  const double cg = cos(angles[2]), sg = sin(angles[2]);
+  R[0] = cacb - sasb * cg;
+  R[1] = -casb - sacb * cg;
+  R[2] = sa * sg;
+  R[3] = sacb + casb * cg;
+  R[4] = -sasb + cacb * cg;
+  R[5] = -ca * sg;
+  R[6] = sb * sg;
+  R[7] = cb * sg;
+  R[8] = cg;
+}
+
+// out = M v for the leading DIM x DIM block of a row-major 3 x 3 M
+template <int DIM, typename R>
+MPM_HD void rot_apply(const double* M, const R* v, R* out) {
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    R s = M[a * 3 + 0] * v[0];
+#pragma unroll
+    for (int b = 1; b < DIM; ++b) s = s + M[a * 3 + b] * v[b];
+    out[a] = s;
+  }
+}
 
 template <int DIM, typename R>
 MPM_HD void apply_velocity_constraints(const NodeBC& bc, R* v, R* a) {
 #pragma unroll
   for (int d = 0; d < DIM; ++d)
     if (bc.vel_mask & (1u << d)) {
-      v[d] = R(bc.vel[d]);
-      a[d] = R(0.);
+      if (!bc.rotated) {
+        v[d] = R(bc.vel[d]);
+        a[d] = R(0.);
+      } else {  // node.tcc:385-401: in the local frame, one direction at a time
+        R lv[DIM], la[DIM];
+        rot_apply<DIM>(bc.irot, v, lv);
+        rot_apply<DIM>(bc.irot, a, la);
+        lv[d] = R(bc.vel[d]);
+        la[d] = R(0.);
+        rot_apply<DIM>(bc.rot, lv, v);
+        rot_apply<DIM>(bc.rot, la, a);
+      }
     }
 }
 
-// node.tcc:510-657 (Cartesian boundaries)
+// node.tcc:456-483
 template <int DIM, typename R>
-MPM_HD void apply_friction_constraints(const NodeBC& bc, const R* vel, R* acc, double dt) {
+MPM_HD void apply_acceleration_constraints(const NodeBC& bc, R* a) {
+#pragma unroll
+  for (int d = 0; d < DIM; ++d)
+    if (bc.acc_mask & (1u << d)) {
+      if (!bc.rotated) {
+        a[d] = R(bc.acc[d]);
+      } else {
+        R la[DIM];
+        rot_apply<DIM>(bc.irot, a, la);
+        la[d] = R(bc.acc[d]);
+        rot_apply<DIM>(bc.rot, la, a);
+      }
+    }
+}
+
+// node.tcc:510-657; on a general boundary in the node's local frame
+template <int DIM, typename R>
+MPM_HD void apply_friction_constraints(const NodeBC& bc, const R* vel_g, R* acc_g, double dt) {
   auto sign = [](const R& value) { return (value > 0.) ? 1. : -1.; };
   const unsigned dir_n = bc.fric_dir;
   const double sign_n = bc.fric_sign > 0 ? 1. : -1.;
   const double mu = bc.mu;
+  R vel_l[DIM], acc_l[DIM];
+  if (bc.rotated) {
+    rot_apply<DIM>(bc.irot, vel_g, vel_l);
+    rot_apply<DIM>(bc.irot, acc_g, acc_l);
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      vel_l[d] = vel_g[d];
+      acc_l[d] = acc_g[d];
+    }
+  }
+  const R* vel = vel_l;
+  R* acc = acc_l;
   if constexpr (DIM == 2) {
     const unsigned dir_t = 1 - dir_n;
     const R acc_n = acc[dir_n];
@@ -912,6 +995,10 @@ MPM_HD void apply_friction_constraints(const NodeBC& bc, const R* vel, R* acc, d
           acc_t -= sign(acc_t) * mu * fabs(acc_n);
       }
       acc[dir_t] = acc_t;
+      if (bc.rotated)
+        rot_apply<DIM>(bc.rot, acc, acc_g);
+      else
+        acc_g[dir_t] = acc_t;
     }
   } else {
     const unsigned t0 = dir_n == 0 ? 1 : 0;
@@ -941,6 +1028,12 @@ MPM_HD void apply_friction_constraints(const NodeBC& bc, const R* vel, R* acc, d
           acc[t0] -= mu * fabs(acc_n) * (acc[t0] / acc_t);
           acc[t1] -= mu * fabs(acc_n) * (acc[t1] / acc_t);
         }
+      }
+      if (bc.rotated) {
+        rot_apply<DIM>(bc.rot, acc, acc_g);
+      } else {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) acc_g[d] = acc[d];
       }
     }
   }

@@ -62,9 +62,9 @@ struct Input {
   };
   std::vector<PSet> psets;
   std::vector<double> stresses;       // nparticles x 6 (optional)
-  std::vector<int64_t> vnid, fnid;
+  std::vector<int64_t> vnid, fnid, enid;
   std::vector<int32_t> vdir, fdir, fsign;
-  std::vector<double> vval, fmu;
+  std::vector<double> vval, fmu, eangles;  // eangles: nodal Euler angles, enid.size() x dim
   struct PVC {
     std::vector<int64_t> ids;         // empty: every particle (set -1)
     int dir;
@@ -254,6 +254,19 @@ Input read_input(const std::string& dir, const std::string& file) {
           in.fsign.push_back(sgn);
           in.fmu.push_back(mu);
         }
+    // mpm_base.tcc:1041-1063, io_mesh_ascii.tcc:351-390: "nid a0 a1 (a2)" per line
+    if (bc.contains("nodal_euler_angles"))
+      for (const auto& line : data_lines(join(dir, bc.at("nodal_euler_angles").as_string()))) {
+        std::istringstream l(line);
+        int64_t n;
+        l >> n;
+        in.enid.push_back(n);
+        for (int d = 0; d < in.dim; ++d) {
+          double a = 0.;
+          l >> a;
+          in.eangles.push_back(a);
+        }
+      }
     if (bc.contains("particles_velocity_constraints")) {
       std::map<long, std::vector<int64_t>> sets;
       if (mesh.contains("entity_sets")) {
@@ -403,6 +416,9 @@ int main(int argc, char** argv) {
   if (!in.fnid.empty())
     check(h, mpm_gpu_add_friction_constraints(h, (int64_t)in.fnid.size(), in.fnid.data(), in.fdir.data(),
                                               in.fsign.data(), in.fmu.data()), "friction constraints");
+  if (!in.enid.empty())
+    check(h, mpm_gpu_set_nodal_euler_angles(h, (int64_t)in.enid.size(), in.enid.data(),
+                                            in.eangles.data()), "nodal Euler angles");
   for (auto& p : in.psets)
     check(h, mpm_gpu_add_particles(h, (int64_t)p.x.size() / in.dim, p.x.data(), p.material), "add_particles");
   check(h, mpm_gpu_initialise(h), "initialise");

@@ -45,6 +45,7 @@ class Problem:
     velocity_constraints: tuple = None   # (nid, dir, value)
     friction_constraints: tuple = None   # (nid, dir, sign, mu)
     particle_velocity_constraints: list = field(default_factory=list)  # [(pids|None, dir, v)]
+    nodal_euler_angles: tuple = None     # (nid, angles n x dim, radians): rotated boundaries
     initial_stress: np.ndarray = None    # nparticles x 6, creation order
     analysis: dict = field(default_factory=dict)
     name: str = ""
@@ -328,6 +329,8 @@ def apply_problem(prob, s, with_particles=True):
         s.add_velocity_constraints(*prob.velocity_constraints)
     if prob.friction_constraints is not None:
         s.add_friction_constraints(*prob.friction_constraints)
+    if prob.nodal_euler_angles is not None:
+        s.set_nodal_euler_angles(*prob.nodal_euler_angles)
     if not with_particles:
         return s
     for pts, mid in prob.particles:

@@ -108,6 +108,13 @@ class Solver:
         self._ck(self.L.mpm_gpu_add_friction_constraints(self.h, len(nid), _i64p(nid), _i32p(d),
                                                          _i32p(s), _dp(m)))
 
+    def set_nodal_euler_angles(self, nid, angles):
+        """Rotated frames (dim Euler angles per node, radians) for the nodes'
+        velocity, acceleration and friction constraints."""
+        nid = np.ascontiguousarray(nid, dtype=np.int64)
+        a = np.ascontiguousarray(angles, dtype=np.float64)
+        self._ck(self.L.mpm_gpu_set_nodal_euler_angles(self.h, len(nid), _i64p(nid), _dp(a)))
+
     def add_particles(self, coords, material_id):
         coords = np.ascontiguousarray(coords, dtype=np.float64)
         self._ck(self.L.mpm_gpu_add_particles(self.h, coords.shape[0], _dp(coords), material_id))

@@ -668,6 +668,8 @@ struct Node {
   unsigned fdir = 0;
   int fsign = 0;
   double mu = 0;
+  bool rotated = false;            // generic_boundary_constraints_
+  double R[9] = {}, Ri[9] = {};    // rotation_matrix_ and its inverse (dim x dim)
 #ifdef _OPENMP
   omp_lock_t lock;
 #endif
@@ -942,18 +944,45 @@ bool locate_particle(Oracle& o, Particle& P) {
 }
 
 // node.tcc:370-403 (Cartesian constraints)
+// y = M x with M dim x dim row-major
+void mat_vec(int dim, const double* M, const double* x, double* y) {
+  for (int a = 0; a < dim; ++a) {
+    double s = M[a * dim + 0] * x[0];
+    for (int b = 1; b < dim; ++b) s = s + M[a * dim + b] * x[b];
+    y[a] = s;
+  }
+}
+
+// node.tcc:370-403
 void node_apply_velocity_constraints(Oracle& o, Node& n) {
   for (const auto& c : n.vel_c) {
     const unsigned direction = c.first % o.dim;
-    n.vel[direction] = c.second;
-    n.acc[direction] = 0.;
+    if (!n.rotated) {
+      n.vel[direction] = c.second;
+      n.acc[direction] = 0.;
+    } else {
+      double lv[3], la[3];
+      mat_vec(o.dim, n.Ri, n.vel, lv);
+      mat_vec(o.dim, n.Ri, n.acc, la);
+      lv[direction] = c.second;
+      la[direction] = 0.;
+      mat_vec(o.dim, n.R, lv, n.vel);
+      mat_vec(o.dim, n.R, la, n.acc);
+    }
   }
 }
 // node.tcc:456-483
 void node_apply_acceleration_constraints(Oracle& o, Node& n) {
   for (const auto& c : n.acc_c) {
     const unsigned direction = c.first % o.dim;
-    n.acc[direction] = c.second;
+    if (!n.rotated) {
+      n.acc[direction] = c.second;
+    } else {
+      double la[3];
+      mat_vec(o.dim, n.Ri, n.acc, la);
+      la[direction] = c.second;
+      mat_vec(o.dim, n.R, la, n.acc);
+    }
   }
 }
 // node.tcc:510-657 (Cartesian)
@@ -963,11 +992,17 @@ void node_apply_friction_constraints(Oracle& o, Node& n, double dt) {
   const unsigned dir_n = n.fdir;
   const double sign_n = sign(n.fsign);
   const double mu = n.mu;
+  // components in the node's frame (the global ones on a Cartesian boundary)
+  double lacc[3] = {n.acc[0], n.acc[1], n.acc[2]}, lvel[3] = {n.vel[0], n.vel[1], n.vel[2]};
+  if (n.rotated) {
+    mat_vec(o.dim, n.Ri, n.acc, lacc);
+    mat_vec(o.dim, n.Ri, n.vel, lvel);
+  }
   if (o.dim == 2) {
     const unsigned dir_t = (2 - 1) - dir_n;
-    const double acc_n = n.acc[dir_n];
-    double acc_t = n.acc[dir_t];
-    const double vel_t = n.vel[dir_t];
+    const double acc_n = lacc[dir_n];
+    double acc_t = lacc[dir_t];
+    const double vel_t = lvel[dir_t];
     if ((acc_n * sign_n) > 0.0) {
       if (vel_t != 0.0) {
         const double vel_net = dt * acc_t + vel_t;
@@ -982,13 +1017,18 @@ void node_apply_friction_constraints(Oracle& o, Node& n, double dt) {
         else
           acc_t -= sign(acc_t) * mu * std::abs(acc_n);
       }
-      n.acc[dir_t] = acc_t;
+      if (!n.rotated) {
+        n.acc[dir_t] = acc_t;
+      } else {
+        lacc[dir_t] = acc_t;
+        mat_vec(o.dim, n.R, lacc, n.acc);
+      }
     }
   } else {
     static const int dirs[3][2] = {{1, 2}, {0, 2}, {0, 1}};
     const unsigned t0 = dirs[dir_n][0], t1 = dirs[dir_n][1];
     double acc[3], vel[3];
-    for (int i = 0; i < 3; ++i) { acc[i] = n.acc[i]; vel[i] = n.vel[i]; }
+    for (int i = 0; i < 3; ++i) { acc[i] = lacc[i]; vel[i] = lvel[i]; }
     const double acc_n = acc[dir_n];
     double acc_t = std::sqrt(acc[t0] * acc[t0] + acc[t1] * acc[t1]);
     const double vel_t = std::sqrt(vel[t0] * vel[t0] + vel[t1] * vel[t1]);
@@ -1015,7 +1055,10 @@ void node_apply_friction_constraints(Oracle& o, Node& n, double dt) {
           acc[t1] -= mu * std::abs(acc_n) * (acc[t1] / acc_t);
         }
       }
-      for (int i = 0; i < 3; ++i) n.acc[i] = acc[i];
+      if (!n.rotated)
+        for (int i = 0; i < 3; ++i) n.acc[i] = acc[i];
+      else
+        mat_vec(3, n.R, acc, n.acc);
     }
   }
 }
@@ -1543,6 +1586,41 @@ int mpmo_add_friction_constraints(void* h, int64_t n, const int64_t* nid, const 
     nd.fdir = (unsigned)dir[i];
     nd.fsign = sign_n[i];
     nd.mu = mu[i];
+  }
+  return 0;
+}
+
+int mpmo_set_nodal_euler_angles(void* h, int64_t n, const int64_t* nid, const double* angles) {
+  Oracle& o = *(Oracle*)h;
+  const int dim = o.dim;
+  for (int64_t i = 0; i < n; ++i) {
+    if (nid[i] < 0 || nid[i] >= (int64_t)o.nodes.size()) return -1;
+    Node& nd = o.nodes[nid[i]];
+    const double* a = angles + i * dim;
+    // mesh.tcc:1318-1345 rotation_matrix: 2D the rotation by a0 + a1 written
+    // through the angle products, 3D Rz(a0) Rx(a2) Rz(a1)
+    const double c0 = std::cos(a[0]), s0 = std::sin(a[0]), c1 = std::cos(a[1]), s1 = std::sin(a[1]);
+    double R[9];
+    if (dim == 2) {
+      R[0] = c0 * c1 - s0 * s1;
+      R[1] = -(c0 * s1) - s0 * c1;
+      R[2] = s0 * c1 + c0 * s1;
+      R[3] = -(s0 * s1) + c0 * c1;
+    } else {
+      const double c2 = std::cos(a[2]), s2 = std::sin(a[2]);
+      R[0] = c0 * c1 - (s0 * s1) * c2;
+      R[1] = -(c0 * s1) - (s0 * c1) * c2;
+      R[2] = s0 * s2;
+      R[3] = s0 * c1 + (c0 * s1) * c2;
+      R[4] = -(s0 * s1) + (c0 * c1) * c2;
+      R[5] = -(c0 * s2);
+      R[6] = s1 * s2;
+      R[7] = c1 * s2;
+      R[8] = c2;
+    }
+    for (int k = 0; k < dim * dim; ++k) nd.R[k] = R[k];
+    inverse(dim, nd.R, nd.Ri);
+    nd.rotated = true;
   }
   return 0;
 }

@@ -84,6 +84,10 @@ int mpmo_add_acceleration_constraints(void* h, int64_t n, const int64_t* nid,
 int mpmo_add_friction_constraints(void* h, int64_t n, const int64_t* nid,
                                   const int32_t* dir, const int32_t* sign_n,
                                   const double* mu);
+/* General boundaries: dim Euler angles (radians) per node; the node's
+ * velocity, acceleration and friction constraints then act in its rotated
+ * frame (mesh.tcc:1318-1345, node.tcc:370-483, 510-657). */
+int mpmo_set_nodal_euler_angles(void* h, int64_t n, const int64_t* nid, const double* angles);
 /* Particle velocity constraint on a list of particle ids (set id -1 = all). */
 int mpmo_add_particle_velocity_constraint(void* h, int64_t n,
                                           const int64_t* pids, int32_t dir,

@@ -70,6 +70,7 @@ def lib():
             f.argtypes = [vp, i64, pi64, pi32, pd]
         L.mpmo_add_friction_constraints.argtypes = [vp, i64, pi64, pi32, pi32, pd]
         L.mpmo_add_particle_velocity_constraint.argtypes = [vp, i64, pi64, i32, dbl]
+        L.mpmo_set_nodal_euler_angles.argtypes = [vp, i64, pi64, pd]
         L.mpmo_add_particles.argtypes = [vp, i64, pd, i32]
         L.mpmo_initialise.argtypes = [vp]
         L.mpmo_set_particles.argtypes = [vp, C.POINTER(Particles)]
@@ -245,6 +246,11 @@ class Oracle:
         m = np.ascontiguousarray(mu, dtype=np.float64)
         self._check(lib().mpmo_add_friction_constraints(self.h, len(nid), _i64p(nid), _i32p(d),
                                                         _i32p(s), _dp(m)))
+
+    def set_nodal_euler_angles(self, nid, angles):
+        nid = np.ascontiguousarray(nid, dtype=np.int64)
+        a = np.ascontiguousarray(angles, dtype=np.float64)
+        self._check(lib().mpmo_set_nodal_euler_angles(self.h, len(nid), _i64p(nid), _dp(a)))
 
     def add_particle_velocity_constraint(self, pids, direction, value):
         if pids is None:
