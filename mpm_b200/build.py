@@ -65,7 +65,7 @@ def build(force=False, verbose=False):
     # the C++ host driver over the C ABI (reads the reference's input files)
     src = os.path.join(HERE, "host", "mpm_gpu_run.cpp")
     if force or _newer(RUNNER, [src, LIB] + hdrs):
-        cmd = [CXX, "-O2", "-std=c++17", "-Wall", "-I", CSRC, "-I", os.path.join(ROOT, "include"),
+        cmd = [CXX, "-O2", "-std=c++17", "-Wall", "-pthread", "-I", CSRC, "-I", os.path.join(ROOT, "include"),
                src, "-o", RUNNER, "-L", LIBDIR, "-lmpm_b200", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))

@@ -21,6 +21,8 @@
 //
 // --parse-only reads and checks the input and prints a summary without
 // touching a GPU.
+#include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -31,6 +33,8 @@
 #include <map>
 #include <sstream>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "json_lite.hpp"
@@ -100,6 +104,74 @@ std::vector<std::string> data_lines(const std::string& path) {
     out.push_back(line.substr(a));
   }
   return out;
+}
+
+// A reference ASCII data file read whole: the [begin, end) ranges of its data
+// lines (the same lines as data_lines keeps).  The large tables (mesh nodes
+// and cells, particles, particle stresses) are parsed from it row-parallel.
+struct DataFile {
+  std::string text;
+  std::vector<size_t> begin, end;
+  size_t size() const { return begin.size(); }
+};
+
+DataFile read_data_file(const std::string& path) {
+  DataFile df;
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) throw std::runtime_error("cannot open " + path);
+  std::fseek(f, 0, SEEK_END);
+  const long n = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  df.text.resize(n > 0 ? (size_t)n : 0);
+  const size_t got = n > 0 ? std::fread(&df.text[0], 1, (size_t)n, f) : 0;
+  std::fclose(f);
+  if (got != df.text.size()) throw std::runtime_error("cannot read " + path);
+  const char* t = df.text.data();
+  const size_t len = df.text.size();
+  size_t pos = 0;
+  while (pos < len) {
+    const char* nl = static_cast<const char*>(std::memchr(t + pos, '\n', len - pos));
+    const size_t e = nl ? (size_t)(nl - t) : len;
+    size_t a = pos;
+    while (a < e && (t[a] == ' ' || t[a] == '\t' || t[a] == '\r')) ++a;
+    if (a < e && !std::memchr(t + pos, '#', e - pos) && !std::memchr(t + pos, '!', e - pos)) {
+      df.begin.push_back(a);
+      df.end.push_back(e);
+    }
+    pos = e + 1;
+  }
+  return df;
+}
+
+// Reads up to ncols whitespace-separated numbers of one line into out (values
+// left as they are where the line ends early, as operator>> does).
+template <typename T>
+void parse_line(const DataFile& df, size_t line, int ncols, T* out) {
+  const char* p = df.text.data() + df.begin[line];
+  const char* e = df.text.data() + df.end[line];
+  for (int k = 0; k < ncols; ++k) {
+    while (p < e && (*p == ' ' || *p == '\t' || *p == '\r')) ++p;
+    if (p < e && *p == '+') ++p;
+    if (p >= e) return;
+    const auto r = std::from_chars(p, e, out[k]);
+    if (r.ec != std::errc()) return;
+    p = r.ptr;
+  }
+}
+
+// rows [first, first + nrows) of ncols numbers each into out, over all host threads
+template <typename T>
+void parse_rows(const DataFile& df, size_t first, int64_t nrows, int ncols, T* out) {
+  if (first + (size_t)nrows > df.size()) throw std::runtime_error("data file too short");
+  const int64_t nt = std::max<int64_t>(
+      1, std::min<int64_t>(std::thread::hardware_concurrency(), nrows / 4096 + 1));
+  std::vector<std::thread> pool;
+  for (int64_t w = 0; w < nt; ++w)
+    pool.emplace_back([&, w]() {
+      const int64_t a = nrows * w / nt, b = nrows * (w + 1) / nt;
+      for (int64_t i = a; i < b; ++i) parse_line(df, first + (size_t)i, ncols, out + i * ncols);
+    });
+  for (auto& t : pool) t.join();
 }
 
 std::string fmt_double(double v) {
@@ -180,52 +252,42 @@ Input read_input(const std::string& dir, const std::string& file) {
   const Json& mesh = root.at("mesh");
   if (mesh.contains("isoparametric")) in.isoparametric = mesh.at("isoparametric").as_bool();
   {
-    const auto lines = data_lines(join(dir, mesh.at("mesh").as_string()));
-    if (lines.empty()) throw std::runtime_error("empty mesh file");
-    std::istringstream h(lines[0]);
-    h >> in.nnodes >> in.ncells;
+    const DataFile df = read_data_file(join(dir, mesh.at("mesh").as_string()));
+    if (df.size() == 0) throw std::runtime_error("empty mesh file");
+    int64_t hdr[2] = {0, 0};
+    parse_line(df, 0, 2, hdr);
+    in.nnodes = hdr[0];
+    in.ncells = hdr[1];
     const int nv = in.dim == 2 ? 4 : 8;
-    if ((int64_t)lines.size() < 1 + in.nnodes + in.ncells) throw std::runtime_error("mesh file too short");
-    in.coords.resize((size_t)in.nnodes * in.dim);
-    for (int64_t n = 0; n < in.nnodes; ++n) {
-      std::istringstream l(lines[1 + n]);
-      for (int d = 0; d < in.dim; ++d) l >> in.coords[n * in.dim + d];
-    }
-    in.cells.resize((size_t)in.ncells * nv);
-    for (int64_t c = 0; c < in.ncells; ++c) {
-      std::istringstream l(lines[1 + in.nnodes + c]);
-      for (int k = 0; k < nv; ++k) l >> in.cells[c * nv + k];
-    }
+    if ((int64_t)df.size() < 1 + in.nnodes + in.ncells) throw std::runtime_error("mesh file too short");
+    in.coords.assign((size_t)in.nnodes * in.dim, 0.);
+    parse_rows(df, 1, in.nnodes, in.dim, in.coords.data());
+    in.cells.assign((size_t)in.ncells * nv, 0);
+    parse_rows(df, 1 + (size_t)in.nnodes, in.ncells, nv, in.cells.data());
   }
   // particles (a count, then coordinates), one file per generator
   for (const Json& p : root.at("particles").arr) {
     const Json& g = p.at("generator");
     if (g.at("type").as_string() != "file") throw std::runtime_error("particle generator must be a file");
-    const auto lines = data_lines(join(dir, g.at("location").as_string()));
+    const DataFile df = read_data_file(join(dir, g.at("location").as_string()));
+    if (df.size() == 0) throw std::runtime_error("empty particle file");
     Input::PSet ps;
     ps.material = (int)g.at("material_id").as_double();
-    std::istringstream h(lines.at(0));
     int64_t n = 0;
-    h >> n;
-    ps.x.resize((size_t)n * in.dim);
-    for (int64_t i = 0; i < n; ++i) {
-      std::istringstream l(lines.at(1 + i));
-      for (int d = 0; d < in.dim; ++d) l >> ps.x[i * in.dim + d];
-    }
+    parse_line(df, 0, 1, &n);
+    ps.x.assign((size_t)n * in.dim, 0.);
+    parse_rows(df, 1, n, in.dim, ps.x.data());
     in.psets.push_back(std::move(ps));
   }
   if (mesh.contains("particles_stresses")) {
     const Json& ps = mesh.at("particles_stresses");
     if (ps.at("type").as_string() != "file") throw std::runtime_error("only file particle stresses are read");
-    const auto lines = data_lines(join(dir, ps.at("location").as_string()));
-    std::istringstream h(lines.at(0));
+    const DataFile df = read_data_file(join(dir, ps.at("location").as_string()));
+    if (df.size() == 0) throw std::runtime_error("empty particle stress file");
     int64_t n = 0;
-    h >> n;
-    in.stresses.resize((size_t)n * 6);
-    for (int64_t i = 0; i < n; ++i) {
-      std::istringstream l(lines.at(1 + i));
-      for (int k = 0; k < 6; ++k) l >> in.stresses[i * 6 + k];
-    }
+    parse_line(df, 0, 1, &n);
+    in.stresses.assign((size_t)n * 6, 0.);
+    parse_rows(df, 1, n, 6, in.stresses.data());
   }
   if (mesh.contains("boundary_conditions")) {
     const Json& bc = mesh.at("boundary_conditions");
