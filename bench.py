@@ -63,6 +63,15 @@ BYTES_PER_PARTICLE = {
         "p2g": 52,
     },
 }
+# DRAM traffic per particle of the particle kernels as ncu measured it
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch, USL MohrCoulomb
+# column of 1,000,000 particles, step 3), scaled by the particles of a launch
+# for the roofline's "traffic": the 4M-particle launch is too large for a
+# multi-pass capture.
+MEASURED_TRAFFIC_PER_PARTICLE = {
+    ("mixed", 3): {"g2p": 329.7, "p2g": 117.0},
+    ("fp64", 3): {"g2p": 615.4, "p2g": 186.3},
+}
 DTYPES = {"fp64": "f64", "mixed": "f32+f64"}
 FIELDS = ("u", "v", "stress", "strain", "F", "volume", "density")
 
@@ -414,7 +423,11 @@ def main():
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                 "bytes_per_particle": bpp.get(name, 0), "bytes_per_launch": bytes_launch,
-                "avg_launch_ms": avg_s * 1e3, "traffic": None,
+                "avg_launch_ms": avg_s * 1e3,
+                "traffic": (MEASURED_TRAFFIC_PER_PARTICLE.get((args.precision, prob.dim), {})
+                            .get(name, 0.0) * n) or None,
+                "traffic_source": "ncu dram bytes per particle on the 1M-particle column, "
+                                  "scaled to this launch's particles",
                 "kernel_shares": {k: v[0] / total for k, v in prof.items() if v[1]}}
 
     cpu = None
