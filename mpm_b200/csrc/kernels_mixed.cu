@@ -4,9 +4,10 @@
 //   * positions and displacements are stored and advanced in FP64;
 //   * the shape functions use a local coordinate computed in FP64 (x and the
 //     cell centroid are FP64) and then rounded;
-//   * P2G accumulates each cell slot with Kahan-compensated FP32 sums, the node
-//     adds its (at most eight) cell partials in FP64 and divides momentum by
-//     mass in FP64;
+//   * P2G forms each particle's contributions in FP32 and sums them per cell
+//     slot in FP64 (one FP64 add per value costs less than a compensated FP32
+//     sum), the node adds its (at most eight) cell partials in FP64 and divides
+//     momentum by mass in FP64;
 //   * the MohrCoulomb elastic predictor and yield check run in FP32 (stress
 //     invariants in FP64, see mc_invariants); plastic returns, points at the
 //     apex and separated points run in FP64 in a dense second kernel (an FP32
@@ -37,13 +38,6 @@
 
 namespace mpm_b200 {
 namespace {
-
-__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
-  const float y = v - c;
-  const float t = s + y;
-  c = (t - s) - y;
-  s = t;
-}
 
 template <int DIM>
 __device__ __forceinline__ float pmf(const DevState& s, int f, int64_t p) {
@@ -85,7 +79,8 @@ __device__ __forceinline__ void cell_nodes_rel(const DevState& s, int c, int* ni
 // The FP64 path's cell tiles (k_p2g_tiles) in FP32: staged local coordinates
 // (the FP64 local coordinate rounded), mass, velocity, -V0 (1 + P), stress
 // and, off a tensor-product grid, J^-1; per (cell, slot) thread 1 + 3 DIM
-// Kahan-compensated FP32 sums over the cell's particles in id order.
+// FP64 sums of the FP32 contributions of the cell's particles in id order,
+// stored as FP32 partials.
 template <int DIM, int MODE, bool BOX>
 struct MTileRows {
   static constexpr bool MM = MODE != 1, FORCES = MODE != 0;
@@ -124,9 +119,9 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
     if (a1 > a0) box_map = cell_map<DIM, true, float>(s, (int)c, nullptr, nullptr);
   }
   const float gv[3] = {g0, g1, g2};
-  float acc[NVAL], cmp[NVAL];
+  double acc[NVAL];
 #pragma unroll
-  for (int v = 0; v < NVAL; ++v) acc[v] = cmp[v] = 0.f;
+  for (int v = 0; v < NVAL; ++v) acc[v] = 0.;
   for (int64_t q0 = q_begin; q0 < q_end; q0 += T) {
     if (q0 != q_begin) __syncthreads();  // the previous chunk is consumed
     if (q0 + t < q_end) {
@@ -169,9 +164,9 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
       const float m = rows[RW::M][r];
       if constexpr (MM) {
         const float mN = m * N;
-        kahan_add(acc[MASS], cmp[MASS], mN);
+        acc[MASS] += (double)mN;
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) kahan_add(acc[MOM + d], cmp[MOM + d], mN * rows[RW::V + d][r]);
+        for (int d = 0; d < DIM; ++d) acc[MOM + d] += (double)(mN * rows[RW::V + d][r]);
       }
       if constexpr (FORCES) {
         const float sc = rows[RW::SC][r];
@@ -179,7 +174,7 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
 #pragma unroll
         for (int q = 0; q < PF<DIM>::NS; ++q) sig[q] = rows[RW::S + q][r];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) kahan_add(acc[FEXT + d], cmp[FEXT + d], (gv[d] * m) * N);
+        for (int d = 0; d < DIM; ++d) acc[FEXT + d] += (double)((gv[d] * m) * N);
         float Dn[DIM];
         if constexpr (BOX) {
           box_map.grad(G, Dn);
@@ -199,7 +194,7 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
           f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
         }
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) kahan_add(acc[FINT + d], cmp[FINT + d], f[d] * sc);
+        for (int d = 0; d < DIM; ++d) acc[FINT + d] += (double)(f[d] * sc);
       }
     }
   }
@@ -207,11 +202,11 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
   float* out = s.partials_f + ((int64_t)c * NV + k) * NVAL;
   if constexpr (MM) {
 #pragma unroll
-    for (int v = MASS; v < FEXT; ++v) out[v] = acc[v] - cmp[v];
+    for (int v = MASS; v < FEXT; ++v) out[v] = (float)acc[v];
   }
   if constexpr (FORCES) {
 #pragma unroll
-    for (int v = FEXT; v < NVAL; ++v) out[v] = acc[v] - cmp[v];
+    for (int v = FEXT; v < NVAL; ++v) out[v] = (float)acc[v];
   }
 }
 
