@@ -272,8 +272,10 @@ __device__ __forceinline__ void node_accel_update_d(const DevState& s, double m,
     if (fabs(acc[d]) < 1.0E-15) acc[d] = 0.;
 }
 
+// 8 blocks per SM: 0.111 -> 0.108 ms per 1M-node launch (more warps in flight
+// on the scattered partial loads, despite small spills)
 template <int DIM, int MODE>
-__global__ void __launch_bounds__(256) k_nodes_mixed(DevState s, double dt, double damping) {
+__global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, double damping) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= s.nn) return;
   const int64_t nn = s.nn;
