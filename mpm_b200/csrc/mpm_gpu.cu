@@ -7,10 +7,13 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <set>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mpm_gpu.h"
@@ -70,6 +73,33 @@ struct HostBC {
   bool rotated = false;  // general boundary: constraints in the frame of these angles
   double angles[3] = {0, 0, 0};
 };
+
+// f(a, b) over [0, n) split across the host's threads (at least 32768 items a
+// thread); the first exception a worker throws is rethrown here.  For the
+// per-particle conversions between the caller's rows and the device layout.
+template <class F>
+void parallel_for(int64_t n, F f) {
+  const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(hw, n / 32768));
+  if (nt == 1) {
+    f((int64_t)0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  std::exception_ptr err;
+  std::mutex mu;
+  for (int64_t w = 0; w < nt; ++w)
+    pool.emplace_back([&, w]() {
+      try {
+        f(n * w / nt, n * (w + 1) / nt);
+      } catch (...) {
+        std::lock_guard<std::mutex> g(mu);
+        if (!err) err = std::current_exception();
+      }
+    });
+  for (auto& t : pool) t.join();
+  if (err) std::rethrow_exception(err);
+}
 
 }  // namespace
 
@@ -846,7 +876,8 @@ void upload_particle_fields(mpm_gpu_t h, const std::vector<double>& pf, const st
   const LayoutM M = layout_m(dim);
   std::vector<double> px((size_t)h->nfields_x() * np, 0.0);
   std::vector<float> pm((size_t)h->nfields_m() * np, 0.f);
-  for (int64_t p = 0; p < np; ++p) {
+  parallel_for(np, [&](int64_t pa, int64_t pb) {
+  for (int64_t p = pa; p < pb; ++p) {
     auto f = [&](int o) { return pf[(size_t)o * np + p]; };
     for (int d = 0; d < dim; ++d) {
       px[(size_t)(PDX<3>::X + d) * np + p] = f(L.X + d);
@@ -863,12 +894,15 @@ void upload_particle_fields(mpm_gpu_t h, const std::vector<double>& pf, const st
     pm[(size_t)M.JP * np + p] = 0.f;
     pm[(size_t)M.MASS * np + p] = (float)f(L.MASS);
   }
+  });
   h->d_pf.upload(px.data(), px.size(), h->stream);
   h->d_pm.upload(pm.data(), pm.size(), h->stream);
   std::vector<float> svf;
   if (h->any_mc) {
     svf.resize((size_t)SVF_N * np);
-    for (size_t i = 0; i < svf.size(); ++i) svf[i] = (float)sv[i];
+    parallel_for((int64_t)svf.size(), [&](int64_t a, int64_t b) {
+      for (int64_t i = a; i < b; ++i) svf[i] = (float)sv[i];
+    });
     h->d_svf.upload(svf.data(), svf.size(), h->stream);
   }
   ck(cudaStreamSynchronize(h->stream), "sync");
@@ -896,7 +930,8 @@ void download_particle_fields(mpm_gpu_t h, std::vector<double>& pf, std::vector<
   h->d_pm.download(pm.data(), pm.size(), h->stream);
   if (h->any_mc) h->d_svf.download(svf.data(), svf.size(), h->stream);
   ck(cudaStreamSynchronize(h->stream), "sync");
-  for (int64_t p = 0; p < np; ++p) {
+  parallel_for(np, [&](int64_t pa, int64_t pb) {
+  for (int64_t p = pa; p < pb; ++p) {
     auto m = [&](int o) { return (double)pm[(size_t)o * np + p]; };
     auto at = [&](int o) -> double& { return pf[(size_t)o * np + p]; };
     for (int d = 0; d < dim; ++d) {
@@ -916,6 +951,7 @@ void download_particle_fields(mpm_gpu_t h, std::vector<double>& pf, std::vector<
       sv[(size_t)SV_PD * np + p] = px[(size_t)M.PDS * np + p];
     }
   }
+  });
 }
 
 // Pack host particle rows (ABI layout) into the device SoA field order.
@@ -929,7 +965,8 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
   const int E = dim == 2 ? PF<2>::E : PF<3>::E, Fo = dim == 2 ? PF<2>::F : PF<3>::F;
   const int VOL = dim == 2 ? PF<2>::VOL : PF<3>::VOL, RHO = dim == 2 ? PF<2>::RHO : PF<3>::RHO;
   const int MASS = dim == 2 ? PF<2>::MASS : PF<3>::MASS;
-  for (int64_t p = 0; p < np; ++p) {
+  parallel_for(np, [&](int64_t pa, int64_t pb) {
+  for (int64_t p = pa; p < pb; ++p) {
     for (int d = 0; d < dim; ++d) {
       at(X + d, p) = in->x ? in->x[p * 3 + d] : h->p_coords[p * dim + d];
       at(U + d, p) = in->u ? in->u[p * 3 + d] : 0.;
@@ -962,8 +999,10 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
     at(VOL, p) = in->volume ? in->volume[p] : 0.;
     at(MASS, p) = in->mass ? in->mass[p] : at(VOL, p) * at(RHO, p);
   }
+  });
   std::vector<int32_t> cell(ns, -1);
-  for (int64_t p = 0; p < np; ++p) {
+  parallel_for(np, [&](int64_t pa, int64_t pb) {
+  for (int64_t p = pa; p < pb; ++p) {
     if (in->cell) {
       const int64_t c = in->cell[p];
       if (c < -1 || c >= h->ncells) throw InvalidArg("particle cell id out of range");
@@ -972,6 +1011,7 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
       cell[p] = (*cells)[p];
     }
   }
+  });
   h->d_cell.upload(cell.data(), ns, h->stream);
   std::vector<uint16_t> mat(h->p_mat);
   mat.resize(ns, 0);
@@ -979,7 +1019,8 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
   std::vector<double> sv;
   if (h->any_mc) {
     sv.assign((size_t)SV_N * ns, 0.0);
-    for (int64_t p = 0; p < np; ++p) {
+    parallel_for(np, [&](int64_t pa, int64_t pb) {
+    for (int64_t p = pa; p < pb; ++p) {
       const MaterialParams& m = h->mats[h->p_mat[p]];
       double s[SV_N] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       if (in->svars)
@@ -988,6 +1029,7 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
         mc_init_state(m, s);
       for (int k = 0; k < SV_N; ++k) sv[(size_t)k * ns + p] = s[k];
     }
+    });
   }
   upload_particle_fields(h, pf, sv);
   ck(cudaStreamSynchronize(h->stream), "sync");
@@ -1379,11 +1421,13 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
   h->set_np(n);
   h->p_coords.assign(n * h->dim, 0.);
   h->p_mat.resize(n);
-  for (int64_t p = 0; p < n; ++p) {
-    auto it = h->mat_index.find(in->material[p]);
-    if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
-    h->p_mat[p] = (uint16_t)it->second;
-  }
+  parallel_for(n, [&](int64_t a, int64_t b) {
+    for (int64_t p = a; p < b; ++p) {
+      auto it = h->mat_index.find(in->material[p]);
+      if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
+      h->p_mat[p] = (uint16_t)it->second;
+    }
+  });
   h->p_vc.assign(n, {});
   h->ntangent = 0;  // a new state has no tangents
   if ((int64_t)h->p_id.size() != n) {
@@ -1600,7 +1644,8 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   const int E = dim == 2 ? PF<2>::E : PF<3>::E, Fo = dim == 2 ? PF<2>::F : PF<3>::F;
   const int VOL = dim == 2 ? PF<2>::VOL : PF<3>::VOL, RHO = dim == 2 ? PF<2>::RHO : PF<3>::RHO;
   const int MASS = dim == 2 ? PF<2>::MASS : PF<3>::MASS;
-  for (int64_t p = 0; p < np; ++p) {
+  parallel_for(np, [&](int64_t pa, int64_t pb) {
+  for (int64_t p = pa; p < pb; ++p) {
     for (int d = 0; d < 3; ++d) {
       const bool in = d < dim;
       if (out->x) out->x[p * 3 + d] = in ? at(X + d, p) : 0.;
@@ -1647,6 +1692,7 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
     if (out->svars)
       for (int k = 0; k < SV_N; ++k) out->svars[p * SV_N + k] = h->any_mc ? sv[(size_t)k * ns + p] : 0.;
   }
+  });
   MPM_END(h)
   return MPM_OK;
 }
