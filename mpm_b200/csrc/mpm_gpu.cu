@@ -257,6 +257,7 @@ struct mpm_gpu_solver {
   DevBuf<int32_t> d_matid, d_list;
   DevBuf<uint32_t> d_nstate;
   DevBuf<uint8_t> d_stage;
+  DevBuf<double> d_rows;  // the caller's particle rows, staged for the device conversion
   uint8_t* h_stage = nullptr;  // pinned, two halves
   size_t h_stage_bytes = 0;
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
@@ -908,52 +909,6 @@ void upload_particle_fields(mpm_gpu_t h, const std::vector<double>& pf, const st
   ck(cudaStreamSynchronize(h->stream), "sync");
 }
 
-// Download the particle fields into the FP64 layout (inverse of
-// upload_particle_fields).
-void download_particle_fields(mpm_gpu_t h, std::vector<double>& pf, std::vector<double>& sv) {
-  const int64_t np = h->npad;
-  const int dim = h->dim;
-  pf.assign((size_t)h->nfields() * np, 0.0);
-  sv.assign(h->any_mc ? (size_t)SV_N * np : 0, 0.0);
-  if (!h->mixed) {
-    h->d_pf.download(pf.data(), pf.size(), h->stream);
-    if (h->any_mc) h->d_sv.download(sv.data(), sv.size(), h->stream);
-    ck(cudaStreamSynchronize(h->stream), "sync");
-    return;
-  }
-  const Layout L = layout(dim);
-  const LayoutM M = layout_m(dim);
-  std::vector<double> px((size_t)h->nfields_x() * np);
-  std::vector<float> pm((size_t)h->nfields_m() * np);
-  std::vector<float> svf(h->any_mc ? (size_t)SVF_N * np : 0);
-  h->d_pf.download(px.data(), px.size(), h->stream);
-  h->d_pm.download(pm.data(), pm.size(), h->stream);
-  if (h->any_mc) h->d_svf.download(svf.data(), svf.size(), h->stream);
-  ck(cudaStreamSynchronize(h->stream), "sync");
-  parallel_for(np, [&](int64_t pa, int64_t pb) {
-  for (int64_t p = pa; p < pb; ++p) {
-    auto m = [&](int o) { return (double)pm[(size_t)o * np + p]; };
-    auto at = [&](int o) -> double& { return pf[(size_t)o * np + p]; };
-    for (int d = 0; d < dim; ++d) {
-      at(L.X + d) = px[(size_t)d * np + p];
-      at(L.U + d) = px[(size_t)(dim + d) * np + p];
-      at(L.V + d) = m(M.V + d);
-    }
-    for (int k = 0; k < L.NS; ++k) at(L.S + k) = m(M.S + k);
-    for (int k = 0; k < L.NE; ++k) at(L.E + k) = m(M.E + k);
-    for (int k = 0; k < L.NFG; ++k) at(L.F + k) = m(M.H + k) + (identity_entry(dim, k) ? 1. : 0.);
-    const double jp = m(M.JP);
-    at(L.VOL) = m(M.V0) * (1. + jp);
-    at(L.RHO) = m(M.RHO0) / (1. + jp);
-    at(L.MASS) = m(M.MASS);
-    if (h->any_mc) {
-      for (int k = 0; k < SVF_N; ++k) sv[(size_t)k * np + p] = (double)svf[(size_t)k * np + p];
-      sv[(size_t)SV_PD * np + p] = px[(size_t)M.PDS * np + p];
-    }
-  }
-  });
-}
-
 // Pack host particle rows (ABI layout) into the device SoA field order.
 void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<int32_t>* cells) {
   const int dim = h->dim;
@@ -1032,6 +987,70 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
     });
   }
   upload_particle_fields(h, pf, sv);
+  ck(cudaStreamSynchronize(h->stream), "sync");
+}
+
+// The caller's particle arrays (rows as in mpm_gpu_particles) placed one after
+// another in h->d_rows; an array whose pointer is null gets offset -1.
+template <class P>
+RowStage stage_rows(mpm_gpu_t h, int64_t n, P* const (&ptr)[10]) {
+  static constexpr int width[10] = {3, 3, 3, 6, 6, 9, 1, 1, 1, SV_N};
+  int64_t off[10], total = 0;
+  for (int k = 0; k < 10; ++k) {
+    off[k] = ptr[k] ? total : -1;
+    if (ptr[k]) total += (int64_t)width[k] * n;
+  }
+  if ((size_t)total > h->d_rows.n) h->d_rows.alloc((size_t)total);
+  RowStage r{n, h->d_rows.p, off[0], off[1], off[2], off[3], off[4], off[5], off[6], off[7], off[8], off[9]};
+  return r;
+}
+int row_width(int k) {
+  static constexpr int width[10] = {3, 3, 3, 6, 6, 9, 1, 1, 1, SV_N};
+  return width[k];
+}
+
+// Load a full particle state (every field given) with plain copies into the
+// staging buffer and one device kernel that writes the device layout, the
+// same values pack_particles writes.  Cell ids, material slots and the 2D
+// zero-component checks stay on the host.
+void load_rows_device(mpm_gpu_t h, const mpm_gpu_particles* in) {
+  const int dim = h->dim;
+  const int64_t np = h->np, ns = h->npad;
+  if (dim == 2)
+    parallel_for(np, [&](int64_t pa, int64_t pb) {
+      for (int64_t p = pa; p < pb; ++p) {
+        const double *sg = in->stress + p * 6, *ep = in->strain + p * 6, *F = in->F + p * 9;
+        if (sg[4] != 0. || sg[5] != 0.)
+          throw InvalidArg("2D particle stress must have zero yz and xz components");
+        if (ep[2] != 0. || ep[4] != 0. || ep[5] != 0.)
+          throw InvalidArg("2D particle strain must have zero zz, yz and xz components");
+        if (F[2] != 0. || F[5] != 0. || F[6] != 0. || F[7] != 0. || F[8] != 1.)
+          throw InvalidArg("2D deformation gradient must have third row and column (0,0,1)");
+      }
+    });
+  std::vector<int32_t> cell(ns, -1);
+  parallel_for(np, [&](int64_t pa, int64_t pb) {
+    for (int64_t p = pa; p < pb; ++p) {
+      const int64_t c = in->cell[p];
+      if (c < -1 || c >= h->ncells) throw InvalidArg("particle cell id out of range");
+      cell[p] = (int32_t)c;
+    }
+  });
+  h->d_cell.upload(cell.data(), ns, h->stream);
+  std::vector<uint16_t> mat(h->p_mat);
+  mat.resize(ns, 0);
+  h->d_mat.upload(mat.data(), ns, h->stream);
+  const double* const ptr[10] = {in->x, in->u, in->v, in->stress, in->strain, in->F,
+                                 in->volume, in->mass, in->density, h->any_mc ? in->svars : nullptr};
+  const RowStage r = stage_rows(h, np, ptr);
+  const int64_t off[10] = {r.x, r.u, r.v, r.stress, r.strain, r.F, r.volume, r.mass, r.density, r.svars};
+  for (int k = 0; k < 10; ++k)
+    if (ptr[k] && np)
+      ck(cudaMemcpyAsync(r.base + off[k], ptr[k], sizeof(double) * row_width(k) * np,
+                         cudaMemcpyHostToDevice, h->stream), "H2D");
+  refresh_state(h);
+  launch_rows_to_state(dim, h->mixed, h->any_mc, h->ds, r, h->stream);
+  ck(cudaGetLastError(), "rows to state");
   ck(cudaStreamSynchronize(h->stream), "sync");
 }
 
@@ -1439,7 +1458,12 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
   h->aux_dirty = true;
   allocate_particles(h);
   upload_pvc(h);
-  pack_particles(h, in, nullptr);
+  const bool full = in->u && in->v && in->stress && in->strain && in->F && in->mass &&
+                    in->density && (!h->any_mc || in->svars);
+  if (full)
+    load_rows_device(h, in);
+  else
+    pack_particles(h, in, nullptr);
   refresh_state(h);
   ck(cudaStreamSynchronize(h->stream), "sync");
   h->initialised = true;
@@ -1629,70 +1653,31 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   if (!h->initialised) throw InvalidArg("no particles");
   if (!out) throw InvalidArg("null output");
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
-  const int dim = h->dim;
   const int64_t np = h->np;
-  std::vector<double> pf, sv;
-  std::vector<int32_t> cell(np);
-  h->d_cell.download(cell.data(), np, h->stream);
-  download_particle_fields(h, pf, sv);
+  std::vector<int32_t> cell(out->cell ? np : 0);
+  if (out->cell) h->d_cell.download(cell.data(), np, h->stream);
+  // the device writes the requested arrays in the caller's row layout into the
+  // staging buffer; one copy each brings them back
+  double* const ptr[10] = {out->x, out->u, out->v, out->stress, out->strain, out->F,
+                           out->volume, out->mass, out->density, out->svars};
+  const RowStage r = stage_rows(h, np, ptr);
+  launch_state_to_rows(h->dim, h->mixed, h->any_mc, h->ds, r, h->stream);
+  ck(cudaGetLastError(), "state to rows");
+  const int64_t off[10] = {r.x, r.u, r.v, r.stress, r.strain, r.F, r.volume, r.mass, r.density, r.svars};
+  for (int k = 0; k < 10; ++k)
+    if (ptr[k] && np)
+      ck(cudaMemcpyAsync(ptr[k], r.base + off[k], sizeof(double) * row_width(k) * np,
+                         cudaMemcpyDeviceToHost, h->stream), "D2H");
+  ck(cudaStreamSynchronize(h->stream), "sync");
   std::vector<int32_t> slot_id(h->mats.size(), -1);  // material slot -> id
   for (auto& kv : h->mat_index) slot_id[kv.second] = kv.first;
-  const int64_t ns = h->npad;
-  auto at = [&](int f, int64_t p) { return pf[(size_t)f * ns + p]; };
-  const int X = dim == 2 ? PF<2>::X : PF<3>::X, U = dim == 2 ? PF<2>::U : PF<3>::U;
-  const int V = dim == 2 ? PF<2>::V : PF<3>::V, S = dim == 2 ? PF<2>::S : PF<3>::S;
-  const int E = dim == 2 ? PF<2>::E : PF<3>::E, Fo = dim == 2 ? PF<2>::F : PF<3>::F;
-  const int VOL = dim == 2 ? PF<2>::VOL : PF<3>::VOL, RHO = dim == 2 ? PF<2>::RHO : PF<3>::RHO;
-  const int MASS = dim == 2 ? PF<2>::MASS : PF<3>::MASS;
-  parallel_for(np, [&](int64_t pa, int64_t pb) {
-  for (int64_t p = pa; p < pb; ++p) {
-    for (int d = 0; d < 3; ++d) {
-      const bool in = d < dim;
-      if (out->x) out->x[p * 3 + d] = in ? at(X + d, p) : 0.;
-      if (out->u) out->u[p * 3 + d] = in ? at(U + d, p) : 0.;
-      if (out->v) out->v[p * 3 + d] = in ? at(V + d, p) : 0.;
-    }
-    if (dim == 2) {
-      if (out->stress) {
-        for (int k = 0; k < 4; ++k) out->stress[p * 6 + k] = at(S + k, p);
-        out->stress[p * 6 + 4] = out->stress[p * 6 + 5] = 0.;
+  if (out->cell || out->material)
+    parallel_for(np, [&](int64_t pa, int64_t pb) {
+      for (int64_t p = pa; p < pb; ++p) {
+        if (out->cell) out->cell[p] = cell[p];
+        if (out->material) out->material[p] = slot_id[h->p_mat[p]];
       }
-      if (out->strain) {
-        out->strain[p * 6 + 0] = at(E + 0, p);
-        out->strain[p * 6 + 1] = at(E + 1, p);
-        out->strain[p * 6 + 2] = 0.;
-        out->strain[p * 6 + 3] = at(E + 2, p);
-        out->strain[p * 6 + 4] = out->strain[p * 6 + 5] = 0.;
-      }
-      if (out->F) {
-        double* F = out->F + p * 9;
-        F[0] = at(Fo + 0, p);
-        F[1] = at(Fo + 1, p);
-        F[2] = 0.;
-        F[3] = at(Fo + 2, p);
-        F[4] = at(Fo + 3, p);
-        F[5] = 0.;
-        F[6] = 0.;
-        F[7] = 0.;
-        F[8] = 1.;
-      }
-    } else {
-      if (out->stress)
-        for (int k = 0; k < 6; ++k) out->stress[p * 6 + k] = at(S + k, p);
-      if (out->strain)
-        for (int k = 0; k < 6; ++k) out->strain[p * 6 + k] = at(E + k, p);
-      if (out->F)
-        for (int k = 0; k < 9; ++k) out->F[p * 9 + k] = at(Fo + k, p);
-    }
-    if (out->volume) out->volume[p] = at(VOL, p);
-    if (out->density) out->density[p] = at(RHO, p);
-    if (out->mass) out->mass[p] = at(MASS, p);
-    if (out->cell) out->cell[p] = cell[p];
-    if (out->material) out->material[p] = slot_id[h->p_mat[p]];
-    if (out->svars)
-      for (int k = 0; k < SV_N; ++k) out->svars[p * SV_N + k] = h->any_mc ? sv[(size_t)k * ns + p] : 0.;
-  }
-  });
+    });
   MPM_END(h)
   return MPM_OK;
 }

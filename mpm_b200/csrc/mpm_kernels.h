@@ -78,6 +78,22 @@ struct PodAux {                 // per-particle data the step never changes
   const int32_t* material_id;   // [material slot] material id
   const uint32_t* nstate;       // [material slot] number of state variables
 };
+// The C ABI's particle rows (mpm_gpu_particles: x, u, v n x 3; stress,
+// strain n x 6; F n x 9; volume, mass, density n; svars n x 9) staged in one
+// device buffer: the offset of each array in doubles, -1 when absent.  The
+// device converts them to and from its own layout, so that loading and
+// reading a state moves the caller's arrays with plain copies.
+struct RowStage {
+  int64_t n;
+  double* base;
+  int64_t x, u, v, stress, strain, F, volume, mass, density, svars;
+};
+// every array present; the device state's padding rows are zeroed
+void launch_rows_to_state(int dim, bool mixed, bool any_mc, const DevState& s, const RowStage& r,
+                          cudaStream_t st);
+// the present arrays are written for the first r.n particles
+void launch_state_to_rows(int dim, bool mixed, bool any_mc, const DevState& s, const RowStage& r,
+                          cudaStream_t st);
 void launch_pod_pack(int dim, bool mixed, const DevState& s, const PodAux& a, const PodLayout& L,
                      const int32_t* list, int64_t count, uint8_t* out, cudaStream_t st);
 // Tangent (sensitivity) step: material parameters differentiated

@@ -149,6 +149,197 @@ __global__ void __launch_bounds__(256) k_pod_pack(DevState s, PodAux a, PodLayou
 
 }  // namespace
 
+namespace {
+
+// F's storage in the device layout (2D: F00 F01 F10 F11; 3D: row-major 3 x 3)
+// and the matching entries of the caller's row-major 3 x 3
+template <int DIM>
+__device__ __forceinline__ int f_row(int k) {
+  return DIM == 2 ? (k < 2 ? k : k + 1) : k;
+}
+template <int DIM>
+__device__ __forceinline__ bool f_diag(int k) {
+  return DIM == 2 ? (k == 0 || k == 3) : (k % 4 == 0);
+}
+// strain Voigt entries kept in 2D: xx, yy, xy
+__device__ __forceinline__ int e_row2(int k) { return k < 2 ? k : 3; }
+
+template <int DIM, bool MIXED>
+__global__ void __launch_bounds__(256) k_rows_to_state(DevState s, RowStage r, int any_mc) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t ns = s.np;
+  if (p >= ns) return;
+  const bool live = p < r.n;
+  auto row = [&](int64_t off, int w, int k) { return live ? r.base[off + p * w + k] : 0.; };
+  constexpr int NS = PF<DIM>::NS, NE = PF<DIM>::NE, NFG = PF<DIM>::NFG;
+  if constexpr (!MIXED) {
+    double* pf = s.pf;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      pf[(PF<DIM>::X + d) * ns + p] = row(r.x, 3, d);
+      pf[(PF<DIM>::U + d) * ns + p] = row(r.u, 3, d);
+      pf[(PF<DIM>::V + d) * ns + p] = row(r.v, 3, d);
+    }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) pf[(PF<DIM>::S + k) * ns + p] = row(r.stress, 6, k);
+#pragma unroll
+    for (int k = 0; k < NE; ++k)
+      pf[(PF<DIM>::E + k) * ns + p] = row(r.strain, 6, DIM == 2 ? e_row2(k) : k);
+#pragma unroll
+    for (int k = 0; k < NFG; ++k) pf[(PF<DIM>::F + k) * ns + p] = row(r.F, 9, f_row<DIM>(k));
+    pf[PF<DIM>::VOL * ns + p] = row(r.volume, 1, 0);
+    pf[PF<DIM>::RHO * ns + p] = row(r.density, 1, 0);
+    pf[PF<DIM>::MASS * ns + p] = row(r.mass, 1, 0);
+    if (any_mc)
+#pragma unroll
+      for (int k = 0; k < SV_N; ++k) s.sv[(int64_t)k * ns + p] = row(r.svars, 9, k);
+  } else {
+    double* px = s.pf;
+    float* pm = s.pm;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      px[(PDX<DIM>::X + d) * ns + p] = row(r.x, 3, d);
+      px[(PDX<DIM>::U + d) * ns + p] = row(r.u, 3, d);
+      pm[(PM<DIM>::V + d) * ns + p] = (float)row(r.v, 3, d);
+    }
+    px[PDX<DIM>::PDS * ns + p] = any_mc ? row(r.svars, 9, SV_PD) : 0.;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) pm[(PM<DIM>::S + k) * ns + p] = (float)row(r.stress, 6, k);
+#pragma unroll
+    for (int k = 0; k < NE; ++k)
+      pm[(PM<DIM>::E + k) * ns + p] = (float)row(r.strain, 6, DIM == 2 ? e_row2(k) : k);
+#pragma unroll
+    for (int k = 0; k < NFG; ++k)
+      pm[(PM<DIM>::H + k) * ns + p] =
+          (float)(row(r.F, 9, f_row<DIM>(k)) - (f_diag<DIM>(k) ? 1. : 0.));
+    pm[PM<DIM>::V0 * ns + p] = (float)row(r.volume, 1, 0);
+    pm[PM<DIM>::RHO0 * ns + p] = (float)row(r.density, 1, 0);
+    pm[PM<DIM>::JP * ns + p] = 0.f;
+    pm[PM<DIM>::MASS * ns + p] = (float)row(r.mass, 1, 0);
+    if (any_mc)
+#pragma unroll
+      for (int k = 0; k < SVF_N; ++k) s.svf[(int64_t)k * ns + p] = (float)row(r.svars, 9, k);
+  }
+}
+
+template <int DIM, bool MIXED>
+__global__ void __launch_bounds__(256) k_state_to_rows(DevState s, RowStage r, int any_mc) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= r.n) return;
+  const int64_t ns = s.np;
+  double* b = r.base;
+  auto put = [&](int64_t off, int w, int k, double v) {
+    if (off >= 0) b[off + p * w + k] = v;
+  };
+  constexpr int NS = PF<DIM>::NS, NE = PF<DIM>::NE, NFG = PF<DIM>::NFG;
+  // the device fields in FP64 (mixed: FP32 ones widened, as the host reads them)
+  double x[DIM], u[DIM], v[DIM], sg[NS], ep[NE], F[NFG], vol, rho, mass, sv[SV_N];
+  if constexpr (!MIXED) {
+    const double* pf = s.pf;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      x[d] = pf[(PF<DIM>::X + d) * ns + p];
+      u[d] = pf[(PF<DIM>::U + d) * ns + p];
+      v[d] = pf[(PF<DIM>::V + d) * ns + p];
+    }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) sg[k] = pf[(PF<DIM>::S + k) * ns + p];
+#pragma unroll
+    for (int k = 0; k < NE; ++k) ep[k] = pf[(PF<DIM>::E + k) * ns + p];
+#pragma unroll
+    for (int k = 0; k < NFG; ++k) F[k] = pf[(PF<DIM>::F + k) * ns + p];
+    vol = pf[PF<DIM>::VOL * ns + p];
+    rho = pf[PF<DIM>::RHO * ns + p];
+    mass = pf[PF<DIM>::MASS * ns + p];
+#pragma unroll
+    for (int k = 0; k < SV_N; ++k) sv[k] = any_mc ? s.sv[(int64_t)k * ns + p] : 0.;
+  } else {
+    const double* px = s.pf;
+    const float* pm = s.pm;
+    auto m = [&](int f) { return (double)pm[(int64_t)f * ns + p]; };
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      x[d] = px[(PDX<DIM>::X + d) * ns + p];
+      u[d] = px[(PDX<DIM>::U + d) * ns + p];
+      v[d] = m(PM<DIM>::V + d);
+    }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) sg[k] = m(PM<DIM>::S + k);
+#pragma unroll
+    for (int k = 0; k < NE; ++k) ep[k] = m(PM<DIM>::E + k);
+#pragma unroll
+    for (int k = 0; k < NFG; ++k) F[k] = m(PM<DIM>::H + k) + (f_diag<DIM>(k) ? 1. : 0.);
+    const double jp = m(PM<DIM>::JP);
+    vol = m(PM<DIM>::V0) * (1. + jp);
+    rho = m(PM<DIM>::RHO0) / (1. + jp);
+    mass = m(PM<DIM>::MASS);
+#pragma unroll
+    for (int k = 0; k < SV_N; ++k) sv[k] = 0.;
+    if (any_mc) {
+#pragma unroll
+      for (int k = 0; k < SVF_N; ++k) sv[k] = (double)s.svf[(int64_t)k * ns + p];
+      sv[SV_PD] = px[PDX<DIM>::PDS * ns + p];
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    put(r.x, 3, d, d < DIM ? x[d] : 0.);
+    put(r.u, 3, d, d < DIM ? u[d] : 0.);
+    put(r.v, 3, d, d < DIM ? v[d] : 0.);
+  }
+  if constexpr (DIM == 3) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      put(r.stress, 6, k, sg[k]);
+      put(r.strain, 6, k, ep[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) put(r.F, 9, k, F[k]);
+  } else {
+    const double s6[6] = {sg[0], sg[1], sg[2], sg[3], 0., 0.};
+    const double e6[6] = {ep[0], ep[1], 0., ep[2], 0., 0.};
+    const double f9[9] = {F[0], F[1], 0., F[2], F[3], 0., 0., 0., 1.};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      put(r.stress, 6, k, s6[k]);
+      put(r.strain, 6, k, e6[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) put(r.F, 9, k, f9[k]);
+  }
+  put(r.volume, 1, 0, vol);
+  put(r.density, 1, 0, rho);
+  put(r.mass, 1, 0, mass);
+#pragma unroll
+  for (int k = 0; k < SV_N; ++k) put(r.svars, 9, k, sv[k]);
+}
+
+}  // namespace
+
+void launch_rows_to_state(int dim, bool mixed, bool any_mc, const DevState& s, const RowStage& r,
+                          cudaStream_t st) {
+  const unsigned nb = (unsigned)((s.np + 255) / 256);
+  if (nb == 0) return;
+  if (dim == 2)
+    mixed ? k_rows_to_state<2, true><<<nb, 256, 0, st>>>(s, r, any_mc)
+          : k_rows_to_state<2, false><<<nb, 256, 0, st>>>(s, r, any_mc);
+  else
+    mixed ? k_rows_to_state<3, true><<<nb, 256, 0, st>>>(s, r, any_mc)
+          : k_rows_to_state<3, false><<<nb, 256, 0, st>>>(s, r, any_mc);
+}
+
+void launch_state_to_rows(int dim, bool mixed, bool any_mc, const DevState& s, const RowStage& r,
+                          cudaStream_t st) {
+  const unsigned nb = (unsigned)((r.n + 255) / 256);
+  if (nb == 0) return;
+  if (dim == 2)
+    mixed ? k_state_to_rows<2, true><<<nb, 256, 0, st>>>(s, r, any_mc)
+          : k_state_to_rows<2, false><<<nb, 256, 0, st>>>(s, r, any_mc);
+  else
+    mixed ? k_state_to_rows<3, true><<<nb, 256, 0, st>>>(s, r, any_mc)
+          : k_state_to_rows<3, false><<<nb, 256, 0, st>>>(s, r, any_mc);
+}
+
 void launch_pod_pack(int dim, bool mixed, const DevState& s, const PodAux& a, const PodLayout& L,
                      const int32_t* list, int64_t count, uint8_t* out, cudaStream_t st) {
   if (count <= 0) return;
