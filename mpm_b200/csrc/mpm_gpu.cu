@@ -49,6 +49,10 @@ struct DevBuf {
     ck(cudaMalloc(&p, sizeof(T) * count), "cudaMalloc");
     n = count;
   }
+  // keeps the allocation when it already holds exactly count elements
+  void resize(size_t count) {
+    if (count != n || (count && !p)) alloc(count);
+  }
   void free() {
     if (p) cudaFree(p);
     p = nullptr;
@@ -259,6 +263,8 @@ struct mpm_gpu_solver {
   DevBuf<uint8_t> d_stage;
   DevBuf<double> d_rows;  // the caller's particle rows, staged for the device conversion
   uint8_t* h_stage = nullptr;  // pinned, two halves
+  double* h_rows = nullptr;    // pinned copy of the staged particle rows
+  size_t h_rows_n = 0;
   size_t h_stage_bytes = 0;
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
 
@@ -732,35 +738,40 @@ void upload_pvc(mpm_gpu_t h) {
   h->p_vc_dirty = false;
 }
 
+// Particle buffers for h->npad rows; a buffer that already has its size (a
+// state of the same particle count loaded again) is kept.
 void allocate_particles(mpm_gpu_t h) {
   const int64_t np = h->npad;
-  h->d_pf.alloc((size_t)(h->mixed ? h->nfields_x() : h->nfields()) * np);
-  if (h->mixed) h->d_pm.alloc((size_t)h->nfields_m() * np);
-  h->d_cell.alloc(np);
-  h->d_mat.alloc(np);
-  if (h->cfg.scheme == MPM_SCHEME_MUSL) h->d_xnext.alloc((size_t)h->dim * np);
+  h->d_pf.resize((size_t)(h->mixed ? h->nfields_x() : h->nfields()) * np);
+  if (h->mixed) h->d_pm.resize((size_t)h->nfields_m() * np);
+  h->d_cell.resize(np);
+  h->d_mat.resize(np);
+  if (h->cfg.scheme == MPM_SCHEME_MUSL) h->d_xnext.resize((size_t)h->dim * np);
   if (h->cfg.velocity_update >= MPM_VELOCITY_ASFLIP) {
-    h->d_mapb.alloc((size_t)h->dim * h->dim * np);
+    h->d_mapb.resize((size_t)h->dim * h->dim * np);
     ck(cudaMemsetAsync(h->d_mapb.p, 0, sizeof(double) * h->dim * h->dim * np, h->stream),
        "memset");
   }
-  h->d_lost.alloc(std::max<int64_t>(1, np));
-  h->d_rank.alloc(std::max<int64_t>(1, np));
-  h->d_order.alloc(std::max<int64_t>(1, np));
+  h->d_lost.resize(std::max<int64_t>(1, np));
+  h->d_rank.resize(std::max<int64_t>(1, np));
+  h->d_order.resize(std::max<int64_t>(1, np));
   h->any_mc = false;
   for (auto& m : h->mats) h->any_mc = h->any_mc || m.type == 1;
-  h->d_sv.free();
-  h->d_svf.free();
-  h->d_plist.free();
-  h->d_pbuf.free();
   if (h->any_mc) {
-    h->d_plist.alloc(np);
-    h->d_pbuf.alloc((size_t)7 * np);
+    h->d_plist.resize(np);
+    h->d_pbuf.resize((size_t)7 * np);
+  } else {
+    h->d_plist.free();
+    h->d_pbuf.free();
   }
   if (h->any_mc && h->mixed)
-    h->d_svf.alloc((size_t)SVF_N * np);
-  else if (h->any_mc)
-    h->d_sv.alloc((size_t)SV_N * np);
+    h->d_svf.resize((size_t)SVF_N * np);
+  else
+    h->d_svf.free();
+  if (h->any_mc && !h->mixed)
+    h->d_sv.resize((size_t)SV_N * np);
+  else
+    h->d_sv.free();
 }
 
 void refresh_state(mpm_gpu_t h) {
@@ -993,9 +1004,10 @@ void pack_particles(mpm_gpu_t h, const mpm_gpu_particles* in, const std::vector<
 // The caller's particle arrays (rows as in mpm_gpu_particles) placed one after
 // another in h->d_rows; an array whose pointer is null gets offset -1.
 template <class P>
-RowStage stage_rows(mpm_gpu_t h, int64_t n, P* const (&ptr)[10]) {
+RowStage stage_rows(mpm_gpu_t h, int64_t n, P* const (&ptr)[10], int64_t& total) {
   static constexpr int width[10] = {3, 3, 3, 6, 6, 9, 1, 1, 1, SV_N};
-  int64_t off[10], total = 0;
+  int64_t off[10];
+  total = 0;
   for (int k = 0; k < 10; ++k) {
     off[k] = ptr[k] ? total : -1;
     if (ptr[k]) total += (int64_t)width[k] * n;
@@ -1007,6 +1019,29 @@ RowStage stage_rows(mpm_gpu_t h, int64_t n, P* const (&ptr)[10]) {
 int row_width(int k) {
   static constexpr int width[10] = {3, 3, 3, 6, 6, 9, 1, 1, 1, SV_N};
   return width[k];
+}
+
+// A pinned host buffer of at least n doubles for the staged rows, kept by the
+// handle; null when the host cannot pin that much (the copies then go to and
+// from the caller's pageable arrays directly).
+double* pinned_rows(mpm_gpu_t h, int64_t n) {
+  if ((size_t)n <= h->h_rows_n) return h->h_rows;
+  if (h->h_rows) cudaFreeHost(h->h_rows);
+  h->h_rows = nullptr;
+  h->h_rows_n = 0;
+  if (cudaHostAlloc(reinterpret_cast<void**>(&h->h_rows), sizeof(double) * n, cudaHostAllocDefault) !=
+      cudaSuccess) {
+    cudaGetLastError();  // clear the failed allocation's error
+    h->h_rows = nullptr;
+    return nullptr;
+  }
+  h->h_rows_n = (size_t)n;
+  return h->h_rows;
+}
+
+// dst[0, n) = src[0, n) on all host threads
+void parallel_copy(double* dst, const double* src, int64_t n) {
+  parallel_for(n, [&](int64_t a, int64_t b) { std::memcpy(dst + a, src + a, sizeof(double) * (b - a)); });
 }
 
 // Load a full particle state (every field given) with plain copies into the
@@ -1042,12 +1077,20 @@ void load_rows_device(mpm_gpu_t h, const mpm_gpu_particles* in) {
   h->d_mat.upload(mat.data(), ns, h->stream);
   const double* const ptr[10] = {in->x, in->u, in->v, in->stress, in->strain, in->F,
                                  in->volume, in->mass, in->density, h->any_mc ? in->svars : nullptr};
-  const RowStage r = stage_rows(h, np, ptr);
+  int64_t total = 0;
+  const RowStage r = stage_rows(h, np, ptr, total);
   const int64_t off[10] = {r.x, r.u, r.v, r.stress, r.strain, r.F, r.volume, r.mass, r.density, r.svars};
-  for (int k = 0; k < 10; ++k)
-    if (ptr[k] && np)
-      ck(cudaMemcpyAsync(r.base + off[k], ptr[k], sizeof(double) * row_width(k) * np,
-                         cudaMemcpyHostToDevice, h->stream), "H2D");
+  if (double* pin = total ? pinned_rows(h, total) : nullptr) {
+    // gather the rows into pinned memory on all host threads, then one DMA copy
+    for (int k = 0; k < 10; ++k)
+      if (ptr[k]) parallel_copy(pin + off[k], ptr[k], (int64_t)row_width(k) * np);
+    ck(cudaMemcpyAsync(r.base, pin, sizeof(double) * total, cudaMemcpyHostToDevice, h->stream), "H2D");
+  } else {
+    for (int k = 0; k < 10; ++k)
+      if (ptr[k] && np)
+        ck(cudaMemcpyAsync(r.base + off[k], ptr[k], sizeof(double) * row_width(k) * np,
+                           cudaMemcpyHostToDevice, h->stream), "H2D");
+  }
   refresh_state(h);
   launch_rows_to_state(dim, h->mixed, h->any_mc, h->ds, r, h->stream);
   ck(cudaGetLastError(), "rows to state");
@@ -1120,6 +1163,7 @@ int mpm_gpu_destroy(mpm_gpu_t h) {
     cudaStreamDestroy(h->stream);
   }
   if (h->h_stage) cudaFreeHost(h->h_stage);
+  if (h->h_rows) cudaFreeHost(h->h_rows);
   for (auto& e : h->stage_ev)
     if (e) cudaEventDestroy(e);
   if (h->graph) cudaGraphExecDestroy(h->graph);
@@ -1660,15 +1704,24 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   // staging buffer; one copy each brings them back
   double* const ptr[10] = {out->x, out->u, out->v, out->stress, out->strain, out->F,
                            out->volume, out->mass, out->density, out->svars};
-  const RowStage r = stage_rows(h, np, ptr);
+  int64_t total = 0;
+  const RowStage r = stage_rows(h, np, ptr, total);
   launch_state_to_rows(h->dim, h->mixed, h->any_mc, h->ds, r, h->stream);
   ck(cudaGetLastError(), "state to rows");
   const int64_t off[10] = {r.x, r.u, r.v, r.stress, r.strain, r.F, r.volume, r.mass, r.density, r.svars};
-  for (int k = 0; k < 10; ++k)
-    if (ptr[k] && np)
-      ck(cudaMemcpyAsync(ptr[k], r.base + off[k], sizeof(double) * row_width(k) * np,
-                         cudaMemcpyDeviceToHost, h->stream), "D2H");
-  ck(cudaStreamSynchronize(h->stream), "sync");
+  if (double* pin = total ? pinned_rows(h, total) : nullptr) {
+    // one DMA copy into pinned memory, then the rows out on all host threads
+    ck(cudaMemcpyAsync(pin, r.base, sizeof(double) * total, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    for (int k = 0; k < 10; ++k)
+      if (ptr[k]) parallel_copy(ptr[k], pin + off[k], (int64_t)row_width(k) * np);
+  } else {
+    for (int k = 0; k < 10; ++k)
+      if (ptr[k] && np)
+        ck(cudaMemcpyAsync(ptr[k], r.base + off[k], sizeof(double) * row_width(k) * np,
+                           cudaMemcpyDeviceToHost, h->stream), "D2H");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+  }
   std::vector<int32_t> slot_id(h->mats.size(), -1);  // material slot -> id
   for (auto& kv : h->mat_index) slot_id[kv.second] = kv.first;
   if (out->cell || out->material)

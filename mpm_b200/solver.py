@@ -208,8 +208,13 @@ class Solver:
         P = _native.Particles()
         for k in ("x", "u", "v"):
             if k in state:
-                a = np.zeros((n, 3))
-                a[:, :self.dim] = np.asarray(state[k])[:, :self.dim]
+                a = np.asarray(state[k])
+                if a.shape == (n, 3) and self.dim == 3:
+                    a = np.ascontiguousarray(a, dtype=np.float64)
+                else:  # rows of 3 components, zero beyond the solver's dimension
+                    b = np.zeros((n, 3))
+                    b[:, :self.dim] = a[:, :self.dim]
+                    a = b
                 keep[k] = a
                 setattr(P, k, _dp(a))
         for k in ("stress", "strain", "F", "volume", "mass", "density", "svars"):
