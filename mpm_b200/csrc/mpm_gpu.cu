@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <exception>
 #include <map>
 #include <memory>
@@ -1021,9 +1022,9 @@ int row_width(int k) {
   return width[k];
 }
 
-// A pinned host buffer of at least n doubles for the staged rows, kept by the
-// handle; null when the host cannot pin that much (the copies then go to and
-// from the caller's pageable arrays directly).
+// A pinned host buffer of at least n doubles for the staged rows (two chunks),
+// kept by the handle; null when the host cannot pin that much (the copies then
+// go to and from the caller's pageable arrays directly).
 double* pinned_rows(mpm_gpu_t h, int64_t n) {
   if ((size_t)n <= h->h_rows_n) return h->h_rows;
   if (h->h_rows) cudaFreeHost(h->h_rows);
@@ -1042,6 +1043,34 @@ double* pinned_rows(mpm_gpu_t h, int64_t n) {
 // dst[0, n) = src[0, n) on all host threads
 void parallel_copy(double* dst, const double* src, int64_t n) {
   parallel_for(n, [&](int64_t a, int64_t b) { std::memcpy(dst + a, src + a, sizeof(double) * (b - a)); });
+}
+
+// Staged rows move through pinned memory in chunks of ROW_CHUNK doubles (64 MiB),
+// two in flight: the host gathers (or scatters) one chunk on all its threads
+// while the DMA engine copies the other.
+constexpr int64_t ROW_CHUNK = (int64_t)8 << 20;
+
+// The part [lo, hi) of the staged-row index space (the arrays one after another
+// at their offsets) copied between the caller's arrays and buf, which holds
+// index lo at buf[0].
+template <class P>
+void rows_range(P* const (&ptr)[10], const int64_t (&off)[10], int64_t np, int64_t lo, int64_t hi,
+                double* buf, bool gather) {
+  for (int k = 0; k < 10; ++k) {
+    if (!ptr[k]) continue;
+    const int64_t a = off[k], b = a + (int64_t)row_width(k) * np;
+    const int64_t s0 = std::max(a, lo), s1 = std::min(b, hi);
+    if (s0 >= s1) continue;
+    if (gather)
+      parallel_copy(buf + (s0 - lo), ptr[k] + (s0 - a), s1 - s0);
+    else if constexpr (!std::is_const<P>::value)
+      parallel_copy(ptr[k] + (s0 - a), buf + (s0 - lo), s1 - s0);
+  }
+}
+
+void ensure_stage_events(mpm_gpu_t h) {
+  for (auto& e : h->stage_ev)
+    if (!e) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 // Load a full particle state (every field given) with plain copies into the
@@ -1080,11 +1109,20 @@ void load_rows_device(mpm_gpu_t h, const mpm_gpu_particles* in) {
   int64_t total = 0;
   const RowStage r = stage_rows(h, np, ptr, total);
   const int64_t off[10] = {r.x, r.u, r.v, r.stress, r.strain, r.F, r.volume, r.mass, r.density, r.svars};
-  if (double* pin = total ? pinned_rows(h, total) : nullptr) {
-    // gather the rows into pinned memory on all host threads, then one DMA copy
-    for (int k = 0; k < 10; ++k)
-      if (ptr[k]) parallel_copy(pin + off[k], ptr[k], (int64_t)row_width(k) * np);
-    ck(cudaMemcpyAsync(r.base, pin, sizeof(double) * total, cudaMemcpyHostToDevice, h->stream), "H2D");
+  const int64_t chunk = std::min(total, ROW_CHUNK);
+  if (double* pin = total ? pinned_rows(h, 2 * chunk) : nullptr) {
+    ensure_stage_events(h);
+    bool busy[2] = {false, false};
+    int k = 0;
+    for (int64_t lo = 0; lo < total; lo += chunk, k ^= 1) {
+      const int64_t hi = std::min(total, lo + chunk);
+      if (busy[k]) ck(cudaEventSynchronize(h->stage_ev[k]), "row copy");
+      rows_range(ptr, off, np, lo, hi, pin + k * chunk, true);
+      ck(cudaMemcpyAsync(r.base + lo, pin + k * chunk, sizeof(double) * (hi - lo),
+                         cudaMemcpyHostToDevice, h->stream), "H2D");
+      ck(cudaEventRecord(h->stage_ev[k], h->stream), "cudaEventRecord");
+      busy[k] = true;
+    }
   } else {
     for (int k = 0; k < 10; ++k)
       if (ptr[k] && np)
@@ -1709,12 +1747,24 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   launch_state_to_rows(h->dim, h->mixed, h->any_mc, h->ds, r, h->stream);
   ck(cudaGetLastError(), "state to rows");
   const int64_t off[10] = {r.x, r.u, r.v, r.stress, r.strain, r.F, r.volume, r.mass, r.density, r.svars};
-  if (double* pin = total ? pinned_rows(h, total) : nullptr) {
-    // one DMA copy into pinned memory, then the rows out on all host threads
-    ck(cudaMemcpyAsync(pin, r.base, sizeof(double) * total, cudaMemcpyDeviceToHost, h->stream), "D2H");
+  const int64_t chunk = std::min(total, ROW_CHUNK);
+  if (double* pin = total ? pinned_rows(h, 2 * chunk) : nullptr) {
+    ensure_stage_events(h);
+    const int64_t nchunks = (total + chunk - 1) / chunk;
+    auto fetch = [&](int64_t c) {  // DMA of chunk c into half c % 2
+      const int64_t lo = c * chunk, hi = std::min(total, lo + chunk);
+      ck(cudaMemcpyAsync(pin + (c % 2) * chunk, r.base + lo, sizeof(double) * (hi - lo),
+                         cudaMemcpyDeviceToHost, h->stream), "D2H");
+      ck(cudaEventRecord(h->stage_ev[c % 2], h->stream), "cudaEventRecord");
+    };
+    for (int64_t c = 0; c < std::min<int64_t>(2, nchunks); ++c) fetch(c);
+    for (int64_t c = 0; c < nchunks; ++c) {
+      ck(cudaEventSynchronize(h->stage_ev[c % 2]), "row copy");
+      const int64_t lo = c * chunk, hi = std::min(total, lo + chunk);
+      rows_range(ptr, off, np, lo, hi, pin + (c % 2) * chunk, false);
+      if (c + 2 < nchunks) fetch(c + 2);
+    }
     ck(cudaStreamSynchronize(h->stream), "sync");
-    for (int k = 0; k < 10; ++k)
-      if (ptr[k]) parallel_copy(ptr[k], pin + off[k], (int64_t)row_width(k) * np);
   } else {
     for (int k = 0; k < 10; ++k)
       if (ptr[k] && np)

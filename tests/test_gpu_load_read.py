@@ -110,3 +110,34 @@ def test_2d_load_rejects_out_of_plane_components():
     st["stress"][3, 4] = 1.0
     with pytest.raises(RuntimeError, match="zero yz and xz"):
         s.load(st)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_state_larger_than_one_copy_chunk(precision):
+    """512,000 particles: the staged rows (42 doubles a particle) span three
+    64 MiB chunks of the pinned copy pipeline in each direction."""
+    prob = P.column_3d(shape=(80, 80, 40), block=(40, 40, 40))
+    s = P.build_solver(prob, precision=precision)
+    s.step(2)
+    st = s.read()
+    assert len(st["x"]) * 42 * 8 > 2 * (64 << 20)
+    s.load(st)
+    back = s.read()
+    for k in ("x", "u", "v", "stress", "strain", "mass", "cell", "material", "svars"):
+        assert np.array_equal(back[k], st[k]), k
+    for k in ("volume", "density"):  # mixed: read as V0 (1 + P), loaded in FP32
+        want = st[k] if precision == "fp64" else st[k].astype(np.float32).astype(np.float64)
+        assert np.array_equal(back[k], want), k
+    if precision == "fp64":
+        assert np.array_equal(back["F"], st["F"])
+    # a subset read: the arrays' offsets in the staged rows shift
+    from mpm_b200 import _native
+    import ctypes as C
+    n = s.nparticles
+    svars = np.full((n, 9), np.nan)
+    density = np.full(n, np.nan)
+    Pt = _native.Particles()
+    Pt.svars = svars.ctypes.data_as(C.POINTER(C.c_double))
+    Pt.density = density.ctypes.data_as(C.POINTER(C.c_double))
+    assert s.L.mpm_gpu_read_particles(s.h, C.byref(Pt)) == 0
+    assert np.array_equal(svars, back["svars"]) and np.array_equal(density, back["density"])
