@@ -12,10 +12,14 @@ Synthetic seeded inputs.
 One JSON line on stdout (rank 0).  ``value`` is device-timed (CUDA events on
 the solver's stream, state resident in HBM) for the chosen precision (mixed by
 default); ``fp64`` holds the FP64 path timed on the same workload and steps and
-the mixed path's per-field deviation from it; ``e2e`` goes through the public
-API with host arrays (load -> K steps -> read back); ``roofline`` reports the
-dominant kernel's algorithmic bytes per launch over its event-timed average
-duration; ``cpu_baseline`` times the CPU oracle on a bounded sample.
+the mixed path's per-field deviation from it; ``accuracy`` gives that deviation
+at fixed step counts (50, 500, 2000 by default) beside the FP64 path's own
+one-ulp floor, and ``late`` a second timed window after them; ``e2e`` goes
+through the public API with host arrays (load -> K steps -> read back);
+``roofline`` reports the dominant kernel's algorithmic bytes per launch over its
+event-timed average duration, and ``roofline.step`` the whole step's bytes per
+particle-step times the throughput; ``cpu_baseline`` times the CPU oracle on a
+bounded sample.
 Under torchrun (N>1) every rank runs an independent replica ("replicas
 only": the multi-GPU slab decomposition is not built), timing is the max over
 ranks.
@@ -72,6 +76,14 @@ MEASURED_TRAFFIC_PER_PARTICLE = {
     ("mixed", 3): {"g2p": 329.7, "p2g": 117.0},
     ("fp64", 3): {"g2p": 615.4, "p2g": 186.3},
 }
+# Algorithmic bytes per particle-step of the whole step (compulsory particle-state
+# traffic plus one write and one read of each nodal field per active node), for
+# the step-level roofline.  3D MohrCoulomb: FP64 576 particle + 26 grid, mixed
+# 340 + 20.  2D MohrCoulomb: mixed 276 + 25; FP64 reads x u v stress strain F
+# V rho m pdstrain (21 doubles) and the cell, writes 25 doubles and the cell
+# (376) + 25 grid.
+STEP_BYTES_PER_PARTICLE = {("fp64", 3): 602, ("mixed", 3): 360, ("fp64", 2): 401,
+                           ("mixed", 2): 301}
 DTYPES = {"fp64": "f64", "mixed": "f32+f64"}
 FIELDS = ("u", "v", "stress", "strain", "F", "volume", "density")
 
@@ -96,6 +108,10 @@ def parse():
                     help="skip the FP64 run reported beside the mixed one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--accuracy-steps", default="50,500,2000",
+                    help="steps at which the mixed path's deviation from the FP64 path (and "
+                         "the FP64 path's own one-ulp floor) is reported; the last one also "
+                         "starts the late timed window ('' skips both)")
     return ap.parse_args()
 
 
@@ -299,6 +315,52 @@ def field_errors(a, b):
     return out
 
 
+def l2_errors(a, b):
+    """||a - b||_2 / ||b||_2 over all particles and components, per field (F
+    compared as F - I)."""
+    out = {}
+    for k in FIELDS:
+        x, y = np.asarray(a[k], float), np.asarray(b[k], float)
+        if k == "F":
+            x, y = x - np.eye(3).reshape(1, 9), y - np.eye(3).reshape(1, 9)
+        out[k] = float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    return out
+
+
+def accuracy_and_late_window(prob, args, world, dev, checkpoints):
+    """Mixed against FP64 at each checkpoint, beside the floor: FP64 against
+    FP64 started from the initial stress moved by one ulp (the run's own
+    conditioning).  Both max-norm (max |a-b| / max |b|) and L2 errors.  Then
+    a late timed window of K steps on each path, after the last checkpoint."""
+    from mpm_b200 import problems as P
+    mixed = P.build_solver(prob, precision="mixed", device=dev)
+    fp64 = P.build_solver(prob, precision="fp64", device=dev)
+    pert = P.build_solver(prob, precision="fp64", device=dev)
+    st = pert.read()
+    st["stress"] = np.where(st["stress"] == 0.0, 0.0, np.nextafter(st["stress"], np.inf))
+    pert.load(st)
+    rows, done = [], 0
+    for c in checkpoints:
+        for s in (mixed, fp64, pert):
+            s.step(c - done)
+        done = c
+        m, f, q = mixed.read(), fp64.read(), pert.read()
+        rows.append({"step": c, "mixed_vs_fp64_max": field_errors(m, f),
+                     "mixed_vs_fp64_l2": l2_errors(m, f),
+                     "fp64_one_ulp_floor_max": field_errors(q, f),
+                     "fp64_one_ulp_floor_l2": l2_errors(q, f)})
+    del pert
+    barrier(world)
+    ms_m = max_over_ranks(mixed.step_timed(args.steps), world)
+    ms_f = max_over_ranks(fp64.step_timed(args.steps), world)
+    n = mixed.nparticles
+    late = {"after_step": done, "steps": args.steps,
+            "value": world * n * args.steps / (ms_m / 1e3), "ms_per_step": ms_m / args.steps,
+            "fp64": {"value": world * n * args.steps / (ms_f / 1e3),
+                     "ms_per_step": ms_f / args.steps}}
+    return rows, late
+
+
 def run_calibration(args, rank, world):
     """Config D: the FP64 forward run and the run carrying derivatives with
     respect to (E, phi), timed on the device, and the gradient of the loss
@@ -328,9 +390,23 @@ def run_calibration(args, rank, world):
     t.step(args.warmup)
     ms_t = max_over_ranks(t.step_timed(args.steps), world)
     t.close()
+    # the reverse sweep: record (checkpoints every 100 steps) + reverse, on the
+    # host clock (both calls return after their device work has finished)
+    a = build(theta)
+    a.step(args.warmup)
+    ones = np.ones((a.nparticles, 3))
+    t0 = time.perf_counter()
+    a.adjoint_record(args.steps, params, checkpoint_every=min(100, args.steps))
+    a.adjoint_reverse(dL_dx=ones)
+    adj_s = max_over_ranks(time.perf_counter() - t0, world)
+    a.close()
     target = final_x((8e6, 32.0))
     x, J = run_with_sensitivities(build, theta, params, args.steps)
     grad = 2.0 * np.einsum("pd,kpd->k", x - target, J)
+    s_adj = build(theta)
+    _, grad_adj = s_adj.adjoint_run(args.steps, params, target,
+                                    checkpoint_every=min(100, args.steps))
+    s_adj.close()
     fd = []
     for k in range(2):
         h = 1e-6 * theta[k]
@@ -352,8 +428,14 @@ def run_calibration(args, rank, world):
             "forward": {"value": world * n * args.steps / (ms_f / 1e3),
                         "ms_per_step": ms_f / args.steps},
             "tangent_over_forward": ms_t / ms_f,
+            "adjoint": {"seconds": adj_s, "checkpoint_every": min(100, args.steps),
+                        "over_forward": adj_s / (ms_f / 1e3),
+                        "note": "record (forward with checkpoints) + reverse sweep (segment "
+                                "recompute + reverse kernels), host clock around both, against "
+                                "the device time of the plain forward run"},
             "gradient": {"loss": "sum |x_final - x_target|^2, target E=8e6, phi=32",
-                         "at": theta.tolist(), "tangent": grad.tolist(), "central_fd": fd,
+                         "at": theta.tolist(), "tangent": grad.tolist(),
+                         "adjoint": [float(v) for v in grad_adj], "central_fd": fd,
                          "fd_relative_step": 1e-6,
                          "relative_error": [abs(g - d) / max(abs(d), 1e-300)
                                             for g, d in zip(grad, fd)]},
@@ -430,6 +512,18 @@ def main():
                                   "scaled to this launch's particles",
                 "kernel_shares": {k: v[0] / total for k, v in prof.items() if v[1]}}
 
+    # whole-step roofline (bytes per particle-step of the step, not of one kernel)
+    sbytes = STEP_BYTES_PER_PARTICLE[(args.precision, prob.dim)]
+    roofline["step"] = {"bytes_per_particle_step": sbytes,
+                        "achieved": value / world * sbytes / 1e9, "unit": "GB/s",
+                        "frac": value / world * sbytes / 1e9 / peak}
+
+    accuracy, late = None, None
+    checkpoints = [int(v) for v in args.accuracy_steps.split(",") if v.strip()]
+    if checkpoints and args.precision == "mixed" and not args.no_fp64_arm:
+        accuracy, late = accuracy_and_late_window(prob, args, world, dev, checkpoints)
+        late["roofline_step_frac"] = late["value"] / world * sbytes / 1e9 / peak
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "column":
         rate, threads, sample = time_cpu_oracle(args.cpu_sample_seconds)
@@ -459,6 +553,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "setup_s": setup_s},
             "fp64": fp64,
+            "accuracy": accuracy, "late": late,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "kernels": {k: {"total_ms": v[0], "launches": v[1]}
                                        for k, v in prof.items() if v[1]},

@@ -161,6 +161,14 @@ int mpm_gpu_set_nodal_euler_angles(mpm_gpu_t h, int64_t n, const int64_t* node_i
  * (mesh.tcc:2114-2148 read_particles_file / create_particles). */
 int mpm_gpu_add_particles(mpm_gpu_t h, int64_t n, const double* coords, int32_t material_id);
 
+/* Material sets (mpm_base.tcc:448-472 "material_sets" -> Particle::assign_material
+ * on every particle of a set, mesh.tcc:1175-1189): the particles with the given
+ * ids (creation order, from 0) take material material_id; ids without a
+ * particle are skipped, as the reference skips them.  Before
+ * mpm_gpu_initialise, which derives mass and the material state from it. */
+int mpm_gpu_assign_particle_materials(mpm_gpu_t h, int64_t n, const int64_t* pids,
+                                      int32_t material_id);
+
 /* Locate particles, volume = cell volume / particles in cell, mass =
  * volume * density, material state initialised (mpm_base.tcc:347-473,
  * particle.tcc:589-626, mpm_explicit.tcc:94-95).  Uploads the state. */
@@ -244,6 +252,42 @@ int mpm_gpu_set_sensitivities(mpm_gpu_t h, int32_t n, const int32_t* material_id
  * for field 0 x, 1 u, 2 v and c < 6 for field 3 stress (unused components 0). */
 int mpm_gpu_read_sensitivities(mpm_gpu_t h, int32_t field, double* out);
 
+/* Reverse-mode adjoint (no counterpart in the reference): gradients of a
+ * loss on the particles' final positions and velocities with respect to up to
+ * two material parameters (kinds as mpm_gpu_set_sensitivities) and to the
+ * initial positions, velocities and stresses, by the discrete adjoint of the
+ * FP64 USL step (FLIP or PIC, tensor-product grid, non-softening materials):
+ * reverse G2P as a deterministic cell-slot scatter, reverse node update with
+ * its velocity and friction constraints, reverse P2G as a per-particle gather,
+ * and the reverse MohrCoulomb return map (its local Jacobian by forward-mode
+ * passes over the return the forward step ran).  Paths of the forward run:
+ * mpm_explicit.tcc:112-190, particle.tcc:630-657, 893-949, 994-1067,
+ * node.tcc:236-345, 510-657, mohr_coulomb.tcc:348-513.
+ *
+ * mpm_gpu_adjoint_record advances nsteps from the current state like
+ * mpm_gpu_step, keeping the particle state every checkpoint_every steps on the
+ * device (ceil(nsteps / checkpoint_every) checkpoints plus checkpoint_every
+ * states of one segment: about 340 B per particle each in 3D; MPM_ERR_ALLOC
+ * with the size when that does not fit).  mpm_gpu_adjoint_reverse then takes
+ * dL/dx and dL/dv at the end (n*3 rows; either may be NULL for zero), recomputes
+ * each segment from its checkpoint and sweeps back through it, and writes
+ * dL/dparameter (nparams) and, when not NULL, dL/dx0, dL/dv0 (n*3) and
+ * dL/dstress0 (n*6) of the state at the start of the record.  It leaves the
+ * solver at the recorded run's end state and may be called again with other
+ * cotangents.  Nodes lighter than 1e-3 of the mean particle mass pass no
+ * cotangents (as the tangent step passes no derivatives there), so the
+ * gradient equals mpm_gpu_set_sensitivities's. */
+int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every, int32_t nparams,
+                           const int32_t* material_ids, const int32_t* kinds);
+int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_dv,
+                            double* dL_dparams, double* dL_dx0, double* dL_dv0,
+                            double* dL_dstress0);
+/* Both in one call for the calibration loss L = sum over particles in the
+ * mesh of |x_final - x_target|^2 (x_target n*3 rows): *loss and dL/dparameter. */
+int mpm_gpu_adjoint_run(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every, int32_t nparams,
+                        const int32_t* material_ids, const int32_t* kinds, const double* x_target,
+                        double* loss, double* dL_dparams);
+
 /* Set the step counter (the resume step of analysis.resume.step; it drives the
  * gravity ramp, mpm_explicit.tcc:145-153). */
 int mpm_gpu_set_current_step(mpm_gpu_t h, int64_t step);
@@ -266,17 +310,18 @@ int mpm_gpu_material_stress_batch(int32_t device, int32_t dim, const char* type,
                                   double* out);
 
 /* The same constitutive update for callers that cannot allocate device memory
- * (a plugin inside another program's memory arena, code running during a
- * stream capture, a real-time loop with a fixed memory budget).  No
- * counterpart in the reference.  It allocates nothing: the points are staged in
- * a fixed array of the library's device image (32768 points, 7.3 MB, held by
- * every GPU that loads the library until the process exits).  n above 32768
- * is rejected with MPM_ERR_INVALID and a message in err (errlen bytes, may be
- * NULL).  All calls share the array; the entry point serialises its callers
- * with a process-wide lock and waits for its copies, so its calls never
- * overlap.  Its first call on a device looks up the array's address with that
- * device current: make it before any stream capture begins.  Uses the legacy
- * default stream. */
+ * (a plugin inside another program's memory arena, a real-time loop with a
+ * fixed memory budget).  No counterpart in the reference.  It allocates
+ * nothing: the points are staged in a fixed array of the library's device
+ * image (32768 points, 7.3 MB, held by every GPU that loads the library until
+ * the process exits).  n above 32768 is rejected with MPM_ERR_INVALID and a
+ * message in err (errlen bytes, may be NULL).  All calls on a device share
+ * its array; the entry point serialises its callers on that device with a
+ * per-device lock and waits for its copies, so its calls never overlap.  Its
+ * first call on a device looks up the array's address with that device
+ * current and keeps it: make that call before any stream capture begins, and
+ * do not reset the device afterwards.  A blocking call on the legacy default
+ * stream (synchronous copies), not one to make during a stream capture. */
 int mpm_gpu_material_stress_batch_noalloc(int32_t device, int32_t dim, const char* type,
                                           const char* json_props, int64_t n,
                                           const double* stress, const double* dstrain,

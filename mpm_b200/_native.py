@@ -52,6 +52,7 @@ SIGNATURES = {
     "mpm_gpu_add_acceleration_constraints": (C.c_int, [_vp, C.c_int64, _pi64, _pi32, _pd]),
     "mpm_gpu_add_friction_constraints": (C.c_int, [_vp, C.c_int64, _pi64, _pi32, _pi32, _pd]),
     "mpm_gpu_add_particles": (C.c_int, [_vp, C.c_int64, _pd, C.c_int32]),
+    "mpm_gpu_assign_particle_materials": (C.c_int, [_vp, C.c_int64, _pi64, C.c_int32]),
     "mpm_gpu_initialise": (C.c_int, [_vp]),
     "mpm_gpu_assign_particle_stresses": (C.c_int, [_vp, C.c_int64, _pd]),
     "mpm_gpu_add_particle_velocity_constraint": (C.c_int, [_vp, C.c_int64, _pi64, C.c_int32,
@@ -73,6 +74,10 @@ SIGNATURES = {
                                     C.c_int32]),
     "mpm_gpu_load_pod": (C.c_int, [_vp, _vp, C.c_int64, C.c_size_t, _psz, _psz, C.c_int32]),
     "mpm_gpu_set_current_step": (C.c_int, [_vp, C.c_int64]),
+    "mpm_gpu_adjoint_record": (C.c_int, [_vp, C.c_int64, C.c_int64, C.c_int32, _pi32, _pi32]),
+    "mpm_gpu_adjoint_reverse": (C.c_int, [_vp, _pd, _pd, _pd, _pd, _pd, _pd]),
+    "mpm_gpu_adjoint_run": (C.c_int, [_vp, C.c_int64, C.c_int64, C.c_int32, _pi32, _pi32, _pd,
+                                      _pd, _pd]),
     "mpm_gpu_set_sensitivities": (C.c_int, [_vp, C.c_int32, _pi32, _pi32]),
     "mpm_gpu_read_sensitivities": (C.c_int, [_vp, C.c_int32, _pd]),
     "mpm_gpu_device_field": (C.c_int, [_vp, C.c_int32, C.POINTER(_vp), _pi64, _pi32]),

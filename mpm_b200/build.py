@@ -31,6 +31,7 @@ UNITS = [
     ("noalloc.cu", []),
     ("pod.cu", []),
     ("kernels_tangent.cu", ["--fmad=false"]),
+    ("kernels_adjoint.cu", ["--fmad=false"]),
 ]
 HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp", "mpm_device.cuh", "mpm_bulk.cuh", "mpm_dual.cuh"]
 

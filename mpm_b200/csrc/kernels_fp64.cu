@@ -862,7 +862,7 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
     if (mc)
       for (int k = 0; k < SV_N; ++k) bulk::load(svr + k * T, s.sv + k * np + p0, T * 8, &bar[1]);
   }
-  const bool okA = bulk::mbar_wait(&bar[0], 0);
+  const bool okA = bulk::mbar_wait(&bar[0], 0) && !(s.test_wait_timeout && !bulk::mbar_wait_never(&bar[0]));
   const int c = okA ? scell[t] : -1;
   const int64_t p = p0 + t;
   const SmemRow r{rows, svr, t, okA ? (int)smat[t] : 0, p0 + t};
@@ -1307,6 +1307,29 @@ void launch_step_fp64(int dim, const DevState& s, const StepArgs& a, cudaStream_
 }
 
 void counting_sort(const DevState& s, cudaStream_t st) { counting_sort_impl(s, st); }
+
+// The first half of a USL step: sort, P2G of mass, momentum and forces, and the
+// node update (FLIP / PIC mapping velocity), leaving the cell-slot partials and
+// the nodal velocity and acceleration of the step.  The reverse sweep of the
+// adjoint recomputes these from a stored step-start state.
+void launch_p2g_nodes_fp64(int dim, const DevState& s, const StepArgs& a, cudaStream_t st) {
+  if (s.np == 0) return;
+  counting_sort_impl(s, st);
+  auto run = [&](auto dimc, auto boxc) {
+    constexpr int DIM = decltype(dimc)::value;
+    constexpr bool BOX = decltype(boxc)::value;
+    constexpr int TT = p2g_tile_t<BOX, 0>();
+    k_p2g_tiles<DIM, 2, BOX, 0><<<nblocks(s.ncells, TT / Elem<DIM>::NV), TT, 0, st>>>(
+        s, a.g[0], a.g[1], a.g[2]);
+    k_nodes<DIM, 1><<<nblocks(s.nn, 256), 256, 0, st>>>(s, a.dt, a.damping);
+  };
+  if (dim == 2)
+    s.structured ? run(std::integral_constant<int, 2>{}, std::true_type{})
+                 : run(std::integral_constant<int, 2>{}, std::false_type{});
+  else
+    s.structured ? run(std::integral_constant<int, 3>{}, std::true_type{})
+                 : run(std::integral_constant<int, 3>{}, std::false_type{});
+}
 
 void launch_locate_fallback(int dim, const DevState& s, int remove_lost, cudaStream_t st) {
   if (dim == 2)

@@ -676,7 +676,7 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
     if (mc)
       for (int k = 0; k < SVF_N; ++k) bulk::load(svr + k * T, s.svf + k * np + p0, T * 4, &bar[1]);
   }
-  const bool okA = bulk::mbar_wait(&bar[0], 0);
+  const bool okA = bulk::mbar_wait(&bar[0], 0) && !(s.test_wait_timeout && !bulk::mbar_wait_never(&bar[0]));
   const int c = okA ? scell[t] : -1;
   const int64_t p = p0 + t;
   const MSmemRow r{mr, svr, t, okA ? (int)smat[t] : 0, p0 + t};

@@ -59,11 +59,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
 
 // Bounded wait for the phase with the given parity (each try_wait suspends
 // the thread for a hardware-limited time).  False: the copies did not arrive.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (int i = 0; i < (1 << 20); ++i)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int tries = 1 << 20) {
+  for (int i = 0; i < tries; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+
+// Test hook of the wait-timeout path: after phase 0 of `bar` has completed,
+// wait a few tries for phase 1, which no thread or copy ever completes, so
+// the wait runs out exactly as a lost copy would make it.  Every copy of
+// phase 0 has landed by then; the caller's final drain waits for the rest.
+__device__ __forceinline__ bool mbar_wait_never(uint64_t* bar) { return mbar_wait(bar, 1, 16); }
 
 // order this thread's generic-proxy shared-memory writes before later
 // bulk-copy reads of them

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 #include <exception>
@@ -187,6 +188,22 @@ Profiler::~Profiler() {
 
 }  // namespace mpm_b200
 
+// The adjoint's record of a forward run: the particle state every `every`
+// steps (checkpoints), room for the states of one segment between two
+// checkpoints (recomputed during the reverse sweep), the end state, and the
+// reverse sweep's work arrays.
+struct AdjointTape {
+  bool recorded = false;
+  int64_t nsteps = 0, every = 0, step0 = 0, np = 0;
+  int nparams = 0;
+  size_t pf_n = 0, sv_n = 0, cell_n = 0;  // elements of one stored state
+  DevBuf<double> ck_pf, ck_sv, seg_pf, seg_sv, fin_pf, fin_sv;
+  DevBuf<int32_t> ck_cell, seg_cell, fin_cell;
+  DevBuf<double> adj, deps, coef, theta, apart, nbar, sv_seed;
+  DevBuf<unsigned char> mats_zero, mats_param;
+  double mass_floor = 0.0;
+};
+
 struct mpm_gpu_solver {
   mpm_gpu_config cfg{};
   int dim = 3, nv = 8;
@@ -284,6 +301,7 @@ struct mpm_gpu_solver {
       d_partt[MAX_TANGENTS];
   DevBuf<unsigned char> d_mats_t;
   DevBuf<double> d_tpbuf;
+  std::unique_ptr<AdjointTape> tape;  // reverse-mode adjoint (mpm_gpu_adjoint_record)
 
   // mixed precision: d_pf holds [x, u, pdstrain] in FP64, the rest is FP32
   bool mixed = false;
@@ -1184,6 +1202,9 @@ int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out) {
   h->dim = cfg->dim;
   h->nv = cfg->dim == 2 ? 4 : 8;
   h->mixed = cfg->precision == MPM_PRECISION_MIXED;
+  // test hook (MPM_B200_TEST_WAIT_TIMEOUT=1): the staged G2P's first copy wait
+  // runs out on purpose, so the MPM_ERR_TIMEOUT path can be exercised
+  if (const char* e = std::getenv("MPM_B200_TEST_WAIT_TIMEOUT")) h->ds.test_wait_timeout = std::atoi(e) != 0;
   if (cudaSetDevice(cfg->device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete h;
@@ -1412,6 +1433,20 @@ int mpm_gpu_add_particles(mpm_gpu_t h, int64_t n, const double* coords, int32_t 
   h->p_coords.insert(h->p_coords.end(), coords, coords + n * h->dim);
   h->p_mat.insert(h->p_mat.end(), (size_t)n, (uint16_t)it->second);
   h->set_np(h->np + n);
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_assign_particle_materials(mpm_gpu_t h, int64_t n, const int64_t* pids,
+                                      int32_t material_id) {
+  MPM_GUARD(h)
+  if (h->initialised) throw InvalidArg("materials are reassigned before mpm_gpu_initialise");
+  auto it = h->mat_index.find(material_id);
+  if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
+  if (n < 0 || (n > 0 && !pids)) throw InvalidArg("bad particle id array");
+  // ids without a particle are skipped (mesh.tcc:1181-1187)
+  for (int64_t k = 0; k < n; ++k)
+    if (pids[k] >= 0 && pids[k] < h->np) h->p_mat[(size_t)pids[k]] = (uint16_t)it->second;
   MPM_END(h)
   return MPM_OK;
 }
@@ -2236,6 +2271,284 @@ int mpm_gpu_material_stress_batch(int32_t device, int32_t dim, const char* type,
     return MPM_ERR_INVALID;
   }
   return MPM_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ adjoint
+namespace {
+
+StepArgs base_step_args(mpm_gpu_t h) {
+  StepArgs a{};
+  a.scheme = h->cfg.scheme;
+  a.flip = h->cfg.velocity_update == MPM_VELOCITY_FLIP ? 1 : 0;
+  a.vupd = h->cfg.velocity_update;
+  a.remove_lost = h->cfg.locate_particles ? 0 : 1;
+  a.dt = h->cfg.dt;
+  a.beta = h->cfg.blending_ratio;
+  a.damping = h->cfg.damping_factor;
+  return a;
+}
+
+// gravity of solver step `step` (the ramp of mpm_explicit.tcc:145-153, as run_steps)
+void set_gravity(mpm_gpu_t h, StepArgs& a, int64_t step) {
+  double gm = 1.0;
+  if (h->cfg.gravity_ramping_time > 0.0)
+    gm = std::min(1.0, static_cast<double>(step) * h->cfg.dt / h->cfg.gravity_ramping_time);
+  for (int d = 0; d < 3; ++d) a.g[d] = d < h->dim ? gm * h->cfg.gravity[d] : 0.;
+}
+
+void copy_state(mpm_gpu_t h, const AdjointTape& t, double* pf, double* sv, int32_t* cell, bool save) {
+  auto cp = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes) ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream), "D2D");
+  };
+  if (save) {
+    cp(pf, h->d_pf.p, t.pf_n * sizeof(double));
+    cp(sv, h->d_sv.p, t.sv_n * sizeof(double));
+    cp(cell, h->d_cell.p, t.cell_n * sizeof(int32_t));
+  } else {
+    cp(h->d_pf.p, pf, t.pf_n * sizeof(double));
+    cp(h->d_sv.p, sv, t.sv_n * sizeof(double));
+    cp(h->d_cell.p, cell, t.cell_n * sizeof(int32_t));
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every, int32_t nparams,
+                           const int32_t* material_ids, const int32_t* kinds) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("initialise or load particles first");
+  if (nsteps < 1 || checkpoint_every < 1) throw InvalidArg("nsteps and checkpoint_every must be >= 1");
+  if (nparams < 0 || nparams > MAX_TANGENTS) throw InvalidArg("at most 2 parameters");
+  if (nparams > 0 && (!material_ids || !kinds)) throw InvalidArg("null parameter list");
+  if (h->mixed) return fail(h, MPM_ERR_UNSUPPORTED, "the adjoint runs in FP64 only");
+  if (h->cfg.scheme != MPM_SCHEME_USL)
+    return fail(h, MPM_ERR_UNSUPPORTED, "the adjoint follows the USL scheme only");
+  if (h->cfg.velocity_update >= MPM_VELOCITY_ASFLIP)
+    return fail(h, MPM_ERR_UNSUPPORTED, "the adjoint follows the FLIP and PIC updates only");
+  if (!h->structured)
+    return fail(h, MPM_ERR_UNSUPPORTED, "the adjoint runs on tensor-product grids (box cells) only");
+  if (h->ds.any_softening)
+    return fail(h, MPM_ERR_UNSUPPORTED, "the adjoint does not differentiate softening materials");
+  if (h->ntangent > 0) return fail(h, MPM_ERR_UNSUPPORTED, "turn sensitivities off first");
+  std::vector<TangentParam> params(nparams);
+  for (int k = 0; k < nparams; ++k) {
+    auto it = h->mat_index.find(material_ids[k]);
+    if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
+    if (kinds[k] < TP_YOUNGS_MODULUS || kinds[k] > TP_DILATION) throw InvalidArg("unknown parameter kind");
+    if (kinds[k] != TP_YOUNGS_MODULUS && h->mats[it->second].type != 1)
+      throw InvalidArg("friction, cohesion and dilation are MohrCoulomb parameters");
+    params[k] = TangentParam{it->second, kinds[k]};
+  }
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  h->tape.reset(new AdjointTape());
+  AdjointTape& t = *h->tape;
+  t.nsteps = nsteps;
+  t.every = checkpoint_every;
+  t.nparams = nparams;
+  t.np = h->np;
+  t.pf_n = h->d_pf.n;
+  t.sv_n = h->d_sv.n;
+  t.cell_n = h->d_cell.n;
+  const int dim = h->dim;
+  const int64_t np = h->npad;
+  const int64_t nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  const int64_t nseg = std::min(checkpoint_every, nsteps);
+  const int ns = dim == 2 ? PF<2>::NS : PF<3>::NS;
+  const size_t state_bytes = t.pf_n * 8 + t.sv_n * 8 + t.cell_n * 4;
+  const size_t work_bytes = (size_t)np * 8 * ((2 * dim + ns + 1) + 6 + (3 * dim + 6) + MAX_TANGENTS) +
+                            (size_t)h->ncells * h->nv * 2 * dim * 8 + (size_t)h->nnodes * (1 + 3 * dim) * 8;
+  const size_t need = state_bytes * (size_t)(nck + nseg + 1) + work_bytes;
+  size_t free_b = 0, total_b = 0;
+  ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+  if (need > free_b) {
+    h->tape.reset();
+    return fail(h, MPM_ERR_ALLOC, "the adjoint needs " + std::to_string(need >> 20) + " MiB (" +
+                                      std::to_string(nck) + " checkpoints and " + std::to_string(nseg) +
+                                      " segment states); " + std::to_string(free_b >> 20) +
+                                      " MiB are free: raise checkpoint_every towards sqrt(nsteps)");
+  }
+  t.ck_pf.alloc(t.pf_n * nck);
+  t.ck_sv.alloc(t.sv_n * nck);
+  t.ck_cell.alloc(t.cell_n * nck);
+  t.seg_pf.alloc(t.pf_n * nseg);
+  t.seg_sv.alloc(t.sv_n * nseg);
+  t.seg_cell.alloc(t.cell_n * nseg);
+  t.fin_pf.alloc(t.pf_n);
+  t.fin_sv.alloc(t.sv_n);
+  t.fin_cell.alloc(t.cell_n);
+  t.adj.alloc((size_t)(2 * dim + ns + 1) * np);
+  t.deps.alloc((size_t)6 * np);
+  t.coef.alloc((size_t)(3 * dim + 6) * np);
+  t.theta.alloc((size_t)MAX_TANGENTS * np);
+  t.apart.alloc((size_t)h->ncells * h->nv * 2 * dim);
+  t.nbar.alloc((size_t)(1 + 3 * dim) * h->nnodes);
+  // Dual materials: zero derivatives (the return map's Jacobian) and the
+  // parameters' derivatives, with the initial state's parameter derivatives
+  {
+    std::vector<unsigned char> mz(tangent_material_bytes() * h->mats.size()),
+        mp(tangent_material_bytes() * h->mats.size());
+    std::vector<double> seed0((size_t)h->mats.size() * SV_N * MAX_TANGENTS),
+        seed((size_t)h->mats.size() * SV_N * MAX_TANGENTS);
+    make_tangent_materials(h->mats.data(), (int)h->mats.size(), nullptr, 0, mz.data(), seed0.data());
+    make_tangent_materials(h->mats.data(), (int)h->mats.size(), params.data(), nparams, mp.data(),
+                           seed.data());
+    t.mats_zero.upload(mz.data(), mz.size(), h->stream);
+    t.mats_param.upload(mp.data(), mp.size(), h->stream);
+    t.sv_seed.upload(seed.data(), seed.size(), h->stream);
+  }
+  // nodes below 1e-3 of the mean particle mass pass no cotangents (the
+  // tangent step's rule, so the two gradients are the same derivative)
+  {
+    std::vector<double> mass(h->np);
+    const int MASSF = dim == 2 ? PF<2>::MASS : PF<3>::MASS;
+    ck(cudaMemcpyAsync(mass.data(), h->d_pf.p + (size_t)MASSF * np, sizeof(double) * h->np,
+                       cudaMemcpyDeviceToHost, h->stream), "D2H");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    double sum = 0.0;
+    for (double v : mass) sum += v;
+    t.mass_floor = h->np > 0 ? 1e-3 * sum / (double)h->np : 0.0;
+  }
+  t.step0 = h->step;
+  for (int64_t s0 = 0; s0 < nsteps; s0 += checkpoint_every) {
+    const int64_t k = s0 / checkpoint_every;
+    copy_state(h, t, t.ck_pf.p + t.pf_n * k, t.ck_sv.p + t.sv_n * k, t.ck_cell.p + t.cell_n * k, true);
+    const int rc = run_steps(h, std::min(checkpoint_every, nsteps - s0), nullptr);
+    if (rc != MPM_OK) {
+      h->tape.reset();
+      return rc;
+    }
+  }
+  t.recorded = true;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_dv,
+                            double* dL_dparams, double* dL_dx0, double* dL_dv0,
+                            double* dL_dstress0) {
+  MPM_GUARD(h)
+  if (!h->tape || !h->tape->recorded) throw InvalidArg("record a forward run first (mpm_gpu_adjoint_record)");
+  AdjointTape& t = *h->tape;
+  if (h->step != t.step0 + t.nsteps || h->np != t.np || h->d_pf.n != t.pf_n)
+    throw InvalidArg("the state changed since the recorded run");
+  if (!dL_dx && !dL_dv) throw InvalidArg("no terminal cotangent (dL_dx and dL_dv are both null)");
+  if (t.nparams > 0 && !dL_dparams) throw InvalidArg("null dL_dparams");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const int dim = h->dim;
+  const int64_t np = h->npad, n = h->np;
+  const int ns = dim == 2 ? PF<2>::NS : PF<3>::NS;
+  const int AX = 0, AV = dim, AS = 2 * dim, AVOL = 2 * dim + ns, AN = 2 * dim + ns + 1;
+  copy_state(h, t, t.fin_pf.p, t.fin_sv.p, t.fin_cell.p, true);
+  {  // terminal cotangents, rows -> the device layout
+    std::vector<double> a((size_t)AN * np, 0.0);
+    for (int64_t p = 0; p < n; ++p)
+      for (int d = 0; d < dim; ++d) {
+        if (dL_dx) a[(size_t)(AX + d) * np + p] = dL_dx[p * 3 + d];
+        if (dL_dv) a[(size_t)(AV + d) * np + p] = dL_dv[p * 3 + d];
+      }
+    t.adj.upload(a.data(), a.size(), h->stream);
+    ck(cudaMemsetAsync(t.theta.p, 0, sizeof(double) * t.theta.n, h->stream), "memset");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+  }
+  AdjointArgs A;
+  A.adj = t.adj.p;
+  A.deps = t.deps.p;
+  A.coef = t.coef.p;
+  A.theta = t.theta.p;
+  A.apart = t.apart.p;
+  A.nbar = t.nbar.p;
+  A.mats_zero = t.mats_zero.p;
+  A.mats_param = t.mats_param.p;
+  A.sv_seed = t.sv_seed.p;
+  A.nparams = t.nparams;
+  A.mass_floor = t.mass_floor;
+  StepArgs a = base_step_args(h);
+  refresh_state(h);
+  const int64_t nck = (t.nsteps + t.every - 1) / t.every;
+  for (int64_t seg = nck - 1; seg >= 0; --seg) {
+    const int64_t s0 = seg * t.every, s1 = std::min(s0 + t.every, t.nsteps);
+    copy_state(h, t, t.ck_pf.p + t.pf_n * seg, t.ck_sv.p + t.sv_n * seg, t.ck_cell.p + t.cell_n * seg,
+               false);
+    for (int64_t k = s0; k < s1 - 1; ++k) {  // the segment's step-start states
+      const int64_t j = k - s0;
+      copy_state(h, t, t.seg_pf.p + t.pf_n * j, t.seg_sv.p + t.sv_n * j, t.seg_cell.p + t.cell_n * j, true);
+      set_gravity(h, a, t.step0 + k);
+      launch_step_fp64(dim, h->ds, a, h->stream, h->prof);
+    }
+    copy_state(h, t, t.seg_pf.p + t.pf_n * (s1 - 1 - s0), t.seg_sv.p + t.sv_n * (s1 - 1 - s0),
+               t.seg_cell.p + t.cell_n * (s1 - 1 - s0), true);
+    for (int64_t k = s1 - 1; k >= s0; --k) {
+      const int64_t j = k - s0;
+      copy_state(h, t, t.seg_pf.p + t.pf_n * j, t.seg_sv.p + t.sv_n * j, t.seg_cell.p + t.cell_n * j, false);
+      set_gravity(h, a, t.step0 + k);
+      launch_p2g_nodes_fp64(dim, h->ds, a, h->stream);
+      launch_adjoint_step(dim, h->ds, A, a, h->stream);
+    }
+    ck(cudaGetLastError(), "adjoint launch");
+  }
+  std::vector<double> adj((size_t)AN * np), theta((size_t)MAX_TANGENTS * np);
+  t.adj.download(adj.data(), adj.size(), h->stream);
+  t.theta.download(theta.data(), theta.size(), h->stream);
+  unsigned words[2] = {0, 0};
+  ck(cudaMemcpyAsync(words, h->d_words.p, sizeof(words), cudaMemcpyDeviceToHost, h->stream), "D2H");
+  // back to the recorded run's end state
+  copy_state(h, t, t.fin_pf.p, t.fin_sv.p, t.fin_cell.p, false);
+  ck(cudaStreamSynchronize(h->stream), "adjoint");
+  if (words[1] & ERR_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite state in the recomputed run");
+  if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded wait on a device copy ran out");
+  for (int q = 0; q < t.nparams; ++q) {  // particle order: a fixed summation order
+    double sum = 0.0;
+    for (int64_t p = 0; p < n; ++p) sum += theta[(size_t)q * np + p];
+    dL_dparams[q] = sum;
+  }
+  for (int64_t p = 0; p < n; ++p) {
+    for (int d = 0; d < 3; ++d) {
+      if (dL_dx0) dL_dx0[p * 3 + d] = d < dim ? adj[(size_t)(AX + d) * np + p] : 0.0;
+      if (dL_dv0) dL_dv0[p * 3 + d] = d < dim ? adj[(size_t)(AV + d) * np + p] : 0.0;
+    }
+    if (dL_dstress0)
+      for (int k = 0; k < 6; ++k) dL_dstress0[p * 6 + k] = k < ns ? adj[(size_t)(AS + k) * np + p] : 0.0;
+  }
+  (void)AVOL;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_adjoint_run(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every, int32_t nparams,
+                        const int32_t* material_ids, const int32_t* kinds, const double* x_target,
+                        double* loss, double* dL_dparams) {
+  if (!h) return MPM_ERR_INVALID;
+  if (!x_target || !loss) return fail(h, MPM_ERR_INVALID, "null x_target or loss");
+  int rc = mpm_gpu_adjoint_record(h, nsteps, checkpoint_every, nparams, material_ids, kinds);
+  if (rc != MPM_OK) return rc;
+  std::vector<double> g;  // dL/dx at the end of the run
+  MPM_GUARD(h)
+  const int dim = h->dim;
+  const int64_t np = h->npad, n = h->np;
+  std::vector<double> x((size_t)dim * np);
+  const int XF = 0;  // PF<DIM>::X
+  ck(cudaMemcpyAsync(x.data(), h->d_pf.p + (size_t)XF * np, sizeof(double) * dim * np,
+                     cudaMemcpyDeviceToHost, h->stream), "D2H");
+  std::vector<int32_t> cell(np);
+  ck(cudaMemcpyAsync(cell.data(), h->d_cell.p, sizeof(int32_t) * np, cudaMemcpyDeviceToHost, h->stream), "D2H");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  g.assign((size_t)n * 3, 0.0);
+  double L = 0.0;
+  for (int64_t p = 0; p < n; ++p) {
+    if (cell[p] < 0) continue;  // removed particles are not in the loss
+    for (int d = 0; d < dim; ++d) {
+      const double r = x[(size_t)d * np + p] - x_target[p * 3 + d];
+      L += r * r;
+      g[p * 3 + d] = 2.0 * r;
+    }
+  }
+  *loss = L;
+  MPM_END(h)
+  return mpm_gpu_adjoint_reverse(h, g.data(), nullptr, dL_dparams, nullptr, nullptr, nullptr);
 }
 
 }  // extern "C"

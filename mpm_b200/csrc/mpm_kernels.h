@@ -109,6 +109,31 @@ size_t tangent_material_bytes();
 // fills out (nmats MaterialT<Dual>) and sv_seed (nmats x SV_N x MAX_TANGENTS)
 void make_tangent_materials(const MaterialParams* mats, int nmats, const TangentParam* params,
                             int nparams, void* out, double* sv_seed);
+// The first half of a USL step (sort, P2G, node update) on the FP64 path.
+void launch_p2g_nodes_fp64(int dim, const DevState& s, const StepArgs& a, cudaStream_t st);
+
+// Reverse sweep of one FP64 USL step (kernels_adjoint.cu).  The particle
+// cotangents adj ([x~ (DIM), v~ (DIM), sigma~ (NS), V~][np]) hold those of the
+// state after the step on entry and of the state before it on return; theta
+// ([nparams][np]) accumulates each particle's share of dL/dparameter.  The
+// forward sort, P2G and node update of the step must have run on the
+// step-start state (partials, nf, order).
+struct AdjointArgs {
+  double* adj = nullptr;
+  double* deps = nullptr;    // [6][np] cotangent of the strain increment
+  double* coef = nullptr;    // [3 DIM + 6][np] coefficients of the node scatter
+  double* theta = nullptr;   // [NT][np]
+  double* apart = nullptr;   // [ncells][NV][2 DIM] cell-slot sums of v~, a~ of the nodes
+  double* nbar = nullptr;    // [1 + 3 DIM][nn] cotangents of m, p, f_ext, f_int
+  const void* mats_zero = nullptr;   // MaterialT<Dual> per slot, zero derivatives
+  const void* mats_param = nullptr;  // MaterialT<Dual> per slot, derivatives = parameters
+  const double* sv_seed = nullptr;   // [slot][SV_N][NT] d(initial state)/d(parameter)
+  int nparams = 0;
+  double mass_floor = 0.0;           // nodes lighter than this pass no cotangents
+};
+void launch_adjoint_step(int dim, const DevState& s, const AdjointArgs& A, const StepArgs& a,
+                         cudaStream_t st);
+
 void launch_material_batch_fp64(int dim, int64_t n, const MaterialParams& m, const double* stress,
                                 const double* dstrain, const double* density, double* state,
                                 double* out, cudaStream_t st);

@@ -147,6 +147,9 @@ struct DevState {
   const MaterialT<float>* mats_f = nullptr;
 
   int any_softening = 0;          // some MohrCoulomb material softens (phi..tc vary)
+  // test hook: the staged G2P's first copy wait runs out on purpose (after its
+  // copies have landed), exercising the ERR_TIMEOUT path without a fault
+  int test_wait_timeout = 0;
 
   // tangents (derivatives with respect to NT material parameters), each in the
   // layout of its value array; null unless sensitivities are enabled

@@ -3,22 +3,27 @@
 //
 // Some callers cannot call cudaMalloc: a constitutive-model plugin invoked from
 // inside another solver's time loop that owns all device memory through its own
-// arena, code running while a stream is being captured (where an allocation
-// would either be refused or recorded into the graph), or a real-time loop that
-// must not pay for, or fail on, an allocation.  This entry point serves them:
-// the points are staged in one fixed array that is part of the library's device
-// image, so the call allocates nothing.
+// arena (an allocation there would bypass the arena's accounting or fail once
+// it holds the whole device), or a real-time loop that must not pay for, or
+// fail on, an allocation.  This entry point serves them: the points are staged
+// in one fixed array that is part of the library's device image, so the call
+// allocates nothing.  It copies synchronously and launches on the legacy
+// default stream, so it is an ordinary blocking call, not one to make while a
+// stream capture is in progress.
 //
 // The array holds MPM_NOALLOC_MAX_POINTS points (28 doubles each, 7.3 MB).  Every
 // GPU that loads the library holds it until the process exits.  All calls on a
 // device share it and it keeps the previous call's contents: nothing in it has
 // to start at zero (every value the kernel reads is copied in by the same call,
 // and every value returned is written by it).  Calls that overlapped on the GPU
-// would race on the array; this entry point takes a process-wide lock and
-// finishes its copies before returning, so calls made through it never
-// overlap.  The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress) with that device current; make that first call before
-// any stream capture begins.
+// would race on the array; this entry point holds a lock per device and
+// finishes its copies before returning, so calls made through it on one device
+// never overlap (calls on different devices use different copies of the array
+// and run concurrently).  The first call on a device looks up the array's
+// device address (cudaGetSymbolAddress) with that device current and keeps
+// it; make that first call before any stream capture begins, and do not reset
+// the device (cudaDeviceReset) after it, since the reset reloads the device
+// image and can move the array.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -49,7 +54,7 @@ constexpr int64_t kOffStress = 0, kOffDstrain = 6 * kMaxPoints, kOffDensity = 12
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_lock;
+std::mutex g_noalloc_lock[kMaxDevices];    // one per device: its copy of the array
 double* g_noalloc_addr[kMaxDevices] = {};  // device address of the array, per device
 
 void set_err(char* err, int64_t errlen, const std::string& msg) {
@@ -93,7 +98,7 @@ extern "C" int mpm_gpu_material_stress_batch_noalloc(int32_t device, int32_t dim
   }
   if (n == 0) return MPM_OK;
 
-  std::lock_guard<std::mutex> guard(g_noalloc_lock);
+  std::lock_guard<std::mutex> guard(g_noalloc_lock[device]);
   int prev = -1;
   cudaGetDevice(&prev);
   auto fail = [&](cudaError_t e, const char* what) {

@@ -75,6 +75,12 @@ struct Input {
     double v;
   };
   std::vector<PVC> pvcs;
+  struct MatSet {                     // material_sets: every particle of a set takes a material
+    int material;
+    std::vector<int64_t> ids;
+  };
+  std::vector<MatSet> matsets;
+  std::vector<std::string> unsupported;  // input entries outside the explicit single-phase path
   int64_t nparticles() const {
     int64_t n = 0;
     for (auto& p : psets) n += (int64_t)p.x.size() / dim;
@@ -289,8 +295,57 @@ Input read_input(const std::string& dir, const std::string& file) {
     in.stresses.assign((size_t)n * 6, 0.);
     parse_rows(df, 1, n, 6, in.stresses.data());
   }
+  // particle entity sets (mpm_base.tcc:1731-1760, io.cc:159-194): id -> particle ids
+  std::map<long, std::vector<int64_t>> sets;
+  if (mesh.contains("entity_sets")) {
+    const Json es = mpm_b200::parse_json(read_file(join(dir, mesh.at("entity_sets").as_string())));
+    if (es.contains("particle_sets"))
+      for (const Json& s : es.at("particle_sets").arr) {
+        std::vector<int64_t> ids;
+        for (const Json& i : s.at("set").arr) ids.push_back((int64_t)i.as_double());
+        sets[(long)s.at("id").as_double()] = ids;
+      }
+  }
+  // material sets (mpm_base.tcc:448-472): applied before the mass is computed
+  if (root.contains("material_sets") && root.at("material_sets").is_array())
+    for (const Json& m : root.at("material_sets").arr) {
+      if (m.contains("phase_id") && (int)m.at("phase_id").as_double() != 0)
+        throw std::runtime_error("material_sets: only the solid phase (phase_id 0) exists here");
+      const long set = (long)m.at("pset_id").as_double();
+      auto it = sets.find(set);
+      if (it == sets.end()) throw std::runtime_error("material_sets: unknown particle set " + std::to_string(set));
+      in.matsets.push_back({(int)m.at("material_id").as_double(), it->second});
+    }
+  // entries the reference would act on but this explicit single-phase path
+  // does not build: a run refuses them rather than silently dropping a load
+  if (root.contains("external_loading_conditions")) {
+    const Json& el = root.at("external_loading_conditions");
+    for (const char* k : {"particle_surface_traction", "concentrated_nodal_forces", "rotation_forces"})
+      if (el.contains(k) && !(el.at(k).is_array() && el.at(k).arr.empty()))
+        in.unsupported.push_back(std::string("external_loading_conditions.") + k);
+  }
+  if (an.contains("resume") && an.at("resume").contains("resume")) {
+    const Json& r = an.at("resume").at("resume");
+    if ((r.is_bool() && r.as_bool()) || (r.type == Json::String && r.as_string() == "true"))
+      in.unsupported.push_back("analysis.resume (read the checkpoint records with mpm_gpu_load_pod)");
+  }
+  for (const char* k : {"pressure_smoothing", "interface", "pore_pressure_smoothing"})
+    if (an.contains(k) && an.at(k).is_bool() && an.at(k).as_bool())
+      in.unsupported.push_back(std::string("analysis.") + k);
   if (mesh.contains("boundary_conditions")) {
     const Json& bc = mesh.at("boundary_conditions");
+    for (const auto& kv : bc.obj) {
+      const std::string& k = kv.first;
+      if (k != "velocity_constraints" && k != "friction_constraints" && k != "nodal_euler_angles" &&
+          k != "particles_velocity_constraints")
+        in.unsupported.push_back("mesh.boundary_conditions." + k);
+    }
+    // a constraint entry that is not a list of objects makes the reference's
+    // reader throw inside its try block and apply none (mpm_base.tcc:1128-1170,
+    // 1236-1270): warn and apply none as well
+    for (const char* k : {"velocity_constraints", "friction_constraints"})
+      if (bc.contains(k) && !bc.at(k).is_array())
+        std::fprintf(stderr, "mpm_gpu_run: warning: boundary_conditions.%s is not a list; none applied\n", k);
     if (bc.contains("velocity_constraints"))
       for (const Json& v : bc.at("velocity_constraints").arr)
         for (const auto& line : data_lines(join(dir, v.at("file").as_string()))) {
@@ -330,16 +385,6 @@ Input read_input(const std::string& dir, const std::string& file) {
         }
       }
     if (bc.contains("particles_velocity_constraints")) {
-      std::map<long, std::vector<int64_t>> sets;
-      if (mesh.contains("entity_sets")) {
-        const Json es = mpm_b200::parse_json(read_file(join(dir, mesh.at("entity_sets").as_string())));
-        if (es.contains("particle_sets"))
-          for (const Json& s : es.at("particle_sets").arr) {
-            std::vector<int64_t> ids;
-            for (const Json& i : s.at("set").arr) ids.push_back((int64_t)i.as_double());
-            sets[(long)s.at("id").as_double()] = ids;
-          }
-      }
       for (const Json& c : bc.at("particles_velocity_constraints").arr) {
         const long set = (long)c.at("pset_id").as_double();
         Input::PVC p;
@@ -438,11 +483,17 @@ int main(int argc, char** argv) {
   const int64_t np = in.nparticles();
   std::printf("dim %d nodes %lld cells %lld particles %lld materials %zu scheme %s velocity_update %s "
               "dt %g nsteps %ld velocity_constraints %zu friction_constraints %zu "
-              "particle_velocity_constraints %zu stresses %s\n",
+              "particle_velocity_constraints %zu stresses %s material_sets %zu\n",
               in.dim, (long long)in.nnodes, (long long)in.ncells, (long long)np, in.mats.size(),
               in.scheme.c_str(), in.vupdate.c_str(), in.dt, in.nsteps, in.vnid.size(), in.fnid.size(),
-              in.pvcs.size(), in.stresses.empty() ? "no" : "yes");
+              in.pvcs.size(), in.stresses.empty() ? "no" : "yes", in.matsets.size());
+  for (const auto& u : in.unsupported) std::printf("unsupported %s\n", u.c_str());
   if (parse_only) return 0;
+  if (!in.unsupported.empty()) {
+    std::fprintf(stderr, "mpm_gpu_run: unsupported input: %s%s\n", in.unsupported[0].c_str(),
+                 in.unsupported.size() > 1 ? " (and more, see --parse-only)" : "");
+    return 1;
+  }
 
   mpm_gpu_config cfg{};
   cfg.dim = in.dim;
@@ -483,6 +534,9 @@ int main(int argc, char** argv) {
                                             in.eangles.data()), "nodal Euler angles");
   for (auto& p : in.psets)
     check(h, mpm_gpu_add_particles(h, (int64_t)p.x.size() / in.dim, p.x.data(), p.material), "add_particles");
+  for (auto& m : in.matsets)
+    check(h, mpm_gpu_assign_particle_materials(h, (int64_t)m.ids.size(), m.ids.data(), m.material),
+          "material sets");
   check(h, mpm_gpu_initialise(h), "initialise");
   if (!in.stresses.empty())
     check(h, mpm_gpu_assign_particle_stresses(h, (int64_t)in.stresses.size() / 6, in.stresses.data()),

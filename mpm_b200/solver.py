@@ -119,6 +119,12 @@ class Solver:
         coords = np.ascontiguousarray(coords, dtype=np.float64)
         self._ck(self.L.mpm_gpu_add_particles(self.h, coords.shape[0], _dp(coords), material_id))
 
+    def assign_particle_materials(self, pids, material_id):
+        """Material set: the particles with these ids take ``material_id``
+        (before ``initialise``; ids without a particle are skipped)."""
+        p = np.ascontiguousarray(pids, dtype=np.int64)
+        self._ck(self.L.mpm_gpu_assign_particle_materials(self.h, len(p), _i64p(p), material_id))
+
     def initialise(self):
         self._ck(self.L.mpm_gpu_initialise(self.h))
 
@@ -277,6 +283,56 @@ class Solver:
         self._ck(self.L.mpm_gpu_read_sensitivities(self.h, self.SENSITIVITY_FIELDS[field],
                                                    _dp(out)))
         return out if field == "stress" else out[:, :, :self.dim]
+
+    def adjoint_record(self, nsteps, params=(), checkpoint_every=100):
+        """Advance ``nsteps`` keeping checkpoints for the reverse sweep;
+        ``params`` as for ``set_sensitivities``."""
+        n = len(params)
+        mids = np.array([m for m, _ in params], dtype=np.int32)
+        kinds = np.array([self.SENSITIVITY_KINDS[k] for _, k in params], dtype=np.int32)
+        self._ck(self.L.mpm_gpu_adjoint_record(self.h, int(nsteps), int(checkpoint_every), n,
+                                               _i32p(mids), _i32p(kinds)))
+        self._nadj = n
+
+    def adjoint_reverse(self, dL_dx=None, dL_dv=None):
+        """Reverse sweep of the recorded run for terminal cotangents dL/dx,
+        dL/dv (particle rows, dim or 3 columns): a dict with dL/dparameter
+        ("params") and the cotangents of the recorded run's initial state
+        ("x0", "v0": n x dim, "stress0": n x 6)."""
+        n = self.nparticles
+
+        def rows(a):
+            if a is None:
+                return None
+            a = np.asarray(a, dtype=np.float64)
+            b = np.zeros((n, 3))
+            b[:, :a.shape[1]] = a
+            return b
+        gx, gv = rows(dL_dx), rows(dL_dv)
+        out = {"params": np.zeros(max(getattr(self, "_nadj", 0), 1)), "x0": np.zeros((n, 3)),
+               "v0": np.zeros((n, 3)), "stress0": np.zeros((n, 6))}
+        self._ck(self.L.mpm_gpu_adjoint_reverse(
+            self.h, _dp(gx) if gx is not None else None, _dp(gv) if gv is not None else None,
+            _dp(out["params"]), _dp(out["x0"]), _dp(out["v0"]), _dp(out["stress0"])))
+        out["params"] = out["params"][:getattr(self, "_nadj", 0)]
+        out["x0"] = out["x0"][:, :self.dim]
+        out["v0"] = out["v0"][:, :self.dim]
+        return out
+
+    def adjoint_run(self, nsteps, params, x_target, checkpoint_every=100):
+        """(loss, dL/dparameter) of L = sum |x_final - x_target|^2."""
+        n = self.nparticles
+        t = np.zeros((n, 3))
+        t[:, :self.dim] = np.asarray(x_target)[:, :self.dim]
+        mids = np.array([m for m, _ in params], dtype=np.int32)
+        kinds = np.array([self.SENSITIVITY_KINDS[k] for _, k in params], dtype=np.int32)
+        loss = C.c_double()
+        grad = np.zeros(max(len(params), 1))
+        self._ck(self.L.mpm_gpu_adjoint_run(self.h, int(nsteps), int(checkpoint_every),
+                                            len(params), _i32p(mids), _i32p(kinds), _dp(t),
+                                            C.byref(loss), _dp(grad)))
+        self._nadj = len(params)
+        return loss.value, grad[:len(params)]
 
     def set_current_step(self, step):
         self._ck(self.L.mpm_gpu_set_current_step(self.h, int(step)))

@@ -245,7 +245,10 @@ def parse_material_file(path, relpath, kind):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MPM_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_reference_kats.py <geomechanics/mpm source tree> "
+                 "(or set MPM_REFERENCE_ROOT)")
     out = {"generator": "tests/golden/make_reference_kats.py"}
     mc_rel = "tests/materials/mohr_coulomb_test.cc"
     le_rel = "tests/materials/linear_elastic_test.cc"

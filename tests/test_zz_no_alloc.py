@@ -1,14 +1,15 @@
 """The no-allocation constitutive update against the allocating one.
 
 mpm_gpu_material_stress_batch_noalloc serves callers that cannot allocate device
-memory (a plugin inside another program's memory arena, code running during a
-stream capture, a real-time loop with a fixed memory budget).  It stages the
-points in a fixed array of the library's device image instead of allocating.
-Here it is called twice in a row through the C ABI and each result is compared
-with mpm_gpu_material_stress_batch on the same input, within the FP64 parity
-tolerance of the other GPU tests.  The second call is smaller than the first, so
-a result that depended on what the first call left in the shared array would
-show up.  This file is collected last on purpose.
+memory (a plugin inside another program's memory arena, a real-time loop with a
+fixed memory budget).  It stages the points in a fixed array of the library's
+device image instead of allocating.  Here it is called twice in a row through
+the C ABI and each result is compared with mpm_gpu_material_stress_batch on the
+same input, within the FP64 parity tolerance of the other GPU tests; the first
+call is also compared with the CPU oracle's material update, so a fault of the
+shared kernel would not pass unseen.  The second call is smaller than the
+first, so a result that depended on what the first call left in the shared
+array would show up.  This file is collected last on purpose.
 """
 import ctypes as C
 import json
@@ -72,6 +73,11 @@ def test_no_alloc_matches_the_allocating_entry_point_on_two_calls():
     assert rc == 0, msg
     _check(ref1, out1)
     _check(ref_st1, st1)
+    # the oracle's material update on a sample of the same points
+    idx = np.arange(0, 20000, 40)
+    ora = np.array([O.material_stress(3, "MohrCoulomb", mc, s1[i], d1[i], r1[i], st0[i])[0]
+                    for i in idx])
+    _check(ora, out1[idx])
     # second call: 2D LinearElastic, fewer points than the first call left behind
     le = P.linear_elastic(1e6, 0.3, 1800.)
     s2, d2, r2 = _inputs(rng, 777, 2)
