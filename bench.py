@@ -354,10 +354,18 @@ def accuracy_and_late_window(prob, args, world, dev, checkpoints):
     ms_m = max_over_ranks(mixed.step_timed(args.steps), world)
     ms_f = max_over_ranks(fp64.step_timed(args.steps), world)
     n = mixed.nparticles
+
+    def kernels(s):
+        s.set_profiling(True)
+        s.step_timed(args.profile_steps)
+        prof = s.kernel_profile()
+        s.set_profiling(False)
+        return {k: v[0] / v[1] for k, v in prof.items() if v[1]}
     late = {"after_step": done, "steps": args.steps,
             "value": world * n * args.steps / (ms_m / 1e3), "ms_per_step": ms_m / args.steps,
+            "kernels_ms_per_launch": kernels(mixed),
             "fp64": {"value": world * n * args.steps / (ms_f / 1e3),
-                     "ms_per_step": ms_f / args.steps}}
+                     "ms_per_step": ms_f / args.steps, "kernels_ms_per_launch": kernels(fp64)}}
     return rows, late
 
 
@@ -399,6 +407,13 @@ def run_calibration(args, rank, world):
     a.adjoint_record(args.steps, params, checkpoint_every=min(100, args.steps))
     a.adjoint_reverse(dL_dx=ones)
     adj_s = max_over_ranks(time.perf_counter() - t0, world)
+    # the same again with per-kernel events (eager launches)
+    a.set_profiling(True)
+    a.adjoint_record(args.steps, params, checkpoint_every=min(100, args.steps))
+    a.adjoint_reverse(dL_dx=ones)
+    adj_kernels = {k: {"total_ms": v[0], "launches": v[1]} for k, v in a.kernel_profile().items()
+                   if v[1]}
+    a.set_profiling(False)
     a.close()
     target = final_x((8e6, 32.0))
     x, J = run_with_sensitivities(build, theta, params, args.steps)
@@ -429,7 +444,7 @@ def run_calibration(args, rank, world):
                         "ms_per_step": ms_f / args.steps},
             "tangent_over_forward": ms_t / ms_f,
             "adjoint": {"seconds": adj_s, "checkpoint_every": min(100, args.steps),
-                        "over_forward": adj_s / (ms_f / 1e3),
+                        "over_forward": adj_s / (ms_f / 1e3), "kernels": adj_kernels,
                         "note": "record (forward with checkpoints) + reverse sweep (segment "
                                 "recompute + reverse kernels), host clock around both, against "
                                 "the device time of the plain forward run"},

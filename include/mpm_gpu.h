@@ -234,6 +234,34 @@ int mpm_gpu_write_pod(mpm_gpu_t h, void* records, int64_t capacity, int64_t* nre
 int mpm_gpu_load_pod(mpm_gpu_t h, const void* records, int64_t n, size_t record_size,
                      const size_t* offsets, const size_t* sizes, int32_t nfields);
 
+/* The particle output and checkpoint file (Mesh::write_particles_hdf5,
+ * mesh.tcc:1573-1613; Mesh::read_particles_hdf5, mesh.tcc:1663-1720): the
+ * PODParticle records of mpm_gpu_write_pod in the reference's own struct
+ * layout (592-byte records, vtable slot first, pod_particle.h:12-62) written as
+ * the HDF5 table H5TBmake_table makes -- dataset "table", compound type with
+ * the field names and types of pod_particle.cc, chunks of 10000 records, no
+ * compression, attributes CLASS, VERSION, TITLE, FIELD_<i>_NAME -- by the
+ * library's own encoder (no HDF5 library involved).  mpm_gpu_load_hdf5 reads
+ * such a table (by field name) and resumes from it as mpm_gpu_load_pod. */
+int mpm_gpu_write_hdf5(mpm_gpu_t h, const char* path);
+int mpm_gpu_load_hdf5(mpm_gpu_t h, const char* path);
+
+/* The table codec itself.  Field types: */
+enum { MPM_H5_F64 = 0, MPM_H5_I64 = 1, MPM_H5_U64 = 2, MPM_H5_I32 = 3, MPM_H5_U32 = 4,
+       MPM_H5_U8 = 5 };
+/* nrecords records of record_size bytes; field f at offsets[f] with type
+ * types[f] and name names[f]; chunk_records records per chunk (10000 in the
+ * reference). */
+int mpm_h5_write_table(const char* path, const char* title, int64_t nrecords, size_t record_size,
+                       int32_t nfields, const char* const* names, const size_t* offsets,
+                       const int32_t* types, const void* records, int64_t chunk_records);
+/* *nrecords receives the table's record count; with records non-NULL (room for
+ * capacity records of record_size bytes) the named fields are copied to the
+ * given offsets (types must match).  err receives a message (errlen bytes). */
+int mpm_h5_read_table(const char* path, int64_t* nrecords, size_t record_size, int32_t nfields,
+                      const char* const* names, const size_t* offsets, const int32_t* types,
+                      void* records, int64_t capacity, char* err, int64_t errlen);
+
 /* Sensitivities (no counterpart in the reference): derivatives of the whole
  * particle state with respect to up to two material parameters, carried by
  * every step after this call (forward-mode differentiation of the FP64 USL

@@ -87,6 +87,13 @@ SIGNATURES = {
                                                         C.c_char_p, C.c_int64, _pd, _pd, _pd,
                                                         _pd, _pd, C.c_char_p, C.c_int64]),
     "mpm_gpu_version": (C.c_char_p, []),
+    "mpm_gpu_write_hdf5": (C.c_int, [_vp, C.c_char_p]),
+    "mpm_gpu_load_hdf5": (C.c_int, [_vp, C.c_char_p]),
+    "mpm_h5_write_table": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64, C.c_size_t, C.c_int32,
+                                     C.POINTER(C.c_char_p), _psz, _pi32, _vp, C.c_int64]),
+    "mpm_h5_read_table": (C.c_int, [C.c_char_p, _pi64, C.c_size_t, C.c_int32,
+                                    C.POINTER(C.c_char_p), _psz, _pi32, _vp, C.c_int64,
+                                    C.c_char_p, C.c_int64]),
 }
 
 _lib = None

@@ -32,6 +32,7 @@ UNITS = [
     ("pod.cu", []),
     ("kernels_tangent.cu", ["--fmad=false"]),
     ("kernels_adjoint.cu", ["--fmad=false"]),
+    ("h5table.cpp", []),
 ]
 HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp", "mpm_device.cuh", "mpm_bulk.cuh", "mpm_dual.cuh"]
 
@@ -51,7 +52,7 @@ def build(force=False, verbose=False):
     objs = []
     for src, extra in UNITS:
         s = os.path.join(CSRC, src)
-        o = os.path.join(objdir, src.replace(".cu", ".o"))
+        o = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if force or _newer(o, [s] + hdrs):
             cmd = [NVCC] + ARCH + COMMON + extra + ["-c", s, "-o", o]

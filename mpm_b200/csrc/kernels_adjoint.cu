@@ -715,33 +715,46 @@ __global__ void __launch_bounds__(128) k_adj_p2g(DevState s, AdjointArgs A, doub
 }
 
 template <int DIM>
-void adjoint_step(const DevState& s, const AdjointArgs& A, const StepArgs& a, cudaStream_t st) {
+void adjoint_step(const DevState& s, const AdjointArgs& A, const StepArgs& a, cudaStream_t st,
+                  Profiler& pr) {
   constexpr int NV = Elem<DIM>::NV;
   if (s.np == 0) return;
   const unsigned pb = nblk(s.np, 128);
   if (s.sv) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
+  pr.begin(K_ADJ_MATERIAL, st);
   k_adj_material<DIM><<<pb, 128, 0, st>>>(s, A, a.dt);
+  pr.end(K_ADJ_MATERIAL, st);
   if (s.sv) {
+    pr.begin(K_ADJ_RETURN, st);
     const unsigned mcb = (unsigned)std::min<int64_t>(nblk(s.np, 128), 148 * 8);
     k_adj_return<DIM><<<mcb, 128, 0, st>>>(s, A);
+    pr.end(K_ADJ_RETURN, st);
   }
+  pr.begin(K_ADJ_KINEMATICS, st);
   if (a.flip)
     k_adj_kinematics<DIM, true><<<pb, 128, 0, st>>>(s, A, a.dt, a.beta);
   else
     k_adj_kinematics<DIM, false><<<pb, 128, 0, st>>>(s, A, a.dt, a.beta);
+  pr.end(K_ADJ_KINEMATICS, st);
+  pr.begin(K_ADJ_SCATTER, st);
   k_adj_scatter<DIM><<<nblk(s.ncells, 256 / NV), 256, 0, st>>>(s, A);
+  pr.end(K_ADJ_SCATTER, st);
+  pr.begin(K_ADJ_NODES, st);
   k_adj_nodes<DIM><<<nblk(s.nn, 128), 128, 0, st>>>(s, A, a.dt, a.damping);
+  pr.end(K_ADJ_NODES, st);
+  pr.begin(K_ADJ_P2G, st);
   k_adj_p2g<DIM><<<pb, 128, 0, st>>>(s, A, a.g[0], a.g[1], a.g[2]);
+  pr.end(K_ADJ_P2G, st);
 }
 
 }  // namespace
 
 void launch_adjoint_step(int dim, const DevState& s, const AdjointArgs& A, const StepArgs& a,
-                         cudaStream_t st) {
+                         cudaStream_t st, Profiler& prof) {
   if (dim == 2)
-    adjoint_step<2>(s, A, a, st);
+    adjoint_step<2>(s, A, a, st, prof);
   else
-    adjoint_step<3>(s, A, a, st);
+    adjoint_step<3>(s, A, a, st, prof);
 }
 
 }  // namespace mpm_b200

@@ -114,7 +114,10 @@ namespace mpm_b200 {
 const char* kernel_name(int kid) {
   static const char* names[K_NKERNELS] = {"sort",  "p2g",   "nodes_velocity", "stress",
                                           "p2g_forces", "nodes_acceleration", "g2p",
-                                          "mc_return", "locate_fallback"};
+                                          "mc_return", "locate_fallback",
+                                          "adjoint_recompute", "adjoint_material",
+                                          "adjoint_return", "adjoint_kinematics",
+                                          "adjoint_scatter", "adjoint_nodes", "adjoint_p2g"};
   return (kid >= 0 && kid < K_NKERNELS) ? names[kid] : "?";
 }
 
@@ -2485,8 +2488,10 @@ int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_d
       const int64_t j = k - s0;
       copy_state(h, t, t.seg_pf.p + t.pf_n * j, t.seg_sv.p + t.sv_n * j, t.seg_cell.p + t.cell_n * j, false);
       set_gravity(h, a, t.step0 + k);
+      h->prof.begin(K_ADJ_RECOMPUTE, h->stream, SORT_KERNELS + 2);
       launch_p2g_nodes_fp64(dim, h->ds, a, h->stream);
-      launch_adjoint_step(dim, h->ds, A, a, h->stream);
+      h->prof.end(K_ADJ_RECOMPUTE, h->stream);
+      launch_adjoint_step(dim, h->ds, A, a, h->stream, h->prof);
     }
     ck(cudaGetLastError(), "adjoint launch");
   }
@@ -2498,6 +2503,7 @@ int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_d
   // back to the recorded run's end state
   copy_state(h, t, t.fin_pf.p, t.fin_sv.p, t.fin_cell.p, false);
   ck(cudaStreamSynchronize(h->stream), "adjoint");
+  h->prof.collect();
   if (words[1] & ERR_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite state in the recomputed run");
   if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded wait on a device copy ran out");
   for (int q = 0; q < t.nparams; ++q) {  // particle order: a fixed summation order
@@ -2549,6 +2555,99 @@ int mpm_gpu_adjoint_run(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every, i
   *loss = L;
   MPM_END(h)
   return mpm_gpu_adjoint_reverse(h, g.data(), nullptr, dL_dparams, nullptr, nullptr, nullptr);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ HDF5 particle table
+namespace {
+
+// The reference's PODParticle (pod_particle.h:12-62) as its compiler lays it
+// out: a vtable pointer first (the struct has a virtual destructor), then the
+// data members at natural alignment; 592 bytes.  Field names and HDF5 types of
+// pod_particle.cc (id and cell_id H5T_NATIVE_LLONG, the two flags
+// H5T_NATIVE_HBOOL, material_id and nstate_vars H5T_NATIVE_UINT).
+struct RefPod {
+  size_t size = 592;
+  std::vector<std::string> names;
+  std::vector<const char*> cnames;
+  size_t off[POD_NFIELDS], sz[POD_NFIELDS];
+  int32_t type[POD_NFIELDS];
+  RefPod() {
+    size_t o = 8;  // vtable pointer
+    int f = 0;
+    auto add = [&](const std::string& n, size_t s, int t) {
+      o = (o + s - 1) / s * s;
+      names.push_back(n);
+      off[f] = o;
+      sz[f] = s;
+      type[f] = t;
+      o += s;
+      ++f;
+    };
+    add("id", 8, MPM_H5_I64);
+    for (const char* n : {"mass", "volume", "pressure"}) add(n, 8, MPM_H5_F64);
+    for (const char* v : {"coord", "displacement", "nsize", "velocity", "acceleration"})
+      for (const char* c : {"_x", "_y", "_z"}) add(std::string(v) + c, 8, MPM_H5_F64);
+    for (const char* n : {"stress_xx", "stress_yy", "stress_zz", "tau_xy", "tau_yz", "tau_xz",
+                          "strain_xx", "strain_yy", "strain_zz", "gamma_xy", "gamma_yz", "gamma_xz"})
+      add(n, 8, MPM_H5_F64);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) add("defgrad_" + std::to_string(i) + std::to_string(j), 8, MPM_H5_F64);
+    add("initialise_mapping_matrix", 1, MPM_H5_U8);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        add("mapping_matrix_" + std::to_string(i) + std::to_string(j), 8, MPM_H5_F64);
+    add("status", 1, MPM_H5_U8);
+    add("cell_id", 8, MPM_H5_I64);
+    add("material_id", 4, MPM_H5_U32);
+    add("nstate_vars", 4, MPM_H5_U32);
+    for (int k = 0; k < 20; ++k) add("svars_" + std::to_string(k), 8, MPM_H5_F64);
+    for (auto& n : names) cnames.push_back(n.c_str());
+  }
+};
+
+const RefPod& ref_pod() {
+  static const RefPod r;
+  return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mpm_gpu_write_hdf5(mpm_gpu_t h, const char* path) {
+  MPM_GUARD(h)
+  if (!path) throw InvalidArg("null path");
+  const RefPod& L = ref_pod();
+  std::vector<uint8_t> rec((size_t)h->np * L.size, 0);
+  int64_t n = 0;
+  const int rc = mpm_gpu_write_pod(h, rec.data(), h->np, &n, L.size, L.off, L.sz, POD_NFIELDS);
+  if (rc != MPM_OK) return rc;
+  // H5TBmake_table("Table Title", file, "table", ..., chunk_size 10000, no fill, no compression)
+  if (mpm_h5_write_table(path, "Table Title", n, L.size, POD_NFIELDS, L.cnames.data(), L.off, L.type,
+                         rec.data(), 10000) != MPM_OK)
+    throw InvalidArg(std::string("cannot write ") + path);
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_load_hdf5(mpm_gpu_t h, const char* path) {
+  const RefPod& L = ref_pod();
+  std::vector<uint8_t> rec;
+  int64_t n = 0;
+  MPM_GUARD(h)
+  if (!path) throw InvalidArg("null path");
+  char err[256] = {0};
+  if (mpm_h5_read_table(path, &n, L.size, POD_NFIELDS, L.cnames.data(), L.off, L.type, nullptr, 0,
+                        err, sizeof(err)) != MPM_OK)
+    throw InvalidArg(err);
+  rec.assign((size_t)n * L.size, 0);
+  if (mpm_h5_read_table(path, &n, L.size, POD_NFIELDS, L.cnames.data(), L.off, L.type, rec.data(), n,
+                        err, sizeof(err)) != MPM_OK)
+    throw InvalidArg(err);
+  MPM_END(h)
+  return mpm_gpu_load_pod(h, rec.data(), n, L.size, L.off, L.sz, POD_NFIELDS);
 }
 
 }  // extern "C"

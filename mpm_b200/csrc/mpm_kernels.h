@@ -32,6 +32,14 @@ enum KernelId {
   K_G2P,            // G2P (+ USL stress update) + locate
   K_MC_RETURN,      // MohrCoulomb plastic returns deferred by the stress update
   K_LOCATE,         // exhaustive locate for particles that left their neighbourhood
+  // the adjoint's reverse sweep
+  K_ADJ_RECOMPUTE,  // sort, P2G and node update recomputed from the stored state
+  K_ADJ_MATERIAL,   // elastic material reverse, plastic points listed
+  K_ADJ_RETURN,     // plastic return-map reverse
+  K_ADJ_KINEMATICS, // G2P reverse
+  K_ADJ_SCATTER,    // node cotangents as cell-slot sums
+  K_ADJ_NODES,      // node update reverse
+  K_ADJ_P2G,        // P2G reverse (gather)
   K_NKERNELS
 };
 constexpr int SCAN_BLOCK = 4096;  // cells per block of the counting-sort scan
@@ -132,7 +140,7 @@ struct AdjointArgs {
   double mass_floor = 0.0;           // nodes lighter than this pass no cotangents
 };
 void launch_adjoint_step(int dim, const DevState& s, const AdjointArgs& A, const StepArgs& a,
-                         cudaStream_t st);
+                         cudaStream_t st, Profiler& prof);
 
 void launch_material_batch_fp64(int dim, int64_t n, const MaterialParams& m, const double* stress,
                                 const double* dstrain, const double* density, double* state,

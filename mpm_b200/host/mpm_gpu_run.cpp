@@ -12,12 +12,15 @@
 // the mesh and particle files (io_mesh_ascii.tcc: mesh, particles,
 // particle stresses, velocity and friction constraints), particle entity sets
 // (io.cc:159-194) with particle velocity constraints -- and calls the same
-// steps on the library.  At the end it prints the solver duration as
-// mpm_explicit.tcc:191-196 does and writes the particles' PODParticle records
-// (pod_particle.h:12-62; the reference would hand them to H5TBmake_table) to
-// <post_processing.path>/particles-<uuid>-<nsteps>.pod: a 16-byte header
-// ("MPMPOD01", record count as int64) then the records, 74 fields in
-// declaration order at natural alignment.
+// steps on the library.  As MPMBase::write_outputs does (mpm_base.tcc:749-756,
+// 577-596; io.cc:94-135) it writes the particles' HDF5 table (the
+// PODParticle records of Mesh::write_particles_hdf5, mesh.tcc:1573-1613) to
+// <post_processing.path><uuid>/particles<step>.h5 at the first step and
+// every output_steps steps, the step zero-padded to the digits of nsteps, and
+// prints the solver duration as mpm_explicit.tcc:191-196 does.  With
+// analysis.resume.resume true it resumes as MPMBase::checkpoint_resume does
+// (mpm_base.tcc:509-551): the particles of particles<resume.step>.h5 of
+// resume.uuid, from that step on.
 //
 // --parse-only reads and checks the input and prints a summary without
 // touching a GPU.
@@ -49,7 +52,10 @@ struct Input {
   std::string scheme = "usf", vupdate = "flip", uuid = "mpm", out_path = "results/";
   double beta = 1.0, dt = 0.0, damping = 0.0, ramp = 0.0;
   double gravity[3] = {0, 0, 0};
-  long nsteps = 0;
+  long nsteps = 0, output_steps = 0;  // output_steps 0: at the start and the end only
+  bool resume = false;
+  std::string resume_uuid;
+  long resume_step = 0;
   bool locate = true;
   bool isoparametric = true;          // mesh "isoparametric" (mpm_base.tcc:767-784 default)
   std::vector<double> coords;         // nnodes x dim
@@ -244,6 +250,8 @@ Input read_input(const std::string& dir, const std::string& file) {
   if (an.contains("uuid")) in.uuid = an.at("uuid").as_string();
   if (root.contains("post_processing") && root.at("post_processing").contains("path"))
     in.out_path = root.at("post_processing").at("path").as_string();
+  if (root.contains("post_processing") && root.at("post_processing").contains("output_steps"))
+    in.output_steps = (long)root.at("post_processing").at("output_steps").as_double();
   if (root.contains("external_loading_conditions") &&
       root.at("external_loading_conditions").contains("gravity")) {
     const Json& g = root.at("external_loading_conditions").at("gravity");
@@ -325,9 +333,15 @@ Input read_input(const std::string& dir, const std::string& file) {
         in.unsupported.push_back(std::string("external_loading_conditions.") + k);
   }
   if (an.contains("resume") && an.at("resume").contains("resume")) {
-    const Json& r = an.at("resume").at("resume");
-    if ((r.is_bool() && r.as_bool()) || (r.type == Json::String && r.as_string() == "true"))
-      in.unsupported.push_back("analysis.resume (read the checkpoint records with mpm_gpu_load_pod)");
+    const Json& r = an.at("resume");
+    const Json& on = r.at("resume");
+    // a string "true" is not a JSON bool: the reference's get<bool>() throws and
+    // the analysis restarts (mpm_base.tcc:520, 544-548)
+    in.resume = on.is_bool() && on.as_bool();
+    if (in.resume) {
+      in.resume_uuid = r.contains("uuid") ? r.at("uuid").as_string() : in.uuid;
+      in.resume_step = r.contains("step") ? (long)r.at("step").as_double() : 0;
+    }
   }
   for (const char* k : {"pressure_smoothing", "interface", "pore_pressure_smoothing"})
     if (an.contains(k) && an.at(k).is_bool() && an.at(k).as_bool())
@@ -402,48 +416,14 @@ Input read_input(const std::string& dir, const std::string& file) {
   return in;
 }
 
-// PODParticle data members at natural alignment (no vtable)
-struct PodRecord {
-  uint64_t id;
-  double mass, volume, pressure;
-  double coord[3], displacement[3], nsize[3], velocity[3], acceleration[3];
-  double stress[6], strain[6], defgrad[9];
-  bool initialise_mapping_matrix;
-  double mapping_matrix[9];
-  bool status;
-  uint64_t cell_id;
-  uint32_t material_id, nstate_vars;
-  double svars[20];
-};
-
-void pod_layout(size_t* off, size_t* sz) {
-  int f = 0;
-  auto put = [&](size_t o, size_t s, int count) {
-    for (int k = 0; k < count; ++k) {
-      off[f] = o + k * s;
-      sz[f] = s;
-      ++f;
-    }
-  };
-  put(offsetof(PodRecord, id), 8, 1);
-  put(offsetof(PodRecord, mass), 8, 1);
-  put(offsetof(PodRecord, volume), 8, 1);
-  put(offsetof(PodRecord, pressure), 8, 1);
-  put(offsetof(PodRecord, coord), 8, 3);
-  put(offsetof(PodRecord, displacement), 8, 3);
-  put(offsetof(PodRecord, nsize), 8, 3);
-  put(offsetof(PodRecord, velocity), 8, 3);
-  put(offsetof(PodRecord, acceleration), 8, 3);
-  put(offsetof(PodRecord, stress), 8, 6);
-  put(offsetof(PodRecord, strain), 8, 6);
-  put(offsetof(PodRecord, defgrad), 8, 9);
-  put(offsetof(PodRecord, initialise_mapping_matrix), 1, 1);
-  put(offsetof(PodRecord, mapping_matrix), 8, 9);
-  put(offsetof(PodRecord, status), 1, 1);
-  put(offsetof(PodRecord, cell_id), 8, 1);
-  put(offsetof(PodRecord, material_id), 4, 1);
-  put(offsetof(PodRecord, nstate_vars), 4, 1);
-  put(offsetof(PodRecord, svars), 8, 20);
+// io.cc:94-135: <path><uuid>/<attribute><step, zero-padded to the digits of
+// max_steps><extension>
+std::string output_file(const std::string& dir, const Input& in, const std::string& uuid, long step) {
+  const int digits = (int)std::log10((double)std::max(in.nsteps, 1L)) + 1;
+  char num[32];
+  std::snprintf(num, sizeof(num), "%0*ld", digits, step);
+  const std::string folder = join(join(dir, in.out_path), uuid) + "/";
+  return folder + "particles" + num + ".h5";
 }
 
 int check(mpm_gpu_t h, int rc, const char* what) {
@@ -537,37 +517,55 @@ int main(int argc, char** argv) {
   for (auto& m : in.matsets)
     check(h, mpm_gpu_assign_particle_materials(h, (int64_t)m.ids.size(), m.ids.data(), m.material),
           "material sets");
-  check(h, mpm_gpu_initialise(h), "initialise");
-  if (!in.stresses.empty())
-    check(h, mpm_gpu_assign_particle_stresses(h, (int64_t)in.stresses.size() / 6, in.stresses.data()),
-          "particle stresses");
+  long step0 = 0;
+  if (in.resume) {
+    // mesh and materials as usual, the particles from the checkpoint file
+    const std::string f = output_file(dir, in, in.resume_uuid, in.resume_step);
+    if (mpm_gpu_load_hdf5(h, f.c_str()) != MPM_OK) {
+      std::fprintf(stderr, "mpm_gpu_run: resume from %s failed: %s; restarting the analysis\n", f.c_str(),
+                   mpm_gpu_last_error(h));
+      in.resume = false;
+    } else {
+      step0 = in.resume_step;
+      in.uuid = in.resume_uuid;
+      check(h, mpm_gpu_set_current_step(h, step0), "set_current_step");
+      std::printf("Checkpoint resume at step %ld of %ld\n", step0, in.nsteps);
+    }
+  }
+  if (!in.resume) {
+    for (auto& m : in.matsets)
+      check(h, mpm_gpu_assign_particle_materials(h, (int64_t)m.ids.size(), m.ids.data(), m.material),
+            "material sets");
+    check(h, mpm_gpu_initialise(h), "initialise");
+    if (!in.stresses.empty())
+      check(h, mpm_gpu_assign_particle_stresses(h, (int64_t)in.stresses.size() / 6, in.stresses.data()),
+            "particle stresses");
+  }
   for (auto& c : in.pvcs)
     check(h, mpm_gpu_add_particle_velocity_constraint(h, c.ids.empty() ? -1 : (int64_t)c.ids.size(),
                                                       c.ids.data(), c.dir, c.v), "particle velocity constraint");
-  double ms = 0.0;
-  check(h, mpm_gpu_step_timed(h, in.nsteps, &ms), "step");
-  std::printf("Explicit solver duration: %.3f ms\n", ms);
-
-  std::vector<PodRecord> rec((size_t)np);
-  std::memset(rec.data(), 0, rec.size() * sizeof(PodRecord));
-  size_t off[74], sz[74];
-  pod_layout(off, sz);
-  int64_t n = 0;
-  check(h, mpm_gpu_write_pod(h, rec.data(), np, &n, sizeof(PodRecord), off, sz, 74), "write_pod");
-  const std::string out = join(dir, in.out_path);
-  std::string cmd = "mkdir -p '" + out + "'";
-  if (std::system(cmd.c_str()) != 0) std::fprintf(stderr, "mpm_gpu_run: cannot create %s\n", out.c_str());
-  const std::string path = join(out, "particles-" + in.uuid + "-" + std::to_string(in.nsteps) + ".pod");
-  FILE* f = std::fopen(path.c_str(), "wb");
-  if (!f) {
-    std::fprintf(stderr, "mpm_gpu_run: cannot write %s\n", path.c_str());
-    return 1;
+  auto write = [&](long step) {
+    const std::string f = output_file(dir, in, in.uuid, step);
+    const std::string folder = f.substr(0, f.rfind('/'));
+    const std::string cmd = "mkdir -p '" + folder + "'";
+    if (std::system(cmd.c_str()) != 0) std::fprintf(stderr, "mpm_gpu_run: cannot create %s\n", folder.c_str());
+    check(h, mpm_gpu_write_hdf5(h, f.c_str()), "write_hdf5");
+    std::printf("wrote %s\n", f.c_str());
+  };
+  // mpm_explicit.tcc:108, 189: outputs at the start (not on resume) and after
+  // every step that completes a multiple of output_steps
+  const long every = in.output_steps > 0 ? in.output_steps : std::max(in.nsteps, 1L);
+  if (!in.resume) write(0);
+  double total_ms = 0.0;
+  for (long s = step0; s < in.nsteps;) {
+    const long next = std::min(in.nsteps, (s / every + 1) * every);
+    double ms = 0.0;
+    check(h, mpm_gpu_step_timed(h, next - s, &ms), "step");
+    total_ms += ms;
+    s = next;
+    if (s % every == 0) write(s);
   }
-  std::fwrite("MPMPOD01", 1, 8, f);
-  std::fwrite(&n, sizeof(n), 1, f);
-  std::fwrite(rec.data(), sizeof(PodRecord), (size_t)n, f);
-  std::fclose(f);
-  std::printf("wrote %lld records to %s\n", (long long)n, path.c_str());
+  std::printf("Explicit solver duration: %.3f ms\n", total_ms);
   mpm_gpu_destroy(h);
   return 0;
 }

@@ -261,6 +261,14 @@ class Solver:
                                          size, offs.ctypes.data_as(psz),
                                          sizes.ctypes.data_as(psz), 74))
 
+    def write_hdf5(self, path):
+        """The reference's HDF5 particle table (Mesh::write_particles_hdf5)."""
+        self._ck(self.L.mpm_gpu_write_hdf5(self.h, str(path).encode()))
+
+    def load_hdf5(self, path):
+        """Checkpoint resume from an HDF5 particle table (Mesh::read_particles_hdf5)."""
+        self._ck(self.L.mpm_gpu_load_hdf5(self.h, str(path).encode()))
+
     SENSITIVITY_KINDS = {"youngs_modulus": 0, "friction": 1, "cohesion": 2, "dilation": 3}
     SENSITIVITY_FIELDS = {"x": 0, "u": 1, "v": 2, "stress": 3}
 

@@ -17,7 +17,7 @@ def test_product_library_exports_header_symbols():
     from mpm_b200 import _native
     assert os.path.exists(_native.LIB_PATH), "libmpm_b200.so not built"
     lib = ctypes.CDLL(_native.LIB_PATH)
-    names = _declared(os.path.join(ROOT, "include", "mpm_gpu.h"), "mpm_gpu_")
+    names = _declared(os.path.join(ROOT, "include", "mpm_gpu.h"), "mpm_(?:gpu|h5)_")
     assert len(names) >= 19
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing

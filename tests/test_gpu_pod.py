@@ -155,3 +155,43 @@ def test_resume_rejects_particles_outside_the_mesh():
     b = P.build_solver(prob, with_particles=False)
     with pytest.raises(MPMError, match="outside the mesh"):
         b.load_pod(rec)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_hdf5_table_holds_the_records(tmp_path, precision):
+    """Mesh::write_particles_hdf5's table: the records write_pod gives."""
+    from mpm_b200 import h5
+    prob = P.column_3d(shape=(12, 6, 8), block=(6, 6, 8), scheme="usl")
+    a = P.build_solver(prob, precision=precision)
+    a.step(7)
+    path = tmp_path / "particles07.h5"
+    a.write_hdf5(path)
+    rec = h5.read_table(path)
+    ref = a.write_pod()
+    assert len(rec) == len(ref) == prob.nparticles
+    for name in ref.dtype.names:
+        assert np.array_equal(rec[name].astype(ref[name].dtype), ref[name]), name
+
+
+def test_hdf5_checkpoint_resumes_the_run(tmp_path):
+    """The HDF5 particle table as the checkpoint (Mesh::read_particles_hdf5,
+    MPMBase::checkpoint_resume): written at step 15, resumed in a new solver,
+    the run reaches step 30 as the uninterrupted one (density to 1e-14,
+    recomputed as mass / volume)."""
+    prob = P.column_3d(shape=(12, 6, 8), block=(6, 6, 8), scheme="usl")
+    precision = "fp64"
+    a = P.build_solver(prob, precision=precision)
+    a.step(15)
+    path = tmp_path / "particles15.h5"
+    a.write_hdf5(path)
+    a.step(15)
+    A = a.read()
+    b = P.build_solver(prob, precision=precision, with_particles=False)
+    b.load_hdf5(path)
+    b.set_current_step(15)
+    b.step(15)
+    B = b.read()
+    for k in ("x", "u", "v", "stress", "strain", "F", "volume", "mass", "svars", "cell",
+              "material"):
+        assert np.array_equal(A[k], B[k]), k
+    assert np.max(np.abs(A["density"] - B["density"]) / A["density"]) < 1e-14
