@@ -212,6 +212,10 @@ __global__ void __launch_bounds__(128) k_adj_material(DevState s, AdjointArgs A,
 #pragma unroll
       for (int k = 0; k < 6; ++k) s.pbuf[(int64_t)k * np + i] = dstrain[k];
       s.pbuf[(int64_t)6 * np + i] = rho;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) A.dsbar[(int64_t)k * np + i] = sbar[k];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) at(A.deps, k, np, p) = 0.;  // the return passes fill the rest
       return;
     }
     separated = sv[SV_YIELD] == 3.;
@@ -245,92 +249,80 @@ __global__ void __launch_bounds__(128) k_adj_material(DevState s, AdjointArgs A,
 // values, the function the forward step evaluated) with respect to the stress
 // and strain-increment entries that vary, two columns per pass, contracted
 // with sigma~'; one more pass with the parameter-seeded material and state.
+// The passes of a point are independent, so each runs on its own thread (one
+// thread per point and pass): the plastic points of a step are far fewer than
+// the threads the GPU holds.  A pass writes only its own entries of sigma~,
+// deps~ and theta; sigma~' comes from the copy taken when the point was listed.
+template <int DIM>
+struct ReturnPasses {
+  static constexpr int NS = PF<DIM>::NS;
+  static constexpr int NE = DIM == 2 ? 3 : 6;  // deps entries that vary (2D: xx, yy, xy)
+  static constexpr int NIN = NS + NE;
+  static constexpr int N = (NIN + 1) / 2 + 1;  // Jacobian passes + the parameter pass
+};
+
 template <int DIM>
 __global__ void __launch_bounds__(128) k_adj_return(DevState s, AdjointArgs A) {
-  constexpr int NS = PF<DIM>::NS;
-  // the entries of sigma (NS stored) and deps (3D: 6; 2D: xx, yy, xy) that vary
-  constexpr int NE = DIM == 2 ? 3 : 6;
+  using RP = ReturnPasses<DIM>;
+  constexpr int NS = RP::NS, NIN = RP::NIN, NPASS = RP::N;
   constexpr int EIDX[6] = {0, 1, DIM == 2 ? 3 : 2, 3, 4, 5};
-  constexpr int NIN = NS + NE;
   const unsigned n = *s.nplastic;
   const int64_t np = s.np;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int64_t work = (int64_t)n * NPASS;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < work;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = w / NPASS;
+    const int pass = (int)(w % NPASS);
     const int64_t p = s.plist[i];
     const int slot = s.mat[p];
-    double sig[6] = {0, 0, 0, 0, 0, 0}, de[6], sbar[6] = {0, 0, 0, 0, 0, 0}, sv0[SV_N];
+    const bool param = pass == NPASS - 1;
+    if (param && A.nparams == 0) continue;
+    D sg[6], dd[6], sv[SV_N], out[6];
+    double sbar[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      sig[k] = s.pf[(int64_t)(PF<DIM>::S + k) * np + p];
-      sbar[k] = at(A.adj, AdjAt<DIM>::S + k, np, p);
+    for (int k = 0; k < 6; ++k) {
+      sg[k] = D(k < NS ? s.pf[(int64_t)(PF<DIM>::S + k) * np + p] : 0.);
+      dd[k] = D(s.pbuf[(int64_t)k * np + i]);
     }
 #pragma unroll
-    for (int k = 0; k < 6; ++k) de[k] = s.pbuf[(int64_t)k * np + i];
+    for (int k = 0; k < NS; ++k) sbar[k] = A.dsbar[(int64_t)k * np + i];
+#pragma unroll
+    for (int k = 0; k < SV_N; ++k) sv[k] = D(s.sv[(int64_t)k * np + p]);
     const double rho = s.pbuf[(int64_t)6 * np + i];
+    const MatD* mats = static_cast<const MatD*>(param ? A.mats_param : A.mats_zero);
+    if (param) {
+      const double* seed = A.sv_seed + (size_t)slot * SV_N * NT;
 #pragma unroll
-    for (int k = 0; k < SV_N; ++k) sv0[k] = s.sv[(int64_t)k * np + p];
-    double gin[NIN];
-    const MatD& mz = static_cast<const MatD*>(A.mats_zero)[slot];
-    for (int j0 = 0; j0 < NIN; j0 += 2) {
-      D sg[6], dd[6], sv[SV_N], out[6];
+      for (int k = 0; k < SV_N; ++k)
 #pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        sg[k] = D(sig[k]);
-        dd[k] = D(de[k]);
-      }
-#pragma unroll
-      for (int k = 0; k < SV_N; ++k) sv[k] = D(sv0[k]);
+        for (int q = 0; q < NT; ++q) sv[k].d[q] = seed[k * NT + q];
+    } else {
       for (int l = 0; l < 2; ++l) {
-        const int j = j0 + l;
+        const int j = 2 * pass + l;
         if (j >= NIN) break;
         if (j < NS)
           sg[j].d[l] = 1.;
         else
           dd[EIDX[j - NS]].d[l] = 1.;
       }
-      D pd = sv[SV_PD];
-      mc_compute_stress<D, D>(mz, sg, dd, D(rho), sv, pd, out);
-      for (int l = 0; l < 2; ++l) {
-        const int j = j0 + l;
-        if (j >= NIN) break;
-        double t = 0.;
-#pragma unroll
-        for (int k = 0; k < NS; ++k) t += sbar[k] * out[k].d[l];
-        gin[j] = t;
-      }
     }
-    if (A.nparams > 0) {
-      const MatD& mq = static_cast<const MatD*>(A.mats_param)[slot];
-      const double* seed = A.sv_seed + (size_t)slot * SV_N * NT;
-      D sg[6], dd[6], sv[SV_N], out[6];
+    D pd = sv[SV_PD];
+    mc_compute_stress<D, D>(mats[slot], sg, dd, D(rho), sv, pd, out);
+    for (int l = 0; l < 2; ++l) {
+      double t = 0.;
 #pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        sg[k] = D(sig[k]);
-        dd[k] = D(de[k]);
+      for (int k = 0; k < NS; ++k) t += sbar[k] * out[k].d[l];
+      if (param) {
+        if (l < A.nparams) at(A.theta, l, np, p) += t;
+        continue;
       }
-#pragma unroll
-      for (int k = 0; k < SV_N; ++k) {
-        sv[k] = D(sv0[k]);
-#pragma unroll
-        for (int q = 0; q < NT; ++q) sv[k].d[q] = seed[k * NT + q];
-      }
-      D pd = sv[SV_PD];
-      mc_compute_stress<D, D>(mq, sg, dd, D(rho), sv, pd, out);
-#pragma unroll
-      for (int q = 0; q < NT; ++q) {
-        if (q >= A.nparams) break;
-        double t = 0.;
-#pragma unroll
-        for (int k = 0; k < NS; ++k) t += sbar[k] * out[k].d[q];
-        at(A.theta, q, np, p) += t;
-      }
+      const int j = 2 * pass + l;
+      if (j >= NIN) break;
+      if (j < NS)
+        at(A.adj, AdjAt<DIM>::S + j, np, p) = t;
+      else
+        at(A.deps, EIDX[j - NS], np, p) = t;
     }
-#pragma unroll
-    for (int k = 0; k < NS; ++k) at(A.adj, AdjAt<DIM>::S + k, np, p) = gin[k];
-    double deb[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < NE; ++k) deb[EIDX[k]] = gin[NS + k];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) at(A.deps, k, np, p) = deb[k];
   }
 }
 
@@ -726,7 +718,8 @@ void adjoint_step(const DevState& s, const AdjointArgs& A, const StepArgs& a, cu
   pr.end(K_ADJ_MATERIAL, st);
   if (s.sv) {
     pr.begin(K_ADJ_RETURN, st);
-    const unsigned mcb = (unsigned)std::min<int64_t>(nblk(s.np, 128), 148 * 8);
+    const unsigned mcb =
+        (unsigned)std::min<int64_t>(nblk(s.np * ReturnPasses<DIM>::N, 128), 148 * 16);
     k_adj_return<DIM><<<mcb, 128, 0, st>>>(s, A);
     pr.end(K_ADJ_RETURN, st);
   }

@@ -21,6 +21,8 @@
 // per-cell P2G, node gather and update, G2P + stress + locate.
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "mpm_bulk.cuh"
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
@@ -102,6 +104,7 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
   using RW = MTileRows<DIM, MODE, BOX>;
   constexpr bool MM = RW::MM, FORCES = RW::FORCES;
   __shared__ float rows[RW::N][T];
+  __shared__ int32_t spid[T];
   const int t = threadIdx.x;
   const int64_t c0 = (int64_t)blockIdx.x * CB;
   if (c0 >= s.ncells) return;
@@ -113,7 +116,34 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
   const bool mine = c < c1;
   const int64_t a0 = mine ? s.start[c] : 0;
   const int64_t a1 = mine ? a0 + s.cnt[c] : 0;
-  if constexpr (MODE != 1) sort_cell_ids<NV>(s.order + a0, (int)(a1 - a0), k);
+  // One staged particle row (one particle per thread, coalesced reads).
+  auto stage = [&](int r, int64_t p) {
+    const int pc = s.cell[p];
+    double x[DIM];
+    load_x<DIM>(s, p, x);
+    float xi[DIM];
+    xi_f32<DIM, BOX>(s, pc, x, xi);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) rows[RW::XI + d][r] = xi[d];
+    rows[RW::M][r] = pmf<DIM>(s, PM<DIM>::MASS, p);
+    if constexpr (MM) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) rows[RW::V + d][r] = pmf<DIM>(s, PM<DIM>::V + d, p);
+    }
+    if constexpr (FORCES) {
+      rows[RW::SC][r] = -(pmf<DIM>(s, PM<DIM>::V0, p) * (1.f + pmf<DIM>(s, PM<DIM>::JP, p)));
+#pragma unroll
+      for (int q = 0; q < PF<DIM>::NS; ++q) rows[RW::S + q][r] = pmf<DIM>(s, PM<DIM>::S + q, p);
+      if constexpr (!BOX) {
+        int nid[NV];
+        float Xr[NV * DIM];
+        cell_nodes_rel<DIM, false>(s, pc, nid, Xr);
+        const CellMap<DIM, false, float> m = cell_map<DIM, false>(s, pc, xi, Xr);
+#pragma unroll
+        for (int q = 0; q < DIM * DIM; ++q) rows[RW::INV + q][r] = m.inv[q];
+      }
+    }
+  };
   CellMap<DIM, BOX, float> box_map;
   if constexpr (BOX && FORCES) {
     if (a1 > a0) box_map = cell_map<DIM, true, float>(s, (int)c, nullptr, nullptr);
@@ -122,80 +152,85 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
   double acc[NVAL];
 #pragma unroll
   for (int v = 0; v < NVAL; ++v) acc[v] = 0.;
-  for (int64_t q0 = q_begin; q0 < q_end; q0 += T) {
-    if (q0 != q_begin) __syncthreads();  // the previous chunk is consumed
-    if (q0 + t < q_end) {
-      const int64_t p = s.order[q0 + t];
-      const int pc = s.cell[p];
-      double x[DIM];
-      load_x<DIM>(s, p, x);
-      float xi[DIM];
-      xi_f32<DIM, BOX>(s, pc, x, xi);
+  // this slot's contributions of staged row r
+  auto add = [&](int r) {
+    float xi[DIM], N, G[DIM];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) rows[RW::XI + d][t] = xi[d];
-      rows[RW::M][t] = pmf<DIM>(s, PM<DIM>::MASS, p);
-      if constexpr (MM) {
+    for (int d = 0; d < DIM; ++d) xi[d] = rows[RW::XI + d][r];
+    node_shape<DIM>(xi, k, N, G);
+    const float m = rows[RW::M][r];
+    if constexpr (MM) {
+      const float mN = m * N;
+      acc[MASS] += (double)mN;
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) rows[RW::V + d][t] = pmf<DIM>(s, PM<DIM>::V + d, p);
+      for (int d = 0; d < DIM; ++d) acc[MOM + d] += (double)(mN * rows[RW::V + d][r]);
+    }
+    if constexpr (FORCES) {
+      const float sc = rows[RW::SC][r];
+      float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int q = 0; q < PF<DIM>::NS; ++q) sig[q] = rows[RW::S + q][r];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) acc[FEXT + d] += (double)((gv[d] * m) * N);
+      float Dn[DIM];
+      if constexpr (BOX) {
+        box_map.grad(G, Dn);
+      } else {
+        CellMap<DIM, false, float> m2;
+#pragma unroll
+        for (int q = 0; q < DIM * DIM; ++q) m2.inv[q] = rows[RW::INV + q][r];
+        m2.grad(G, Dn);
       }
-      if constexpr (FORCES) {
-        rows[RW::SC][t] = -(pmf<DIM>(s, PM<DIM>::V0, p) * (1.f + pmf<DIM>(s, PM<DIM>::JP, p)));
-#pragma unroll
-        for (int q = 0; q < PF<DIM>::NS; ++q) rows[RW::S + q][t] = pmf<DIM>(s, PM<DIM>::S + q, p);
-        if constexpr (!BOX) {
-          int nid[NV];
-          float Xr[NV * DIM];
-          cell_nodes_rel<DIM, false>(s, pc, nid, Xr);
-          const CellMap<DIM, false, float> m = cell_map<DIM, false>(s, pc, xi, Xr);
-#pragma unroll
-          for (int q = 0; q < DIM * DIM; ++q) rows[RW::INV + q][t] = m.inv[q];
-        }
+      float f[DIM];
+      if constexpr (DIM == 2) {
+        f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
+        f[1] = Dn[1] * sig[1] + Dn[0] * sig[3];
+      } else {
+        f[0] = Dn[0] * sig[0] + Dn[1] * sig[3] + Dn[2] * sig[5];
+        f[1] = Dn[1] * sig[1] + Dn[0] * sig[3] + Dn[2] * sig[4];
+        f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
       }
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) acc[FINT + d] += (double)(f[d] * sc);
+    }
+  };
+  if (MODE == 2 && q_end - q_begin <= T) {
+    // The whole tile in one staged chunk (the usual case): each (cell, slot)
+    // thread takes its cell's staged rows in ascending particle id by selection
+    // over the staged ids, so the cell segments of `order` need no sorting in
+    // global memory (no block barriers for it).  The order of the sums is the
+    // same as below: particle id order within each cell.
+    if (q_begin + t < q_end) {
+      const int64_t p = s.order[q_begin + t];
+      stage(t, p);
+      spid[t] = (int32_t)p;
     }
     __syncthreads();
-    const int64_t j0 = a0 > q0 ? a0 : q0;
-    const int64_t j1 = a1 < q0 + T ? a1 : q0 + T;
-    for (int64_t j = j0; j < j1; ++j) {
-      const int r = (int)(j - q0);
-      float xi[DIM], N, G[DIM];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) xi[d] = rows[RW::XI + d][r];
-      node_shape<DIM>(xi, k, N, G);
-      const float m = rows[RW::M][r];
-      if constexpr (MM) {
-        const float mN = m * N;
-        acc[MASS] += (double)mN;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) acc[MOM + d] += (double)(mN * rows[RW::V + d][r]);
-      }
-      if constexpr (FORCES) {
-        const float sc = rows[RW::SC][r];
-        float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int q = 0; q < PF<DIM>::NS; ++q) sig[q] = rows[RW::S + q][r];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) acc[FEXT + d] += (double)((gv[d] * m) * N);
-        float Dn[DIM];
-        if constexpr (BOX) {
-          box_map.grad(G, Dn);
-        } else {
-          CellMap<DIM, false, float> m2;
-#pragma unroll
-          for (int q = 0; q < DIM * DIM; ++q) m2.inv[q] = rows[RW::INV + q][r];
-          m2.grad(G, Dn);
+    const int l0 = (int)(a0 - q_begin), n = (int)(a1 - a0);
+    int32_t last = -1;
+    for (int r = 0; r < n; ++r) {
+      int32_t best = INT32_MAX;
+      int bi = 0;
+      for (int j = 0; j < n; ++j) {
+        const int32_t id = spid[l0 + j];
+        if (id > last && id < best) {
+          best = id;
+          bi = j;
         }
-        float f[DIM];
-        if constexpr (DIM == 2) {
-          f[0] = Dn[0] * sig[0] + Dn[1] * sig[3];
-          f[1] = Dn[1] * sig[1] + Dn[0] * sig[3];
-        } else {
-          f[0] = Dn[0] * sig[0] + Dn[1] * sig[3] + Dn[2] * sig[5];
-          f[1] = Dn[1] * sig[1] + Dn[0] * sig[3] + Dn[2] * sig[4];
-          f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
-        }
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) acc[FINT + d] += (double)(f[d] * sc);
       }
+      add(l0 + bi);
+      last = best;
+    }
+  } else {
+    // each cell's particle ids in ascending order in the first mapping of a step
+    if constexpr (MODE != 1) sort_cell_ids<NV>(s.order + a0, (int)(a1 - a0), k);
+    for (int64_t q0 = q_begin; q0 < q_end; q0 += T) {
+      if (q0 != q_begin) __syncthreads();  // the previous chunk is consumed
+      if (q0 + t < q_end) stage(t, s.order[q0 + t]);
+      __syncthreads();
+      const int64_t j0 = a0 > q0 ? a0 : q0;
+      const int64_t j1 = a1 < q0 + T ? a1 : q0 + T;
+      for (int64_t j = j0; j < j1; ++j) add((int)(j - q0));
     }
   }
   if (!mine || a1 == a0) return;  // empty cells keep no partials

@@ -202,7 +202,7 @@ struct AdjointTape {
   size_t pf_n = 0, sv_n = 0, cell_n = 0;  // elements of one stored state
   DevBuf<double> ck_pf, ck_sv, seg_pf, seg_sv, fin_pf, fin_sv;
   DevBuf<int32_t> ck_cell, seg_cell, fin_cell;
-  DevBuf<double> adj, deps, coef, theta, apart, nbar, sv_seed;
+  DevBuf<double> adj, deps, dsbar, coef, theta, apart, nbar, sv_seed;
   DevBuf<unsigned char> mats_zero, mats_param;
   double mass_floor = 0.0;
 };
@@ -2362,7 +2362,7 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
   const int64_t nseg = std::min(checkpoint_every, nsteps);
   const int ns = dim == 2 ? PF<2>::NS : PF<3>::NS;
   const size_t state_bytes = t.pf_n * 8 + t.sv_n * 8 + t.cell_n * 4;
-  const size_t work_bytes = (size_t)np * 8 * ((2 * dim + ns + 1) + 6 + (3 * dim + 6) + MAX_TANGENTS) +
+  const size_t work_bytes = (size_t)np * 8 * ((2 * dim + ns + 1) + 6 + ns + (3 * dim + 6) + MAX_TANGENTS) +
                             (size_t)h->ncells * h->nv * 2 * dim * 8 + (size_t)h->nnodes * (1 + 3 * dim) * 8;
   const size_t need = state_bytes * (size_t)(nck + nseg + 1) + work_bytes;
   size_t free_b = 0, total_b = 0;
@@ -2385,6 +2385,7 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
   t.fin_cell.alloc(t.cell_n);
   t.adj.alloc((size_t)(2 * dim + ns + 1) * np);
   t.deps.alloc((size_t)6 * np);
+  t.dsbar.alloc((size_t)ns * np);
   t.coef.alloc((size_t)(3 * dim + 6) * np);
   t.theta.alloc((size_t)MAX_TANGENTS * np);
   t.apart.alloc((size_t)h->ncells * h->nv * 2 * dim);
@@ -2460,6 +2461,7 @@ int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_d
   AdjointArgs A;
   A.adj = t.adj.p;
   A.deps = t.deps.p;
+  A.dsbar = t.dsbar.p;
   A.coef = t.coef.p;
   A.theta = t.theta.p;
   A.apart = t.apart.p;

@@ -129,6 +129,7 @@ void launch_p2g_nodes_fp64(int dim, const DevState& s, const StepArgs& a, cudaSt
 struct AdjointArgs {
   double* adj = nullptr;
   double* deps = nullptr;    // [6][np] cotangent of the strain increment
+  double* dsbar = nullptr;   // [NS][np] sigma~' of the listed plastic points (list order)
   double* coef = nullptr;    // [3 DIM + 6][np] coefficients of the node scatter
   double* theta = nullptr;   // [NT][np]
   double* apart = nullptr;   // [ncells][NV][2 DIM] cell-slot sums of v~, a~ of the nodes

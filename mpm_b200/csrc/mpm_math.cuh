@@ -14,8 +14,10 @@
 
 #ifdef __CUDACC__
 #define MPM_HD __host__ __device__ __forceinline__
+#define MPM_HD_OUTLINE __host__ __device__ __noinline__
 #else
 #define MPM_HD inline
+#define MPM_HD_OUTLINE inline
 #endif
 
 namespace mpm_b200 {
@@ -703,6 +705,28 @@ MPM_HD void mc_df_dp(const MaterialT<R>& m, int yield_type, const R* sv, const L
   (void)phi;
 }
 
+// Out-of-line copies of the three heavy pieces of the return map, for the
+// full (non-deferred) update: it evaluates each at up to four places (trial
+// stress, old stress, every correction, the final stress), and one shared body
+// keeps the kernels that run it -- the dense plastic-return kernels -- small
+// enough for the instruction cache (inlined, their warps stalled mostly on
+// instruction fetch).  Same arithmetic, so the same results.
+template <typename R>
+MPM_HD_OUTLINE void mc_invariants_o(const R* s, R* sv, LodeTrig<R>& lt) {
+  mc_invariants(s, sv, lt);
+}
+template <typename R>
+MPM_HD_OUTLINE int mc_yield_state_o(R* yf, const R* sv, const LodeTrig<R>& lt,
+                                    const FrictionTrig<R>& ft) {
+  return mc_yield_state(yf, sv, lt, ft);
+}
+template <typename R>
+MPM_HD_OUTLINE void mc_df_dp_o(const MaterialT<R>& m, int yield_type, const R* sv,
+                               const LodeTrig<R>& lt, const FrictionTrig<R>& ft, R pdstrain,
+                               const R* s, R* df, R* dp, R* dp_dq, R* softening) {
+  mc_df_dp(m, yield_type, sv, lt, ft, pdstrain, s, df, dp, dp_dq, softening);
+}
+
 template <typename R>
 MPM_HD R huge_value() {
   return R(1.7976931348623157e308);
@@ -776,8 +800,6 @@ MPM_HD int mc_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R
   const R Tolerance = R(1E-1);
   R softening_trial = R(0), dp_dq_trial = R(0);
   R df_trial[6], dp_trial[6];
-  mc_df_dp(m, yt_trial, sv, lt, ft, pdstrain, trial, df_trial, dp_trial, &dp_dq_trial,
-           &softening_trial);
   R yield_trial = R(0);
   if (yt_trial == MC_TENSILE) {
     sv[SV_YIELD] = R(2);
@@ -787,16 +809,20 @@ MPM_HD int mc_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R
     sv[SV_YIELD] = R(1);
     yield_trial = yf_trial[1];
   }
-  R lambda_trial = yield_trial / (row_de_dot(m, df_trial, dp_trial) + softening_trial);
-  mc_invariants(stress, sv, lt);
+  // the trial stress's invariants, for its dF/dsigma and dP/dsigma below: the
+  // reference evaluates them here, but only the branch of an old stress off
+  // the yield surface uses them, so they are evaluated there (same inputs)
+  const LodeTrig<R> lt_trial = lt;
+  const R sv_trial[3] = {sv[SV_EPS], sv[SV_RHO], sv[SV_THETA]};
+  mc_invariants_o(stress, sv, lt);
   R yf[2];
-  const int yt = mc_yield_state(yf, sv, lt, ft);
+  const int yt = mc_yield_state_o(yf, sv, lt, ft);
   R yield = huge_value<R>();
   if (yt == MC_TENSILE) yield = yf[0];
   if (yt == MC_SHEAR) yield = yf[1];
   R softening = R(0), dp_dq = R(0);
   R df[6], dp[6];
-  mc_df_dp(m, yt, sv, lt, ft, pdstrain, stress, df, dp, &dp_dq, &softening);
+  mc_df_dp_o(m, yt, sv, lt, ft, pdstrain, stress, df, dp, &dp_dq, &softening);
   const R lambda = row_de_dot(m, df, dstrain) / (row_de_dot(m, df, dp) + softening);
   R upd[6];
 #pragma unroll
@@ -806,22 +832,31 @@ MPM_HD int mc_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R
     sub_lambda_de(m, lambda, dp, upd);
     dpdstrain = lambda * dp_dq;
   } else {
+    R svt[SV_N];
+#pragma unroll
+    for (int k = 0; k < SV_N; ++k) svt[k] = sv[k];
+    svt[SV_EPS] = sv_trial[0];
+    svt[SV_RHO] = sv_trial[1];
+    svt[SV_THETA] = sv_trial[2];
+    mc_df_dp_o(m, yt_trial, svt, lt_trial, ft, pdstrain, trial, df_trial, dp_trial, &dp_dq_trial,
+               &softening_trial);
+    const R lambda_trial = yield_trial / (row_de_dot(m, df_trial, dp_trial) + softening_trial);
     sub_lambda_de(m, lambda_trial, dp_trial, upd);
     dpdstrain = lambda_trial * dp_dq_trial;
   }
   for (int itr = 0; itr < 100; ++itr) {
-    mc_invariants(upd, sv, lt);
-    yt_trial = mc_yield_state(yf_trial, sv, lt, ft);
+    mc_invariants_o(upd, sv, lt);
+    yt_trial = mc_yield_state_o(yf_trial, sv, lt, ft);
     if (yf_trial[0] < Tolerance && yf_trial[1] < Tolerance) break;
-    mc_df_dp(m, yt_trial, sv, lt, ft, pdstrain, upd, df_trial, dp_trial, &dp_dq_trial,
-             &softening_trial);
+    mc_df_dp_o(m, yt_trial, sv, lt, ft, pdstrain, upd, df_trial, dp_trial, &dp_dq_trial,
+               &softening_trial);
     if (yt_trial == MC_TENSILE) yield_trial = yf_trial[0];
     if (yt_trial == MC_SHEAR) yield_trial = yf_trial[1];
-    lambda_trial = yield_trial / (row_de_dot(m, df_trial, dp_trial) + softening_trial);
+    const R lambda_trial = yield_trial / (row_de_dot(m, df_trial, dp_trial) + softening_trial);
     sub_lambda_de(m, lambda_trial, dp_trial, upd);
     dpdstrain += lambda_trial * dp_dq_trial;
   }
-  mc_invariants(upd, sv, lt);
+  mc_invariants_o(upd, sv, lt);
   pdstrain_io += PD(dpdstrain);
   bool finite = true;
 #pragma unroll

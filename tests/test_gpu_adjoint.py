@@ -59,8 +59,8 @@ def test_adjoint_gradient_equals_the_tangent_gradient(case):
         make, steps, every = (lambda th: _column(th)), 150, 40
     elif case == "tensile_apex":  # c = 200 Pa, no tension cutoff: tensile and apex returns
         make, steps, every = (lambda th: _column(th, c=200.0, tc=0.0, dt=5e-6)), 60, 7
-    else:
-        make, steps, every = (lambda th: _column(th, vu="pic")), 150, 60
+    else:  # PIC damps the motion: the weaker material yields within the run
+        make, steps, every = (lambda th: _column(th, c=200.0, tc=0.0, dt=5e-6, vu="pic")), 80, 30
     target = _target(make, steps)
     gt = _tangent_grad(make, steps, target)
     _, ga = _adjoint_grad(make, steps, target, every)
@@ -118,13 +118,19 @@ def test_adjoint_matches_central_differences_of_the_gpu_loss():
 
 def test_initial_state_gradient_matches_central_differences():
     """dL/dx0, dL/dv0 and dL/dstress0 of a LinearElastic 3D column in a slip
-    box, for a few particles and components (no frictional floor here: its
-    stick / slip switch is a kink that central differences may straddle)."""
+    box, for a few particles and components.  The step snaps entries below
+    1e-15 to zero and a frictional floor switches between stick and slip: at
+    such kinks the derivative is that of the branch taken, which central
+    differences straddle.  So the column starts from random velocities (no
+    nodal velocity or strain rate exactly zero) and has no frictional floor."""
     steps = 60
     prob = P.column_3d(shape=(12, 8, 10), block=(6, 4, 6), material="LinearElastic", E=1e6,
                        scheme="usl", dt=1e-5)
     prob.friction_constraints = None
     s = P.build_solver(prob)
+    st0 = s.read()
+    st0["v"] = np.random.default_rng(11).normal(0.0, 1e-2, st0["v"].shape)
+    s.load(st0)
     st0 = s.read()
     s.step(steps)
     rng = np.random.default_rng(5)
