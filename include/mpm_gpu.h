@@ -316,6 +316,26 @@ int mpm_gpu_adjoint_run(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every, i
                         const int32_t* material_ids, const int32_t* kinds, const double* x_target,
                         double* loss, double* dL_dparams);
 
+/* Slab decomposition (the reference's MPI halo sum and particle migration,
+ * mesh.tcc:187-205, 737-1040): a run split along x into slabs of whole cell
+ * columns, one solver per rank, each holding its columns plus one ghost column
+ * per side.  mpm_gpu_step_begin runs a USL step's sort and P2G;
+ * mpm_gpu_halo_pack writes the cell-slot partial sums and particle counts of
+ * one x-column of cells (layer, the column's x index) to dst, and
+ * mpm_gpu_halo_unpack writes such a buffer into a column (the caller moves
+ * the buffers between ranks, e.g. with NCCL); mpm_gpu_step_end runs the rest
+ * of the step (node update, G2P, plastic returns, locate) and counts it.
+ * Buffers hold mpm_gpu_halo_bytes bytes and are device memory.
+ * mpm_gpu_layer_count counts the particles whose cell's x index is below x_lo
+ * and at or above x_hi (the ones to migrate).  USL, FLIP / PIC, tensor-product
+ * grids. */
+int mpm_gpu_step_begin(mpm_gpu_t h);
+int mpm_gpu_step_end(mpm_gpu_t h);
+int mpm_gpu_halo_bytes(mpm_gpu_t h, int64_t* bytes);
+int mpm_gpu_halo_pack(mpm_gpu_t h, int32_t layer, void* dst);
+int mpm_gpu_halo_unpack(mpm_gpu_t h, int32_t layer, const void* src);
+int mpm_gpu_layer_count(mpm_gpu_t h, int32_t x_lo, int32_t x_hi, int64_t* below, int64_t* above);
+
 /* Set the step counter (the resume step of analysis.resume.step; it drives the
  * gravity ramp, mpm_explicit.tcc:145-153). */
 int mpm_gpu_set_current_step(mpm_gpu_t h, int64_t step);

@@ -87,6 +87,12 @@ SIGNATURES = {
                                                         C.c_char_p, C.c_int64, _pd, _pd, _pd,
                                                         _pd, _pd, C.c_char_p, C.c_int64]),
     "mpm_gpu_version": (C.c_char_p, []),
+    "mpm_gpu_step_begin": (C.c_int, [_vp]),
+    "mpm_gpu_step_end": (C.c_int, [_vp]),
+    "mpm_gpu_halo_bytes": (C.c_int, [_vp, _pi64]),
+    "mpm_gpu_halo_pack": (C.c_int, [_vp, C.c_int32, _vp]),
+    "mpm_gpu_halo_unpack": (C.c_int, [_vp, C.c_int32, _vp]),
+    "mpm_gpu_layer_count": (C.c_int, [_vp, C.c_int32, C.c_int32, _pi64, _pi64]),
     "mpm_gpu_write_hdf5": (C.c_int, [_vp, C.c_char_p]),
     "mpm_gpu_load_hdf5": (C.c_int, [_vp, C.c_char_p]),
     "mpm_h5_write_table": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64, C.c_size_t, C.c_int32,

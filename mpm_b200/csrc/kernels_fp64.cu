@@ -1195,6 +1195,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
       default: k_g2p<DIM, STRESS, 4, BOX><<<pb128, 128, 0, st>>>(s, a.dt, a.beta); break;
     }
   };
+  if (a.scheme == 1 && a.phase == 2) goto usl_second_half;
   pr.begin(K_SORT, st, SORT_KERNELS);
   counting_sort_impl(s, st);
   pr.end(K_SORT, st);
@@ -1230,6 +1231,8 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     pr.begin(K_P2G, st);
     p2g(std::integral_constant<int, 2>{});
     pr.end(K_P2G, st);
+    if (a.phase == 1) return;
+  usl_second_half:
     pr.begin(K_NODES_VEL, st);
     k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);

@@ -104,7 +104,6 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
   using RW = MTileRows<DIM, MODE, BOX>;
   constexpr bool MM = RW::MM, FORCES = RW::FORCES;
   __shared__ float rows[RW::N][T];
-  __shared__ int32_t spid[T];
   const int t = threadIdx.x;
   const int64_t c0 = (int64_t)blockIdx.x * CB;
   if (c0 >= s.ncells) return;
@@ -194,44 +193,15 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
       for (int d = 0; d < DIM; ++d) acc[FINT + d] += (double)(f[d] * sc);
     }
   };
-  if (MODE == 2 && q_end - q_begin <= T) {
-    // The whole tile in one staged chunk (the usual case): each (cell, slot)
-    // thread takes its cell's staged rows in ascending particle id by selection
-    // over the staged ids, so the cell segments of `order` need no sorting in
-    // global memory (no block barriers for it).  The order of the sums is the
-    // same as below: particle id order within each cell.
-    if (q_begin + t < q_end) {
-      const int64_t p = s.order[q_begin + t];
-      stage(t, p);
-      spid[t] = (int32_t)p;
-    }
+  // each cell's particle ids in ascending order in the first mapping of a step
+  if constexpr (MODE != 1) sort_cell_ids<NV>(s.order + a0, (int)(a1 - a0), k);
+  for (int64_t q0 = q_begin; q0 < q_end; q0 += T) {
+    if (q0 != q_begin) __syncthreads();  // the previous chunk is consumed
+    if (q0 + t < q_end) stage(t, s.order[q0 + t]);
     __syncthreads();
-    const int l0 = (int)(a0 - q_begin), n = (int)(a1 - a0);
-    int32_t last = -1;
-    for (int r = 0; r < n; ++r) {
-      int32_t best = INT32_MAX;
-      int bi = 0;
-      for (int j = 0; j < n; ++j) {
-        const int32_t id = spid[l0 + j];
-        if (id > last && id < best) {
-          best = id;
-          bi = j;
-        }
-      }
-      add(l0 + bi);
-      last = best;
-    }
-  } else {
-    // each cell's particle ids in ascending order in the first mapping of a step
-    if constexpr (MODE != 1) sort_cell_ids<NV>(s.order + a0, (int)(a1 - a0), k);
-    for (int64_t q0 = q_begin; q0 < q_end; q0 += T) {
-      if (q0 != q_begin) __syncthreads();  // the previous chunk is consumed
-      if (q0 + t < q_end) stage(t, s.order[q0 + t]);
-      __syncthreads();
-      const int64_t j0 = a0 > q0 ? a0 : q0;
-      const int64_t j1 = a1 < q0 + T ? a1 : q0 + T;
-      for (int64_t j = j0; j < j1; ++j) add((int)(j - q0));
-    }
+    const int64_t j0 = a0 > q0 ? a0 : q0;
+    const int64_t j1 = a1 < q0 + T ? a1 : q0 + T;
+    for (int64_t j = j0; j < j1; ++j) add((int)(j - q0));
   }
   if (!mine || a1 == a0) return;  // empty cells keep no partials
   float* out = s.partials_f + ((int64_t)c * NV + k) * NVAL;
@@ -892,6 +862,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     pr.end(K_MC_RETURN, st);
   };
   const float g0 = (float)a.g[0], g1 = (float)a.g[1], g2 = (float)a.g[2];
+  if (a.scheme == 1 && a.phase == 2) goto usl_second_half;
   pr.begin(K_SORT, st, SORT_KERNELS);
   counting_sort(s, st);
   pr.end(K_SORT, st);
@@ -899,6 +870,8 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     pr.begin(K_P2G, st);
     k_p2g_tiles_mixed<DIM, 2, BOX><<<tb, tile, 0, st>>>(s, g0, g1, g2);
     pr.end(K_P2G, st);
+    if (a.phase == 1) return;
+  usl_second_half:
     pr.begin(K_NODES_VEL, st);
     k_nodes_mixed<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);

@@ -2653,3 +2653,170 @@ int mpm_gpu_load_hdf5(mpm_gpu_t h, const char* path) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ slab decomposition
+namespace {
+
+// One x-layer of a tensor-product grid's cells (cell (i, j, k) for fixed i):
+// its cell-slot partials (nval values of each of its NV slots, as P2G left
+// them) and its particle counts, packed as [ny nz][NV nval] values then
+// [ny nz] counts.  T is the partials' element type.
+template <typename T>
+__global__ void k_halo_pack(const T* partials, const int32_t* cnt, int32_t i, int32_t nx,
+                            int64_t ncols, int nvals, T* vals, int32_t* counts) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ncols * nvals) return;
+  const int64_t col = e / nvals, v = e % nvals;
+  const int64_t c = i + (int64_t)nx * col;
+  vals[e] = partials[c * nvals + v];
+  if (v == 0) counts[col] = cnt[c];
+}
+template <typename T>
+__global__ void k_halo_unpack(T* partials, int32_t* cnt, int32_t i, int32_t nx, int64_t ncols,
+                              int nvals, const T* vals, const int32_t* counts) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ncols * nvals) return;
+  const int64_t col = e / nvals, v = e % nvals;
+  const int64_t c = i + (int64_t)nx * col;
+  partials[c * nvals + v] = vals[e];
+  if (v == 0) cnt[c] = counts[col];
+}
+// particles whose cell's x index is below x_lo or at or above x_hi
+__global__ void k_layer_count(const int32_t* cell, int64_t np, int32_t nx, int32_t x_lo, int32_t x_hi,
+                              unsigned long long* out) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int c = cell[p];
+  if (c < 0) return;
+  const int i = c % nx;
+  if (i < x_lo) atomicAdd(&out[0], 1ull);
+  if (i >= x_hi) atomicAdd(&out[1], 1ull);
+}
+
+StepArgs slab_step_args(mpm_gpu_t h, int phase) {
+  StepArgs a = base_step_args(h);
+  set_gravity(h, a, h->step);
+  a.phase = phase;
+  return a;
+}
+
+int64_t halo_cols(mpm_gpu_t h) { return (int64_t)h->gcells[1] * (h->dim == 3 ? h->gcells[2] : 1); }
+int halo_nvals(mpm_gpu_t h) { return h->nv * (1 + 3 * h->dim); }
+
+}  // namespace
+
+extern "C" {
+
+int mpm_gpu_step_begin(mpm_gpu_t h) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("initialise or load particles first");
+  if (h->cfg.scheme != MPM_SCHEME_USL || h->ntangent > 0 || h->cfg.velocity_update >= MPM_VELOCITY_ASFLIP)
+    return fail(h, MPM_ERR_UNSUPPORTED, "the split step follows the USL FLIP / PIC step only");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  refresh_state(h);
+  const StepArgs a = slab_step_args(h, 1);
+  if (h->mixed)
+    launch_step_mixed(h->dim, h->ds, a, h->stream, h->prof);
+  else
+    launch_step_fp64(h->dim, h->ds, a, h->stream, h->prof);
+  ck(cudaGetLastError(), "kernel launch");
+  ck(cudaStreamSynchronize(h->stream), "step_begin");
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_step_end(mpm_gpu_t h) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("initialise or load particles first");
+  if (h->cfg.scheme != MPM_SCHEME_USL || h->ntangent > 0 || h->cfg.velocity_update >= MPM_VELOCITY_ASFLIP)
+    return fail(h, MPM_ERR_UNSUPPORTED, "the split step follows the USL FLIP / PIC step only");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const StepArgs a = slab_step_args(h, 2);
+  if (h->mixed)
+    launch_step_mixed(h->dim, h->ds, a, h->stream, h->prof);
+  else
+    launch_step_fp64(h->dim, h->ds, a, h->stream, h->prof);
+  ck(cudaGetLastError(), "kernel launch");
+  ++h->step;
+  unsigned words[2] = {0, 0};
+  ck(cudaMemcpyAsync(words, h->d_words.p, sizeof(words), cudaMemcpyDeviceToHost, h->stream), "D2H");
+  ck(cudaStreamSynchronize(h->stream), "step_end");
+  if (words[1] & ERR_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite particle position");
+  if (words[1] & ERR_OUTSIDE) return fail(h, MPM_ERR_OUTSIDE, "Particle(s) outside the mesh domain");
+  if (words[1] & ERR_BADCELL) return fail(h, MPM_ERR_INVALID, "corrupt particle cell index");
+  if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded wait on a device copy ran out");
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_halo_bytes(mpm_gpu_t h, int64_t* bytes) {
+  MPM_GUARD(h)
+  if (!bytes) throw InvalidArg("null bytes");
+  if (!h->structured) return fail(h, MPM_ERR_UNSUPPORTED, "halo layers need a tensor-product grid");
+  const int64_t cols = halo_cols(h);
+  *bytes = cols * halo_nvals(h) * (int64_t)(h->mixed ? sizeof(float) : sizeof(double)) + cols * 4;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+static int halo_copy(mpm_gpu_t h, int32_t layer, void* buf, bool pack) {
+  MPM_GUARD(h)
+  if (!buf) throw InvalidArg("null halo buffer");
+  if (!h->structured) return fail(h, MPM_ERR_UNSUPPORTED, "halo layers need a tensor-product grid");
+  if (layer < 0 || layer >= h->gcells[0]) throw InvalidArg("layer outside the grid");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  const int64_t cols = halo_cols(h);
+  const int nvals = halo_nvals(h);
+  const int64_t n = cols * nvals;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  const size_t esz = h->mixed ? sizeof(float) : sizeof(double);
+  int32_t* counts = reinterpret_cast<int32_t*>(static_cast<char*>(buf) + n * esz);
+  if (h->mixed) {
+    float* v = static_cast<float*>(buf);
+    if (pack)
+      k_halo_pack<float><<<blocks, 256, 0, h->stream>>>(h->d_partials_f.p, h->d_cnt.p, layer, h->gcells[0],
+                                                        cols, nvals, v, counts);
+    else
+      k_halo_unpack<float><<<blocks, 256, 0, h->stream>>>(h->d_partials_f.p, h->d_cnt.p, layer, h->gcells[0],
+                                                          cols, nvals, v, counts);
+  } else {
+    double* v = static_cast<double*>(buf);
+    if (pack)
+      k_halo_pack<double><<<blocks, 256, 0, h->stream>>>(h->d_partials.p, h->d_cnt.p, layer, h->gcells[0],
+                                                         cols, nvals, v, counts);
+    else
+      k_halo_unpack<double><<<blocks, 256, 0, h->stream>>>(h->d_partials.p, h->d_cnt.p, layer,
+                                                           h->gcells[0], cols, nvals, v, counts);
+  }
+  ck(cudaGetLastError(), "halo kernel");
+  ck(cudaStreamSynchronize(h->stream), "halo");
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_halo_pack(mpm_gpu_t h, int32_t layer, void* dst) { return halo_copy(h, layer, dst, true); }
+int mpm_gpu_halo_unpack(mpm_gpu_t h, int32_t layer, const void* src) {
+  return halo_copy(h, layer, const_cast<void*>(src), false);
+}
+
+int mpm_gpu_layer_count(mpm_gpu_t h, int32_t x_lo, int32_t x_hi, int64_t* below, int64_t* above) {
+  MPM_GUARD(h)
+  if (!below || !above) throw InvalidArg("null output");
+  if (!h->structured) return fail(h, MPM_ERR_UNSUPPORTED, "layers need a tensor-product grid");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  DevBuf<unsigned long long> c;
+  c.alloc(2);
+  ck(cudaMemsetAsync(c.p, 0, 16, h->stream), "memset");
+  if (h->npad > 0)
+    k_layer_count<<<(unsigned)((h->npad + 255) / 256), 256, 0, h->stream>>>(h->d_cell.p, h->npad,
+                                                                           h->gcells[0], x_lo, x_hi, c.p);
+  unsigned long long r[2] = {0, 0};
+  c.download(r, 2, h->stream);
+  ck(cudaStreamSynchronize(h->stream), "layer count");
+  *below = (int64_t)r[0];
+  *above = (int64_t)r[1];
+  MPM_END(h)
+  return MPM_OK;
+}
+
+}  // extern "C"

@@ -19,6 +19,8 @@ struct StepArgs {
   double beta;       // FLIP/PIC blending ratio
   double damping;    // Cundall damping factor
   double g[3];       // gravity of this step (ramp applied)
+  int phase;         // USL: 0 the whole step, 1 sort and P2G only, 2 the rest (node
+                     // update onward) -- a slab run exchanges halo partials between them
 };
 
 // Kernels of one step, for launch counting and per-kernel event timing.

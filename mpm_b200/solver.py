@@ -261,6 +261,31 @@ class Solver:
                                          size, offs.ctypes.data_as(psz),
                                          sizes.ctypes.data_as(psz), 74))
 
+    # ---- slab decomposition (mpm_b200.slab): a USL step in two halves with the
+    # halo partials of one x-column of cells moved between them
+    def step_begin(self):
+        self._ck(self.L.mpm_gpu_step_begin(self.h))
+
+    def step_end(self):
+        self._ck(self.L.mpm_gpu_step_end(self.h))
+
+    def halo_bytes(self):
+        n = C.c_int64()
+        self._ck(self.L.mpm_gpu_halo_bytes(self.h, C.byref(n)))
+        return n.value
+
+    def halo_pack(self, layer, dst_ptr):
+        self._ck(self.L.mpm_gpu_halo_pack(self.h, int(layer), C.c_void_p(dst_ptr)))
+
+    def halo_unpack(self, layer, src_ptr):
+        self._ck(self.L.mpm_gpu_halo_unpack(self.h, int(layer), C.c_void_p(src_ptr)))
+
+    def layer_count(self, x_lo, x_hi):
+        """Particles whose cell's x index is below x_lo, and at or above x_hi."""
+        a, b = C.c_int64(), C.c_int64()
+        self._ck(self.L.mpm_gpu_layer_count(self.h, int(x_lo), int(x_hi), C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def write_hdf5(self, path):
         """The reference's HDF5 particle table (Mesh::write_particles_hdf5)."""
         self._ck(self.L.mpm_gpu_write_hdf5(self.h, str(path).encode()))
