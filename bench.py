@@ -28,9 +28,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -96,11 +94,20 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--block", default="100,100,50", help="particle block in cells")
     ap.add_argument("--workload", default="column",
-                    choices=["column", "footing", "ensemble", "calibration"],
+                    choices=["column", "footing", "ensemble", "calibration", "launch-list",
+                             "late-step"],
                     help="column: the 4M-particle granular column (default); footing: the "
                          "16M-particle footing on a slope over a foundation; ensemble: 512 "
                          "independent 2D slopes in one solver; calibration: derivatives of "
-                         "the 256k-particle column's final positions with respect to (E, phi)")
+                         "the 256k-particle column's final positions with respect to (E, phi); "
+                         "launch-list: one launch of every kernel (mixed and FP64 steps of a "
+                         "1M-particle column, state conversions, records, one reversed "
+                         "calibration step) inside a profiler start/stop window, for "
+                         "ncu --profile-from-start off; late-step: the 1M-particle column "
+                         "advanced --late-steps steps, then one step inside a profiler window "
+                         "(prints no bench line)")
+    ap.add_argument("--late-steps", type=int, default=2000,
+                    help="late-step workload: steps before the profiled step")
     ap.add_argument("--profile-steps", type=int, default=20,
                     help="steps timed per kernel after the timed window")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
@@ -148,67 +155,71 @@ def max_over_ranks(x, world):
 
 
 class Clocks:
-    """Sample nvidia-smi clocks and throttle reasons during the timed region."""
-    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """Sample the SM clock and the clock-event (throttle) reasons of the
+    bench's GPU during the timed region.
+
+    A thread polls NVML as fast as it answers (a sample every few tens of
+    microseconds): the timed region of a default run lasts tens of
+    milliseconds, shorter than nvidia-smi's sampling period.  The step calls
+    release the GIL, so the thread samples while the steps run.  The GPU is
+    found by its UUID, so CUDA_VISIBLE_DEVICES does not matter."""
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
     def __init__(self, device):
-        self.device = device
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "50"],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
-        except FileNotFoundError:
-            self.p = None
-        time.sleep(1.0)  # nvidia-smi needs a moment before its first sample
+        import threading
+        self.samples = []  # (perf_counter, sm MHz, max sm MHz, reasons bitmask)
         self.window = [None, None]
+        self.nvml = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(device).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            self.nvml, self.h = pynvml, h
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.nvml = None
+            return
+        self.run = True
+        self.t = threading.Thread(target=self._poll, daemon=True)
+        self.t.start()
+
+    def _poll(self):
+        nv, h = self.nvml, self.h
+        while self.run:
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+            except Exception:
+                break
+            self.samples.append((time.perf_counter(), mhz, self.max_mhz, rs))
+            if self.window[0] is None:
+                time.sleep(0.002)  # before the timed region: sample slowly
 
     def mark_start(self):
-        import datetime
-        self.window[0] = datetime.datetime.now()
+        self.window[0] = time.perf_counter()
 
     def mark_end(self):
-        import datetime
-        self.window[1] = datetime.datetime.now()
+        self.window[1] = time.perf_counter()
 
     def stop(self):
-        if self.p is None:
+        if self.nvml is None:
             return None
-        self.p.terminate()
-        try:
-            self.p.wait(5)
-        except subprocess.TimeoutExpired:
-            self.p.kill()
-        self.f.flush()
-        import datetime
-        rows, all_rows = [], []
-        with open(self.f.name) as f:
-            for line in f:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) < 10:
-                    continue
-                try:
-                    ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
-                    row = (float(parts[2]), float(parts[3]), parts[5:])
-                except ValueError:
-                    continue
-                all_rows.append(row)
-                if self.window[0] and self.window[1] and self.window[0] <= ts <= self.window[1]:
-                    rows.append(row)
-        os.unlink(self.f.name)
+        self.run = False
+        self.t.join(5)
+        lo, hi = self.window
+        rows = [r for r in self.samples if lo is not None and hi is not None and lo <= r[0] <= hi]
         in_window = bool(rows)
         if not rows:
-            rows = all_rows[-3:]  # the timed region was shorter than the sampling period
+            rows = self.samples[-3:]
         if not rows:
             return None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r[1:5])
-                          if v.lower().startswith("active")})
-        return {"sm_mhz": statistics.median(r[0] for r in rows),
-                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
-                "samples": len(rows), "in_timed_window": in_window}
+        reasons = sorted({n for *_, rs in rows for n, bit in self.REASONS if rs & bit})
+        return {"sm_mhz": statistics.median(r[1] for r in rows),
+                "sm_max_mhz": max(r[2] for r in rows), "reasons": reasons,
+                "samples": len(rows), "in_timed_window": in_window, "source": "nvml"}
 
 
 def measured_peaks():
@@ -458,6 +469,62 @@ def run_calibration(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def run_late_step(args):
+    """The 1M-particle column advanced --late-steps steps (most points plastic
+    by step 2000), its per-kernel times over 5 profiled steps, then one step
+    inside a profiler window (for ncu --profile-from-start off)."""
+    import torch
+    from mpm_b200 import problems as P
+    s = P.build_solver(P.column_3d(block=(50, 50, 50)), precision=args.precision)
+    s.step(args.late_steps)
+    ys = s.read()["svars"][:, 0]
+    s.set_profiling(True)
+    s.step_timed(5)
+    prof = {k: round(v[0] / v[1], 4) for k, v in s.kernel_profile().items() if v[1]}
+    s.set_profiling(False)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    s.step(1)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"workload": "late-step", "precision": args.precision,
+                      "after_step": args.late_steps, "particles": s.nparticles,
+                      "plastic_fraction": float(np.mean(ys != 0)), "kernels_ms_per_launch": prof}))
+
+
+def run_launch_list():
+    """One launch of every kernel of the product inside a profiler window
+    (cudaProfilerStart/Stop), for a launch list with per-kernel DRAM bytes:
+    a mixed and an FP64 step of the 1M-particle column (eager launches), the
+    host-row/device-layout conversions both ways, the PODParticle records, and
+    one recorded and reversed step of the calibration column."""
+    import torch
+    from mpm_b200 import problems as P
+    col = P.column_3d(block=(50, 50, 50))
+    m = P.build_solver(col, precision="mixed")
+    m.step(5)
+    m.set_profiling(True)
+    f = P.build_solver(col, precision="fp64")
+    f.step(5)
+    f.set_profiling(True)
+    cal = P.build_solver(P.config_d(), precision="fp64")
+    cal.step(3)
+    st = m.read()
+    n = cal.nparticles
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    m.step(1)
+    f.step(1)
+    m.load(st)
+    m.read()
+    f.write_pod()
+    cal.adjoint_record(1, [(0, "youngs_modulus"), (0, "friction")], checkpoint_every=1)
+    cal.adjoint_reverse(dL_dx=np.ones((n, 3)))
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"workload": "launch-list", "particles": [m.nparticles, n]}))
+
+
 def main():
     args = parse()
     rank, world = dist_init(args.gpus)
@@ -466,6 +533,12 @@ def main():
         return
     if args.workload == "calibration":
         run_calibration(args, rank, world)
+        return
+    if args.workload == "launch-list":
+        run_launch_list()
+        return
+    if args.workload == "late-step":
+        run_late_step(args)
         return
     from mpm_b200 import problems as P
     block = tuple(int(v) for v in args.block.split(","))

@@ -191,16 +191,15 @@ def test_reference_fixture_runs_as_the_api_and_the_oracle(tmp_path, dim, scheme)
     _strip_unsupported(d, fname, js)
     r = _driver(d, fname)
     assert r.returncode == 0, r.stderr
-    path = os.path.join(d, "results", f"particles-mpm-explicit-{dim}d-10.pod")
-    raw = open(path, "rb").read()
-    n = int(np.frombuffer(raw[8:16], dtype=np.int64)[0])
-    rec = np.frombuffer(raw[16:], dtype=pod.POD_DTYPE, count=n)
+    from mpm_b200 import h5
+    # post_processing.path + analysis.uuid, the step padded to the digits of nsteps
+    rec = h5.read_table(os.path.join(d, "results", js["analysis"]["uuid"], "particles10.h5"))
     s, pts = _api_run(dim, scheme)
     s.step(10)
     ref = s.write_pod()
-    assert n == len(ref) == len(PARTICLES[dim])
+    assert len(rec) == len(ref) == len(PARTICLES[dim])
     for name in pod.NAMES:
-        assert np.array_equal(rec[name], ref[name]), name
+        assert np.array_equal(rec[name].astype(ref[name].dtype), ref[name]), name
     assert np.all(rec["material_id"] == 1)
     o = _oracle_run(dim, scheme, pts)
     o.step(10)
