@@ -113,6 +113,9 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-fp64-arm", action="store_true",
                     help="skip the FP64 run reported beside the mixed one")
+    ap.add_argument("--autotune-steps", type=int, default=5,
+                    help="steps per launch-shape candidate of the autotuner before the "
+                         "warm-up (0 keeps the default launch shape)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--accuracy-steps", default="50,500,2000",
@@ -298,6 +301,8 @@ def time_arm(prob, precision, args, world, dev, clocks=None):
     t0 = time.perf_counter()
     s = P.build_solver(prob, precision=precision, device=dev)
     setup_s = time.perf_counter() - t0
+    # launch shape timed on this state, then the state restored
+    s.tune_report = s.autotune(args.autotune_steps) if args.autotune_steps else None
     s.step(args.warmup)
     barrier(world)
     launches0 = s.launch_count
@@ -361,6 +366,9 @@ def accuracy_and_late_window(prob, args, world, dev, checkpoints):
                      "fp64_one_ulp_floor_max": field_errors(q, f),
                      "fp64_one_ulp_floor_l2": l2_errors(q, f)})
     del pert
+    # the launch shape re-timed on the late state (the state is restored)
+    tune_m = mixed.autotune(args.autotune_steps) if args.autotune_steps else None
+    tune_f = fp64.autotune(args.autotune_steps) if args.autotune_steps else None
     barrier(world)
     ms_m = max_over_ranks(mixed.step_timed(args.steps), world)
     ms_f = max_over_ranks(fp64.step_timed(args.steps), world)
@@ -374,9 +382,10 @@ def accuracy_and_late_window(prob, args, world, dev, checkpoints):
         return {k: v[0] / v[1] for k, v in prof.items() if v[1]}
     late = {"after_step": done, "steps": args.steps,
             "value": world * n * args.steps / (ms_m / 1e3), "ms_per_step": ms_m / args.steps,
-            "kernels_ms_per_launch": kernels(mixed),
+            "kernels_ms_per_launch": kernels(mixed), "launch_shape": tune_m,
             "fp64": {"value": world * n * args.steps / (ms_f / 1e3),
-                     "ms_per_step": ms_f / args.steps, "kernels_ms_per_launch": kernels(fp64)}}
+                     "ms_per_step": ms_f / args.steps, "kernels_ms_per_launch": kernels(fp64),
+                     "launch_shape": tune_f}}
     return rows, late
 
 
@@ -409,18 +418,24 @@ def run_calibration(args, rank, world):
     t.step(args.warmup)
     ms_t = max_over_ranks(t.step_timed(args.steps), world)
     t.close()
-    # the reverse sweep: record (checkpoints every 100 steps) + reverse, on the
-    # host clock (both calls return after their device work has finished)
+    # the reverse sweep: record + reverse, on the host clock (both calls return
+    # after their device work has finished); every step's start state kept
+    # (no recompute), and checkpoints sqrt(steps) apart (least memory, every
+    # segment recomputed)
     a = build(theta)
     a.step(args.warmup)
     ones = np.ones((a.nparticles, 3))
-    t0 = time.perf_counter()
-    a.adjoint_record(args.steps, params, checkpoint_every=min(100, args.steps))
-    a.adjoint_reverse(dL_dx=ones)
-    adj_s = max_over_ranks(time.perf_counter() - t0, world)
+    every_sqrt = int(np.ceil(np.sqrt(args.steps)))
+    adj_times = {}
+    for every in (1, every_sqrt):
+        t0 = time.perf_counter()
+        a.adjoint_record(args.steps, params, checkpoint_every=every)
+        a.adjoint_reverse(dL_dx=ones)
+        adj_times[every] = max_over_ranks(time.perf_counter() - t0, world)
+    adj_s = adj_times[1]
     # the same again with per-kernel events (eager launches)
     a.set_profiling(True)
-    a.adjoint_record(args.steps, params, checkpoint_every=min(100, args.steps))
+    a.adjoint_record(args.steps, params, checkpoint_every=1)
     a.adjoint_reverse(dL_dx=ones)
     adj_kernels = {k: {"total_ms": v[0], "launches": v[1]} for k, v in a.kernel_profile().items()
                    if v[1]}
@@ -430,8 +445,7 @@ def run_calibration(args, rank, world):
     x, J = run_with_sensitivities(build, theta, params, args.steps)
     grad = 2.0 * np.einsum("pd,kpd->k", x - target, J)
     s_adj = build(theta)
-    _, grad_adj = s_adj.adjoint_run(args.steps, params, target,
-                                    checkpoint_every=min(100, args.steps))
+    _, grad_adj = s_adj.adjoint_run(args.steps, params, target, checkpoint_every=every_sqrt)
     s_adj.close()
     fd = []
     for k in range(2):
@@ -454,11 +468,15 @@ def run_calibration(args, rank, world):
             "forward": {"value": world * n * args.steps / (ms_f / 1e3),
                         "ms_per_step": ms_f / args.steps},
             "tangent_over_forward": ms_t / ms_f,
-            "adjoint": {"seconds": adj_s, "checkpoint_every": min(100, args.steps),
+            "adjoint": {"seconds": adj_s, "checkpoint_every": 1,
                         "over_forward": adj_s / (ms_f / 1e3), "kernels": adj_kernels,
-                        "note": "record (forward with checkpoints) + reverse sweep (segment "
+                        "sqrt_checkpoints": {"checkpoint_every": every_sqrt,
+                                             "seconds": adj_times[every_sqrt],
+                                             "over_forward": adj_times[every_sqrt] / (ms_f / 1e3)},
+                        "note": "record (forward keeping checkpoints) + reverse sweep (segment "
                                 "recompute + reverse kernels), host clock around both, against "
-                                "the device time of the plain forward run"},
+                                "the device time of the plain forward run; the gradient below "
+                                "comes from the sqrt-spaced checkpoints"},
             "gradient": {"loss": "sum |x_final - x_target|^2, target E=8e6, phi=32",
                          "at": theta.tolist(), "tangent": grad.tolist(),
                          "adjoint": [float(v) for v in grad_adj], "central_fd": fd,
@@ -643,7 +661,8 @@ def main():
             "fp64": fp64,
             "accuracy": accuracy, "late": late,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "kernels": {k: {"total_ms": v[0], "launches": v[1]}
+            "clocks": clk, "launch_shape": s.tune_report,
+            "kernels": {k: {"total_ms": v[0], "launches": v[1]}
                                        for k, v in prof.items() if v[1]},
         }
         print(json.dumps(line), flush=True)

@@ -195,6 +195,23 @@ int mpm_gpu_step(mpm_gpu_t h, int64_t nsteps);
  * "solver duration", mpm_explicit.tcc:191-196). */
 int mpm_gpu_step_timed(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms);
 
+/* Launch shape of the steps (no counterpart in the reference, whose steps
+ * are host loops): threads of a P2G cell tile on a tensor-product grid (128
+ * or 256), threads of a node-kernel block (128 or 256), blocks per SM of the
+ * plastic-return kernel (4, 8 or 16); 0 keeps the built-in default (256, 256,
+ * 8).  Results do not depend on it.  mpm_gpu_get_launch_shape writes the
+ * three values in use.  mpm_gpu_autotune times each candidate over `steps`
+ * steps (at least 3) of the solver's own state, one field at a time, keeps
+ * the fastest, and restores the particle state and step counter, so the run
+ * then continues exactly as without it; report (report_len bytes, may be
+ * NULL) receives the per-candidate milliseconds per step as JSON.  It holds a
+ * copy of the particle state on the device meanwhile (MPM_ERR_ALLOC if that
+ * does not fit).  Not with sensitivities on. */
+int mpm_gpu_set_launch_shape(mpm_gpu_t h, int32_t p2g_tile, int32_t node_threads,
+                             int32_t return_blocks_per_sm);
+int mpm_gpu_get_launch_shape(mpm_gpu_t h, int32_t* shape);
+int mpm_gpu_autotune(mpm_gpu_t h, int64_t steps, char* report, size_t report_len);
+
 /* Per-kernel device timing (CUDA events around every launch on the solver's
  * stream).  Enabling or disabling resets the counters.  Kernel indices run
  * from 0 while the call succeeds; name receives a static string. */
@@ -294,7 +311,9 @@ int mpm_gpu_read_sensitivities(mpm_gpu_t h, int32_t field, double* out);
  *
  * mpm_gpu_adjoint_record advances nsteps from the current state like
  * mpm_gpu_step, keeping the particle state every checkpoint_every steps on the
- * device (ceil(nsteps / checkpoint_every) checkpoints plus checkpoint_every
+ * device (0: every step when half the free device memory holds them -- the
+ * reverse sweep then recomputes no step -- else ceil(sqrt(nsteps)) apart;
+ * ceil(nsteps / checkpoint_every) checkpoints plus checkpoint_every
  * states of one segment: about 340 B per particle each in 3D; MPM_ERR_ALLOC
  * with the size when that does not fit).  mpm_gpu_adjoint_reverse then takes
  * dL/dx and dL/dv at the end (n*3 rows; either may be NULL for zero), recomputes

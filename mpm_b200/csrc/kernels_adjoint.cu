@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(128) k_adj_material(DevState s, AdjointArgs A,
 #pragma unroll
     for (int k = 0; k < SV_N; ++k) sv[k] = s.sv[(int64_t)k * np + p];
     if (mc_stress<double, double, true>(mp, sig, dstrain, rho, sv, sv[SV_PD], out) == MC_DEFERRED) {
-      const unsigned i = defer_slot(s);
+      const unsigned i = defer_slot_by_cost(s, p);
       s.plist[i] = (int32_t)p;
 #pragma unroll
       for (int k = 0; k < 6; ++k) s.pbuf[(int64_t)k * np + i] = dstrain[k];
@@ -266,12 +266,12 @@ __global__ void __launch_bounds__(128) k_adj_return(DevState s, AdjointArgs A) {
   using RP = ReturnPasses<DIM>;
   constexpr int NS = RP::NS, NIN = RP::NIN, NPASS = RP::N;
   constexpr int EIDX[6] = {0, 1, DIM == 2 ? 3 : 2, 3, 4, 5};
-  const unsigned n = *s.nplastic;
+  const unsigned nl = *s.nplastic, n = nl + *s.nplastic_heavy;
   const int64_t np = s.np;
   const int64_t work = (int64_t)n * NPASS;
   for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < work;
        w += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = w / NPASS;
+    const int64_t i = list_slot(s, (unsigned)(w / NPASS), nl);
     const int pass = (int)(w % NPASS);
     const int64_t p = s.plist[i];
     const int slot = s.mat[p];
@@ -712,7 +712,7 @@ void adjoint_step(const DevState& s, const AdjointArgs& A, const StepArgs& a, cu
   constexpr int NV = Elem<DIM>::NV;
   if (s.np == 0) return;
   const unsigned pb = nblk(s.np, 128);
-  if (s.sv) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
+  if (s.sv) cudaMemsetAsync(s.nplastic, 0, 2 * sizeof(unsigned), st);  // and nplastic_heavy
   pr.begin(K_ADJ_MATERIAL, st);
   k_adj_material<DIM><<<pb, 128, 0, st>>>(s, A, a.dt);
   pr.end(K_ADJ_MATERIAL, st);

@@ -193,11 +193,18 @@ struct TileRows {
   static constexpr int N = MV + (MM && AFF ? DIM * DIM : 0);
 };
 
-template <int DIM, int MODE, bool BOX, int AFF>
-__global__ void __launch_bounds__(p2g_tile_t<BOX, AFF>(), MPM_P2G_TILE_MIN_BLOCKS)
+// On box cells without the affine rows the tile may also take 128 threads (a
+// launch-shape choice); the blocks per SM scale so that the registers per
+// thread stay the same.
+template <bool BOX, int AFF, int T>
+constexpr int tile_min_blocks() {
+  return BOX && !AFF ? MPM_P2G_TILE_MIN_BLOCKS * 256 / T : MPM_P2G_TILE_MIN_BLOCKS;
+}
+
+template <int DIM, int MODE, bool BOX, int AFF, int T = p2g_tile_t<BOX, AFF>()>
+__global__ void __launch_bounds__(T, (tile_min_blocks<BOX, AFF, T>()))
     k_p2g_tiles(DevState s, double g0, double g1, double g2) {
   constexpr int NV = Elem<DIM>::NV;
-  constexpr int T = p2g_tile_t<BOX, AFF>();
   constexpr int CB = T / NV;
   constexpr int NVAL = PV<DIM>::N;
   using RW = TileRows<DIM, MODE, BOX, AFF>;
@@ -349,20 +356,23 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX, AFF>(), MPM_P2G_TILE_MIN_BLOCK
 // Adds the partial sums of the node's cells (ascending cell id) for the value
 // range [v0, v0 + nv); returns false when no cell of the node holds particles
 // (the node is inactive, cell.tcc:171-177).
-template <int DIM>
-__device__ __forceinline__ bool gather_node(const DevState& s, int64_t node, int v0, int nv,
-                                            double* sum) {
+template <int DIM, int V0, int NVS>
+__device__ __forceinline__ bool gather_node(const DevState& s, int64_t node, double* sum) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int NVAL = PV<DIM>::N;
-  for (int v = 0; v < nv; ++v) sum[v] = 0.;
+#pragma unroll
+  for (int v = 0; v < NVS; ++v) sum[v] = 0.;
   bool active = false;
   auto add = [&](int c, int slot) {
-    const double* src = s.partials + ((int64_t)c * NV + slot) * NVAL + v0;
+    double src[NVS];
+    load_partial_row<double, NVAL, V0, NVS>(s.partials + ((int64_t)c * NV + slot) * NVAL, src);
     if (!active) {
-      for (int v = 0; v < nv; ++v) sum[v] = src[v];
+#pragma unroll
+      for (int v = 0; v < NVS; ++v) sum[v] = src[v];
       active = true;
     } else {
-      for (int v = 0; v < nv; ++v) sum[v] = sum[v] + src[v];
+#pragma unroll
+      for (int v = 0; v < NVS; ++v) sum[v] = sum[v] + src[v];
     }
   };
   if (s.structured) {
@@ -423,14 +433,14 @@ __global__ void __launch_bounds__(256) k_nodes(DevState s, double dt, double dam
   if (n >= s.nn) return;
   const int64_t nn = s.nn;
   double sum[PV<DIM>::N];
-  const int v0 = MODE == 2 ? PV<DIM>::FEXT : 0;
-  const int nv = MODE == 0 ? 1 + DIM : (MODE == 1 ? PV<DIM>::N : 2 * DIM);
-  if (!gather_node<DIM>(s, n, v0, nv, sum)) return;
+  constexpr int V0 = MODE == 2 ? PV<DIM>::FEXT : 0;
+  constexpr int NVS = MODE == 0 ? 1 + DIM : (MODE == 1 ? PV<DIM>::N : 2 * DIM);
+  if (!gather_node<DIM, V0, NVS>(s, n, sum)) return;
   const int bci = s.bc_index[n];
   double vel[DIM], acc[DIM];
   if constexpr (MODE == 2) {
     double mm[1];
-    gather_node<DIM>(s, n, PV<DIM>::MASS, 1, mm);
+    gather_node<DIM, PV<DIM>::MASS, 1>(s, n, mm);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       vel[d] = s.nf[(int64_t)(NF<DIM>::VEL + d) * nn + n];
@@ -581,7 +591,7 @@ __device__ __forceinline__ void stress_update(const DevState& s, const Row& r, i
     if (mc_stress<double, double, true>(mp, sig, dstrain, rho, sv, sv[SV_PD], out) == MC_DEFERRED) {
       // plastic: the return runs in k_mc_return from the unchanged stress and state
       deferred = true;
-      const unsigned i = defer_slot(s);
+      const unsigned i = defer_slot_by_cost(s, r.index());
       s.plist[i] = (int32_t)r.index();
 #pragma unroll
       for (int k = 0; k < 6; ++k) s.pbuf[(int64_t)k * s.np + i] = dstrain[k];
@@ -1057,13 +1067,16 @@ __global__ void __launch_bounds__(128) k_commit_locate(DevState s) {
 }
 
 // The MohrCoulomb returns deferred by stress_update, one thread per listed
-// particle (grid-stride), from the particle's stress and state before the
-// step's update: the same call, with the same inputs, as the undeferred update.
+// particle (grid-stride over the light entries, then the heavy ones), from the
+// particle's stress and state before the step's update: the same call, with
+// the same inputs, as the undeferred update.  Records the return's number of
+// corrections for the next step's grouping.
 template <int DIM>
 __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return(DevState s) {
-  const unsigned n = *s.nplastic;
+  const unsigned nl = *s.nplastic, n = nl + *s.nplastic_heavy;
   const int64_t np = s.np;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned i = list_slot(s, t, nl);
     const int64_t p = s.plist[i];
     double sig[6] = {0, 0, 0, 0, 0, 0}, de[6], sv[SV_N], out[6];
 #pragma unroll
@@ -1073,7 +1086,9 @@ __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return(Dev
     const double rho = s.pbuf[(int64_t)6 * np + i];
 #pragma unroll
     for (int k = 0; k < SV_N; ++k) sv[k] = s.sv[(int64_t)k * np + p];
-    material_compute_stress(s.mats[s.mat[p]], sig, de, rho, sv, out);
+    int nc = 0;
+    material_compute_stress(s.mats[s.mat[p]], sig, de, rho, sv, out, &nc);
+    s.rpass[p] = (uint8_t)(nc < 255 ? nc : 255);
 #pragma unroll
     for (int k = 0; k < SV_N; ++k) s.sv[(int64_t)k * np + p] = sv[k];
 #pragma unroll
@@ -1160,9 +1175,10 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
   const int64_t np = s.np, nn = s.nn;
   if (np == 0) return;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
-  if (s.sv) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
-  const unsigned pb128 = nblocks(np, 128), nb = nblocks(nn, 256);
-  const unsigned mcb = (unsigned)std::min<int64_t>(nblocks(np, 128), 148 * 8);
+  if (s.sv) cudaMemsetAsync(s.nplastic, 0, 2 * sizeof(unsigned), st);  // and nplastic_heavy
+  const unsigned nt = (unsigned)node_block(a);
+  const unsigned pb128 = nblocks(np, 128), nb = nblocks(nn, nt);
+  const unsigned mcb = (unsigned)std::min<int64_t>(nblocks(np, 128), 148 * return_blocks(a));
   auto mc_returns = [&]() {
     if (!s.sv) return;
     pr.begin(K_MC_RETURN, st);
@@ -1174,8 +1190,12 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     auto launch = [&](auto aff) {
       constexpr int AFF = decltype(aff)::value;
       constexpr int TT = p2g_tile_t<BOX, AFF>();
-      k_p2g_tiles<DIM, MODE, BOX, AFF><<<nblocks(s.ncells, TT / Elem<DIM>::NV), TT, 0, st>>>(
-          s, a.g[0], a.g[1], a.g[2]);
+      if (BOX && !AFF && tile_threads(a, BOX) == 128)
+        k_p2g_tiles<DIM, MODE, BOX, AFF, 128><<<nblocks(s.ncells, 128 / Elem<DIM>::NV), 128, 0, st>>>(
+            s, a.g[0], a.g[1], a.g[2]);
+      else
+        k_p2g_tiles<DIM, MODE, BOX, AFF><<<nblocks(s.ncells, TT / Elem<DIM>::NV), TT, 0, st>>>(
+            s, a.g[0], a.g[1], a.g[2]);
     };
     if constexpr (MODE != 1) {  // the mass-momentum mapping velocity
       if (a.vupd == 2 || a.vupd == 4) return launch(std::integral_constant<int, 1>{});
@@ -1204,7 +1224,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     p2g(std::integral_constant<int, 2>{});
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
-    k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    k_nodes<DIM, 1><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
     if (a.flip)
@@ -1218,7 +1238,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     p2g(std::integral_constant<int, 0>{});
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
-    k_nodes<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    k_nodes<DIM, 0><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_STRESS, st);
     k_stress<DIM, BOX><<<pb128, 128, 0, st>>>(s, a.dt);
@@ -1234,7 +1254,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     if (a.phase == 1) return;
   usl_second_half:
     pr.begin(K_NODES_VEL, st);
-    k_nodes<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    k_nodes<DIM, 1><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
     const size_t sm = staged_smem_bytes<DIM>(s.sv != nullptr);
@@ -1254,7 +1274,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     p2g(std::integral_constant<int, 0>{});
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
-    k_nodes<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    k_nodes<DIM, 0><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_STRESS, st);
     k_stress<DIM, BOX><<<pb128, 128, 0, st>>>(s, a.dt);
@@ -1264,7 +1284,7 @@ void step_impl(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& 
     p2g(std::integral_constant<int, 1>{});
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
-    k_nodes<DIM, 2><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    k_nodes<DIM, 2><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_G2P, st);
     g2p(std::false_type{});

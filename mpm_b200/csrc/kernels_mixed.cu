@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "mpm_bulk.cuh"
 #include "mpm_device.cuh"
@@ -93,11 +94,17 @@ struct MTileRows {
   static constexpr int N = INV + (FORCES && !BOX ? DIM * DIM : 0);
 };
 
-template <int DIM, int MODE, bool BOX>
-__global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOCKS)
+// On box cells the tile may also take 128 threads (a launch-shape choice);
+// the blocks per SM scale so that the registers per thread stay the same.
+template <bool BOX, int T>
+constexpr int mixed_tile_min_blocks() {
+  return BOX ? MPM_MIXED_P2G_TILE_MIN_BLOCKS * 256 / T : MPM_MIXED_P2G_TILE_MIN_BLOCKS;
+}
+
+template <int DIM, int MODE, bool BOX, int T = p2g_tile_t<BOX>()>
+__global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T>()))
     k_p2g_tiles_mixed(DevState s, float g0, float g1, float g2) {
   constexpr int NV = Elem<DIM>::NV;
-  constexpr int T = p2g_tile_t<BOX>();
   constexpr int CB = T / NV;
   constexpr int NVAL = 1 + 3 * DIM;
   constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM;
@@ -217,16 +224,18 @@ __global__ void __launch_bounds__(p2g_tile_t<BOX>(), MPM_MIXED_P2G_TILE_MIN_BLOC
 
 // ---------------------------------------------------------------- node update
 // The cell partials of a node (ascending cell id) added in FP64.
-template <int DIM>
-__device__ __forceinline__ bool gather_node_mixed(const DevState& s, int64_t node, int v0, int nv,
-                                                  double* sum) {
+template <int DIM, int V0, int NVS>
+__device__ __forceinline__ bool gather_node_mixed(const DevState& s, int64_t node, double* sum) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int NVAL = 1 + 3 * DIM;
-  for (int v = 0; v < nv; ++v) sum[v] = 0.;
+#pragma unroll
+  for (int v = 0; v < NVS; ++v) sum[v] = 0.;
   bool active = false;
   auto add = [&](int c, int slot) {
-    const float* src = s.partials_f + ((int64_t)c * NV + slot) * NVAL + v0;
-    for (int v = 0; v < nv; ++v) sum[v] += (double)src[v];
+    float src[NVS];
+    load_partial_row<float, NVAL, V0, NVS>(s.partials_f + ((int64_t)c * NV + slot) * NVAL, src);
+#pragma unroll
+    for (int v = 0; v < NVS; ++v) sum[v] += (double)src[v];
     active = true;
   };
   if (s.structured) {
@@ -286,14 +295,14 @@ __global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, d
   const int64_t nn = s.nn;
   constexpr int NVAL = 1 + 3 * DIM;
   double sum[NVAL];
-  const int v0 = MODE == 2 ? 1 + DIM : 0;
-  const int nv = MODE == 0 ? 1 + DIM : (MODE == 1 ? NVAL : 2 * DIM);
-  if (!gather_node_mixed<DIM>(s, n, v0, nv, sum)) return;
+  constexpr int V0 = MODE == 2 ? 1 + DIM : 0;
+  constexpr int NVS = MODE == 0 ? 1 + DIM : (MODE == 1 ? NVAL : 2 * DIM);
+  if (!gather_node_mixed<DIM, V0, NVS>(s, n, sum)) return;
   const int bci = s.bc_index[n];
   double vel[DIM], acc[DIM];
   if constexpr (MODE == 2) {
     double mm[1];
-    gather_node_mixed<DIM>(s, n, 0, 1, mm);
+    gather_node_mixed<DIM, 0, 1>(s, n, mm);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       vel[d] = (double)s.nfv[(int64_t)d * nn + n];
@@ -482,7 +491,7 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, const Row
     } else {
       // plastic, apex or separated: the FP64 update of k_mc_return_mixed
       deferred = true;
-      const unsigned i = defer_slot(s);
+      const unsigned i = defer_slot_by_cost(s, r.index());
       s.plist[i] = (int32_t)r.index();
 #pragma unroll
       for (int k = 0; k < 6; ++k) s.pbuf_f[(int64_t)k * s.np + i] = dstrain[k];
@@ -801,13 +810,16 @@ void prefer_shared_memory() {
 }
 
 // The MohrCoulomb updates deferred by stress_update_mixed, one thread per
-// listed particle: the full FP64 update (mohr_coulomb.tcc:348-513) from the
-// FP32 stress and state before the step's update, rounded back to FP32.
+// listed particle (the light entries, then the heavy ones): the full FP64
+// update (mohr_coulomb.tcc:348-513) from the FP32 stress and state before the
+// step's update, rounded back to FP32; the number of corrections is kept for
+// the next step's grouping.
 template <int DIM>
 __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return_mixed(DevState s) {
-  const unsigned n = *s.nplastic;
+  const unsigned nl = *s.nplastic, n = nl + *s.nplastic_heavy;
   const int64_t np = s.np;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned i = list_slot(s, t, nl);
     const int64_t p = s.plist[i];
     const MGlobalRow<DIM> r{s, p};
     const int mi = s.mat[p];
@@ -828,7 +840,9 @@ __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return_mix
 #pragma unroll
     for (int k = 0; k < SVF_N; ++k) svd[k] = (double)svf[k];
     svd[SV_PD] = r.pd();
-    mc_compute_stress<double, double>(s.mats[mi], sd, ded, (double)rho, svd, svd[SV_PD], od);
+    int nc = 0;
+    mc_compute_stress<double, double>(s.mats[mi], sd, ded, (double)rho, svd, svd[SV_PD], od, &nc);
+    s.rpass[p] = (uint8_t)(nc < 255 ? nc : 255);
 #pragma unroll
     for (int k = 0; k < 6; ++k) out[k] = (float)od[k];
 #pragma unroll
@@ -851,29 +865,40 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
   const int64_t np = s.np, nn = s.nn;
   if (np == 0) return;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
-  if (s.svf) cudaMemsetAsync(s.nplastic, 0, sizeof(unsigned), st);
-  const unsigned pb = nblk(np, 128), nb = nblk(nn, 256), tile = p2g_tile_t<BOX>();
-  const unsigned tb = nblk(s.ncells, tile / Elem<DIM>::NV);
-  const unsigned mcb = (unsigned)(pb < 148 * 8 ? pb : 148 * 8);
+  if (s.svf) cudaMemsetAsync(s.nplastic, 0, 2 * sizeof(unsigned), st);  // and nplastic_heavy
+  const float g0 = (float)a.g[0], g1 = (float)a.g[1], g2 = (float)a.g[2];
+  const unsigned nt = (unsigned)node_block(a);
+  const unsigned pb = nblk(np, 128), nb = nblk(nn, nt);
+  const unsigned mcap = 148u * (unsigned)return_blocks(a);
+  const unsigned mcb = pb < mcap ? pb : mcap;
+  // P2G cell tiles of the step's launch shape
+  auto p2g = [&](auto mode) {
+    constexpr int MODE = decltype(mode)::value;
+    constexpr int NV = Elem<DIM>::NV;
+    if (BOX && tile_threads(a, BOX) == 128)
+      k_p2g_tiles_mixed<DIM, MODE, BOX, 128><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s, g0, g1, g2);
+    else
+      k_p2g_tiles_mixed<DIM, MODE, BOX><<<nblk(s.ncells, p2g_tile_t<BOX>() / NV), p2g_tile_t<BOX>(),
+                                          0, st>>>(s, g0, g1, g2);
+  };
   auto mc_returns = [&]() {
     if (!s.svf) return;
     pr.begin(K_MC_RETURN, st);
     k_mc_return_mixed<DIM><<<mcb, 128, 0, st>>>(s);
     pr.end(K_MC_RETURN, st);
   };
-  const float g0 = (float)a.g[0], g1 = (float)a.g[1], g2 = (float)a.g[2];
   if (a.scheme == 1 && a.phase == 2) goto usl_second_half;
   pr.begin(K_SORT, st, SORT_KERNELS);
   counting_sort(s, st);
   pr.end(K_SORT, st);
   if (a.scheme == 1) {  // USL
     pr.begin(K_P2G, st);
-    k_p2g_tiles_mixed<DIM, 2, BOX><<<tb, tile, 0, st>>>(s, g0, g1, g2);
+    p2g(std::integral_constant<int, 2>{});
     pr.end(K_P2G, st);
     if (a.phase == 1) return;
   usl_second_half:
     pr.begin(K_NODES_VEL, st);
-    k_nodes_mixed<DIM, 1><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    k_nodes_mixed<DIM, 1><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
     const size_t sm = mixed_staged_smem_bytes<DIM>(s.svf != nullptr);
@@ -888,20 +913,20 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     mc_returns();
   } else {  // USF
     pr.begin(K_P2G, st);
-    k_p2g_tiles_mixed<DIM, 0, BOX><<<tb, tile, 0, st>>>(s, g0, g1, g2);
+    p2g(std::integral_constant<int, 0>{});
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
-    k_nodes_mixed<DIM, 0><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    k_nodes_mixed<DIM, 0><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_STRESS, st);
     k_stress_mixed<DIM, BOX><<<pb, 128, 0, st>>>(s, (float)a.dt);
     pr.end(K_STRESS, st);
     mc_returns();
     pr.begin(K_P2G_FORCES, st);
-    k_p2g_tiles_mixed<DIM, 1, BOX><<<tb, tile, 0, st>>>(s, g0, g1, g2);
+    p2g(std::integral_constant<int, 1>{});
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
-    k_nodes_mixed<DIM, 2><<<nb, 256, 0, st>>>(s, a.dt, a.damping);
+    k_nodes_mixed<DIM, 2><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_G2P, st);
     if (a.flip)

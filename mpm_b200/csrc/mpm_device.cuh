@@ -4,6 +4,8 @@
 // compiles them with its own floating-point contraction setting.
 #pragma once
 
+#include <type_traits>
+
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -30,6 +32,51 @@ __device__ __forceinline__ unsigned defer_slot(const DevState& s) {
   if (g.thread_rank() == 0) base = atomicAdd(s.nplastic, g.size());
   base = g.shfl(base, 0);
   return base + g.thread_rank();
+}
+
+// A slot in the deferred list of the value steps for particle p: from the
+// front when its last return took at most one correction, from the back
+// otherwise (see DevState::nplastic_heavy).  One atomic per class per group of
+// lanes that defer together.
+__device__ __forceinline__ unsigned defer_slot_by_cost(const DevState& s, int64_t p) {
+  const bool heavy = s.rpass[p] > 1;
+  const unsigned act = __activemask();
+  const unsigned hv = __ballot_sync(act, heavy), lt = act & ~hv;
+  const int lane = threadIdx.x & 31;
+  const int lead_h = __ffs(hv) - 1, lead_l = __ffs(lt) - 1;
+  unsigned base = 0;
+  if (lane == lead_l) base = atomicAdd(s.nplastic, (unsigned)__popc(lt));
+  if (lane == lead_h) base = atomicAdd(s.nplastic_heavy, (unsigned)__popc(hv));
+  base = __shfl_sync(act, base, heavy ? lead_h : lead_l);
+  const unsigned below = (1u << lane) - 1u;
+  const unsigned k = base + (unsigned)__popc((heavy ? hv : lt) & below);
+  return heavy ? (unsigned)(s.np - 1) - k : k;
+}
+
+// Slot of the t-th entry of the list filled by defer_slot_by_cost
+// (n_light = *nplastic entries from the front, then the heavy ones).
+__device__ __forceinline__ unsigned list_slot(const DevState& s, unsigned t, unsigned n_light) {
+  return t < n_light ? t : (unsigned)(s.np - 1) - (t - n_light);
+}
+
+// Values V0 .. V0 + NVS - 1 of one cell-slot partial row of NVAL values:
+// pairs loaded as one 8- or 16-byte access when the row length and the first
+// value are even (rows then start on a multiple of two values).
+template <typename T, int NVAL, int V0, int NVS>
+__device__ __forceinline__ void load_partial_row(const T* row, T* out) {
+  if constexpr (NVAL % 2 == 0 && V0 % 2 == 0 && NVS % 2 == 0) {
+    using T2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    const T2* r2 = reinterpret_cast<const T2*>(row + V0);
+#pragma unroll
+    for (int k = 0; k < NVS / 2; ++k) {
+      const T2 v = r2[k];
+      out[2 * k] = v.x;
+      out[2 * k + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < NVS; ++v) out[v] = row[V0 + v];
+  }
 }
 
 template <int DIM>

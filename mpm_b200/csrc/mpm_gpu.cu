@@ -258,6 +258,7 @@ struct mpm_gpu_solver {
   DevBuf<unsigned> d_words;  // [0] nlost, [1] err, [2] nplastic
   DevBuf<int32_t> d_plist;
   DevBuf<double> d_pbuf;
+  DevBuf<uint8_t> d_rpass;
   DevBuf<MaterialParams> d_mats;
   DevBuf<double> d_axis[3];
   DevBuf<double> d_axis_ihl[3];
@@ -289,6 +290,9 @@ struct mpm_gpu_solver {
   size_t h_stage_bytes = 0;
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
 
+  // launch shape of the value steps (mpm_gpu_set_launch_shape, mpm_gpu_autotune);
+  // zeros are the built-in defaults
+  int shape_p2g_tile = 0, shape_node_threads = 0, shape_return_bps = 0;
   // one captured step, replayed while the device state and step arguments
   // stay the same
   cudaGraphExec_t graph = nullptr;
@@ -782,9 +786,12 @@ void allocate_particles(mpm_gpu_t h) {
   if (h->any_mc) {
     h->d_plist.resize(np);
     h->d_pbuf.resize((size_t)7 * np);
+    h->d_rpass.resize(std::max<int64_t>(1, np));
+    ck(cudaMemsetAsync(h->d_rpass.p, 0, std::max<int64_t>(1, np), h->stream), "memset");
   } else {
     h->d_plist.free();
     h->d_pbuf.free();
+    h->d_rpass.free();
   }
   if (h->any_mc && h->mixed)
     h->d_svf.resize((size_t)SVF_N * np);
@@ -844,6 +851,7 @@ void refresh_state(mpm_gpu_t h) {
   s.nlost = h->d_words.p;
   s.err = h->d_words.p + 1;
   s.nplastic = h->d_words.p + 2;
+  s.nplastic_heavy = h->d_words.p + 3;
   for (int k = 0; k < MAX_TANGENTS; ++k) {
     const bool on = h->ntangent > 0;
     s.pft[k] = on ? h->d_pft[k].p : nullptr;
@@ -857,6 +865,7 @@ void refresh_state(mpm_gpu_t h) {
   s.any_softening = 0;
   for (auto& m : h->mats) s.any_softening |= (m.type == 1 && m.softening) ? 1 : 0;
   s.plist = h->any_mc ? h->d_plist.p : nullptr;
+  s.rpass = h->any_mc ? h->d_rpass.p : nullptr;
   s.pbuf = h->any_mc ? h->d_pbuf.p : nullptr;
   s.pbuf_f = h->any_mc ? reinterpret_cast<float*>(h->d_pbuf.p) : nullptr;
   s.mats = h->d_mats.p;
@@ -1594,15 +1603,14 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
 static bool same_step(const DevState& a, const DevState& b, const StepArgs& x, const StepArgs& y) {
   return std::memcmp(&a, &b, sizeof(DevState)) == 0 && x.scheme == y.scheme && x.flip == y.flip && x.vupd == y.vupd &&
          x.remove_lost == y.remove_lost && x.dt == y.dt && x.beta == y.beta &&
-         x.damping == y.damping && x.g[0] == y.g[0] && x.g[1] == y.g[1] && x.g[2] == y.g[2];
+         x.damping == y.damping && x.g[0] == y.g[0] && x.g[1] == y.g[1] && x.g[2] == y.g[2] &&
+         x.p2g_tile == y.p2g_tile && x.node_threads == y.node_threads &&
+         x.return_blocks_per_sm == y.return_blocks_per_sm;
 }
 
-static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
-  MPM_GUARD(h)
-  if (!h->initialised) throw InvalidArg("initialise or load particles first");
-  if (nsteps < 0) throw InvalidArg("negative step count");
-  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
-  refresh_state(h);  // constraint or material tables may have been reallocated
+// The step arguments of the solver's configuration and launch shape (gravity
+// and phase set by the caller).
+static StepArgs base_step_args(mpm_gpu_t h) {
   StepArgs a{};
   a.scheme = h->cfg.scheme;
   a.flip = h->cfg.velocity_update == MPM_VELOCITY_FLIP ? 1 : 0;
@@ -1611,6 +1619,19 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
   a.dt = h->cfg.dt;
   a.beta = h->cfg.blending_ratio;
   a.damping = h->cfg.damping_factor;
+  a.p2g_tile = h->shape_p2g_tile;
+  a.node_threads = h->shape_node_threads;
+  a.return_blocks_per_sm = h->shape_return_bps;
+  return a;
+}
+
+static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("initialise or load particles first");
+  if (nsteps < 0) throw InvalidArg("negative step count");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  refresh_state(h);  // constraint or material tables may have been reallocated
+  StepArgs a = base_step_args(h);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (elapsed_ms) {
     ck(cudaEventCreate(&e0), "cudaEventCreate");
@@ -1696,6 +1717,131 @@ int mpm_gpu_step(mpm_gpu_t h, int64_t nsteps) { return run_steps(h, nsteps, null
 int mpm_gpu_step_timed(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
   if (!elapsed_ms) return fail(h, MPM_ERR_INVALID, "null elapsed_ms");
   return run_steps(h, nsteps, elapsed_ms);
+}
+
+int mpm_gpu_set_launch_shape(mpm_gpu_t h, int32_t p2g_tile, int32_t node_threads,
+                             int32_t return_blocks_per_sm) {
+  MPM_GUARD(h)
+  if (p2g_tile != 0 && p2g_tile != 128 && p2g_tile != 256)
+    throw InvalidArg("p2g_tile must be 0 (default), 128 or 256");
+  if (node_threads != 0 && node_threads != 128 && node_threads != 256)
+    throw InvalidArg("node_threads must be 0 (default), 128 or 256");
+  if (return_blocks_per_sm != 0 && return_blocks_per_sm != 4 && return_blocks_per_sm != 8 &&
+      return_blocks_per_sm != 16)
+    throw InvalidArg("return_blocks_per_sm must be 0 (default), 4, 8 or 16");
+  h->shape_p2g_tile = p2g_tile;
+  h->shape_node_threads = node_threads;
+  h->shape_return_bps = return_blocks_per_sm;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_get_launch_shape(mpm_gpu_t h, int32_t* shape) {
+  MPM_GUARD(h)
+  if (!shape) throw InvalidArg("null shape");
+  const StepArgs a = base_step_args(h);
+  shape[0] = tile_threads(a, h->structured);
+  shape[1] = node_block(a);
+  shape[2] = return_blocks(a);
+  MPM_END(h)
+  return MPM_OK;
+}
+
+// Time each launch-shape candidate on the solver's own state, one field at a
+// time (P2G tile, node block, return blocks per SM; each field's best kept
+// while the next is tried), restoring the particle state and step counter
+// before every trial and at the end.  The launch shape changes no result, so
+// the run continues exactly as it would have.
+int mpm_gpu_autotune(mpm_gpu_t h, int64_t steps, char* report, size_t report_len) {
+  MPM_GUARD(h)
+  if (!h->initialised) throw InvalidArg("initialise or load particles first");
+  if (steps < 3) throw InvalidArg("autotune needs at least 3 steps per trial");
+  if (h->ntangent > 0) throw InvalidArg("turn sensitivities off first");
+  ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  // the state a step changes
+  struct Part {
+    void* p;
+    size_t bytes;
+  };
+  std::vector<Part> parts = {{h->d_pf.p, h->d_pf.n * sizeof(double)},
+                             {h->d_sv.p, h->d_sv.n * sizeof(double)},
+                             {h->d_pm.p, h->d_pm.n * sizeof(float)},
+                             {h->d_svf.p, h->d_svf.n * sizeof(float)},
+                             {h->d_cell.p, h->d_cell.n * sizeof(int32_t)},
+                             {h->d_mapb.p, h->d_mapb.n * sizeof(double)},
+                             {h->d_rpass.p, h->d_rpass.n * sizeof(uint8_t)}};
+  size_t total = 0;
+  for (auto& q : parts)
+    if (q.p) total += (q.bytes + 255) & ~(size_t)255;
+  uint8_t* snap = nullptr;
+  if (cudaMalloc(&snap, std::max<size_t>(total, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, MPM_ERR_ALLOC, "autotune needs " + std::to_string(total >> 20) +
+                                      " MiB of device memory for a copy of the particle state");
+  }
+  auto copy = [&](bool save) {
+    size_t off = 0;
+    for (auto& q : parts) {
+      if (!q.p || !q.bytes) continue;
+      void* d = save ? (void*)(snap + off) : q.p;
+      const void* src = save ? q.p : (const void*)(snap + off);
+      ck(cudaMemcpyAsync(d, src, q.bytes, cudaMemcpyDeviceToDevice, h->stream), "D2D");
+      off += (q.bytes + 255) & ~(size_t)255;
+    }
+  };
+  const int64_t step0 = h->step;
+  const int saved[3] = {h->shape_p2g_tile, h->shape_node_threads, h->shape_return_bps};
+  int* field[3] = {&h->shape_p2g_tile, &h->shape_node_threads, &h->shape_return_bps};
+  const char* names[3] = {"p2g_tile", "node_threads", "return_blocks_per_sm"};
+  const std::vector<int> cand[3] = {
+      h->structured ? std::vector<int>{256, 128} : std::vector<int>{128}, {256, 128}, {8, 4, 16}};
+  std::string js = "{\"steps_per_trial\": " + std::to_string(steps) + ", \"trials\": {";
+  int rc = MPM_OK;
+  try {
+    copy(true);
+    for (int f = 0; f < 3 && rc == MPM_OK; ++f) {
+      double best = 1e300;
+      int best_v = cand[f][0];
+      js += std::string(f ? ", " : "") + "\"" + names[f] + "\": {";
+      for (size_t k = 0; k < cand[f].size() && rc == MPM_OK; ++k) {
+        *field[f] = cand[f][k];
+        copy(false);
+        h->step = step0;
+        double ms = 0.;
+        rc = run_steps(h, steps, &ms);
+        js += std::string(k ? ", " : "") + "\"" + std::to_string(cand[f][k]) + "\": " +
+              std::to_string(ms / (double)steps);
+        if (ms < best) {
+          best = ms;
+          best_v = cand[f][k];
+        }
+      }
+      js += "}";
+      *field[f] = best_v;
+    }
+    copy(false);
+    h->step = step0;
+    ck(cudaStreamSynchronize(h->stream), "autotune");
+  } catch (...) {
+    cudaFree(snap);
+    for (int f = 0; f < 3; ++f) *field[f] = saved[f];
+    throw;
+  }
+  cudaFree(snap);
+  if (rc != MPM_OK) {  // a trial failed: keep the old shape, report its error
+    for (int f = 0; f < 3; ++f) *field[f] = saved[f];
+    return rc;
+  }
+  js += "}, \"chosen\": {\"p2g_tile\": " + std::to_string(h->shape_p2g_tile) +
+        ", \"node_threads\": " + std::to_string(h->shape_node_threads) +
+        ", \"return_blocks_per_sm\": " + std::to_string(h->shape_return_bps) + "}}";
+  if (report && report_len) {
+    const size_t n = std::min(js.size(), report_len - 1);
+    std::memcpy(report, js.data(), n);
+    report[n] = '\0';
+  }
+  MPM_END(h)
+  return MPM_OK;
 }
 
 int mpm_gpu_set_profiling(mpm_gpu_t h, int32_t enable) {
@@ -2281,17 +2427,6 @@ int mpm_gpu_material_stress_batch(int32_t device, int32_t dim, const char* type,
 // ------------------------------------------------------------ adjoint
 namespace {
 
-StepArgs base_step_args(mpm_gpu_t h) {
-  StepArgs a{};
-  a.scheme = h->cfg.scheme;
-  a.flip = h->cfg.velocity_update == MPM_VELOCITY_FLIP ? 1 : 0;
-  a.vupd = h->cfg.velocity_update;
-  a.remove_lost = h->cfg.locate_particles ? 0 : 1;
-  a.dt = h->cfg.dt;
-  a.beta = h->cfg.blending_ratio;
-  a.damping = h->cfg.damping_factor;
-  return a;
-}
 
 // gravity of solver step `step` (the ramp of mpm_explicit.tcc:145-153, as run_steps)
 void set_gravity(mpm_gpu_t h, StepArgs& a, int64_t step) {
@@ -2324,7 +2459,8 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
                            const int32_t* material_ids, const int32_t* kinds) {
   MPM_GUARD(h)
   if (!h->initialised) throw InvalidArg("initialise or load particles first");
-  if (nsteps < 1 || checkpoint_every < 1) throw InvalidArg("nsteps and checkpoint_every must be >= 1");
+  if (nsteps < 1 || checkpoint_every < 0)
+    throw InvalidArg("nsteps must be >= 1 and checkpoint_every >= 0 (0: chosen by the library)");
   if (nparams < 0 || nparams > MAX_TANGENTS) throw InvalidArg("at most 2 parameters");
   if (nparams > 0 && (!material_ids || !kinds)) throw InvalidArg("null parameter list");
   if (h->mixed) return fail(h, MPM_ERR_UNSUPPORTED, "the adjoint runs in FP64 only");
@@ -2350,7 +2486,6 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
   h->tape.reset(new AdjointTape());
   AdjointTape& t = *h->tape;
   t.nsteps = nsteps;
-  t.every = checkpoint_every;
   t.nparams = nparams;
   t.np = h->np;
   t.pf_n = h->d_pf.n;
@@ -2358,15 +2493,28 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
   t.cell_n = h->d_cell.n;
   const int dim = h->dim;
   const int64_t np = h->npad;
-  const int64_t nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
-  const int64_t nseg = std::min(checkpoint_every, nsteps);
   const int ns = dim == 2 ? PF<2>::NS : PF<3>::NS;
   const size_t state_bytes = t.pf_n * 8 + t.sv_n * 8 + t.cell_n * 4;
   const size_t work_bytes = (size_t)np * 8 * ((2 * dim + ns + 1) + 6 + ns + (3 * dim + 6) + MAX_TANGENTS) +
                             (size_t)h->ncells * h->nv * 2 * dim * 8 + (size_t)h->nnodes * (1 + 3 * dim) * 8;
-  const size_t need = state_bytes * (size_t)(nck + nseg + 1) + work_bytes;
+  auto need_for = [&](int64_t every) {
+    const int64_t nck = (nsteps + every - 1) / every;
+    return state_bytes * (size_t)(nck + std::min(every, nsteps) + 1) + work_bytes;
+  };
   size_t free_b = 0, total_b = 0;
   ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+  if (checkpoint_every == 0) {
+    // every step's start state kept when half the free memory holds them (the
+    // reverse sweep then recomputes nothing), else checkpoints sqrt(nsteps)
+    // apart, the least memory
+    checkpoint_every = 1;
+    if (need_for(1) > free_b / 2)
+      checkpoint_every = std::max<int64_t>(1, (int64_t)std::ceil(std::sqrt((double)nsteps)));
+  }
+  t.every = checkpoint_every;
+  const int64_t nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  const int64_t nseg = std::min(checkpoint_every, nsteps);
+  const size_t need = need_for(checkpoint_every);
   if (need > free_b) {
     h->tape.reset();
     return fail(h, MPM_ERR_ALLOC, "the adjoint needs " + std::to_string(need >> 20) + " MiB (" +
@@ -2484,11 +2632,12 @@ int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_d
       set_gravity(h, a, t.step0 + k);
       launch_step_fp64(dim, h->ds, a, h->stream, h->prof);
     }
-    copy_state(h, t, t.seg_pf.p + t.pf_n * (s1 - 1 - s0), t.seg_sv.p + t.sv_n * (s1 - 1 - s0),
-               t.seg_cell.p + t.cell_n * (s1 - 1 - s0), true);
+    // the device state is now the last step's start: reversed first, with no copy
     for (int64_t k = s1 - 1; k >= s0; --k) {
       const int64_t j = k - s0;
-      copy_state(h, t, t.seg_pf.p + t.pf_n * j, t.seg_sv.p + t.sv_n * j, t.seg_cell.p + t.cell_n * j, false);
+      if (k < s1 - 1)
+        copy_state(h, t, t.seg_pf.p + t.pf_n * j, t.seg_sv.p + t.sv_n * j, t.seg_cell.p + t.cell_n * j,
+                   false);
       set_gravity(h, a, t.step0 + k);
       h->prof.begin(K_ADJ_RECOMPUTE, h->stream, SORT_KERNELS + 2);
       launch_p2g_nodes_fp64(dim, h->ds, a, h->stream);

@@ -21,7 +21,19 @@ struct StepArgs {
   double g[3];       // gravity of this step (ramp applied)
   int phase;         // USL: 0 the whole step, 1 sort and P2G only, 2 the rest (node
                      // update onward) -- a slab run exchanges halo partials between them
+  // Launch shape of the value steps (the results do not depend on it):
+  // threads of a P2G cell tile on box cells (128 or 256), threads of a
+  // node-kernel block (128 or 256), blocks per SM of the plastic-return kernel
+  // (4, 8 or 16).  Zero selects the built-in default.
+  int p2g_tile;
+  int node_threads;
+  int return_blocks_per_sm;
 };
+
+// The launch shape a step uses: the built-in defaults where a field is zero.
+inline int tile_threads(const StepArgs& a, bool box) { return box && a.p2g_tile ? a.p2g_tile : (box ? 256 : 128); }
+inline int node_block(const StepArgs& a) { return a.node_threads ? a.node_threads : 256; }
+inline int return_blocks(const StepArgs& a) { return a.return_blocks_per_sm ? a.return_blocks_per_sm : 8; }
 
 // Kernels of one step, for launch counting and per-kernel event timing.
 enum KernelId {

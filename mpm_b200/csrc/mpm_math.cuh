@@ -752,7 +752,7 @@ enum { MC_OK = 0, MC_NONFINITE = 1, MC_DEFERRED = 2 };
 // elastic ones through the return iterations.
 template <typename R, typename PD, bool DEFER>
 MPM_HD int mc_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R density, R* sv,
-                     PD& pdstrain_io, R* out) {
+                     PD& pdstrain_io, R* out, int* corrections = nullptr) {
   const R critical_density = m.min_packing * m.grain_density;
   const R pdstrain = R(pdstrain_io);
   if (m.softening && pdstrain > m.pd_peak) {
@@ -844,7 +844,8 @@ MPM_HD int mc_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R
     sub_lambda_de(m, lambda_trial, dp_trial, upd);
     dpdstrain = lambda_trial * dp_dq_trial;
   }
-  for (int itr = 0; itr < 100; ++itr) {
+  int itr = 0;
+  for (; itr < 100; ++itr) {
     mc_invariants_o(upd, sv, lt);
     yt_trial = mc_yield_state_o(yf_trial, sv, lt, ft);
     if (yf_trial[0] < Tolerance && yf_trial[1] < Tolerance) break;
@@ -856,6 +857,7 @@ MPM_HD int mc_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R
     sub_lambda_de(m, lambda_trial, dp_trial, upd);
     dpdstrain += lambda_trial * dp_dq_trial;
   }
+  if (corrections) *corrections = itr;
   mc_invariants_o(upd, sv, lt);
   pdstrain_io += PD(dpdstrain);
   bool finite = true;
@@ -870,8 +872,9 @@ MPM_HD int mc_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R
 // The full update; false when the return left the stress non-finite.
 template <typename R, typename PD>
 MPM_HD bool mc_compute_stress(const MaterialT<R>& m, const R* stress, const R* dstrain, R density,
-                              R* sv, PD& pdstrain_io, R* out) {
-  return mc_stress<R, PD, false>(m, stress, dstrain, density, sv, pdstrain_io, out) == MC_OK;
+                              R* sv, PD& pdstrain_io, R* out, int* corrections = nullptr) {
+  return mc_stress<R, PD, false>(m, stress, dstrain, density, sv, pdstrain_io, out, corrections) ==
+         MC_OK;
 }
 
 // Material<Tdim>::compute_stress dispatch (material.h:97-106)
@@ -891,13 +894,13 @@ MPM_HD bool material_compute_stress(const MaterialT<R>& m, const R* stress, cons
 // FP64 form used by the FP64 kernels: the state array holds pdstrain in SV_PD.
 MPM_HD void material_compute_stress(const MaterialParams& m, const double* stress,
                                     const double* dstrain, double density, double* sv,
-                                    double* out) {
+                                    double* out, int* corrections = nullptr) {
   if (m.type == 0) {
     double pd = 0.;
     material_compute_stress<double, double>(m, stress, dstrain, density, sv, pd, out);
     return;
   }
-  material_compute_stress<double, double>(m, stress, dstrain, density, sv, sv[SV_PD], out);
+  mc_compute_stress<double, double>(m, stress, dstrain, density, sv, sv[SV_PD], out, corrections);
 }
 
 // ---------------------------------------------------------------- node update

@@ -136,6 +136,13 @@ struct DevState {
   double* pbuf = nullptr;        // [7][np] (FP64 path)
   float* pbuf_f = nullptr;       // [7][np] (mixed path, same allocation)
   unsigned* nplastic = nullptr;
+  // The value steps fill the list from both ends: points whose last return
+  // took at most one correction from slot 0 up (nplastic of them), the others
+  // from slot np - 1 down (nplastic_heavy), so that the lanes of a warp in the
+  // return kernel carry returns of similar length.  rpass[p] is the number of
+  // corrections of particle p's last return (0 for a point never returned).
+  unsigned* nplastic_heavy = nullptr;
+  uint8_t* rpass = nullptr;      // [np]
   unsigned* err = nullptr;       // ErrorBits
 
   // mixed precision (null on the FP64 path)

@@ -55,7 +55,7 @@ if torch is not None:
             return g, None, None, None
 
 
-def adjoint_gradient(build, theta, params, nsteps, x_target, checkpoint_every=100):
+def adjoint_gradient(build, theta, params, nsteps, x_target, checkpoint_every=0):
     """(loss, dL/dtheta) of L = sum |x_final - x_target|^2 by the reverse sweep."""
     s = build(theta)
     loss, g = s.adjoint_run(nsteps, params, x_target, checkpoint_every)
@@ -73,7 +73,7 @@ if torch is not None:
         particle positions (float64 tensor, n x dim)."""
 
         @staticmethod
-        def forward(ctx, theta, build, params, nsteps, checkpoint_every=100):
+        def forward(ctx, theta, build, params, nsteps, checkpoint_every=0):
             s = build(theta.detach().cpu().numpy())
             s.adjoint_record(nsteps, params, checkpoint_every)
             ctx.solver = s

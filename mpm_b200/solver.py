@@ -150,6 +150,27 @@ class Solver:
         self._ck(self.L.mpm_gpu_step_timed(self.h, n, C.byref(ms)))
         return ms.value
 
+    def set_launch_shape(self, p2g_tile=0, node_threads=0, return_blocks_per_sm=0):
+        """Launch shape of the steps (0: the built-in default); results do
+        not depend on it."""
+        self._ck(self.L.mpm_gpu_set_launch_shape(self.h, int(p2g_tile), int(node_threads),
+                                                 int(return_blocks_per_sm)))
+
+    def launch_shape(self):
+        """(p2g_tile, node_threads, return_blocks_per_sm) in use."""
+        out = (C.c_int32 * 3)()
+        self._ck(self.L.mpm_gpu_get_launch_shape(self.h, out))
+        return tuple(int(v) for v in out)
+
+    def autotune(self, steps=5):
+        """Time the launch-shape candidates on this solver's state and keep
+        the fastest; the state and step counter are restored, so the run
+        continues as without it.  Returns the report (ms per step per
+        candidate, the chosen shape)."""
+        buf = C.create_string_buffer(4096)
+        self._ck(self.L.mpm_gpu_autotune(self.h, int(steps), buf, len(buf)))
+        return json.loads(buf.value.decode())
+
     def set_profiling(self, enable=True):
         self._ck(self.L.mpm_gpu_set_profiling(self.h, 1 if enable else 0))
 
@@ -317,7 +338,7 @@ class Solver:
                                                    _dp(out)))
         return out if field == "stress" else out[:, :, :self.dim]
 
-    def adjoint_record(self, nsteps, params=(), checkpoint_every=100):
+    def adjoint_record(self, nsteps, params=(), checkpoint_every=0):
         """Advance ``nsteps`` keeping checkpoints for the reverse sweep;
         ``params`` as for ``set_sensitivities``."""
         n = len(params)
@@ -352,7 +373,7 @@ class Solver:
         out["v0"] = out["v0"][:, :self.dim]
         return out
 
-    def adjoint_run(self, nsteps, params, x_target, checkpoint_every=100):
+    def adjoint_run(self, nsteps, params, x_target, checkpoint_every=0):
         """(loss, dL/dparameter) of L = sum |x_final - x_target|^2."""
         n = self.nparticles
         t = np.zeros((n, 3))

@@ -183,6 +183,26 @@ def test_reverse_restores_the_end_state_and_repeats_bitwise():
         assert np.array_equal(r1[k], r2[k]), k
 
 
+def test_checkpoint_spacing_does_not_change_the_gradient():
+    """Every spacing -- each step kept (no recompute), the library's choice,
+    uneven segments, one segment -- gives the same gradient bit for bit: the
+    recomputed steps are the forward steps' own arithmetic."""
+    make = lambda th: _column(th)
+    w = None
+    out = {}
+    for every in (1, 0, 7, 45):
+        s = P.build_solver(make(THETA), precision="fp64")
+        s.adjoint_record(45, PARAMS, checkpoint_every=every)
+        if w is None:
+            x = s.read()["x"]
+            w = np.cos(np.arange(x.size)).reshape(x.shape)
+        out[every] = s.adjoint_reverse(dL_dx=w)
+        s.close()
+    for every, r in out.items():
+        for k in ("params", "x0", "v0", "stress0"):
+            assert np.array_equal(r[k], out[1][k]), (every, k)
+
+
 def test_autograd_function_runs_the_reverse_sweep():
     torch = pytest.importorskip("torch")
     from mpm_b200.sensitivity import AdjointPositions
