@@ -113,6 +113,9 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-fp64-arm", action="store_true",
                     help="skip the FP64 run reported beside the mixed one")
+    ap.add_argument("--launch-shape", default="",
+                    help="p2g_tile,node_threads,return_blocks_per_sm to use instead of "
+                         "autotuning (e.g. 128,256,8)")
     ap.add_argument("--autotune-steps", type=int, default=5,
                     help="steps per launch-shape candidate of the autotuner before the "
                          "warm-up (0 keeps the default launch shape)")
@@ -301,8 +304,13 @@ def time_arm(prob, precision, args, world, dev, clocks=None):
     t0 = time.perf_counter()
     s = P.build_solver(prob, precision=precision, device=dev)
     setup_s = time.perf_counter() - t0
-    # launch shape timed on this state, then the state restored
-    s.tune_report = s.autotune(args.autotune_steps) if args.autotune_steps else None
+    # launch shape timed on this state, then the state restored (or given)
+    s.tune_report = None
+    if args.launch_shape:
+        s.set_launch_shape(*(int(v) for v in args.launch_shape.split(",")))
+        s.tune_report = {"given": list(s.launch_shape())}
+    elif args.autotune_steps:
+        s.tune_report = s.autotune(args.autotune_steps)
     s.step(args.warmup)
     barrier(world)
     launches0 = s.launch_count
@@ -367,8 +375,12 @@ def accuracy_and_late_window(prob, args, world, dev, checkpoints):
                      "fp64_one_ulp_floor_l2": l2_errors(q, f)})
     del pert
     # the launch shape re-timed on the late state (the state is restored)
-    tune_m = mixed.autotune(args.autotune_steps) if args.autotune_steps else None
-    tune_f = fp64.autotune(args.autotune_steps) if args.autotune_steps else None
+    tune_m = tune_f = None
+    if args.launch_shape:
+        for s in (mixed, fp64):
+            s.set_launch_shape(*(int(v) for v in args.launch_shape.split(",")))
+    elif args.autotune_steps:
+        tune_m, tune_f = mixed.autotune(args.autotune_steps), fp64.autotune(args.autotune_steps)
     barrier(world)
     ms_m = max_over_ranks(mixed.step_timed(args.steps), world)
     ms_f = max_over_ranks(fp64.step_timed(args.steps), world)
@@ -422,18 +434,21 @@ def run_calibration(args, rank, world):
     # after their device work has finished); every step's start state kept
     # (no recompute), and checkpoints sqrt(steps) apart (least memory, every
     # segment recomputed)
-    a = build(theta)
-    a.step(args.warmup)
-    ones = np.ones((a.nparticles, 3))
     every_sqrt = int(np.ceil(np.sqrt(args.steps)))
     adj_times = {}
-    for every in (1, every_sqrt):
+    for every in (1, every_sqrt):  # each from the same warmed-up start
+        a = build(theta)
+        a.step(args.warmup)
+        ones = np.ones((a.nparticles, 3))
         t0 = time.perf_counter()
         a.adjoint_record(args.steps, params, checkpoint_every=every)
         a.adjoint_reverse(dL_dx=ones)
         adj_times[every] = max_over_ranks(time.perf_counter() - t0, world)
+        a.close()
     adj_s = adj_times[1]
     # the same again with per-kernel events (eager launches)
+    a = build(theta)
+    a.step(args.warmup)
     a.set_profiling(True)
     a.adjoint_record(args.steps, params, checkpoint_every=1)
     a.adjoint_reverse(dL_dx=ones)

@@ -201,7 +201,8 @@ int mpm_gpu_step_timed(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms);
  * plastic-return kernel (4, 8 or 16); 0 keeps the built-in default (256, 256,
  * 8).  Results do not depend on it.  mpm_gpu_get_launch_shape writes the
  * three values in use.  mpm_gpu_autotune times each candidate over `steps`
- * steps (at least 3) of the solver's own state, one field at a time, keeps
+ * steps (at least 3, after 2 untimed ones) of the solver's own state, one
+ * field at a time, keeps
  * the fastest, and restores the particle state and step counter, so the run
  * then continues exactly as without it; report (report_len bytes, may be
  * NULL) receives the per-candidate milliseconds per step as JSON.  It holds a

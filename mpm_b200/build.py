@@ -34,7 +34,7 @@ UNITS = [
     ("kernels_adjoint.cu", ["--fmad=false"]),
     ("h5table.cpp", []),
 ]
-HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp", "mpm_device.cuh", "mpm_bulk.cuh", "mpm_dual.cuh"]
+HEADERS = ["mpm_math.cuh", "mpm_state.cuh", "mpm_kernels.h", "json_lite.hpp", "mpm_device.cuh", "mpm_bulk.cuh", "mpm_dual.cuh", "mpm_return.cuh"]
 
 
 def _newer(target, deps):

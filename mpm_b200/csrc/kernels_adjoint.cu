@@ -38,6 +38,7 @@
 #include "mpm_device.cuh"
 #include "mpm_dual.cuh"
 #include "mpm_kernels.h"
+#include "mpm_return.cuh"
 #include "mpm_state.cuh"
 
 namespace mpm_b200 {
@@ -306,8 +307,8 @@ __global__ void __launch_bounds__(128) k_adj_return(DevState s, AdjointArgs A) {
           dd[EIDX[j - NS]].d[l] = 1.;
       }
     }
-    D pd = sv[SV_PD];
-    mc_compute_stress<D, D>(mats[slot], sg, dd, D(rho), sv, pd, out);
+    int nc = 0;
+    mc_return<D>(mats[slot], sg, dd, D(rho), sv, out, &nc);
     for (int l = 0; l < 2; ++l) {
       double t = 0.;
 #pragma unroll

@@ -21,6 +21,7 @@
 #include "mpm_bulk.cuh"
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
+#include "mpm_return.cuh"
 #include "mpm_state.cuh"
 
 // Minimum resident blocks per SM requested from the register allocator for
@@ -29,7 +30,7 @@
 #define MPM_G2P_MIN_BLOCKS 4  // 1.41 -> 1.01 ms per 4M-particle step despite spills
 #endif
 #ifndef MPM_MC_RETURN_MIN_BLOCKS
-#define MPM_MC_RETURN_MIN_BLOCKS 6  // 0.167 -> 0.155 ms at step 400 of the 4M column
+#define MPM_MC_RETURN_MIN_BLOCKS 4  // pass-loop return, 1M column at step 2000: 2 / 3 / 4 / 6 blocks -> FP64 0.362 / 0.320 / 0.323 / 0.403 ms, mixed 0.370 / 0.318 / 0.311 / 0.384 ms
 #endif
 #ifndef MPM_P2G_TILE_MIN_BLOCKS
 #define MPM_P2G_TILE_MIN_BLOCKS 4  // 64 registers on a grid: 0.39 -> 0.345 ms (4M, 3D); 5, 6 spill
@@ -1068,9 +1069,10 @@ __global__ void __launch_bounds__(128) k_commit_locate(DevState s) {
 
 // The MohrCoulomb returns deferred by stress_update, one thread per listed
 // particle (grid-stride over the light entries, then the heavy ones), from the
-// particle's stress and state before the step's update: the same call, with
-// the same inputs, as the undeferred update.  Records the return's number of
-// corrections for the next step's grouping.
+// particle's stress and state before the step's update: the evaluations of
+// the undeferred update with the same inputs, run as mc_return's passes, so
+// the same results.  Records the return's number of corrections for the next
+// step's grouping.
 template <int DIM>
 __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return(DevState s) {
   const unsigned nl = *s.nplastic, n = nl + *s.nplastic_heavy;
@@ -1087,7 +1089,7 @@ __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return(Dev
 #pragma unroll
     for (int k = 0; k < SV_N; ++k) sv[k] = s.sv[(int64_t)k * np + p];
     int nc = 0;
-    material_compute_stress(s.mats[s.mat[p]], sig, de, rho, sv, out, &nc);
+    mc_return(s.mats[s.mat[p]], sig, de, rho, sv, out, &nc);  // a MohrCoulomb point
     s.rpass[p] = (uint8_t)(nc < 255 ? nc : 255);
 #pragma unroll
     for (int k = 0; k < SV_N; ++k) s.sv[(int64_t)k * np + p] = sv[k];

@@ -27,13 +27,14 @@
 #include "mpm_bulk.cuh"
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
+#include "mpm_return.cuh"
 #include "mpm_state.cuh"
 
 #ifndef MPM_MIXED_G2P_MIN_BLOCKS
 #define MPM_MIXED_G2P_MIN_BLOCKS 6  // 80 registers, no spills: 0.478 -> 0.374 ms (4M, 3D)
 #endif
 #ifndef MPM_MC_RETURN_MIN_BLOCKS
-#define MPM_MC_RETURN_MIN_BLOCKS 6  // 0.167 -> 0.155 ms at step 400 of the 4M column
+#define MPM_MC_RETURN_MIN_BLOCKS 4  // pass-loop return, 1M column at step 2000: 2 / 3 / 4 / 6 blocks -> FP64 0.362 / 0.320 / 0.323 / 0.403 ms, mixed 0.370 / 0.318 / 0.311 / 0.384 ms
 #endif
 #ifndef MPM_MIXED_P2G_TILE_MIN_BLOCKS
 #define MPM_MIXED_P2G_TILE_MIN_BLOCKS 5  // 48 registers, small spills: 0.32 -> 0.26 ms (4M, 3D)
@@ -49,6 +50,38 @@ __device__ __forceinline__ float pmf(const DevState& s, int f, int64_t p) {
 template <int DIM>
 __device__ __forceinline__ void set_pmf(const DevState& s, int f, int64_t p, float v) {
   s.pm[(int64_t)f * s.np + p] = v;
+}
+
+// The nodal velocity (and, with ACC, acceleration) of node n from its
+// nfv record (nfv_stride floats: 3D v0 v1 v2 a0 | a1 a2 - -, 2D v0 v1 a0 a1).
+template <int DIM, bool ACC>
+__device__ __forceinline__ void load_nfv(const float* nfv, int64_t n, float* v, float* a) {
+  const float4* q = reinterpret_cast<const float4*>(nfv + n * nfv_stride(DIM));
+  const float4 h0 = q[0];
+  v[0] = h0.x;
+  v[1] = h0.y;
+  if constexpr (DIM == 3) {
+    v[2] = h0.z;
+    if constexpr (ACC) {
+      const float4 h1 = q[1];
+      a[0] = h0.w;
+      a[1] = h1.x;
+      a[2] = h1.y;
+    }
+  } else if constexpr (ACC) {
+    a[0] = h0.z;
+    a[1] = h0.w;
+  }
+}
+template <int DIM>
+__device__ __forceinline__ void store_nfv(float* nfv, int64_t n, const float* v, const float* a) {
+  float4* q = reinterpret_cast<float4*>(nfv + n * nfv_stride(DIM));
+  if constexpr (DIM == 3) {
+    q[0] = make_float4(v[0], v[1], v[2], a[0]);
+    q[1] = make_float4(a[1], a[2], 0.f, 0.f);
+  } else {
+    q[0] = make_float4(v[0], v[1], a[0], a[1]);
+  }
 }
 
 // local coordinate in FP64, rounded to FP32 for the shape functions
@@ -292,7 +325,6 @@ template <int DIM, int MODE>
 __global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, double damping) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= s.nn) return;
-  const int64_t nn = s.nn;
   constexpr int NVAL = 1 + 3 * DIM;
   double sum[NVAL];
   constexpr int V0 = MODE == 2 ? 1 + DIM : 0;
@@ -303,10 +335,12 @@ __global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, d
   if constexpr (MODE == 2) {
     double mm[1];
     gather_node_mixed<DIM, 0, 1>(s, n, mm);
+    float vf[DIM], af[DIM];
+    load_nfv<DIM, true>(s.nfv, n, vf, af);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-      vel[d] = (double)s.nfv[(int64_t)d * nn + n];
-      acc[d] = (double)s.nfv[(int64_t)(DIM + d) * nn + n];
+      vel[d] = (double)vf[d];
+      acc[d] = (double)af[d];
     }
     node_accel_update_d<DIM>(s, mm[0], &sum[0], &sum[DIM], vel, acc, bci, dt, damping);
   } else {
@@ -324,11 +358,13 @@ __global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, d
     if constexpr (MODE == 1)
       node_accel_update_d<DIM>(s, m, &sum[1 + DIM], &sum[1 + 2 * DIM], vel, acc, bci, dt, damping);
   }
+  float vf[DIM], af[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    s.nfv[(int64_t)d * nn + n] = (float)vel[d];
-    s.nfv[(int64_t)(DIM + d) * nn + n] = (float)acc[d];
+    vf[d] = (float)vel[d];
+    af[d] = (float)acc[d];
   }
+  store_nfv<DIM>(s.nfv, n, vf, af);
 }
 
 // ------------------------------------------------------- stress and strain
@@ -399,7 +435,6 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, const Row
                                                     const int* nid, const float* D, float dt) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int NS = PF<DIM>::NS;
-  const int64_t nn = s.nn;
   const float* Dc = s.dndx_cf + (int64_t)c * NV * DIM;
   float Hi[DIM * DIM];
 #pragma unroll
@@ -409,8 +444,7 @@ __device__ __forceinline__ void stress_update_mixed(const DevState& s, const Row
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
     float vel[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) vel[d] = s.nfv[(int64_t)d * nn + nid[i]];
+    load_nfv<DIM, false>(s.nfv, nid[i], vel, nullptr);
 #pragma unroll
     for (int a = 0; a < DIM; ++a)
 #pragma unroll
@@ -566,7 +600,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   if (p >= s.np) return;
   const int c = s.cell[p];
   if (c < 0) return;
-  const int64_t np = s.np, nn = s.nn;
+  const int64_t np = s.np;
   double x[DIM];
   load_x<DIM>(s, p, x);
   float xi[DIM], N[NV], Xr[NV * DIM];
@@ -579,11 +613,13 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.f;
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
+    float vn[DIM], an[DIM];
+    load_nfv<DIM, FLIP>(s.nfv, nid[i], vn, an);
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * s.nfv[(int64_t)d * nn + nid[i]];
+    for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * vn[d];
     if constexpr (FLIP) {
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * s.nfv[(int64_t)(DIM + d) * nn + nid[i]];
+      for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * an[d];
     }
   }
   const float dtf = (float)dt;
@@ -668,7 +704,7 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   int16_t* spvc = reinterpret_cast<int16_t*>(smat + T);
   const int t = threadIdx.x;
   const int64_t p0 = (int64_t)blockIdx.x * T;
-  const int64_t np = s.np, nn = s.nn;
+  const int64_t np = s.np;
   if (t == 0) {
     timed_out = 0;
     bulk::mbar_init(&bar[0], 1);
@@ -711,11 +747,13 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
     for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.f;
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
+      float vn[DIM], an[DIM];
+      load_nfv<DIM, FLIP>(s.nfv, nid[i], vn, an);
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * s.nfv[(int64_t)d * nn + nid[i]];
+      for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * vn[d];
       if constexpr (FLIP) {
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * s.nfv[(int64_t)(DIM + d) * nn + nid[i]];
+        for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * an[d];
       }
     }
     const float dtf = (float)dt;
@@ -811,9 +849,9 @@ void prefer_shared_memory() {
 
 // The MohrCoulomb updates deferred by stress_update_mixed, one thread per
 // listed particle (the light entries, then the heavy ones): the full FP64
-// update (mohr_coulomb.tcc:348-513) from the FP32 stress and state before the
-// step's update, rounded back to FP32; the number of corrections is kept for
-// the next step's grouping.
+// update (mohr_coulomb.tcc:348-513, as mc_return's passes) from the FP32
+// stress and state before the step's update, rounded back to FP32; the number
+// of corrections is kept for the next step's grouping.
 template <int DIM>
 __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return_mixed(DevState s) {
   const unsigned nl = *s.nplastic, n = nl + *s.nplastic_heavy;
@@ -841,7 +879,7 @@ __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return_mix
     for (int k = 0; k < SVF_N; ++k) svd[k] = (double)svf[k];
     svd[SV_PD] = r.pd();
     int nc = 0;
-    mc_compute_stress<double, double>(s.mats[mi], sd, ded, (double)rho, svd, svd[SV_PD], od, &nc);
+    mc_return<double>(s.mats[mi], sd, ded, (double)rho, svd, od, &nc);
     s.rpass[p] = (uint8_t)(nc < 255 ? nc : 255);
 #pragma unroll
     for (int k = 0; k < 6; ++k) out[k] = (float)od[k];

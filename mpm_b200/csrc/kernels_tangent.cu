@@ -19,6 +19,7 @@
 #include "mpm_device.cuh"
 #include "mpm_dual.cuh"
 #include "mpm_kernels.h"
+#include "mpm_return.cuh"
 #include "mpm_state.cuh"
 
 #ifndef MPM_TANGENT_G2P_MIN_BLOCKS
@@ -617,7 +618,8 @@ __global__ void __launch_bounds__(128, MPM_TANGENT_RETURN_MIN_BLOCKS) k_mc_retur
 #pragma unroll
     for (int k = 0; k < SV_N; ++k) sv[k] = ld(s.sv, s.svt, (int64_t)k * np + p);
     const MatD& mp = static_cast<const MatD*>(s.mats_t)[s.mat[p]];
-    mc_compute_stress<D, D>(mp, sig, de, rho, sv, sv[SV_PD], out);
+    int nc = 0;
+    mc_return<D>(mp, sig, de, rho, sv, out, &nc);
 #pragma unroll
     for (int k = 0; k < SV_N; ++k) st(s.sv, const_cast<double* const*>(s.svt), (int64_t)k * np + p, sv[k]);
 #pragma unroll

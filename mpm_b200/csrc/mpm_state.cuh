@@ -59,6 +59,11 @@ struct NF {
                        VEL = 1 + 3 * DIM, ACC = 1 + 4 * DIM, NNF = 1 + 5 * DIM;
 };
 
+// Mixed-precision nodal velocity and acceleration: one record per node of
+// nfv_stride floats, 16-byte aligned, so that a particle kernel gathers a node
+// with one (2D: v0 v1 a0 a1) or two (3D: v0 v1 v2 a0 | a1 a2 - -) 16-byte loads.
+constexpr int nfv_stride(int dim) { return dim == 3 ? 8 : 4; }
+
 // particle velocity constraint record: mask bit d => v[d] = value[d]
 struct ParticleVC {
   uint32_t mask;
@@ -148,7 +153,7 @@ struct DevState {
   // mixed precision (null on the FP64 path)
   float* pm = nullptr;            // [PM::NF][np]
   float* svf = nullptr;           // [SVF_N][np]
-  float* nfv = nullptr;           // [2 DIM][nn] nodal velocity, acceleration
+  float* nfv = nullptr;           // [nn][nfv_stride(DIM)] nodal velocity, acceleration
   float* partials_f = nullptr;    // [ncells][NV][1 + 3 DIM]
   float* dndx_cf = nullptr;       // [ncells][NV][DIM]
   const MaterialT<float>* mats_f = nullptr;
