@@ -2486,8 +2486,15 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
     params[k] = TangentParam{it->second, kinds[k]};
   }
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
-  h->tape.reset(new AdjointTape());
+  // a tape of an earlier record keeps its buffers: a calibration loop records
+  // and reverses the same run shape again and again
+  if (!h->tape) h->tape.reset(new AdjointTape());
   AdjointTape& t = *h->tape;
+  t.recorded = false;
+  const size_t held = t.ck_pf.n * 8 + t.ck_sv.n * 8 + t.ck_cell.n * 4 + t.seg_pf.n * 8 +
+                      t.seg_sv.n * 8 + t.seg_cell.n * 4 + t.fin_pf.n * 8 + t.fin_sv.n * 8 +
+                      t.fin_cell.n * 4 + (t.adj.n + t.deps.n + t.dsbar.n + t.coef.n + t.theta.n +
+                                          t.apart.n + t.nbar.n) * 8;
   t.nsteps = nsteps;
   t.nparams = nparams;
   t.np = h->np;
@@ -2506,6 +2513,7 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
   };
   size_t free_b = 0, total_b = 0;
   ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+  free_b += held;  // the tape's own buffers count as available
   if (checkpoint_every == 0) {
     // every step's start state kept when half the free memory holds them (the
     // reverse sweep then recomputes nothing), else checkpoints sqrt(nsteps)
@@ -2525,22 +2533,22 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
                                       " segment states); " + std::to_string(free_b >> 20) +
                                       " MiB are free: raise checkpoint_every towards sqrt(nsteps)");
   }
-  t.ck_pf.alloc(t.pf_n * nck);
-  t.ck_sv.alloc(t.sv_n * nck);
-  t.ck_cell.alloc(t.cell_n * nck);
-  t.seg_pf.alloc(t.pf_n * nseg);
-  t.seg_sv.alloc(t.sv_n * nseg);
-  t.seg_cell.alloc(t.cell_n * nseg);
-  t.fin_pf.alloc(t.pf_n);
-  t.fin_sv.alloc(t.sv_n);
-  t.fin_cell.alloc(t.cell_n);
-  t.adj.alloc((size_t)(2 * dim + ns + 1) * np);
-  t.deps.alloc((size_t)6 * np);
-  t.dsbar.alloc((size_t)ns * np);
-  t.coef.alloc((size_t)(3 * dim + 6) * np);
-  t.theta.alloc((size_t)MAX_TANGENTS * np);
-  t.apart.alloc((size_t)h->ncells * h->nv * 2 * dim);
-  t.nbar.alloc((size_t)(1 + 3 * dim) * h->nnodes);
+  t.ck_pf.resize(t.pf_n * nck);
+  t.ck_sv.resize(t.sv_n * nck);
+  t.ck_cell.resize(t.cell_n * nck);
+  t.seg_pf.resize(t.pf_n * nseg);
+  t.seg_sv.resize(t.sv_n * nseg);
+  t.seg_cell.resize(t.cell_n * nseg);
+  t.fin_pf.resize(t.pf_n);
+  t.fin_sv.resize(t.sv_n);
+  t.fin_cell.resize(t.cell_n);
+  t.adj.resize((size_t)(2 * dim + ns + 1) * np);
+  t.deps.resize((size_t)6 * np);
+  t.dsbar.resize((size_t)ns * np);
+  t.coef.resize((size_t)(3 * dim + 6) * np);
+  t.theta.resize((size_t)MAX_TANGENTS * np);
+  t.apart.resize((size_t)h->ncells * h->nv * 2 * dim);
+  t.nbar.resize((size_t)(1 + 3 * dim) * h->nnodes);
   // Dual materials: zero derivatives (the return map's Jacobian) and the
   // parameters' derivatives, with the initial state's parameter derivatives
   {
