@@ -2,12 +2,15 @@
 // that mirrors the reference's MPMBase initialisation, device buffers and the
 // step loop.
 #include <cuda_runtime.h>
+#include <sched.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
 #include <type_traits>
 #include <exception>
 #include <map>
@@ -80,30 +83,114 @@ struct HostBC {
   double angles[3] = {0, 0, 0};
 };
 
+// Host worker threads kept for the life of the process, for the per-particle
+// conversions between the caller's rows and the device layout and the staged
+// copies through pinned memory: a parallel_for wakes them instead of starting
+// threads (the staged copies call it once per 64 MiB chunk).  One job runs at a
+// time; a call made while a job runs (another handle's thread, or a nested
+// call from a worker) runs on its own thread.
+class HostPool {
+ public:
+  static HostPool& get() {
+    static HostPool pool;
+    return pool;
+  }
+  int64_t threads() const { return (int64_t)workers_.size() + 1; }
+  // false when the pool is busy: the caller runs the job itself
+  template <class Job>
+  bool run(int64_t ntasks, Job& job) {
+    std::unique_lock<std::mutex> busy(busy_, std::try_to_lock);
+    if (!busy.owns_lock() || in_worker()) return false;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      task_ = [&job](int64_t t) { job(t); };
+      ntasks_ = ntasks;
+      next_ = 1;  // task 0 runs on the calling thread
+      done_ = 0;
+      ++gen_;
+    }
+    cv_.notify_all();
+    job(0);
+    finish_one();
+    std::unique_lock<std::mutex> g(mu_);
+    all_done_.wait(g, [&] { return done_ == ntasks_; });
+    task_ = nullptr;
+    return true;
+  }
+
+ private:
+  HostPool() {
+    int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+    cpu_set_t set;  // the CPUs this process may run on, when fewer
+    if (sched_getaffinity(0, sizeof(set), &set) == 0) hw = std::min<int64_t>(hw, CPU_COUNT(&set));
+    hw = std::max<int64_t>(1, hw);
+    for (int64_t w = 1; w < hw; ++w) workers_.emplace_back([this] { loop(); });
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : workers_) t.join();
+  }
+  static bool& in_worker() {
+    static thread_local bool w = false;
+    return w;
+  }
+  void finish_one() {
+    std::lock_guard<std::mutex> g(mu_);
+    if (++done_ == ntasks_) all_done_.notify_all();
+  }
+  void loop() {
+    in_worker() = true;
+    uint64_t seen = 0;
+    std::unique_lock<std::mutex> g(mu_);
+    for (;;) {
+      cv_.wait(g, [&] { return stop_ || (gen_ != seen && next_ < ntasks_); });
+      if (stop_) return;
+      while (next_ < ntasks_) {
+        const int64_t t = next_++;
+        auto task = task_;
+        g.unlock();
+        task(t);
+        g.lock();
+        if (++done_ == ntasks_) all_done_.notify_all();
+      }
+      seen = gen_;
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex busy_, mu_;
+  std::condition_variable cv_, all_done_;
+  std::function<void(int64_t)> task_;
+  int64_t ntasks_ = 0, next_ = 0, done_ = 0;
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+};
+
 // f(a, b) over [0, n) split across the host's threads (at least 32768 items a
-// thread); the first exception a worker throws is rethrown here.  For the
-// per-particle conversions between the caller's rows and the device layout.
+// thread); the first exception a worker throws is rethrown here.
 template <class F>
 void parallel_for(int64_t n, F f) {
-  const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
-  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(hw, n / 32768));
+  HostPool& pool = HostPool::get();
+  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(pool.threads(), n / 32768));
   if (nt == 1) {
     f((int64_t)0, n);
     return;
   }
-  std::vector<std::thread> pool;
   std::exception_ptr err;
   std::mutex mu;
-  for (int64_t w = 0; w < nt; ++w)
-    pool.emplace_back([&, w]() {
-      try {
-        f(n * w / nt, n * (w + 1) / nt);
-      } catch (...) {
-        std::lock_guard<std::mutex> g(mu);
-        if (!err) err = std::current_exception();
-      }
-    });
-  for (auto& t : pool) t.join();
+  auto job = [&](int64_t w) {
+    try {
+      f(n * w / nt, n * (w + 1) / nt);
+    } catch (...) {
+      std::lock_guard<std::mutex> g(mu);
+      if (!err) err = std::current_exception();
+    }
+  };
+  if (!pool.run(nt, job))
+    for (int64_t w = 0; w < nt; ++w) job(w);
   if (err) std::rethrow_exception(err);
 }
 
