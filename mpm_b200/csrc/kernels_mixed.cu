@@ -592,9 +592,13 @@ __global__ void __launch_bounds__(128) k_stress_mixed(DevState s, float dt) {
 }
 
 // --------------------------------------------------------------------- G2P
-template <int DIM, bool STRESS, bool FLIP, bool BOX>
+// MUSL (mpm_scheme_musl.tcc:20-35): the kinematics without committing the
+// positions -- the updated ones go to xnext (k_commit_locate_mixed commits them
+// after the second mapping and the stress update), no locate here.
+template <int DIM, bool STRESS, bool FLIP, bool BOX, bool MUSL = false>
 __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
     k_g2p_mixed(DevState s, double dt, float beta) {
+  static_assert(!(MUSL && STRESS), "MUSL updates the stress after its second mapping");
   constexpr int NV = Elem<DIM>::NV;
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= s.np) return;
@@ -640,7 +644,10 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   for (int d = 0; d < DIM; ++d) {
     const double dx = (double)nvel[d] * dt;  // FP64 position / displacement update
     xn[d] = x[d] + dx;
-    s.pf[(int64_t)(PDX<DIM>::X + d) * np + p] = xn[d];
+    if constexpr (MUSL)
+      s.xnext[(int64_t)d * np + p] = xn[d];
+    else
+      s.pf[(int64_t)(PDX<DIM>::X + d) * np + p] = xn[d];
     s.pf[(int64_t)(PDX<DIM>::U + d) * np + p] += dx;
   }
   const int pv = s.pvc[p];
@@ -652,6 +659,7 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   }
 #pragma unroll
   for (int d = 0; d < DIM; ++d) set_pmf<DIM>(s, PM<DIM>::V + d, p, v[d]);
+  if constexpr (MUSL) return;
   if constexpr (STRESS) {
     float D[NV * DIM];
     dn_dx_all_f<DIM, BOX>(s, c, xi, Xr, D);
@@ -660,6 +668,35 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   bool finite = true;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) finite = finite && isfinite(xn[d]);
+  if (!finite) {
+    raise_err(s, ERR_NONFINITE);
+    s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+    return;
+  }
+  const int nc = locate_near<DIM>(s, xn, c);
+  if (nc >= 0) {
+    if (nc != c) s.cell[p] = nc;
+  } else {
+    s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+  }
+}
+
+// MUSL end of step: the new positions (FP64) replace the old, then locate
+template <int DIM>
+__global__ void __launch_bounds__(128) k_commit_locate_mixed(DevState s) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.np) return;
+  const int c = s.cell[p];
+  if (c < 0) return;
+  const int64_t np = s.np;
+  double xn[DIM];
+  bool finite = true;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    xn[d] = s.xnext[(int64_t)d * np + p];
+    s.pf[(int64_t)(PDX<DIM>::X + d) * np + p] = xn[d];
+    finite = finite && isfinite(xn[d]);
+  }
   if (!finite) {
     raise_err(s, ERR_NONFINITE);
     s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
@@ -929,7 +966,35 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
   pr.begin(K_SORT, st, SORT_KERNELS);
   counting_sort(s, st);
   pr.end(K_SORT, st);
-  if (a.scheme == 1) {  // USL
+  if (a.scheme == 2) {  // MUSL (mpm_scheme_musl.tcc:20-35)
+    pr.begin(K_P2G, st);
+    p2g(std::integral_constant<int, 2>{});
+    pr.end(K_P2G, st);
+    pr.begin(K_NODES_VEL, st);
+    k_nodes_mixed<DIM, 1><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
+    pr.end(K_NODES_VEL, st);
+    pr.begin(K_G2P, st);
+    if (a.flip)
+      k_g2p_mixed<DIM, false, true, BOX, true><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
+    else
+      k_g2p_mixed<DIM, false, false, BOX, true><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
+    pr.end(K_G2P, st);
+    // mass and momentum again with the updated velocities, nodal velocity,
+    // then the stress update at the step's positions
+    pr.begin(K_P2G_FORCES, st);
+    p2g(std::integral_constant<int, 0>{});
+    pr.end(K_P2G_FORCES, st);
+    pr.begin(K_NODES_ACC, st);
+    k_nodes_mixed<DIM, 0><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
+    pr.end(K_NODES_ACC, st);
+    pr.begin(K_STRESS, st);
+    k_stress_mixed<DIM, BOX><<<pb, 128, 0, st>>>(s, (float)a.dt);
+    pr.end(K_STRESS, st);
+    mc_returns();
+    pr.begin(K_LOCATE, st);
+    k_commit_locate_mixed<DIM><<<pb, 128, 0, st>>>(s);
+    pr.end(K_LOCATE, st);
+  } else if (a.scheme == 1) {  // USL
     pr.begin(K_P2G, st);
     p2g(std::integral_constant<int, 2>{});
     pr.end(K_P2G, st);

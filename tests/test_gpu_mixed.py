@@ -47,7 +47,7 @@ def test_linear_elastic_2d_within_1e5_of_fp64():
     assert all(v <= 1e-5 for v in errs.values()), errs
 
 
-@pytest.mark.parametrize("scheme", ["usf", "usl"])
+@pytest.mark.parametrize("scheme", ["usf", "usl", "musl"])
 def test_mohr_coulomb_3d_short_horizon_within_1e5(scheme):
     prob = P.column_3d(shape=(20, 10, 10), block=(10, 10, 10), scheme=scheme)
     m, f = _run(prob, 50, "mixed"), _run(prob, 50, "fp64")
@@ -136,3 +136,13 @@ def test_footing_on_slope_mixed():
     errs = _errors(m, f)
     assert all(v <= 3e-4 for v in errs.values()), errs
     assert errs["u"] <= 1e-5 and errs["v"] <= 5e-5, errs
+
+
+def test_musl_2d_linear_elastic_within_1e5_of_fp64():
+    """MUSL (mpm_scheme_musl.tcc:20-35) in mixed precision: the 2D LinearElastic
+    column over 1,000 steps, every field within 1e-5 of the FP64 MUSL run."""
+    prob = P.column_2d(scheme="musl")
+    m, f = _run(prob, 1000, "mixed"), _run(prob, 1000, "fp64")
+    assert np.array_equal(m["cell"], f["cell"])
+    errs = _errors(m, f)
+    assert all(v <= 1e-5 for v in errs.values()), errs
