@@ -64,8 +64,8 @@ enum { MPM_PRECISION_FP64 = 0, MPM_PRECISION_MIXED = 1 };
 /* Analysis settings (mpm_base.tcc:3-207; mpm_explicit.tcc:8-13, 145-153). */
 typedef struct {
   int32_t dim;              /* 2 (quad4 / ED2Q4) or 3 (hex8 / ED3H8) */
-  int32_t scheme;           /* MPM_SCHEME_USF / MPM_SCHEME_USL / MPM_SCHEME_MUSL (FP64;
-                               mpm_scheme_musl.tcc:20-35) */
+  int32_t scheme;           /* MPM_SCHEME_USF / MPM_SCHEME_USL / MPM_SCHEME_MUSL (FP64 and
+                               mixed; mpm_scheme_musl.tcc:20-35) */
   int32_t velocity_update;  /* MPM_VELOCITY_FLIP / PIC (particle.tcc:1018-1067), or the
                                affine ASFLIP / APIC and Taylor TPIC updates, which carry a
                                mapping matrix per particle (particle.tcc:630-721,
@@ -315,8 +315,9 @@ int mpm_gpu_read_sensitivities(mpm_gpu_t h, int32_t field, double* out);
  * device (0: every step when half the free device memory holds them -- the
  * reverse sweep then recomputes no step -- else ceil(sqrt(nsteps)) apart;
  * ceil(nsteps / checkpoint_every) checkpoints plus checkpoint_every
- * states of one segment: about 340 B per particle each in 3D; MPM_ERR_ALLOC
- * with the size when that does not fit).  mpm_gpu_adjoint_reverse then takes
+ * states of one segment, each holding the fields the reverse sweep reads --
+ * x, v, stress, volume, density, mass, MohrCoulomb state, cell: about 200 B
+ * per particle in 3D; MPM_ERR_ALLOC with the size when that does not fit).  mpm_gpu_adjoint_reverse then takes
  * dL/dx and dL/dv at the end (n*3 rows; either may be NULL for zero), recomputes
  * each segment from its checkpoint and sweeps back through it, and writes
  * dL/dparameter (nparams) and, when not NULL, dL/dx0, dL/dv0 (n*3) and

@@ -287,6 +287,14 @@ struct AdjointTape {
   int64_t nsteps = 0, every = 0, step0 = 0, np = 0;
   int nparams = 0;
   size_t pf_n = 0, sv_n = 0, cell_n = 0;  // elements of one stored state
+  // Checkpoints and segment states keep only the particle rows the recompute
+  // and the reverse kernels read -- x, v, stress, volume, density, mass --
+  // not u, strain and F, which no later position, velocity or stress depends
+  // on; the run's end state is kept whole.  Row ranges [first, last) of the
+  // FP64 particle buffer, in units of npad.
+  int nranges = 0;
+  int range[3][2] = {};
+  size_t pfc_n = 0;  // elements of one compact particle state
   DevBuf<double> ck_pf, ck_sv, seg_pf, seg_sv, fin_pf, fin_sv;
   DevBuf<int32_t> ck_cell, seg_cell, fin_cell;
   DevBuf<double> adj, deps, dsbar, coef, theta, apart, nbar, sv_seed;
@@ -1280,8 +1288,6 @@ int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out) {
   if (cfg->dim != 2 && cfg->dim != 3) return MPM_ERR_INVALID;
   if (cfg->scheme != MPM_SCHEME_USF && cfg->scheme != MPM_SCHEME_USL &&
       cfg->scheme != MPM_SCHEME_MUSL)
-    return MPM_ERR_UNSUPPORTED;
-  if (cfg->scheme == MPM_SCHEME_MUSL && cfg->precision != MPM_PRECISION_FP64)
     return MPM_ERR_UNSUPPORTED;
   if (cfg->velocity_update < MPM_VELOCITY_FLIP || cfg->velocity_update > MPM_VELOCITY_APIC)
     return MPM_ERR_UNSUPPORTED;
@@ -2526,16 +2532,36 @@ void set_gravity(mpm_gpu_t h, StepArgs& a, int64_t step) {
   for (int d = 0; d < 3; ++d) a.g[d] = d < h->dim ? gm * h->cfg.gravity[d] : 0.;
 }
 
-void copy_state(mpm_gpu_t h, const AdjointTape& t, double* pf, double* sv, int32_t* cell, bool save) {
+// Save the solver's particle state to (pf, sv, cell) or restore it from there:
+// the whole FP64 particle buffer (full), or the compact rows of t.range one
+// after another.
+void copy_state(mpm_gpu_t h, const AdjointTape& t, double* pf, double* sv, int32_t* cell, bool save,
+                bool full = false) {
   auto cp = [&](void* dst, const void* src, size_t bytes) {
     if (bytes) ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream), "D2D");
   };
+  if (full) {
+    if (save)
+      cp(pf, h->d_pf.p, t.pf_n * sizeof(double));
+    else
+      cp(h->d_pf.p, pf, t.pf_n * sizeof(double));
+  } else {
+    const size_t np = (size_t)h->npad;
+    size_t at = 0;
+    for (int r = 0; r < t.nranges; ++r) {
+      const size_t n = (size_t)(t.range[r][1] - t.range[r][0]) * np;
+      double* dev = h->d_pf.p + (size_t)t.range[r][0] * np;
+      if (save)
+        cp(pf + at, dev, n * sizeof(double));
+      else
+        cp(dev, pf + at, n * sizeof(double));
+      at += n;
+    }
+  }
   if (save) {
-    cp(pf, h->d_pf.p, t.pf_n * sizeof(double));
     cp(sv, h->d_sv.p, t.sv_n * sizeof(double));
     cp(cell, h->d_cell.p, t.cell_n * sizeof(int32_t));
   } else {
-    cp(h->d_pf.p, pf, t.pf_n * sizeof(double));
     cp(h->d_sv.p, sv, t.sv_n * sizeof(double));
     cp(h->d_cell.p, cell, t.cell_n * sizeof(int32_t));
   }
@@ -2586,17 +2612,35 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
   t.nparams = nparams;
   t.np = h->np;
   t.pf_n = h->d_pf.n;
+  {
+    const bool d3 = h->dim == 3;
+    const int X = d3 ? PF<3>::X : PF<2>::X, V = d3 ? PF<3>::V : PF<2>::V,
+              S = d3 ? PF<3>::S : PF<2>::S, NS = d3 ? PF<3>::NS : PF<2>::NS,
+              VOL = d3 ? PF<3>::VOL : PF<2>::VOL, MASS = d3 ? PF<3>::MASS : PF<2>::MASS;
+    static_assert(PF<3>::V + 3 == PF<3>::S && PF<2>::V + 2 == PF<2>::S, "v then stress");
+    static_assert(PF<3>::VOL + 1 == PF<3>::RHO && PF<3>::RHO + 1 == PF<3>::MASS, "V, rho, m");
+    static_assert(PF<2>::VOL + 1 == PF<2>::RHO && PF<2>::RHO + 1 == PF<2>::MASS, "V, rho, m");
+    const int rg[3][2] = {{X, X + h->dim}, {V, S + NS}, {VOL, MASS + 1}};
+    t.nranges = 3;
+    t.pfc_n = 0;
+    for (int r = 0; r < 3; ++r) {
+      t.range[r][0] = rg[r][0];
+      t.range[r][1] = rg[r][1];
+      t.pfc_n += (size_t)(rg[r][1] - rg[r][0]) * (size_t)h->npad;
+    }
+  }
   t.sv_n = h->d_sv.n;
   t.cell_n = h->d_cell.n;
   const int dim = h->dim;
   const int64_t np = h->npad;
   const int ns = dim == 2 ? PF<2>::NS : PF<3>::NS;
-  const size_t state_bytes = t.pf_n * 8 + t.sv_n * 8 + t.cell_n * 4;
+  const size_t state_bytes = t.pfc_n * 8 + t.sv_n * 8 + t.cell_n * 4;  // a compact state
   const size_t work_bytes = (size_t)np * 8 * ((2 * dim + ns + 1) + 6 + ns + (3 * dim + 6) + MAX_TANGENTS) +
                             (size_t)h->ncells * h->nv * 2 * dim * 8 + (size_t)h->nnodes * (1 + 3 * dim) * 8;
+  const size_t end_bytes = t.pf_n * 8 + t.sv_n * 8 + t.cell_n * 4;  // the whole end state
   auto need_for = [&](int64_t every) {
     const int64_t nck = (nsteps + every - 1) / every;
-    return state_bytes * (size_t)(nck + std::min(every, nsteps) + 1) + work_bytes;
+    return state_bytes * (size_t)(nck + std::min(every, nsteps)) + end_bytes + work_bytes;
   };
   size_t free_b = 0, total_b = 0;
   ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
@@ -2620,10 +2664,10 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
                                       " segment states); " + std::to_string(free_b >> 20) +
                                       " MiB are free: raise checkpoint_every towards sqrt(nsteps)");
   }
-  t.ck_pf.resize(t.pf_n * nck);
+  t.ck_pf.resize(t.pfc_n * nck);
   t.ck_sv.resize(t.sv_n * nck);
   t.ck_cell.resize(t.cell_n * nck);
-  t.seg_pf.resize(t.pf_n * nseg);
+  t.seg_pf.resize(t.pfc_n * nseg);
   t.seg_sv.resize(t.sv_n * nseg);
   t.seg_cell.resize(t.cell_n * nseg);
   t.fin_pf.resize(t.pf_n);
@@ -2665,7 +2709,7 @@ int mpm_gpu_adjoint_record(mpm_gpu_t h, int64_t nsteps, int64_t checkpoint_every
   t.step0 = h->step;
   for (int64_t s0 = 0; s0 < nsteps; s0 += checkpoint_every) {
     const int64_t k = s0 / checkpoint_every;
-    copy_state(h, t, t.ck_pf.p + t.pf_n * k, t.ck_sv.p + t.sv_n * k, t.ck_cell.p + t.cell_n * k, true);
+    copy_state(h, t, t.ck_pf.p + t.pfc_n * k, t.ck_sv.p + t.sv_n * k, t.ck_cell.p + t.cell_n * k, true);
     const int rc = run_steps(h, std::min(checkpoint_every, nsteps - s0), nullptr);
     if (rc != MPM_OK) {
       h->tape.reset();
@@ -2692,7 +2736,7 @@ int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_d
   const int64_t np = h->npad, n = h->np;
   const int ns = dim == 2 ? PF<2>::NS : PF<3>::NS;
   const int AX = 0, AV = dim, AS = 2 * dim, AVOL = 2 * dim + ns, AN = 2 * dim + ns + 1;
-  copy_state(h, t, t.fin_pf.p, t.fin_sv.p, t.fin_cell.p, true);
+  copy_state(h, t, t.fin_pf.p, t.fin_sv.p, t.fin_cell.p, true, true);
   {  // terminal cotangents, rows -> the device layout
     std::vector<double> a((size_t)AN * np, 0.0);
     for (int64_t p = 0; p < n; ++p)
@@ -2722,11 +2766,11 @@ int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_d
   const int64_t nck = (t.nsteps + t.every - 1) / t.every;
   for (int64_t seg = nck - 1; seg >= 0; --seg) {
     const int64_t s0 = seg * t.every, s1 = std::min(s0 + t.every, t.nsteps);
-    copy_state(h, t, t.ck_pf.p + t.pf_n * seg, t.ck_sv.p + t.sv_n * seg, t.ck_cell.p + t.cell_n * seg,
+    copy_state(h, t, t.ck_pf.p + t.pfc_n * seg, t.ck_sv.p + t.sv_n * seg, t.ck_cell.p + t.cell_n * seg,
                false);
     for (int64_t k = s0; k < s1 - 1; ++k) {  // the segment's step-start states
       const int64_t j = k - s0;
-      copy_state(h, t, t.seg_pf.p + t.pf_n * j, t.seg_sv.p + t.sv_n * j, t.seg_cell.p + t.cell_n * j, true);
+      copy_state(h, t, t.seg_pf.p + t.pfc_n * j, t.seg_sv.p + t.sv_n * j, t.seg_cell.p + t.cell_n * j, true);
       set_gravity(h, a, t.step0 + k);
       launch_step_fp64(dim, h->ds, a, h->stream, h->prof);
     }
@@ -2734,7 +2778,7 @@ int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_d
     for (int64_t k = s1 - 1; k >= s0; --k) {
       const int64_t j = k - s0;
       if (k < s1 - 1)
-        copy_state(h, t, t.seg_pf.p + t.pf_n * j, t.seg_sv.p + t.sv_n * j, t.seg_cell.p + t.cell_n * j,
+        copy_state(h, t, t.seg_pf.p + t.pfc_n * j, t.seg_sv.p + t.sv_n * j, t.seg_cell.p + t.cell_n * j,
                    false);
       set_gravity(h, a, t.step0 + k);
       h->prof.begin(K_ADJ_RECOMPUTE, h->stream, SORT_KERNELS + 2);
@@ -2750,7 +2794,7 @@ int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_d
   unsigned words[2] = {0, 0};
   ck(cudaMemcpyAsync(words, h->d_words.p, sizeof(words), cudaMemcpyDeviceToHost, h->stream), "D2H");
   // back to the recorded run's end state
-  copy_state(h, t, t.fin_pf.p, t.fin_sv.p, t.fin_cell.p, false);
+  copy_state(h, t, t.fin_pf.p, t.fin_sv.p, t.fin_cell.p, false, true);
   ck(cudaStreamSynchronize(h->stream), "adjoint");
   h->prof.collect();
   if (words[1] & ERR_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite state in the recomputed run");
