@@ -540,10 +540,13 @@ def run_launch_list():
     """One launch of every kernel of the product inside a profiler window
     (cudaProfilerStart/Stop), for a launch list with per-kernel DRAM bytes:
     a mixed and an FP64 step of the 1M-particle column (eager launches), the
-    host-row/device-layout conversions both ways, the PODParticle records, and
-    one recorded and reversed step of the calibration column."""
+    host-row/device-layout conversions both ways, the PODParticle records, a
+    slab step's halo pack / unpack and layer count, one step of the
+    calibration column carrying derivatives, one recorded and reversed step of
+    it, and the batch constitutive update of 262,144 MohrCoulomb points."""
     import torch
     from mpm_b200 import problems as P
+    from mpm_b200.solver import material_stress_batch
     col = P.column_3d(block=(50, 50, 50))
     m = P.build_solver(col, precision="mixed")
     m.step(5)
@@ -553,8 +556,17 @@ def run_launch_list():
     f.set_profiling(True)
     cal = P.build_solver(P.config_d(), precision="fp64")
     cal.step(3)
+    tan = P.build_solver(P.config_d(), precision="fp64")
+    tan.step(3)
+    tan.set_sensitivities([(0, "youngs_modulus"), (0, "friction")])
     st = m.read()
     n = cal.nparticles
+    halo = torch.empty(f.halo_bytes(), dtype=torch.uint8, device="cuda")
+    props = P.mohr_coulomb(1e7, 0.3, 1800., 30., 1000., 0.)
+    rng = np.random.default_rng(7)
+    npts = 1 << 18
+    sig = np.tile(np.array([-2e4, -2e4, -4e4, 0., 0., 0.]), (npts, 1)) * rng.uniform(0.5, 1.5, (npts, 1))
+    deps = rng.normal(0.0, 2e-4, (npts, 6))
     torch.cuda.synchronize()
     torch.cuda.profiler.start()
     m.step(1)
@@ -562,8 +574,15 @@ def run_launch_list():
     m.load(st)
     m.read()
     f.write_pod()
+    f.step_begin()
+    f.halo_pack(10, halo.data_ptr())
+    f.halo_unpack(10, halo.data_ptr())
+    f.step_end()
+    f.layer_count(10, 190)
+    tan.step(1)
     cal.adjoint_record(1, [(0, "youngs_modulus"), (0, "friction")], checkpoint_every=1)
     cal.adjoint_reverse(dL_dx=np.ones((n, 3)))
+    material_stress_batch(3, "MohrCoulomb3D", props, sig, deps, 1800.)
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
     print(json.dumps({"workload": "launch-list", "particles": [m.nparticles, n]}))
