@@ -420,15 +420,24 @@ def run_calibration(args, rank, world):
         s.close()
         return x
 
+    def kernels(s):  # per-kernel ms per step over a 20-step eager window
+        s.set_profiling(True)
+        s.step_timed(20)
+        prof = {k: round(v[0] / 20, 4) for k, v in s.kernel_profile().items() if v[1]}
+        s.set_profiling(False)
+        return prof
+
     f = build(theta)
     f.step(args.warmup)
     ms_f = max_over_ranks(f.step_timed(args.steps), world)
     n = f.nparticles
+    fwd_kernels = kernels(f)
     f.close()
     t = build(theta)
     t.set_sensitivities(params)
     t.step(args.warmup)
     ms_t = max_over_ranks(t.step_timed(args.steps), world)
+    tan_kernels = kernels(t)
     t.close()
     # the reverse sweep: record + reverse, on the host clock (both calls return
     # after their device work has finished); every step's start state kept
@@ -490,6 +499,7 @@ def run_calibration(args, rank, world):
             "forward": {"value": world * n * args.steps / (ms_f / 1e3),
                         "ms_per_step": ms_f / args.steps},
             "tangent_over_forward": ms_t / ms_f,
+            "kernels_ms_per_step": {"forward": fwd_kernels, "tangent": tan_kernels},
             "adjoint": {"seconds": adj_s, "checkpoint_every": 1,
                         "over_forward": adj_s / (ms_f / 1e3), "kernels": adj_kernels,
                         "first_call_seconds": adj_first[1],

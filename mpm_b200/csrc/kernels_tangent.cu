@@ -260,12 +260,20 @@ __device__ __forceinline__ bool gather_node_tangent(const DevState& s, int64_t n
   bool active = false;
   auto add = [&](int c, int slot) {
     const int64_t o = ((int64_t)c * NV + slot) * NVAL;
-    if (!active) {
-      for (int v = 0; v < NVAL; ++v) sum[v] = ld(s.partials, s.partt, o + v);
-      active = true;
-    } else {
-      for (int v = 0; v < NVAL; ++v) sum[v] = sum[v] + ld(s.partials, s.partt, o + v);
+    // the row of values and of each derivative, loaded in pairs where aligned
+    double val[NVAL], der[NT][NVAL];
+    load_partial_row<double, NVAL, 0, NVAL>(s.partials + o, val);
+#pragma unroll
+    for (int k = 0; k < NT; ++k) load_partial_row<double, NVAL, 0, NVAL>(s.partt[k] + o, der[k]);
+#pragma unroll
+    for (int v = 0; v < NVAL; ++v) {
+      D x;
+      x.v = val[v];
+#pragma unroll
+      for (int k = 0; k < NT; ++k) x.d[k] = der[k][v];
+      sum[v] = active ? sum[v] + x : x;
     }
+    active = true;
   };
   if (s.structured) {
     constexpr int NC = DIM == 2 ? 4 : 8;
