@@ -69,7 +69,7 @@ typedef struct {
   int32_t velocity_update;  /* MPM_VELOCITY_FLIP / PIC (particle.tcc:1018-1067), or the
                                affine ASFLIP / APIC and Taylor TPIC updates, which carry a
                                mapping matrix per particle (particle.tcc:630-721,
-                               1071-1139, 1663-1730; FP64, USF and USL) */
+                               1071-1139, 1663-1730; USF and USL, FP64 and mixed) */
   int32_t precision;        /* MPM_PRECISION_FP64: every quantity in FP64, rounding as the
                                reference's CPU run (the parity mode);
                                MPM_PRECISION_MIXED: FP32 transfers and constitutive update

@@ -31,6 +31,7 @@
 #include "mpm_state.cuh"
 
 #ifndef MPM_MIXED_G2P_MIN_BLOCKS
+#define MPM_MIXED_AFFINE_G2P_MIN_BLOCKS 4  // the nodal velocities stay in registers for B
 #define MPM_MIXED_G2P_MIN_BLOCKS 6  // 80 registers, no spills: 0.478 -> 0.374 ms (4M, 3D)
 #endif
 #ifndef MPM_MC_RETURN_MIN_BLOCKS
@@ -116,32 +117,39 @@ __device__ __forceinline__ void cell_nodes_rel(const DevState& s, int c, int* ni
 // (the FP64 local coordinate rounded), mass, velocity, -V0 (1 + P), stress
 // and, off a tensor-product grid, J^-1; per (cell, slot) thread 1 + 3 DIM
 // FP64 sums of the FP32 contributions of the cell's particles in id order,
-// stored as FP32 partials.
-template <int DIM, int MODE, bool BOX>
+// stored as FP32 partials.  AFF: the mass-momentum mapping velocity v + M r of
+// the affine (1: M = B D^-1) or Taylor (2: M = B) updates, with M formed in
+// FP64 by the staging thread and the branch vectors r taken from FP64
+// positions relative to the cell's first node, both rounded to FP32.
+template <int DIM, int MODE, bool BOX, int AFF = 0>
 struct MTileRows {
   static constexpr bool MM = MODE != 1, FORCES = MODE != 0;
   static constexpr int XI = 0, M = DIM, V = DIM + 1;
   static constexpr int SC = V + (MM ? DIM : 0);
   static constexpr int S = SC + 1;
   static constexpr int INV = S + (FORCES ? PF<DIM>::NS : 0);
-  static constexpr int N = INV + (FORCES && !BOX ? DIM * DIM : 0);
+  static constexpr int XP = INV + (FORCES && !BOX ? DIM * DIM : 0);  // x - node 0
+  static constexpr int MV = XP + (MM && AFF ? DIM : 0);              // mapping matrix
+  static constexpr int N = MV + (MM && AFF ? DIM * DIM : 0);
 };
 
 // On box cells the tile may also take 128 threads (a launch-shape choice);
 // the blocks per SM scale so that the registers per thread stay the same.
-template <bool BOX, int T>
+// The mapping-velocity tiles (128 threads) form the FP64 matrix when they
+// stage a row and take up to 128 registers.
+template <bool BOX, int T, int AFF = 0>
 constexpr int mixed_tile_min_blocks() {
-  return BOX ? MPM_MIXED_P2G_TILE_MIN_BLOCKS * 256 / T : MPM_MIXED_P2G_TILE_MIN_BLOCKS;
+  return AFF ? 4 : BOX ? MPM_MIXED_P2G_TILE_MIN_BLOCKS * 256 / T : MPM_MIXED_P2G_TILE_MIN_BLOCKS;
 }
 
-template <int DIM, int MODE, bool BOX, int T = p2g_tile_t<BOX>()>
-__global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T>()))
+template <int DIM, int MODE, bool BOX, int T = p2g_tile_t<BOX>(), int AFF = 0>
+__global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T, AFF>()))
     k_p2g_tiles_mixed(DevState s, float g0, float g1, float g2) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int CB = T / NV;
   constexpr int NVAL = 1 + 3 * DIM;
   constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM;
-  using RW = MTileRows<DIM, MODE, BOX>;
+  using RW = MTileRows<DIM, MODE, BOX, AFF>;
   constexpr bool MM = RW::MM, FORCES = RW::FORCES;
   __shared__ float rows[RW::N][T];
   const int t = threadIdx.x;
@@ -169,6 +177,17 @@ __global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T>()))
 #pragma unroll
       for (int d = 0; d < DIM; ++d) rows[RW::V + d][r] = pmf<DIM>(s, PM<DIM>::V + d, p);
     }
+    if constexpr (MM && AFF) {
+      int nid[NV];
+      double X[NV * DIM], xid[DIM], Mv[DIM * DIM];
+      cell_nodes_coords<DIM>(s, pc, nid, X);
+      particle_xi<DIM, BOX>(s, pc, x, xid);
+      mapping_velocity_matrix<DIM, AFF>(s, p, pc, x, xid, Mv);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) rows[RW::XP + d][r] = (float)(x[d] - X[d]);
+#pragma unroll
+      for (int q = 0; q < DIM * DIM; ++q) rows[RW::MV + q][r] = (float)Mv[q];
+    }
     if constexpr (FORCES) {
       rows[RW::SC][r] = -(pmf<DIM>(s, PM<DIM>::V0, p) * (1.f + pmf<DIM>(s, PM<DIM>::JP, p)));
 #pragma unroll
@@ -187,6 +206,14 @@ __global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T>()))
   if constexpr (BOX && FORCES) {
     if (a1 > a0) box_map = cell_map<DIM, true, float>(s, (int)c, nullptr, nullptr);
   }
+  float xkr[DIM];  // this slot's node relative to the cell's first node (AFF)
+  if constexpr (MM && AFF) {
+    int nid[NV];
+    double X[NV * DIM];
+    if (a1 > a0) cell_nodes_coords<DIM>(s, (int)c, nid, X);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xkr[d] = a1 > a0 ? (float)(X[k * DIM + d] - X[d]) : 0.f;
+  }
   const float gv[3] = {g0, g1, g2};
   double acc[NVAL];
 #pragma unroll
@@ -201,8 +228,23 @@ __global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T>()))
     if constexpr (MM) {
       const float mN = m * N;
       acc[MASS] += (double)mN;
+      float mv[DIM];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) acc[MOM + d] += (double)(mN * rows[RW::V + d][r]);
+      for (int d = 0; d < DIM; ++d) mv[d] = rows[RW::V + d][r];
+      if constexpr (AFF) {
+        float br[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) br[d] = xkr[d] - rows[RW::XP + d][r];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          float sum = rows[RW::MV + a * DIM + 0][r] * br[0];
+#pragma unroll
+          for (int b = 1; b < DIM; ++b) sum = sum + rows[RW::MV + a * DIM + b][r] * br[b];
+          mv[a] += sum;
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) acc[MOM + d] += (double)(mN * mv[d]);
     }
     if constexpr (FORCES) {
       const float sc = rows[RW::SC][r];
@@ -681,6 +723,163 @@ __global__ void __launch_bounds__(128, MPM_MIXED_G2P_MIN_BLOCKS)
   }
 }
 
+// G2P of the velocity updates that carry a mapping matrix (particle.tcc:
+// 1071-1139, 1663-1730), k_g2p<DIM, STRESS, VU, BOX> of the FP64 path with the
+// nodal values in FP32: the matrix B at the step-start position -- affine
+// sum_i N_i v_i r_i^T (APIC, ASFLIP; r_i = node i - x from FP64 positions) or
+// the velocity gradient sum_i v_i dN_i/dx^T (TPIC), entries below 1e-15 set to
+// zero, kept in FP64 -- then APIC and TPIC take the PIC update and ASFLIP the
+// FLIP/PIC blend for the velocity and the separable blend for the position.
+template <int DIM, bool STRESS, int VU, bool BOX>
+__global__ void __launch_bounds__(128, MPM_MIXED_AFFINE_G2P_MIN_BLOCKS)
+    k_g2p_mixed_affine(DevState s, double dt, float beta) {
+  static_assert(VU >= 2, "the mapping-matrix updates");
+  constexpr int NV = Elem<DIM>::NV;
+  constexpr bool ASFLIP = VU == 2, TPIC = VU == 3;  // 4 APIC
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.np) return;
+  const int c = s.cell[p];
+  if (c < 0) return;
+  const int64_t np = s.np;
+  const float dtf = (float)dt;
+  double x[DIM];
+  load_x<DIM>(s, p, x);
+  float xi[DIM], N[NV], Xr[NV * DIM], xr[DIM];
+  int nid[NV];
+  xi_f32<DIM, BOX>(s, c, x, xi);
+  shapefn<DIM>(xi, N);
+  {
+    // the branch vectors r_i = X_i - x as (X_i - X_0) - (x - X_0) in FP32
+    double X[NV * DIM];
+    cell_nodes_coords<DIM>(s, c, nid, X);
+#pragma unroll
+    for (int n = 0; n < NV; ++n)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) Xr[n * DIM + d] = (float)(X[n * DIM + d] - X[d]);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xr[d] = (float)(x[d] - X[d]);
+  }
+  float nvel[DIM], nacc[DIM], vn[NV][DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) nvel[d] = nacc[d] = 0.f;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    float an[DIM];
+    load_nfv<DIM, ASFLIP>(s.nfv, nid[i], vn[i], an);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nvel[d] += N[i] * vn[i][d];
+    if constexpr (ASFLIP) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) nacc[d] += N[i] * an[d];
+    }
+  }
+  float D[NV * DIM];
+  if constexpr (TPIC || ASFLIP || STRESS) dn_dx_all_f<DIM, BOX>(s, c, xi, Xr, D);
+  float B[DIM * DIM];
+#pragma unroll
+  for (int q = 0; q < DIM * DIM; ++q) B[q] = 0.f;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    float r[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) r[d] = Xr[i * DIM + d] - xr[d];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) {
+        if constexpr (TPIC)
+          B[a * DIM + b] += vn[i][a] * D[i * DIM + b];
+        else
+          B[a * DIM + b] += (N[i] * vn[i][a]) * r[b];
+      }
+  }
+#pragma unroll
+  for (int q = 0; q < DIM * DIM; ++q) {
+    if (fabsf(B[q]) < 1.E-15f) B[q] = 0.f;
+    s.mapb[(int64_t)q * np + p] = (double)B[q];
+  }
+  float v[DIM], sep[DIM];  // sep: the velocity that moves the particle
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    v[d] = pmf<DIM>(s, PM<DIM>::V + d, p);
+    sep[d] = nvel[d];
+  }
+  if constexpr (ASFLIP) {
+    // beta (particle.tcc:1711-1730): 0 next to a velocity-constrained node or
+    // when the deformation gradient increment compresses
+    float bp = 1.f;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      const int bci = s.bc_index[nid[i]];
+      if (bci >= 0 && s.bcs[bci].vel_mask != 0) bp = 0.f;
+    }
+    // det(I + A) < 1 with A = sum_i v_i dN_i/dx^T dt: the test is on
+    // det(I + A) - 1 = tr A + (sum of A's principal 2x2 minors) + det A, which
+    // FP32 resolves down to A's own rounding (1 + A in FP32 would lose every
+    // increment below 6e-8 and flip the sign of J - 1 against the FP64 run)
+    float A[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) A[a * 3 + b] += vn[i][a] * D[i * DIM + b] * dtf;
+#pragma unroll
+    for (int q = 0; q < 9; ++q)
+      if (fabsf(A[q]) < 1.E-15f) A[q] = 0.f;  // the snaps of F's entries at 1e-15
+    const float tr = A[0] + A[4] + A[8];
+    const float m2 = (A[0] * A[4] - A[1] * A[3]) + (A[0] * A[8] - A[2] * A[6]) + (A[4] * A[8] - A[5] * A[7]);
+    const float d3 = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+                     A[2] * (A[3] * A[7] - A[4] * A[6]);
+    if (tr + m2 + d3 < 0.f) bp = 0.f;
+    // particle.tcc:1096-1110: FLIP/PIC blend for the velocity, the separable
+    // blend for the position
+    float flip[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) flip[d] = v[d] + nacc[d] * dtf;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      sep[d] = bp * beta * flip[d] + (1.f - bp * beta) * nvel[d];
+      v[d] = beta * flip[d] + (1.f - beta) * nvel[d];
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = nvel[d];
+  }
+  double xn[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const double dx = (double)sep[d] * dt;  // FP64 position / displacement update
+    xn[d] = x[d] + dx;
+    s.pf[(int64_t)(PDX<DIM>::X + d) * np + p] = xn[d];
+    s.pf[(int64_t)(PDX<DIM>::U + d) * np + p] += dx;
+  }
+  const int pv = s.pvc[p];
+  if (pv >= 0) {
+    const ParticleVC& r = s.pvcs[pv];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      if (r.mask & (1u << d)) v[d] = (float)r.value[d];
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) set_pmf<DIM>(s, PM<DIM>::V + d, p, v[d]);
+  if constexpr (STRESS) stress_update_mixed<DIM>(s, MGlobalRow<DIM>{s, p}, c, nid, D, dtf);
+  bool finite = true;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) finite = finite && isfinite(xn[d]);
+  if (!finite) {
+    raise_err(s, ERR_NONFINITE);
+    s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+    return;
+  }
+  const int nc = locate_near<DIM>(s, xn, c);
+  if (nc >= 0) {
+    if (nc != c) s.cell[p] = nc;
+  } else {
+    s.lost[atomicAdd(s.nlost, 1u)] = (int32_t)p;
+  }
+}
+
 // MUSL end of step: the new positions (FP64) replace the old, then locate
 template <int DIM>
 __global__ void __launch_bounds__(128) k_commit_locate_mixed(DevState s) {
@@ -950,11 +1149,32 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
   auto p2g = [&](auto mode) {
     constexpr int MODE = decltype(mode)::value;
     constexpr int NV = Elem<DIM>::NV;
+    if constexpr (MODE != 1) {  // the mass-momentum mapping velocity (128-thread tiles)
+      if (a.vupd == 2 || a.vupd == 4) {
+        k_p2g_tiles_mixed<DIM, MODE, BOX, 128, 1><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s, g0, g1, g2);
+        return;
+      }
+      if (a.vupd == 3) {
+        k_p2g_tiles_mixed<DIM, MODE, BOX, 128, 2><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s, g0, g1, g2);
+        return;
+      }
+    }
     if (BOX && tile_threads(a, BOX) == 128)
       k_p2g_tiles_mixed<DIM, MODE, BOX, 128><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s, g0, g1, g2);
     else
       k_p2g_tiles_mixed<DIM, MODE, BOX><<<nblk(s.ncells, p2g_tile_t<BOX>() / NV), p2g_tile_t<BOX>(),
                                           0, st>>>(s, g0, g1, g2);
+  };
+  // G2P of the mapping-matrix updates (ASFLIP 2, TPIC 3, APIC 4)
+  auto g2p_affine = [&](auto stress) {
+    constexpr bool STRESS = decltype(stress)::value;
+    const float b = (float)a.beta;
+    if (a.vupd == 2)
+      k_g2p_mixed_affine<DIM, STRESS, 2, BOX><<<pb, 128, 0, st>>>(s, a.dt, b);
+    else if (a.vupd == 3)
+      k_g2p_mixed_affine<DIM, STRESS, 3, BOX><<<pb, 128, 0, st>>>(s, a.dt, b);
+    else
+      k_g2p_mixed_affine<DIM, STRESS, 4, BOX><<<pb, 128, 0, st>>>(s, a.dt, b);
   };
   auto mc_returns = [&]() {
     if (!s.svf) return;
@@ -1005,7 +1225,9 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
     const size_t sm = mixed_staged_smem_bytes<DIM>(s.svf != nullptr);
-    if (a.flip) {
+    if (a.vupd >= 2) {
+      g2p_affine(std::true_type{});
+    } else if (a.flip) {
       prefer_shared_memory<k_g2p_mixed_staged<DIM, true, BOX>>();
       k_g2p_mixed_staged<DIM, true, BOX><<<pb, MSTAGE_T, sm, st>>>(s, a.dt, (float)a.beta);
     } else {
@@ -1032,7 +1254,9 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     k_nodes_mixed<DIM, 2><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_G2P, st);
-    if (a.flip)
+    if (a.vupd >= 2)
+      g2p_affine(std::false_type{});
+    else if (a.flip)
       k_g2p_mixed<DIM, false, true, BOX><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);
     else
       k_g2p_mixed<DIM, false, false, BOX><<<pb, 128, 0, st>>>(s, a.dt, (float)a.beta);

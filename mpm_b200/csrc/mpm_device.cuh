@@ -268,6 +268,50 @@ __device__ __forceinline__ void dn_dx_node(const double* xi, const Map& map, int
   map.grad(&G[n * DIM], Dn);
 }
 
+// The matrix M of the mapping velocity v + M r_i of particle p in cell c
+// (position x, local coordinates xi): B D^-1 (AFF 1) with the shape tensor
+// D = sum_i N_i r_i r_i^T, or B (AFF 2).
+template <int DIM, int AFF>
+__device__ __forceinline__ void mapping_velocity_matrix(const DevState& s, int64_t p, int c,
+                                                        const double* x, const double* xi,
+                                                        double* M) {
+  constexpr int NV = Elem<DIM>::NV;
+  double B[DIM * DIM];
+#pragma unroll
+  for (int q = 0; q < DIM * DIM; ++q) B[q] = s.mapb[(int64_t)q * s.np + p];
+  if constexpr (AFF == 2) {
+#pragma unroll
+    for (int q = 0; q < DIM * DIM; ++q) M[q] = B[q];
+  } else {
+    int nid[NV];
+    double X[NV * DIM], N[NV], T[DIM * DIM], Ti[DIM * DIM];
+    cell_nodes_coords<DIM>(s, c, nid, X);
+    shapefn<DIM>(xi, N);
+#pragma unroll
+    for (int q = 0; q < DIM * DIM; ++q) T[q] = 0.;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double r[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) r[d] = X[i * DIM + d] - x[d];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int b = 0; b < DIM; ++b) T[a * DIM + b] += (N[i] * r[a]) * r[b];
+    }
+    inverse<DIM>(T, Ti);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) {
+        double sum = B[a * DIM + 0] * Ti[0 * DIM + b];
+#pragma unroll
+        for (int k = 1; k < DIM; ++k) sum = sum + B[a * DIM + k] * Ti[k * DIM + b];
+        M[a * DIM + b] = sum;
+      }
+  }
+}
+
 // ------------------------------------------------------------ P2G cell tiles
 // Threads per tile: 256 on a tensor-product grid; 128 on a general mesh,
 // whose staged rows add J^-1 and whose threads need more registers, and with

@@ -1291,10 +1291,9 @@ int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out) {
     return MPM_ERR_UNSUPPORTED;
   if (cfg->velocity_update < MPM_VELOCITY_FLIP || cfg->velocity_update > MPM_VELOCITY_APIC)
     return MPM_ERR_UNSUPPORTED;
-  // the mapping-matrix updates run on the FP64 USF / USL path (MUSL's second
+  // the mapping-matrix updates run on the USF / USL paths (MUSL's second
   // mapping would take its branch vectors from the updated positions)
-  if (cfg->velocity_update >= MPM_VELOCITY_ASFLIP &&
-      (cfg->precision != MPM_PRECISION_FP64 || cfg->scheme == MPM_SCHEME_MUSL))
+  if (cfg->velocity_update >= MPM_VELOCITY_ASFLIP && cfg->scheme == MPM_SCHEME_MUSL)
     return MPM_ERR_UNSUPPORTED;
   if (cfg->precision != MPM_PRECISION_FP64 && cfg->precision != MPM_PRECISION_MIXED)
     return MPM_ERR_UNSUPPORTED;

@@ -146,3 +146,38 @@ def test_musl_2d_linear_elastic_within_1e5_of_fp64():
     assert np.array_equal(m["cell"], f["cell"])
     errs = _errors(m, f)
     assert all(v <= 1e-5 for v in errs.values()), errs
+
+
+def _mapping_error(m, f):
+    return float(np.max(np.abs(m["mapping"] - f["mapping"])) / np.max(np.abs(f["mapping"])))
+
+
+@pytest.mark.parametrize("vu", ["asflip", "tpic", "apic"])
+@pytest.mark.parametrize("scheme", ["usf", "usl"])
+def test_mapping_matrix_updates_2d_within_1e5_of_fp64(vu, scheme):
+    """ASFLIP / TPIC / APIC (particle.tcc:1071-1139, 1663-1730) in mixed
+    precision: the 2D LinearElastic column over 1,000 steps, every field within
+    1e-5 of the FP64 run of the same update, the mapping matrix within 1e-4
+    (it is a difference of nodal velocities, formed from FP32 values)."""
+    prob = P.column_2d(scheme=scheme, velocity_update=vu)
+    m, f = _run(prob, 1000, "mixed"), _run(prob, 1000, "fp64")
+    assert np.array_equal(m["cell"], f["cell"])
+    errs = _errors(m, f)
+    assert all(v <= 1e-5 for v in errs.values()), (vu, scheme, errs)
+    assert _mapping_error(m, f) <= 1e-4, (vu, scheme, _mapping_error(m, f))
+
+
+@pytest.mark.parametrize("vu", ["asflip", "tpic", "apic"])
+def test_mapping_matrix_updates_3d_mohr_coulomb_short_horizon(vu):
+    """The cohesive column (c = 2 kPa, psi = 5 deg) over 50 USL steps: every
+    field within 1e-5.  In the cohesionless column APIC and TPIC bring the
+    top corner's points to the apex (tension state) within 50 steps; those
+    few points' stresses are then within 7e-4 of FP64, every other point's
+    within 7e-7, which is the apex return's conditioning."""
+    prob = P.column_3d(shape=(20, 10, 10), block=(10, 10, 10), scheme="usl", velocity_update=vu,
+                       c=2000., psi=5.)
+    m, f = _run(prob, 50, "mixed"), _run(prob, 50, "fp64")
+    assert np.array_equal(m["cell"], f["cell"])
+    errs = _errors(m, f)
+    assert all(v <= 1e-5 for v in errs.values()), (vu, errs)
+    assert _mapping_error(m, f) <= 1e-4, (vu, _mapping_error(m, f))

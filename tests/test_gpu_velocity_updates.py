@@ -62,8 +62,7 @@ def test_mapping_matrix_load_and_read():
     assert np.array_equal(s.read()["mapping"], b)
 
 
-@pytest.mark.parametrize("over", [dict(precision="mixed"), dict(scheme="musl"),
-                                  dict(scheme="musl", precision="mixed")])
+@pytest.mark.parametrize("over", [dict(scheme="musl"), dict(scheme="musl", precision="mixed")])
 def test_unsupported_combinations_are_refused(over):
     prob = small_column_2d(velocity_update="apic")
     with pytest.raises(MPMError):
