@@ -328,6 +328,23 @@ def time_arm(prob, precision, args, world, dev, clocks=None):
     return s, ms, prof, launches, setup_s
 
 
+def time_persistent(prob, args, world, dev):
+    """The persistent form of the mixed USL step (every pass of K steps in one
+    cooperative launch, grid barriers between the passes) timed like the
+    per-pass graph arm: same warm-up, K steps per launch, device events; its
+    results are bitwise those of the graph arm (tests/test_gpu_persistent.py)."""
+    from mpm_b200 import problems as P
+    s = P.build_solver(prob, precision="mixed", device=dev)
+    s.set_persistent(args.steps)
+    s.step(args.warmup)
+    barrier(world)
+    ms = max_over_ranks(s.step_timed(args.steps), world)
+    n = s.nparticles
+    s.close()
+    return {"ms_per_step": ms / args.steps, "value": world * n * args.steps / (ms / 1e3),
+            "steps_per_launch": args.steps, "launches": 1}
+
+
 def field_errors(a, b):
     """max |a - b| / max |b| per field (F compared as F - I)."""
     out = {}
@@ -640,6 +657,12 @@ def main():
                 "mixed_vs_fp64_field_errors": field_errors(state, s64.read())}
         del s64
 
+    # the persistent form of the same step (one launch for the K steps)
+    persistent = None
+    if args.precision == "mixed" and prob.analysis.get("scheme", "usl") == "usl":
+        persistent = time_persistent(prob, args, world, dev)
+        persistent["graph_over_persistent"] = (ms / args.steps) / persistent["ms_per_step"]
+
     # end to end through the public API with host arrays
     st = state
     h2d = sum(np.asarray(st[k]).nbytes for k in ("x", "u", "v", "stress", "strain", "F", "volume",
@@ -713,7 +736,7 @@ def main():
                        "kernel_profile_steps": args.profile_steps,
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "setup_s": setup_s},
-            "fp64": fp64,
+            "fp64": fp64, "persistent": persistent,
             "accuracy": accuracy, "late": late,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "launch_shape": s.tune_report,

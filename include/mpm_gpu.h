@@ -213,6 +213,19 @@ int mpm_gpu_set_launch_shape(mpm_gpu_t h, int32_t p2g_tile, int32_t node_threads
 int mpm_gpu_get_launch_shape(mpm_gpu_t h, int32_t* shape);
 int mpm_gpu_autotune(mpm_gpu_t h, int64_t steps, char* report, size_t report_len);
 
+/* Persistent steps (the batched form's one-launch step; no counterpart in the
+ * reference): with steps_per_launch > 0, mpm_gpu_step advances up to that
+ * many whole steps per cooperative kernel launch, every block resident, the
+ * passes of a step (sort, P2G, node update, G2P and stress, plastic returns,
+ * exhaustive locate) separated by grid barriers with bounded waits
+ * (MPM_ERR_TIMEOUT when one runs out); 0 returns to one launch per pass,
+ * replayed from a CUDA graph (the default).  Results are bit for bit those
+ * of the per-pass launches.  Mixed precision, USL, FLIP or PIC, on a
+ * tensor-product grid, without sensitivities (MPM_ERR_UNSUPPORTED
+ * otherwise: here for the configuration, at mpm_gpu_step for the mesh and
+ * sensitivities); per-kernel profiling steps run per pass. */
+int mpm_gpu_set_persistent(mpm_gpu_t h, int32_t steps_per_launch);
+
 /* Per-kernel device timing (CUDA events around every launch on the solver's
  * stream).  Enabling or disabling resets the counters.  Kernel indices run
  * from 0 while the call succeeds; name receives a static string. */

@@ -41,28 +41,8 @@ namespace mpm_b200 {
 namespace {
 
 // ------------------------------------------------------------ counting sort
-// Per-cell counts and each particle's slot within its cell.  The lanes of a
-// warp in the same cell (most of them: particles are stored in cell order)
-// share one atomic; the slot order within a cell is not deterministic either
-// way and P2G sorts every cell's segment.
 __global__ void __launch_bounds__(256) k_count(DevState s) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool in = p < s.np;
-  const int c = in ? s.cell[p] : -1;
-  if (c >= s.ncells) raise_err(s, ERR_BADCELL);
-  const bool valid = c >= 0 && c < s.ncells;
-  const unsigned active = __ballot_sync(0xffffffffu, valid);  // every lane of the warp
-  if (!valid) {
-    if (in) s.rank[p] = -1;
-    return;
-  }
-  const unsigned same = __match_any_sync(active, c);
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(same) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(&s.cnt[c], __popc(same));
-  base = __shfl_sync(same, base, leader);
-  s.rank[p] = base + __popc(same & ((1u << lane) - 1u));
+  count_particle(s, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // exclusive scan of n ints, SCAN_BLOCK per block (1024 threads x 4)
@@ -112,11 +92,7 @@ __global__ void __launch_bounds__(256) k_scan_add(int32_t* out, const int32_t* b
 }
 
 __global__ void __launch_bounds__(256) k_fill(DevState s) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= s.np) return;
-  const int c = s.cell[p];
-  if (c < 0 || c >= s.ncells) return;
-  s.order[s.start[c] + s.rank[p]] = (int32_t)p;
+  fill_particle(s, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------- P2G tiles
@@ -1059,45 +1035,7 @@ __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return(Dev
 // contains the point).  Grid-stride over the lost list; usually empty.
 template <int DIM>
 __global__ void k_locate_fallback(DevState s, int remove_lost) {
-  const unsigned count = *s.nlost;
-  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-    const int64_t p = s.lost[k];
-    double x[DIM];
-    load_x<DIM>(s, p, x);
-    int found = -1;
-    if (s.structured) {
-      found = structured_scan<DIM>(x, s.gcells, s.axis, s.geom);
-    } else {
-      bool inside = true;
-      int b[3] = {0, 0, 0};
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        const double f = floor((x[d] - s.bmin[d]) / s.bsize[d]);
-        if (!(f >= 0.) || f >= (double)s.bn[d])
-          inside = false;
-        else
-          b[d] = (int)f;
-      }
-      if (inside) {
-        const int64_t bi = ((int64_t)b[2] * s.bn[1] + b[1]) * s.bn[0] + b[0];
-        for (int j = s.bin_off[bi]; j < s.bin_off[bi + 1]; ++j) {
-          const int cid = s.bin_cells[j];
-          double xi[DIM];
-          if (cell_point_in<DIM>(s, cid, x, xi)) {
-            found = cid;
-            break;
-          }
-        }
-      }
-    }
-    if (found >= 0) {
-      s.cell[p] = found;
-    } else if (remove_lost) {
-      s.cell[p] = -1;
-    } else {
-      raise_err(s, ERR_OUTSIDE);
-    }
-  }
+  locate_lost<DIM>(s, remove_lost, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 inline unsigned nblocks(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }

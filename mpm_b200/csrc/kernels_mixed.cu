@@ -26,16 +26,29 @@
 
 #include "mpm_bulk.cuh"
 #include "mpm_device.cuh"
+#include "mpm_grid.cuh"
 #include "mpm_kernels.h"
 #include "mpm_return.cuh"
 #include "mpm_state.cuh"
 
 #ifndef MPM_MIXED_G2P_MIN_BLOCKS
-#define MPM_MIXED_AFFINE_G2P_MIN_BLOCKS 4  // the nodal velocities stay in registers for B
 #define MPM_MIXED_G2P_MIN_BLOCKS 6  // 80 registers, no spills: 0.478 -> 0.374 ms (4M, 3D)
+#endif
+#ifndef MPM_MIXED_AFFINE_G2P_MIN_BLOCKS
+#define MPM_MIXED_AFFINE_G2P_MIN_BLOCKS 4  // the nodal velocities stay in registers for B
 #endif
 #ifndef MPM_MC_RETURN_MIN_BLOCKS
 #define MPM_MC_RETURN_MIN_BLOCKS 4  // pass-loop return, 1M column at step 2000: 2 / 3 / 4 / 6 blocks -> FP64 0.362 / 0.320 / 0.323 / 0.403 ms, mixed 0.370 / 0.318 / 0.311 / 0.384 ms
+#endif
+// Blocks per SM of the persistent step kernel (3D, 2D).  Measured with 20
+// steps per launch, ms per step on the 4M-particle column / the 512-slope
+// ensemble: 4 blocks 1.303 / 3.018, 6 blocks 1.128 / 2.382, 8 blocks 1.161 /
+// 2.047 (per-pass launches: 0.748 / 1.555).
+#ifndef MPM_PERSISTENT_MIN_BLOCKS_3D
+#define MPM_PERSISTENT_MIN_BLOCKS_3D 6
+#endif
+#ifndef MPM_PERSISTENT_MIN_BLOCKS_2D
+#define MPM_PERSISTENT_MIN_BLOCKS_2D 8
 #endif
 #ifndef MPM_MIXED_P2G_TILE_MIN_BLOCKS
 #define MPM_MIXED_P2G_TILE_MIN_BLOCKS 5  // 48 registers, small spills: 0.32 -> 0.26 ms (4M, 3D)
@@ -142,9 +155,11 @@ constexpr int mixed_tile_min_blocks() {
   return AFF ? 4 : BOX ? MPM_MIXED_P2G_TILE_MIN_BLOCKS * 256 / T : MPM_MIXED_P2G_TILE_MIN_BLOCKS;
 }
 
-template <int DIM, int MODE, bool BOX, int T = p2g_tile_t<BOX>(), int AFF = 0>
-__global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T, AFF>()))
-    k_p2g_tiles_mixed(DevState s, float g0, float g1, float g2) {
+// One tile (block-sized group of cells, tile index bx) of the P2G pass; the
+// block's threads are the tile's (cell, slot) pairs.
+template <int DIM, int MODE, bool BOX, int T, int AFF = 0>
+__device__ __forceinline__ void p2g_tile_mixed(const DevState& s, float g0, float g1, float g2,
+                                               int64_t bx) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int CB = T / NV;
   constexpr int NVAL = 1 + 3 * DIM;
@@ -153,7 +168,7 @@ __global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T, AFF>()))
   constexpr bool MM = RW::MM, FORCES = RW::FORCES;
   __shared__ float rows[RW::N][T];
   const int t = threadIdx.x;
-  const int64_t c0 = (int64_t)blockIdx.x * CB;
+  const int64_t c0 = bx * CB;
   if (c0 >= s.ncells) return;
   const int64_t c1 = c0 + CB < s.ncells ? c0 + CB : s.ncells;
   const int64_t q_begin = s.start[c0], q_end = s.start[c1 - 1] + s.cnt[c1 - 1];
@@ -297,6 +312,12 @@ __global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T, AFF>()))
   }
 }
 
+template <int DIM, int MODE, bool BOX, int T = p2g_tile_t<BOX>(), int AFF = 0>
+__global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T, AFF>()))
+    k_p2g_tiles_mixed(DevState s, float g0, float g1, float g2) {
+  p2g_tile_mixed<DIM, MODE, BOX, T, AFF>(s, g0, g1, g2, blockIdx.x);
+}
+
 // ---------------------------------------------------------------- node update
 // The cell partials of a node (ascending cell id) added in FP64.
 template <int DIM, int V0, int NVS>
@@ -364,8 +385,8 @@ __device__ __forceinline__ void node_accel_update_d(const DevState& s, double m,
 // 8 blocks per SM: 0.111 -> 0.108 ms per 1M-node launch (more warps in flight
 // on the scattered partial loads, despite small spills)
 template <int DIM, int MODE>
-__global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, double damping) {
-  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void node_update_mixed(const DevState& s, double dt, double damping,
+                                                  int64_t n) {
   if (n >= s.nn) return;
   constexpr int NVAL = 1 + 3 * DIM;
   double sum[NVAL];
@@ -407,6 +428,11 @@ __global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, d
     af[d] = (float)acc[d];
   }
   store_nfv<DIM>(s.nfv, n, vf, af);
+}
+
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, double damping) {
+  node_update_mixed<DIM, MODE>(s, dt, damping, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ------------------------------------------------------- stress and strain
@@ -921,16 +947,17 @@ constexpr size_t mixed_staged_smem_bytes(bool mc) {
          MSTAGE_T * (4 + 2 + 2);
 }
 
+// One block of MSTAGE_T particles (block index bx) with the staging buffers
+// smem, the two initialised copy barriers bar in the phase of the given
+// parity, and the block's timed-out flag.
 template <int DIM, bool FLIP, bool BOX>
-__global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
-    k_g2p_mixed_staged(DevState s, double dt, float beta) {
+__device__ __forceinline__ void g2p_staged_block_mixed(const DevState& s, double dt, float beta,
+                                                       int64_t bx, unsigned char* smem, uint64_t* bar,
+                                                       unsigned parity, int& timed_out) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int T = MSTAGE_T;
   constexpr int XROWS = 2 * DIM;       // x, u
   constexpr int MROWS = PM<DIM>::MASS;  // v .. P
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ uint64_t bar[2];
-  __shared__ int timed_out;
   const bool mc = s.svf != nullptr;
   double* xr = reinterpret_cast<double*>(smem);
   float* mr = reinterpret_cast<float*>(xr + XROWS * T);
@@ -939,14 +966,9 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   uint16_t* smat = reinterpret_cast<uint16_t*>(scell + T);
   int16_t* spvc = reinterpret_cast<int16_t*>(smat + T);
   const int t = threadIdx.x;
-  const int64_t p0 = (int64_t)blockIdx.x * T;
+  const int64_t p0 = bx * T;
   const int64_t np = s.np;
-  if (t == 0) {
-    timed_out = 0;
-    bulk::mbar_init(&bar[0], 1);
-    bulk::mbar_init(&bar[1], 1);
-    bulk::fence_barrier_init();
-  }
+  if (t == 0) timed_out = 0;
   __syncthreads();
   if (t == 0) {
     bulk::mbar_arrive_expect_tx(&bar[0], 2 * DIM * T * 8 + DIM * T * 4 + T * (4 + 2 + 2));
@@ -962,7 +984,9 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
     if (mc)
       for (int k = 0; k < SVF_N; ++k) bulk::load(svr + k * T, s.svf + k * np + p0, T * 4, &bar[1]);
   }
-  const bool okA = bulk::mbar_wait(&bar[0], 0) && !(s.test_wait_timeout && !bulk::mbar_wait_never(&bar[0]));
+  // the test hook waits for the next phase, which no copy completes
+  const bool okA = bulk::mbar_wait(&bar[0], parity) &&
+                   !(s.test_wait_timeout && !bulk::mbar_wait(&bar[0], parity ^ 1u, 16));
   const int c = okA ? scell[t] : -1;
   const int64_t p = p0 + t;
   const MSmemRow r{mr, svr, t, okA ? (int)smat[t] : 0, p0 + t};
@@ -1022,7 +1046,7 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
 #pragma unroll
     for (int d = 0; d < DIM; ++d) r.m(PM<DIM>::V + d) = v[d];
   }
-  const bool okB = okA && bulk::mbar_wait(&bar[1], 0);
+  const bool okB = okA && bulk::mbar_wait(&bar[1], parity);
   if (!okA || !okB) timed_out = 1;
   if (active && okB) {
     // node ids and coordinates again rather than kept live across the wait
@@ -1037,8 +1061,8 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   if (timed_out) {
     if (t == 0) {
       raise_err(s, ERR_TIMEOUT);
-      bulk::mbar_wait(&bar[0], 0);
-      bulk::mbar_wait(&bar[1], 0);
+      bulk::mbar_wait(&bar[0], parity);
+      bulk::mbar_wait(&bar[1], parity);
     }
     return;
   }
@@ -1071,6 +1095,20 @@ __global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
   if (t == 0) bulk::store_wait_all();
 }
 
+template <int DIM, bool FLIP, bool BOX>
+__global__ void __launch_bounds__(MSTAGE_T, MPM_MIXED_G2P_MIN_BLOCKS)
+    k_g2p_mixed_staged(DevState s, double dt, float beta) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar[2];
+  __shared__ int timed_out;
+  if (threadIdx.x == 0) {
+    bulk::mbar_init(&bar[0], 1);
+    bulk::mbar_init(&bar[1], 1);
+    bulk::fence_barrier_init();
+  }
+  g2p_staged_block_mixed<DIM, FLIP, BOX>(s, dt, beta, blockIdx.x, smem, bar, 0u, timed_out);
+}
+
 template <auto Kernel>
 void prefer_shared_memory() {
   static unsigned done = 0;  // one bit per device
@@ -1088,11 +1126,12 @@ void prefer_shared_memory() {
 // update (mohr_coulomb.tcc:348-513, as mc_return's passes) from the FP32
 // stress and state before the step's update, rounded back to FP32; the number
 // of corrections is kept for the next step's grouping.
+// The FP64 returns of listed entries begin, begin + stride, ...
 template <int DIM>
-__global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return_mixed(DevState s) {
+__device__ __forceinline__ void mc_return_mixed_range(const DevState& s, unsigned begin, unsigned stride) {
   const unsigned nl = *s.nplastic, n = nl + *s.nplastic_heavy;
   const int64_t np = s.np;
-  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+  for (unsigned t = begin; t < n; t += stride) {
     const unsigned i = list_slot(s, t, nl);
     const int64_t p = s.plist[i];
     const MGlobalRow<DIM> r{s, p};
@@ -1132,7 +1171,167 @@ __global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return_mix
   }
 }
 
+template <int DIM>
+__global__ void __launch_bounds__(128, MPM_MC_RETURN_MIN_BLOCKS) k_mc_return_mixed(DevState s) {
+  mc_return_mixed_range<DIM>(s, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 inline unsigned nblk(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+// ------------------------------------------------------ persistent steps
+// The exclusive scan of the counts of chunk `chunk` (SCAN_BLOCK cells; T
+// threads, SCAN_BLOCK / T consecutive cells each) into start, and the chunk's
+// total into bsum[chunk].
+template <int T>
+__device__ __forceinline__ void scan_chunk(const int32_t* cnt, int32_t* start, int32_t* bsum,
+                                           int64_t n, int64_t chunk, int32_t* red) {
+  constexpr int PER = SCAN_BLOCK / T;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int64_t base = chunk * SCAN_BLOCK + (int64_t)t * PER;
+  int32_t v[PER], run = 0;
+#pragma unroll
+  for (int i = 0; i < PER; ++i) v[i] = base + i < n ? cnt[base + i] : 0;
+#pragma unroll
+  for (int i = 0; i < PER; ++i) run += v[i];
+  int32_t x = run;  // inclusive scan of the thread totals within the warp
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int32_t y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) red[w] = x;
+  __syncthreads();
+  int32_t prefix = x - run;
+  for (int k = 0; k < w; ++k) prefix += red[k];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    if (base + i < n) start[base + i] = prefix;
+    prefix += v[i];
+  }
+  if (t == T - 1) bsum[chunk] = prefix;
+  __syncthreads();  // red is reused by the next chunk
+}
+
+// The total of bsum[0, count) by the block's T threads (every thread gets it).
+template <int T>
+__device__ __forceinline__ int32_t block_total(const int32_t* bsum, int64_t count, int32_t* red) {
+  int32_t x = 0;
+  for (int64_t j = threadIdx.x; j < count; j += T) x += bsum[j];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+  __syncthreads();
+  int32_t total = 0;
+#pragma unroll
+  for (int k = 0; k < T / 32; ++k) total += red[k];
+  __syncthreads();
+  return total;
+}
+
+// K whole mixed USL steps on a tensor-product grid in one cooperative launch.
+// Each pass is the body of the corresponding one-pass kernel of step_mixed,
+// over block-sized pieces (cell tiles, particle blocks, node blocks) taken
+// grid-stride, so the results are bit for bit those of the per-pass launches
+// (the P2G tiles have 128 threads; each cell's particle ids are sorted before
+// they are added, so the slot order the counting sort leaves does not matter):
+//   count | scan chunks | chunk prefixes | fill | P2G | nodes |
+//   G2P + stress (and the next step's counts zeroed) | returns [| locate]
+template <int DIM, bool FLIP>
+__global__ void __launch_bounds__(MSTAGE_T, DIM == 2 ? MPM_PERSISTENT_MIN_BLOCKS_2D : MPM_PERSISTENT_MIN_BLOCKS_3D)
+    k_steps_persistent_mixed(DevState s, StepArgs a, PersistentArgs q) {
+  constexpr int T = MSTAGE_T;
+  constexpr int NV = Elem<DIM>::NV;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar[2];
+  __shared__ int timed_out, go;
+  __shared__ int32_t red[T / 32];
+  const int t = threadIdx.x;
+  const unsigned G = gridDim.x;
+  const int64_t np = s.np, nc = s.ncells;
+  const int64_t pblocks = (np + T - 1) / T, tiles = (nc + T / NV - 1) / (T / NV);
+  const int64_t nodeblocks = (s.nn + T - 1) / T, chunks = (nc + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  const unsigned gi = blockIdx.x * T + t, gs = G * T;  // grid-stride start and stride
+  unsigned gen = 0;
+  if (t == 0) {
+    bulk::mbar_init(&bar[0], 1);
+    bulk::mbar_init(&bar[1], 1);
+    bulk::fence_barrier_init();
+    gen = ld_acquire_gpu(&q.barrier[1]);
+  }
+  for (int64_t i = gi; i < nc; i += gs) s.cnt[i] = 0;
+  if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+  unsigned parity = 0;
+  for (int64_t k = 0; k < q.nsteps; ++k) {
+    double gm = 1.0;  // the host's ramp, the same operations
+    if (q.ramp > 0.0) gm = fmin(1.0, static_cast<double>(q.step0 + k) * a.dt / q.ramp);
+    const float g0 = (float)(DIM > 0 ? gm * q.gravity[0] : 0.);
+    const float g1 = (float)(DIM > 1 ? gm * q.gravity[1] : 0.);
+    const float g2 = (float)(DIM > 2 ? gm * q.gravity[2] : 0.);
+    // counting sort
+    if (blockIdx.x == 0 && t == 0) {
+      *s.nlost = 0;
+      if (s.svf) *s.nplastic = *s.nplastic_heavy = 0;
+    }
+    for (int64_t b = blockIdx.x; b < pblocks; b += G) count_particle(s, b * T + t);
+    if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+    for (int64_t b = blockIdx.x; b < chunks; b += G) scan_chunk<T>(s.cnt, s.start, s.bsum, nc, b, red);
+    if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+    for (int64_t b = blockIdx.x; b < chunks; b += G) {
+      const int32_t prefix = block_total<T>(s.bsum, b, red);
+      for (int64_t i = b * SCAN_BLOCK + t; i < nc && i < (b + 1) * SCAN_BLOCK; i += T) s.start[i] += prefix;
+      if (b == chunks - 1 && t == 0) s.start[nc] = prefix + s.bsum[b];
+    }
+    if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+    for (int64_t b = blockIdx.x; b < pblocks; b += G) fill_particle(s, b * T + t);
+    if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+    // P2G of mass, momentum and forces
+    for (int64_t b = blockIdx.x; b < tiles; b += G) {
+      p2g_tile_mixed<DIM, 2, true, T>(s, g0, g1, g2, b);
+      __syncthreads();  // the tile's staged rows are consumed
+    }
+    if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+    for (int64_t b = blockIdx.x; b < nodeblocks; b += G) node_update_mixed<DIM, 1>(s, a.dt, a.damping, b * T + t);
+    if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+    // G2P with the stress update; the counts are free once the nodes are done
+    for (int64_t b = blockIdx.x; b < pblocks; b += G) {
+      g2p_staged_block_mixed<DIM, FLIP, true>(s, a.dt, (float)a.beta, b, smem, bar, parity, timed_out);
+      parity ^= 1u;
+      __syncthreads();  // the block's staging buffers are free again
+    }
+    for (int64_t i = gi; i < nc; i += gs) s.cnt[i] = 0;
+    if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+    if (s.svf) {
+      mc_return_mixed_range<DIM>(s, gi, gs);
+      if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+    }
+    if (ld_acquire_gpu(s.nlost) != 0) {  // the same value in every block
+      locate_lost<DIM>(s, a.remove_lost, gi, gs);
+      if (!grid_barrier(s, q.barrier, G, gen, go)) return;
+    }
+  }
+}
+
+template <int DIM, bool FLIP>
+cudaError_t launch_persistent(const DevState& s, const StepArgs& a, const PersistentArgs& q,
+                              cudaStream_t st) {
+  auto kernel = k_steps_persistent_mixed<DIM, FLIP>;
+  const size_t sm = mixed_staged_smem_bytes<DIM>(s.svf != nullptr);
+  prefer_shared_memory<k_steps_persistent_mixed<DIM, FLIP>>();
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, MSTAGE_T, sm);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+  e = cudaMemsetAsync(q.barrier, 0, 2 * sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  DevState sv = s;
+  StepArgs av = a;
+  PersistentArgs qv = q;
+  void* args[] = {&sv, &av, &qv};
+  return cudaLaunchCooperativeKernel((const void*)kernel, dim3((unsigned)(per_sm * sms)), dim3(MSTAGE_T),
+                                     args, sm, st);
+}
 
 template <int DIM, bool BOX>
 void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler& pr) {
@@ -1268,6 +1467,14 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
 }
 
 }  // namespace
+
+cudaError_t launch_steps_persistent_mixed(int dim, const DevState& s, const StepArgs& a,
+                                          const PersistentArgs& q, cudaStream_t st) {
+  if (s.np == 0 || q.nsteps <= 0) return cudaSuccess;
+  if (dim == 2)
+    return a.flip ? launch_persistent<2, true>(s, a, q, st) : launch_persistent<2, false>(s, a, q, st);
+  return a.flip ? launch_persistent<3, true>(s, a, q, st) : launch_persistent<3, false>(s, a, q, st);
+}
 
 void launch_step_mixed(int dim, const DevState& s, const StepArgs& a, cudaStream_t st,
                        Profiler& prof) {

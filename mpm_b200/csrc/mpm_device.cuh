@@ -479,5 +479,86 @@ __device__ __forceinline__ int locate_near(const DevState& s, const double* x, i
 }
 
 
+// ------------------------------------------------------------ counting sort
+// The passes of the per-step counting sort of particles by cell, as bodies
+// that a one-kernel-per-pass launch and the persistent step kernel share.
+// Per-cell counts and each particle's slot within its cell.  The lanes of a
+// warp in the same cell (most of them: particles are stored in cell order)
+// share one atomic; the slot order within a cell is not deterministic either
+// way and P2G sorts every cell's segment.
+__device__ __forceinline__ void count_particle(const DevState& s, int64_t p) {
+  const bool in = p < s.np;
+  const int c = in ? s.cell[p] : -1;
+  if (c >= s.ncells) raise_err(s, ERR_BADCELL);
+  const bool valid = c >= 0 && c < s.ncells;
+  const unsigned active = __ballot_sync(0xffffffffu, valid);  // every lane of the warp
+  if (!valid) {
+    if (in) s.rank[p] = -1;
+    return;
+  }
+  const unsigned same = __match_any_sync(active, c);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(same) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&s.cnt[c], __popc(same));
+  base = __shfl_sync(same, base, leader);
+  s.rank[p] = base + __popc(same & ((1u << lane) - 1u));
+}
+
+// The particle's place in the cell-sorted order (start of its cell + rank).
+__device__ __forceinline__ void fill_particle(const DevState& s, int64_t p) {
+  if (p >= s.np) return;
+  const int c = s.cell[p];
+  if (c < 0 || c >= s.ncells) return;
+  s.order[s.start[c] + s.rank[p]] = (int32_t)p;
+}
+
+// The exhaustive locate of the particles that left their cell's neighbourhood
+// in G2P (mesh.tcc:1116-1151 over all cells); listed entries begin, begin +
+// stride, ...
+template <int DIM>
+__device__ __forceinline__ void locate_lost(const DevState& s, int remove_lost, unsigned begin,
+                                            unsigned stride) {
+  const unsigned count = *s.nlost;
+  for (unsigned k = begin; k < count; k += stride) {
+    const int64_t p = s.lost[k];
+    double x[DIM];
+    load_x<DIM>(s, p, x);
+    int found = -1;
+    if (s.structured) {
+      found = structured_scan<DIM>(x, s.gcells, s.axis, s.geom);
+    } else {
+      bool inside = true;
+      int b[3] = {0, 0, 0};
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const double f = floor((x[d] - s.bmin[d]) / s.bsize[d]);
+        if (!(f >= 0.) || f >= (double)s.bn[d])
+          inside = false;
+        else
+          b[d] = (int)f;
+      }
+      if (inside) {
+        const int64_t bi = ((int64_t)b[2] * s.bn[1] + b[1]) * s.bn[0] + b[0];
+        for (int j = s.bin_off[bi]; j < s.bin_off[bi + 1]; ++j) {
+          const int cid = s.bin_cells[j];
+          double xi[DIM];
+          if (cell_point_in<DIM>(s, cid, x, xi)) {
+            found = cid;
+            break;
+          }
+        }
+      }
+    }
+    if (found >= 0) {
+      s.cell[p] = found;
+    } else if (remove_lost) {
+      s.cell[p] = -1;
+    } else {
+      raise_err(s, ERR_OUTSIDE);
+    }
+  }
+}
+
 }  // namespace
 }  // namespace mpm_b200

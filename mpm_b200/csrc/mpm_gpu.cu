@@ -350,7 +350,7 @@ struct mpm_gpu_solver {
   DevBuf<uint8_t> d_active;
   DevBuf<int16_t> d_pvc;
   DevBuf<CellGeom> d_geom;
-  DevBuf<unsigned> d_words;  // [0] nlost, [1] err, [2] nplastic
+  DevBuf<unsigned> d_words;  // [0] nlost, [1] err, [2] nplastic, [3] nplastic_heavy, [4, 6) grid barrier
   DevBuf<int32_t> d_plist;
   DevBuf<double> d_pbuf;
   DevBuf<uint8_t> d_rpass;
@@ -388,6 +388,7 @@ struct mpm_gpu_solver {
   // launch shape of the value steps (mpm_gpu_set_launch_shape, mpm_gpu_autotune);
   // zeros are the built-in defaults
   int shape_p2g_tile = 0, shape_node_threads = 0, shape_return_bps = 0;
+  int persistent_steps = 0;  // > 0: steps per persistent launch
   // one captured step, replayed while the device state and step arguments
   // stay the same
   cudaGraphExec_t graph = nullptr;
@@ -746,8 +747,8 @@ void upload_mesh(mpm_gpu_t h) {
   h->d_active.alloc(h->nnodes);
   ck(cudaMemsetAsync(h->d_active.p, 0, h->nnodes, st), "memset");
   ck(cudaMemsetAsync(h->d_nf.p, 0, sizeof(double) * h->nnf() * h->nnodes, st), "memset");
-  h->d_words.alloc(4);
-  ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 4, st), "memset");
+  h->d_words.alloc(6);
+  ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 6, st), "memset");
   if (h->structured)
     for (int d = 0; d < 3; ++d) {
       h->d_axis[d].upload(h->axis[d].data(), h->axis[d].size(), st);
@@ -1738,6 +1739,23 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
     else
       launch_step_fp64(h->dim, h->ds, a, h->stream, h->prof);
   };
+  if (h->persistent_steps > 0 && !h->prof.enabled) {
+    if (!h->structured || h->ntangent > 0)
+      return fail(h, MPM_ERR_UNSUPPORTED,
+                  "persistent steps need a tensor-product grid and no sensitivities");
+    PersistentArgs q{};
+    for (int d = 0; d < 3; ++d) q.gravity[d] = d < h->dim ? h->cfg.gravity[d] : 0.;
+    q.ramp = h->cfg.gravity_ramping_time;
+    q.barrier = h->d_words.p + 4;
+    for (int64_t s = 0; s < nsteps; s += q.nsteps) {
+      q.nsteps = std::min<int64_t>(h->persistent_steps, nsteps - s);
+      q.step0 = h->step;
+      ck(launch_steps_persistent_mixed(h->dim, h->ds, a, q, h->stream), "persistent step launch");
+      h->prof.launches += 1;
+      h->step += q.nsteps;
+    }
+    nsteps = 0;  // done: the loop below only finishes the call
+  }
   // A step whose device state and arguments match the captured one replays the
   // captured CUDA graph (one graph launch instead of the step's kernel
   // launches).  The first step of a call runs eagerly (it sets the kernels'
@@ -1824,6 +1842,17 @@ int mpm_gpu_set_launch_shape(mpm_gpu_t h, int32_t p2g_tile, int32_t node_threads
   h->shape_p2g_tile = p2g_tile;
   h->shape_node_threads = node_threads;
   h->shape_return_bps = return_blocks_per_sm;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_set_persistent(mpm_gpu_t h, int32_t steps_per_launch) {
+  MPM_GUARD(h)
+  if (steps_per_launch < 0) throw InvalidArg("negative steps per launch");
+  if (steps_per_launch > 0 &&
+      (!h->mixed || h->cfg.scheme != MPM_SCHEME_USL || h->cfg.velocity_update > MPM_VELOCITY_PIC))
+    return fail(h, MPM_ERR_UNSUPPORTED, "persistent steps run the mixed USL step with FLIP or PIC");
+  h->persistent_steps = steps_per_launch;
   MPM_END(h)
   return MPM_OK;
 }

@@ -84,6 +84,20 @@ void launch_step_fp64(int dim, const DevState& s, const StepArgs& a, cudaStream_
                       Profiler& prof);
 void launch_step_mixed(int dim, const DevState& s, const StepArgs& a, cudaStream_t st,
                        Profiler& prof);
+// The persistent form of the mixed USL step (FLIP or PIC, tensor-product
+// grid): one cooperative launch runs `nsteps` whole steps, the passes of
+// which are separated by grid barriers.  a.g is ignored: the gravity of step
+// k is the ramp of step0 + k applied to `gravity` (mpm_explicit.tcc:145-153).
+// `barrier` holds two words of device memory.  Returns the launch's error.
+struct PersistentArgs {
+  int64_t nsteps;
+  int64_t step0;
+  double gravity[3];
+  double ramp;  // gravity ramping time (0: none)
+  unsigned* barrier;
+};
+cudaError_t launch_steps_persistent_mixed(int dim, const DevState& s, const StepArgs& a,
+                                          const PersistentArgs& q, cudaStream_t st);
 // shared by both paths: the per-step counting sort and the exhaustive locate
 void counting_sort(const DevState& s, cudaStream_t st);
 void launch_locate_fallback(int dim, const DevState& s, int remove_lost, cudaStream_t st);

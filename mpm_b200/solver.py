@@ -156,6 +156,12 @@ class Solver:
         self._ck(self.L.mpm_gpu_set_launch_shape(self.h, int(p2g_tile), int(node_threads),
                                                  int(return_blocks_per_sm)))
 
+    def set_persistent(self, steps_per_launch):
+        """Advance up to ``steps_per_launch`` whole steps per persistent
+        (cooperative) kernel launch; 0 returns to one launch per pass,
+        replayed from a CUDA graph.  Bit for bit the same results."""
+        self._ck(self.L.mpm_gpu_set_persistent(self.h, int(steps_per_launch)))
+
     def launch_shape(self):
         """(p2g_tile, node_threads, return_blocks_per_sm) in use."""
         out = (C.c_int32 * 3)()
