@@ -907,7 +907,7 @@ __global__ void __launch_bounds__(STAGE_T, MPM_G2P_MIN_BLOCKS)
       }
     }
   }
-  if (t == 0) bulk::store_wait_all();
+  if (t == 0) bulk::store_wait_read();
 }
 
 // MUSL particle kinematics (particle.tcc:994-1067 as in k_g2p): the new

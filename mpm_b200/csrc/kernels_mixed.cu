@@ -950,7 +950,9 @@ constexpr size_t mixed_staged_smem_bytes(bool mc) {
 // One block of MSTAGE_T particles (block index bx) with the staging buffers
 // smem, the two initialised copy barriers bar in the phase of the given
 // parity, and the block's timed-out flag.
-template <int DIM, bool FLIP, bool BOX>
+// WRITES_DONE: wait for the block's stores to complete (a later pass of the
+// same launch reads them), else only until they have read shared memory.
+template <int DIM, bool FLIP, bool BOX, bool WRITES_DONE = false>
 __device__ __forceinline__ void g2p_staged_block_mixed(const DevState& s, double dt, float beta,
                                                        int64_t bx, unsigned char* smem, uint64_t* bar,
                                                        unsigned parity, int& timed_out) {
@@ -1092,7 +1094,12 @@ __device__ __forceinline__ void g2p_staged_block_mixed(const DevState& s, double
       }
     }
   }
-  if (t == 0) bulk::store_wait_all();
+  if (t == 0) {
+    if constexpr (WRITES_DONE)
+      bulk::store_wait_all();
+    else
+      bulk::store_wait_read();
+  }
 }
 
 template <int DIM, bool FLIP, bool BOX>
@@ -1294,7 +1301,8 @@ __global__ void __launch_bounds__(MSTAGE_T, DIM == 2 ? MPM_PERSISTENT_MIN_BLOCKS
     if (!grid_barrier(s, q.barrier, G, gen, go)) return;
     // G2P with the stress update; the counts are free once the nodes are done
     for (int64_t b = blockIdx.x; b < pblocks; b += G) {
-      g2p_staged_block_mixed<DIM, FLIP, true>(s, a.dt, (float)a.beta, b, smem, bar, parity, timed_out);
+      g2p_staged_block_mixed<DIM, FLIP, true, true>(s, a.dt, (float)a.beta, b, smem, bar, parity,
+                                                    timed_out);
       parity ^= 1u;
       __syncthreads();  // the block's staging buffers are free again
     }

@@ -93,5 +93,16 @@ __device__ __forceinline__ void store_wait_all() {
   asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
+// wait until every committed store has read its shared-memory source: enough
+// before a block exits (its shared memory may then be reused), since the
+// writes complete before the kernel does
+__device__ __forceinline__ void store_wait_read() {
+#ifdef MPM_BULK_STORE_FULL_WAIT
+  store_wait_all();
+#else
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+#endif
+}
+
 }  // namespace bulk
 }  // namespace mpm_b200
