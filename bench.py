@@ -14,15 +14,16 @@ the solver's stream, state resident in HBM) for the chosen precision (mixed by
 default); ``fp64`` holds the FP64 path timed on the same workload and steps and
 the mixed path's per-field deviation from it; ``accuracy`` gives that deviation
 at fixed step counts (50, 500, 2000 by default) beside the FP64 path's own
-one-ulp floor, and ``late`` a second timed window after them; ``e2e`` goes
-through the public API with host arrays (load -> K steps -> read back);
+one-ulp floor, and ``late`` a second timed window after them; ``persistent``
+times the one-launch persistent form of the same step; ``e2e`` goes through the
+public API with page-locked host arrays (load -> K steps -> read back);
 ``roofline`` reports the dominant kernel's algorithmic bytes per launch over its
 event-timed average duration, and ``roofline.step`` the whole step's bytes per
 particle-step times the throughput; ``cpu_baseline`` times the CPU oracle on a
 bounded sample.
-Under torchrun (N>1) every rank runs an independent replica ("replicas
-only": the multi-GPU slab decomposition is not built), timing is the max over
-ranks.
+Under torchrun (N>1) every rank runs an independent replica (weak scaling; one
+run cut into slabs over several GPUs is mpm_b200.slab, not timed here), timing
+is the max over ranks.
 """
 import argparse
 import json
@@ -663,19 +664,32 @@ def main():
         persistent = time_persistent(prob, args, world, dev)
         persistent["graph_over_persistent"] = (ms / args.steps) / persistent["ms_per_step"]
 
-    # end to end through the public API with host arrays
-    st = state
-    h2d = sum(np.asarray(st[k]).nbytes for k in ("x", "u", "v", "stress", "strain", "F", "volume",
-                                                 "mass", "density", "cell", "material", "svars"))
+    # end to end through the public API with the state in page-locked host
+    # arrays (the library's pinned_empty; pageable arrays if the host cannot
+    # pin them): load, K steps, read back into host arrays
+    from mpm_b200 import MPMError
+    try:
+        st, outb, host_mem = s.state_buffers(pinned=True), s.state_buffers(pinned=True), "page-locked"
+    except MPMError:
+        st, outb, host_mem = s.state_buffers(), s.state_buffers(), "pageable"
+    for k in st:
+        if k in ("x", "u", "v"):
+            st[k][:] = 0.0
+            st[k][:, :prob.dim] = state[k]
+        else:
+            st[k][...] = state[k]
+    h2d = sum(np.asarray(st[k]).nbytes for k in st)
     barrier(world)
     t1 = time.perf_counter()
     s.load(st)
     s.step(args.steps)
-    out = s.read()
+    out = s.read(out=outb)
     e2e_s = max_over_ranks(time.perf_counter() - t1, world)
-    d2h = sum(np.asarray(out[k]).nbytes for k in out)
+    d2h = sum(np.asarray(outb[k]).nbytes for k in outb)
     e2e = {"value": world * n * args.steps / e2e_s, "unit": "particle-steps/s",
-           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+           "host_memory": host_mem}
+    del out
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()

@@ -184,8 +184,18 @@ int mpm_gpu_assign_particle_stresses(mpm_gpu_t h, int64_t n, const double* stres
 int mpm_gpu_add_particle_velocity_constraint(mpm_gpu_t h, int64_t n, const int64_t* pids,
                                              int32_t dir, double velocity);
 
-/* Replace the full particle state (e.g. restart from a checkpoint). */
+/* Replace the full particle state (e.g. restart from a checkpoint).  Arrays in
+ * page-locked host memory (mpm_gpu_host_alloc, cudaHostAlloc or
+ * cudaHostRegister; each array inside one such allocation) are copied by the
+ * DMA engine directly; pageable arrays go through the library's own pinned
+ * staging buffer, gathered on all host threads. */
 int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* p);
+
+/* Page-locked host memory for particle arrays that are loaded and read often
+ * (no counterpart in the reference): *ptr receives `bytes` bytes, NULL with
+ * MPM_ERR_ALLOC when the host cannot pin them; free with mpm_gpu_host_free. */
+int mpm_gpu_host_alloc(size_t bytes, void** ptr);
+int mpm_gpu_host_free(void* ptr);
 
 /* Advance nsteps explicit steps (mpm_explicit.tcc:112-190). */
 int mpm_gpu_step(mpm_gpu_t h, int64_t nsteps);
@@ -237,6 +247,8 @@ int64_t mpm_gpu_launch_count(mpm_gpu_t h);
 
 int64_t mpm_gpu_nparticles(mpm_gpu_t h);
 int64_t mpm_gpu_current_step(mpm_gpu_t h);
+/* The particle state into the caller's arrays (those given); page-locked ones
+ * are written by the DMA engine directly, as in mpm_gpu_load_particles. */
 int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out);
 
 /* Particle output and checkpoint records.  Particle::pod (particle.tcc:180-306)

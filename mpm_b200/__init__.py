@@ -6,6 +6,6 @@ the C ABI of include/mpm_gpu.h; this package is the Python host side.
 """
 from ._native import MPMError, lib  # noqa: F401
 from .problems import Problem, build_solver  # noqa: F401
-from .solver import Solver, material_stress_batch  # noqa: F401
+from .solver import Solver, material_stress_batch, pinned_empty  # noqa: F401
 
-__all__ = ["Solver", "MPMError", "Problem", "build_solver", "material_stress_batch", "lib"]
+__all__ = ["Solver", "MPMError", "Problem", "build_solver", "material_stress_batch", "pinned_empty", "lib"]

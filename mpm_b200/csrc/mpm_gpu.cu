@@ -339,7 +339,7 @@ struct mpm_gpu_solver {
   int64_t npad = 0;
   std::vector<double> p_coords;         // np*dim (creation)
   std::vector<uint16_t> p_mat;
-  std::vector<std::map<unsigned, double>> p_vc;  // per particle velocity constraints
+  std::map<int64_t, std::map<unsigned, double>> p_vc;  // velocity constraints of constrained particles
   bool p_vc_dirty = false;
 
   // device
@@ -834,10 +834,11 @@ void upload_pvc(mpm_gpu_t h) {
   std::vector<int16_t> idx(h->npad, -1);
   std::vector<ParticleVC> table;
   std::map<std::string, int> dedup;
-  for (int64_t p = 0; p < h->np; ++p) {
-    if (p >= (int64_t)h->p_vc.size() || h->p_vc[p].empty()) continue;
+  for (const auto& pc : h->p_vc) {
+    const int64_t p = pc.first;
+    if (p >= h->np || pc.second.empty()) continue;
     ParticleVC r{};
-    for (auto& c : h->p_vc[p]) {
+    for (auto& c : pc.second) {
       r.mask |= 1u << c.first;
       r.value[c.first] = c.second;
     }
@@ -1194,6 +1195,27 @@ void rows_range(P* const (&ptr)[10], const int64_t (&off)[10], int64_t np, int64
   }
 }
 
+// True when each given array lies in page-locked host memory (its first and
+// last byte), so the DMA engine can copy it without staging.
+template <class P>
+bool page_locked(P* const (&ptr)[10], int64_t np) {
+  bool any = false;
+  for (int k = 0; k < 10; ++k) {
+    if (!ptr[k] || np == 0) continue;
+    const char* a = reinterpret_cast<const char*>(ptr[k]);
+    for (const char* q : {a, a + sizeof(double) * row_width(k) * np - 1}) {
+      cudaPointerAttributes attr{};
+      if (cudaPointerGetAttributes(&attr, q) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+      if (attr.type != cudaMemoryTypeHost) return false;
+    }
+    any = true;
+  }
+  return any;
+}
+
 void ensure_stage_events(mpm_gpu_t h) {
   for (auto& e : h->stage_ev)
     if (!e) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
@@ -1236,7 +1258,13 @@ void load_rows_device(mpm_gpu_t h, const mpm_gpu_particles* in) {
   const RowStage r = stage_rows(h, np, ptr, total);
   const int64_t off[10] = {r.x, r.u, r.v, r.stress, r.strain, r.F, r.volume, r.mass, r.density, r.svars};
   const int64_t chunk = std::min(total, ROW_CHUNK);
-  if (double* pin = total ? pinned_rows(h, 2 * chunk) : nullptr) {
+  const bool direct = page_locked(ptr, np);
+  if (direct) {
+    for (int k = 0; k < 10; ++k)
+      if (ptr[k] && np)
+        ck(cudaMemcpyAsync(r.base + off[k], ptr[k], sizeof(double) * row_width(k) * np,
+                           cudaMemcpyHostToDevice, h->stream), "H2D");
+  } else if (double* pin = total ? pinned_rows(h, 2 * chunk) : nullptr) {
     ensure_stage_events(h);
     bool busy[2] = {false, false};
     int k = 0;
@@ -1282,6 +1310,25 @@ MaterialParams material_from_json(int dim, const char* type, const char* json_pr
 extern "C" {
 
 const char* mpm_gpu_version(void) { return MPM_VERSION; }
+
+int mpm_gpu_host_alloc(size_t bytes, void** ptr) {
+  if (!ptr) return MPM_ERR_INVALID;
+  *ptr = nullptr;
+  if (cudaHostAlloc(ptr, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    return MPM_ERR_ALLOC;
+  }
+  return MPM_OK;
+}
+
+int mpm_gpu_host_free(void* ptr) {
+  if (ptr && cudaFreeHost(ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return MPM_ERR_CUDA;
+  }
+  return MPM_OK;
+}
 
 int mpm_gpu_create(const mpm_gpu_config* cfg, mpm_gpu_t* out) {
   if (!cfg || !out) return MPM_ERR_INVALID;
@@ -1586,7 +1633,6 @@ int mpm_gpu_initialise(mpm_gpu_t h) {
     mass[p] = vol[p] * rho[p];
   }
   allocate_particles(h);
-  if (h->p_vc.size() < (size_t)np) h->p_vc.resize(np);
   upload_pvc(h);
   mpm_gpu_particles in{};
   in.volume = vol.data();
@@ -1635,7 +1681,6 @@ int mpm_gpu_add_particle_velocity_constraint(mpm_gpu_t h, int64_t n, const int64
                                              int32_t dir, double velocity) {
   MPM_GUARD(h)
   if (dir < 0 || dir >= h->dim) throw InvalidArg("Invalid direction of velocity constraint");
-  if (h->p_vc.size() < (size_t)h->np) h->p_vc.resize(h->np);
   if (n < 0) {
     for (int64_t p = 0; p < h->np; ++p) h->p_vc[p][(unsigned)dir] = velocity;
   } else {
@@ -1660,7 +1705,9 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
     throw InvalidArg("load_particles needs x, volume, cell and material");
   ck(cudaSetDevice(h->cfg.device), "cudaSetDevice");
   h->set_np(n);
-  h->p_coords.assign(n * h->dim, 0.);
+  h->p_coords.resize(n * h->dim);
+  double* pc = h->p_coords.data();
+  parallel_for(n * h->dim, [&](int64_t a, int64_t b) { std::fill(pc + a, pc + b, 0.); });
   h->p_mat.resize(n);
   parallel_for(n, [&](int64_t a, int64_t b) {
     for (int64_t p = a; p < b; ++p) {
@@ -1669,7 +1716,7 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
       h->p_mat[p] = (uint16_t)it->second;
     }
   });
-  h->p_vc.assign(n, {});
+  h->p_vc.clear();
   h->ntangent = 0;  // a new state has no tangents
   if ((int64_t)h->p_id.size() != n) {
     h->p_id.resize(n);
@@ -2056,7 +2103,13 @@ int mpm_gpu_read_particles(mpm_gpu_t h, mpm_gpu_particles* out) {
   ck(cudaGetLastError(), "state to rows");
   const int64_t off[10] = {r.x, r.u, r.v, r.stress, r.strain, r.F, r.volume, r.mass, r.density, r.svars};
   const int64_t chunk = std::min(total, ROW_CHUNK);
-  if (double* pin = total ? pinned_rows(h, 2 * chunk) : nullptr) {
+  if (page_locked(ptr, np)) {
+    for (int k = 0; k < 10; ++k)
+      if (ptr[k] && np)
+        ck(cudaMemcpyAsync(ptr[k], r.base + off[k], sizeof(double) * row_width(k) * np,
+                           cudaMemcpyDeviceToHost, h->stream), "D2H");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+  } else if (double* pin = total ? pinned_rows(h, 2 * chunk) : nullptr) {
     ensure_stage_events(h);
     const int64_t nchunks = (total + chunk - 1) / chunk;
     auto fetch = [&](int64_t c) {  // DMA of chunk c into half c % 2

@@ -33,6 +33,22 @@ def _i32p(a):
     return a.ctypes.data_as(C.POINTER(C.c_int32))
 
 
+def pinned_empty(shape, dtype=np.float64):
+    """An uninitialised numpy array in page-locked host memory
+    (mpm_gpu_host_alloc), freed when the array and its views are gone.
+    Solver.load and Solver.read copy such arrays by DMA directly."""
+    import weakref
+    L = _native.lib()
+    nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+    ptr = C.c_void_p()
+    rc = L.mpm_gpu_host_alloc(max(nbytes, 1), C.byref(ptr))
+    if rc != 0:
+        raise MPMError(rc, "mpm_gpu_host_alloc: cannot pin %d bytes" % nbytes)
+    buf = (C.c_char * max(nbytes, 1)).from_address(ptr.value)
+    weakref.finalize(buf, L.mpm_gpu_host_free, C.c_void_p(ptr.value))
+    return np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+
 class Solver:
     """Thin owner of one ``mpm_gpu_t`` handle."""
 
@@ -212,18 +228,34 @@ class Solver:
         "isoparametric" flag; before the particles are added)."""
         self._ck(self.L.mpm_gpu_set_isoparametric(self.h, 1 if on else 0))
 
-    def read(self):
-        """Particle state as numpy arrays (rows = particles)."""
+    def state_buffers(self, pinned=False):
+        """Empty arrays for ``read(out=...)`` and ``load``: x, u, v as (n, 3)
+        rows, in page-locked memory with ``pinned`` (see pinned_empty)."""
         n = self.nparticles
-        out = {"x": np.zeros((n, 3)), "u": np.zeros((n, 3)), "v": np.zeros((n, 3)),
-               "stress": np.zeros((n, 6)), "strain": np.zeros((n, 6)), "F": np.zeros((n, 9)),
-               "volume": np.zeros(n), "mass": np.zeros(n), "density": np.zeros(n),
-               "cell": np.zeros(n, dtype=np.int64), "material": np.zeros(n, dtype=np.int32),
-               "svars": np.zeros((n, 9))}
+        new = pinned_empty if pinned else (lambda shape, dtype=np.float64: np.zeros(shape, dtype))
+        return {"x": new((n, 3)), "u": new((n, 3)), "v": new((n, 3)), "stress": new((n, 6)),
+                "strain": new((n, 6)), "F": new((n, 9)), "volume": new((n,)), "mass": new((n,)),
+                "density": new((n,)), "cell": new((n,), np.int64), "material": new((n,), np.int32),
+                "svars": new((n, 9))}
+
+    def read(self, out=None):
+        """Particle state as numpy arrays (rows = particles); with ``out`` (the
+        arrays of ``state_buffers``) the state is written into them."""
+        n = self.nparticles
+        if out is None:
+            out = self.state_buffers()
+        else:
+            out = dict(out)
         P = _native.Particles()
-        for k, a in out.items():
-            if a.dtype == np.float64:
-                setattr(P, k, _dp(a))
+        for k, w in (("stress", 6), ("strain", 6), ("F", 9), ("volume", 0), ("mass", 0),
+                     ("density", 0), ("svars", 9), ("x", 3), ("u", 3), ("v", 3)):
+            a = out[k]
+            if a.shape != ((n, w) if w else (n,)) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("read: %s must be a C-contiguous float64 array of %s rows" % (k, w or 1))
+            setattr(P, k, _dp(a))
+        for k, t in (("cell", np.int64), ("material", np.int32)):
+            if out[k].shape != (n,) or out[k].dtype != t or not out[k].flags.c_contiguous:
+                raise ValueError("read: %s must be a C-contiguous %s array" % (k, np.dtype(t).name))
         P.cell = _i64p(out["cell"])
         P.material = _i32p(out["material"])
         self._ck(self.L.mpm_gpu_read_particles(self.h, C.byref(P)))

@@ -141,3 +141,29 @@ def test_state_larger_than_one_copy_chunk(precision):
     Pt.density = density.ctypes.data_as(C.POINTER(C.c_double))
     assert s.L.mpm_gpu_read_particles(s.h, C.byref(Pt)) == 0
     assert np.array_equal(svars, back["svars"]) and np.array_equal(density, back["density"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_page_locked_arrays_load_and_read_as_pageable_ones(precision):
+    """Arrays in page-locked memory (pinned_empty) are copied by DMA directly,
+    pageable ones through the staging pipeline: the same state either way,
+    and a read into page-locked arrays equals the plain read."""
+    from mpm_b200 import pinned_empty
+    prob = P.column_3d(shape=(80, 80, 40), block=(40, 40, 40))
+    s = P.build_solver(prob, precision=precision)
+    s.step(3)
+    ref = s.read()
+    pin = s.state_buffers(pinned=True)
+    got = s.read(out=pin)
+    for k in ref:
+        assert np.array_equal(got[k], ref[k]), k
+    s.load(ref)  # the step-3 state from pageable arrays ...
+    s.step(2)
+    after_pageable = s.read()
+    s.load(pin)  # ... and from page-locked ones
+    s.step(2)
+    after_pinned = s.read(out=s.state_buffers(pinned=True))
+    for k in after_pageable:
+        assert np.array_equal(after_pinned[k], after_pageable[k]), k
+    a = pinned_empty((5, 3))
+    assert a.shape == (5, 3) and a.dtype == np.float64
