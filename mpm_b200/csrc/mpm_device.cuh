@@ -482,27 +482,31 @@ __device__ __forceinline__ int locate_near(const DevState& s, const double* x, i
 // ------------------------------------------------------------ counting sort
 // The passes of the per-step counting sort of particles by cell, as bodies
 // that a one-kernel-per-pass launch and the persistent step kernel share.
-// Per-cell counts and each particle's slot within its cell.  The lanes of a
-// warp in the same cell (most of them: particles are stored in cell order)
-// share one atomic; the slot order within a cell is not deterministic either
-// way and P2G sorts every cell's segment.
+// Per-cell counts and each particle's slot within its cell.  Particles are
+// stored mostly in cell order, so the lanes of a warp form runs of equal
+// cells: each run's first lane adds the run's length with one atomic and the
+// others take the following slots.  The slot order within a cell is not
+// deterministic either way, and P2G sorts every cell's segment.  Every lane
+// of the warp takes part (p at or beyond np is an empty lane).  Against one
+// atomic per distinct cell of the warp (__match_any_sync): the 512-slope
+// ensemble's sort 0.180 -> 0.165 ms, the 4M column's unchanged.
 __device__ __forceinline__ void count_particle(const DevState& s, int64_t p) {
   const bool in = p < s.np;
-  const int c = in ? s.cell[p] : -1;
+  const int lane = threadIdx.x & 31;
+  int c = in ? s.cell[p] : -1;
   if (c >= s.ncells) raise_err(s, ERR_BADCELL);
   const bool valid = c >= 0 && c < s.ncells;
-  const unsigned active = __ballot_sync(0xffffffffu, valid);  // every lane of the warp
-  if (!valid) {
-    if (in) s.rank[p] = -1;
-    return;
-  }
-  const unsigned same = __match_any_sync(active, c);
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(same) - 1;
+  if (!valid) c = -1 - lane;  // a run of its own
+  const int prev = __shfl_up_sync(0xffffffffu, c, 1);
+  const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || c != prev);
+  const unsigned upto = lane == 31 ? 0xffffffffu : (2u << lane) - 1u;  // lanes 0..lane
+  const int head = 31 - __clz(heads & upto);
+  const unsigned above = heads & ~upto;
+  const int next = above ? __ffs(above) - 1 : 32;
   int base = 0;
-  if (lane == leader) base = atomicAdd(&s.cnt[c], __popc(same));
-  base = __shfl_sync(same, base, leader);
-  s.rank[p] = base + __popc(same & ((1u << lane) - 1u));
+  if (lane == head && valid) base = atomicAdd(&s.cnt[c], next - head);
+  base = __shfl_sync(0xffffffffu, base, head);
+  if (in) s.rank[p] = valid ? base + (lane - head) : -1;
 }
 
 // The particle's place in the cell-sorted order (start of its cell + rank).
