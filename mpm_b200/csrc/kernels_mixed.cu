@@ -128,8 +128,9 @@ __device__ __forceinline__ void cell_nodes_rel(const DevState& s, int c, int* ni
 // ---------------------------------------------------------------- P2G tiles
 // The FP64 path's cell tiles (k_p2g_tiles) in FP32: staged local coordinates
 // (the FP64 local coordinate rounded), mass, velocity, -V0 (1 + P), stress
-// and, off a tensor-product grid, J^-1; per (cell, slot) thread 1 + 3 DIM
-// FP64 sums of the FP32 contributions of the cell's particles in id order,
+// and, off a tensor-product grid, J^-1; per (cell, slot) thread 1 + 2 DIM
+// FP64 sums (mass, momentum, internal force; the body force is formed by the
+// node update) of the FP32 contributions of the cell's particles in id order,
 // stored as FP32 partials.  AFF: the mass-momentum mapping velocity v + M r of
 // the affine (1: M = B D^-1) or Taylor (2: M = B) updates, with M formed in
 // FP64 by the staging thread and the branch vectors r taken from FP64
@@ -137,7 +138,8 @@ __device__ __forceinline__ void cell_nodes_rel(const DevState& s, int c, int* ni
 template <int DIM, int MODE, bool BOX, int AFF = 0>
 struct MTileRows {
   static constexpr bool MM = MODE != 1, FORCES = MODE != 0;
-  static constexpr int XI = 0, M = DIM, V = DIM + 1;
+  static constexpr int XI = 0, M = DIM;  // the mass row only with mass and momentum
+  static constexpr int V = M + (MM ? 1 : 0);
   static constexpr int SC = V + (MM ? DIM : 0);
   static constexpr int S = SC + 1;
   static constexpr int INV = S + (FORCES ? PF<DIM>::NS : 0);
@@ -158,12 +160,11 @@ constexpr int mixed_tile_min_blocks() {
 // One tile (block-sized group of cells, tile index bx) of the P2G pass; the
 // block's threads are the tile's (cell, slot) pairs.
 template <int DIM, int MODE, bool BOX, int T, int AFF = 0>
-__device__ __forceinline__ void p2g_tile_mixed(const DevState& s, float g0, float g1, float g2,
-                                               int64_t bx) {
+__device__ __forceinline__ void p2g_tile_mixed(const DevState& s, int64_t bx) {
   constexpr int NV = Elem<DIM>::NV;
   constexpr int CB = T / NV;
-  constexpr int NVAL = 1 + 3 * DIM;
-  constexpr int MASS = 0, MOM = 1, FEXT = 1 + DIM, FINT = 1 + 2 * DIM;
+  constexpr int NVAL = mixed_nval(DIM);
+  constexpr int MASS = 0, MOM = 1, FINT = 1 + DIM;
   using RW = MTileRows<DIM, MODE, BOX, AFF>;
   constexpr bool MM = RW::MM, FORCES = RW::FORCES;
   __shared__ float rows[RW::N][T];
@@ -187,7 +188,7 @@ __device__ __forceinline__ void p2g_tile_mixed(const DevState& s, float g0, floa
     xi_f32<DIM, BOX>(s, pc, x, xi);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) rows[RW::XI + d][r] = xi[d];
-    rows[RW::M][r] = pmf<DIM>(s, PM<DIM>::MASS, p);
+    if constexpr (MM) rows[RW::M][r] = pmf<DIM>(s, PM<DIM>::MASS, p);
     if constexpr (MM) {
 #pragma unroll
       for (int d = 0; d < DIM; ++d) rows[RW::V + d][r] = pmf<DIM>(s, PM<DIM>::V + d, p);
@@ -229,7 +230,6 @@ __device__ __forceinline__ void p2g_tile_mixed(const DevState& s, float g0, floa
 #pragma unroll
     for (int d = 0; d < DIM; ++d) xkr[d] = a1 > a0 ? (float)(X[k * DIM + d] - X[d]) : 0.f;
   }
-  const float gv[3] = {g0, g1, g2};
   double acc[NVAL];
 #pragma unroll
   for (int v = 0; v < NVAL; ++v) acc[v] = 0.;
@@ -239,9 +239,8 @@ __device__ __forceinline__ void p2g_tile_mixed(const DevState& s, float g0, floa
 #pragma unroll
     for (int d = 0; d < DIM; ++d) xi[d] = rows[RW::XI + d][r];
     node_shape<DIM>(xi, k, N, G);
-    const float m = rows[RW::M][r];
     if constexpr (MM) {
-      const float mN = m * N;
+      const float mN = rows[RW::M][r] * N;
       acc[MASS] += (double)mN;
       float mv[DIM];
 #pragma unroll
@@ -266,8 +265,6 @@ __device__ __forceinline__ void p2g_tile_mixed(const DevState& s, float g0, floa
       float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
       for (int q = 0; q < PF<DIM>::NS; ++q) sig[q] = rows[RW::S + q][r];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) acc[FEXT + d] += (double)((gv[d] * m) * N);
       float Dn[DIM];
       if constexpr (BOX) {
         box_map.grad(G, Dn);
@@ -304,18 +301,18 @@ __device__ __forceinline__ void p2g_tile_mixed(const DevState& s, float g0, floa
   float* out = s.partials_f + ((int64_t)c * NV + k) * NVAL;
   if constexpr (MM) {
 #pragma unroll
-    for (int v = MASS; v < FEXT; ++v) out[v] = (float)acc[v];
+    for (int v = MASS; v < FINT; ++v) out[v] = (float)acc[v];
   }
   if constexpr (FORCES) {
 #pragma unroll
-    for (int v = FEXT; v < NVAL; ++v) out[v] = (float)acc[v];
+    for (int v = FINT; v < NVAL; ++v) out[v] = (float)acc[v];
   }
 }
 
 template <int DIM, int MODE, bool BOX, int T = p2g_tile_t<BOX>(), int AFF = 0>
 __global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T, AFF>()))
-    k_p2g_tiles_mixed(DevState s, float g0, float g1, float g2) {
-  p2g_tile_mixed<DIM, MODE, BOX, T, AFF>(s, g0, g1, g2, blockIdx.x);
+    k_p2g_tiles_mixed(DevState s) {
+  p2g_tile_mixed<DIM, MODE, BOX, T, AFF>(s, blockIdx.x);
 }
 
 // ---------------------------------------------------------------- node update
@@ -323,7 +320,7 @@ __global__ void __launch_bounds__(T, (mixed_tile_min_blocks<BOX, T, AFF>()))
 template <int DIM, int V0, int NVS>
 __device__ __forceinline__ bool gather_node_mixed(const DevState& s, int64_t node, double* sum) {
   constexpr int NV = Elem<DIM>::NV;
-  constexpr int NVAL = 1 + 3 * DIM;
+  constexpr int NVAL = mixed_nval(DIM);
 #pragma unroll
   for (int v = 0; v < NVS; ++v) sum[v] = 0.;
   bool active = false;
@@ -384,14 +381,17 @@ __device__ __forceinline__ void node_accel_update_d(const DevState& s, double m,
 
 // 8 blocks per SM: 0.111 -> 0.108 ms per 1M-node launch (more warps in flight
 // on the scattered partial loads, despite small spills)
+// The body force of a node is gravity times its mass (particle.tcc:893-898
+// summed over the node's particles: sum_p g m_p N_p = g sum_p m_p N_p), formed
+// here in FP64 from the gathered mass instead of carried in the partials.
 template <int DIM, int MODE>
 __device__ __forceinline__ void node_update_mixed(const DevState& s, double dt, double damping,
-                                                  int64_t n) {
+                                                  const double* g, int64_t n) {
   if (n >= s.nn) return;
-  constexpr int NVAL = 1 + 3 * DIM;
+  constexpr int NVAL = mixed_nval(DIM);
   double sum[NVAL];
   constexpr int V0 = MODE == 2 ? 1 + DIM : 0;
-  constexpr int NVS = MODE == 0 ? 1 + DIM : (MODE == 1 ? NVAL : 2 * DIM);
+  constexpr int NVS = MODE == 0 ? 1 + DIM : (MODE == 1 ? NVAL : DIM);
   if (!gather_node_mixed<DIM, V0, NVS>(s, n, sum)) return;
   const int bci = s.bc_index[n];
   double vel[DIM], acc[DIM];
@@ -405,7 +405,10 @@ __device__ __forceinline__ void node_update_mixed(const DevState& s, double dt, 
       vel[d] = (double)vf[d];
       acc[d] = (double)af[d];
     }
-    node_accel_update_d<DIM>(s, mm[0], &sum[0], &sum[DIM], vel, acc, bci, dt, damping);
+    double fe[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) fe[d] = g[d] * mm[0];
+    node_accel_update_d<DIM>(s, mm[0], fe, &sum[0], vel, acc, bci, dt, damping);
   } else {
     const double m = sum[0];
 #pragma unroll
@@ -418,8 +421,12 @@ __device__ __forceinline__ void node_update_mixed(const DevState& s, double dt, 
         if (fabs(vel[d]) < 1.E-15) vel[d] = 0.;
     }
     if (bci >= 0) apply_velocity_constraints<DIM>(s.bcs[bci], vel, acc);
-    if constexpr (MODE == 1)
-      node_accel_update_d<DIM>(s, m, &sum[1 + DIM], &sum[1 + 2 * DIM], vel, acc, bci, dt, damping);
+    if constexpr (MODE == 1) {
+      double fe[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) fe[d] = g[d] * m;
+      node_accel_update_d<DIM>(s, m, fe, &sum[1 + DIM], vel, acc, bci, dt, damping);
+    }
   }
   float vf[DIM], af[DIM];
 #pragma unroll
@@ -431,8 +438,10 @@ __device__ __forceinline__ void node_update_mixed(const DevState& s, double dt, 
 }
 
 template <int DIM, int MODE>
-__global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, double damping) {
-  node_update_mixed<DIM, MODE>(s, dt, damping, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, double damping, double g0,
+                                                        double g1, double g2) {
+  const double g[3] = {g0, g1, g2};
+  node_update_mixed<DIM, MODE>(s, dt, damping, g, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ------------------------------------------------------- stress and strain
@@ -1271,9 +1280,7 @@ __global__ void __launch_bounds__(MSTAGE_T, DIM == 2 ? MPM_PERSISTENT_MIN_BLOCKS
   for (int64_t k = 0; k < q.nsteps; ++k) {
     double gm = 1.0;  // the host's ramp, the same operations
     if (q.ramp > 0.0) gm = fmin(1.0, static_cast<double>(q.step0 + k) * a.dt / q.ramp);
-    const float g0 = (float)(DIM > 0 ? gm * q.gravity[0] : 0.);
-    const float g1 = (float)(DIM > 1 ? gm * q.gravity[1] : 0.);
-    const float g2 = (float)(DIM > 2 ? gm * q.gravity[2] : 0.);
+    const double g[3] = {gm * q.gravity[0], gm * q.gravity[1], gm * q.gravity[2]};
     // counting sort
     if (blockIdx.x == 0 && t == 0) {
       *s.nlost = 0;
@@ -1293,11 +1300,11 @@ __global__ void __launch_bounds__(MSTAGE_T, DIM == 2 ? MPM_PERSISTENT_MIN_BLOCKS
     if (!grid_barrier(s, q.barrier, G, gen, go)) return;
     // P2G of mass, momentum and forces
     for (int64_t b = blockIdx.x; b < tiles; b += G) {
-      p2g_tile_mixed<DIM, 2, true, T>(s, g0, g1, g2, b);
+      p2g_tile_mixed<DIM, 2, true, T>(s, b);
       __syncthreads();  // the tile's staged rows are consumed
     }
     if (!grid_barrier(s, q.barrier, G, gen, go)) return;
-    for (int64_t b = blockIdx.x; b < nodeblocks; b += G) node_update_mixed<DIM, 1>(s, a.dt, a.damping, b * T + t);
+    for (int64_t b = blockIdx.x; b < nodeblocks; b += G) node_update_mixed<DIM, 1>(s, a.dt, a.damping, g, b * T + t);
     if (!grid_barrier(s, q.barrier, G, gen, go)) return;
     // G2P with the stress update; the counts are free once the nodes are done
     for (int64_t b = blockIdx.x; b < pblocks; b += G) {
@@ -1347,7 +1354,6 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
   if (np == 0) return;
   cudaMemsetAsync(s.nlost, 0, sizeof(unsigned), st);
   if (s.svf) cudaMemsetAsync(s.nplastic, 0, 2 * sizeof(unsigned), st);  // and nplastic_heavy
-  const float g0 = (float)a.g[0], g1 = (float)a.g[1], g2 = (float)a.g[2];
   const unsigned nt = (unsigned)node_block(a);
   const unsigned pb = nblk(np, 128), nb = nblk(nn, nt);
   const unsigned mcap = 148u * (unsigned)return_blocks(a);
@@ -1358,19 +1364,19 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     constexpr int NV = Elem<DIM>::NV;
     if constexpr (MODE != 1) {  // the mass-momentum mapping velocity (128-thread tiles)
       if (a.vupd == 2 || a.vupd == 4) {
-        k_p2g_tiles_mixed<DIM, MODE, BOX, 128, 1><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s, g0, g1, g2);
+        k_p2g_tiles_mixed<DIM, MODE, BOX, 128, 1><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s);
         return;
       }
       if (a.vupd == 3) {
-        k_p2g_tiles_mixed<DIM, MODE, BOX, 128, 2><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s, g0, g1, g2);
+        k_p2g_tiles_mixed<DIM, MODE, BOX, 128, 2><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s);
         return;
       }
     }
     if (BOX && tile_threads(a, BOX) == 128)
-      k_p2g_tiles_mixed<DIM, MODE, BOX, 128><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s, g0, g1, g2);
+      k_p2g_tiles_mixed<DIM, MODE, BOX, 128><<<nblk(s.ncells, 128 / NV), 128, 0, st>>>(s);
     else
       k_p2g_tiles_mixed<DIM, MODE, BOX><<<nblk(s.ncells, p2g_tile_t<BOX>() / NV), p2g_tile_t<BOX>(),
-                                          0, st>>>(s, g0, g1, g2);
+                                          0, st>>>(s);
   };
   // G2P of the mapping-matrix updates (ASFLIP 2, TPIC 3, APIC 4)
   auto g2p_affine = [&](auto stress) {
@@ -1398,7 +1404,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     p2g(std::integral_constant<int, 2>{});
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
-    k_nodes_mixed<DIM, 1><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
+    k_nodes_mixed<DIM, 1><<<nb, nt, 0, st>>>(s, a.dt, a.damping, a.g[0], a.g[1], a.g[2]);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
     if (a.flip)
@@ -1412,7 +1418,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     p2g(std::integral_constant<int, 0>{});
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
-    k_nodes_mixed<DIM, 0><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
+    k_nodes_mixed<DIM, 0><<<nb, nt, 0, st>>>(s, a.dt, a.damping, a.g[0], a.g[1], a.g[2]);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_STRESS, st);
     k_stress_mixed<DIM, BOX><<<pb, 128, 0, st>>>(s, (float)a.dt);
@@ -1428,7 +1434,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     if (a.phase == 1) return;
   usl_second_half:
     pr.begin(K_NODES_VEL, st);
-    k_nodes_mixed<DIM, 1><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
+    k_nodes_mixed<DIM, 1><<<nb, nt, 0, st>>>(s, a.dt, a.damping, a.g[0], a.g[1], a.g[2]);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_G2P, st);
     const size_t sm = mixed_staged_smem_bytes<DIM>(s.svf != nullptr);
@@ -1448,7 +1454,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     p2g(std::integral_constant<int, 0>{});
     pr.end(K_P2G, st);
     pr.begin(K_NODES_VEL, st);
-    k_nodes_mixed<DIM, 0><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
+    k_nodes_mixed<DIM, 0><<<nb, nt, 0, st>>>(s, a.dt, a.damping, a.g[0], a.g[1], a.g[2]);
     pr.end(K_NODES_VEL, st);
     pr.begin(K_STRESS, st);
     k_stress_mixed<DIM, BOX><<<pb, 128, 0, st>>>(s, (float)a.dt);
@@ -1458,7 +1464,7 @@ void step_mixed(const DevState& s, const StepArgs& a, cudaStream_t st, Profiler&
     p2g(std::integral_constant<int, 1>{});
     pr.end(K_P2G_FORCES, st);
     pr.begin(K_NODES_ACC, st);
-    k_nodes_mixed<DIM, 2><<<nb, nt, 0, st>>>(s, a.dt, a.damping);
+    k_nodes_mixed<DIM, 2><<<nb, nt, 0, st>>>(s, a.dt, a.damping, a.g[0], a.g[1], a.g[2]);
     pr.end(K_NODES_ACC, st);
     pr.begin(K_G2P, st);
     if (a.vupd >= 2)

@@ -770,11 +770,10 @@ void upload_mesh(mpm_gpu_t h) {
     h->d_nc_slot.alloc(std::max<size_t>(1, h->nc_slot.size()));
     h->d_nc_slot.upload(h->nc_slot.data(), h->nc_slot.size(), st);
   }
-  const int nval = 1 + 3 * dim;
   if (h->mixed)
-    h->d_partials_f.alloc((size_t)h->ncells * h->nv * nval);
+    h->d_partials_f.alloc((size_t)h->ncells * h->nv * mixed_nval(dim));
   else
-    h->d_partials.alloc((size_t)h->ncells * h->nv * nval);
+    h->d_partials.alloc((size_t)h->ncells * h->nv * (1 + 3 * dim));
   h->d_cnt.alloc(h->ncells);
   h->d_start.alloc(h->ncells + 1);
   const int64_t nb = (h->ncells + SCAN_BLOCK - 1) / SCAN_BLOCK;
@@ -3073,7 +3072,7 @@ StepArgs slab_step_args(mpm_gpu_t h, int phase) {
 }
 
 int64_t halo_cols(mpm_gpu_t h) { return (int64_t)h->gcells[1] * (h->dim == 3 ? h->gcells[2] : 1); }
-int halo_nvals(mpm_gpu_t h) { return h->nv * (1 + 3 * h->dim); }
+int halo_nvals(mpm_gpu_t h) { return h->nv * (h->mixed ? mixed_nval(h->dim) : 1 + 3 * h->dim); }
 
 }  // namespace
 

@@ -63,6 +63,10 @@ struct NF {
 // nfv_stride floats, 16-byte aligned, so that a particle kernel gathers a node
 // with one (2D: v0 v1 a0 a1) or two (3D: v0 v1 v2 a0 | a1 a2 - -) 16-byte loads.
 constexpr int nfv_stride(int dim) { return dim == 3 ? 8 : 4; }
+// Values of a mixed-precision cell-slot partial row: mass, momentum (DIM) and
+// internal force (DIM); the body force is gravity times the nodal mass, formed
+// by the node update.  (The FP64 rows also carry the body force, 1 + 3 DIM.)
+constexpr int mixed_nval(int dim) { return 1 + 2 * dim; }
 
 // particle velocity constraint record: mask bit d => v[d] = value[d]
 struct ParticleVC {
