@@ -299,14 +299,15 @@ __device__ __forceinline__ void p2g_tile_mixed(const DevState& s, int64_t bx) {
   }
   if (!mine || a1 == a0) return;  // empty cells keep no partials
   float* out = s.partials_f + ((int64_t)c * NV + k) * NVAL;
-  if constexpr (MM) {
+  float row[NVAL];  // the padding stays zero
 #pragma unroll
-    for (int v = MASS; v < FINT; ++v) out[v] = (float)acc[v];
-  }
-  if constexpr (FORCES) {
-#pragma unroll
-    for (int v = FINT; v < NVAL; ++v) out[v] = (float)acc[v];
-  }
+  for (int v = 0; v < NVAL; ++v) row[v] = (float)acc[v];
+  if constexpr (MM && FORCES)
+    store_partial_row<NVAL, 0, NVAL>(out, row);
+  else if constexpr (MM)
+    store_partial_row<NVAL, MASS, FINT>(out, row);
+  else
+    store_partial_row<NVAL, FINT, NVAL - FINT>(out, row + FINT);
 }
 
 template <int DIM, int MODE, bool BOX, int T = p2g_tile_t<BOX>(), int AFF = 0>
@@ -390,8 +391,8 @@ __device__ __forceinline__ void node_update_mixed(const DevState& s, double dt, 
   if (n >= s.nn) return;
   constexpr int NVAL = mixed_nval(DIM);
   double sum[NVAL];
-  constexpr int V0 = MODE == 2 ? 1 + DIM : 0;
-  constexpr int NVS = MODE == 0 ? 1 + DIM : (MODE == 1 ? NVAL : DIM);
+  constexpr int V0 = MODE == 2 ? 1 + DIM : 0;  // MODE 2: the internal force and the padding
+  constexpr int NVS = MODE == 0 ? 1 + DIM : (MODE == 1 ? NVAL : NVAL - (1 + DIM));
   if (!gather_node_mixed<DIM, V0, NVS>(s, n, sum)) return;
   const int bci = s.bc_index[n];
   double vel[DIM], acc[DIM];

@@ -60,11 +60,22 @@ __device__ __forceinline__ unsigned list_slot(const DevState& s, unsigned t, uns
 }
 
 // Values V0 .. V0 + NVS - 1 of one cell-slot partial row of NVAL values:
-// pairs loaded as one 8- or 16-byte access when the row length and the first
-// value are even (rows then start on a multiple of two values).
+// FP32 quadruples as one 16-byte access when the row length, the first value
+// and the count are multiples of four; pairs as one 8- or 16-byte access when
+// they are even (rows then start on a multiple of two values).
 template <typename T, int NVAL, int V0, int NVS>
 __device__ __forceinline__ void load_partial_row(const T* row, T* out) {
-  if constexpr (NVAL % 2 == 0 && V0 % 2 == 0 && NVS % 2 == 0) {
+  if constexpr (sizeof(T) == 4 && NVAL % 4 == 0 && V0 % 4 == 0 && NVS % 4 == 0) {
+    const float4* r4 = reinterpret_cast<const float4*>(row + V0);
+#pragma unroll
+    for (int k = 0; k < NVS / 4; ++k) {
+      const float4 v = r4[k];
+      out[4 * k] = v.x;
+      out[4 * k + 1] = v.y;
+      out[4 * k + 2] = v.z;
+      out[4 * k + 3] = v.w;
+    }
+  } else if constexpr (NVAL % 2 == 0 && V0 % 2 == 0 && NVS % 2 == 0) {
     using T2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
     const T2* r2 = reinterpret_cast<const T2*>(row + V0);
 #pragma unroll
@@ -76,6 +87,24 @@ __device__ __forceinline__ void load_partial_row(const T* row, T* out) {
   } else {
 #pragma unroll
     for (int v = 0; v < NVS; ++v) out[v] = row[V0 + v];
+  }
+}
+
+// Values V0 .. V0 + NVS - 1 of an FP32 partial row of NVAL values stored with
+// the widest accesses load_partial_row would read them with.
+template <int NVAL, int V0, int NVS>
+__device__ __forceinline__ void store_partial_row(float* row, const float* in) {
+  if constexpr (NVAL % 4 == 0 && V0 % 4 == 0 && NVS % 4 == 0) {
+    float4* r4 = reinterpret_cast<float4*>(row + V0);
+#pragma unroll
+    for (int k = 0; k < NVS / 4; ++k) r4[k] = make_float4(in[4 * k], in[4 * k + 1], in[4 * k + 2], in[4 * k + 3]);
+  } else if constexpr (NVAL % 2 == 0 && V0 % 2 == 0 && NVS % 2 == 0) {
+    float2* r2 = reinterpret_cast<float2*>(row + V0);
+#pragma unroll
+    for (int k = 0; k < NVS / 2; ++k) r2[k] = make_float2(in[2 * k], in[2 * k + 1]);
+  } else {
+#pragma unroll
+    for (int v = 0; v < NVS; ++v) row[V0 + v] = in[v];
   }
 }
 

@@ -64,9 +64,10 @@ struct NF {
 // with one (2D: v0 v1 a0 a1) or two (3D: v0 v1 v2 a0 | a1 a2 - -) 16-byte loads.
 constexpr int nfv_stride(int dim) { return dim == 3 ? 8 : 4; }
 // Values of a mixed-precision cell-slot partial row: mass, momentum (DIM) and
-// internal force (DIM); the body force is gravity times the nodal mass, formed
-// by the node update.  (The FP64 rows also carry the body force, 1 + 3 DIM.)
-constexpr int mixed_nval(int dim) { return 1 + 2 * dim; }
+// internal force (DIM) -- the body force is gravity times the nodal mass,
+// formed by the node update (the FP64 rows also carry it, 1 + 3 DIM) -- padded
+// to 8 (3D) or 6 (2D) floats, so that a row moves in 16- or 8-byte accesses.
+constexpr int mixed_nval(int dim) { return dim == 3 ? 8 : 6; }
 
 // particle velocity constraint record: mask bit d => v[d] = value[d]
 struct ParticleVC {
