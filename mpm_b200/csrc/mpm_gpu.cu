@@ -1863,7 +1863,7 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
   if (words[1] & ERR_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite particle position");
   if (words[1] & ERR_OUTSIDE) return fail(h, MPM_ERR_OUTSIDE, "Particle(s) outside the mesh domain");
   if (words[1] & ERR_BADCELL) return fail(h, MPM_ERR_INVALID, "corrupt particle cell index");
-  if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded wait on a device copy ran out");
+  if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded device wait (copy, scan or grid barrier) ran out");
   MPM_END(h)
   return MPM_OK;
 }
@@ -2878,7 +2878,7 @@ int mpm_gpu_adjoint_reverse(mpm_gpu_t h, const double* dL_dx, const double* dL_d
   ck(cudaStreamSynchronize(h->stream), "adjoint");
   h->prof.collect();
   if (words[1] & ERR_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite state in the recomputed run");
-  if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded wait on a device copy ran out");
+  if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded device wait (copy, scan or grid barrier) ran out");
   for (int q = 0; q < t.nparams; ++q) {  // particle order: a fixed summation order
     double sum = 0.0;
     for (int64_t p = 0; p < n; ++p) sum += theta[(size_t)q * np + p];
@@ -3115,7 +3115,7 @@ int mpm_gpu_step_end(mpm_gpu_t h) {
   if (words[1] & ERR_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite particle position");
   if (words[1] & ERR_OUTSIDE) return fail(h, MPM_ERR_OUTSIDE, "Particle(s) outside the mesh domain");
   if (words[1] & ERR_BADCELL) return fail(h, MPM_ERR_INVALID, "corrupt particle cell index");
-  if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded wait on a device copy ran out");
+  if (words[1] & ERR_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded device wait (copy, scan or grid barrier) ran out");
   MPM_END(h)
   return MPM_OK;
 }

@@ -80,7 +80,7 @@ enum ErrorBits : unsigned {
   ERR_OUTSIDE = 1u,     // a particle left the mesh (locate_particles on)
   ERR_NONFINITE = 2u,   // NaN or Inf in a particle position
   ERR_BADCELL = 4u,     // corrupt cell index found by a bounds check
-  ERR_TIMEOUT = 8u      // a bounded wait on a copy ran out
+  ERR_TIMEOUT = 8u      // a bounded wait (copy, scan chain, grid barrier) ran out
 };
 
 struct DevState {
