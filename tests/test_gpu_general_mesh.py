@@ -88,19 +88,25 @@ def test_renumbered_mesh_matches_the_grid_run():
 
 @pytest.mark.parametrize("mesh", ["renumbered", "distorted"])
 def test_mixed_precision_on_general_mesh(mesh):
-    """The mixed-precision kernels' general-mesh path: within 1e-5 of FP64."""
+    """The mixed-precision kernels' general-mesh path against FP64 over 50
+    steps: within 1e-5 plus twice the spread of FP64 runs whose initial states
+    differ by FP32 rounding (the bar of the cohesionless column in
+    test_gpu_mixed).  Most points of these columns return on the tension
+    branch; near the floor those returns turn the FP32 rounding of the initial
+    state alone into a 3e-6 velocity difference on the renumbered mesh, and
+    the mixed path's largest errors (1e-5) sit on the same points."""
+    from tests.test_gpu_mixed import _run
+
     def make():
         prob = small_column_3d(scheme="usl", dt=1e-5, c=2000., psi=5.)
         return renumber_nodes(prob) if mesh == "renumbered" else distort_interior(prob)
 
-    out = {}
-    for prec in ("fp64", "mixed"):
-        s = P.build_solver(make(), precision=prec)
-        s.step(50)
-        out[prec] = s.read()
-    assert np.array_equal(out["mixed"]["cell"], out["fp64"]["cell"])
-    errs = field_errors(out["mixed"], out["fp64"], ("u", "v", "stress", "strain"))
-    assert all(v <= 1e-5 for v in errs.values()), errs
+    f, m, fl = _run(make(), 50, "fp64"), _run(make(), 50, "mixed"), _run(make(), 50, "fp64", floor=True)
+    assert np.array_equal(m["cell"], f["cell"])
+    fields = ("u", "v", "stress", "strain")
+    em, ef = field_errors(m, f, fields), field_errors(fl, f, fields)
+    for k in fields:
+        assert em[k] <= 2 * ef[k] + 1e-5, (k, em[k], ef[k])
 
 
 @pytest.mark.parametrize("scheme", ["usf", "usl"])
