@@ -1313,7 +1313,7 @@ const char* mpm_gpu_version(void) { return MPM_VERSION; }
 int mpm_gpu_host_alloc(size_t bytes, void** ptr) {
   if (!ptr) return MPM_ERR_INVALID;
   *ptr = nullptr;
-  if (cudaHostAlloc(ptr, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+  if (cudaHostAlloc(ptr, bytes ? bytes : 1, cudaHostAllocPortable) != cudaSuccess) {  // every device's context
     cudaGetLastError();
     *ptr = nullptr;
     return MPM_ERR_ALLOC;
@@ -1709,10 +1709,17 @@ int mpm_gpu_load_particles(mpm_gpu_t h, int64_t n, const mpm_gpu_particles* in) 
   parallel_for(n * h->dim, [&](int64_t a, int64_t b) { std::fill(pc + a, pc + b, 0.); });
   h->p_mat.resize(n);
   parallel_for(n, [&](int64_t a, int64_t b) {
+    int32_t last_id = 0;
+    int last_slot = -1;  // runs of one material look the map up once
     for (int64_t p = a; p < b; ++p) {
-      auto it = h->mat_index.find(in->material[p]);
-      if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
-      h->p_mat[p] = (uint16_t)it->second;
+      const int32_t id = in->material[p];
+      if (last_slot < 0 || id != last_id) {
+        auto it = h->mat_index.find(id);
+        if (it == h->mat_index.end()) throw InvalidArg("unknown material id");
+        last_id = id;
+        last_slot = it->second;
+      }
+      h->p_mat[p] = (uint16_t)last_slot;
     }
   });
   h->p_vc.clear();
