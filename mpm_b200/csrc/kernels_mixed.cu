@@ -32,7 +32,10 @@
 #include "mpm_state.cuh"
 
 #ifndef MPM_MIXED_G2P_MIN_BLOCKS
-#define MPM_MIXED_G2P_MIN_BLOCKS 6  // 80 registers, no spills: 0.478 -> 0.374 ms (4M, 3D)
+// 80 registers: 0.478 -> 0.374 ms (4M, 3D).  7 and 8 blocks (72 / 64 registers, more
+// spills): early steps g2p 0.389 -> 0.377 / 0.379 ms, step at 2000 0.542 -> 0.545 /
+// 0.547 ms (1M column): no net gain over a run.
+#define MPM_MIXED_G2P_MIN_BLOCKS 6
 #endif
 #ifndef MPM_MIXED_AFFINE_G2P_MIN_BLOCKS
 #define MPM_MIXED_AFFINE_G2P_MIN_BLOCKS 4  // the nodal velocities stay in registers for B
