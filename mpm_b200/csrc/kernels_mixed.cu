@@ -130,7 +130,8 @@ __device__ __forceinline__ void cell_nodes_rel(const DevState& s, int c, int* ni
 
 // ---------------------------------------------------------------- P2G tiles
 // The FP64 path's cell tiles (k_p2g_tiles) in FP32: staged local coordinates
-// (the FP64 local coordinate rounded), mass, velocity, -V0 (1 + P), stress
+// (the FP64 local coordinate rounded), mass, velocity, the stress times the
+// particle's -V0 (1 + P)
 // and, off a tensor-product grid, J^-1; per (cell, slot) thread 1 + 2 DIM
 // FP64 sums (mass, momentum, internal force; the body force is formed by the
 // node update) of the FP32 contributions of the cell's particles in id order,
@@ -143,8 +144,7 @@ struct MTileRows {
   static constexpr bool MM = MODE != 1, FORCES = MODE != 0;
   static constexpr int XI = 0, M = DIM;  // the mass row only with mass and momentum
   static constexpr int V = M + (MM ? 1 : 0);
-  static constexpr int SC = V + (MM ? DIM : 0);
-  static constexpr int S = SC + 1;
+  static constexpr int S = V + (MM ? DIM : 0);  // stress times -V0 (1 + P)
   static constexpr int INV = S + (FORCES ? PF<DIM>::NS : 0);
   static constexpr int XP = INV + (FORCES && !BOX ? DIM * DIM : 0);  // x - node 0
   static constexpr int MV = XP + (MM && AFF ? DIM : 0);              // mapping matrix
@@ -208,9 +208,9 @@ __device__ __forceinline__ void p2g_tile_mixed(const DevState& s, int64_t bx) {
       for (int q = 0; q < DIM * DIM; ++q) rows[RW::MV + q][r] = (float)Mv[q];
     }
     if constexpr (FORCES) {
-      rows[RW::SC][r] = -(pmf<DIM>(s, PM<DIM>::V0, p) * (1.f + pmf<DIM>(s, PM<DIM>::JP, p)));
+      const float sc = -(pmf<DIM>(s, PM<DIM>::V0, p) * (1.f + pmf<DIM>(s, PM<DIM>::JP, p)));
 #pragma unroll
-      for (int q = 0; q < PF<DIM>::NS; ++q) rows[RW::S + q][r] = pmf<DIM>(s, PM<DIM>::S + q, p);
+      for (int q = 0; q < PF<DIM>::NS; ++q) rows[RW::S + q][r] = sc * pmf<DIM>(s, PM<DIM>::S + q, p);
       if constexpr (!BOX) {
         int nid[NV];
         float Xr[NV * DIM];
@@ -264,7 +264,6 @@ __device__ __forceinline__ void p2g_tile_mixed(const DevState& s, int64_t bx) {
       for (int d = 0; d < DIM; ++d) acc[MOM + d] += (double)(mN * mv[d]);
     }
     if constexpr (FORCES) {
-      const float sc = rows[RW::SC][r];
       float sig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
       for (int q = 0; q < PF<DIM>::NS; ++q) sig[q] = rows[RW::S + q][r];
@@ -287,7 +286,7 @@ __device__ __forceinline__ void p2g_tile_mixed(const DevState& s, int64_t bx) {
         f[2] = Dn[2] * sig[2] + Dn[1] * sig[4] + Dn[0] * sig[5];
       }
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) acc[FINT + d] += (double)(f[d] * sc);
+      for (int d = 0; d < DIM; ++d) acc[FINT + d] += (double)f[d];
     }
   };
   // each cell's particle ids in ascending order in the first mapping of a step
