@@ -225,7 +225,8 @@ int mpm_gpu_autotune(mpm_gpu_t h, int64_t steps, char* report, size_t report_len
 
 /* Persistent steps (the batched form's one-launch step; no counterpart in the
  * reference): with steps_per_launch > 0, mpm_gpu_step advances up to that
- * many whole steps per cooperative kernel launch, every block resident, the
+ * many whole steps per cooperative kernel launch (after the first launch of a
+ * call, launches of that many steps replay a captured CUDA graph), every block resident, the
  * passes of a step (sort, P2G, node update, G2P and stress, plastic returns,
  * exhaustive locate) separated by grid barriers with bounded waits
  * (MPM_ERR_TIMEOUT when one runs out); 0 returns to one launch per pass,
@@ -235,6 +236,10 @@ int mpm_gpu_autotune(mpm_gpu_t h, int64_t steps, char* report, size_t report_len
  * otherwise: here for the configuration, at mpm_gpu_step for the mesh and
  * sensitivities); per-kernel profiling steps run per pass. */
 int mpm_gpu_set_persistent(mpm_gpu_t h, int32_t steps_per_launch);
+/* The steps per persistent launch in use (0: off) and whether its launches of
+ * that many steps replay a captured CUDA graph (1) or are launched directly (0:
+ * none captured yet, or the capture was not possible). */
+int mpm_gpu_get_persistent(mpm_gpu_t h, int32_t* steps_per_launch, int32_t* graph_replayed);
 
 /* Per-kernel device timing (CUDA events around every launch on the solver's
  * stream).  Enabling or disabling resets the counters.  Kernel indices run

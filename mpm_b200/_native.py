@@ -62,6 +62,7 @@ SIGNATURES = {
     "mpm_gpu_step_timed": (C.c_int, [_vp, C.c_int64, _pd]),
     "mpm_gpu_set_launch_shape": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32]),
     "mpm_gpu_set_persistent": (C.c_int, [_vp, C.c_int32]),
+    "mpm_gpu_get_persistent": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "mpm_gpu_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(C.c_void_p)]),
     "mpm_gpu_host_free": (C.c_int, [C.c_void_p]),
     "mpm_gpu_get_launch_shape": (C.c_int, [_vp, C.POINTER(C.c_int32)]),

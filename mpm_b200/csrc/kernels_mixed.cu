@@ -1270,19 +1270,21 @@ __global__ void __launch_bounds__(MSTAGE_T, DIM == 2 ? MPM_PERSISTENT_MIN_BLOCKS
   const int64_t pblocks = (np + T - 1) / T, tiles = (nc + T / NV - 1) / (T / NV);
   const int64_t nodeblocks = (s.nn + T - 1) / T, chunks = (nc + SCAN_BLOCK - 1) / SCAN_BLOCK;
   const unsigned gi = blockIdx.x * T + t, gs = G * T;  // grid-stride start and stride
+  __shared__ long long step0;
   unsigned gen = 0;
   if (t == 0) {
     bulk::mbar_init(&bar[0], 1);
     bulk::mbar_init(&bar[1], 1);
     bulk::fence_barrier_init();
     gen = ld_acquire_gpu(&q.barrier[1]);
+    step0 = *q.step;  // block 0 advances it only after the last barrier
   }
   for (int64_t i = gi; i < nc; i += gs) s.cnt[i] = 0;
   if (!grid_barrier(s, q.barrier, G, gen, go)) return;
   unsigned parity = 0;
   for (int64_t k = 0; k < q.nsteps; ++k) {
     double gm = 1.0;  // the host's ramp, the same operations
-    if (q.ramp > 0.0) gm = fmin(1.0, static_cast<double>(q.step0 + k) * a.dt / q.ramp);
+    if (q.ramp > 0.0) gm = fmin(1.0, static_cast<double>(step0 + k) * a.dt / q.ramp);
     const double g[3] = {gm * q.gravity[0], gm * q.gravity[1], gm * q.gravity[2]};
     // counting sort
     if (blockIdx.x == 0 && t == 0) {
@@ -1327,6 +1329,7 @@ __global__ void __launch_bounds__(MSTAGE_T, DIM == 2 ? MPM_PERSISTENT_MIN_BLOCKS
       if (!grid_barrier(s, q.barrier, G, gen, go)) return;
     }
   }
+  if (blockIdx.x == 0 && t == 0) *q.step = step0 + q.nsteps;
 }
 
 template <int DIM, bool FLIP>

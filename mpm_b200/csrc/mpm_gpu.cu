@@ -350,7 +350,8 @@ struct mpm_gpu_solver {
   DevBuf<uint8_t> d_active;
   DevBuf<int16_t> d_pvc;
   DevBuf<CellGeom> d_geom;
-  DevBuf<unsigned> d_words;  // [0] nlost, [1] err, [2] nplastic, [3] nplastic_heavy, [4, 6) grid barrier
+  DevBuf<unsigned> d_words;  // [0] nlost, [1] err, [2] nplastic, [3] nplastic_heavy, [4, 6) grid barrier,
+                             // [6, 8) the persistent launches' step counter (int64)
   DevBuf<int32_t> d_plist;
   DevBuf<double> d_pbuf;
   DevBuf<uint8_t> d_rpass;
@@ -392,6 +393,12 @@ struct mpm_gpu_solver {
   // one captured step, replayed while the device state and step arguments
   // stay the same
   cudaGraphExec_t graph = nullptr;
+  // the persistent launch of persistent_steps steps, captured (its state, arguments)
+  cudaGraphExec_t pgraph = nullptr;
+  DevState pgraph_state{};
+  StepArgs pgraph_args{};
+  int64_t pgraph_steps = 0;
+  bool pgraph_ok = true;
   DevState graph_state{};
   StepArgs graph_args{};
   int64_t graph_launches = 0;
@@ -747,8 +754,8 @@ void upload_mesh(mpm_gpu_t h) {
   h->d_active.alloc(h->nnodes);
   ck(cudaMemsetAsync(h->d_active.p, 0, h->nnodes, st), "memset");
   ck(cudaMemsetAsync(h->d_nf.p, 0, sizeof(double) * h->nnf() * h->nnodes, st), "memset");
-  h->d_words.alloc(6);
-  ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 6, st), "memset");
+  h->d_words.alloc(8);
+  ck(cudaMemsetAsync(h->d_words.p, 0, sizeof(unsigned) * 8, st), "memset");
   if (h->structured)
     for (int d = 0; d < 3; ++d) {
       h->d_axis[d].upload(h->axis[d].data(), h->axis[d].size(), st);
@@ -1377,6 +1384,7 @@ int mpm_gpu_destroy(mpm_gpu_t h) {
   for (auto& e : h->stage_ev)
     if (e) cudaEventDestroy(e);
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->pgraph) cudaGraphExecDestroy(h->pgraph);
   delete h;
   return MPM_OK;
 }
@@ -1800,10 +1808,49 @@ static int run_steps(mpm_gpu_t h, int64_t nsteps, double* elapsed_ms) {
     for (int d = 0; d < 3; ++d) q.gravity[d] = d < h->dim ? h->cfg.gravity[d] : 0.;
     q.ramp = h->cfg.gravity_ramping_time;
     q.barrier = h->d_words.p + 4;
+    q.step = reinterpret_cast<long long*>(h->d_words.p + 6);
+    const long long step_now = h->step;  // each launch advances the device copy
+    ck(cudaMemcpyAsync(q.step, &step_now, sizeof(step_now), cudaMemcpyHostToDevice, h->stream), "H2D");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    // Launches of persistent_steps steps replay one captured CUDA graph (the
+    // barrier reset and the cooperative launch); the first launch of a call
+    // and a shorter last one run directly.
+    bool eager_done_p = false;
     for (int64_t s = 0; s < nsteps; s += q.nsteps) {
       q.nsteps = std::min<int64_t>(h->persistent_steps, nsteps - s);
-      q.step0 = h->step;
-      ck(launch_steps_persistent_mixed(h->dim, h->ds, a, q, h->stream), "persistent step launch");
+      bool launched = false;
+      if (q.nsteps == h->persistent_steps && eager_done_p && h->pgraph_ok) {
+        if (!(h->pgraph && h->pgraph_steps == q.nsteps && same_step(h->pgraph_state, h->ds, h->pgraph_args, a))) {
+          if (h->pgraph) cudaGraphExecDestroy(h->pgraph);
+          h->pgraph = nullptr;
+          cudaGraph_t g = nullptr;
+          bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+          if (ok) {
+            const cudaError_t le = launch_steps_persistent_mixed(h->dim, h->ds, a, q, h->stream);
+            ok = cudaStreamEndCapture(h->stream, &g) == cudaSuccess && le == cudaSuccess && g != nullptr;
+            ok = ok && cudaGraphInstantiate(&h->pgraph, g, 0) == cudaSuccess;
+            if (g) cudaGraphDestroy(g);
+          }
+          if (ok) {
+            h->pgraph_state = h->ds;
+            h->pgraph_args = a;
+            h->pgraph_steps = q.nsteps;
+          } else {  // no capture of the cooperative launch here: direct launches from now on
+            cudaGetLastError();
+            if (h->pgraph) cudaGraphExecDestroy(h->pgraph);
+            h->pgraph = nullptr;
+            h->pgraph_ok = false;
+          }
+        }
+        if (h->pgraph) {
+          ck(cudaGraphLaunch(h->pgraph, h->stream), "cudaGraphLaunch");
+          launched = true;
+        }
+      }
+      if (!launched) {
+        ck(launch_steps_persistent_mixed(h->dim, h->ds, a, q, h->stream), "persistent step launch");
+        eager_done_p = true;
+      }
       h->prof.launches += 1;
       h->step += q.nsteps;
     }
@@ -1906,6 +1953,15 @@ int mpm_gpu_set_persistent(mpm_gpu_t h, int32_t steps_per_launch) {
       (!h->mixed || h->cfg.scheme != MPM_SCHEME_USL || h->cfg.velocity_update > MPM_VELOCITY_PIC))
     return fail(h, MPM_ERR_UNSUPPORTED, "persistent steps run the mixed USL step with FLIP or PIC");
   h->persistent_steps = steps_per_launch;
+  MPM_END(h)
+  return MPM_OK;
+}
+
+int mpm_gpu_get_persistent(mpm_gpu_t h, int32_t* steps_per_launch, int32_t* graph_replayed) {
+  MPM_GUARD(h)
+  if (!steps_per_launch || !graph_replayed) throw InvalidArg("null output");
+  *steps_per_launch = h->persistent_steps;
+  *graph_replayed = h->pgraph != nullptr && h->pgraph_steps == h->persistent_steps ? 1 : 0;
   MPM_END(h)
   return MPM_OK;
 }

@@ -87,11 +87,13 @@ void launch_step_mixed(int dim, const DevState& s, const StepArgs& a, cudaStream
 // The persistent form of the mixed USL step (FLIP or PIC, tensor-product
 // grid): one cooperative launch runs `nsteps` whole steps, the passes of
 // which are separated by grid barriers.  a.g is ignored: the gravity of step
-// k is the ramp of step0 + k applied to `gravity` (mpm_explicit.tcc:145-153).
-// `barrier` holds two words of device memory.  Returns the launch's error.
+// k is the ramp of *step + k applied to `gravity` (mpm_explicit.tcc:145-153),
+// and the launch advances *step (device memory) by nsteps, so that a launch
+// captured in a CUDA graph replays for any step.  `barrier` holds two words
+// of device memory.  Returns the launch's error.
 struct PersistentArgs {
   int64_t nsteps;
-  int64_t step0;
+  long long* step;
   double gravity[3];
   double ramp;  // gravity ramping time (0: none)
   unsigned* barrier;

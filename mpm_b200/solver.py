@@ -178,6 +178,13 @@ class Solver:
         replayed from a CUDA graph.  Bit for bit the same results."""
         self._ck(self.L.mpm_gpu_set_persistent(self.h, int(steps_per_launch)))
 
+    def persistent(self):
+        """(steps per persistent launch, 0 when off; whether those launches
+        replay a captured CUDA graph)."""
+        n, g = C.c_int32(), C.c_int32()
+        self._ck(self.L.mpm_gpu_get_persistent(self.h, C.byref(n), C.byref(g)))
+        return n.value, bool(g.value)
+
     def launch_shape(self):
         """(p2g_tile, node_threads, return_blocks_per_sm) in use."""
         out = (C.c_int32 * 3)()

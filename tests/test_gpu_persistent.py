@@ -80,6 +80,20 @@ def test_packed_ensemble_bitwise():
     _assert_same(g, p, "ensemble")
 
 
+def test_full_launches_replay_a_captured_graph():
+    """After the first launch of a call, launches of steps_per_launch steps
+    replay one captured CUDA graph (barrier reset + cooperative launch) whose
+    kernel reads the step from device memory: bitwise the per-pass result."""
+    prob = P.column_3d(shape=(20, 10, 10), block=(10, 10, 10), scheme="usl")
+    prob.analysis["gravity_ramping_time"] = 3e-5  # the ramp spans the first 15 steps
+    g, p = _both(prob, [20, 20], 4)
+    _assert_same(g, p, "graph-replayed persistent launches")
+    s = P.build_solver(prob, precision="mixed")
+    s.set_persistent(4)
+    s.step(12)
+    assert s.persistent() == (4, True)
+
+
 @pytest.mark.parametrize("over", [dict(precision="fp64"), dict(scheme="usf"), dict(scheme="musl"),
                                   dict(velocity_update="apic")])
 def test_other_configurations_are_refused(over):
