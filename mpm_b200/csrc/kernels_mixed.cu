@@ -54,7 +54,10 @@
 #define MPM_PERSISTENT_MIN_BLOCKS_2D 8
 #endif
 #ifndef MPM_MIXED_P2G_TILE_MIN_BLOCKS
-#define MPM_MIXED_P2G_TILE_MIN_BLOCKS 5  // 48 registers, small spills: 0.32 -> 0.26 ms (4M, 3D)
+// 48 registers, small spills: 0.32 -> 0.26 ms (4M, 3D); against 4 and 6 (64 / 40
+// registers) with the body force at the node: 128-thread tiles 0.193 vs 0.206 / 0.203
+// ms, 256-thread tiles 0.216 vs 0.237 / 0.227 ms.
+#define MPM_MIXED_P2G_TILE_MIN_BLOCKS 5
 #endif
 
 namespace mpm_b200 {
