@@ -47,6 +47,11 @@
 // steps per launch, ms per step on the 4M-particle column / the 512-slope
 // ensemble: 4 blocks 1.303 / 3.018, 6 blocks 1.128 / 2.382, 8 blocks 1.161 /
 // 2.047 (per-pass launches: 0.748 / 1.555).
+#ifndef MPM_MIXED_NODES_MIN_BLOCKS
+// 256-thread blocks, 32 registers; 6 and 4 blocks (40 / 64 registers), 4M column:
+// 0.048 / 0.054 ms against 0.049 ms
+#define MPM_MIXED_NODES_MIN_BLOCKS 8
+#endif
 #ifndef MPM_PERSISTENT_MIN_BLOCKS_3D
 #define MPM_PERSISTENT_MIN_BLOCKS_3D 6
 #endif
@@ -444,7 +449,7 @@ __device__ __forceinline__ void node_update_mixed(const DevState& s, double dt, 
 }
 
 template <int DIM, int MODE>
-__global__ void __launch_bounds__(256, 8) k_nodes_mixed(DevState s, double dt, double damping, double g0,
+__global__ void __launch_bounds__(256, MPM_MIXED_NODES_MIN_BLOCKS) k_nodes_mixed(DevState s, double dt, double damping, double g0,
                                                         double g1, double g2) {
   const double g[3] = {g0, g1, g2};
   node_update_mixed<DIM, MODE>(s, dt, damping, g, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
